@@ -1,0 +1,34 @@
+"""CPU oracle for the PCG hot path -- TEST INFRASTRUCTURE ONLY.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline legs import
+this package, as the checker (and, in bench.py, as the timed CPU reference).
+The product library ba_b200 never imports it.
+
+Two checkers:
+* ``liboracle.so``: the C restatement in pcg_oracle.c (CG<LAD>, lmp cg(),
+  IterateControl, CSR SpMV, BLAS-1, Jacobi, MPIR-style refinement);
+* ``_ref/libhiflow_lmp_ref.so``: HiFlow3's own lmp CPU sources (NAIVE and
+  OPENMP implementations, lPreconditioner_Jacobi, lmp cg()) compiled by
+  oracle/ref/Makefile, with a driver restating CG<LAD> over those objects.
+"""
+from .oracle import (  # noqa: F401
+    CTRL_FAIL_DIV,
+    CTRL_FAIL_MAXITS,
+    CTRL_ITERATE,
+    CTRL_SUCCESS_ABS,
+    CTRL_SUCCESS_REL,
+    IMPL_NAIVE,
+    IMPL_OPENMP,
+    OracleResult,
+    cg,
+    dot,
+    invdiag,
+    iterate_check,
+    lmp_cg,
+    mpir,
+    ref_available,
+    ref_cg,
+    ref_lmp_cg,
+    ref_spmv,
+    spmv,
+)

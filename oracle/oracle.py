@@ -1,0 +1,218 @@
+"""ctypes bindings of the CPU oracle -- TEST INFRASTRUCTURE ONLY.
+
+See pcg_oracle.c (restatement) and ref/ref_driver.cc (reference sources).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+_REF_PATH = os.path.join(_HERE, "_ref", "libhiflow_lmp_ref.so")
+
+CTRL_ITERATE, CTRL_SUCCESS_ABS, CTRL_SUCCESS_REL, CTRL_FAIL_DIV, CTRL_FAIL_MAXITS = range(5)
+IMPL_NAIVE, IMPL_OPENMP = 0, 1
+
+_lib = None
+_ref = None
+
+_i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_ip = C.POINTER(C.c_int)
+_dp = C.POINTER(C.c_double)
+
+
+def _load():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            raise RuntimeError(f"oracle not built: {_LIB_PATH} (run `make -C oracle`)")
+        lib = C.CDLL(_LIB_PATH)
+        for s, fp in (("d", _f64p), ("f", _f32p)):
+            T = C.c_double if s == "d" else C.c_float
+            getattr(lib, f"orc_spmv_{s}").argtypes = [C.c_int, _i32p, _i32p, fp, fp, fp]
+            getattr(lib, f"orc_dot_{s}").argtypes = [C.c_int, fp, fp]
+            getattr(lib, f"orc_dot_{s}").restype = T
+            getattr(lib, f"orc_invdiag_{s}").argtypes = [C.c_int, _i32p, _i32p, fp, fp]
+            getattr(lib, f"orc_cg_{s}").argtypes = [
+                C.c_int, _i32p, _i32p, fp, fp, fp, C.c_int, C.c_double, C.c_double,
+                C.c_double, C.c_int, fp, fp, _ip, _dp, _dp]
+            getattr(lib, f"orc_lmp_cg_{s}").argtypes = [
+                C.c_int, _i32p, _i32p, fp, fp, fp, T, T, _ip, fp]
+        lib.orc_iterate_check.argtypes = [C.c_int, C.c_double, C.c_int, C.c_double, C.c_double,
+                                          C.c_double, _dp]
+        lib.orc_mpir_d.argtypes = [C.c_int, _i32p, _i32p, _f64p, _f32p, _f64p, _f64p, C.c_int,
+                                   C.c_double, C.c_double, C.c_int, _f64p, _f32p, _f64p, _f32p,
+                                   _ip, _ip, _dp, _dp]
+        _lib = lib
+    return _lib
+
+
+def ref_available() -> bool:
+    return os.path.exists(_REF_PATH)
+
+
+def _load_ref():
+    global _ref
+    if _ref is None:
+        if not ref_available():
+            raise RuntimeError(f"reference checker not built: {_REF_PATH} (run `make -C oracle`)")
+        lib = C.CDLL(_REF_PATH)
+        for s, fp in (("d", _f64p), ("f", _f32p)):
+            getattr(lib, f"ref_spmv_{s}").argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _i32p, _i32p,
+                                                     fp, fp, fp]
+            getattr(lib, f"ref_cg_solve_{s}").argtypes = [
+                C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _i32p, _i32p, fp, fp, fp, C.c_int,
+                C.c_double, C.c_double, C.c_double, _ip, _dp, _dp, _dp]
+        lib.ref_lmp_cg_d.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f64p, _f64p,
+                                     _f64p, C.c_double, C.c_double, _ip]
+        _ref = lib
+    return _ref
+
+
+def _sfx(dtype) -> tuple[str, type]:
+    dt = np.dtype(dtype)
+    if dt == np.float64:
+        return "d", np.float64
+    if dt == np.float32:
+        return "f", np.float32
+    raise TypeError(f"unsupported dtype {dt}")
+
+
+def _csr(rowptr, col, val, dtype):
+    return (np.ascontiguousarray(rowptr, np.int32), np.ascontiguousarray(col, np.int32),
+            np.ascontiguousarray(val, dtype))
+
+
+@dataclass
+class OracleResult:
+    x: np.ndarray
+    iters: int
+    res: float
+    res_init: float
+    state: int
+
+    @property
+    def res_rel(self) -> float:
+        return self.res / self.res_init if self.res_init > 0 else 0.0
+
+
+def iterate_check(step: int, value: float, maxits: int, atol: float, rtol: float, dtol: float,
+                  first: float) -> tuple[int, float]:
+    f = C.c_double(first)
+    st = _load().orc_iterate_check(step, value, maxits, atol, rtol, dtol, C.byref(f))
+    return st, f.value
+
+
+def spmv(rowptr, col, val, x, dtype=np.float64) -> np.ndarray:
+    s, T = _sfx(dtype)
+    rp, c, v = _csr(rowptr, col, val, T)
+    n = rp.shape[0] - 1
+    y = np.empty(n, T)
+    getattr(_load(), f"orc_spmv_{s}")(n, rp, c, v, np.ascontiguousarray(x, T), y)
+    return y
+
+
+def dot(a, b, dtype=np.float64) -> float:
+    s, T = _sfx(dtype)
+    a = np.ascontiguousarray(a, T)
+    return float(getattr(_load(), f"orc_dot_{s}")(a.shape[0], a, np.ascontiguousarray(b, T)))
+
+
+def invdiag(rowptr, col, val, dtype=np.float64) -> np.ndarray:
+    s, T = _sfx(dtype)
+    rp, c, v = _csr(rowptr, col, val, T)
+    n = rp.shape[0] - 1
+    out = np.empty(n, T)
+    bad = getattr(_load(), f"orc_invdiag_{s}")(n, rp, c, v, out)
+    if bad >= 0:
+        raise ValueError(f"row {bad} has no nonzero diagonal")
+    return out
+
+
+def cg(rowptr, col, val, b, x0=None, *, maxits=1000, atol=1e-12, rtol=1e-8, dtol=1e8,
+       precond=True, dtype=np.float64) -> OracleResult:
+    """CG<LAD>::SolvePrecond (precond) / SolveNoPrecond restated in C."""
+    s, T = _sfx(dtype)
+    rp, c, v = _csr(rowptr, col, val, T)
+    n = rp.shape[0] - 1
+    x = np.zeros(n, T) if x0 is None else np.array(x0, T)
+    inv = invdiag(rp, c, v, T) if precond else np.zeros(1, T)
+    work = np.empty(5 * n, T)
+    it, res, res0 = C.c_int(), C.c_double(), C.c_double()
+    st = getattr(_load(), f"orc_cg_{s}")(n, rp, c, v, np.ascontiguousarray(b, T), x, int(maxits),
+                                         atol, rtol, dtol, int(bool(precond)), inv, work,
+                                         C.byref(it), C.byref(res), C.byref(res0))
+    return OracleResult(x, it.value, res.value, res0.value, st)
+
+
+def lmp_cg(rowptr, col, val, b, x0=None, *, rel_eps=1e-10, abs_eps=0.0, max_iter=10000,
+           dtype=np.float64) -> OracleResult:
+    """lmp cg() restated in C; iters is cg()'s returned max_iter."""
+    s, T = _sfx(dtype)
+    rp, c, v = _csr(rowptr, col, val, T)
+    n = rp.shape[0] - 1
+    x = np.zeros(n, T) if x0 is None else np.array(x0, T)
+    mi = C.c_int(int(max_iter))
+    getattr(_load(), f"orc_lmp_cg_{s}")(n, rp, c, v, np.ascontiguousarray(b, T), x, rel_eps,
+                                        abs_eps, C.byref(mi), np.empty(3 * n, T))
+    return OracleResult(x, mi.value, float("nan"), float("nan"), 0)
+
+
+def mpir(rowptr, col, val, b, *, rtol=1e-10, inner_rtol=1e-4, inner_maxits=100000,
+         max_outer=50) -> tuple[OracleResult, int]:
+    """FP64 refinement around a float Jacobi-PCG (MPIR structure)."""
+    rp, c, v = _csr(rowptr, col, val, np.float64)
+    v32 = v.astype(np.float32)
+    n = rp.shape[0] - 1
+    x = np.zeros(n, np.float64)
+    inv = invdiag(rp, c, v, np.float64)
+    inv32 = invdiag(rp, c, v32, np.float32)
+    outer, inner, res, res0 = C.c_int(), C.c_int(), C.c_double(), C.c_double()
+    st = _load().orc_mpir_d(n, rp, c, v, v32, np.ascontiguousarray(b, np.float64), x, max_outer,
+                            rtol, inner_rtol, inner_maxits, inv, inv32, np.empty(3 * n),
+                            np.empty(8 * n, np.float32), C.byref(outer), C.byref(inner),
+                            C.byref(res), C.byref(res0))
+    return OracleResult(x, inner.value, res.value, res0.value, st), outer.value
+
+
+def ref_spmv(rowptr, col, val, x, *, impl=IMPL_NAIVE, nthreads=1, dtype=np.float64) -> np.ndarray:
+    """CPUsimple/CPUopenmp_CSR_lMatrix::VectorMult from the reference sources."""
+    s, T = _sfx(dtype)
+    rp, c, v = _csr(rowptr, col, val, T)
+    n = rp.shape[0] - 1
+    y = np.empty(n, T)
+    getattr(_load_ref(), f"ref_spmv_{s}")(impl, nthreads, n, c.shape[0], rp, c, v,
+                                          np.ascontiguousarray(x, T), y)
+    return y
+
+
+def ref_cg(rowptr, col, val, b, x0=None, *, maxits=1000, atol=1e-12, rtol=1e-8, dtol=1e8,
+           precond=True, impl=IMPL_NAIVE, nthreads=1, dtype=np.float64) -> OracleResult:
+    """CG<LAD> restated over the reference's compiled lmp objects."""
+    s, T = _sfx(dtype)
+    rp, c, v = _csr(rowptr, col, val, T)
+    n = rp.shape[0] - 1
+    x = np.zeros(n, T) if x0 is None else np.array(x0, T)
+    it, res, res0, rel = C.c_int(), C.c_double(), C.c_double(), C.c_double()
+    st = getattr(_load_ref(), f"ref_cg_solve_{s}")(
+        impl, nthreads, int(bool(precond)), n, c.shape[0], rp, c, v, np.ascontiguousarray(b, T), x,
+        int(maxits), atol, rtol, dtol, C.byref(it), C.byref(res), C.byref(res0), C.byref(rel))
+    return OracleResult(x, it.value, res.value, res0.value, st)
+
+
+def ref_lmp_cg(rowptr, col, val, b, x0=None, *, rel_eps=1e-10, abs_eps=0.0, max_iter=10000,
+               impl=IMPL_NAIVE, nthreads=1) -> OracleResult:
+    """The reference's own lmp cg() (lmp/solvers/cg.cc:35)."""
+    rp, c, v = _csr(rowptr, col, val, np.float64)
+    n = rp.shape[0] - 1
+    x = np.zeros(n) if x0 is None else np.array(x0, np.float64)
+    mi = C.c_int(int(max_iter))
+    _load_ref().ref_lmp_cg_d(impl, nthreads, n, c.shape[0], rp, c, v,
+                             np.ascontiguousarray(b, np.float64), x, rel_eps, abs_eps, C.byref(mi))
+    return OracleResult(x, mi.value, float("nan"), float("nan"), 0)

@@ -1,0 +1,231 @@
+/*
+ * CPU oracle for the PCG hot path -- TEST INFRASTRUCTURE ONLY.
+ *
+ * A plain-C restatement of HiFlow3's CPU algorithms for the Jacobi-PCG path,
+ * used by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg as
+ * the checker.  The product library (ba_b200/) never links or calls this.
+ * Built by oracle/Makefile into oracle/liboracle.so.
+ *
+ * Parity is pinned in two ways: against the known answers in the reference's
+ * own tests (tests/cg_test.cc:92-94, tests/lmp_test.cc:80-82,
+ * tests/cuda_test.cc:76-78; committed as tests/golden/), and against the
+ * reference's own lmp sources compiled into oracle/_ref/ (oracle/ref/).
+ *
+ * Every routine is instantiated for double (suffix _d) and float (suffix _f);
+ * arithmetic and accumulation happen in that type, as in the reference's
+ * templates.
+ */
+#include <math.h>
+#include <stddef.h>
+#include <stdint.h>
+
+/* IterateControl states, numbered as the B200 library's solver status. */
+enum { CTRL_ITERATE = 0, CTRL_SUCCESS_ABS = 1, CTRL_SUCCESS_REL = 2,
+       CTRL_FAIL_DIV = 3, CTRL_FAIL_MAXITS = 4 };
+
+/* IterateControl::Check (common/iterate_control.cc:80-107): the first call
+ * (step 0) records the initial residual; success if res <= atol or
+ * res < rtol * res0 (strict); divergence if res > dtol * res0; failure once
+ * step >= maxits. */
+int orc_iterate_check(int step, double value, int maxits, double atol,
+                      double rtol, double dtol, double *first_value) {
+  if (step == 0) *first_value = value;
+  if (value <= atol) return CTRL_SUCCESS_ABS;
+  if (value < rtol * (*first_value)) return CTRL_SUCCESS_REL;
+  if (value > dtol * (*first_value)) return CTRL_FAIL_DIV;
+  if (step >= maxits) return CTRL_FAIL_MAXITS;
+  return CTRL_ITERATE;
+}
+
+#define ORACLE_INSTANTIATE(T, S, SQRT)                                            \
+  /* CPUsimple_CSR_lMatrix::VectorMult (lmp/CPUsimple_csr_lmatrix.cc:92-111):  \
+   * y_i = sum_j val[j] * x[col[j]] in stored order, accumulated in T. */      \
+  void orc_spmv_##S(int n, const int *rowptr, const int *col, const T *val,    \
+                    const T *x, T *y) {                                        \
+    for (int i = 0; i < n; ++i) {                                              \
+      T res = 0;                                                               \
+      for (int j = rowptr[i]; j != rowptr[i + 1]; ++j)                         \
+        res += val[j] * x[col[j]];                                             \
+      y[i] = res;                                                              \
+    }                                                                          \
+  }                                                                            \
+  /* CPUsimple_lVector::Dot (lmp/CPUsimple_lvector.cc:162-222): that file     \
+   * defines CLANG_VECTORIZE (:29), so the sum is one accumulator fed first    \
+   * with the n % 5 leading products one by one, then with groups of five      \
+   * products each summed left to right before being added. */                \
+  T orc_dot_##S(int n, const T *a, const T *b) {                               \
+    T acc = 0;                                                                 \
+    const int m = n % 5;                                                       \
+    for (int i = 0; i < m; ++i) acc += a[i] * b[i];                            \
+    for (int i = m; i + 4 < n; i += 5)                                         \
+      acc += a[i] * b[i] + a[i + 1] * b[i + 1] + a[i + 2] * b[i + 2] +         \
+             a[i + 3] * b[i + 3] + a[i + 4] * b[i + 4];                        \
+    return acc;                                                                \
+  }                                                                            \
+  /* CPUsimple_lVector::Axpy (lmp/CPUsimple_lvector.cc:254-310):               \
+   * this += scalar * vec. */                                                  \
+  void orc_axpy_##S(int n, T *y, const T *x, T alpha) {                        \
+    for (int i = 0; i < n; ++i) y[i] += alpha * x[i];                          \
+  }                                                                            \
+  /* CPUsimple_lVector::ScaleAdd (lmp/CPUsimple_lvector.cc:329-395):           \
+   * this = scalar * this + vec. */                                            \
+  void orc_scaleadd_##S(int n, T *y, T scalar, const T *x) {                   \
+    for (int i = 0; i < n; ++i) y[i] = scalar * y[i] + x[i];                   \
+  }                                                                            \
+  /* CPU_lVector::ElementWiseMult (lmp/lvector_cpu.cc:485-493). */             \
+  void orc_ewmult_##S(int n, T *y, const T *x) {                               \
+    for (int i = 0; i < n; ++i) y[i] *= x[i];                                  \
+  }                                                                            \
+  /* CPU_CSR_lMatrix::extract_invdiagelements (lmp/lmatrix_csr_cpu.cc:         \
+   * 2426-2441): inv_D[i] = 1 / a_ii, a_ii the first stored entry of row i     \
+   * whose column is i (diag_ptr_).  Returns the first row without a nonzero   \
+   * diagonal, or -1. */                                                       \
+  int orc_invdiag_##S(int n, const int *rowptr, const int *col, const T *val,  \
+                      T *invd) {                                               \
+    for (int i = 0; i < n; ++i) {                                              \
+      int k = -1;                                                              \
+      for (int j = rowptr[i]; j < rowptr[i + 1]; ++j)                          \
+        if (col[j] == i) { k = j; break; }                                     \
+      if (k < 0 || val[k] == 0) return i;                                      \
+      invd[i] = (T)(1. / val[k]);                                              \
+    }                                                                          \
+    return -1;                                                                 \
+  }                                                                            \
+  /* CG<LAD>::SolveNoPrecond / SolvePrecond (linear_solver/cg.h:87-246) on one \
+   * rank, with the block-Jacobi(Jacobi) preconditioner                        \
+   * (lmp/lpreconditioner.cc:184-200: z = copy(r) .* inv_D).  work must hold   \
+   * 4n (no precond) or 5n (Jacobi) values.  Returns the IterateControl        \
+   * state; iters/res/res_init follow CG's iter_/res_/res_init_. */            \
+  int orc_cg_##S(int n, const int *rowptr, const int *col, const T *val,       \
+                 const T *b, T *x, int maxits, double atol, double rtol,       \
+                 double dtol, int precond, const T *invd, T *work, int *iters, \
+                 double *res_out, double *res_init_out) {                      \
+    T *r = work, *p = work + n, *Ap = work + 2 * (size_t)n;                    \
+    T *z = work + 3 * (size_t)n;                                               \
+    T alpha, beta, gamma, ressq;                                               \
+    double res, first = 0.;                                                    \
+    int iter = 0, state;                                                       \
+    orc_spmv_##S(n, rowptr, col, val, x, r);                                   \
+    orc_scaleadd_##S(n, r, (T)-1., b);                                         \
+    ressq = orc_dot_##S(n, r, r);                                              \
+    res = (double)SQRT(ressq);                                                 \
+    *res_init_out = res;                                                       \
+    state = orc_iterate_check(iter, res, maxits, atol, rtol, dtol, &first);    \
+    if (precond) {                                                             \
+      for (int i = 0; i < n; ++i) z[i] = r[i];                                 \
+      orc_ewmult_##S(n, z, invd);                                              \
+      for (int i = 0; i < n; ++i) p[i] = z[i];                                 \
+      beta = orc_dot_##S(n, r, z);                                             \
+    } else {                                                                   \
+      for (int i = 0; i < n; ++i) p[i] = r[i];                                 \
+      beta = ressq;                                                            \
+    }                                                                          \
+    while (state == CTRL_ITERATE) {                                            \
+      ++iter;                                                                  \
+      orc_spmv_##S(n, rowptr, col, val, p, Ap);                                \
+      alpha = beta / orc_dot_##S(n, Ap, p);                                    \
+      orc_axpy_##S(n, x, p, alpha);                                            \
+      orc_axpy_##S(n, r, Ap, -alpha);                                          \
+      ressq = orc_dot_##S(n, r, r);                                            \
+      res = (double)SQRT(ressq);                                               \
+      state = orc_iterate_check(iter, res, maxits, atol, rtol, dtol, &first);  \
+      if (state != CTRL_ITERATE) break;                                        \
+      if (precond) {                                                           \
+        for (int i = 0; i < n; ++i) z[i] = r[i];                               \
+        orc_ewmult_##S(n, z, invd);                                            \
+        gamma = orc_dot_##S(n, r, z);                                          \
+        beta = gamma / beta;                                                   \
+        orc_scaleadd_##S(n, p, beta, z);                                       \
+        beta = gamma;                                                          \
+      } else {                                                                 \
+        beta = ressq / beta;                                                   \
+        orc_scaleadd_##S(n, p, beta, r);                                       \
+        beta = ressq;                                                          \
+      }                                                                        \
+    }                                                                          \
+    *iters = iter;                                                             \
+    *res_out = res;                                                            \
+    return state;                                                              \
+  }                                                                            \
+  /* lmp cg() / CGFunctor::operator() (lmp/solvers/cg.h:93-209): plain CG      \
+   * (the reference computes z but never uses it, cg.h:153 vs :157), stop on   \
+   * norm <= max(rel_eps * norm0, abs_eps) checked after each update; on exit  \
+   * max_iter holds the 0-based index of the breaking iteration (cg.h:201). */ \
+  int orc_lmp_cg_##S(int n, const int *rowptr, const int *col, const T *val,   \
+                     const T *b, T *x, T rel_eps, T abs_eps, int *max_iter,    \
+                     T *work) {                                                \
+    T *p = work, *q = work + n, *r = work + 2 * (size_t)n;                     \
+    for (int i = 0; i < n; ++i) p[i] = 0;                                      \
+    orc_spmv_##S(n, rowptr, col, val, x, r);                                   \
+    orc_scaleadd_##S(n, r, (T)-1.0, b);                                        \
+    T rho = orc_dot_##S(n, r, r);                                              \
+    T norm = SQRT(rho);                                             \
+    T beta = 0, rho_old;                                                       \
+    T crit = rel_eps * norm > abs_eps ? rel_eps * norm : abs_eps;              \
+    int iter = 0;                                                              \
+    for (; iter < *max_iter; ++iter) {                                         \
+      orc_scaleadd_##S(n, p, beta, r);                                         \
+      orc_spmv_##S(n, rowptr, col, val, p, q);                                 \
+      T alpha = rho / orc_dot_##S(n, p, q);                                    \
+      orc_axpy_##S(n, x, p, alpha);                                            \
+      orc_axpy_##S(n, r, q, -alpha);                                           \
+      rho_old = rho;                                                           \
+      rho = orc_dot_##S(n, r, r);                                              \
+      beta = rho / rho_old;                                                    \
+      norm = SQRT(rho);                                             \
+      if (norm <= crit) break;                                                 \
+    }                                                                          \
+    *max_iter = iter;                                                          \
+    return 0;                                                                  \
+  }
+
+ORACLE_INSTANTIATE(double, d, sqrt)
+ORACLE_INSTANTIATE(float, f, sqrtf)
+
+/*
+ * Mixed-precision iterative refinement around a float inner CG, structured
+ * like MPIR<LAD_high, LAD_low>::SolveImpl (linear_solver/mpir.cc:52-230)
+ * without smoothers: double residual r = b - A x; loop { cast r to float;
+ * float Jacobi-PCG on the float matrix from a zero start to inner_rtol; cast
+ * the correction to double; x += c; recompute the double residual }.  The
+ * outer stopping test is relative to the INITIAL residual.  (The reference
+ * overwrites res0_ with the latest residual after every pass, mpir.cc:239,
+ * so its relative test compares against the previous pass instead; the
+ * north-star tolerance is stated relative to the initial residual.)
+ * work must hold 3n doubles + 6n floats.  Returns 0 on success, 1 if
+ * max_outer passes did not reach the tolerance.
+ */
+int orc_mpir_d(int n, const int *rowptr, const int *col, const double *val,
+               const float *val32, const double *b, double *x, int max_outer,
+               double rtol, double inner_rtol, int inner_maxits,
+               const double *invd, const float *invd32, double *work64,
+               float *work32, int *outer_iters, int *inner_iters_total,
+               double *res_out, double *res_init_out) {
+  double *r = work64, *c = work64 + n;
+  float *r32 = work32, *c32 = work32 + n, *w32 = work32 + 2 * (size_t)n;
+  (void)invd;
+  orc_spmv_d(n, rowptr, col, val, x, r);
+  orc_scaleadd_d(n, r, -1., b);
+  double res = sqrt(orc_dot_d(n, r, r));
+  const double res0 = res;
+  *res_init_out = res0;
+  int k = 0, inner_total = 0;
+  while (res > rtol * res0 && k < max_outer) {
+    ++k;
+    for (int i = 0; i < n; ++i) { r32[i] = (float)r[i]; c32[i] = 0.f; }
+    int it = 0;
+    double ires, ires0;
+    orc_cg_f(n, rowptr, col, val32, r32, c32, inner_maxits, 0., inner_rtol,
+             1e30, 1, invd32, w32, &it, &ires, &ires0);
+    inner_total += it;
+    for (int i = 0; i < n; ++i) c[i] = (double)c32[i];
+    orc_axpy_d(n, x, c, 1.);
+    orc_spmv_d(n, rowptr, col, val, x, r);
+    orc_scaleadd_d(n, r, -1., b);
+    res = sqrt(orc_dot_d(n, r, r));
+  }
+  *outer_iters = k;
+  *inner_iters_total = inner_total;
+  *res_out = res;
+  return res <= rtol * res0 ? 0 : 1;
+}

@@ -1,0 +1,238 @@
+// Reference CPU checker driver (TEST INFRASTRUCTURE ONLY).
+//
+// Linked against HiFlow3's own lmp CPU sources, compiled unmodified from the
+// reference tree by oracle/ref/Makefile into oracle/_ref/libhiflow_lmp_ref.so.
+// Only tests, __graft_entry__.smoke() and bench.py's CPU-baseline legs load
+// it, and only as the checker / the timed CPU reference.  The product path
+// (ba_b200/) never links or calls it.
+//
+// Exposes a plain C ABI over the reference classes:
+//   * ref_spmv_*      -> CPUsimple_CSR_lMatrix / CPUopenmp_CSR_lMatrix
+//                        ::VectorMult (lmp/CPUsimple_csr_lmatrix.cc:92-111,
+//                        lmp/openmp/CPUopenmp_csr_lmatrix.cc:145-165)
+//   * ref_cg_solve_*  -> a single-rank restatement of CG<LAD>::SolveNoPrecond
+//                        / SolvePrecond (linear_solver/cg.h:87-246) with the
+//                        stopping test of IterateControl::Check
+//                        (common/iterate_control.cc:80-107), issued as the
+//                        same sequence of compiled lVector/lMatrix calls and
+//                        lPreconditioner_Jacobi (lmp/lpreconditioner.cc:125-200).
+//                        On one rank CoupledVector::Dot is the interior Dot plus
+//                        an identity all-reduce and CoupledMatrix::VectorMult is
+//                        the diagonal block's VectorMult, so the restatement
+//                        issues exactly the arithmetic the reference does.
+//   * ref_lmp_cg_*    -> the reference's own lmp cg() (lmp/solvers/cg.cc:35).
+#include <cmath>
+#include <vector>
+
+#include "config.h"
+#include "lmatrix_csr_cpu.h"
+#include "lpreconditioner.h"
+#include "lvector_cpu.h"
+#include "solvers/cg.h"
+
+using namespace hiflow::la;
+
+namespace {
+
+enum { IMPL_NAIVE = 0, IMPL_OPENMP = 1 };
+
+// IterateControl states (common/iterate_control.h): kIterate,
+// kFailureDivergenceTol, kFailureMaxitsExceeded, kSuccessAbsoluteTol,
+// kSuccessRelativeTol.  Numbered as in the B200 library's solver status.
+enum { CTRL_ITERATE = 0, CTRL_SUCCESS_ABS = 1, CTRL_SUCCESS_REL = 2,
+       CTRL_FAIL_DIV = 3, CTRL_FAIL_MAXITS = 4 };
+
+// IterateControl::Check, common/iterate_control.cc:80-107.
+int control_check(int step, double value, int maxits, double atol, double rtol,
+                  double dtol, double *first_value) {
+  if (step == 0) *first_value = value;
+  if (value <= atol) return CTRL_SUCCESS_ABS;
+  if (value < rtol * (*first_value)) return CTRL_SUCCESS_REL;
+  if (value > dtol * (*first_value)) return CTRL_FAIL_DIV;
+  if (step >= maxits) return CTRL_FAIL_MAXITS;
+  return CTRL_ITERATE;
+}
+
+template < typename T >
+lVector< T > *make_vector(int impl, int n, const char *name) {
+  if (impl == IMPL_OPENMP) return new CPUopenmp_lVector< T >(n, name);
+  return new CPUsimple_lVector< T >(n, name);
+}
+
+// Builds a CPU CSR matrix through the reference's own COO->CSR path
+// (CPU_CSR_lMatrix::TransformFromCOO, lmp/lmatrix_csr_cpu.cc:883-906), which
+// also sets diag_ptr_ used by extract_invdiagelements.
+template < typename T >
+CPU_CSR_lMatrix< T > *make_matrix(int impl, int nthreads, int n, int nnz,
+                                  const int *rowptr, const int *col,
+                                  const T *val) {
+  std::vector< int > rows(nnz);
+  for (int i = 0; i < n; ++i)
+    for (int j = rowptr[i]; j < rowptr[i + 1]; ++j) rows[j] = i;
+  CPUsimple_CSR_lMatrix< T > *sm =
+      new CPUsimple_CSR_lMatrix< T >(nnz, n, n, "A");
+  sm->TransformFromCOO(rows.data(), col, val, n, n, nnz);
+  if (impl != IMPL_OPENMP) return sm;
+  CPUopenmp_CSR_lMatrix< T > *om = new CPUopenmp_CSR_lMatrix< T >();
+  om->CopyStructureFrom(*sm);
+  om->CopyFrom(*sm);
+  om->set_num_threads(nthreads);
+  delete sm;
+  return om;
+}
+
+template < typename T >
+int cg_solve(int impl, int nthreads, int precond, int n, int nnz,
+             const int *rowptr, const int *col, const T *val, const T *bh,
+             T *xh, int maxits, double atol, double rtol, double dtol,
+             int *iters, double *res_out, double *res_init_out,
+             double *res_rel_out) {
+  CPU_CSR_lMatrix< T > *A = make_matrix< T >(impl, nthreads, n, nnz, rowptr,
+                                             col, val);
+  lVector< T > *b = make_vector< T >(impl, n, "b");
+  lVector< T > *x = make_vector< T >(impl, n, "x");
+  lVector< T > *r = make_vector< T >(impl, n, "r");
+  lVector< T > *p = make_vector< T >(impl, n, "p");
+  lVector< T > *z = make_vector< T >(impl, n, "z");
+  lVector< T > *Ap = make_vector< T >(impl, n, "Ap");
+  b->SetBlockValues(0, n, bh);
+  x->SetBlockValues(0, n, xh);
+
+  lPreconditioner_Jacobi< T > jac;
+  if (precond) {
+    jac.Init();
+    jac.SetupOperator(*A);
+    jac.SetReuse(true);
+    jac.Build(r, z);
+  }
+
+  int state = CTRL_ITERATE;
+  double first = 0.;
+  int iter = 0;
+  T alpha, beta, gamma, ressquared;
+  double res;
+
+  // initialization step (cg.h:104-121 / :184-204)
+  A->VectorMult(*x, r);
+  r->ScaleAdd(static_cast< T >(-1.), *b); // coupled r.ScaleAdd(b, -1)
+  ressquared = r->Dot(*r);
+  res = std::sqrt(ressquared);
+  const double res_init = res;
+  state = control_check(iter, res, maxits, atol, rtol, dtol, &first);
+  if (precond) {
+    z->Zeros();
+    jac.ApplylPreconditioner(*r, z);
+    p->CopyFrom(*z);
+    beta = r->Dot(*z);
+  } else {
+    p->CopyFrom(*r);
+    beta = ressquared;
+  }
+
+  // main loop (cg.h:124-148 / :207-233)
+  while (state == CTRL_ITERATE) {
+    ++iter;
+    A->VectorMult(*p, Ap);
+    alpha = beta / (Ap->Dot(*p));
+    x->Axpy(*p, alpha);
+    r->Axpy(*Ap, -alpha);
+    ressquared = r->Dot(*r);
+    res = std::sqrt(ressquared);
+    state = control_check(iter, res, maxits, atol, rtol, dtol, &first);
+    if (state != CTRL_ITERATE) break;
+    if (precond) {
+      z->Zeros();
+      jac.ApplylPreconditioner(*r, z);
+      gamma = r->Dot(*z);
+      beta = gamma / beta;
+      p->ScaleAdd(beta, *z); // coupled p.ScaleAdd(z, beta)
+      beta = gamma;
+    } else {
+      beta = ressquared / beta;
+      p->ScaleAdd(beta, *r);
+      beta = ressquared;
+    }
+  }
+
+  x->GetBlockValues(0, n, xh);
+  *iters = iter;
+  *res_out = res;
+  *res_init_out = res_init;
+  *res_rel_out = res_init > 0. ? res / res_init : 0.;
+  if (precond) jac.Clear();
+  delete Ap; delete z; delete p; delete r; delete x; delete b; delete A;
+  return state;
+}
+
+template < typename T >
+int spmv(int impl, int nthreads, int n, int nnz, const int *rowptr,
+         const int *col, const T *val, const T *xh, T *yh) {
+  CPU_CSR_lMatrix< T > *A = make_matrix< T >(impl, nthreads, n, nnz, rowptr,
+                                             col, val);
+  lVector< T > *x = make_vector< T >(impl, n, "x");
+  lVector< T > *y = make_vector< T >(impl, n, "y");
+  x->SetBlockValues(0, n, xh);
+  A->VectorMult(*x, y);
+  y->GetBlockValues(0, n, yh);
+  delete y; delete x; delete A;
+  return 0;
+}
+
+template < typename T >
+int lmp_cg(int impl, int nthreads, int n, int nnz, const int *rowptr,
+           const int *col, const T *val, const T *bh, T *xh, T rel_eps,
+           T abs_eps, int *max_iter) {
+  CPU_CSR_lMatrix< T > *A = make_matrix< T >(impl, nthreads, n, nnz, rowptr,
+                                             col, val);
+  lVector< T > *b = make_vector< T >(impl, n, "b");
+  lVector< T > *x = make_vector< T >(impl, n, "x");
+  b->SetBlockValues(0, n, bh);
+  x->SetBlockValues(0, n, xh);
+  int rv = cg(x, b, A, rel_eps, abs_eps, *max_iter, -1);
+  x->GetBlockValues(0, n, xh);
+  delete x; delete b; delete A;
+  return rv;
+}
+
+} // namespace
+
+extern "C" {
+
+int ref_spmv_d(int impl, int nthreads, int n, int nnz, const int *rowptr,
+               const int *col, const double *val, const double *x, double *y) {
+  return spmv< double >(impl, nthreads, n, nnz, rowptr, col, val, x, y);
+}
+
+int ref_spmv_f(int impl, int nthreads, int n, int nnz, const int *rowptr,
+               const int *col, const float *val, const float *x, float *y) {
+  return spmv< float >(impl, nthreads, n, nnz, rowptr, col, val, x, y);
+}
+
+int ref_cg_solve_d(int impl, int nthreads, int precond, int n, int nnz,
+                   const int *rowptr, const int *col, const double *val,
+                   const double *b, double *x, int maxits, double atol,
+                   double rtol, double dtol, int *iters, double *res,
+                   double *res_init, double *res_rel) {
+  return cg_solve< double >(impl, nthreads, precond, n, nnz, rowptr, col, val,
+                            b, x, maxits, atol, rtol, dtol, iters, res,
+                            res_init, res_rel);
+}
+
+int ref_cg_solve_f(int impl, int nthreads, int precond, int n, int nnz,
+                   const int *rowptr, const int *col, const float *val,
+                   const float *b, float *x, int maxits, double atol,
+                   double rtol, double dtol, int *iters, double *res,
+                   double *res_init, double *res_rel) {
+  return cg_solve< float >(impl, nthreads, precond, n, nnz, rowptr, col, val,
+                           b, x, maxits, atol, rtol, dtol, iters, res,
+                           res_init, res_rel);
+}
+
+int ref_lmp_cg_d(int impl, int nthreads, int n, int nnz, const int *rowptr,
+                 const int *col, const double *val, const double *b, double *x,
+                 double rel_eps, double abs_eps, int *max_iter) {
+  return lmp_cg< double >(impl, nthreads, n, nnz, rowptr, col, val, b, x,
+                          rel_eps, abs_eps, max_iter);
+}
+
+} // extern "C"
