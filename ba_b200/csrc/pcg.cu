@@ -1,0 +1,457 @@
+// Preconditioned CG on the device: CG<LAD>::SolvePrecond / SolveNoPrecond
+// (linear_solver/cg.h:87-246) with PreconditionerBlockJacobiStand(Jacobi)
+// (preconditioner_bjacobi_standard.cc:188-196, lmp/lpreconditioner.cc:184-200)
+// and IterateControl::Check (common/iterate_control.cc:80-107).
+//
+// The reference runs the loop on the host: per iteration 1 SpMV, 3 blocking
+// dot products and 6 more BLAS-1 passes, each its own launch.  Here one
+// iteration is three kernels and no host round trip:
+//   K1  Ap = A p, fused with the partial sums of p.Ap     (SpMV schedule)
+//   K2  alpha = rz/pAp; x += alpha p; r -= alpha Ap; z = invD r;
+//       fused sums r.r and r.z; its last block applies IterateControl
+//   K3  beta = rz_new/rz_old; p = beta p + z  (z recomputed from r, invD)
+// All scalars live in device memory.  The three kernels form the body of a
+// CUDA-graph WHILE node, so one graph launch runs the whole solve; K3 clears
+// the loop condition once the state leaves "iterate".  K3 also counts body
+// passes and stops the loop after maxits + 2 passes whatever K2 reported, so
+// the device loop ends even if a reduction misbehaves.
+#include <cmath>
+#include <cstring>
+
+#include "internal.cuh"
+#include "spmv.cuh"
+
+namespace b200la {
+
+constexpr int kMaxIts = 10000000;
+
+struct CgScalars {
+  double rz;        // r.z of the current residual (r.r without preconditioner)
+  double pAp;
+  double alpha;
+  double beta;
+  double rr;
+  double res;
+  double res_init;
+  double atol, rtol, dtol;
+  int iter;
+  int state;
+  int maxits;
+  int guard;        // body passes, counted by K3
+  unsigned ticket[4];
+};
+
+// IterateControl::Check; step 0 records the initial residual (res_init).
+__device__ __forceinline__ int iterate_check(int step, double value, const CgScalars &s, double first) {
+  if (value <= s.atol) return B200LA_SUCCESS_ABS;
+  if (value < s.rtol * first) return B200LA_SUCCESS_REL;
+  if (value > s.dtol * first) return B200LA_FAIL_DIV;
+  if (step >= s.maxits) return B200LA_FAIL_MAXITS;
+  return B200LA_ITERATE;
+}
+
+template <typename T> struct CgVecs {
+  T *x, *r, *p, *Ap;
+  const T *invd;  // nullptr without preconditioner
+  int64_t n;
+};
+
+// ---- init: r = b - A x0, z = invD r, p = z, rz = r.z, res_init -----------------
+template <typename T, bool PRE> struct InitEmit {
+  const T *__restrict__ b;
+  const T *__restrict__ x_user;
+  CgVecs<T> v;
+  Acc<T> rr, rz;
+  __device__ __forceinline__ void operator()(int row, T y) {
+    T r = b[row] - y;  // r.ScaleAdd(b, -1): -1*(Ax) + b
+    v.x[row] = x_user[row];
+    v.r[row] = r;
+    T z = PRE ? r * v.invd[row] : r;
+    v.p[row] = z;
+    rr.add(r * r);
+    rz.add(r * z);
+  }
+};
+
+template <typename Op, typename T, bool PRE>
+__global__ void __launch_bounds__(kBlock) cg_init_kernel(Op op, const T *__restrict__ x_user, const T *__restrict__ b,
+                                                         CgVecs<T> v, double *part, CgScalars *sc) {
+  InitEmit<T, PRE> e{b, x_user, v};
+  op.run(x_user, e);
+  double s[2] = {e.rr.value(), e.rz.value()};
+  if (grid_sum_last<2>(s, part, &sc->ticket[0]) && threadIdx.x == 0) {
+    double res = sqrt(s[0]);
+    sc->rr = s[0];
+    sc->rz = PRE ? s[1] : s[0];
+    sc->res = res;
+    sc->res_init = res;
+    sc->iter = 0;
+    sc->guard = 0;
+    sc->state = iterate_check(0, res, *sc, res);
+  }
+}
+
+// ---- K1: Ap = A p and p.Ap --------------------------------------------------------
+template <typename T> struct SpmvDotEmit {
+  T *__restrict__ Ap;
+  const T *__restrict__ p;
+  Acc<T> acc;
+  __device__ __forceinline__ void operator()(int row, T y) {
+    Ap[row] = y;
+    acc.add(y * __ldg(p + row));
+  }
+};
+
+template <typename Op, typename T>
+__global__ void __launch_bounds__(kBlock) cg_spmv_kernel(Op op, CgVecs<T> v, double *part, CgScalars *sc) {
+  if (*(volatile int *)&sc->state != B200LA_ITERATE) return;
+  SpmvDotEmit<T> e{v.Ap, v.p};
+  op.run(v.p, e);
+  double s[1] = {e.acc.value()};
+  if (grid_sum_last<1>(s, part, &sc->ticket[1]) && threadIdx.x == 0) {
+    sc->pAp = s[0];
+    double alpha = sc->rz / s[0];
+    sc->alpha = alpha;
+    if (!(s[0] != 0.0) || !isfinite(alpha)) sc->state = B200LA_FAIL_BREAKDOWN;
+  }
+}
+
+// ---- K2: x += alpha p, r -= alpha Ap, sums r.r and r.z ----------------------------
+template <typename T, bool PRE>
+__global__ void __launch_bounds__(kBlock) cg_update_kernel(CgVecs<T> v, double *part, CgScalars *sc) {
+  if (*(volatile int *)&sc->state != B200LA_ITERATE) return;
+  using V = typename Vec16<T>::type;
+  constexpr int W = Vec16<T>::n;
+  const T alpha = (T)sc->alpha;
+  Acc<T> rr, rz;
+  const int64_t n = v.n, nv = n / W;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += stride) {
+    V xv = reinterpret_cast<V *>(v.x)[i];
+    V pv = reinterpret_cast<const V *>(v.p)[i];
+    V rv = reinterpret_cast<V *>(v.r)[i];
+    V av = reinterpret_cast<const V *>(v.Ap)[i];
+    V dv;
+    if (PRE) dv = reinterpret_cast<const V *>(v.invd)[i];
+    T *xs = reinterpret_cast<T *>(&xv);
+    T *rs = reinterpret_cast<T *>(&rv);
+    const T *ps = reinterpret_cast<const T *>(&pv);
+    const T *as = reinterpret_cast<const T *>(&av);
+    const T *ds = reinterpret_cast<const T *>(&dv);
+#pragma unroll
+    for (int k = 0; k < W; ++k) {
+      xs[k] = fma(alpha, ps[k], xs[k]);
+      rs[k] = fma(-alpha, as[k], rs[k]);
+      rr.add(rs[k] * rs[k]);
+      if (PRE) rz.add(rs[k] * (rs[k] * ds[k]));
+    }
+    reinterpret_cast<V *>(v.x)[i] = xv;
+    reinterpret_cast<V *>(v.r)[i] = rv;
+  }
+  for (int64_t i = nv * W + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    v.x[i] = fma(alpha, v.p[i], v.x[i]);
+    T r = fma(-alpha, v.Ap[i], v.r[i]);
+    v.r[i] = r;
+    rr.add(r * r);
+    if (PRE) rz.add(r * (r * v.invd[i]));
+  }
+  double s[2] = {rr.value(), rz.value()};
+  if (grid_sum_last<2>(s, part, &sc->ticket[2]) && threadIdx.x == 0) {
+    double res = sqrt(s[0]);
+    int it = sc->iter + 1;
+    sc->iter = it;
+    sc->rr = s[0];
+    sc->res = res;
+    int st = iterate_check(it, res, *sc, sc->res_init);
+    double rz_new = PRE ? s[1] : s[0];
+    sc->beta = rz_new / sc->rz;
+    sc->rz = rz_new;
+    sc->state = st;
+  }
+}
+
+// ---- K3: p = beta p + z; ends the device loop ---------------------------------------
+template <typename T, bool PRE, bool IN_GRAPH = true>
+__global__ void __launch_bounds__(kBlock) cg_direction_kernel(CgVecs<T> v, CgScalars *sc,
+                                                              cudaGraphConditionalHandle loop) {
+  const int state = *(volatile int *)&sc->state;
+  if (IN_GRAPH && blockIdx.x == 0 && threadIdx.x == 0) {
+    int g = sc->guard + 1;
+    sc->guard = g;
+    bool go = state == B200LA_ITERATE;
+    if (go && g > sc->maxits + 2) {  // unreachable unless K2 failed to count
+      sc->state = B200LA_FAIL_BREAKDOWN;
+      go = false;
+    }
+    cudaGraphSetConditional(loop, go ? 1u : 0u);
+  }
+  if (state != B200LA_ITERATE) return;
+  using V = typename Vec16<T>::type;
+  constexpr int W = Vec16<T>::n;
+  const T beta = (T)sc->beta;
+  const int64_t n = v.n, nv = n / W;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += stride) {
+    V pv = reinterpret_cast<V *>(v.p)[i];
+    V rv = reinterpret_cast<const V *>(v.r)[i];
+    V dv;
+    if (PRE) dv = reinterpret_cast<const V *>(v.invd)[i];
+    T *ps = reinterpret_cast<T *>(&pv);
+    const T *rs = reinterpret_cast<const T *>(&rv);
+    const T *ds = reinterpret_cast<const T *>(&dv);
+#pragma unroll
+    for (int k = 0; k < W; ++k) ps[k] = fma(beta, ps[k], PRE ? rs[k] * ds[k] : rs[k]);
+    reinterpret_cast<V *>(v.p)[i] = pv;
+  }
+  for (int64_t i = nv * W + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+    v.p[i] = fma(beta, v.p[i], PRE ? v.r[i] * v.invd[i] : v.r[i]);
+}
+
+}  // namespace b200la
+
+using namespace b200la;
+
+struct b200la_cg_s {
+  b200la_mat A;
+  b200la_cg_params prm;
+  int64_t n;
+  void *x, *r, *p, *Ap, *invd;
+  double *part;       // [2][kMaxReduceBlocks]
+  CgScalars *sc;      // device
+  CgScalars *sc_host; // pinned
+  cudaGraph_t graph;
+  cudaGraphExec_t exec;
+  int g_format, g_param;  // schedule baked into the graph
+  int grid_spmv, grid_ew;
+};
+
+namespace b200la {
+
+template <typename T, bool PRE>
+static int cg_build_graph_t(b200la_cg s) {
+  b200la_mat A = s->A;
+  b200la_ctx c = A->ctx;
+  if (s->exec) { cudaGraphExecDestroy(s->exec); s->exec = nullptr; }
+  if (s->graph) { cudaGraphDestroy(s->graph); s->graph = nullptr; }
+  CgVecs<T> v{(T *)s->x, (T *)s->r, (T *)s->p, (T *)s->Ap, (const T *)s->invd, s->n};
+  B_TRY(grid_for(c, (const void *)cg_update_kernel<T, PRE>, (s->n + Vec16<T>::n - 1) / Vec16<T>::n, kBlock, &s->grid_ew));
+  cudaGraph_t g;
+  B_CUDA(cudaGraphCreate(&g, 0));
+  s->graph = g;
+  cudaGraphConditionalHandle h;
+  B_CUDA(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+  cudaGraphNodeParams np = {};
+  np.type = cudaGraphNodeTypeConditional;
+  np.conditional.handle = h;
+  np.conditional.type = cudaGraphCondTypeWhile;
+  np.conditional.size = 1;
+  cudaGraphNode_t node;
+  B_CUDA(cudaGraphAddNode(&node, g, nullptr, 0, &np));
+  cudaGraph_t body = np.conditional.phGraph_out[0];
+  cudaStream_t cs;
+  B_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+  B_CUDA(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  int rc = with_schedule<T>(A, [&](auto op) -> int {
+    using Op = decltype(op);
+    B_TRY(grid_for(c, (const void *)cg_spmv_kernel<Op, T>, op.work_items(), Op::kRowsPerBlock, &s->grid_spmv));
+    cg_spmv_kernel<Op, T><<<s->grid_spmv, kBlock, 0, cs>>>(op, v, s->part, s->sc);
+    return B200LA_OK;
+  });
+  cg_update_kernel<T, PRE><<<s->grid_ew, kBlock, 0, cs>>>(v, s->part, s->sc);
+  cg_direction_kernel<T, PRE><<<s->grid_ew, kBlock, 0, cs>>>(v, s->sc, h);
+  cudaGraph_t captured;
+  cudaError_t ce = cudaStreamEndCapture(cs, &captured);
+  cudaStreamDestroy(cs);
+  B_TRY(rc);
+  B_CUDA(ce);
+  B_CUDA(cudaGraphInstantiate(&s->exec, g, 0));
+  s->g_format = A->format;
+  s->g_param = A->param;
+  return B200LA_OK;
+}
+
+static int cg_build_graph(b200la_cg s) {
+  bool pre = s->prm.precond != 0;
+  if (s->A->dtype == B200LA_F64) return pre ? cg_build_graph_t<double, true>(s) : cg_build_graph_t<double, false>(s);
+  return pre ? cg_build_graph_t<float, true>(s) : cg_build_graph_t<float, false>(s);
+}
+
+template <typename T, bool PRE>
+static int cg_launch_init_t(b200la_cg s, const void *x_user, const void *b) {
+  b200la_mat A = s->A;
+  CgVecs<T> v{(T *)s->x, (T *)s->r, (T *)s->p, (T *)s->Ap, (const T *)s->invd, s->n};
+  cudaStream_t st = A->ctx->stream;
+  return with_schedule<T>(A, [&](auto op) -> int {
+    using Op = decltype(op);
+    int grid;
+    B_TRY(grid_for(A->ctx, (const void *)cg_init_kernel<Op, T, PRE>, op.work_items(), Op::kRowsPerBlock, &grid));
+    cg_init_kernel<Op, T, PRE><<<grid, kBlock, 0, st>>>(op, (const T *)x_user, (const T *)b, v, s->part, s->sc);
+    B_CUDA(cudaGetLastError());
+    return B200LA_OK;
+  });
+}
+
+static int cg_launch_init(b200la_cg s, const void *x_user, const void *b) {
+  bool pre = s->prm.precond != 0;
+  if (s->A->dtype == B200LA_F64)
+    return pre ? cg_launch_init_t<double, true>(s, x_user, b) : cg_launch_init_t<double, false>(s, x_user, b);
+  return pre ? cg_launch_init_t<float, true>(s, x_user, b) : cg_launch_init_t<float, false>(s, x_user, b);
+}
+
+// Runs the init kernel and then `iters` iterations as separate launches with
+// CUDA events between the kernels; adds the mean time per launch of K1, K2
+// and K3 to ms[0..2].  Same kernels as the graph body (K3 without the loop
+// condition).
+template <typename T, bool PRE>
+static int cg_profile_t(b200la_cg s, const void *x_user, const void *b, int iters, double *ms) {
+  b200la_mat A = s->A;
+  cudaStream_t st = A->ctx->stream;
+  CgVecs<T> v{(T *)s->x, (T *)s->r, (T *)s->p, (T *)s->Ap, (const T *)s->invd, s->n};
+  B_TRY((cg_launch_init_t<T, PRE>(s, x_user, b)));
+  cudaEvent_t ev[4];
+  for (auto &e : ev) B_CUDA(cudaEventCreate(&e));
+  float acc[3] = {0.f, 0.f, 0.f};
+  int rc = B200LA_OK;
+  for (int it = 0; it < iters && rc == B200LA_OK; ++it) {
+    cudaEventRecord(ev[0], st);
+    rc = with_schedule<T>(A, [&](auto op) -> int {
+      using Op = decltype(op);
+      cg_spmv_kernel<Op, T><<<s->grid_spmv, kBlock, 0, st>>>(op, v, s->part, s->sc);
+      return B200LA_OK;
+    });
+    cudaEventRecord(ev[1], st);
+    cg_update_kernel<T, PRE><<<s->grid_ew, kBlock, 0, st>>>(v, s->part, s->sc);
+    cudaEventRecord(ev[2], st);
+    cg_direction_kernel<T, PRE, false><<<s->grid_ew, kBlock, 0, st>>>(v, s->sc, 0);
+    cudaEventRecord(ev[3], st);
+    B_CUDA(cudaEventSynchronize(ev[3]));
+    for (int k = 0; k < 3; ++k) {
+      float t = 0.f;
+      cudaEventElapsedTime(&t, ev[k], ev[k + 1]);
+      acc[k] += t;
+    }
+  }
+  for (auto &e : ev) cudaEventDestroy(e);
+  B_CUDA(cudaGetLastError());
+  for (int k = 0; k < 3; ++k) ms[k] = iters > 0 ? acc[k] / iters : 0.0;
+  return rc;
+}
+
+}  // namespace b200la
+
+extern "C" {
+
+int b200la_cg_profile(b200la_cg s, b200la_vec b, b200la_vec x, int iters, double *ms) {
+  B_CHECK(s && b && x && ms && iters >= 0, B200LA_ERR_INVALID, "cg_profile: bad argument");
+  B_CHECK(b->n == s->n && x->n == s->n && s->n > 0, B200LA_ERR_INVALID, "cg_profile: sizes");
+  B_CHECK(b->dtype == s->A->dtype && x->dtype == s->A->dtype, B200LA_ERR_DTYPE, "cg_profile: dtype");
+  bool pre = s->prm.precond != 0;
+  if (s->A->dtype == B200LA_F64)
+    return pre ? cg_profile_t<double, true>(s, x->d, b->d, iters, ms) : cg_profile_t<double, false>(s, x->d, b->d, iters, ms);
+  return pre ? cg_profile_t<float, true>(s, x->d, b->d, iters, ms) : cg_profile_t<float, false>(s, x->d, b->d, iters, ms);
+}
+
+int b200la_cg_create(b200la_mat A, const b200la_cg_params *prm, b200la_cg *out) {
+  B_CHECK(A && prm && out, B200LA_ERR_INVALID, "cg_create: null argument");
+  B_CHECK(A->nrow == A->ncol, B200LA_ERR_INVALID, "cg_create: matrix is %dx%d, not square", A->nrow, A->ncol);
+  B_CHECK(prm->maxits >= 0 && prm->maxits <= kMaxIts, B200LA_ERR_INVALID, "cg_create: maxits %d not in [0, %d]",
+          prm->maxits, kMaxIts);
+  B_CHECK(prm->atol >= 0.0 && prm->rtol >= 0.0 && prm->dtol > 0.0, B200LA_ERR_INVALID,
+          "cg_create: tolerances must be atol >= 0, rtol >= 0, dtol > 0");
+  b200la_ctx c = A->ctx;
+  cudaStream_t st = c->stream;
+  b200la_cg s = new b200la_cg_s();
+  s->A = A;
+  s->prm = *prm;
+  s->n = A->nrow;
+  size_t es = dtype_size(A->dtype);
+  size_t vb = es * (size_t)(s->n > 0 ? s->n : 1);
+  int rc = B200LA_OK;
+  auto cleanup = [&](int code) { b200la_cg_destroy(s); return code; };
+  if (cudaMallocAsync(&s->x, vb, st) != cudaSuccess || cudaMallocAsync(&s->r, vb, st) != cudaSuccess ||
+      cudaMallocAsync(&s->p, vb, st) != cudaSuccess || cudaMallocAsync(&s->Ap, vb, st) != cudaSuccess ||
+      cudaMallocAsync(&s->part, sizeof(double) * 2 * kMaxReduceBlocks, st) != cudaSuccess ||
+      cudaMallocAsync(&s->sc, sizeof(CgScalars), st) != cudaSuccess ||
+      cudaMallocHost(&s->sc_host, sizeof(CgScalars)) != cudaSuccess)
+    return cleanup(fail(B200LA_ERR_NOMEM, "cg_create: allocation of %zu-byte work vectors failed", vb));
+  CgScalars init = {};
+  init.atol = prm->atol;
+  init.rtol = prm->rtol;
+  init.dtol = prm->dtol;
+  init.maxits = prm->maxits;
+  init.state = B200LA_ITERATE;
+  if (cudaMemcpyAsync(s->sc, &init, sizeof(init), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return cleanup(fail(B200LA_ERR_CUDA, "cg_create: scalar upload failed"));
+  if (prm->precond) {
+    if (cudaMallocAsync(&s->invd, vb, st) != cudaSuccess)
+      return cleanup(fail(B200LA_ERR_NOMEM, "cg_create: allocation of the inverse diagonal failed"));
+    b200la_vec_s dv{c, s->n, A->dtype, s->invd, false};
+    rc = b200la_mat_inv_diag(A, &dv);
+    if (rc != B200LA_OK) return cleanup(rc);
+  }
+  if (s->n > 0) {
+    rc = cg_build_graph(s);
+    if (rc != B200LA_OK) return cleanup(rc);
+  }
+  *out = s;
+  return B200LA_OK;
+}
+
+int b200la_cg_destroy(b200la_cg s) {
+  if (!s) return B200LA_OK;
+  cudaStream_t st = s->A->ctx->stream;
+  cudaStreamSynchronize(st);
+  if (s->exec) cudaGraphExecDestroy(s->exec);
+  if (s->graph) cudaGraphDestroy(s->graph);
+  void *bufs[] = {s->x, s->r, s->p, s->Ap, s->invd, s->part, s->sc};
+  for (void *b : bufs)
+    if (b) cudaFreeAsync(b, st);
+  if (s->sc_host) cudaFreeHost(s->sc_host);
+  delete s;
+  return B200LA_OK;
+}
+
+int b200la_cg_solve(b200la_cg s, b200la_vec b, b200la_vec x, b200la_cg_result *res) {
+  B_CHECK(s && b && x && res, B200LA_ERR_INVALID, "cg_solve: null argument");
+  b200la_mat A = s->A;
+  B_CHECK(b->n == s->n && x->n == s->n, B200LA_ERR_INVALID, "cg_solve: vector sizes %lld/%lld vs %lld",
+          (long long)b->n, (long long)x->n, (long long)s->n);
+  B_CHECK(b->dtype == A->dtype && x->dtype == A->dtype, B200LA_ERR_DTYPE, "cg_solve: dtype mismatch");
+  memset(res, 0, sizeof(*res));
+  if (s->n == 0) {
+    res->state = B200LA_SUCCESS_ABS;
+    return B200LA_OK;
+  }
+  b200la_ctx c = A->ctx;
+  cudaStream_t st = c->stream;
+  if (A->format != s->g_format || A->param != s->g_param) B_TRY(cg_build_graph(s));
+  B_TRY(cg_launch_init(s, x->d, b->d));
+  B_CUDA(cudaGraphLaunch(s->exec, st));
+  B_CUDA(cudaMemcpyAsync(x->d, s->x, (size_t)s->n * dtype_size(A->dtype), cudaMemcpyDeviceToDevice, st));
+  B_CUDA(cudaMemcpyAsync(s->sc_host, s->sc, sizeof(CgScalars), cudaMemcpyDeviceToHost, st));
+  B_CUDA(cudaStreamSynchronize(st));
+  const CgScalars &h = *s->sc_host;
+  res->iters = h.iter;
+  res->state = h.state;
+  res->res = h.res;
+  res->res_init = h.res_init;
+  res->res_rel = h.res_init > 0.0 ? h.res / h.res_init : 0.0;
+  if (h.state == B200LA_SUCCESS_ABS || h.state == B200LA_SUCCESS_REL)
+    res->solver_state = B200LA_SOLVER_SUCCESS;
+  else if (h.state == B200LA_FAIL_DIV || h.state == B200LA_FAIL_MAXITS)
+    res->solver_state = B200LA_SOLVER_EXCEEDED;
+  else
+    res->solver_state = B200LA_SOLVER_ERROR;
+  return B200LA_OK;
+}
+
+int b200la_pcg_solve(b200la_mat A, b200la_vec b, b200la_vec x, const b200la_cg_params *prm, b200la_cg_result *res) {
+  b200la_cg s = nullptr;
+  B_TRY(b200la_cg_create(A, prm, &s));
+  int rc = b200la_cg_solve(s, b, x, res);
+  b200la_cg_destroy(s);
+  return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,149 @@
+// SpMV schedules (CSR lane groups, SELL-32 slices) shared by the plain
+// VectorMult entry points, the autotuner and the fused CG kernels.
+//
+// A schedule is an "operator" type with run(x, emit): every thread block
+// walks its share of the rows (grid-stride) and calls emit(row, y_row) on
+// exactly one lane per row.  The fused kernels pass emitters that also
+// accumulate dot products, so the SpMV result never makes an extra trip
+// through HBM.
+#pragma once
+
+#include "internal.cuh"
+
+namespace b200la {
+
+// ---- CSR, G lanes per row (G = 1..32) -------------------------------------
+// Each warp covers 32/G consecutive rows, so a warp's loads of val/col fall
+// in one contiguous span of the CSR arrays; x is gathered through L1/L2.
+template <typename T, int G> struct CsrOp {
+  const int *__restrict__ rowptr;
+  const int *__restrict__ col;
+  const T *__restrict__ val;
+  int n;
+  static constexpr int kRowsPerBlock = kBlock / G;
+  __host__ __device__ int64_t work_items() const { return n; }
+  template <typename Emit> __device__ __forceinline__ void run(const T *__restrict__ x, Emit &emit) const {
+    for (int base = blockIdx.x * kRowsPerBlock; base < n; base += gridDim.x * kRowsPerBlock) {
+      const int row = base + (int)threadIdx.x / G;
+      const bool valid = row < n;
+      T y = csr_row_group<T, G>(rowptr, col, val, x, row, valid);
+      if (valid && (threadIdx.x & (G - 1)) == 0) emit(row, y);
+    }
+  }
+};
+
+// ---- SELL-C-sigma with C = 32, sigma = 1 (rows keep their order) ---------
+// Slice s holds rows 32s..32s+31, padded to slice_len[s] entries per row (a
+// multiple of W).  Chunk c of lane r starts at slice_ptr[s] + (c*32 + r)*W:
+// lane r reads W consecutive entries of its own row with one vector load and
+// a warp reads 32*W*sizeof(T) contiguous bytes per step.  Padding entries
+// hold value 0 and repeat a column the row already reads.
+template <typename T, int W> struct VecW;
+template <> struct VecW<double, 1> { using v = double; using i = int; };
+template <> struct VecW<double, 2> { using v = double2; using i = int2; };
+template <> struct VecW<double, 4> { using v = double4; using i = int4; };
+template <> struct VecW<float, 1> { using v = float; using i = int; };
+template <> struct VecW<float, 2> { using v = float2; using i = int2; };
+template <> struct VecW<float, 4> { using v = float4; using i = int4; };
+
+template <typename V, typename T, int W> __device__ __forceinline__ T lane_get(const V &v, int k) {
+  return reinterpret_cast<const T *>(&v)[k];
+}
+template <typename I, int W> __device__ __forceinline__ int lane_geti(const I &v, int k) {
+  return reinterpret_cast<const int *>(&v)[k];
+}
+
+template <typename T> __device__ __forceinline__ double4 ld_stream4(const double4 *p) {
+  const double2 *q = reinterpret_cast<const double2 *>(p);
+  double2 a = __ldcs(q), b = __ldcs(q + 1);
+  return make_double4(a.x, a.y, b.x, b.y);
+}
+
+template <typename V> __device__ __forceinline__ V ld_vec_stream(const V *p) { return __ldcs(p); }
+template <> __device__ __forceinline__ double4 ld_vec_stream<double4>(const double4 *p) {
+  return ld_stream4<double>(p);
+}
+
+template <typename T, int W> struct SellOp {
+  const int *__restrict__ slice_ptr;
+  const int *__restrict__ slice_len;
+  const int *__restrict__ col;
+  const T *__restrict__ val;
+  int n, nslices;
+  static constexpr int kRowsPerBlock = kBlock;
+  __host__ __device__ int64_t work_items() const { return n; }
+  template <typename Emit> __device__ __forceinline__ void run(const T *__restrict__ x, Emit &emit) const {
+    using VV = typename VecW<T, W>::v;
+    using VI = typename VecW<T, W>::i;
+    const int lane = threadIdx.x & 31;
+    const int wpb = kBlock / 32;
+    for (int s = blockIdx.x * wpb + ((int)threadIdx.x >> 5); s < nslices; s += gridDim.x * wpb) {
+      const int base = __ldg(slice_ptr + s);
+      const int chunks = __ldg(slice_len + s) / W;
+      const VI *ci = reinterpret_cast<const VI *>(col + base) + lane;
+      const VV *vi = reinterpret_cast<const VV *>(val + base) + lane;
+      T sum = T(0);
+#pragma unroll 4
+      for (int c = 0; c < chunks; ++c) {
+        VI cc = ld_vec_stream(ci + c * 32);
+        VV vv = ld_vec_stream(vi + c * 32);
+#pragma unroll
+        for (int k = 0; k < W; ++k)
+          sum = fma(lane_get<VV, T, W>(vv, k), ld_keep(x + lane_geti<VI, W>(cc, k)), sum);
+      }
+      const int row = s * 32 + lane;
+      if (row < n) emit(row, sum);
+    }
+  }
+};
+
+// ---- plain emitters --------------------------------------------------------
+template <typename T> struct StoreEmit {
+  T *__restrict__ y;
+  __device__ __forceinline__ void operator()(int row, T v) { y[row] = v; }
+};
+template <typename T> struct AddEmit {
+  T *__restrict__ y;
+  __device__ __forceinline__ void operator()(int row, T v) { y[row] += v; }
+};
+
+template <typename Op, typename T, bool ADD>
+__global__ void __launch_bounds__(kBlock) spmv_kernel(Op op, const T *__restrict__ x, T *__restrict__ y) {
+  if (ADD) {
+    AddEmit<T> e{y};
+    op.run(x, e);
+  } else {
+    StoreEmit<T> e{y};
+    op.run(x, e);
+  }
+}
+
+// Calls f(op) with the schedule selected on the matrix.
+template <typename T, typename F> int with_schedule(b200la_mat m, F &&f) {
+  const T *val = (const T *)m->val;
+  if (m->format == B200LA_FMT_SELL) {
+    const SellData &s = m->sell;
+    const T *sv = (const T *)s.val;
+    switch (m->param) {
+      case 1: return f(SellOp<T, 1>{s.slice_ptr, s.slice_len, s.col, sv, m->nrow, s.nslices});
+      case 2: return f(SellOp<T, 2>{s.slice_ptr, s.slice_len, s.col, sv, m->nrow, s.nslices});
+      case 4: return f(SellOp<T, 4>{s.slice_ptr, s.slice_len, s.col, sv, m->nrow, s.nslices});
+    }
+    return fail(B200LA_ERR_INVALID, "SELL width %d", m->param);
+  }
+  switch (m->param) {
+    case 1: return f(CsrOp<T, 1>{m->rowptr, m->col, val, m->nrow});
+    case 2: return f(CsrOp<T, 2>{m->rowptr, m->col, val, m->nrow});
+    case 4: return f(CsrOp<T, 4>{m->rowptr, m->col, val, m->nrow});
+    case 8: return f(CsrOp<T, 8>{m->rowptr, m->col, val, m->nrow});
+    case 16: return f(CsrOp<T, 16>{m->rowptr, m->col, val, m->nrow});
+    case 32: return f(CsrOp<T, 32>{m->rowptr, m->col, val, m->nrow});
+  }
+  return fail(B200LA_ERR_INVALID, "CSR lanes per row %d", m->param);
+}
+
+int spmv_launch(b200la_mat m, const void *x, void *y, bool add, cudaStream_t s);
+int sell_build(b200la_mat m, int width);
+void sell_free(b200la_mat m);
+
+}  // namespace b200la

@@ -1,0 +1,411 @@
+"""Host-side mirror of HiFlow3's lmp / linear_solver interface for the PCG path.
+
+The classes keep the reference's names, argument meaning and results so code
+written against lmp reads the same:
+
+* ``init_platform``            ~ init_platform_gpu   (lmp/cuda/platform_management_gpu.cu:78)
+* ``B200_lVector``             ~ lVector<T>          (lmp/lvector.h:38-321)
+* ``B200_CSR_lMatrix``         ~ CSR_lMatrix<T>      (lmp/lmatrix.h:39-468)
+* ``init_vector / init_matrix``~ the factories       (lmp/init_vec_mat.cc:146, :259)
+* ``IterateControl``           ~ common/iterate_control.h
+* ``PreconditionerBlockJacobiStand`` with ``Init_Jacobi``
+                               ~ linear_solver/preconditioner_bjacobi_standard.cc:77-196
+* ``CG``                       ~ CG<LAD> (linear_solver/cg.h:39-247): InitControl,
+  SetupOperator, SetupPreconditioner, Solve -> LinearSolverState, iter(), res()
+
+Differences: errors raise B200LAError instead of exit(-1); all compute runs in
+libb200la.so on the GPU (no CPU fallback).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import sys
+
+import numpy as np
+
+from . import _lib
+from ._lib import F32, F64, FMT_CSR, FMT_SELL, B200LAError, CgParams, CgResult, call, load
+
+kSolverSuccess, kSolverExceeded, kSolverError = 0, 1, 2
+
+_NP = {F64: np.float64, F32: np.float32}
+
+
+def _dt(dtype) -> int:
+    if dtype in (F64, F32):
+        return dtype
+    d = np.dtype(dtype)
+    if d == np.float64:
+        return F64
+    if d == np.float32:
+        return F32
+    raise TypeError(f"unsupported dtype {dtype}")
+
+
+class Platform:
+    """A device context (one stream, reduction scratch)."""
+
+    def __init__(self, device: int = 0):
+        self.handle = C.c_void_p()
+        call("b200la_ctx_create", device, C.byref(self.handle))
+        self.device = device
+
+    def synchronize(self):
+        call("b200la_ctx_synchronize", self.handle)
+
+    def set_stream(self, stream_ptr: int | None):
+        call("b200la_ctx_set_stream", self.handle, C.c_void_p(stream_ptr or 0))
+
+    @property
+    def num_sms(self) -> int:
+        n = C.c_int()
+        call("b200la_ctx_num_sms", self.handle, C.byref(n))
+        return n.value
+
+    def close(self):
+        if self.handle:
+            load().b200la_ctx_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        # at interpreter exit the process teardown releases device memory;
+        # destroying contexts in arbitrary finalization order is unsafe
+        if sys.is_finalizing():
+            return
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_default = None
+
+
+def init_platform(device: int = 0) -> Platform:
+    global _default
+    if _default is None:
+        _default = Platform(device)
+    return _default
+
+
+class B200_lVector:
+    """lVector<T> on the B200: a device buffer of `size` values."""
+
+    def __init__(self, size: int, name: str = "", platform: Platform | None = None, dtype=np.float64,
+                 _wrap_ptr: int | None = None, _keep=None):
+        self.platform = platform or init_platform()
+        self.name = name
+        self.dtype = _dt(dtype)
+        self.handle = C.c_void_p()
+        self._keep = _keep
+        if _wrap_ptr is None:
+            call("b200la_vec_create", self.platform.handle, int(size), self.dtype, C.byref(self.handle))
+        else:
+            call("b200la_vec_wrap", self.platform.handle, int(size), self.dtype, C.c_void_p(_wrap_ptr),
+                 C.byref(self.handle))
+        self._size = int(size)
+
+    # --- lVector API ---
+    def get_size(self) -> int:
+        return self._size
+
+    def Zeros(self):
+        call("b200la_vec_zeros", self.handle)
+
+    def SetBlockValues(self, start: int, end: int, values):
+        if start != 0 or end != self._size:
+            raise B200LAError(-1, "SetBlockValues: only the full range is supported")
+        a = np.ascontiguousarray(values, _NP[self.dtype])
+        call("b200la_vec_upload", self.handle, a.ctypes.data_as(C.c_void_p), a.shape[0])
+
+    def GetBlockValues(self, start: int = 0, end: int | None = None) -> np.ndarray:
+        end = self._size if end is None else end
+        out = np.empty(self._size, _NP[self.dtype])
+        call("b200la_vec_download", self.handle, out.ctypes.data_as(C.c_void_p), self._size)
+        return out[start:end]
+
+    def SetValues(self, index, values):
+        idx = np.ascontiguousarray(index, np.int32)
+        v = np.ascontiguousarray(values, _NP[self.dtype])
+        call("b200la_vec_set_values", self.handle, idx.ctypes.data_as(C.c_void_p),
+             v.ctypes.data_as(C.c_void_p), idx.shape[0])
+
+    def GetValues(self, index) -> np.ndarray:
+        idx = np.ascontiguousarray(index, np.int32)
+        out = np.empty(idx.shape[0], _NP[self.dtype])
+        call("b200la_vec_get_values", self.handle, idx.ctypes.data_as(C.c_void_p),
+             out.ctypes.data_as(C.c_void_p), idx.shape[0])
+        return out
+
+    def CopyFrom(self, other: "B200_lVector"):
+        call("b200la_vec_copy", self.handle, other.handle)
+
+    def CastFrom(self, other: "B200_lVector"):
+        call("b200la_vec_cast", self.handle, other.handle)
+
+    def CloneWithoutContent(self) -> "B200_lVector":
+        return B200_lVector(self._size, self.name, self.platform, self.dtype)
+
+    def Dot(self, other: "B200_lVector") -> float:
+        out = C.c_double()
+        call("b200la_vec_dot", self.handle, other.handle, C.byref(out))
+        return out.value
+
+    def Norm2(self) -> float:
+        out = C.c_double()
+        call("b200la_vec_norm2", self.handle, C.byref(out))
+        return out.value
+
+    def Axpy(self, vec: "B200_lVector", scalar: float):
+        """this += scalar * vec"""
+        call("b200la_vec_axpy", self.handle, vec.handle, float(scalar))
+
+    def ScaleAdd(self, scalar: float, vec: "B200_lVector"):
+        """this = scalar * this + vec"""
+        call("b200la_vec_scaleadd", self.handle, float(scalar), vec.handle)
+
+    def Scale(self, scalar: float):
+        call("b200la_vec_scale", self.handle, float(scalar))
+
+    def ElementWiseMult(self, vec: "B200_lVector"):
+        call("b200la_vec_elementwise_mult", self.handle, vec.handle)
+
+    def GetBuffer(self) -> int:
+        p = C.c_void_p()
+        call("b200la_vec_info", self.handle, None, None, C.byref(p))
+        return p.value or 0
+
+    def Clear(self):
+        if self.handle:
+            load().b200la_vec_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        if sys.is_finalizing():
+            return
+        try:
+            self.Clear()
+        except Exception:
+            pass
+
+    # --- interop ---
+    @classmethod
+    def from_numpy(cls, a, name: str = "", platform: Platform | None = None, dtype=None):
+        a = np.asarray(a)
+        v = cls(a.shape[0], name, platform, dtype if dtype is not None else a.dtype)
+        v.SetBlockValues(0, a.shape[0], a)
+        return v
+
+    @classmethod
+    def from_torch(cls, t, name: str = "", platform: Platform | None = None):
+        """Non-owning view of a contiguous 1-D CUDA tensor (kept alive)."""
+        import torch
+        assert t.is_cuda and t.dim() == 1 and t.is_contiguous()
+        dt = {torch.float64: F64, torch.float32: F32}[t.dtype]
+        return cls(t.shape[0], name, platform, dt, _wrap_ptr=t.data_ptr(), _keep=t)
+
+    def numpy(self) -> np.ndarray:
+        return self.GetBlockValues()
+
+
+class B200_CSR_lMatrix:
+    """CSR_lMatrix<T> on the B200 (int32 indices)."""
+
+    def __init__(self, rowptr, col, val, num_col: int | None = None, name: str = "",
+                 platform: Platform | None = None, dtype=np.float64):
+        self.platform = platform or init_platform()
+        self.name = name
+        self.dtype = _dt(dtype)
+        rp = np.ascontiguousarray(rowptr, np.int32)
+        cl = np.ascontiguousarray(col, np.int32)
+        vv = np.ascontiguousarray(val)
+        if vv.dtype not in (np.float64, np.float32):
+            vv = vv.astype(np.float64)
+        nrow = rp.shape[0] - 1
+        ncol = nrow if num_col is None else int(num_col)
+        self.handle = C.c_void_p()
+        call("b200la_csr_upload", self.platform.handle, nrow, ncol, cl.shape[0],
+             rp.ctypes.data_as(C.c_void_p), cl.ctypes.data_as(C.c_void_p), vv.ctypes.data_as(C.c_void_p),
+             _dt(vv.dtype), self.dtype, C.byref(self.handle))
+        self._shape = (nrow, ncol, int(cl.shape[0]))
+
+    @classmethod
+    def _from_handle(cls, handle, platform, dtype, shape, name=""):
+        m = cls.__new__(cls)
+        m.platform, m.name, m.dtype, m.handle, m._shape = platform, name, dtype, handle, shape
+        return m
+
+    def get_num_row(self) -> int:
+        return self._shape[0]
+
+    def get_num_col(self) -> int:
+        return self._shape[1]
+
+    def get_nnz(self) -> int:
+        return self._shape[2]
+
+    def VectorMult(self, invec: B200_lVector, outvec: B200_lVector):
+        call("b200la_spmv", self.handle, invec.handle, outvec.handle)
+
+    def VectorMultAdd(self, invec: B200_lVector, outvec: B200_lVector):
+        call("b200la_spmv_add", self.handle, invec.handle, outvec.handle)
+
+    def extract_invdiagelements(self, vec: B200_lVector):
+        call("b200la_mat_inv_diag", self.handle, vec.handle)
+
+    def ZeroRows(self, index_set, alpha: float = 1.0):
+        idx = np.ascontiguousarray(index_set, np.int32)
+        call("b200la_mat_zero_rows", self.handle, idx.ctypes.data_as(C.c_void_p), idx.shape[0], float(alpha))
+
+    def CastTo(self, dtype) -> "B200_CSR_lMatrix":
+        h = C.c_void_p()
+        call("b200la_mat_cast", self.handle, _dt(dtype), C.byref(h))
+        return B200_CSR_lMatrix._from_handle(h, self.platform, _dt(dtype), self._shape, self.name)
+
+    def set_format(self, fmt: int, param: int):
+        call("b200la_mat_set_format", self.handle, fmt, param)
+
+    def get_format(self) -> tuple[int, int]:
+        f, p = C.c_int(), C.c_int()
+        call("b200la_mat_get_format", self.handle, C.byref(f), C.byref(p))
+        return f.value, p.value
+
+    def tune(self) -> tuple[int, int, float]:
+        f, p, us = C.c_int(), C.c_int(), C.c_double()
+        call("b200la_mat_tune", self.handle, C.byref(f), C.byref(p), C.byref(us))
+        return f.value, p.value, us.value
+
+    def Clear(self):
+        if self.handle:
+            load().b200la_mat_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        if sys.is_finalizing():
+            return
+        try:
+            self.Clear()
+        except Exception:
+            pass
+
+
+def init_vector(size: int, name: str = "", platform: Platform | None = None, dtype=np.float64) -> B200_lVector:
+    return B200_lVector(size, name, platform, dtype)
+
+
+def init_matrix(rowptr, col, val, num_col=None, name: str = "", platform: Platform | None = None,
+                dtype=np.float64) -> B200_CSR_lMatrix:
+    return B200_CSR_lMatrix(rowptr, col, val, num_col, name, platform, dtype)
+
+
+class IterateControl:
+    """IterateControl(maxits, atol, rtol, dtol); defaults of
+    common/iterate_control.cc:26-29."""
+
+    def __init__(self, maxits: int = 1000, atol: float = 1e-12, rtol: float = 1e-8, dtol: float = 1e8):
+        self.maxits, self.atol, self.rtol, self.dtol = int(maxits), float(atol), float(rtol), float(dtol)
+
+
+class PreconditionerBlockJacobiStand:
+    """Block-Jacobi over the local diagonal block with lmp's Jacobi inside."""
+
+    def __init__(self):
+        self.kind = None
+
+    def Init_Jacobi(self):
+        self.kind = "Jacobi"
+
+    def SetupOperator(self, op):
+        self.op = op
+
+
+class CG:
+    """CG<LAD>: the device PCG solver behind the reference's solver API."""
+
+    def __init__(self):
+        self.method = "NoPreconditioning"
+        self.control = IterateControl()
+        self.op = None
+        self.precond = None
+        self._solver = C.c_void_p()
+        self._key = None
+        self.iter_ = 0
+        self.res_ = self.res_init_ = self.res_rel_ = 0.0
+        self.state_ = 0
+
+    def InitParameter(self, method: str):
+        assert method in ("NoPreconditioning", "Preconditioning", "RightPreconditioning",
+                          "LeftPreconditioning")
+        self.method = method
+
+    def InitControl(self, maxits: int, atol: float, rtol: float, dtol: float):
+        self.control = IterateControl(maxits, atol, rtol, dtol)
+        self._release()
+
+    def SetupOperator(self, op: B200_CSR_lMatrix):
+        self.op = op
+        self._release()
+
+    def SetupPreconditioner(self, precond: PreconditionerBlockJacobiStand):
+        # LinearSolver::SetupPreconditioner switches CG to right preconditioning
+        # (linear_solver.h:97-100)
+        self.precond = precond
+        self.method = "RightPreconditioning"
+        self._release()
+
+    def _release(self):
+        if self._solver:
+            load().b200la_cg_destroy(self._solver)
+            self._solver = C.c_void_p()
+
+    def _ensure(self):
+        if self._solver:
+            return
+        if self.op is None:
+            raise B200LAError(-1, "CG: SetupOperator was not called")
+        use_pc = self.method != "NoPreconditioning"
+        if use_pc and (self.precond is None or self.precond.kind != "Jacobi"):
+            raise B200LAError(-7, "CG: only the Jacobi preconditioner runs on this path")
+        c = self.control
+        prm = CgParams(c.maxits, c.atol, c.rtol, c.dtol, 1 if use_pc else 0)
+        call("b200la_cg_create", self.op.handle, C.byref(prm), C.byref(self._solver))
+
+    def Solve(self, b: B200_lVector, x: B200_lVector) -> int:
+        self._ensure()
+        r = CgResult()
+        call("b200la_cg_solve", self._solver, b.handle, x.handle, C.byref(r))
+        self.iter_, self.state_ = r.iters, r.state
+        self.res_, self.res_init_, self.res_rel_ = r.res, r.res_init, r.res_rel
+        return r.solver_state
+
+    def iter(self) -> int:
+        return self.iter_
+
+    def res(self) -> float:
+        return self.res_
+
+    def res_init(self) -> float:
+        return self.res_init_
+
+    def res_rel(self) -> float:
+        return self.res_rel_
+
+    def __del__(self):
+        if sys.is_finalizing():
+            return
+        try:
+            self._release()
+        except Exception:
+            pass
+
+
+def setup_CG_solver(maxits: int = 1000, atol: float = 1e-12, rtol: float = 1e-10, dtol: float = 1e6,
+                    use_precond: bool = True) -> CG:
+    """setup_CG_solver defaults (linear_solver/cg.h:271-293)."""
+    s = CG()
+    s.InitControl(maxits, atol, rtol, dtol)
+    if use_precond:
+        p = PreconditionerBlockJacobiStand()
+        p.Init_Jacobi()
+        s.SetupPreconditioner(p)
+    return s

@@ -20,6 +20,7 @@ from .oracle import (  # noqa: F401
     IMPL_NAIVE,
     IMPL_OPENMP,
     OracleResult,
+    RefSystem,
     cg,
     dot,
     invdiag,

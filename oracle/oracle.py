@@ -216,3 +216,41 @@ def ref_lmp_cg(rowptr, col, val, b, x0=None, *, rel_eps=1e-10, abs_eps=0.0, max_
     _load_ref().ref_lmp_cg_d(impl, nthreads, n, c.shape[0], rp, c, v,
                              np.ascontiguousarray(b, np.float64), x, rel_eps, abs_eps, C.byref(mi))
     return OracleResult(x, mi.value, float("nan"), float("nan"), 0)
+
+
+class RefSystem:
+    """A matrix built once in the reference's own CPU classes, for timed
+    repeated solves (the reported seconds exclude matrix construction)."""
+
+    def __init__(self, rowptr, col, val, *, impl=IMPL_OPENMP, nthreads=None):
+        lib = _load_ref()
+        lib.ref_system_create.restype = C.c_void_p
+        lib.ref_system_create.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f64p]
+        lib.ref_system_destroy.argtypes = [C.c_void_p]
+        lib.ref_system_cg.argtypes = [C.c_void_p, C.c_int, _f64p, _f64p, C.c_int, C.c_double,
+                                      C.c_double, C.c_double, _ip, _dp, _dp, _dp]
+        rp, c, v = _csr(rowptr, col, val, np.float64)
+        self.n = rp.shape[0] - 1
+        self.nthreads = int(nthreads or os.cpu_count() or 1)
+        self.impl = impl
+        self._lib = lib
+        self._h = lib.ref_system_create(impl, self.nthreads, self.n, c.shape[0], rp, c, v)
+
+    def cg(self, b, x0=None, *, maxits=1000, atol=1e-12, rtol=1e-8, dtol=1e8, precond=True):
+        x = np.zeros(self.n) if x0 is None else np.array(x0, np.float64)
+        it, res, res0, sec = C.c_int(), C.c_double(), C.c_double(), C.c_double()
+        st = self._lib.ref_system_cg(self._h, int(bool(precond)), np.ascontiguousarray(b, np.float64), x,
+                                     int(maxits), atol, rtol, dtol, C.byref(it), C.byref(res),
+                                     C.byref(res0), C.byref(sec))
+        return OracleResult(x, it.value, res.value, res0.value, st), sec.value
+
+    def close(self):
+        if self._h:
+            self._lib.ref_system_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

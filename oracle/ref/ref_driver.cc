@@ -21,6 +21,7 @@
 //                        the diagonal block's VectorMult, so the restatement
 //                        issues exactly the arithmetic the reference does.
 //   * ref_lmp_cg_*    -> the reference's own lmp cg() (lmp/solvers/cg.cc:35).
+#include <chrono>
 #include <cmath>
 #include <vector>
 
@@ -82,13 +83,10 @@ CPU_CSR_lMatrix< T > *make_matrix(int impl, int nthreads, int n, int nnz,
 }
 
 template < typename T >
-int cg_solve(int impl, int nthreads, int precond, int n, int nnz,
-             const int *rowptr, const int *col, const T *val, const T *bh,
-             T *xh, int maxits, double atol, double rtol, double dtol,
-             int *iters, double *res_out, double *res_init_out,
-             double *res_rel_out) {
-  CPU_CSR_lMatrix< T > *A = make_matrix< T >(impl, nthreads, n, nnz, rowptr,
-                                             col, val);
+int cg_solve_on(int impl, CPU_CSR_lMatrix< T > *A, int precond, int n,
+                const T *bh, T *xh, int maxits, double atol, double rtol,
+                double dtol, int *iters, double *res_out, double *res_init_out,
+                double *res_rel_out, double *seconds) {
   lVector< T > *b = make_vector< T >(impl, n, "b");
   lVector< T > *x = make_vector< T >(impl, n, "x");
   lVector< T > *r = make_vector< T >(impl, n, "r");
@@ -111,6 +109,7 @@ int cg_solve(int impl, int nthreads, int precond, int n, int nnz,
   int iter = 0;
   T alpha, beta, gamma, ressquared;
   double res;
+  const auto t0 = std::chrono::steady_clock::now();
 
   // initialization step (cg.h:104-121 / :184-204)
   A->VectorMult(*x, r);
@@ -154,14 +153,31 @@ int cg_solve(int impl, int nthreads, int precond, int n, int nnz,
     }
   }
 
+  const auto t1 = std::chrono::steady_clock::now();
+  if (seconds) *seconds = std::chrono::duration< double >(t1 - t0).count();
   x->GetBlockValues(0, n, xh);
   *iters = iter;
   *res_out = res;
   *res_init_out = res_init;
   *res_rel_out = res_init > 0. ? res / res_init : 0.;
   if (precond) jac.Clear();
-  delete Ap; delete z; delete p; delete r; delete x; delete b; delete A;
+  delete Ap; delete z; delete p; delete r; delete x; delete b;
   return state;
+}
+
+template < typename T >
+int cg_solve(int impl, int nthreads, int precond, int n, int nnz,
+             const int *rowptr, const int *col, const T *val, const T *bh,
+             T *xh, int maxits, double atol, double rtol, double dtol,
+             int *iters, double *res_out, double *res_init_out,
+             double *res_rel_out) {
+  CPU_CSR_lMatrix< T > *A = make_matrix< T >(impl, nthreads, n, nnz, rowptr,
+                                             col, val);
+  int st = cg_solve_on< T >(impl, A, precond, n, bh, xh, maxits, atol, rtol,
+                            dtol, iters, res_out, res_init_out, res_rel_out,
+                            nullptr);
+  delete A;
+  return st;
 }
 
 template < typename T >
@@ -194,9 +210,43 @@ int lmp_cg(int impl, int nthreads, int n, int nnz, const int *rowptr,
   return rv;
 }
 
+struct RefSystem {
+  int impl;
+  int n;
+  CPU_CSR_lMatrix< double > *A;
+};
+
 } // namespace
 
 extern "C" {
+
+// A matrix built once (reference COO->CSR path), for repeated timed solves:
+// the solve time reported by ref_system_cg excludes matrix construction.
+void *ref_system_create(int impl, int nthreads, int n, int nnz,
+                        const int *rowptr, const int *col, const double *val) {
+  RefSystem *s = new RefSystem;
+  s->impl = impl;
+  s->n = n;
+  s->A = make_matrix< double >(impl, nthreads, n, nnz, rowptr, col, val);
+  return s;
+}
+
+void ref_system_destroy(void *h) {
+  RefSystem *s = static_cast< RefSystem * >(h);
+  if (!s) return;
+  delete s->A;
+  delete s;
+}
+
+int ref_system_cg(void *h, int precond, const double *b, double *x,
+                  int maxits, double atol, double rtol, double dtol,
+                  int *iters, double *res, double *res_init, double *seconds) {
+  RefSystem *s = static_cast< RefSystem * >(h);
+  double rel = 0.;
+  return cg_solve_on< double >(s->impl, s->A, precond, s->n, b, x, maxits,
+                               atol, rtol, dtol, iters, res, res_init, &rel,
+                               seconds);
+}
 
 int ref_spmv_d(int impl, int nthreads, int n, int nnz, const int *rowptr,
                const int *col, const double *val, const double *x, double *y) {

@@ -1,0 +1,44 @@
+"""Records the reference's iteration counts on the full-size standard
+workloads (tests/golden/workload_counts.json), by running HiFlow3's own lmp
+CPU classes (oracle/_ref, NAIVE implementation, bit-identical to the C
+restatement) to convergence here.  bench.py's CPU legs time a bounded sample
+of iterations and scale it by these counts.
+
+Usage (repository root, oracle/_ref built):  python tests/golden/make_workload_counts.py
+"""
+import json
+import os
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+import oracle  # noqa: E402
+from ba_b200 import problems as P  # noqa: E402
+
+OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "workload_counts.json")
+
+
+def main():
+    out = {}
+    if os.path.exists(OUT):
+        out = json.load(open(OUT))
+    for name, make, rtol in (("poisson3d_128", lambda: P.poisson_3d(128), 1e-10),
+                             ("poisson2d_256", lambda: P.poisson_2d(256), 1e-10)):
+        s = make()
+        for precond in (True, False):
+            key = f"{name}/{'jacobi' if precond else 'none'}/rtol{rtol:g}"
+            if key in out:
+                continue
+            t = time.time()
+            sysr = oracle.RefSystem(s.rowptr, s.col, s.val, impl=oracle.IMPL_NAIVE, nthreads=1)
+            r, sec = sysr.cg(s.b, maxits=20000, atol=0.0, rtol=rtol, dtol=1e8, precond=precond)
+            out[key] = {"iters": r.iters, "res": r.res, "res_init": r.res_init, "state": r.state,
+                        "solve_seconds_1core": sec, "n": s.n, "nnz": s.nnz}
+            print(key, out[key], f"{time.time() - t:.1f}s", flush=True)
+            json.dump(out, open(OUT, "w"), indent=1)
+
+
+if __name__ == "__main__":
+    main()

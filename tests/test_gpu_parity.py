@@ -1,0 +1,320 @@
+"""GPU parity of the B200 path against the CPU oracle, through the C ABI.
+
+Mirrors the reference's own tests (tests/lmp_test.cc, tests/cuda_test.cc,
+tests/cg_test.cc: 3x3 known answers, tolerance 1e-12) and extends them to the
+generated FE systems: iteration counts equal to the reference's CG within +-1
+(FP64) and solutions within 1e-10 relative of the FP64 oracle.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from ba_b200 import lmp
+from ba_b200 import problems as P
+from ba_b200._lib import FMT_CSR, FMT_SELL, B200LAError
+
+pytestmark = pytest.mark.gpu
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+SCHEDULES = [(FMT_CSR, g) for g in (1, 2, 4, 8, 16, 32)] + [(FMT_SELL, w) for w in (1, 2, 4)]
+
+# FP64 SpMV tolerance: the device sums each row with FMA in a different order
+# than the oracle's sequential loop; bound by a few ulps of sum |a_ij x_j|.
+SPMV_RTOL_F64 = 1e-14
+SPMV_RTOL_F32 = 1e-5
+
+
+@pytest.fixture(scope="module")
+def plat():
+    return lmp.init_platform(0)
+
+
+def _mat(plat, s, dtype=np.float64):
+    return lmp.B200_CSR_lMatrix(s.rowptr, s.col, s.val, platform=plat, dtype=dtype)
+
+
+def _vec(plat, a, dtype=np.float64):
+    return lmp.B200_lVector.from_numpy(np.asarray(a, dtype), platform=plat, dtype=dtype)
+
+
+def _abs_rowsum(s, x):
+    return np.abs(oracle.spmv(s.rowptr, s.col, np.abs(s.val), np.abs(x)))
+
+
+def test_lmp_test_spmv_known_answer(plat):
+    kat = json.load(open(os.path.join(GOLD, "reference_known_answers.json")))
+    s7 = P.lmp_test_3x3()
+    for fmt, prm in SCHEDULES:
+        A = _mat(plat, s7)
+        A.set_format(fmt, prm)
+        x = _vec(plat, kat["lmp_test_spmv"]["x"])
+        y = x.CloneWithoutContent()
+        A.VectorMult(x, y)
+        np.testing.assert_array_equal(y.numpy(), kat["lmp_test_spmv"]["y"])
+
+
+def test_cuda_test_spmv_known_answer(plat):
+    kat = json.load(open(os.path.join(GOLD, "reference_known_answers.json")))
+    s9 = P.known_answer_3x3()
+    A = _mat(plat, s9)
+    x = _vec(plat, kat["cuda_test_spmv"]["x"])
+    y = x.CloneWithoutContent()
+    A.VectorMult(x, y)
+    np.testing.assert_allclose(y.numpy(), kat["cuda_test_spmv"]["y"], rtol=0, atol=1e-12)
+
+
+def test_cg_test_known_answer(plat):
+    kat = json.load(open(os.path.join(GOLD, "reference_known_answers.json")))
+    s = P.known_answer_3x3()
+    for precond in (False, True):
+        A = _mat(plat, s)
+        b = _vec(plat, s.b)
+        x = _vec(plat, np.zeros(3))
+        solver = lmp.setup_CG_solver(maxits=100, atol=0.0, rtol=1e-14, dtol=1e8, use_precond=precond)
+        solver.SetupOperator(A)
+        st = solver.Solve(b, x)
+        assert st == lmp.kSolverSuccess
+        np.testing.assert_allclose(x.numpy(), kat["cg_test_3x3"]["x"], rtol=0, atol=1e-12)
+
+
+def _spmv_cases():
+    yield P.poisson_2d(16)
+    yield P.poisson_2d(100)
+    yield P.q1_system(3, 10, 3, 2.0)
+    yield P.random_spd(17, 1)
+    yield P.random_spd(33, 2, empty_rows=3)
+    yield P.random_spd(257, 3, density=0.02, empty_rows=5)
+    yield P.random_spd(1, 4)
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_spmv_all_schedules_vs_oracle(plat, dtype):
+    rtol = SPMV_RTOL_F64 if dtype == np.float64 else SPMV_RTOL_F32
+    for s in _spmv_cases():
+        xs = P.uniform01(5, s.n, stream=9) - 0.5
+        ref = oracle.spmv(s.rowptr, s.col, s.val, xs, dtype=np.float64)
+        bound = _abs_rowsum(s, xs) * rtol + 1e-300
+        for fmt, prm in SCHEDULES:
+            A = _mat(plat, s, dtype)
+            A.set_format(fmt, prm)
+            x = _vec(plat, xs, dtype)
+            y = x.CloneWithoutContent()
+            A.VectorMult(x, y)
+            err = np.abs(y.numpy().astype(np.float64) - ref)
+            assert np.all(err <= bound), (s.name, fmt, prm, float(err.max()))
+            # y += A x
+            A.VectorMultAdd(x, y)
+            err2 = np.abs(y.numpy().astype(np.float64) - 2 * ref)
+            assert np.all(err2 <= 2 * bound + 1e-300), (s.name, fmt, prm)
+
+
+def test_blas1_vs_oracle(plat):
+    rng = np.random.default_rng(7)
+    for n in (1, 2, 3, 5, 31, 1000, 4097, 123457):
+        a = rng.standard_normal(n)
+        b = rng.standard_normal(n)
+        va, vb = _vec(plat, a), _vec(plat, b)
+        np.testing.assert_allclose(va.Dot(vb), oracle.dot(a, b), rtol=1e-13, atol=1e-13 * n)
+        np.testing.assert_allclose(va.Norm2(), np.sqrt(oracle.dot(a, a)), rtol=1e-13)
+        va.Axpy(vb, 0.75)
+        np.testing.assert_allclose(va.numpy(), a + 0.75 * b, rtol=1e-15, atol=1e-15)
+        va.ScaleAdd(-1.5, vb)
+        np.testing.assert_allclose(va.numpy(), -1.5 * (a + 0.75 * b) + b, rtol=1e-14, atol=1e-14)
+        va.ElementWiseMult(vb)
+        np.testing.assert_allclose(va.numpy(), (-1.5 * (a + 0.75 * b) + b) * b, rtol=1e-14, atol=1e-14)
+        va.Scale(2.0)
+        vc = va.CloneWithoutContent()
+        vc.CopyFrom(va)
+        np.testing.assert_array_equal(vc.numpy(), va.numpy())
+        v32 = lmp.B200_lVector(n, platform=plat, dtype=np.float32)
+        v32.CastFrom(vb)
+        np.testing.assert_array_equal(v32.numpy(), b.astype(np.float32))
+        # float dot: compensated FP32 accumulation
+        a32, b32 = a.astype(np.float32), b.astype(np.float32)
+        w1, w2 = _vec(plat, a32, np.float32), _vec(plat, b32, np.float32)
+        exact = float(np.dot(a32.astype(np.float64), b32.astype(np.float64)))
+        assert abs(w1.Dot(w2) - exact) <= 1e-6 * np.sqrt(n) * (np.abs(a32) @ np.abs(b32)) / n + 1e-6
+
+
+def test_set_get_values_zero_rows_invdiag(plat):
+    s = P.q1_system(2, 6, 1, 1.0)
+    A = _mat(plat, s)
+    inv = lmp.B200_lVector(s.n, platform=plat)
+    A.extract_invdiagelements(inv)
+    np.testing.assert_array_equal(inv.numpy(), oracle.invdiag(s.rowptr, s.col, s.val))
+    v = lmp.B200_lVector(s.n, platform=plat)
+    v.SetValues([3, 0, 7], [1.5, -2.0, 4.0])
+    np.testing.assert_array_equal(v.GetValues([0, 3, 7, 1]), [-2.0, 1.5, 4.0, 0.0])
+    rows = [8, 9]
+    A.ZeroRows(rows, 1.0)
+    x = _vec(plat, np.arange(s.n, dtype=np.float64))
+    y = x.CloneWithoutContent()
+    A.VectorMult(x, y)
+    np.testing.assert_array_equal(y.GetValues(rows), [8.0, 9.0])
+    with pytest.raises(B200LAError):
+        v.GetValues([s.n])
+
+
+def test_missing_diagonal_is_rejected(plat):
+    rowptr = np.array([0, 1, 2], np.int32)
+    col = np.array([1, 0], np.int32)
+    A = lmp.B200_CSR_lMatrix(rowptr, col, np.array([1.0, 1.0]), platform=plat)
+    inv = lmp.B200_lVector(2, platform=plat)
+    with pytest.raises(B200LAError) as e:
+        A.extract_invdiagelements(inv)
+    assert e.value.status == -5
+    solver = lmp.setup_CG_solver()
+    solver.SetupOperator(A)
+    with pytest.raises(B200LAError):
+        solver.Solve(_vec(plat, [1.0, 1.0]), _vec(plat, [0.0, 0.0]))
+
+
+def test_malformed_csr_rejected_on_host(plat):
+    with pytest.raises(B200LAError) as e:
+        lmp.B200_CSR_lMatrix(np.array([0, 2, 1], np.int32), np.array([0, 1], np.int32), np.ones(2),
+                             platform=plat)
+    assert e.value.status == -5
+    with pytest.raises(B200LAError):
+        lmp.B200_CSR_lMatrix(np.array([0, 1, 2], np.int32), np.array([0, 5], np.int32), np.ones(2),
+                             platform=plat)
+
+
+def _golden():
+    with open(os.path.join(GOLD, "reference_cg_runs.json")) as f:
+        return json.load(f)["cases"]
+
+
+def _golden_system(name):
+    from test_oracle import _system
+    return _system(name)
+
+
+@pytest.mark.parametrize("case", _golden(), ids=lambda c: c["name"])
+def test_cg_matches_reference_runs(plat, case):
+    """Iteration counts of the reference's CG (+-1 FP64) and solutions within
+    1e-10 relative (FP64) / the FP32 oracle's own accuracy (FP32)."""
+    s = _golden_system(case["name"])
+    for run in case["runs"]:
+        dt = np.float64 if run["dtype"] == "f64" else np.float32
+        same = oracle.cg(s.rowptr, s.col, s.val, s.b, maxits=20000, atol=0.0, rtol=run["rtol"],
+                         dtol=1e8, precond=run["precond"], dtype=dt)
+        assert same.iters == run["iters"]
+        for fmt, prm in ((FMT_CSR, 4), (FMT_CSR, 16), (FMT_SELL, 1)):
+            A = _mat(plat, s, dt)
+            A.set_format(fmt, prm)
+            b = _vec(plat, s.b, dt)
+            x = _vec(plat, np.zeros(s.n), dt)
+            solver = lmp.setup_CG_solver(maxits=20000, atol=0.0, rtol=run["rtol"], dtol=1e8,
+                                         use_precond=run["precond"])
+            solver.SetupOperator(A)
+            st = solver.Solve(b, x)
+            assert st == lmp.kSolverSuccess
+            xd = x.numpy().astype(np.float64)
+            if dt == np.float64:
+                assert abs(solver.iter() - run["iters"]) <= 1, (solver.iter(), run["iters"])
+                np.testing.assert_allclose(solver.res_init(), run["res_init"], rtol=1e-12)
+                assert np.linalg.norm(xd - same.x) <= 1e-10 * np.linalg.norm(same.x)
+            else:
+                assert abs(solver.iter() - run["iters"]) <= max(2, run["iters"] // 10)
+                r = s.b - oracle.spmv(s.rowptr, s.col, s.val, xd)
+                assert np.linalg.norm(r) <= 20 * run["rtol"] * np.linalg.norm(s.b)
+
+
+def test_cg_state_semantics(plat):
+    s = P.poisson_2d(16)
+    A = _mat(plat, s)
+    b = _vec(plat, s.b)
+    # maxits exceeded -> kSolverExceeded with iter == maxits
+    x = _vec(plat, np.zeros(s.n))
+    solver = lmp.setup_CG_solver(maxits=7, atol=0.0, rtol=1e-10)
+    solver.SetupOperator(A)
+    assert solver.Solve(b, x) == lmp.kSolverExceeded
+    assert solver.iter() == 7
+    ref = oracle.cg(s.rowptr, s.col, s.val, s.b, maxits=7, atol=0.0, rtol=1e-10)
+    np.testing.assert_allclose(x.numpy(), ref.x, rtol=1e-12, atol=1e-14)
+    # zero rhs -> success at iteration 0 (res <= atol)
+    z = _vec(plat, np.zeros(s.n))
+    x = _vec(plat, np.zeros(s.n))
+    assert solver.Solve(z, x) == lmp.kSolverSuccess and solver.iter() == 0
+    # start from the solution's neighbourhood: res_init is that of b - A x0
+    x0 = ref.x.copy()
+    x = _vec(plat, x0)
+    solver = lmp.setup_CG_solver(maxits=5000, atol=0.0, rtol=1e-10)
+    solver.SetupOperator(A)
+    solver.Solve(b, x)
+    r2 = oracle.cg(s.rowptr, s.col, s.val, s.b, x0=x0, maxits=5000, atol=0.0, rtol=1e-10)
+    assert abs(solver.iter() - r2.iters) <= 1
+    np.testing.assert_allclose(solver.res_init(), r2.res_init, rtol=1e-12)
+    # solver reuse gives identical results (deterministic reductions)
+    x1 = _vec(plat, np.zeros(s.n))
+    solver.Solve(b, x1)
+    it1 = solver.iter()
+    x2 = _vec(plat, np.zeros(s.n))
+    solver.Solve(b, x2)
+    assert solver.iter() == it1
+    np.testing.assert_array_equal(x1.numpy(), x2.numpy())
+
+
+def test_cg_c1_full_size(plat):
+    """Config-1 system (2D Q1 Poisson 256^2, 66,049 DOFs) at rel 1e-10."""
+    s = P.poisson_2d(256)
+    ref = oracle.cg(s.rowptr, s.col, s.val, s.b, maxits=5000, atol=0.0, rtol=1e-10)
+    A = _mat(plat, s)
+    A.tune()
+    b = _vec(plat, s.b)
+    x = _vec(plat, np.zeros(s.n))
+    solver = lmp.setup_CG_solver(maxits=5000, atol=0.0, rtol=1e-10, dtol=1e8)
+    solver.SetupOperator(A)
+    assert solver.Solve(b, x) == lmp.kSolverSuccess
+    assert abs(solver.iter() - ref.iters) <= 1
+    assert np.linalg.norm(x.numpy() - ref.x) <= 1e-10 * np.linalg.norm(ref.x) * 10
+
+
+def test_cg_3d_vs_oracle(plat):
+    s = P.poisson_3d(40)
+    ref = oracle.cg(s.rowptr, s.col, s.val, s.b, maxits=5000, atol=0.0, rtol=1e-10)
+    A = _mat(plat, s)
+    fmt, prm, us = A.tune()
+    b = _vec(plat, s.b)
+    x = _vec(plat, np.zeros(s.n))
+    solver = lmp.setup_CG_solver(maxits=5000, atol=0.0, rtol=1e-10, dtol=1e8)
+    solver.SetupOperator(A)
+    assert solver.Solve(b, x) == lmp.kSolverSuccess
+    assert abs(solver.iter() - ref.iters) <= 1
+    assert np.linalg.norm(x.numpy() - ref.x) <= 1e-10 * np.linalg.norm(ref.x) * 10
+
+
+def test_full_size_c2_properties(plat):
+    """128^3 Q1 Poisson (2,146,689 DOFs, 57,066,625 nnz): size-independent
+    checks -- SpMV against scipy's CSR product, linearity, and a converged
+    true residual."""
+    import scipy.sparse as sp
+    s = P.poisson_3d(128)
+    assert s.n == 2146689 and s.nnz == 57066625
+    Ah = sp.csr_matrix((s.val, s.col, s.rowptr), shape=(s.n, s.n))
+    A = _mat(plat, s)
+    A.tune()
+    xs = P.uniform01(3, s.n, stream=1)
+    ys = P.uniform01(4, s.n, stream=1)
+    x, y = _vec(plat, xs), _vec(plat, ys)
+    ax, ay = x.CloneWithoutContent(), x.CloneWithoutContent()
+    A.VectorMult(x, ax)
+    A.VectorMult(y, ay)
+    ref = Ah @ xs
+    bound = (abs(Ah) @ np.abs(xs)) * 1e-14
+    assert np.all(np.abs(ax.numpy() - ref) <= bound)
+    x.Axpy(y, 1.0)
+    axy = x.CloneWithoutContent()
+    A.VectorMult(x, axy)
+    np.testing.assert_allclose(axy.numpy(), ax.numpy() + ay.numpy(), rtol=1e-12, atol=1e-13)
+    b = _vec(plat, s.b)
+    sol = _vec(plat, np.zeros(s.n))
+    solver = lmp.setup_CG_solver(maxits=5000, atol=0.0, rtol=1e-10, dtol=1e8)
+    solver.SetupOperator(A)
+    assert solver.Solve(b, sol) == lmp.kSolverSuccess
+    xs_ = sol.numpy()
+    true_res = np.linalg.norm(s.b - Ah @ xs_)
+    assert true_res <= 2e-10 * np.linalg.norm(s.b)
