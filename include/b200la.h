@@ -100,6 +100,23 @@ int b200la_vec_scaleadd(b200la_vec y, double alpha, b200la_vec x); /* y.ScaleAdd
 int b200la_vec_scale(b200la_vec v, double alpha);                  /* Scale */
 int b200la_vec_elementwise_mult(b200la_vec y, b200la_vec x);       /* ElementWiseMult: y .*= x */
 
+/* Dot product that allocates nothing (no counterpart in the reference; its
+ * lmp Dot is the entry above).  For callers that cannot call cudaMalloc:
+ * cudaMalloc/cudaFree can stall the whole device while overlapped work is in
+ * flight, and applications that give all device memory to their own pool, or
+ * run this library as a plug-in under a fixed quota, may not allocate
+ * outside it.  x and y are device buffers of n values of dtype on the current
+ * device; the total is written to *out (host) after `stream` (a
+ * cudaStream_t, NULL = legacy default stream) is synchronised.  The reduction
+ * scratch is one fixed ~32 KB __device__ array that every GPU loading the
+ * library keeps until exit, so n is limited to 16,777,216 elements; larger n
+ * is rejected with B200LA_ERR_UNSUPPORTED.  The first call on a device looks
+ * up the array's device address and caches it; make that first call before
+ * any stream capture.  All calls share the array: calls that overlap on the
+ * GPU race and must be serialised by the caller. */
+int b200la_dot_noalloc(const void *x, const void *y, int64_t n, int dtype, void *stream,
+                       double *out);
+
 /* ---- matrices: lMatrix<T> / CSR_lMatrix<T> (lmp/lmatrix.h:39-468),
  * GPU_CSR_lMatrix (lmp/cuda/lmatrix_csr_gpu.cc) ----------------------------
  * Upload a host CSR (row pointer int32[nrow+1], col int32[nnz], values of
