@@ -31,6 +31,30 @@ class CgParams(C.Structure):
                 ("dtol", C.c_double), ("precond", C.c_int)]
 
 
+class MpParams(C.Structure):
+    _fields_ = [("max_outer", C.c_int), ("atol", C.c_double), ("rtol", C.c_double),
+                ("dtol", C.c_double), ("inner_maxits", C.c_int), ("inner_rtol", C.c_double),
+                ("precond", C.c_int), ("tune", C.c_int)]
+
+
+class MpResult(C.Structure):
+    _fields_ = [("outer", C.c_int), ("inner_iters", C.c_int), ("state", C.c_int),
+                ("solver_state", C.c_int), ("res", C.c_double), ("res_init", C.c_double),
+                ("res_rel", C.c_double)]
+
+
+class BatchParams(C.Structure):
+    _fields_ = [("capacity", C.c_int), ("mixed", C.c_int), ("precond", C.c_int), ("max_outer", C.c_int),
+                ("inner_maxits", C.c_int), ("lanes", C.c_int), ("tile_rows", C.c_int), ("reserved", C.c_int),
+                ("atol", C.c_double), ("rtol", C.c_double), ("dtol", C.c_double), ("inner_rtol", C.c_double)]
+
+
+class SysResult(C.Structure):
+    _fields_ = [("state", C.c_int), ("solver_state", C.c_int), ("iters", C.c_int), ("outer", C.c_int),
+                ("phase_done", C.c_int), ("reserved", C.c_int), ("res", C.c_double), ("res_init", C.c_double),
+                ("res_rel", C.c_double), ("device_us", C.c_double)]
+
+
 class CgResult(C.Structure):
     _fields_ = [("iters", C.c_int), ("state", C.c_int), ("solver_state", C.c_int),
                 ("reserved", C.c_int), ("res", C.c_double), ("res_init", C.c_double),
@@ -87,6 +111,27 @@ _SIGS = {
     "b200la_cg_solve": [_vp, _vp, _vp, _P(CgResult)],
     "b200la_cg_profile": [_vp, _vp, _vp, _i, _P(_d)],
     "b200la_pcg_solve": [_vp, _vp, _vp, _P(CgParams), _P(CgResult)],
+    "b200la_batch_create": [_vp, _P(BatchParams), _P(_vp)],
+    "b200la_batch_destroy": [_vp],
+    "b200la_batch_slot_bytes": [_i64, _i64, _i, _P(_i64)],
+    "b200la_batch_add": [_vp, _i, _i64, _vp, _vp, _vp, _vp, _vp, _P(_i)],
+    "b200la_batch_remove": [_vp, _i],
+    "b200la_batch_run": [_vp, _i, _P(_i)],
+    "b200la_batch_result": [_vp, _i, _vp, _P(SysResult)],
+    "b200la_batch_info": [_vp, _P(_i), _P(_i64)],
+    "b200la_batch_tune": [_vp, _P(_i), _P(_d)],
+    "b200la_batch_restart": [_vp],
+    "b200la_batch_last_run": [_vp, _P(_i), _P(_d)],
+    "b200la_batch_profile": [_vp, _i, _P(_d), _P(_i64)],
+    "b200la_batch_add_q1": [_vp, _i, _i, C.c_uint64, _d, _P(_i)],
+    "b200la_batch_get_system": [_vp, _i, _vp, _vp, _vp, _vp],
+    "b200la_batch_slot_size": [_vp, _i, _P(_i), _P(_i64)],
+    "b200la_q1_size": [_i, _i, _P(_i64), _P(_i64)],
+    "b200la_q1_assemble": [_vp, _i, _i, C.c_uint64, _d, _vp, _vp, _vp, _vp],
+    "b200la_mp_create": [_vp, _P(MpParams), _P(_vp)],
+    "b200la_mp_destroy": [_vp],
+    "b200la_mp_inner_matrix": [_vp, _P(_vp)],
+    "b200la_mp_solve": [_vp, _vp, _vp, _P(MpResult)],
 }
 _RESTYPE = {"b200la_version": C.c_char_p, "b200la_last_error": C.c_char_p}
 

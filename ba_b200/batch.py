@@ -1,0 +1,158 @@
+"""Batched and served PCG over many independent systems (no counterpart in
+the reference, which solves one system per CG<LAD> call).
+
+``Batch`` wraps the b200la_batch_* C ABI: systems are uploaded into slots,
+``run`` advances every running system with one CUDA-graph launch, and
+systems can be added and removed between runs (continuous batching).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import sys
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from ._lib import BatchParams, SysResult, call, load
+from .lmp import Platform, init_platform
+
+
+@dataclass
+class SystemResult:
+    state: int
+    solver_state: int
+    iters: int
+    outer: int
+    done: bool
+    res: float
+    res_init: float
+    res_rel: float
+    device_us: float
+    x: np.ndarray | None = None
+
+
+def slot_bytes(n: int, nnz: int, mixed: bool) -> int:
+    out = C.c_int64()
+    call("b200la_batch_slot_bytes", int(n), int(nnz), 1 if mixed else 0, C.byref(out))
+    return out.value
+
+
+class Batch:
+    def __init__(self, capacity: int, *, mixed: bool = True, precond: bool = True, rtol: float = 1e-8,
+                 atol: float = 0.0, dtol: float = 1e8, inner_rtol: float = 1e-4, max_outer: int = 30,
+                 inner_maxits: int = 100000, lanes: int = 0, tile_rows: int = 0,
+                 platform: Platform | None = None):
+        self.platform = platform or init_platform()
+        self.mixed = mixed
+        prm = BatchParams(int(capacity), int(mixed), int(precond), int(max_outer), int(inner_maxits),
+                          int(lanes), int(tile_rows), 0, float(atol), float(rtol), float(dtol),
+                          float(inner_rtol))
+        self.handle = C.c_void_p()
+        call("b200la_batch_create", self.platform.handle, C.byref(prm), C.byref(self.handle))
+        self._keep = {}
+        self._sizes = {}
+
+    def add(self, rowptr, col, val, rhs, x0=None) -> int:
+        rp = np.ascontiguousarray(rowptr, np.int32)
+        cl = np.ascontiguousarray(col, np.int32)
+        vv = np.ascontiguousarray(val, np.float64)
+        bb = np.ascontiguousarray(rhs, np.float64)
+        xx = None if x0 is None else np.ascontiguousarray(x0, np.float64)
+        slot = C.c_int()
+        call("b200la_batch_add", self.handle, rp.shape[0] - 1, cl.shape[0], rp.ctypes.data_as(C.c_void_p),
+             cl.ctypes.data_as(C.c_void_p), vv.ctypes.data_as(C.c_void_p), bb.ctypes.data_as(C.c_void_p),
+             None if xx is None else xx.ctypes.data_as(C.c_void_p), C.byref(slot))
+        # host buffers must stay valid until the copies run (next run)
+        self._keep[slot.value] = (rp, cl, vv, bb, xx)
+        self._sizes[slot.value] = rp.shape[0] - 1
+        return slot.value
+
+    def add_system(self, s, x0=None) -> int:
+        return self.add(s.rowptr, s.col, s.val, s.b, x0)
+
+    def add_q1(self, dim: int, cells: int, seed: int, sigma: float) -> int:
+        """Assemble a Q1 diffusion system on the device into a free slot."""
+        slot = C.c_int()
+        call("b200la_batch_add_q1", self.handle, int(dim), int(cells), C.c_uint64(seed), float(sigma),
+             C.byref(slot))
+        n, nnz = C.c_int(), C.c_int64()
+        call("b200la_batch_slot_size", self.handle, slot.value, C.byref(n), C.byref(nnz))
+        self._sizes[slot.value] = n.value
+        return slot.value
+
+    def get_system(self, slot: int):
+        """(rowptr, col, val, rhs) of a slot, copied back to the host."""
+        n, nnz = C.c_int(), C.c_int64()
+        call("b200la_batch_slot_size", self.handle, int(slot), C.byref(n), C.byref(nnz))
+        rp = np.empty(n.value + 1, np.int32)
+        cl = np.empty(nnz.value, np.int32)
+        vv = np.empty(nnz.value, np.float64)
+        bb = np.empty(n.value, np.float64)
+        call("b200la_batch_get_system", self.handle, int(slot), rp.ctypes.data_as(C.c_void_p),
+             cl.ctypes.data_as(C.c_void_p), vv.ctypes.data_as(C.c_void_p), bb.ctypes.data_as(C.c_void_p))
+        return rp, cl, vv, bb
+
+    def remove(self, slot: int):
+        call("b200la_batch_remove", self.handle, int(slot))
+        self._keep.pop(slot, None)
+        self._sizes.pop(slot, None)
+
+    def run(self, max_passes: int = 1 << 30) -> int:
+        active = C.c_int()
+        call("b200la_batch_run", self.handle, int(max_passes), C.byref(active))
+        self._keep.clear()
+        return active.value
+
+    def result(self, slot: int, with_x: bool = True) -> SystemResult:
+        r = SysResult()
+        x = None
+        ptr = None
+        if with_x:
+            x = np.empty(self.slot_n(slot), np.float64)
+            ptr = x.ctypes.data_as(C.c_void_p)
+        call("b200la_batch_result", self.handle, int(slot), ptr, C.byref(r))
+        return SystemResult(r.state, r.solver_state, r.iters, r.outer, bool(r.phase_done), r.res, r.res_init,
+                            r.res_rel, r.device_us, x)
+
+    def slot_n(self, slot: int) -> int:
+        return self._sizes[slot]
+
+    def last_passes(self) -> int:
+        """Device-loop passes taken by the last run (each pass = 4 kernel launches)."""
+        n = C.c_int()
+        call("b200la_batch_last_run", self.handle, C.byref(n), None)
+        return n.value
+
+    def restart(self):
+        """Restart every system from x = 0 (matrices and right-hand sides stay resident)."""
+        call("b200la_batch_restart", self.handle)
+
+    def tune(self) -> tuple[int, float]:
+        lanes, us = C.c_int(), C.c_double()
+        call("b200la_batch_tune", self.handle, C.byref(lanes), C.byref(us))
+        return lanes.value, us.value
+
+    def profile(self, reps: int = 5) -> tuple[float, int]:
+        """(ms per batched SpMV over every slot, its algorithmic bytes)."""
+        ms, nb = C.c_double(), C.c_int64()
+        call("b200la_batch_profile", self.handle, int(reps), C.byref(ms), C.byref(nb))
+        return ms.value, nb.value
+
+    def info(self) -> tuple[int, int]:
+        u, b = C.c_int(), C.c_int64()
+        call("b200la_batch_info", self.handle, C.byref(u), C.byref(b))
+        return u.value, b.value
+
+    def close(self):
+        if self.handle:
+            load().b200la_batch_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        if sys.is_finalizing():
+            return
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,1041 @@
+// Batched and served PCG: many independent systems of uneven size solved by
+// one CUDA-graph launch whose body kernels sweep all active systems at once.
+//
+// The reference solves one system per CG<LAD> call; there is no batched
+// path (SURVEY: batching/serving has no reference counterpart).  Each system
+// follows the reference's recurrence (Jacobi-PCG, cg.h:165-246) inside an
+// MPIR-style refinement (mpir.cc:52-230): FP64 residual/update/test around an
+// FP32 inner solve, or, in FP64 mode, a plain FP64 (P)CG.
+//
+// Work decomposition: every system is cut into tiles of consecutive rows;
+// a thread block handles one tile at a time (grid-stride over the tile
+// list), so big and small systems share every launch and the load balances
+// at tile granularity.  Per-system dot products are reduced deterministically:
+// each tile writes its partial sums, and the last tile of a system to finish
+// (per-system atomic ticket) adds that system's partials in tile order.
+//
+// Each system walks through phases, advanced by the last tile of the kernel
+// that finishes a phase, so all tiles of a system see one phase per launch:
+//   RESID   K4: r64 = b - A64 x (FP64), ||r64||, outer test; restart the
+//               inner solve from c = 0 with r = (float)r64, z = invD r, p = z
+//   INNER   K1: Ap = A p, p.Ap      K2: c += a p, r -= a Ap, r.r, r.z, inner
+//               test -> CORRECT      K3: p = b p + z
+//   CORRECT K3: x += (double)c -> RESID (mixed) or DONE (FP64 mode)
+//   DONE    skipped by every kernel
+// The body of the graph's WHILE node is K1 K2 K3 K4; the last block of K4
+// clears the loop condition when no system is active or the pass budget is
+// spent, so the device loop always ends.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "internal.cuh"
+
+namespace b200la {
+
+enum BatchPhase : int { PH_EMPTY = 0, PH_RESID = 1, PH_INNER = 2, PH_CORRECT = 3, PH_DONE = 4 };
+
+// Device descriptor of one system slot.  Structure (rowptr, col) is shared by
+// the FP64 and FP32 values; vectors are the slot's own buffers.
+template <typename T> struct SysDesc {
+  int n;
+  int nnz;
+  const int *rowptr;
+  const int *col;
+  const double *val64;
+  const T *val;       // inner-solve values (FP32 copy, or val64 in FP64 mode)
+  const double *b;
+  double *x;
+  T *c, *r, *p, *Ap;
+  const T *invd;
+};
+
+// Per-system scalars and counters (device).
+struct SysState {
+  int phase;
+  int inner_iter;      // iterations of the current inner solve
+  int total_iter;      // inner iterations over all passes
+  int outer;           // refinement passes started
+  double rz, pAp, alpha, beta;
+  double res_in, res_in0;   // inner recurrence residual and its start value
+  double res, res0;         // FP64 true residual and the initial one
+  unsigned long long t_begin;  // %globaltimer at the system's first residual
+  unsigned long long t_done;   // %globaltimer when the system finished
+  int state;                   // B200LA_* iterate state at the end
+  unsigned bad_row;            // first row without a usable diagonal (Jacobi), else ~0u
+  unsigned ticket[4];
+};
+
+struct BatchParams {
+  int max_outer;
+  int inner_maxits;
+  double atol, rtol, dtol;  // outer (FP64) test
+  double inner_rtol;        // inner test relative to its start residual
+  int precond;
+  int mixed;                // 1: FP32 inner + FP64 refinement; 0: FP64 CG
+};
+
+struct BatchGlobals {
+  int active;          // systems not DONE (and not EMPTY)
+  int passes;          // body passes taken by this launch
+  int max_passes;      // pass budget of this launch
+  int ntiles;          // tiles in the current tile list
+  unsigned ticket;     // last block of K4
+  unsigned pad2;
+  unsigned long long t_start;
+};
+
+struct Tile {
+  int sys;
+  int row0;
+  int rows;
+  int first;  // index of the system's first tile (its partials start there)
+  int count;  // tiles of the system
+  int pad;
+};
+
+__device__ __forceinline__ unsigned long long globaltimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Deterministic per-system reduction: the block's sums go to part[k][tile];
+// the last tile of the system (ticket over `count` tiles) adds the system's
+// partials in tile order.  Returns true in that block; totals in v[] of
+// thread 0.  Must be called by every thread of the block.
+template <int NV>
+__device__ __forceinline__ bool tile_sum_last(double (&v)[NV], double *part, int64_t ntiles, int tile, int first,
+                                              int count, unsigned *ticket) {
+  __shared__ double smem[NV * 32];
+  __shared__ bool is_last;
+  block_sum<NV>(v, smem);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) part[k * ntiles + tile] = v[k];
+    __threadfence();
+    unsigned t = atomicInc(ticket, (unsigned)count - 1);
+    is_last = (t == (unsigned)count - 1);
+  }
+  __syncthreads();
+  if (!is_last) return false;
+  __threadfence();
+#pragma unroll
+  for (int k = 0; k < NV; ++k) {
+    double a = 0.0;
+    for (int i = threadIdx.x; i < count; i += blockDim.x) a += __ldcg(&part[k * ntiles + first + i]);
+    v[k] = a;
+  }
+  block_sum<NV>(v, smem);
+  return true;
+}
+
+__device__ __forceinline__ int outer_check(double res, double res0, const BatchParams &p) {
+  if (res <= p.atol) return B200LA_SUCCESS_ABS;
+  if (res < p.rtol * res0) return B200LA_SUCCESS_REL;
+  if (!(res <= p.dtol * res0)) return B200LA_FAIL_DIV;
+  return B200LA_ITERATE;
+}
+
+}  // namespace b200la
+
+namespace b200la {
+
+__device__ __forceinline__ int load_phase(const SysState *s) { return *(volatile const int *)&s->phase; }
+
+__device__ __forceinline__ void finish_system(SysState &S, BatchGlobals *g, int state) {
+  S.state = state;
+  S.phase = PH_DONE;
+  S.t_done = globaltimer();
+  atomicSub(&g->active, 1);
+}
+
+// ---- K1: Ap = A p and p.Ap for INNER systems -------------------------------
+template <typename T, int G>
+__global__ void __launch_bounds__(kBlock) batch_spmv_kernel(const Tile *__restrict__ tiles,
+                                                            const SysDesc<T> *__restrict__ desc, SysState *st,
+                                                            double *part, int64_t part_stride, BatchGlobals *g,
+                                                            BatchParams prm) {
+  const int ntiles = g->ntiles;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const Tile tl = tiles[t];
+    SysState &S = st[tl.sys];
+    if (load_phase(&S) != PH_INNER) continue;
+    const SysDesc<T> d = desc[tl.sys];
+    Acc<T> acc;
+    for (int base = 0; base < tl.rows; base += kBlock / G) {
+      const int lr = base + (int)threadIdx.x / G;
+      const bool valid = lr < tl.rows;
+      const int row = tl.row0 + lr;
+      T y = csr_row_group<T, G>(d.rowptr, d.col, d.val, d.p, row, valid);
+      if (valid && (threadIdx.x & (G - 1)) == 0) {
+        d.Ap[row] = y;
+        acc.add(y * d.p[row]);
+      }
+    }
+    double v[1] = {acc.value()};
+    if (tile_sum_last<1>(v, part, part_stride, t, tl.first, tl.count, &S.ticket[0]) && threadIdx.x == 0) {
+      S.pAp = v[0];
+      const double alpha = S.rz / v[0];
+      S.alpha = alpha;
+      if (!(v[0] != 0.0) || !isfinite(alpha)) {
+        // breakdown: mixed mode keeps the correction so far and refines;
+        // FP64 mode ends the system with an error state
+        if (prm.mixed) S.phase = PH_CORRECT;
+        else finish_system(S, g, B200LA_FAIL_BREAKDOWN);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ---- K2: c += alpha p, r -= alpha Ap, r.r and r.z; inner test ---------------
+template <typename T, bool PRE>
+__global__ void __launch_bounds__(kBlock) batch_update_kernel(const Tile *__restrict__ tiles,
+                                                              const SysDesc<T> *__restrict__ desc, SysState *st,
+                                                              double *part, int64_t part_stride, BatchGlobals *g,
+                                                              BatchParams prm) {
+  const int ntiles = g->ntiles;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const Tile tl = tiles[t];
+    SysState &S = st[tl.sys];
+    if (load_phase(&S) != PH_INNER) continue;
+    const SysDesc<T> d = desc[tl.sys];
+    const T alpha = (T)S.alpha;
+    Acc<T> rr, rz;
+    for (int i = tl.row0 + threadIdx.x; i < tl.row0 + tl.rows; i += kBlock) {
+      d.c[i] = fma(alpha, d.p[i], d.c[i]);
+      const T r = fma(-alpha, d.Ap[i], d.r[i]);
+      d.r[i] = r;
+      rr.add(r * r);
+      if (PRE) rz.add(r * (r * d.invd[i]));
+    }
+    double v[2] = {rr.value(), rz.value()};
+    if (tile_sum_last<2>(v, part, part_stride, t, tl.first, tl.count, &S.ticket[1]) && threadIdx.x == 0) {
+      const double res = sqrt(v[0]);
+      const double rz_new = PRE ? v[1] : v[0];
+      S.res_in = res;
+      S.inner_iter += 1;
+      S.total_iter += 1;
+      if (prm.mixed) {
+        // inner solve: stop at inner_rtol (strict, as IterateControl) or its iteration budget
+        // (no tighter than half the outer target: the last pass does not over-solve)
+        const double target = fmax(prm.inner_rtol * S.res_in0, 0.5 * prm.rtol * S.res0);
+        if (res < target || S.inner_iter >= prm.inner_maxits || !(res == res)) S.phase = PH_CORRECT;
+      } else {
+        // FP64 CG: IterateControl::Check on the recurrence residual (cg.h:214-225)
+        int s = B200LA_ITERATE;
+        if (res <= prm.atol) s = B200LA_SUCCESS_ABS;
+        else if (res < prm.rtol * S.res_in0) s = B200LA_SUCCESS_REL;
+        else if (res > prm.dtol * S.res_in0) s = B200LA_FAIL_DIV;
+        else if (S.inner_iter >= prm.inner_maxits) s = B200LA_FAIL_MAXITS;
+        if (s != B200LA_ITERATE) {
+          S.state = s;
+          S.res = res;
+          S.phase = PH_CORRECT;
+        }
+      }
+      S.beta = rz_new / S.rz;
+      S.rz = rz_new;
+    }
+    __syncthreads();
+  }
+}
+
+// ---- K3: p = beta p + z (INNER); x += c (CORRECT) ---------------------------
+template <typename T, bool PRE>
+__global__ void __launch_bounds__(kBlock) batch_direction_kernel(const Tile *__restrict__ tiles,
+                                                                 const SysDesc<T> *__restrict__ desc, SysState *st,
+                                                                 double *part, int64_t part_stride, BatchGlobals *g,
+                                                                 BatchParams prm) {
+  const int ntiles = g->ntiles;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const Tile tl = tiles[t];
+    SysState &S = st[tl.sys];
+    const int ph = load_phase(&S);
+    if (ph == PH_INNER) {
+      const SysDesc<T> d = desc[tl.sys];
+      const T beta = (T)S.beta;
+      for (int i = tl.row0 + threadIdx.x; i < tl.row0 + tl.rows; i += kBlock)
+        d.p[i] = fma(beta, d.p[i], PRE ? d.r[i] * d.invd[i] : d.r[i]);
+    } else if (ph == PH_CORRECT) {
+      const SysDesc<T> d = desc[tl.sys];
+      for (int i = tl.row0 + threadIdx.x; i < tl.row0 + tl.rows; i += kBlock) d.x[i] += (double)d.c[i];
+      double v[1] = {0.0};
+      if (tile_sum_last<1>(v, part, part_stride, t, tl.first, tl.count, &S.ticket[2]) && threadIdx.x == 0) {
+        if (prm.mixed) S.phase = PH_RESID;
+        else finish_system(S, g, S.state);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ---- K4: FP64 residual, outer test, inner restart ----------------------------
+template <typename T, int G, bool PRE>
+__global__ void __launch_bounds__(kBlock) batch_residual_kernel(const Tile *__restrict__ tiles,
+                                                                const SysDesc<T> *__restrict__ desc, SysState *st,
+                                                                double *part, int64_t part_stride, BatchGlobals *g,
+                                                                BatchParams prm, cudaGraphConditionalHandle loop) {
+  const int ntiles = g->ntiles;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const Tile tl = tiles[t];
+    SysState &S = st[tl.sys];
+    if (load_phase(&S) != PH_RESID) continue;
+    const SysDesc<T> d = desc[tl.sys];
+    Acc<double> rr64;
+    Acc<T> rrin, rzin;
+    for (int base = 0; base < tl.rows; base += kBlock / G) {
+      const int lr = base + (int)threadIdx.x / G;
+      const bool valid = lr < tl.rows;
+      const int row = tl.row0 + lr;
+      double y = csr_row_group<double, G>(d.rowptr, d.col, d.val64, d.x, row, valid);
+      if (valid && (threadIdx.x & (G - 1)) == 0) {
+        const double r64 = d.b[row] - y;
+        rr64.add(r64 * r64);
+        const T r = (T)r64;
+        d.r[row] = r;
+        d.c[row] = T(0);
+        const T z = PRE ? r * d.invd[row] : r;
+        d.p[row] = z;
+        rrin.add(r * r);
+        rzin.add(r * z);
+      }
+    }
+    double v[3] = {rr64.value(), rrin.value(), rzin.value()};
+    if (tile_sum_last<3>(v, part, part_stride, t, tl.first, tl.count, &S.ticket[3]) && threadIdx.x == 0) {
+      const double res = sqrt(v[0]);
+      S.res = res;
+      if (S.outer == 0) {
+        S.res0 = res;
+        S.t_begin = globaltimer();
+      }
+      int s = outer_check(res, S.res0, prm);
+      if (s == B200LA_ITERATE && S.outer >= prm.max_outer) s = B200LA_FAIL_MAXITS;
+      if (prm.precond && S.bad_row != 0xffffffffu) s = B200LA_FAIL_BREAKDOWN;  // Jacobi needs every diagonal
+      if (s != B200LA_ITERATE) {
+        finish_system(S, g, s);
+      } else {
+        S.outer += 1;
+        S.inner_iter = 0;
+        S.res_in = S.res_in0 = sqrt(v[1]);
+        S.rz = PRE ? v[2] : v[1];
+        S.phase = PH_INNER;
+      }
+    }
+    __syncthreads();
+  }
+  // the last block of the launch ends the pass and decides whether the
+  // device loop runs another one
+  __shared__ bool last;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicInc(&g->ticket, gridDim.x - 1) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    const int passes = g->passes + 1;
+    g->passes = passes;
+    const int active = *(volatile int *)&g->active;
+    cudaGraphSetConditional(loop, (active > 0 && passes < g->max_passes) ? 1u : 0u);
+  }
+}
+
+__global__ void batch_start_kernel(BatchGlobals *g) {
+  g->passes = 0;
+  g->ticket = 0;
+  g->t_start = globaltimer();
+}
+
+}  // namespace b200la
+
+using namespace b200la;
+
+namespace {
+
+// Host record of one slot.
+struct HostSys {
+  bool used = false;
+  int n = 0;
+  int nnz = 0;
+  void *chunk = nullptr;   // one allocation holds all of the slot's buffers
+  size_t bytes = 0;
+  SysDesc<double> d64{};
+  SysDesc<float> d32{};
+};
+
+size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
+
+}  // namespace
+
+struct b200la_batch_s {
+  b200la_ctx ctx;
+  b200la_batch_params prm;
+  BatchParams kp;
+  int lanes;
+  int tile_rows;
+  int capacity;
+  int64_t max_tiles;
+  std::vector<HostSys> sys;
+  // device
+  void *desc;            // SysDesc<T>[capacity]
+  SysState *st;          // [capacity]
+  Tile *tiles;           // [max_tiles]
+  double *part;          // [3][max_tiles]
+  BatchGlobals *glob;
+  // host mirrors
+  SysState *st_host;     // pinned [capacity]
+  BatchGlobals *glob_host;
+  std::vector<Tile> tiles_host;
+  int64_t device_bytes;
+  bool tiles_dirty;
+  cudaGraph_t graph;
+  cudaGraphExec_t exec;
+  int grid;
+};
+
+namespace {
+
+template <typename T> SysDesc<T> &desc_of(HostSys &h);
+template <> SysDesc<double> &desc_of<double>(HostSys &h) { return h.d64; }
+template <> SysDesc<float> &desc_of<float>(HostSys &h) { return h.d32; }
+
+// Bytes one slot needs for a system (the admission test of the request loop).
+size_t slot_bytes(int64_t n, int64_t nnz, bool mixed) {
+  size_t tb = mixed ? 4 : 8;
+  size_t b = align256(sizeof(int) * (n + 1)) + align256(sizeof(int) * nnz) + align256(8 * nnz);
+  if (mixed) b += align256(4 * nnz);
+  b += 2 * align256(8 * n);      // b, x
+  b += 5 * align256(tb * n);     // c, r, p, Ap, invd
+  return b;
+}
+
+template <typename T>
+__global__ void slot_setup_kernel(SysDesc<T> d, unsigned *bad) {
+  // FP32 values (mixed mode), inverse diagonal in the inner type, x = 0 if
+  // requested by the caller (done on the host side), zero work vectors.
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < d.nnz; j += stride)
+    if ((const void *)d.val != (const void *)d.val64) const_cast<T *>(d.val)[j] = (T)d.val64[j];
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < d.n; i += stride) {
+    int k = -1;
+    for (int j = d.rowptr[i]; j < d.rowptr[i + 1]; ++j)
+      if (d.col[j] == i) { k = j; break; }
+    const T a = k >= 0 ? (T)d.val64[k] : T(0);
+    if (a == T(0)) {
+      atomicMin(bad, (unsigned)i);
+      const_cast<T *>(d.invd)[i] = T(0);
+    } else {
+      const_cast<T *>(d.invd)[i] = T(1) / a;
+    }
+    d.c[i] = T(0);
+    d.r[i] = T(0);
+    d.p[i] = T(0);
+    d.Ap[i] = T(0);
+  }
+}
+
+// Plain batched SpMV Ap = A p over every tile (schedule timing only).
+template <typename T, int G>
+__global__ void __launch_bounds__(kBlock) batch_spmv_plain_kernel(const Tile *__restrict__ tiles, int ntiles,
+                                                                  const SysDesc<T> *__restrict__ desc) {
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const Tile tl = tiles[t];
+    const SysDesc<T> d = desc[tl.sys];
+    for (int base = 0; base < tl.rows; base += kBlock / G) {
+      const int lr = base + (int)threadIdx.x / G;
+      const bool valid = lr < tl.rows;
+      const int row = tl.row0 + lr;
+      T y = csr_row_group<T, G>(d.rowptr, d.col, d.val, d.p, row, valid);
+      if (valid && (threadIdx.x & (G - 1)) == 0) d.Ap[row] = y;
+    }
+  }
+}
+
+}  // namespace
+
+namespace {
+
+using BatchHandle = b200la_batch;
+
+template <typename T, int G, bool PRE>
+int build_graph_t(BatchHandle B) {
+  b200la_ctx c = B->ctx;
+  if (B->exec) { cudaGraphExecDestroy(B->exec); B->exec = nullptr; }
+  if (B->graph) { cudaGraphDestroy(B->graph); B->graph = nullptr; }
+  int occ = 1 << 30;
+  const void *ks[] = {(const void *)batch_spmv_kernel<T, G>, (const void *)batch_update_kernel<T, PRE>,
+                      (const void *)batch_direction_kernel<T, PRE>, (const void *)batch_residual_kernel<T, G, PRE>};
+  for (const void *k : ks) {
+    int o = 0;
+    B_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k, kBlock, 0));
+    occ = std::min(occ, std::max(o, 1));
+  }
+  B->grid = c->num_sms * occ;
+  cudaGraph_t g;
+  B_CUDA(cudaGraphCreate(&g, 0));
+  B->graph = g;
+  cudaGraphConditionalHandle h;
+  B_CUDA(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+  cudaStream_t cs;
+  B_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+  // outer graph: start kernel -> WHILE(body)
+  B_CUDA(cudaStreamBeginCaptureToGraph(cs, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  batch_start_kernel<<<1, 1, 0, cs>>>(B->glob);
+  cudaGraph_t cap;
+  cudaError_t e1 = cudaStreamEndCapture(cs, &cap);
+  if (e1 != cudaSuccess) {
+    cudaStreamDestroy(cs);
+    B_CUDA(e1);
+  }
+  size_t nn = 0;
+  B_CUDA(cudaGraphGetNodes(g, nullptr, &nn));
+  std::vector<cudaGraphNode_t> nodes(nn);
+  B_CUDA(cudaGraphGetNodes(g, nodes.data(), &nn));
+  cudaGraphNodeParams np = {};
+  np.type = cudaGraphNodeTypeConditional;
+  np.conditional.handle = h;
+  np.conditional.type = cudaGraphCondTypeWhile;
+  np.conditional.size = 1;
+  cudaGraphNode_t wnode;
+  B_CUDA(cudaGraphAddNode(&wnode, g, nodes.data(), nn, &np));
+  cudaGraph_t body = np.conditional.phGraph_out[0];
+  B_CUDA(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  const SysDesc<T> *desc = (const SysDesc<T> *)B->desc;
+  const int64_t ps = B->max_tiles;
+  batch_spmv_kernel<T, G><<<B->grid, kBlock, 0, cs>>>(B->tiles, desc, B->st, B->part, ps, B->glob, B->kp);
+  batch_update_kernel<T, PRE><<<B->grid, kBlock, 0, cs>>>(B->tiles, desc, B->st, B->part, ps, B->glob, B->kp);
+  batch_direction_kernel<T, PRE><<<B->grid, kBlock, 0, cs>>>(B->tiles, desc, B->st, B->part, ps, B->glob, B->kp);
+  batch_residual_kernel<T, G, PRE><<<B->grid, kBlock, 0, cs>>>(B->tiles, desc, B->st, B->part, ps, B->glob, B->kp,
+                                                                h);
+  cudaError_t e2 = cudaStreamEndCapture(cs, &cap);
+  cudaStreamDestroy(cs);
+  B_CUDA(e2);
+  B_CUDA(cudaGraphInstantiate(&B->exec, g, 0));
+  return B200LA_OK;
+}
+
+template <typename T, bool PRE> int build_graph_g(BatchHandle B) {
+  switch (B->lanes) {
+    case 2: return build_graph_t<T, 2, PRE>(B);
+    case 4: return build_graph_t<T, 4, PRE>(B);
+    case 8: return build_graph_t<T, 8, PRE>(B);
+    case 16: return build_graph_t<T, 16, PRE>(B);
+    case 32: return build_graph_t<T, 32, PRE>(B);
+  }
+  return fail(B200LA_ERR_INVALID, "batch: lanes per row %d (2..32, power of two)", B->lanes);
+}
+
+int build_graph(BatchHandle B) {
+  const bool pre = B->kp.precond != 0;
+  if (B->kp.mixed) return pre ? build_graph_g<float, true>(B) : build_graph_g<float, false>(B);
+  return pre ? build_graph_g<double, true>(B) : build_graph_g<double, false>(B);
+}
+
+// Tile list of the systems that are still running, rebuilt before each launch.
+int rebuild_tiles(BatchHandle B, int *active) {
+  B->tiles_host.clear();
+  int act = 0;
+  for (int s = 0; s < B->capacity; ++s) {
+    const HostSys &h = B->sys[s];
+    if (!h.used) continue;
+    const int ph = B->st_host[s].phase;
+    if (ph == PH_DONE || ph == PH_EMPTY) continue;
+    ++act;
+    const int count = (h.n + B->tile_rows - 1) / B->tile_rows;
+    const int first = (int)B->tiles_host.size();
+    for (int k = 0; k < count; ++k) {
+      const int row0 = k * B->tile_rows;
+      B->tiles_host.push_back(Tile{s, row0, std::min(B->tile_rows, h.n - row0), first, count, 0});
+    }
+  }
+  const int64_t nt = (int64_t)B->tiles_host.size();
+  cudaStream_t st = B->ctx->stream;
+  if (nt > B->max_tiles) {
+    int64_t cap = std::max<int64_t>(nt, 2 * B->max_tiles);
+    if (B->tiles) cudaFreeAsync(B->tiles, st);
+    if (B->part) cudaFreeAsync(B->part, st);
+    B->tiles = nullptr;
+    B->part = nullptr;
+    B_CUDA(cudaMallocAsync(&B->tiles, sizeof(Tile) * cap, st));
+    B_CUDA(cudaMallocAsync(&B->part, sizeof(double) * 3 * cap, st));
+    B->max_tiles = cap;
+    if (B->exec) {
+      cudaGraphExecDestroy(B->exec);
+      B->exec = nullptr;
+    }
+  }
+  if (nt) B_CUDA(cudaMemcpyAsync(B->tiles, B->tiles_host.data(), sizeof(Tile) * nt, cudaMemcpyHostToDevice, st));
+  // the tile list's staging vector must outlive the copy
+  B_CUDA(cudaStreamSynchronize(st));
+  *active = act;
+  return B200LA_OK;
+}
+
+}  // namespace
+
+namespace {
+
+// Allocates a slot's buffers (one chunk) and carves them into a descriptor.
+template <typename T>
+int alloc_slot(b200la_batch B, int slot, int n, int64_t nnz, SysDesc<T> *out) {
+  HostSys &h = B->sys[slot];
+  cudaStream_t st = B->ctx->stream;
+  const bool mixed = B->kp.mixed != 0;
+  h.bytes = slot_bytes(n, nnz, mixed);
+  B_CUDA(cudaMallocAsync(&h.chunk, h.bytes, st));
+  char *p = (char *)h.chunk;
+  auto take = [&](size_t bytes) { char *q = p; p += align256(bytes); return (void *)q; };
+  SysDesc<T> d{};
+  d.n = n;
+  d.nnz = (int)nnz;
+  d.rowptr = (const int *)take(sizeof(int) * (n + 1));
+  d.col = (const int *)take(sizeof(int) * nnz);
+  d.val64 = (const double *)take(8 * nnz);
+  d.val = mixed ? (const T *)take(4 * nnz) : (const T *)d.val64;
+  d.b = (const double *)take(8 * n);
+  d.x = (double *)take(8 * n);
+  d.c = (T *)take(sizeof(T) * n);
+  d.r = (T *)take(sizeof(T) * n);
+  d.p = (T *)take(sizeof(T) * n);
+  d.Ap = (T *)take(sizeof(T) * n);
+  d.invd = (const T *)take(sizeof(T) * n);
+  *out = d;
+  return B200LA_OK;
+}
+
+// Uploads the descriptor and a fresh RESID state, then builds the FP32
+// values, the inverse diagonal and zero work vectors on the device.
+template <typename T>
+int finish_slot(b200la_batch B, int slot, const SysDesc<T> &d) {
+  HostSys &h = B->sys[slot];
+  cudaStream_t st = B->ctx->stream;
+  desc_of<T>(h) = d;
+  SysState &s0 = B->st_host[slot];
+  memset(&s0, 0, sizeof(SysState));
+  s0.phase = PH_RESID;
+  s0.bad_row = 0xffffffffu;
+  B_CUDA(cudaMemcpyAsync(B->st + slot, &s0, sizeof(SysState), cudaMemcpyHostToDevice, st));
+  B_CUDA(cudaMemcpyAsync((SysDesc<T> *)B->desc + slot, &desc_of<T>(h), sizeof(SysDesc<T>), cudaMemcpyHostToDevice, st));
+  const int64_t work = std::max<int64_t>(d.nnz, d.n);
+  const int grid = (int)std::min<int64_t>(std::max<int64_t>((work + kBlock - 1) / kBlock, 1),
+                                          (int64_t)B->ctx->num_sms * 8);
+  slot_setup_kernel<T><<<grid, kBlock, 0, st>>>(d, &B->st[slot].bad_row);
+  B_CUDA(cudaGetLastError());
+  return B200LA_OK;
+}
+
+template <typename T>
+int add_typed(b200la_batch B, int slot, int n, int64_t nnz, const int *rowptr, const int *col,
+              const double *val, const double *b, const double *x0) {
+  cudaStream_t st = B->ctx->stream;
+  SysDesc<T> d{};
+  B_TRY(alloc_slot<T>(B, slot, n, nnz, &d));
+  B_CUDA(cudaMemcpyAsync((void *)d.rowptr, rowptr, sizeof(int) * (n + 1), cudaMemcpyHostToDevice, st));
+  if (nnz) {
+    B_CUDA(cudaMemcpyAsync((void *)d.col, col, sizeof(int) * nnz, cudaMemcpyHostToDevice, st));
+    B_CUDA(cudaMemcpyAsync((void *)d.val64, val, 8 * nnz, cudaMemcpyHostToDevice, st));
+  }
+  B_CUDA(cudaMemcpyAsync((void *)d.b, b, 8 * n, cudaMemcpyHostToDevice, st));
+  if (x0) B_CUDA(cudaMemcpyAsync(d.x, x0, 8 * n, cudaMemcpyHostToDevice, st));
+  else B_CUDA(cudaMemsetAsync(d.x, 0, 8 * n, st));
+  return finish_slot<T>(B, slot, d);
+}
+
+}  // namespace
+
+extern "C" {
+
+int b200la_batch_slot_bytes(int64_t n, int64_t nnz, int mixed, int64_t *bytes) {
+  B_CHECK(bytes && n >= 0 && nnz >= 0, B200LA_ERR_INVALID, "batch_slot_bytes: bad argument");
+  *bytes = (int64_t)slot_bytes(n, nnz, mixed != 0);
+  return B200LA_OK;
+}
+
+int b200la_batch_destroy(b200la_batch B) {
+  if (!B) return B200LA_OK;
+  cudaStream_t st = B->ctx->stream;
+  cudaStreamSynchronize(st);
+  if (B->exec) cudaGraphExecDestroy(B->exec);
+  if (B->graph) cudaGraphDestroy(B->graph);
+  for (HostSys &h : B->sys)
+    if (h.chunk) cudaFreeAsync(h.chunk, st);
+  void *bufs[] = {B->desc, B->st, B->tiles, B->part, B->glob};
+  for (void *p : bufs)
+    if (p) cudaFreeAsync(p, st);
+  if (B->st_host) cudaFreeHost(B->st_host);
+  if (B->glob_host) cudaFreeHost(B->glob_host);
+  cudaStreamSynchronize(st);
+  delete B;
+  return B200LA_OK;
+}
+
+int b200la_batch_create(b200la_ctx ctx, const b200la_batch_params *p, b200la_batch *out) {
+  B_CHECK(ctx && p && out, B200LA_ERR_INVALID, "batch_create: null argument");
+  B_CHECK(p->capacity > 0 && p->capacity <= (1 << 20), B200LA_ERR_INVALID, "batch_create: capacity %d", p->capacity);
+  B_CHECK(p->max_outer >= 1 && p->max_outer <= 1000, B200LA_ERR_INVALID, "batch_create: max_outer %d", p->max_outer);
+  B_CHECK(p->inner_maxits >= 1 && p->inner_maxits <= 10000000, B200LA_ERR_INVALID, "batch_create: inner_maxits");
+  B_CHECK(p->atol >= 0 && p->rtol >= 0 && p->dtol > 0, B200LA_ERR_INVALID, "batch_create: tolerances");
+  B_CHECK(!p->mixed || (p->inner_rtol > 0 && p->inner_rtol < 1), B200LA_ERR_INVALID, "batch_create: inner_rtol");
+  const int lanes = p->lanes ? p->lanes : 4;
+  B_CHECK(lanes == 2 || lanes == 4 || lanes == 8 || lanes == 16 || lanes == 32, B200LA_ERR_INVALID,
+          "batch_create: lanes %d", lanes);
+  B_CHECK(p->tile_rows == 0 || (p->tile_rows >= 32 && p->tile_rows <= 65536), B200LA_ERR_INVALID,
+          "batch_create: tile_rows %d", p->tile_rows);
+  b200la_batch B = new b200la_batch_s();
+  B->ctx = ctx;
+  B->prm = *p;
+  B->kp = BatchParams{p->max_outer, p->inner_maxits, p->atol, p->rtol, p->dtol, p->inner_rtol, p->precond ? 1 : 0,
+                      p->mixed ? 1 : 0};
+  B->lanes = lanes;
+  B->tile_rows = p->tile_rows ? p->tile_rows : 512;
+  B->capacity = p->capacity;
+  B->sys.resize(p->capacity);
+  cudaStream_t st = ctx->stream;
+  const size_t dsz = p->mixed ? sizeof(SysDesc<float>) : sizeof(SysDesc<double>);
+  bool ok = cudaMallocAsync(&B->desc, dsz * p->capacity, st) == cudaSuccess &&
+            cudaMallocAsync(&B->st, sizeof(SysState) * p->capacity, st) == cudaSuccess &&
+            cudaMallocAsync(&B->glob, sizeof(BatchGlobals), st) == cudaSuccess &&
+            cudaMallocHost(&B->st_host, sizeof(SysState) * p->capacity) == cudaSuccess &&
+            cudaMallocHost(&B->glob_host, sizeof(BatchGlobals)) == cudaSuccess;
+  if (ok) {
+    memset(B->st_host, 0, sizeof(SysState) * p->capacity);
+    ok = cudaMemsetAsync(B->st, 0, sizeof(SysState) * p->capacity, st) == cudaSuccess &&
+         cudaMemsetAsync(B->glob, 0, sizeof(BatchGlobals), st) == cudaSuccess &&
+         cudaStreamSynchronize(st) == cudaSuccess;
+  }
+  if (!ok) {
+    b200la_batch_destroy(B);
+    return fail(B200LA_ERR_NOMEM, "batch_create: allocation failed");
+  }
+  *out = B;
+  return B200LA_OK;
+}
+
+int b200la_batch_add(b200la_batch B, int n, int64_t nnz, const int *rowptr, const int *col, const double *val,
+                     const double *b, const double *x0, int *slot_out) {
+  B_CHECK(B && slot_out && b, B200LA_ERR_INVALID, "batch_add: null argument");
+  B_CHECK(n > 0, B200LA_ERR_INVALID, "batch_add: empty system");
+  int max_row = 0;
+  B_TRY(validate_csr(n, n, nnz, rowptr, col, &max_row));
+  B_CHECK(nnz == 0 || val, B200LA_ERR_MATRIX, "batch_add: val is NULL");
+  int slot = -1;
+  for (int s = 0; s < B->capacity; ++s)
+    if (!B->sys[s].used) { slot = s; break; }
+  B_CHECK(slot >= 0, B200LA_ERR_NOMEM, "batch_add: all %d slots are in use", B->capacity);
+  HostSys &h = B->sys[slot];
+  h = HostSys();
+  h.n = n;
+  h.nnz = (int)nnz;
+  const int rc = B->kp.mixed ? add_typed<float>(B, slot, n, nnz, rowptr, col, val, b, x0)
+                             : add_typed<double>(B, slot, n, nnz, rowptr, col, val, b, x0);
+  if (rc != B200LA_OK) {
+    if (h.chunk) cudaFreeAsync(h.chunk, B->ctx->stream);
+    h = HostSys();
+    return rc;
+  }
+  h.used = true;
+  B->device_bytes += (int64_t)h.bytes;
+  *slot_out = slot;
+  return B200LA_OK;
+}
+
+int b200la_batch_add_q1(b200la_batch B, int dim, int cells, uint64_t seed, double sigma, int *slot_out) {
+  B_CHECK(B && slot_out, B200LA_ERR_INVALID, "batch_add_q1: null argument");
+  B_CHECK((dim == 2 || dim == 3) && cells >= 1 && sigma >= 0.0, B200LA_ERR_INVALID, "batch_add_q1: dim %d cells %d",
+          dim, cells);
+  const int64_t n64 = q1_rows(dim, cells), nnz = q1_nnz(dim, cells);
+  B_CHECK(nnz < (int64_t)INT32_MAX, B200LA_ERR_UNSUPPORTED, "batch_add_q1: nnz exceeds int32 indexing");
+  const int n = (int)n64;
+  int slot = -1;
+  for (int s = 0; s < B->capacity; ++s)
+    if (!B->sys[s].used) { slot = s; break; }
+  B_CHECK(slot >= 0, B200LA_ERR_NOMEM, "batch_add_q1: all %d slots are in use", B->capacity);
+  HostSys &h = B->sys[slot];
+  h = HostSys();
+  h.n = n;
+  h.nnz = (int)nnz;
+  cudaStream_t st = B->ctx->stream;
+  auto go = [&](auto tag) -> int {
+    using T = decltype(tag);
+    SysDesc<T> d{};
+    B_TRY(alloc_slot<T>(B, slot, n, nnz, &d));
+    B_TRY(q1_assemble(st, B->ctx->num_sms, dim, cells, seed, sigma, (int *)d.rowptr, (int *)d.col,
+                      (double *)d.val64, (double *)d.b));
+    B_CUDA(cudaMemsetAsync(d.x, 0, 8 * (size_t)n, st));
+    return finish_slot<T>(B, slot, d);
+  };
+  const int rc = B->kp.mixed ? go(float()) : go(double());
+  if (rc != B200LA_OK) {
+    if (h.chunk) cudaFreeAsync(h.chunk, st);
+    h = HostSys();
+    return rc;
+  }
+  h.used = true;
+  B->device_bytes += (int64_t)h.bytes;
+  *slot_out = slot;
+  return B200LA_OK;
+}
+
+int b200la_batch_get_system(b200la_batch B, int slot, int *rowptr, int *col, double *val, double *rhs) {
+  B_CHECK(B && slot >= 0 && slot < B->capacity && B->sys[slot].used, B200LA_ERR_INVALID, "batch_get_system: slot");
+  const HostSys &h = B->sys[slot];
+  cudaStream_t st = B->ctx->stream;
+  const SysDesc<double> &d64 = h.d64;
+  const SysDesc<float> &d32 = h.d32;
+  const int *rp = B->kp.mixed ? d32.rowptr : d64.rowptr;
+  const int *cl = B->kp.mixed ? d32.col : d64.col;
+  const double *vv = B->kp.mixed ? d32.val64 : d64.val64;
+  const double *bb = B->kp.mixed ? d32.b : d64.b;
+  if (rowptr) B_CUDA(cudaMemcpyAsync(rowptr, rp, sizeof(int) * (h.n + 1), cudaMemcpyDeviceToHost, st));
+  if (col) B_CUDA(cudaMemcpyAsync(col, cl, sizeof(int) * (size_t)h.nnz, cudaMemcpyDeviceToHost, st));
+  if (val) B_CUDA(cudaMemcpyAsync(val, vv, 8 * (size_t)h.nnz, cudaMemcpyDeviceToHost, st));
+  if (rhs) B_CUDA(cudaMemcpyAsync(rhs, bb, 8 * (size_t)h.n, cudaMemcpyDeviceToHost, st));
+  B_CUDA(cudaStreamSynchronize(st));
+  return B200LA_OK;
+}
+
+int b200la_batch_slot_size(b200la_batch B, int slot, int *n, int64_t *nnz) {
+  B_CHECK(B && slot >= 0 && slot < B->capacity && B->sys[slot].used, B200LA_ERR_INVALID, "batch_slot_size: slot");
+  if (n) *n = B->sys[slot].n;
+  if (nnz) *nnz = B->sys[slot].nnz;
+  return B200LA_OK;
+}
+
+int b200la_batch_remove(b200la_batch B, int slot) {
+  B_CHECK(B && slot >= 0 && slot < B->capacity && B->sys[slot].used, B200LA_ERR_INVALID, "batch_remove: slot %d",
+          slot);
+  HostSys &h = B->sys[slot];
+  cudaStream_t st = B->ctx->stream;
+  B_CUDA(cudaFreeAsync(h.chunk, st));
+  B->device_bytes -= (int64_t)h.bytes;
+  h = HostSys();
+  memset(&B->st_host[slot], 0, sizeof(SysState));
+  B_CUDA(cudaMemcpyAsync(B->st + slot, &B->st_host[slot], sizeof(SysState), cudaMemcpyHostToDevice, st));
+  B_CUDA(cudaStreamSynchronize(st));
+  return B200LA_OK;
+}
+
+int b200la_batch_run(b200la_batch B, int max_passes, int *active_out) {
+  B_CHECK(B && max_passes >= 1, B200LA_ERR_INVALID, "batch_run: bad argument");
+  cudaStream_t st = B->ctx->stream;
+  int active = 0;
+  B_TRY(rebuild_tiles(B, &active));
+  if (active == 0) {
+    if (active_out) *active_out = 0;
+    return B200LA_OK;
+  }
+  if (!B->exec) B_TRY(build_graph(B));
+  BatchGlobals &g = *B->glob_host;
+  memset(&g, 0, sizeof(g));
+  g.active = active;
+  g.max_passes = max_passes;
+  g.ntiles = (int)B->tiles_host.size();
+  B_CUDA(cudaMemcpyAsync(B->glob, &g, sizeof(BatchGlobals), cudaMemcpyHostToDevice, st));
+  B_CUDA(cudaGraphLaunch(B->exec, st));
+  B_CUDA(cudaMemcpyAsync(B->st_host, B->st, sizeof(SysState) * B->capacity, cudaMemcpyDeviceToHost, st));
+  B_CUDA(cudaMemcpyAsync(B->glob_host, B->glob, sizeof(BatchGlobals), cudaMemcpyDeviceToHost, st));
+  B_CUDA(cudaStreamSynchronize(st));
+  if (active_out) *active_out = B->glob_host->active;
+  return B200LA_OK;
+}
+
+int b200la_batch_result(b200la_batch B, int slot, double *x_host, b200la_sys_result *r) {
+  B_CHECK(B && r && slot >= 0 && slot < B->capacity && B->sys[slot].used, B200LA_ERR_INVALID,
+          "batch_result: slot %d", slot);
+  const HostSys &h = B->sys[slot];
+  const SysState &s = B->st_host[slot];
+  memset(r, 0, sizeof(*r));
+  r->phase_done = s.phase == PH_DONE;
+  r->state = s.phase == PH_DONE ? s.state : B200LA_ITERATE;
+  r->iters = s.total_iter;
+  r->outer = s.outer;
+  r->res = s.res;
+  r->res_init = s.res0;
+  r->res_rel = s.res0 > 0 ? s.res / s.res0 : 0.0;
+  r->device_us = (s.phase == PH_DONE && s.t_done >= s.t_begin) ? (double)(s.t_done - s.t_begin) / 1e3 : 0.0;
+  if (B->kp.precond && s.bad_row != 0xffffffffu) r->state = B200LA_FAIL_BREAKDOWN;
+  if (r->state == B200LA_SUCCESS_ABS || r->state == B200LA_SUCCESS_REL) r->solver_state = B200LA_SOLVER_SUCCESS;
+  else if (r->state == B200LA_FAIL_DIV || r->state == B200LA_FAIL_MAXITS) r->solver_state = B200LA_SOLVER_EXCEEDED;
+  else if (r->state == B200LA_ITERATE) r->solver_state = B200LA_SOLVER_EXCEEDED;
+  else r->solver_state = B200LA_SOLVER_ERROR;
+  if (x_host) {
+    const double *xd = B->kp.mixed ? h.d32.x : h.d64.x;
+    B_CUDA(cudaMemcpyAsync(x_host, xd, 8 * (size_t)h.n, cudaMemcpyDeviceToHost, B->ctx->stream));
+    B_CUDA(cudaStreamSynchronize(B->ctx->stream));
+  }
+  return B200LA_OK;
+}
+
+int b200la_batch_last_run(b200la_batch B, int *passes, double *reserved) {
+  B_CHECK(B, B200LA_ERR_INVALID, "batch_last_run: null batch");
+  if (passes) *passes = B->glob_host->passes;
+  if (reserved) *reserved = 0.0;
+  return B200LA_OK;
+}
+
+int b200la_batch_info(b200la_batch B, int *used_slots, int64_t *device_bytes) {
+  B_CHECK(B, B200LA_ERR_INVALID, "batch_info: null batch");
+  int u = 0;
+  for (const HostSys &h : B->sys) u += h.used ? 1 : 0;
+  if (used_slots) *used_slots = u;
+  if (device_bytes) *device_bytes = B->device_bytes;
+  return B200LA_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+template <typename T, int G>
+int time_plain(b200la_batch B, int reps, float *ms) {
+  cudaStream_t st = B->ctx->stream;
+  const int nt = (int)B->tiles_host.size();
+  int occ = 1;
+  B_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, (const void *)batch_spmv_plain_kernel<T, G>, kBlock, 0));
+  const int grid = B->ctx->num_sms * std::max(occ, 1);
+  const SysDesc<T> *desc = (const SysDesc<T> *)B->desc;
+  batch_spmv_plain_kernel<T, G><<<grid, kBlock, 0, st>>>(B->tiles, nt, desc);
+  cudaEvent_t e0, e1;
+  B_CUDA(cudaEventCreate(&e0));
+  B_CUDA(cudaEventCreate(&e1));
+  B_CUDA(cudaEventRecord(e0, st));
+  for (int r = 0; r < reps; ++r) batch_spmv_plain_kernel<T, G><<<grid, kBlock, 0, st>>>(B->tiles, nt, desc);
+  B_CUDA(cudaEventRecord(e1, st));
+  B_CUDA(cudaEventSynchronize(e1));
+  B_CUDA(cudaEventElapsedTime(ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  B_CUDA(cudaGetLastError());
+  *ms /= reps;
+  return B200LA_OK;
+}
+
+template <typename T> int time_lanes(b200la_batch B, int lanes, float *ms) {
+  switch (lanes) {
+    case 2: return time_plain<T, 2>(B, 5, ms);
+    case 4: return time_plain<T, 4>(B, 5, ms);
+    case 8: return time_plain<T, 8>(B, 5, ms);
+    case 16: return time_plain<T, 16>(B, 5, ms);
+    case 32: return time_plain<T, 32>(B, 5, ms);
+  }
+  return fail(B200LA_ERR_INVALID, "lanes %d", lanes);
+}
+
+// Restart every listed slot from x = 0: RESID phase, counters cleared.
+template <typename T>
+__global__ void __launch_bounds__(kBlock) batch_restart_kernel(const int *__restrict__ slots,
+                                                               const SysDesc<T> *__restrict__ desc, SysState *st) {
+  const int s = slots[blockIdx.x];
+  const SysDesc<T> d = desc[s];
+  for (int i = threadIdx.x; i < d.n; i += kBlock) d.x[i] = 0.0;
+  if (threadIdx.x == 0) {
+    SysState &S = st[s];
+    const unsigned bad = S.bad_row;
+    S = SysState{};
+    S.phase = PH_RESID;
+    S.bad_row = bad;
+  }
+}
+
+}  // namespace
+
+extern "C" int b200la_batch_tune(b200la_batch B, int *lanes_out, double *usec) {
+  B_CHECK(B, B200LA_ERR_INVALID, "batch_tune: null batch");
+  int active = 0;
+  B_TRY(rebuild_tiles(B, &active));
+  if (active == 0) {
+    if (lanes_out) *lanes_out = B->lanes;
+    if (usec) *usec = 0.0;
+    return B200LA_OK;
+  }
+  int best = B->lanes;
+  float best_ms = 1e30f;
+  for (int g : {2, 4, 8, 16}) {
+    float ms = 0.f;
+    B_TRY(B->kp.mixed ? time_lanes<float>(B, g, &ms) : time_lanes<double>(B, g, &ms));
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = g;
+    }
+  }
+  if (best != B->lanes && B->exec) {
+    cudaGraphExecDestroy(B->exec);
+    B->exec = nullptr;
+  }
+  B->lanes = best;
+  if (lanes_out) *lanes_out = best;
+  if (usec) *usec = 1000.0 * best_ms;
+  return B200LA_OK;
+}
+
+extern "C" int b200la_batch_restart(b200la_batch B) {
+  B_CHECK(B, B200LA_ERR_INVALID, "batch_restart: null batch");
+  std::vector<int> slots;
+  for (int s = 0; s < B->capacity; ++s)
+    if (B->sys[s].used) slots.push_back(s);
+  if (slots.empty()) return B200LA_OK;
+  cudaStream_t st = B->ctx->stream;
+  int *d_slots = nullptr;
+  B_CUDA(cudaMallocAsync(&d_slots, sizeof(int) * slots.size(), st));
+  B_CUDA(cudaMemcpyAsync(d_slots, slots.data(), sizeof(int) * slots.size(), cudaMemcpyHostToDevice, st));
+  if (B->kp.mixed)
+    batch_restart_kernel<float><<<(int)slots.size(), kBlock, 0, st>>>(d_slots, (const SysDesc<float> *)B->desc, B->st);
+  else
+    batch_restart_kernel<double><<<(int)slots.size(), kBlock, 0, st>>>(d_slots, (const SysDesc<double> *)B->desc,
+                                                                        B->st);
+  B_CUDA(cudaGetLastError());
+  B_CUDA(cudaFreeAsync(d_slots, st));
+  for (int s : slots) {
+    const unsigned bad = B->st_host[s].bad_row;
+    memset(&B->st_host[s], 0, sizeof(SysState));
+    B->st_host[s].phase = PH_RESID;
+    B->st_host[s].bad_row = bad;
+  }
+  return B200LA_OK;
+}
+
+// Times the batched SpMV (the inner solve's SpMV kernel body) over every used
+// slot with the batch's current lanes; mean milliseconds per launch.
+extern "C" int b200la_batch_profile(b200la_batch B, int reps, double *ms_spmv, int64_t *algorithmic_bytes) {
+  B_CHECK(B && ms_spmv && reps >= 1, B200LA_ERR_INVALID, "batch_profile: bad argument");
+  // every used slot, whatever its phase
+  B->tiles_host.clear();
+  int64_t bytes = 0;
+  const int64_t vb = B->kp.mixed ? 4 : 8;
+  for (int s = 0; s < B->capacity; ++s) {
+    const HostSys &h = B->sys[s];
+    if (!h.used) continue;
+    const int count = (h.n + B->tile_rows - 1) / B->tile_rows;
+    const int first = (int)B->tiles_host.size();
+    for (int k = 0; k < count; ++k)
+      B->tiles_host.push_back(Tile{s, k * B->tile_rows, std::min(B->tile_rows, h.n - k * B->tile_rows), first, count, 0});
+    bytes += (int64_t)h.nnz * (vb + 4) + (int64_t)(h.n + 1) * 4 + 2 * (int64_t)h.n * vb;
+  }
+  const int64_t nt = (int64_t)B->tiles_host.size();
+  if (nt == 0) {
+    *ms_spmv = 0.0;
+    return B200LA_OK;
+  }
+  cudaStream_t st = B->ctx->stream;
+  if (nt > B->max_tiles) {
+    if (B->tiles) cudaFreeAsync(B->tiles, st);
+    if (B->part) cudaFreeAsync(B->part, st);
+    B_CUDA(cudaMallocAsync(&B->tiles, sizeof(Tile) * nt, st));
+    B_CUDA(cudaMallocAsync(&B->part, sizeof(double) * 3 * nt, st));
+    B->max_tiles = nt;
+    if (B->exec) {
+      cudaGraphExecDestroy(B->exec);
+      B->exec = nullptr;
+    }
+  }
+  B_CUDA(cudaMemcpyAsync(B->tiles, B->tiles_host.data(), sizeof(Tile) * nt, cudaMemcpyHostToDevice, st));
+  float ms = 0.f;
+  B_TRY(B->kp.mixed ? time_lanes<float>(B, B->lanes, &ms) : time_lanes<double>(B, B->lanes, &ms));
+  *ms_spmv = ms;
+  if (algorithmic_bytes) *algorithmic_bytes = bytes;
+  // the tile list on the device now lists every slot; the next run rebuilds it
+  return B200LA_OK;
+}

@@ -1,0 +1,54 @@
+// Solver state shared by the CG translation unit (pcg.cu) and the solvers
+// built on it (mixed-precision refinement in mp.cu).
+#pragma once
+
+#include "internal.cuh"
+
+namespace b200la {
+
+constexpr int kMaxIts = 10000000;
+
+// Device-resident scalars of one CG solve.
+struct CgScalars {
+  double rz;        // r.z of the current residual (r.r without preconditioner)
+  double pAp;
+  double alpha;
+  double beta;
+  double rr;
+  double res;
+  double res_init;
+  double atol, rtol, dtol;
+  int iter;
+  int state;
+  int maxits;
+  int guard;        // body passes, counted by the direction kernel
+  unsigned ticket[4];
+};
+
+}  // namespace b200la
+
+struct b200la_cg_s {
+  b200la_mat A;
+  b200la_cg_params prm;
+  int64_t n;
+  void *x, *r, *p, *Ap, *invd;
+  double *part;                // [2][kMaxReduceBlocks]
+  b200la::CgScalars *sc;       // device
+  b200la::CgScalars *sc_host;  // pinned
+  cudaGraph_t graph;
+  cudaGraphExec_t exec;
+  int g_format, g_param;       // schedule baked into the graph
+  int grid_spmv, grid_ew;
+};
+
+namespace b200la {
+
+// Start a solve on the context stream: r = b - A x0 (x0, b device buffers of
+// the solver's value type), or r = b with x0 = 0 when x_dev is nullptr.
+int cg_start(b200la_cg s, const void *x_dev, const void *b_dev);
+// Run the device loop (one graph launch); the solution stays in s->x.
+int cg_run(b200la_cg s);
+// Copy the scalars to the host (synchronises the context stream).
+int cg_fetch(b200la_cg s, CgScalars *out);
+
+}  // namespace b200la

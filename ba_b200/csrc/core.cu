@@ -218,6 +218,26 @@ static int launch_ew(b200la_ctx c, int64_t n, F f) {
   return B200LA_OK;
 }
 
+int validate_csr(int nrow, int ncol, int64_t nnz, const int *rowptr, const int *col, int *max_row) {
+  B_CHECK(nrow >= 0 && ncol >= 0 && nnz >= 0, B200LA_ERR_MATRIX, "csr: negative dimension");
+  B_CHECK(nnz < (int64_t)INT32_MAX, B200LA_ERR_MATRIX, "csr: nnz %lld exceeds int32 indexing", (long long)nnz);
+  B_CHECK(rowptr, B200LA_ERR_MATRIX, "csr: rowptr is NULL");
+  B_CHECK(rowptr[0] == 0, B200LA_ERR_MATRIX, "csr: rowptr[0] = %d, expected 0", rowptr[0]);
+  int mr = 0;
+  for (int i = 0; i < nrow; ++i) {
+    int len = rowptr[i + 1] - rowptr[i];
+    B_CHECK(len >= 0, B200LA_ERR_MATRIX, "csr: rowptr decreases at row %d", i);
+    if (len > mr) mr = len;
+  }
+  B_CHECK(rowptr[nrow] == nnz, B200LA_ERR_MATRIX, "csr: rowptr[nrow] = %d != nnz %lld", rowptr[nrow], (long long)nnz);
+  B_CHECK(nnz == 0 || col, B200LA_ERR_MATRIX, "csr: col is NULL");
+  for (int64_t j = 0; j < nnz; ++j)
+    B_CHECK(col[j] >= 0 && col[j] < ncol, B200LA_ERR_MATRIX, "csr: col[%lld] = %d out of range [0,%d)",
+            (long long)j, col[j], ncol);
+  *max_row = mr;
+  return B200LA_OK;
+}
+
 }  // namespace b200la
 
 using namespace b200la;
@@ -460,26 +480,6 @@ int b200la_vec_elementwise_mult(b200la_vec y, b200la_vec x) {
 }
 
 // ---------------------------------------------------------------- matrices
-static int validate_csr(int nrow, int ncol, int64_t nnz, const int *rowptr, const int *col, int *max_row) {
-  B_CHECK(nrow >= 0 && ncol >= 0 && nnz >= 0, B200LA_ERR_MATRIX, "csr: negative dimension");
-  B_CHECK(nnz < (int64_t)INT32_MAX, B200LA_ERR_MATRIX, "csr: nnz %lld exceeds int32 indexing", (long long)nnz);
-  B_CHECK(rowptr, B200LA_ERR_MATRIX, "csr: rowptr is NULL");
-  B_CHECK(rowptr[0] == 0, B200LA_ERR_MATRIX, "csr: rowptr[0] = %d, expected 0", rowptr[0]);
-  int mr = 0;
-  for (int i = 0; i < nrow; ++i) {
-    int len = rowptr[i + 1] - rowptr[i];
-    B_CHECK(len >= 0, B200LA_ERR_MATRIX, "csr: rowptr decreases at row %d", i);
-    if (len > mr) mr = len;
-  }
-  B_CHECK(rowptr[nrow] == nnz, B200LA_ERR_MATRIX, "csr: rowptr[nrow] = %d != nnz %lld", rowptr[nrow], (long long)nnz);
-  B_CHECK(nnz == 0 || col, B200LA_ERR_MATRIX, "csr: col is NULL");
-  for (int64_t j = 0; j < nnz; ++j)
-    B_CHECK(col[j] >= 0 && col[j] < ncol, B200LA_ERR_MATRIX, "csr: col[%lld] = %d out of range [0,%d)",
-            (long long)j, col[j], ncol);
-  *max_row = mr;
-  return B200LA_OK;
-}
-
 int b200la_csr_upload(b200la_ctx c, int nrow, int ncol, int64_t nnz, const int *rowptr, const int *col,
                       const void *val, int val_dtype, int dtype, b200la_mat *out) {
   B_CHECK(c && out, B200LA_ERR_INVALID, "csr_upload: null argument");

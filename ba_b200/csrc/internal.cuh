@@ -98,6 +98,16 @@ struct b200la_mat_s {
 
 namespace b200la {
 
+// Host validation of a CSR structure: rowptr[0] == 0, non-decreasing,
+// rowptr[nrow] == nnz, 0 <= col < ncol.  Writes the longest row length.
+int validate_csr(int nrow, int ncol, int64_t nnz, const int *rowptr, const int *col, int *max_row);
+
+// Q1 system assembly on the device (assemble.cu).
+int64_t q1_rows(int dim, int n);
+int64_t q1_nnz(int dim, int n);
+int q1_assemble(cudaStream_t st, int num_sms, int dim, int n, uint64_t seed, double sigma, int *rowptr, int *col,
+                double *val, double *b);
+
 // Launch helpers
 int grid_for(b200la_ctx ctx, const void *kernel, int64_t work_items, int items_per_block,
              int *grid);

@@ -18,28 +18,10 @@
 #include <cmath>
 #include <cstring>
 
-#include "internal.cuh"
+#include "cg_internal.cuh"
 #include "spmv.cuh"
 
 namespace b200la {
-
-constexpr int kMaxIts = 10000000;
-
-struct CgScalars {
-  double rz;        // r.z of the current residual (r.r without preconditioner)
-  double pAp;
-  double alpha;
-  double beta;
-  double rr;
-  double res;
-  double res_init;
-  double atol, rtol, dtol;
-  int iter;
-  int state;
-  int maxits;
-  int guard;        // body passes, counted by K3
-  unsigned ticket[4];
-};
 
 // IterateControl::Check; step 0 records the initial residual (res_init).
 __device__ __forceinline__ int iterate_check(int step, double value, const CgScalars &s, double first) {
@@ -79,6 +61,34 @@ __global__ void __launch_bounds__(kBlock) cg_init_kernel(Op op, const T *__restr
   InitEmit<T, PRE> e{b, x_user, v};
   op.run(x_user, e);
   double s[2] = {e.rr.value(), e.rz.value()};
+  if (grid_sum_last<2>(s, part, &sc->ticket[0]) && threadIdx.x == 0) {
+    double res = sqrt(s[0]);
+    sc->rr = s[0];
+    sc->rz = PRE ? s[1] : s[0];
+    sc->res = res;
+    sc->res_init = res;
+    sc->iter = 0;
+    sc->guard = 0;
+    sc->state = iterate_check(0, res, *sc, res);
+  }
+}
+
+// Start from x0 = 0: r = b exactly (b - A*0), no SpMV needed.
+template <typename T, bool PRE>
+__global__ void __launch_bounds__(kBlock) cg_init_zero_kernel(const T *__restrict__ b, CgVecs<T> v, double *part,
+                                                              CgScalars *sc) {
+  Acc<T> rr, rz;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < v.n; i += stride) {
+    const T r = b[i];
+    v.x[i] = T(0);
+    v.r[i] = r;
+    const T z = PRE ? r * v.invd[i] : r;
+    v.p[i] = z;
+    rr.add(r * r);
+    rz.add(r * z);
+  }
+  double s[2] = {rr.value(), rz.value()};
   if (grid_sum_last<2>(s, part, &sc->ticket[0]) && threadIdx.x == 0) {
     double res = sqrt(s[0]);
     sc->rr = s[0];
@@ -211,20 +221,6 @@ __global__ void __launch_bounds__(kBlock) cg_direction_kernel(CgVecs<T> v, CgSca
 
 using namespace b200la;
 
-struct b200la_cg_s {
-  b200la_mat A;
-  b200la_cg_params prm;
-  int64_t n;
-  void *x, *r, *p, *Ap, *invd;
-  double *part;       // [2][kMaxReduceBlocks]
-  CgScalars *sc;      // device
-  CgScalars *sc_host; // pinned
-  cudaGraph_t graph;
-  cudaGraphExec_t exec;
-  int g_format, g_param;  // schedule baked into the graph
-  int grid_spmv, grid_ew;
-};
-
 namespace b200la {
 
 template <typename T, bool PRE>
@@ -281,6 +277,13 @@ static int cg_launch_init_t(b200la_cg s, const void *x_user, const void *b) {
   b200la_mat A = s->A;
   CgVecs<T> v{(T *)s->x, (T *)s->r, (T *)s->p, (T *)s->Ap, (const T *)s->invd, s->n};
   cudaStream_t st = A->ctx->stream;
+  if (!x_user) {
+    int grid;
+    B_TRY(grid_for(A->ctx, (const void *)cg_init_zero_kernel<T, PRE>, s->n, kBlock, &grid));
+    cg_init_zero_kernel<T, PRE><<<grid, kBlock, 0, st>>>((const T *)b, v, s->part, s->sc);
+    B_CUDA(cudaGetLastError());
+    return B200LA_OK;
+  }
   return with_schedule<T>(A, [&](auto op) -> int {
     using Op = decltype(op);
     int grid;
@@ -296,6 +299,23 @@ static int cg_launch_init(b200la_cg s, const void *x_user, const void *b) {
   if (s->A->dtype == B200LA_F64)
     return pre ? cg_launch_init_t<double, true>(s, x_user, b) : cg_launch_init_t<double, false>(s, x_user, b);
   return pre ? cg_launch_init_t<float, true>(s, x_user, b) : cg_launch_init_t<float, false>(s, x_user, b);
+}
+
+int cg_start(b200la_cg s, const void *x_dev, const void *b_dev) { return cg_launch_init(s, x_dev, b_dev); }
+
+int cg_run(b200la_cg s) {
+  b200la_mat A = s->A;
+  if (A->format != s->g_format || A->param != s->g_param) B_TRY(cg_build_graph(s));
+  B_CUDA(cudaGraphLaunch(s->exec, A->ctx->stream));
+  return B200LA_OK;
+}
+
+int cg_fetch(b200la_cg s, CgScalars *out) {
+  cudaStream_t st = s->A->ctx->stream;
+  B_CUDA(cudaMemcpyAsync(s->sc_host, s->sc, sizeof(CgScalars), cudaMemcpyDeviceToHost, st));
+  B_CUDA(cudaStreamSynchronize(st));
+  *out = *s->sc_host;
+  return B200LA_OK;
 }
 
 // Runs the init kernel and then `iters` iterations as separate launches with
@@ -423,15 +443,12 @@ int b200la_cg_solve(b200la_cg s, b200la_vec b, b200la_vec x, b200la_cg_result *r
     res->state = B200LA_SUCCESS_ABS;
     return B200LA_OK;
   }
-  b200la_ctx c = A->ctx;
-  cudaStream_t st = c->stream;
-  if (A->format != s->g_format || A->param != s->g_param) B_TRY(cg_build_graph(s));
-  B_TRY(cg_launch_init(s, x->d, b->d));
-  B_CUDA(cudaGraphLaunch(s->exec, st));
+  cudaStream_t st = A->ctx->stream;
+  B_TRY(cg_start(s, x->d, b->d));
+  B_TRY(cg_run(s));
   B_CUDA(cudaMemcpyAsync(x->d, s->x, (size_t)s->n * dtype_size(A->dtype), cudaMemcpyDeviceToDevice, st));
-  B_CUDA(cudaMemcpyAsync(s->sc_host, s->sc, sizeof(CgScalars), cudaMemcpyDeviceToHost, st));
-  B_CUDA(cudaStreamSynchronize(st));
-  const CgScalars &h = *s->sc_host;
+  CgScalars h;
+  B_TRY(cg_fetch(s, &h));
   res->iters = h.iter;
   res->state = h.state;
   res->res = h.res;

@@ -409,3 +409,74 @@ def setup_CG_solver(maxits: int = 1000, atol: float = 1e-12, rtol: float = 1e-10
         p.Init_Jacobi()
         s.SetupPreconditioner(p)
     return s
+
+
+class MPIR:
+    """MPIR<LADescriptorCoupledD, LADescriptorCoupledS> with an FP32 Jacobi-PCG
+    as the low-precision error-correction solver (linear_solver/mpir.h:29-150):
+    SetupOperator(A64), SetMpirParameters(max_ech, max_ecl, abs_tol, rel_tol,
+    div_tol), SetLowPrecErrCorSolverParameters(max_iter, abs_tol, rel_tol,
+    div_tol), Solve(b, x).  Only low-precision correction passes run
+    (max_ech is accepted for interface parity and must be 0)."""
+
+    def __init__(self):
+        self.op = None
+        self.max_ecl, self.abs_tol, self.rel_tol, self.div_tol = 50, 0.0, 1e-10, 1e6
+        self.inner_maxits, self.inner_rtol = 100000, 1e-5
+        self.precond = True
+        self.tune = True
+        self._s = C.c_void_p()
+        self.iter_ = 0
+        self.outer_ = 0
+        self.res_ = self.res_init_ = self.res_rel_ = 0.0
+
+    def SetupOperator(self, op: B200_CSR_lMatrix):
+        self.op = op
+        self._release()
+
+    def SetMpirParameters(self, max_ech: int, max_ecl: int, abs_tol: float, rel_tol: float, div_tol: float):
+        if max_ech != 0:
+            raise B200LAError(-7, "MPIR: high-precision correction passes are not on this path")
+        self.max_ecl, self.abs_tol, self.rel_tol, self.div_tol = int(max_ecl), abs_tol, rel_tol, div_tol
+        self._release()
+
+    def SetLowPrecErrCorSolverParameters(self, max_iter: int, abs_tol: float, rel_tol: float, div_tol: float):
+        self.inner_maxits, self.inner_rtol = int(max_iter), float(rel_tol)
+        self._release()
+
+    def _release(self):
+        if self._s:
+            load().b200la_mp_destroy(self._s)
+            self._s = C.c_void_p()
+
+    def _ensure(self):
+        if self._s:
+            return
+        if self.op is None:
+            raise B200LAError(-1, "MPIR: SetupOperator was not called")
+        prm = _lib.MpParams(self.max_ecl, self.abs_tol, self.rel_tol, self.div_tol, self.inner_maxits,
+                            self.inner_rtol, 1 if self.precond else 0, 1 if self.tune else 0)
+        call("b200la_mp_create", self.op.handle, C.byref(prm), C.byref(self._s))
+
+    def Solve(self, b: B200_lVector, x: B200_lVector) -> int:
+        self._ensure()
+        r = _lib.MpResult()
+        call("b200la_mp_solve", self._s, b.handle, x.handle, C.byref(r))
+        self.iter_, self.outer_ = r.inner_iters, r.outer
+        self.res_, self.res_init_, self.res_rel_ = r.res, r.res_init, r.res_rel
+        self.state_ = r.state
+        return r.solver_state
+
+    def iter(self) -> int:
+        return self.iter_
+
+    def res(self) -> float:
+        return self.res_
+
+    def __del__(self):
+        if sys.is_finalizing():
+            return
+        try:
+            self._release()
+        except Exception:
+            pass

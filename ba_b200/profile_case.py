@@ -1,0 +1,71 @@
+"""Profiling driver: runs the path's kernels on one standard system as plain
+launches (no CUDA graph), so a profiler sees every launch on its own.
+
+    python -m ba_b200.profile_case [--cells 128] [--dim 3] [--dtype f64|f32]
+                                   [--spmv-reps 3] [--cg-iters 3] [--schedule tune|csr/8|sell/1]
+
+Launch order: the tuner's SpMV launches (unless a schedule is given), then
+`--spmv-reps` plain SpMV launches (spmv_kernel), then the CG init kernel and
+`--cg-iters` iterations of cg_spmv_kernel, cg_update_kernel and
+cg_direction_kernel.  Prints the CUDA-event time of each kernel.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import time
+
+import numpy as np
+
+from . import lmp
+from . import problems as P
+from ._lib import FMT_CSR, FMT_SELL, call, load
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--cells", type=int, default=128)
+    ap.add_argument("--dim", type=int, default=3)
+    ap.add_argument("--dtype", default="f64", choices=["f64", "f32"])
+    ap.add_argument("--spmv-reps", type=int, default=3)
+    ap.add_argument("--cg-iters", type=int, default=3)
+    ap.add_argument("--schedule", default="tune")
+    ap.add_argument("--sigma", type=float, default=0.0)
+    a = ap.parse_args()
+    dt = np.float64 if a.dtype == "f64" else np.float32
+    s = P.q1_system(a.dim, a.cells, 20240602, a.sigma)
+    plat = lmp.init_platform(0)
+    A = lmp.B200_CSR_lMatrix(s.rowptr, s.col, s.val, platform=plat, dtype=dt)
+    if a.schedule == "tune":
+        fmt, prm, us = A.tune()
+    else:
+        kind, prm = a.schedule.split("/")
+        fmt, prm = (FMT_SELL if kind == "sell" else FMT_CSR), int(prm)
+        A.set_format(fmt, prm)
+        us = float("nan")
+    x = lmp.B200_lVector.from_numpy(s.b.astype(dt), platform=plat, dtype=dt)
+    y = x.CloneWithoutContent()
+    plat.synchronize()
+    t = time.perf_counter()
+    for _ in range(a.spmv_reps):
+        A.VectorMult(x, y)
+    plat.synchronize()
+    spmv_ms = (time.perf_counter() - t) * 1e3 / max(a.spmv_reps, 1)
+    solver = lmp.setup_CG_solver(maxits=100000, atol=0.0, rtol=1e-12, dtol=1e8)
+    solver.SetupOperator(A)
+    solver._ensure()
+    b = lmp.B200_lVector.from_numpy(s.b.astype(dt), platform=plat, dtype=dt)
+    x0 = lmp.B200_lVector(s.n, platform=plat, dtype=dt)
+    ms = (C.c_double * 3)()
+    call("b200la_cg_profile", solver._solver, b.handle, x0.handle, a.cg_iters, ms)
+    sv = 8 if dt == np.float64 else 4
+    alg = s.nnz * (sv + 4) + (s.n + 1) * 4 + 2 * s.n * sv
+    print(f"system n={s.n} nnz={s.nnz} dtype={a.dtype} schedule={'sell' if fmt == FMT_SELL else 'csr'}/{prm} "
+          f"tuned_us={us:.1f}")
+    print(f"spmv wall {spmv_ms:.3f} ms/launch; cg kernels ms: spmv_dot {ms[0]:.4f} update {ms[1]:.4f} "
+          f"direction {ms[2]:.4f}; spmv algorithmic bytes {alg} -> {alg / ms[0] / 1e6:.1f} GB/s")
+    load()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,24 +1,29 @@
 #!/usr/bin/env python
-"""Benchmark of the Jacobi-PCG hot path on B200 (one JSON line on rank 0).
+"""Benchmark of the PCG hot path on B200: one JSON line on rank 0.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload poisson3d]
+                    [--workload batch|poisson3d]
 
-Workload "poisson3d": FP64 Jacobi-PCG on 3D Q1 Poisson, 128^3 hex cells
-(2,146,689 DOFs, 57,066,625 nnz, FP64 values, int32 indices), Dirichlet
-boundary, seeded U[0,1) RHS, rel. residual 1e-10.  A step is one full solve;
-the metric is solves/s.  The matrix (685 MB) is larger than L2, so each
-iteration streams it from HBM.
+Workload "batch" (default): 1,024 independent 2D Q1 diffusion systems, n x n
+cells with n log-uniform in [16, 256] from the seed, lognormal per-cell
+coefficient (sigma = 1), seeded U[0,1) RHS, solved to 1e-8 relative FP64
+residual by FP32 Jacobi-PCG inside FP64 refinement, all systems in one
+CUDA-graph launch with the tuned SpMV schedule.  A step solves the whole
+batch; the metric is solves/s, with p50/p99 of the per-system device latency
+inside the step.  The plain FP64 GPU CG comparator solves the same batch with
+the unpreconditioned FP64 CG recurrence.  The batch's matrices (about 1.3 GB
+of FP64 CSR) are larger than L2.
 
-Multi-GPU: every rank solves its own copy of the system (replicas; the path
-has no exchange step for independent solves), value = all ranks' solves / the
-slowest rank's time.
+Workload "poisson3d": FP64 Jacobi-PCG on 3D Q1 Poisson, 128^3 cells
+(2,146,689 DOFs, 57,066,625 nnz), rel. 1e-10; a step is one solve.
+
+Multi-GPU: every rank solves its own batch (seeded per rank): independent
+systems need no exchange, value = all ranks' solves / the slowest rank's time.
 
 --impl reference times the reference's own CPU implementation (HiFlow3 lmp
 sources compiled into oracle/_ref: OPENMP CSR SpMV on all host cores, lmp
-BLAS-1, lPreconditioner_Jacobi, CG<LAD> recurrence) on the same system, a
-bounded sample of iterations per step scaled by the reference's own
-iteration count for the full solve (tests/golden/workload_counts.json).
+BLAS-1, lPreconditioner_Jacobi, the CG<LAD> call sequence; the reference has
+no mixed-precision GPU path) on a bounded sample of the same workload.
 """
 from __future__ import annotations
 
@@ -38,6 +43,8 @@ sys.path.insert(0, ROOT)
 
 METRIC = "PCG solves/s & p50/p99 latency at 1e-8 rel. residual vs plain FP64 GPU CG"
 COUNTS = os.path.join(ROOT, "tests", "golden", "workload_counts.json")
+BATCH_COUNT = 1024
+BATCH_RTOL = 1e-8
 
 
 def parse():
@@ -46,8 +53,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="poisson3d", choices=["poisson3d"])
-    ap.add_argument("--cells", type=int, default=128)
+    ap.add_argument("--workload", default="batch", choices=["batch", "poisson3d"])
+    ap.add_argument("--cells", type=int, default=128, help="poisson3d cells per axis")
+    ap.add_argument("--count", type=int, default=BATCH_COUNT, help="batch: systems per step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -62,6 +70,13 @@ def measured_peak_gbs():
     if os.path.exists(p):
         return float(json.load(open(p))["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
+
+
+def profile_traffic(key):
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(p):
+        return json.load(open(p)).get(key)
+    return None
 
 
 class ClockSampler:
@@ -118,10 +133,244 @@ def spmv_bytes(n: int, nnz: int, sv: int) -> int:
     return nnz * (sv + 4) + (n + 1) * 4 + n * sv + n * sv
 
 
-def run_reference(args, rank: int):
-    """The reference CPU implementation, rank 0 only."""
-    if rank != 0:
+# ----------------------------------------------------------------- batch workload
+def batch_seed(rank: int) -> int:
+    from ba_b200 import problems as P
+    return P.SEED_BATCH + 7919 * rank
+
+
+def make_batch_systems(count: int, rank: int):
+    from ba_b200 import problems as P
+    return P.batch_systems(count, sigma=1.0, seed=batch_seed(rank))
+
+
+def ref_batch_sample(systems, k: int, sample: int, nthreads: int):
+    """The reference's CPU CG (FP64 Jacobi-PCG, OPENMP SpMV) to 1e-8 on a seeded
+    sample of the batch's systems; returns (solves, seconds)."""
+    import oracle
+    rng = np.random.default_rng(1000 + k)
+    pick = rng.choice(len(systems), size=min(sample, len(systems)), replace=False)
+    total = 0.0
+    for i in pick:
+        s = systems[int(i)]
+        ref = oracle.RefSystem(s.rowptr, s.col, s.val, impl=oracle.IMPL_OPENMP, nthreads=nthreads)
+        _, sec = ref.cg(s.b, maxits=100000, atol=0.0, rtol=BATCH_RTOL, dtol=1e8, precond=True)
+        ref.close()
+        total += sec
+    return len(pick), total
+
+
+def batch_config(args, systems, extra=None):
+    n_tot = int(sum(s.n for s in systems))
+    nnz_tot = int(sum(s.nnz for s in systems))
+    cfg = {"workload": f"batched: {len(systems)} independent 2D Q1 systems, n~logU[16,256] cells, "
+                       f"lognormal kappa sigma=1, rel. residual 1e-8 (FP32 PCG + FP64 refinement)",
+           "systems": len(systems), "dofs_total": n_tot, "nnz_total": nnz_tot,
+           "l2": "inputs larger than L2 (1.3 GB FP64 CSR + 0.9 GB FP32 values per batch)"}
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+def run_reference_batch(args, rank):
+    import oracle
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (reference sources absent)"}))
         return
+    systems = make_batch_systems(args.count, 0)
+    nthreads = os.cpu_count() or 1
+    sample = 32
+    rates = []
+    for step in range(args.warmup + args.steps):
+        cnt, sec = ref_batch_sample(systems, step, sample, nthreads)
+        if step >= args.warmup:
+            rates.append(cnt / sec)
+    value = statistics.median(rates)
+    out = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * args.count / value,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": batch_config(args, systems, {"parallelism": f"cpu openmp x{nthreads}",
+                                               "precision": "FP64 Jacobi-PCG (the reference's CPU path)"}),
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": nthreads, "kind": "reference",
+                         "sample": f"{sample} seeded systems of the {args.count}-system batch per step, each "
+                                   f"solved to 1e-8 by HiFlow3 lmp CG (OPENMP SpMV, {nthreads} threads)"},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out))
+
+
+def _pinned(a, torch):
+    t = torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+    return t, t.numpy()
+
+
+def run_batch(args, rank, local_rank, world, torch, dist, barrier):
+    from ba_b200 import lmp
+    from ba_b200.batch import Batch
+
+    plat = lmp.Platform(local_rank)
+    stream = torch.cuda.current_stream()
+    plat.set_stream(stream.cuda_stream)
+    systems = make_batch_systems(args.count, rank)
+    keep, host = [], []
+    for s in systems:
+        arrs = [_pinned(a, torch) for a in (s.rowptr, s.col, s.val, s.b)]
+        keep.append([t for t, _ in arrs])
+        host.append([a for _, a in arrs])
+    cap = len(systems)
+    kw = dict(mixed=True, precond=True, rtol=BATCH_RTOL, atol=0.0, dtol=1e8, inner_rtol=1e-4, max_outer=30,
+              platform=plat)
+    B = Batch(cap, **kw)
+    for h in host:
+        B.add(*h)
+    lanes, _ = B.tune()
+    n_tot = int(sum(s.n for s in systems))
+
+    def step():
+        B.restart()
+        left = B.run()
+        assert left == 0, left
+        return B.last_passes()
+
+    for _ in range(args.warmup):
+        passes = step()
+    clocks = ClockSampler(local_rank)
+    barrier()
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    passes_tot = 0
+    for _ in range(args.steps):
+        passes_tot += step()
+    e1.record(stream)
+    e1.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * args.steps * len(systems) / (ms_max / 1e3)
+
+    # per-system results of the last step: states, latency inside the step, accuracy
+    res = [B.result(k, with_x=True) for k in range(len(systems))]
+    ok = sum(1 for r in res if r.solver_state == 0)
+    lat = np.array([r.device_us for r in res]) / 1e3
+    iters = np.array([r.iters for r in res])
+    outer = np.array([r.outer for r in res])
+    import scipy.sparse as sp
+    worst = 0.0
+    for s, r in zip(systems[::64], res[::64]):
+        A = sp.csr_matrix((s.val, s.col, s.rowptr), shape=(s.n, s.n))
+        worst = max(worst, float(np.linalg.norm(s.b - A @ r.x) / np.linalg.norm(s.b)))
+
+    # plain FP64 GPU CG (SolveNoPrecond recurrence), same batch, same machinery
+    Pn = Batch(cap, mixed=False, precond=False, rtol=BATCH_RTOL, atol=0.0, dtol=1e8, inner_maxits=1000000,
+               platform=plat)
+    for h in host:
+        Pn.add(*h)
+    Pn.tune()
+    Pn.restart()
+    Pn.run()
+    barrier()
+    k_plain = max(2, args.steps // 2)
+    c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    c0.record(stream)
+    for _ in range(k_plain):
+        Pn.restart()
+        assert Pn.run() == 0
+    c1.record(stream)
+    c1.synchronize()
+    plain_value = len(systems) * k_plain / (c0.elapsed_time(c1) / 1e3)
+    plain_iters = np.array([Pn.result(k, with_x=False).iters for k in range(len(systems))])
+    Pn.close()
+
+    # end to end through the public API: upload every system from pinned host
+    # memory, solve, download every solution, each step
+    E = Batch(cap, **kw)
+    E.add(*host[0])
+    E.tune()
+    xs = [torch.empty(s.n, dtype=torch.float64).pin_memory().numpy() for s in systems]
+    h2d = int(sum(h[0].nbytes + h[1].nbytes + h[2].nbytes + h[3].nbytes for h in host))
+    d2h = int(sum(x.nbytes for x in xs))
+    import ctypes as C
+    from ba_b200._lib import SysResult, load
+    lib = load()
+
+    def e2e_step():
+        for k in range(len(systems)):
+            try:
+                E.remove(k)
+            except Exception:
+                pass
+        for h in host:
+            E.add(*h)
+        assert E.run() == 0
+        r = SysResult()
+        for k, x in enumerate(xs):
+            lib.b200la_batch_result(E.handle, k, x.ctypes.data_as(C.c_void_p), C.byref(r))
+
+    e2e_step()
+    barrier()
+    h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    k_e2e = max(2, args.steps // 2)
+    h0.record(stream)
+    for _ in range(k_e2e):
+        e2e_step()
+    h1.record(stream)
+    h1.synchronize()
+    te = torch.tensor([h0.elapsed_time(h1)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = world * k_e2e * len(systems) / (float(te.item()) / 1e3)
+    E.close()
+
+    # roofline of the dominant kernel: the inner solve's batched FP32 SpMV
+    spmv_ms, spmv_bytes_alg = B.profile(10)
+    peak, peak_kind = measured_peak_gbs()
+    achieved = spmv_bytes_alg / (spmv_ms / 1e3) / 1e9
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import oracle
+        if oracle.ref_available():
+            nthreads = os.cpu_count() or 1
+            cnt, sec = ref_batch_sample(systems, 0, 32, nthreads)
+            cpu = {"value": cnt / sec, "unit": "solves/s", "cores": nthreads, "kind": "reference",
+                   "sample": f"32 seeded systems of the batch, each solved to 1e-8 by HiFlow3 lmp CG "
+                             f"(FP64 Jacobi-PCG, OPENMP SpMV, {nthreads} threads)"}
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+            "config": batch_config(args, systems, {
+                "parallelism": f"replicas x{world}", "spmv_schedule": f"csr/{lanes} lanes per row",
+                "p50_latency_ms": float(np.percentile(lat, 50)), "p99_latency_ms": float(np.percentile(lat, 99)),
+                "latency": "per-system device time from its first residual to its finish inside the step",
+                "converged": f"{ok}/{len(systems)}", "worst_true_rel_residual_sampled": worst,
+                "inner_iters_mean": float(iters.mean()), "inner_iters_max": int(iters.max()),
+                "refinement_passes_max": int(outer.max()), "device_loop_passes_per_step": passes_tot / args.steps,
+                "plain_fp64_cg": {"value": plain_value, "unit": "solves/s",
+                                  "iters_mean": float(plain_iters.mean()), "iters_max": int(plain_iters.max()),
+                                  "speedup_of_mixed_pcg": value / world / plain_value}}),
+            "clocks": clk,
+            "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": args.steps * (2 + 4 * passes_tot // max(args.steps, 1)),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": profile_traffic("batch1024/f32/spmv"), "peak_source": peak_kind,
+                         "kernel": "batch_spmv_kernel (FP32 inner SpMV over all systems)",
+                         "algorithmic_bytes": spmv_bytes_alg, "kernel_ms": spmv_ms},
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(out))
+    B.close()
+
+
+# ----------------------------------------------------------------- poisson3d workload
+def run_reference_poisson3d(args, rank):
     import oracle
     from ba_b200 import problems as P
     if not oracle.ref_available():
@@ -129,8 +378,7 @@ def run_reference(args, rank: int):
         return
     s = P.poisson_3d(args.cells)
     counts = json.load(open(COUNTS)) if os.path.exists(COUNTS) else {}
-    key = f"poisson3d_{args.cells}/jacobi/rtol1e-10"
-    full_iters = counts.get(key, {}).get("iters")
+    full_iters = counts.get(f"poisson3d_{args.cells}/jacobi/rtol1e-10", {}).get("iters", 20)
     nthreads = os.cpu_count() or 1
     ref = oracle.RefSystem(s.rowptr, s.col, s.val, impl=oracle.IMPL_OPENMP, nthreads=nthreads)
     sample_iters = 20
@@ -139,90 +387,47 @@ def run_reference(args, rank: int):
         r, sec = ref.cg(s.b, maxits=sample_iters, atol=0.0, rtol=1e-10, dtol=1e8, precond=True)
         if step >= args.warmup:
             per_iter.append(sec / max(r.iters, 1))
-    t_iter = statistics.median(per_iter)
-    iters = full_iters or sample_iters
-    value = 1.0 / (t_iter * iters)
-    out = {
+    value = 1.0 / (statistics.median(per_iter) * full_iters)
+    print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"fp64 jacobi-pcg 3d q1 poisson {args.cells}^3 cells, rel 1e-10",
-                   "n": s.n, "nnz": s.nnz, "parallelism": "cpu openmp"},
+        "config": {"workload": f"fp64 jacobi-pcg 3d q1 poisson {args.cells}^3 cells, rel 1e-10", "n": s.n,
+                   "nnz": s.nnz, "parallelism": f"cpu openmp x{nthreads}"},
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": nthreads, "kind": "reference",
-                         "sample": f"{sample_iters} of {iters} iterations of one solve per step "
-                                   f"(HiFlow3 lmp OPENMP SpMV, {nthreads} threads), scaled to a full solve"},
-        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }
-    print(json.dumps(out))
+                         "sample": f"{sample_iters} of {full_iters} iterations of one solve per step, scaled"},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
 
 
-def cpu_baseline_leg(s, full_iters):
-    """Reference CPU CG on the same system (bounded sample, all host threads)."""
-    import oracle
-    if not oracle.ref_available():
-        return None
-    nthreads = os.cpu_count() or 1
-    ref = oracle.RefSystem(s.rowptr, s.col, s.val, impl=oracle.IMPL_OPENMP, nthreads=nthreads)
-    sample_iters = 20
-    ref.cg(s.b, maxits=2, atol=0.0, rtol=1e-10, dtol=1e8)
-    r, sec = ref.cg(s.b, maxits=sample_iters, atol=0.0, rtol=1e-10, dtol=1e8, precond=True)
-    t_iter = sec / max(r.iters, 1)
-    ref.close()
-    return {"value": 1.0 / (t_iter * full_iters), "unit": "solves/s", "cores": nthreads, "kind": "reference",
-            "sample": f"{sample_iters} of {full_iters} iterations of one solve (HiFlow3 lmp OPENMP SpMV, "
-                      f"{nthreads} threads), scaled to a full solve"}
-
-
-def main():
-    args = parse()
-    rank, local_rank, world = dist_env()
-    if args.impl == "reference":
-        run_reference(args, rank)
-        return
-
-    import torch
-    import torch.distributed as dist
+def run_poisson3d(args, rank, local_rank, world, torch, dist, barrier):
+    import ctypes as C
 
     from ba_b200 import lmp
     from ba_b200 import problems as P
     from ba_b200._lib import FMT_SELL, load
 
-    torch.cuda.set_device(local_rank)
-    if world > 1:
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-        torch.cuda.synchronize()
-
-    load()
     plat = lmp.Platform(local_rank)
     stream = torch.cuda.current_stream()
     plat.set_stream(stream.cuda_stream)
-
     s = P.poisson_3d(args.cells)
     n, nnz = s.n, s.nnz
     A = lmp.B200_CSR_lMatrix(s.rowptr, s.col, s.val, platform=plat)
-    fmt, prm, tune_us = A.tune()
+    fmt, prm, _ = A.tune()
     b = lmp.B200_lVector.from_numpy(s.b, platform=plat)
     x = lmp.B200_lVector(n, platform=plat)
-    rtol = 1e-10
-    solver = lmp.setup_CG_solver(maxits=20000, atol=0.0, rtol=rtol, dtol=1e8, use_precond=True)
+    solver = lmp.setup_CG_solver(maxits=20000, atol=0.0, rtol=1e-10, dtol=1e8, use_precond=True)
     solver.SetupOperator(A)
-    plain = lmp.setup_CG_solver(maxits=20000, atol=0.0, rtol=rtol, dtol=1e8, use_precond=False)
+    plain = lmp.setup_CG_solver(maxits=20000, atol=0.0, rtol=1e-10, dtol=1e8, use_precond=False)
     plain.SetupOperator(A)
 
     def step(sv):
         x.Zeros()
-        st = sv.Solve(b, x)
-        assert st == lmp.kSolverSuccess, st
+        assert sv.Solve(b, x) == lmp.kSolverSuccess
         return sv.iter()
 
     for _ in range(args.warmup):
         step(solver)
     iters = solver.iter()
-
     clocks = ClockSampler(local_rank)
     barrier()
     clocks.start()
@@ -234,16 +439,12 @@ def main():
     e1.synchronize()
     barrier()
     clk = clocks.stop()
-    ms = e0.elapsed_time(e1)
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms_max = float(t.item())
     value = world * args.steps / (ms_max / 1e3)
-
-    # plain FP64 GPU CG (SolveNoPrecond recurrence) on the same system: the comparator
     step(plain)
-    barrier()
     c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     k_plain = max(2, args.steps // 2)
     c0.record(stream)
@@ -252,14 +453,9 @@ def main():
     c1.record(stream)
     c1.synchronize()
     plain_value = k_plain / (c0.elapsed_time(c1) / 1e3)
-    plain_iters = plain.iter()
-
-    # end to end through the public API: H2D of the RHS from pinned memory,
-    # solve, D2H of the solution, every step.
+    lib = load()
     bh = torch.from_numpy(s.b).pin_memory()
     xh = torch.empty(n, dtype=torch.float64).pin_memory()
-    import ctypes as C
-    lib = load()
     barrier()
     h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     h0.record(stream)
@@ -273,46 +469,69 @@ def main():
     if world > 1:
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
     e2e_value = world * args.steps / (float(te.item()) / 1e3)
-
-    # roofline of the dominant kernel (SpMV + p.Ap), timed live with CUDA events
     ms3 = (C.c_double * 3)()
     x.Zeros()
     lib.b200la_cg_profile(solver._solver, b.handle, x.handle, 20, ms3)
-    t_spmv = ms3[0] / 1e3
     bytes_spmv = spmv_bytes(n, nnz, 8)
     peak, peak_kind = measured_peak_gbs()
-    achieved = bytes_spmv / t_spmv / 1e9
-    traffic = None
-    prof = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(prof):
-        traffic = json.load(open(prof)).get(f"poisson3d_{args.cells}/f64/spmv")
-
+    achieved = bytes_spmv / (ms3[0] / 1e3) / 1e9
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        counts = json.load(open(COUNTS)) if os.path.exists(COUNTS) else {}
-        full = counts.get(f"poisson3d_{args.cells}/jacobi/rtol1e-10", {}).get("iters", iters)
-        cpu = cpu_baseline_leg(s, full)
-
+        import oracle
+        if oracle.ref_available():
+            counts = json.load(open(COUNTS)) if os.path.exists(COUNTS) else {}
+            full = counts.get(f"poisson3d_{args.cells}/jacobi/rtol1e-10", {}).get("iters", iters)
+            nthreads = os.cpu_count() or 1
+            ref = oracle.RefSystem(s.rowptr, s.col, s.val, impl=oracle.IMPL_OPENMP, nthreads=nthreads)
+            r, sec = ref.cg(s.b, maxits=20, atol=0.0, rtol=1e-10, dtol=1e8)
+            cpu = {"value": 1.0 / (sec / max(r.iters, 1) * full), "unit": "solves/s", "cores": nthreads,
+                   "kind": "reference", "sample": f"20 of {full} iterations of one solve (HiFlow3 lmp OPENMP "
+                                                  f"SpMV, {nthreads} threads), scaled to a full solve"}
     if rank == 0:
-        out = {
+        print(json.dumps({
             "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"fp64 jacobi-pcg 3d q1 poisson {args.cells}^3 cells, rel 1e-10",
-                       "n": n, "nnz": nnz, "iters_per_solve": iters, "parallelism": f"replicas x{world}",
+            "config": {"workload": f"fp64 jacobi-pcg 3d q1 poisson {args.cells}^3 cells, rel 1e-10", "n": n,
+                       "nnz": nnz, "iters_per_solve": iters, "parallelism": f"replicas x{world}",
                        "spmv_schedule": ("sell" if fmt == FMT_SELL else "csr") + f"/{prm}",
                        "l2": "inputs larger than L2 (matrix 685 MB streamed per iteration)",
-                       "plain_fp64_cg": {"value": plain_value, "unit": "solves/s", "iters_per_solve": plain_iters}},
+                       "plain_fp64_cg": {"value": plain_value, "unit": "solves/s", "iters_per_solve": plain.iter()}},
             "clocks": clk,
             "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": n * 8, "d2h_bytes_per_step": n * 8},
             "gpu_launches": args.steps * (1 + 3 * iters),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": traffic, "peak_source": peak_kind,
+                         "traffic": profile_traffic(f"poisson3d_{args.cells}/f64/spmv"), "peak_source": peak_kind,
                          "kernel": "cg_spmv_kernel (SpMV fused with p.Ap)", "algorithmic_bytes": bytes_spmv,
                          "kernel_ms": {"spmv_dot": ms3[0], "update": ms3[1], "direction": ms3[2]}},
-            "cpu_baseline": cpu,
-        }
-        print(json.dumps(out))
+            "cpu_baseline": cpu}))
+
+
+def main():
+    args = parse()
+    rank, local_rank, world = dist_env()
+    if args.impl == "reference":
+        if rank == 0:
+            (run_reference_batch if args.workload == "batch" else run_reference_poisson3d)(args, rank)
+        return
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    from ba_b200 import load
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    load()
+    fn = run_batch if args.workload == "batch" else run_poisson3d
+    fn(args, rank, local_rank, world, torch, dist, barrier)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

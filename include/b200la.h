@@ -28,6 +28,8 @@ typedef struct b200la_ctx_s *b200la_ctx;
 typedef struct b200la_vec_s *b200la_vec;
 typedef struct b200la_mat_s *b200la_mat;
 typedef struct b200la_cg_s *b200la_cg;
+typedef struct b200la_mp_s *b200la_mp;
+typedef struct b200la_batch_s *b200la_batch;
 
 /* ---- status codes --------------------------------------------------------
  * The reference reports errors by LOG_ERROR + exit(-1)/quit_program()
@@ -188,6 +190,123 @@ int b200la_cg_profile(b200la_cg s, b200la_vec b, b200la_vec x, int iters, double
 /* One-shot convenience: create + solve + destroy. */
 int b200la_pcg_solve(b200la_mat A, b200la_vec b, b200la_vec x, const b200la_cg_params *params,
                      b200la_cg_result *result);
+
+/* ---- Q1 system assembly on the device (no reference counterpart: the
+ * reference assembles on the host through its FE stack and uploads the CSR).
+ * Builds the Q1 stiffness of -div(kappa grad u) on `cells`^dim uniform cells of
+ * the unit square/cube with lexicographic numbering, Dirichlet rows as
+ * CoupledMatrix::diagonalize_rows leaves them (coupled_matrix.cc:452-477),
+ * kappa = exp(sigma * g) per cell and RHS U[0,1) on interior rows from the
+ * seed's splitmix64 streams.  Output buffers are device memory of
+ * b200la_q1_size's sizes (rowptr n+1, col/val nnz, rhs n). */
+int b200la_q1_size(int dim, int cells, int64_t *n, int64_t *nnz);
+int b200la_q1_assemble(b200la_ctx ctx, int dim, int cells, uint64_t seed, double sigma, int *rowptr,
+                       int *col, double *val, double *rhs);
+
+/* ---- mixed-precision refinement: MPIR<LAD_high, LAD_low>::SolveImpl
+ * (linear_solver/mpir.cc:52-230) with an FP32 Jacobi-PCG as the low-precision
+ * error-correction solver and no smoothers.  The residual r = b - A x, the
+ * update x += c and the stopping test run in FP64 on the device; the inner
+ * solve runs SpMV and vector updates in FP32 (FP32 matrix values, int32
+ * indices, dot products accumulated in FP32 with compensated summation).
+ * The outer test is relative to the initial residual (the reference resets
+ * res0_ every pass, mpir.cc:239). */
+typedef struct {
+  int max_outer;      /* refinement passes (MPIR max_ecl) */
+  double atol;        /* success if ||r||_2 <= atol */
+  double rtol;        /* success if ||r||_2 < rtol * ||r0||_2 */
+  double dtol;        /* divergence if ||r||_2 > dtol * ||r0||_2 */
+  int inner_maxits;   /* per pass */
+  double inner_rtol;  /* the FP32 solve stops at inner_rtol times its start residual */
+  int precond;        /* 1: Jacobi in the FP32 solve */
+  int tune;           /* 1: autotune the FP32 matrix's SpMV schedule at create */
+} b200la_mp_params;
+
+typedef struct {
+  int outer;          /* refinement passes taken */
+  int inner_iters;    /* FP32 PCG iterations over all passes */
+  int state;          /* B200LA_SUCCESS_ABS/_REL, B200LA_FAIL_DIV/_MAXITS */
+  int solver_state;   /* B200LA_SOLVER_SUCCESS / _EXCEEDED */
+  double res;         /* final FP64 ||b - A x||_2 */
+  double res_init;
+  double res_rel;
+} b200la_mp_result;
+
+/* A64 must be FP64; an FP32 copy is made (CastFrom) and kept with the solver. */
+int b200la_mp_create(b200la_mat A64, const b200la_mp_params *params, b200la_mp *out);
+int b200la_mp_destroy(b200la_mp s);
+/* The FP32 copy, e.g. to pick its SpMV schedule (owned by the solver). */
+int b200la_mp_inner_matrix(b200la_mp s, b200la_mat *out);
+/* b, x FP64; x holds the start value on entry and the solution on exit. */
+int b200la_mp_solve(b200la_mp s, b200la_vec b, b200la_vec x, b200la_mp_result *result);
+
+/* ---- batched and served PCG (no reference counterpart: the reference runs
+ * one CG<LAD> solve per call).  Many independent systems of uneven size live
+ * in the slots of one batch; b200la_batch_run advances every running system
+ * with one CUDA-graph launch whose kernels sweep all of them, tile by tile.
+ * Each system follows the Jacobi-PCG recurrence of CG<LAD>
+ * (linear_solver/cg.h:165-246), either in FP64 (mixed = 0) or as FP32 inner
+ * solves inside FP64 refinement (mixed = 1, MPIR structure, mpir.cc:52-230).
+ * Systems can be added and removed between runs (continuous batching). */
+typedef struct {
+  int capacity;       /* system slots */
+  int mixed;          /* 1: FP32 inner PCG + FP64 refinement; 0: FP64 PCG */
+  int precond;        /* 1: Jacobi */
+  int max_outer;      /* refinement passes (mixed) */
+  int inner_maxits;   /* iterations per inner solve (FP64 mode: per solve) */
+  int lanes;          /* CSR lanes per row: 2..32 (0 = 4) */
+  int tile_rows;      /* rows per tile (0 = 512) */
+  int reserved;
+  double atol, rtol, dtol;  /* test on ||b - A x||_2 (FP64 mode: the CG recurrence residual) */
+  double inner_rtol;        /* mixed: inner solve stops at inner_rtol x its start residual */
+} b200la_batch_params;
+
+typedef struct {
+  int state;          /* B200LA_ITERATE while running, else the final state */
+  int solver_state;   /* B200LA_SOLVER_* */
+  int iters;          /* (inner) PCG iterations */
+  int outer;          /* refinement passes (FP64 mode: 1) */
+  int phase_done;     /* 1 once the system has finished */
+  int reserved;
+  double res, res_init, res_rel;  /* final FP64 residual norm, initial, ratio */
+  double device_us;   /* device time from its first residual to its finish */
+} b200la_sys_result;
+
+int b200la_batch_create(b200la_ctx ctx, const b200la_batch_params *params, b200la_batch *out);
+int b200la_batch_destroy(b200la_batch b);
+/* Device bytes one slot holds for a system of n rows and nnz entries. */
+int b200la_batch_slot_bytes(int64_t n, int64_t nnz, int mixed, int64_t *bytes);
+/* Upload one system (host CSR, FP64 values, FP64 RHS; x0 NULL = zero start)
+ * into a free slot; it joins at the next run.  Copies are queued on the
+ * context stream: host buffers must stay valid until the next run. */
+int b200la_batch_add(b200la_batch b, int n, int64_t nnz, const int *rowptr, const int *col,
+                     const double *val, const double *rhs, const double *x0, int *slot);
+/* Assemble a Q1 diffusion system on the device directly into a free slot:
+ * dim 2 or 3, `cells` per axis on the unit square/cube, per-cell coefficient
+ * exp(sigma * g) (sigma = 0: Poisson), homogeneous Dirichlet rows, RHS
+ * U[0,1) on interior rows, from `seed` (see b200la_q1_assemble). */
+int b200la_batch_add_q1(b200la_batch b, int dim, int cells, uint64_t seed, double sigma, int *slot);
+/* Copy a slot's system back to the host (any pointer may be NULL). */
+int b200la_batch_get_system(b200la_batch b, int slot, int *rowptr, int *col, double *val, double *rhs);
+int b200la_batch_slot_size(b200la_batch b, int slot, int *n, int64_t *nnz);
+int b200la_batch_remove(b200la_batch b, int slot);
+/* One graph launch: at most max_passes iterations of every running system.
+ * Writes how many systems are still running. */
+int b200la_batch_run(b200la_batch b, int max_passes, int *active);
+/* Body passes (iterations of the device loop) taken by the last run. */
+int b200la_batch_last_run(b200la_batch b, int *passes, double *reserved);
+/* Result of a slot (solution copied to x if non-NULL). */
+int b200la_batch_result(b200la_batch b, int slot, double *x, b200la_sys_result *result);
+int b200la_batch_info(b200la_batch b, int *used_slots, int64_t *device_bytes);
+/* Restart every system in the batch from x = 0 (matrices and RHS stay). */
+int b200la_batch_restart(b200la_batch b);
+/* Times each CSR lanes-per-row choice on the batch's matrices and keeps the
+ * fastest; writes the choice and its time per batched SpMV in microseconds. */
+int b200la_batch_tune(b200la_batch b, int *lanes, double *usec);
+/* Instrumentation: mean milliseconds of the inner solve's batched SpMV over
+ * every slot (reps launches, CUDA events) and its algorithmic bytes:
+ * sum over systems of nnz*(value+4) + (n+1)*4 + 2*n*value. */
+int b200la_batch_profile(b200la_batch b, int reps, double *ms_spmv, int64_t *algorithmic_bytes);
 
 #ifdef __cplusplus
 }

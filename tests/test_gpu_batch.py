@@ -1,0 +1,175 @@
+"""Batched / continuously batched PCG on the GPU against the CPU oracle.
+
+* FP64 mode: each system in a mixed batch takes the reference CG's
+  iteration count (+-1) and matches the oracle's solution within 1e-10.
+* Mixed mode (FP32 inner + FP64 refinement): every system reaches the stated
+  FP64 relative residual; its error against the FP64 oracle is bounded.
+* Isolation: a system's result is the same alone, in the mix, and when it is
+  admitted while other systems are already running (per-system reductions are
+  deterministic, so the results agree bit for bit).
+"""
+import numpy as np
+import pytest
+
+import oracle
+from ba_b200 import lmp
+from ba_b200 import problems as P
+from ba_b200.batch import Batch
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def plat():
+    return lmp.init_platform(0)
+
+
+def _mix(seed=1, count=12):
+    out = []
+    for k in range(count):
+        dim = 2 if k % 3 else 3
+        n = [6, 17, 31, 9, 40, 12][k % 6] if dim == 2 else [4, 7, 10][k % 3]
+        sigma = [0.0, 1.0, 2.0][k % 3]
+        out.append(P.q1_system(dim, n, seed * 100 + k, sigma, f"mix{k}"))
+    return out
+
+
+def test_fp64_batch_matches_reference_cg(plat):
+    systems = _mix()
+    B = Batch(len(systems), mixed=False, precond=True, rtol=1e-10, atol=0.0, dtol=1e8, platform=plat)
+    slots = [B.add_system(s) for s in systems]
+    assert B.run() == 0
+    for s, sl in zip(systems, slots):
+        r = B.result(sl)
+        ref = oracle.cg(s.rowptr, s.col, s.val, s.b, maxits=100000, atol=0.0, rtol=1e-10, dtol=1e8)
+        assert r.done and r.solver_state == lmp.kSolverSuccess, (s.name, r)
+        assert abs(r.iters - ref.iters) <= 1, (s.name, r.iters, ref.iters)
+        assert np.linalg.norm(r.x - ref.x) <= 1e-10 * np.linalg.norm(ref.x), s.name
+        np.testing.assert_allclose(r.res_init, ref.res_init, rtol=1e-12)
+
+
+def test_fp64_batch_plain_cg(plat):
+    """Unpreconditioned FP64 CG (the plain comparator).  On sigma <= 1 systems
+    the iteration count is the reference's +-1.  On the sigma = 2 systems
+    (coefficient contrast ~e^6 without Jacobi scaling) CG's count is
+    sensitive to rounding -- the device's FMA rows and tree-ordered dots move
+    it by a few iterations, as they do for the single-system device CG -- so
+    there the bar is +-2% and the solution within 1e-10 of the oracle's."""
+    systems = _mix(seed=2, count=6)
+    B = Batch(8, mixed=False, precond=False, rtol=1e-10, atol=0.0, platform=plat)
+    slots = [B.add_system(s) for s in systems]
+    B.run()
+    rows = []
+    for s, sl in zip(systems, slots):
+        r = B.result(sl)
+        ref = oracle.cg(s.rowptr, s.col, s.val, s.b, maxits=100000, atol=0.0, rtol=1e-10, precond=False)
+        # single-system device CG on the same matrix, for comparison
+        A = lmp.B200_CSR_lMatrix(s.rowptr, s.col, s.val, platform=plat)
+        A.set_format(1, 4)
+        bv = lmp.B200_lVector.from_numpy(s.b, platform=plat)
+        xv = lmp.B200_lVector(s.n, platform=plat)
+        cg = lmp.setup_CG_solver(maxits=100000, atol=0.0, rtol=1e-10, dtol=1e8, use_precond=False)
+        cg.SetupOperator(A)
+        cg.Solve(bv, xv)
+        rows.append((s.name, s.n, r.iters, cg.iter(), ref.iters,
+                     float(np.linalg.norm(r.x - ref.x) / np.linalg.norm(ref.x))))
+    sig = {s.name: s.meta["sigma"] for s in systems}
+    bad = [x for x in rows
+           if abs(x[2] - x[4]) > (1 if sig[x[0]] <= 1.0 else max(1, 0.02 * x[4])) or x[5] > 1e-10]
+    assert not bad, rows
+
+
+def _true_rel_res(s, x):
+    return np.linalg.norm(s.b - oracle.spmv(s.rowptr, s.col, s.val, x)) / np.linalg.norm(s.b)
+
+
+def test_mixed_batch_reaches_tolerance(plat):
+    sizes = P.batch_sizes(24, lo=16, hi=64, seed=5)
+    systems = [P.q1_system(2, int(n), 500 + k, 1.0, f"b{k}") for k, n in enumerate(sizes)]
+    B = Batch(32, mixed=True, precond=True, rtol=1e-8, inner_rtol=1e-4, platform=plat)
+    B.tune()
+    slots = [B.add_system(s) for s in systems]
+    assert B.run() == 0
+    for s, sl in zip(systems, slots):
+        r = B.result(sl)
+        assert r.done and r.solver_state == lmp.kSolverSuccess, (s.name, r)
+        assert r.res_rel < 1e-8
+        tr = _true_rel_res(s, r.x)
+        assert tr < 1.0001e-8, (s.name, tr)
+        ref = oracle.cg(s.rowptr, s.col, s.val, s.b, maxits=100000, atol=0.0, rtol=1e-13)
+        err = np.linalg.norm(r.x - ref.x) / np.linalg.norm(ref.x)
+        assert err < 1e-5, (s.name, err)
+        assert r.outer >= 2 and r.device_us > 0
+
+
+def test_isolation_alone_vs_mix_vs_late_admission(plat):
+    systems = _mix(seed=3, count=9)
+    probe = systems[4]
+    kw = dict(mixed=True, precond=True, rtol=1e-9, inner_rtol=1e-4, platform=plat)
+    # alone
+    A = Batch(1, **kw)
+    a = A.add_system(probe)
+    A.run()
+    alone = A.result(a)
+    # in the mix
+    M = Batch(16, **kw)
+    slots = [M.add_system(s) for s in systems]
+    M.run()
+    mixed = M.result(slots[4])
+    # admitted while the others are running (continuous batching)
+    L = Batch(16, **kw)
+    others = [L.add_system(s) for k, s in enumerate(systems) if k != 4]
+    assert L.run(max_passes=7) > 0
+    late = L.add_system(probe)
+    while L.run(max_passes=5) > 0:
+        pass
+    late_r = L.result(late)
+    for r in (mixed, late_r):
+        assert r.iters == alone.iters and r.outer == alone.outer
+        np.testing.assert_array_equal(r.x, alone.x)
+    for k, sl in zip([k for k in range(9) if k != 4], others):
+        r = L.result(sl)
+        np.testing.assert_array_equal(r.x, M.result(slots[k]).x)
+
+
+def test_slots_capacity_remove_and_bad_diagonal(plat):
+    B = Batch(2, mixed=False, rtol=1e-10, atol=0.0, platform=plat)
+    s = P.poisson_2d(8)
+    a = B.add_system(s)
+    b = B.add_system(s)
+    with pytest.raises(lmp.B200LAError):
+        B.add_system(s)
+    B.run()
+    B.remove(a)
+    used, nbytes = B.info()
+    assert used == 1 and nbytes > 0
+    # a row without a diagonal: the Jacobi solve ends with an error state
+    rowptr = np.array([0, 2, 3], np.int32)
+    col = np.array([0, 1, 0], np.int32)
+    c = B.add(rowptr, col, np.array([2.0, 1.0, 1.0]), np.array([1.0, 1.0]))
+    B.run()
+    r = B.result(c)
+    assert r.done and r.solver_state == lmp.kSolverError
+    assert B.result(b).solver_state == lmp.kSolverSuccess
+
+
+@pytest.mark.parametrize("dim,cells,sigma", [(2, 9, 0.0), (2, 33, 1.0), (3, 6, 0.0), (3, 11, 2.0)])
+def test_device_assembly_matches_host_generator(plat, dim, cells, sigma):
+    """The device-built Q1 system equals ba_b200.problems' host system:
+    structure and RHS bit for bit, values bit for bit for sigma = 0 and within
+    a few ulps of the coefficient for sigma > 0 (device exp/log/cos)."""
+    B = Batch(2, mixed=True, platform=plat)
+    slot = B.add_q1(dim, cells, 4321, sigma)
+    rp, cl, vv, bb = B.get_system(slot)
+    s = P.q1_system(dim, cells, 4321, sigma)
+    np.testing.assert_array_equal(rp, s.rowptr)
+    np.testing.assert_array_equal(cl, s.col)
+    np.testing.assert_array_equal(bb, s.b)
+    if sigma == 0.0:
+        np.testing.assert_array_equal(vv, s.val)
+    else:
+        np.testing.assert_allclose(vv, s.val, rtol=1e-13, atol=1e-300)
+    B.run()
+    r = B.result(slot)
+    assert r.done and r.solver_state == lmp.kSolverSuccess
+    assert _true_rel_res(s, r.x) < 1.001e-8
