@@ -113,7 +113,7 @@ _SIGS = {
     "b200la_pcg_solve": [_vp, _vp, _vp, _P(CgParams), _P(CgResult)],
     "b200la_batch_create": [_vp, _P(BatchParams), _P(_vp)],
     "b200la_batch_destroy": [_vp],
-    "b200la_batch_slot_bytes": [_i64, _i64, _i, _P(_i64)],
+    "b200la_batch_slot_bytes": [_i64, _i64, _i, _i, _P(_i64)],
     "b200la_batch_add": [_vp, _i, _i64, _vp, _vp, _vp, _vp, _vp, _P(_i)],
     "b200la_batch_remove": [_vp, _i],
     "b200la_batch_run": [_vp, _i, _P(_i)],
@@ -122,6 +122,7 @@ _SIGS = {
     "b200la_batch_tune": [_vp, _P(_i), _P(_d)],
     "b200la_batch_restart": [_vp],
     "b200la_batch_last_run": [_vp, _P(_i), _P(_d)],
+    "b200la_batch_solve": [_vp, _i, _P(_i)],
     "b200la_batch_profile": [_vp, _i, _P(_d), _P(_i64)],
     "b200la_batch_add_q1": [_vp, _i, _i, C.c_uint64, _d, _P(_i)],
     "b200la_batch_get_system": [_vp, _i, _vp, _vp, _vp, _vp],

@@ -32,9 +32,9 @@ class SystemResult:
     x: np.ndarray | None = None
 
 
-def slot_bytes(n: int, nnz: int, mixed: bool) -> int:
+def slot_bytes(n: int, nnz: int, max_row: int, mixed: bool) -> int:
     out = C.c_int64()
-    call("b200la_batch_slot_bytes", int(n), int(nnz), 1 if mixed else 0, C.byref(out))
+    call("b200la_batch_slot_bytes", int(n), int(nnz), int(max_row), 1 if mixed else 0, C.byref(out))
     return out.value
 
 
@@ -117,6 +117,14 @@ class Batch:
 
     def slot_n(self, slot: int) -> int:
         return self._sizes[slot]
+
+    def solve(self, chunk_passes: int = 32) -> int:
+        """Run until every system has finished, compacting the tile list every
+        chunk_passes passes; returns the passes taken."""
+        n = C.c_int()
+        call("b200la_batch_solve", self.handle, int(chunk_passes), C.byref(n))
+        self._keep.clear()
+        return n.value
 
     def last_passes(self) -> int:
         """Device-loop passes taken by the last run (each pass = 4 kernel launches)."""

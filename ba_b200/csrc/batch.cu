@@ -1,30 +1,39 @@
 // Batched and served PCG: many independent systems of uneven size solved by
-// one CUDA-graph launch whose body kernels sweep all active systems at once.
+// one CUDA-graph launch whose body kernels sweep all running systems at once.
 //
-// The reference solves one system per CG<LAD> call; there is no batched
-// path (SURVEY: batching/serving has no reference counterpart).  Each system
-// follows the reference's recurrence (Jacobi-PCG, cg.h:165-246) inside an
-// MPIR-style refinement (mpir.cc:52-230): FP64 residual/update/test around an
+// The reference solves one system per CG<LAD> call; it has no batched path.
+// Each system here follows the reference's recurrence (Jacobi-PCG,
+// linear_solver/cg.h:165-246) inside an MPIR-style refinement
+// (linear_solver/mpir.cc:52-230): FP64 residual, update and test around an
 // FP32 inner solve, or, in FP64 mode, a plain FP64 (P)CG.
 //
-// Work decomposition: every system is cut into tiles of consecutive rows;
-// a thread block handles one tile at a time (grid-stride over the tile
-// list), so big and small systems share every launch and the load balances
-// at tile granularity.  Per-system dot products are reduced deterministically:
-// each tile writes its partial sums, and the last tile of a system to finish
-// (per-system atomic ticket) adds that system's partials in tile order.
+// Work decomposition: every system is cut into tiles of consecutive rows (a
+// multiple of 32); a thread block handles one tile at a time (grid-stride
+// over the tile list), so large and small systems share every launch and the
+// load balances at tile granularity.  Per-system dot products are reduced
+// deterministically: each tile writes its partial sums, and the last tile of
+// the system to finish (per-system atomic ticket) adds the system's partials
+// in tile order.  A system's arithmetic therefore does not depend on what
+// else is in the batch.
+//
+// Matrices are stored twice: CSR as uploaded (host-facing, setup), and a
+// sliced ELL copy used by both SpMVs: slices of 32 rows, every row padded to
+// the system's longest row `ell`; entry k of row 32s+l sits at
+// (s*ell + k)*32 + l, so a warp reads 32 consecutive values per step and the
+// loads of one row do not depend on a row pointer.
 //
 // Each system walks through phases, advanced by the last tile of the kernel
-// that finishes a phase, so all tiles of a system see one phase per launch:
-//   RESID   K4: r64 = b - A64 x (FP64), ||r64||, outer test; restart the
-//               inner solve from c = 0 with r = (float)r64, z = invD r, p = z
-//   INNER   K1: Ap = A p, p.Ap      K2: c += a p, r -= a Ap, r.r, r.z, inner
-//               test -> CORRECT      K3: p = b p + z
+// that ends a phase, so all tiles of a system see one phase per launch:
+//   RESID   K1: r64 = b - A64 x (FP64), ||r64||, outer test; restart the inner
+//               solve from c = 0 with r = (T)r64, z = invD r, p = z -> START
+//   START   K3: opens the inner solve (-> INNER) once every tile saw START
+//   INNER   K1: Ap = A p, p.Ap   K2: c += a p, r -= a Ap, r.r, r.z, inner test
+//               (-> CORRECT)     K3: p = b p + z
 //   CORRECT K3: x += (double)c -> RESID (mixed) or DONE (FP64 mode)
 //   DONE    skipped by every kernel
-// The body of the graph's WHILE node is K1 K2 K3 K4; the last block of K4
-// clears the loop condition when no system is active or the pass budget is
-// spent, so the device loop always ends.
+// One pass of the device loop is K1 K2 K3; the last block of K3 ends the
+// pass and clears the graph's WHILE condition when no system is running or
+// the pass budget is spent, so the device loop always ends.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -34,17 +43,19 @@
 
 namespace b200la {
 
-enum BatchPhase : int { PH_EMPTY = 0, PH_RESID = 1, PH_INNER = 2, PH_CORRECT = 3, PH_DONE = 4 };
+enum BatchPhase : int { PH_EMPTY = 0, PH_RESID = 1, PH_INNER = 2, PH_CORRECT = 3, PH_DONE = 4, PH_START = 5 };
 
-// Device descriptor of one system slot.  Structure (rowptr, col) is shared by
-// the FP64 and FP32 values; vectors are the slot's own buffers.
+// Device descriptor of one system slot.
 template <typename T> struct SysDesc {
   int n;
   int nnz;
-  const int *rowptr;
+  const int *rowptr;  // CSR as uploaded
   const int *col;
   const double *val64;
-  const T *val;       // inner-solve values (FP32 copy, or val64 in FP64 mode)
+  int ell;            // sliced ELL width (longest row)
+  const int *scol;    // sliced ELL columns
+  const T *sval;      // sliced ELL values in the inner type
+  const double *sval64;  // sliced ELL values in FP64 (== sval in FP64 mode)
   const double *b;
   double *x;
   T *c, *r, *p, *Ap;
@@ -58,8 +69,8 @@ struct SysState {
   int total_iter;      // inner iterations over all passes
   int outer;           // refinement passes started
   double rz, pAp, alpha, beta;
-  double res_in, res_in0;   // inner recurrence residual and its start value
-  double res, res0;         // FP64 true residual and the initial one
+  double res_in, res_in0;      // inner recurrence residual and its start value
+  double res, res0;            // FP64 true residual and the initial one
   unsigned long long t_begin;  // %globaltimer at the system's first residual
   unsigned long long t_done;   // %globaltimer when the system finished
   int state;                   // B200LA_* iterate state at the end
@@ -78,17 +89,17 @@ struct BatchParams {
 
 struct BatchGlobals {
   int active;          // systems not DONE (and not EMPTY)
-  int passes;          // body passes taken by this launch
+  int passes;          // passes taken by this launch
   int max_passes;      // pass budget of this launch
   int ntiles;          // tiles in the current tile list
-  unsigned ticket;     // last block of K4
-  unsigned pad2;
+  unsigned ticket;     // last block of K3
+  unsigned pad;
   unsigned long long t_start;
 };
 
 struct Tile {
   int sys;
-  int row0;
+  int row0;   // a multiple of 32
   int rows;
   int first;  // index of the system's first tile (its partials start there)
   int count;  // tiles of the system
@@ -138,10 +149,6 @@ __device__ __forceinline__ int outer_check(double res, double res0, const BatchP
   return B200LA_ITERATE;
 }
 
-}  // namespace b200la
-
-namespace b200la {
-
 __device__ __forceinline__ int load_phase(const SysState *s) { return *(volatile const int *)&s->phase; }
 
 __device__ __forceinline__ void finish_system(SysState &S, BatchGlobals *g, int state) {
@@ -151,25 +158,100 @@ __device__ __forceinline__ void finish_system(SysState &S, BatchGlobals *g, int 
   atomicSub(&g->active, 1);
 }
 
-// ---- K1: Ap = A p and p.Ap for INNER systems -------------------------------
-template <typename T, int G>
-__global__ void __launch_bounds__(kBlock) batch_spmv_kernel(const Tile *__restrict__ tiles,
-                                                            const SysDesc<T> *__restrict__ desc, SysState *st,
-                                                            double *part, int64_t part_stride, BatchGlobals *g,
-                                                            BatchParams prm) {
+// One row of y = A x per lane from the sliced ELL layout (V = value type of
+// the stored values, X = type of x).
+template <typename V, typename X>
+__device__ __forceinline__ V sell_row(const int *__restrict__ scol, const V *__restrict__ sval, int ell,
+                                      const X *__restrict__ x, int slice, int lane) {
+  const int64_t base = (int64_t)slice * ell * 32 + lane;
+  const int *cp = scol + base;
+  const V *vp = sval + base;
+  V sum = V(0);
+#pragma unroll 9
+  for (int k = 0; k < ell; ++k) sum = fma(ld_stream(vp + k * 32), (V)ld_keep(x + ld_stream(cp + k * 32)), sum);
+  return sum;
+}
+
+}  // namespace b200la
+
+namespace b200la {
+
+// ---- RESID tiles (run by K1): FP64 residual, outer test, inner restart ------
+// r64 = b - A64 x with the FP64 sliced-ELL values, ||r64||, then the inner
+// solve restarts from c = 0 with r = (T)r64, z = invD r, p = z.  The
+// system's last tile applies the outer test: DONE, or START.
+template <typename T, bool PRE>
+__device__ __forceinline__ void resid_tile(const Tile &tl, int t, const SysDesc<T> &d, SysState &S, double *part,
+                                           int64_t part_stride, BatchGlobals *g, const BatchParams &prm) {
+  Acc<double> rr64;
+  Acc<T> rrin, rzin;
+  const int lane = threadIdx.x & 31;
+  const int nsl = (tl.rows + 31) >> 5;
+  for (int sl = (int)threadIdx.x >> 5; sl < nsl; sl += kBlock / 32) {
+    const int slice = (tl.row0 >> 5) + sl;
+    const double y = sell_row<double, double>(d.scol, d.sval64, d.ell, d.x, slice, lane);
+    const int row = slice * 32 + lane;
+    if (row < tl.row0 + tl.rows) {
+      const double r64 = d.b[row] - y;
+      rr64.add(r64 * r64);
+      const T r = (T)r64;
+      d.r[row] = r;
+      d.c[row] = T(0);
+      const T z = PRE ? r * d.invd[row] : r;
+      d.p[row] = z;
+      rrin.add(r * r);
+      rzin.add(r * z);
+    }
+  }
+  double v[3] = {rr64.value(), rrin.value(), rzin.value()};
+  if (tile_sum_last<3>(v, part, part_stride, t, tl.first, tl.count, &S.ticket[3]) && threadIdx.x == 0) {
+    const double res = sqrt(v[0]);
+    S.res = res;
+    if (S.outer == 0) {
+      S.res0 = res;
+      S.t_begin = globaltimer();
+    }
+    int s = outer_check(res, S.res0, prm);
+    if (s == B200LA_ITERATE && S.outer >= prm.max_outer) s = B200LA_FAIL_MAXITS;
+    if (prm.precond && S.bad_row != 0xffffffffu) s = B200LA_FAIL_BREAKDOWN;  // Jacobi needs every diagonal
+    if (s != B200LA_ITERATE) {
+      finish_system(S, g, s);
+    } else {
+      S.outer += 1;
+      S.inner_iter = 0;
+      S.res_in = S.res_in0 = sqrt(v[1]);
+      S.rz = PRE ? v[2] : v[1];
+      S.phase = PH_START;
+    }
+  }
+}
+
+// ---- K1: Ap = A p and p.Ap for INNER systems; RESID systems ------------------
+template <typename T, bool PRE>
+__global__ void __launch_bounds__(kBlock, 6) batch_spmv_kernel(const Tile *__restrict__ tiles,
+                                                               const SysDesc<T> *__restrict__ desc, SysState *st,
+                                                               double *part, int64_t part_stride, BatchGlobals *g,
+                                                               BatchParams prm) {
   const int ntiles = g->ntiles;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const Tile tl = tiles[t];
     SysState &S = st[tl.sys];
-    if (load_phase(&S) != PH_INNER) continue;
+    const int ph = load_phase(&S);
+    if (ph != PH_INNER && ph != PH_RESID) continue;
     const SysDesc<T> d = desc[tl.sys];
+    if (ph == PH_RESID) {
+      resid_tile<T, PRE>(tl, t, d, S, part, part_stride, g, prm);
+      __syncthreads();
+      continue;
+    }
     Acc<T> acc;
-    for (int base = 0; base < tl.rows; base += kBlock / G) {
-      const int lr = base + (int)threadIdx.x / G;
-      const bool valid = lr < tl.rows;
-      const int row = tl.row0 + lr;
-      T y = csr_row_group<T, G>(d.rowptr, d.col, d.val, d.p, row, valid);
-      if (valid && (threadIdx.x & (G - 1)) == 0) {
+    const int nsl = (tl.rows + 31) >> 5;
+    for (int sl = warp; sl < nsl; sl += kBlock / 32) {
+      const int slice = (tl.row0 >> 5) + sl;
+      const T y = sell_row<T, T>(d.scol, d.sval, d.ell, d.p, slice, lane);
+      const int row = slice * 32 + lane;
+      if (row < tl.row0 + tl.rows) {
         d.Ap[row] = y;
         acc.add(y * d.p[row]);
       }
@@ -192,10 +274,10 @@ __global__ void __launch_bounds__(kBlock) batch_spmv_kernel(const Tile *__restri
 
 // ---- K2: c += alpha p, r -= alpha Ap, r.r and r.z; inner test ---------------
 template <typename T, bool PRE>
-__global__ void __launch_bounds__(kBlock) batch_update_kernel(const Tile *__restrict__ tiles,
-                                                              const SysDesc<T> *__restrict__ desc, SysState *st,
-                                                              double *part, int64_t part_stride, BatchGlobals *g,
-                                                              BatchParams prm) {
+__global__ void __launch_bounds__(kBlock, 6) batch_update_kernel(const Tile *__restrict__ tiles,
+                                                                 const SysDesc<T> *__restrict__ desc, SysState *st,
+                                                                 double *part, int64_t part_stride, BatchGlobals *g,
+                                                                 BatchParams prm) {
   const int ntiles = g->ntiles;
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const Tile tl = tiles[t];
@@ -204,7 +286,35 @@ __global__ void __launch_bounds__(kBlock) batch_update_kernel(const Tile *__rest
     const SysDesc<T> d = desc[tl.sys];
     const T alpha = (T)S.alpha;
     Acc<T> rr, rz;
-    for (int i = tl.row0 + threadIdx.x; i < tl.row0 + tl.rows; i += kBlock) {
+    // 16-byte vectors over the tile (tile starts are multiples of 32 rows and
+    // every slot vector is 256-byte aligned), then the ragged tail
+    using V = typename Vec16<T>::type;
+    constexpr int W = Vec16<T>::n;
+    const int nv = tl.rows / W;
+    for (int q = threadIdx.x; q < nv; q += kBlock) {
+      const int i = tl.row0 + q * W;
+      V cv = *reinterpret_cast<const V *>(d.c + i);
+      V rv = *reinterpret_cast<const V *>(d.r + i);
+      const V pv = *reinterpret_cast<const V *>(d.p + i);
+      const V av = *reinterpret_cast<const V *>(d.Ap + i);
+      V dv;
+      if (PRE) dv = *reinterpret_cast<const V *>(d.invd + i);
+      T *cs = reinterpret_cast<T *>(&cv);
+      T *rs = reinterpret_cast<T *>(&rv);
+      const T *ps = reinterpret_cast<const T *>(&pv);
+      const T *as = reinterpret_cast<const T *>(&av);
+      const T *ds = reinterpret_cast<const T *>(&dv);
+#pragma unroll
+      for (int k = 0; k < W; ++k) {
+        cs[k] = fma(alpha, ps[k], cs[k]);
+        rs[k] = fma(-alpha, as[k], rs[k]);
+        rr.add(rs[k] * rs[k]);
+        if (PRE) rz.add(rs[k] * (rs[k] * ds[k]));
+      }
+      *reinterpret_cast<V *>(d.c + i) = cv;
+      *reinterpret_cast<V *>(d.r + i) = rv;
+    }
+    for (int i = tl.row0 + nv * W + threadIdx.x; i < tl.row0 + tl.rows; i += kBlock) {
       d.c[i] = fma(alpha, d.p[i], d.c[i]);
       const T r = fma(-alpha, d.Ap[i], d.r[i]);
       d.r[i] = r;
@@ -219,8 +329,9 @@ __global__ void __launch_bounds__(kBlock) batch_update_kernel(const Tile *__rest
       S.inner_iter += 1;
       S.total_iter += 1;
       if (prm.mixed) {
-        // inner solve: stop at inner_rtol (strict, as IterateControl) or its iteration budget
-        // (no tighter than half the outer target: the last pass does not over-solve)
+        // inner solve: stop at inner_rtol (strict, as IterateControl), no
+        // tighter than half the outer target (the last pass does not
+        // over-solve), or at its iteration budget
         const double target = fmax(prm.inner_rtol * S.res_in0, 0.5 * prm.rtol * S.res0);
         if (res < target || S.inner_iter >= prm.inner_maxits || !(res == res)) S.phase = PH_CORRECT;
       } else {
@@ -243,12 +354,12 @@ __global__ void __launch_bounds__(kBlock) batch_update_kernel(const Tile *__rest
   }
 }
 
-// ---- K3: p = beta p + z (INNER); x += c (CORRECT) ---------------------------
-template <typename T, bool PRE>
-__global__ void __launch_bounds__(kBlock) batch_direction_kernel(const Tile *__restrict__ tiles,
-                                                                 const SysDesc<T> *__restrict__ desc, SysState *st,
-                                                                 double *part, int64_t part_stride, BatchGlobals *g,
-                                                                 BatchParams prm) {
+// ---- K3: p = beta p + z (INNER); x += c (CORRECT); START -> INNER; end of pass
+template <typename T, bool PRE, bool IN_GRAPH = true>
+__global__ void __launch_bounds__(kBlock, 8) batch_direction_kernel(const Tile *__restrict__ tiles,
+                                                                    const SysDesc<T> *__restrict__ desc, SysState *st,
+                                                                    double *part, int64_t part_stride, BatchGlobals *g,
+                                                                    BatchParams prm, cudaGraphConditionalHandle loop) {
   const int ntiles = g->ntiles;
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const Tile tl = tiles[t];
@@ -257,7 +368,23 @@ __global__ void __launch_bounds__(kBlock) batch_direction_kernel(const Tile *__r
     if (ph == PH_INNER) {
       const SysDesc<T> d = desc[tl.sys];
       const T beta = (T)S.beta;
-      for (int i = tl.row0 + threadIdx.x; i < tl.row0 + tl.rows; i += kBlock)
+      using V = typename Vec16<T>::type;
+      constexpr int W = Vec16<T>::n;
+      const int nv = tl.rows / W;
+      for (int q = threadIdx.x; q < nv; q += kBlock) {
+        const int i = tl.row0 + q * W;
+        V pv = *reinterpret_cast<const V *>(d.p + i);
+        const V rv = *reinterpret_cast<const V *>(d.r + i);
+        V dv;
+        if (PRE) dv = *reinterpret_cast<const V *>(d.invd + i);
+        T *ps = reinterpret_cast<T *>(&pv);
+        const T *rs = reinterpret_cast<const T *>(&rv);
+        const T *ds = reinterpret_cast<const T *>(&dv);
+#pragma unroll
+        for (int k = 0; k < W; ++k) ps[k] = fma(beta, ps[k], PRE ? rs[k] * ds[k] : rs[k]);
+        *reinterpret_cast<V *>(d.p + i) = pv;
+      }
+      for (int i = tl.row0 + nv * W + threadIdx.x; i < tl.row0 + tl.rows; i += kBlock)
         d.p[i] = fma(beta, d.p[i], PRE ? d.r[i] * d.invd[i] : d.r[i]);
     } else if (ph == PH_CORRECT) {
       const SysDesc<T> d = desc[tl.sys];
@@ -267,62 +394,12 @@ __global__ void __launch_bounds__(kBlock) batch_direction_kernel(const Tile *__r
         if (prm.mixed) S.phase = PH_RESID;
         else finish_system(S, g, S.state);
       }
-    }
-    __syncthreads();
-  }
-}
-
-// ---- K4: FP64 residual, outer test, inner restart ----------------------------
-template <typename T, int G, bool PRE>
-__global__ void __launch_bounds__(kBlock) batch_residual_kernel(const Tile *__restrict__ tiles,
-                                                                const SysDesc<T> *__restrict__ desc, SysState *st,
-                                                                double *part, int64_t part_stride, BatchGlobals *g,
-                                                                BatchParams prm, cudaGraphConditionalHandle loop) {
-  const int ntiles = g->ntiles;
-  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const Tile tl = tiles[t];
-    SysState &S = st[tl.sys];
-    if (load_phase(&S) != PH_RESID) continue;
-    const SysDesc<T> d = desc[tl.sys];
-    Acc<double> rr64;
-    Acc<T> rrin, rzin;
-    for (int base = 0; base < tl.rows; base += kBlock / G) {
-      const int lr = base + (int)threadIdx.x / G;
-      const bool valid = lr < tl.rows;
-      const int row = tl.row0 + lr;
-      double y = csr_row_group<double, G>(d.rowptr, d.col, d.val64, d.x, row, valid);
-      if (valid && (threadIdx.x & (G - 1)) == 0) {
-        const double r64 = d.b[row] - y;
-        rr64.add(r64 * r64);
-        const T r = (T)r64;
-        d.r[row] = r;
-        d.c[row] = T(0);
-        const T z = PRE ? r * d.invd[row] : r;
-        d.p[row] = z;
-        rrin.add(r * r);
-        rzin.add(r * z);
-      }
-    }
-    double v[3] = {rr64.value(), rrin.value(), rzin.value()};
-    if (tile_sum_last<3>(v, part, part_stride, t, tl.first, tl.count, &S.ticket[3]) && threadIdx.x == 0) {
-      const double res = sqrt(v[0]);
-      S.res = res;
-      if (S.outer == 0) {
-        S.res0 = res;
-        S.t_begin = globaltimer();
-      }
-      int s = outer_check(res, S.res0, prm);
-      if (s == B200LA_ITERATE && S.outer >= prm.max_outer) s = B200LA_FAIL_MAXITS;
-      if (prm.precond && S.bad_row != 0xffffffffu) s = B200LA_FAIL_BREAKDOWN;  // Jacobi needs every diagonal
-      if (s != B200LA_ITERATE) {
-        finish_system(S, g, s);
-      } else {
-        S.outer += 1;
-        S.inner_iter = 0;
-        S.res_in = S.res_in0 = sqrt(v[1]);
-        S.rz = PRE ? v[2] : v[1];
+    } else if (ph == PH_START) {
+      // K1 wrote the restart; open the inner solve once every tile of the
+      // system has passed this point
+      double v[1] = {0.0};
+      if (tile_sum_last<1>(v, part, part_stride, t, tl.first, tl.count, &S.ticket[2]) && threadIdx.x == 0)
         S.phase = PH_INNER;
-      }
     }
     __syncthreads();
   }
@@ -339,7 +416,7 @@ __global__ void __launch_bounds__(kBlock) batch_residual_kernel(const Tile *__re
     const int passes = g->passes + 1;
     g->passes = passes;
     const int active = *(volatile int *)&g->active;
-    cudaGraphSetConditional(loop, (active > 0 && passes < g->max_passes) ? 1u : 0u);
+    if (IN_GRAPH) cudaGraphSetConditional(loop, (active > 0 && passes < g->max_passes) ? 1u : 0u);
   }
 }
 
@@ -349,76 +426,29 @@ __global__ void batch_start_kernel(BatchGlobals *g) {
   g->t_start = globaltimer();
 }
 
-}  // namespace b200la
-
-using namespace b200la;
-
-namespace {
-
-// Host record of one slot.
-struct HostSys {
-  bool used = false;
-  int n = 0;
-  int nnz = 0;
-  void *chunk = nullptr;   // one allocation holds all of the slot's buffers
-  size_t bytes = 0;
-  SysDesc<double> d64{};
-  SysDesc<float> d32{};
-};
-
-size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
-
-}  // namespace
-
-struct b200la_batch_s {
-  b200la_ctx ctx;
-  b200la_batch_params prm;
-  BatchParams kp;
-  int lanes;
-  int tile_rows;
-  int capacity;
-  int64_t max_tiles;
-  std::vector<HostSys> sys;
-  // device
-  void *desc;            // SysDesc<T>[capacity]
-  SysState *st;          // [capacity]
-  Tile *tiles;           // [max_tiles]
-  double *part;          // [3][max_tiles]
-  BatchGlobals *glob;
-  // host mirrors
-  SysState *st_host;     // pinned [capacity]
-  BatchGlobals *glob_host;
-  std::vector<Tile> tiles_host;
-  int64_t device_bytes;
-  bool tiles_dirty;
-  cudaGraph_t graph;
-  cudaGraphExec_t exec;
-  int grid;
-};
-
-namespace {
-
-template <typename T> SysDesc<T> &desc_of(HostSys &h);
-template <> SysDesc<double> &desc_of<double>(HostSys &h) { return h.d64; }
-template <> SysDesc<float> &desc_of<float>(HostSys &h) { return h.d32; }
-
-// Bytes one slot needs for a system (the admission test of the request loop).
-size_t slot_bytes(int64_t n, int64_t nnz, bool mixed) {
-  size_t tb = mixed ? 4 : 8;
-  size_t b = align256(sizeof(int) * (n + 1)) + align256(sizeof(int) * nnz) + align256(8 * nnz);
-  if (mixed) b += align256(4 * nnz);
-  b += 2 * align256(8 * n);      // b, x
-  b += 5 * align256(tb * n);     // c, r, p, Ap, invd
-  return b;
-}
-
+// Slot set-up after the CSR arrived: sliced-ELL copies (inner type and
+// FP64), the inverse diagonal in the inner type, zero work vectors.
 template <typename T>
 __global__ void slot_setup_kernel(SysDesc<T> d, unsigned *bad) {
-  // FP32 values (mixed mode), inverse diagonal in the inner type, x = 0 if
-  // requested by the caller (done on the host side), zero work vectors.
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < d.nnz; j += stride)
-    if ((const void *)d.val != (const void *)d.val64) const_cast<T *>(d.val)[j] = (T)d.val64[j];
+  const int64_t padded_rows = (int64_t)(d.n + 31) / 32 * 32;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < padded_rows; i += stride) {
+    int start = 0, len = 0, pad = 0;
+    if (i < d.n) {
+      start = d.rowptr[i];
+      len = d.rowptr[i + 1] - start;
+      pad = len > 0 ? d.col[start + len - 1] : (int)i;
+    }
+    const int64_t base = (i >> 5) * (int64_t)d.ell * 32 + (i & 31);
+    for (int k = 0; k < d.ell; ++k) {
+      const bool real = k < len;
+      const int64_t pos = base + (int64_t)k * 32;
+      const_cast<int *>(d.scol)[pos] = real ? d.col[start + k] : pad;
+      const_cast<T *>(d.sval)[pos] = real ? (T)d.val64[start + k] : T(0);
+      if ((const void *)d.sval64 != (const void *)d.sval)
+        const_cast<double *>(d.sval64)[pos] = real ? d.val64[start + k] : 0.0;
+    }
+  }
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < d.n; i += stride) {
     int k = -1;
     for (int j = d.rowptr[i]; j < d.rowptr[i + 1]; ++j)
@@ -437,43 +467,210 @@ __global__ void slot_setup_kernel(SysDesc<T> d, unsigned *bad) {
   }
 }
 
-// Plain batched SpMV Ap = A p over every tile (schedule timing only).
-template <typename T, int G>
-__global__ void __launch_bounds__(kBlock) batch_spmv_plain_kernel(const Tile *__restrict__ tiles, int ntiles,
-                                                                  const SysDesc<T> *__restrict__ desc) {
+// Plain batched SpMV Ap = A p over every tile (timing only).
+template <typename T>
+__global__ void __launch_bounds__(kBlock, 8) batch_spmv_plain_kernel(const Tile *__restrict__ tiles, int ntiles,
+                                                                     const SysDesc<T> *__restrict__ desc) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const Tile tl = tiles[t];
     const SysDesc<T> d = desc[tl.sys];
-    for (int base = 0; base < tl.rows; base += kBlock / G) {
-      const int lr = base + (int)threadIdx.x / G;
-      const bool valid = lr < tl.rows;
-      const int row = tl.row0 + lr;
-      T y = csr_row_group<T, G>(d.rowptr, d.col, d.val, d.p, row, valid);
-      if (valid && (threadIdx.x & (G - 1)) == 0) d.Ap[row] = y;
+    const int nsl = (tl.rows + 31) >> 5;
+    for (int sl = warp; sl < nsl; sl += kBlock / 32) {
+      const int slice = (tl.row0 >> 5) + sl;
+      const T y = sell_row<T, T>(d.scol, d.sval, d.ell, d.p, slice, lane);
+      const int row = slice * 32 + lane;
+      if (row < tl.row0 + tl.rows) d.Ap[row] = y;
     }
   }
 }
 
+// Restart every listed slot from x = 0: RESID phase, counters cleared.
+template <typename T>
+__global__ void __launch_bounds__(kBlock) batch_restart_kernel(const int *__restrict__ slots,
+                                                               const SysDesc<T> *__restrict__ desc, SysState *st) {
+  const int s = slots[blockIdx.x];
+  const SysDesc<T> d = desc[s];
+  for (int i = threadIdx.x; i < d.n; i += kBlock) d.x[i] = 0.0;
+  if (threadIdx.x == 0) {
+    SysState &S = st[s];
+    const unsigned bad = S.bad_row;
+    S = SysState{};
+    S.phase = PH_RESID;
+    S.bad_row = bad;
+  }
+}
+
+}  // namespace b200la
+
+using namespace b200la;
+
+namespace {
+
+// Host record of one slot.
+struct HostSys {
+  bool used = false;
+  int n = 0;
+  int nnz = 0;
+  void *chunk = nullptr;  // one allocation holds all of the slot's buffers
+  size_t bytes = 0;
+  SysDesc<double> d64{};
+  SysDesc<float> d32{};
+};
+
+size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
+
 }  // namespace
+
+struct b200la_batch_s {
+  b200la_ctx ctx;
+  b200la_batch_params prm;
+  BatchParams kp;
+  int tile_rows;
+  int capacity;
+  int64_t max_tiles;
+  std::vector<HostSys> sys;
+  // device
+  void *desc;         // SysDesc<T>[capacity]
+  SysState *st;       // [capacity]
+  Tile *tiles;        // [max_tiles]
+  double *part;       // [3][max_tiles]
+  BatchGlobals *glob;
+  // host mirrors
+  SysState *st_host;  // pinned [capacity]
+  BatchGlobals *glob_host;
+  std::vector<Tile> tiles_host;
+  int64_t device_bytes;
+  cudaGraph_t graph;
+  cudaGraphExec_t exec;
+};
 
 namespace {
 
 using BatchHandle = b200la_batch;
 
-template <typename T, int G, bool PRE>
-int build_graph_t(BatchHandle B) {
+template <typename T> SysDesc<T> &desc_of(HostSys &h);
+template <> SysDesc<double> &desc_of<double>(HostSys &h) { return h.d64; }
+template <> SysDesc<float> &desc_of<float>(HostSys &h) { return h.d32; }
+
+// Bytes one slot needs for a system (the admission test of the request loop).
+size_t slot_bytes(int64_t n, int64_t nnz, int64_t ell, bool mixed) {
+  const size_t tb = mixed ? 4 : 8;
+  const size_t padded = (size_t)((n + 31) / 32) * 32 * (size_t)ell;
+  size_t b = align256(sizeof(int) * (n + 1)) + align256(sizeof(int) * nnz) + align256(8 * nnz);
+  b += align256(4 * padded) + align256(tb * padded);  // sliced-ELL columns and values
+  if (mixed) b += align256(8 * padded);               // and the FP64 values for the residual
+  b += 2 * align256(8 * n);                            // b, x
+  b += 5 * align256(tb * n);                           // c, r, p, Ap, invd
+  return b;
+}
+
+// Allocates a slot's buffers (one chunk) and carves them into a descriptor.
+template <typename T>
+int alloc_slot(BatchHandle B, int slot, int n, int64_t nnz, int ell, SysDesc<T> *out) {
+  HostSys &h = B->sys[slot];
+  cudaStream_t st = B->ctx->stream;
+  const bool mixed = B->kp.mixed != 0;
+  h.bytes = slot_bytes(n, nnz, ell, mixed);
+  B_CUDA(cudaMallocAsync(&h.chunk, h.bytes, st));
+  char *p = (char *)h.chunk;
+  auto take = [&](size_t bytes) { char *q = p; p += align256(bytes); return (void *)q; };
+  SysDesc<T> d{};
+  d.n = n;
+  d.nnz = (int)nnz;
+  d.rowptr = (const int *)take(sizeof(int) * (n + 1));
+  d.col = (const int *)take(sizeof(int) * nnz);
+  d.val64 = (const double *)take(8 * nnz);
+  const size_t padded = (size_t)((n + 31) / 32) * 32 * (size_t)ell;
+  d.ell = ell;
+  d.scol = (const int *)take(4 * padded);
+  d.sval = (const T *)take(sizeof(T) * padded);
+  d.sval64 = mixed ? (const double *)take(8 * padded) : (const double *)d.sval;
+  d.b = (const double *)take(8 * n);
+  d.x = (double *)take(8 * n);
+  d.c = (T *)take(sizeof(T) * n);
+  d.r = (T *)take(sizeof(T) * n);
+  d.p = (T *)take(sizeof(T) * n);
+  d.Ap = (T *)take(sizeof(T) * n);
+  d.invd = (const T *)take(sizeof(T) * n);
+  *out = d;
+  return B200LA_OK;
+}
+
+// Uploads the descriptor and a fresh RESID state, then builds the sliced-ELL
+// copies, the inverse diagonal and zero work vectors on the device.
+template <typename T>
+int finish_slot(BatchHandle B, int slot, const SysDesc<T> &d) {
+  HostSys &h = B->sys[slot];
+  cudaStream_t st = B->ctx->stream;
+  desc_of<T>(h) = d;
+  SysState &s0 = B->st_host[slot];
+  memset(&s0, 0, sizeof(SysState));
+  s0.phase = PH_RESID;
+  s0.bad_row = 0xffffffffu;
+  B_CUDA(cudaMemcpyAsync(B->st + slot, &s0, sizeof(SysState), cudaMemcpyHostToDevice, st));
+  B_CUDA(cudaMemcpyAsync((SysDesc<T> *)B->desc + slot, &desc_of<T>(h), sizeof(SysDesc<T>), cudaMemcpyHostToDevice,
+                         st));
+  const int64_t work = (int64_t)d.n + 32;
+  const int grid = (int)std::min<int64_t>(std::max<int64_t>((work + kBlock - 1) / kBlock, 1),
+                                          (int64_t)B->ctx->num_sms * 8);
+  slot_setup_kernel<T><<<grid, kBlock, 0, st>>>(d, &B->st[slot].bad_row);
+  B_CUDA(cudaGetLastError());
+  return B200LA_OK;
+}
+
+template <typename T>
+int add_typed(BatchHandle B, int slot, int n, int64_t nnz, int ell, const int *rowptr, const int *col,
+              const double *val, const double *b, const double *x0) {
+  cudaStream_t st = B->ctx->stream;
+  SysDesc<T> d{};
+  B_TRY(alloc_slot<T>(B, slot, n, nnz, ell, &d));
+  B_CUDA(cudaMemcpyAsync((void *)d.rowptr, rowptr, sizeof(int) * (n + 1), cudaMemcpyHostToDevice, st));
+  if (nnz) {
+    B_CUDA(cudaMemcpyAsync((void *)d.col, col, sizeof(int) * nnz, cudaMemcpyHostToDevice, st));
+    B_CUDA(cudaMemcpyAsync((void *)d.val64, val, 8 * nnz, cudaMemcpyHostToDevice, st));
+  }
+  B_CUDA(cudaMemcpyAsync((void *)d.b, b, 8 * n, cudaMemcpyHostToDevice, st));
+  if (x0) B_CUDA(cudaMemcpyAsync(d.x, x0, 8 * n, cudaMemcpyHostToDevice, st));
+  else B_CUDA(cudaMemsetAsync(d.x, 0, 8 * n, st));
+  return finish_slot<T>(B, slot, d);
+}
+
+int kernel_grid(b200la_ctx c, const void *k, int *grid) {
+  int o = 0;
+  B_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k, kBlock, 0));
+  *grid = c->num_sms * std::max(o, 1);
+  return B200LA_OK;
+}
+
+template <typename T, bool PRE, bool IN_GRAPH>
+int pass_grids(BatchHandle B, int g[3]) {
   b200la_ctx c = B->ctx;
+  B_TRY(kernel_grid(c, (const void *)batch_spmv_kernel<T, PRE>, &g[0]));
+  B_TRY(kernel_grid(c, (const void *)batch_update_kernel<T, PRE>, &g[1]));
+  B_TRY(kernel_grid(c, (const void *)batch_direction_kernel<T, PRE, IN_GRAPH>, &g[2]));
+  return B200LA_OK;
+}
+
+// One pass (K1 K2 K3) on stream st: captured into the graph body, or
+// launched from the host loop when graphs are off.
+template <typename T, bool PRE, bool IN_GRAPH>
+void launch_pass(BatchHandle B, const int g[3], cudaStream_t st, cudaGraphConditionalHandle h) {
+  const SysDesc<T> *desc = (const SysDesc<T> *)B->desc;
+  const int64_t ps = B->max_tiles;
+  batch_spmv_kernel<T, PRE><<<g[0], kBlock, 0, st>>>(B->tiles, desc, B->st, B->part, ps, B->glob, B->kp);
+  batch_update_kernel<T, PRE><<<g[1], kBlock, 0, st>>>(B->tiles, desc, B->st, B->part, ps, B->glob, B->kp);
+  batch_direction_kernel<T, PRE, IN_GRAPH><<<g[2], kBlock, 0, st>>>(B->tiles, desc, B->st, B->part, ps, B->glob,
+                                                                    B->kp, h);
+}
+
+// Graph: start kernel -> WHILE(pass).
+template <typename T, bool PRE>
+int build_graph_t(BatchHandle B) {
   if (B->exec) { cudaGraphExecDestroy(B->exec); B->exec = nullptr; }
   if (B->graph) { cudaGraphDestroy(B->graph); B->graph = nullptr; }
-  int occ = 1 << 30;
-  const void *ks[] = {(const void *)batch_spmv_kernel<T, G>, (const void *)batch_update_kernel<T, PRE>,
-                      (const void *)batch_direction_kernel<T, PRE>, (const void *)batch_residual_kernel<T, G, PRE>};
-  for (const void *k : ks) {
-    int o = 0;
-    B_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k, kBlock, 0));
-    occ = std::min(occ, std::max(o, 1));
-  }
-  B->grid = c->num_sms * occ;
+  int grids[3] = {1, 1, 1};
+  B_TRY((pass_grids<T, PRE, true>(B, grids)));
   cudaGraph_t g;
   B_CUDA(cudaGraphCreate(&g, 0));
   B->graph = g;
@@ -481,7 +678,6 @@ int build_graph_t(BatchHandle B) {
   B_CUDA(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
   cudaStream_t cs;
   B_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
-  // outer graph: start kernel -> WHILE(body)
   B_CUDA(cudaStreamBeginCaptureToGraph(cs, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
   batch_start_kernel<<<1, 1, 0, cs>>>(B->glob);
   cudaGraph_t cap;
@@ -503,13 +699,7 @@ int build_graph_t(BatchHandle B) {
   B_CUDA(cudaGraphAddNode(&wnode, g, nodes.data(), nn, &np));
   cudaGraph_t body = np.conditional.phGraph_out[0];
   B_CUDA(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-  const SysDesc<T> *desc = (const SysDesc<T> *)B->desc;
-  const int64_t ps = B->max_tiles;
-  batch_spmv_kernel<T, G><<<B->grid, kBlock, 0, cs>>>(B->tiles, desc, B->st, B->part, ps, B->glob, B->kp);
-  batch_update_kernel<T, PRE><<<B->grid, kBlock, 0, cs>>>(B->tiles, desc, B->st, B->part, ps, B->glob, B->kp);
-  batch_direction_kernel<T, PRE><<<B->grid, kBlock, 0, cs>>>(B->tiles, desc, B->st, B->part, ps, B->glob, B->kp);
-  batch_residual_kernel<T, G, PRE><<<B->grid, kBlock, 0, cs>>>(B->tiles, desc, B->st, B->part, ps, B->glob, B->kp,
-                                                                h);
+  launch_pass<T, PRE, true>(B, grids, cs, h);
   cudaError_t e2 = cudaStreamEndCapture(cs, &cap);
   cudaStreamDestroy(cs);
   B_CUDA(e2);
@@ -517,140 +707,123 @@ int build_graph_t(BatchHandle B) {
   return B200LA_OK;
 }
 
-template <typename T, bool PRE> int build_graph_g(BatchHandle B) {
-  switch (B->lanes) {
-    case 2: return build_graph_t<T, 2, PRE>(B);
-    case 4: return build_graph_t<T, 4, PRE>(B);
-    case 8: return build_graph_t<T, 8, PRE>(B);
-    case 16: return build_graph_t<T, 16, PRE>(B);
-    case 32: return build_graph_t<T, 32, PRE>(B);
-  }
-  return fail(B200LA_ERR_INVALID, "batch: lanes per row %d (2..32, power of two)", B->lanes);
-}
-
 int build_graph(BatchHandle B) {
   const bool pre = B->kp.precond != 0;
-  if (B->kp.mixed) return pre ? build_graph_g<float, true>(B) : build_graph_g<float, false>(B);
-  return pre ? build_graph_g<double, true>(B) : build_graph_g<double, false>(B);
+  if (B->kp.mixed) return pre ? build_graph_t<float, true>(B) : build_graph_t<float, false>(B);
+  return pre ? build_graph_t<double, true>(B) : build_graph_t<double, false>(B);
 }
 
-// Tile list of the systems that are still running, rebuilt before each launch.
-int rebuild_tiles(BatchHandle B, int *active) {
+// Host-loop mode (graphs off, B200LA_GRAPHS=0): the same kernels, with the
+// pass budget and the running count checked from the host every 8 passes.
+template <typename T, bool PRE>
+int host_loop_t(BatchHandle B) {
+  cudaStream_t st = B->ctx->stream;
+  int grids[3] = {1, 1, 1};
+  B_TRY((pass_grids<T, PRE, false>(B, grids)));
+  batch_start_kernel<<<1, 1, 0, st>>>(B->glob);
+  for (;;) {
+    for (int k = 0; k < 8; ++k) launch_pass<T, PRE, false>(B, grids, st, 0);
+    B_CUDA(cudaGetLastError());
+    B_CUDA(cudaMemcpyAsync(B->glob_host, B->glob, sizeof(BatchGlobals), cudaMemcpyDeviceToHost, st));
+    B_CUDA(cudaStreamSynchronize(st));
+    if (B->glob_host->active <= 0 || B->glob_host->passes >= B->glob_host->max_passes) break;
+  }
+  return B200LA_OK;
+}
+
+int host_loop(BatchHandle B) {
+  const bool pre = B->kp.precond != 0;
+  if (B->kp.mixed) return pre ? host_loop_t<float, true>(B) : host_loop_t<float, false>(B);
+  return pre ? host_loop_t<double, true>(B) : host_loop_t<double, false>(B);
+}
+
+// Grows the tile and partial arrays to hold nt tiles (the graph bakes their
+// addresses in, so it is rebuilt after a reallocation).
+int ensure_tiles(BatchHandle B, int64_t nt) {
+  if (nt <= B->max_tiles) return B200LA_OK;
+  cudaStream_t st = B->ctx->stream;
+  const int64_t cap = std::max<int64_t>(nt, 2 * B->max_tiles);
+  if (B->tiles) cudaFreeAsync(B->tiles, st);
+  if (B->part) cudaFreeAsync(B->part, st);
+  B->tiles = nullptr;
+  B->part = nullptr;
+  B_CUDA(cudaMallocAsync(&B->tiles, sizeof(Tile) * cap, st));
+  B_CUDA(cudaMallocAsync(&B->part, sizeof(double) * 3 * cap, st));
+  B->max_tiles = cap;
+  if (B->exec) {
+    cudaGraphExecDestroy(B->exec);
+    B->exec = nullptr;
+  }
+  return B200LA_OK;
+}
+
+// Tile list of the given slots (all used slots, or only those still running).
+int upload_tiles(BatchHandle B, bool running_only, int *count, int64_t *alg_bytes) {
   B->tiles_host.clear();
   int act = 0;
+  int64_t bytes = 0;
+  const int64_t vb = B->kp.mixed ? 4 : 8;
   for (int s = 0; s < B->capacity; ++s) {
     const HostSys &h = B->sys[s];
     if (!h.used) continue;
     const int ph = B->st_host[s].phase;
-    if (ph == PH_DONE || ph == PH_EMPTY) continue;
+    if (running_only && (ph == PH_DONE || ph == PH_EMPTY)) continue;
     ++act;
-    const int count = (h.n + B->tile_rows - 1) / B->tile_rows;
+    const int tiles = (h.n + B->tile_rows - 1) / B->tile_rows;
     const int first = (int)B->tiles_host.size();
-    for (int k = 0; k < count; ++k) {
+    for (int k = 0; k < tiles; ++k) {
       const int row0 = k * B->tile_rows;
-      B->tiles_host.push_back(Tile{s, row0, std::min(B->tile_rows, h.n - row0), first, count, 0});
+      B->tiles_host.push_back(Tile{s, row0, std::min(B->tile_rows, h.n - row0), first, tiles, 0});
     }
+    bytes += (int64_t)h.nnz * (vb + 4) + (int64_t)(h.n + 1) * 4 + 2 * (int64_t)h.n * vb;
   }
   const int64_t nt = (int64_t)B->tiles_host.size();
+  B_TRY(ensure_tiles(B, nt));
   cudaStream_t st = B->ctx->stream;
-  if (nt > B->max_tiles) {
-    int64_t cap = std::max<int64_t>(nt, 2 * B->max_tiles);
-    if (B->tiles) cudaFreeAsync(B->tiles, st);
-    if (B->part) cudaFreeAsync(B->part, st);
-    B->tiles = nullptr;
-    B->part = nullptr;
-    B_CUDA(cudaMallocAsync(&B->tiles, sizeof(Tile) * cap, st));
-    B_CUDA(cudaMallocAsync(&B->part, sizeof(double) * 3 * cap, st));
-    B->max_tiles = cap;
-    if (B->exec) {
-      cudaGraphExecDestroy(B->exec);
-      B->exec = nullptr;
-    }
-  }
   if (nt) B_CUDA(cudaMemcpyAsync(B->tiles, B->tiles_host.data(), sizeof(Tile) * nt, cudaMemcpyHostToDevice, st));
-  // the tile list's staging vector must outlive the copy
+  // the staging vector must outlive the copy
   B_CUDA(cudaStreamSynchronize(st));
-  *active = act;
+  *count = act;
+  if (alg_bytes) *alg_bytes = bytes;
   return B200LA_OK;
 }
 
-}  // namespace
-
-namespace {
-
-// Allocates a slot's buffers (one chunk) and carves them into a descriptor.
-template <typename T>
-int alloc_slot(b200la_batch B, int slot, int n, int64_t nnz, SysDesc<T> *out) {
-  HostSys &h = B->sys[slot];
-  cudaStream_t st = B->ctx->stream;
-  const bool mixed = B->kp.mixed != 0;
-  h.bytes = slot_bytes(n, nnz, mixed);
-  B_CUDA(cudaMallocAsync(&h.chunk, h.bytes, st));
-  char *p = (char *)h.chunk;
-  auto take = [&](size_t bytes) { char *q = p; p += align256(bytes); return (void *)q; };
-  SysDesc<T> d{};
-  d.n = n;
-  d.nnz = (int)nnz;
-  d.rowptr = (const int *)take(sizeof(int) * (n + 1));
-  d.col = (const int *)take(sizeof(int) * nnz);
-  d.val64 = (const double *)take(8 * nnz);
-  d.val = mixed ? (const T *)take(4 * nnz) : (const T *)d.val64;
-  d.b = (const double *)take(8 * n);
-  d.x = (double *)take(8 * n);
-  d.c = (T *)take(sizeof(T) * n);
-  d.r = (T *)take(sizeof(T) * n);
-  d.p = (T *)take(sizeof(T) * n);
-  d.Ap = (T *)take(sizeof(T) * n);
-  d.invd = (const T *)take(sizeof(T) * n);
-  *out = d;
-  return B200LA_OK;
+int find_free_slot(BatchHandle B) {
+  for (int s = 0; s < B->capacity; ++s)
+    if (!B->sys[s].used) return s;
+  return -1;
 }
 
-// Uploads the descriptor and a fresh RESID state, then builds the FP32
-// values, the inverse diagonal and zero work vectors on the device.
 template <typename T>
-int finish_slot(b200la_batch B, int slot, const SysDesc<T> &d) {
-  HostSys &h = B->sys[slot];
+int time_plain(BatchHandle B, int reps, float *ms) {
   cudaStream_t st = B->ctx->stream;
-  desc_of<T>(h) = d;
-  SysState &s0 = B->st_host[slot];
-  memset(&s0, 0, sizeof(SysState));
-  s0.phase = PH_RESID;
-  s0.bad_row = 0xffffffffu;
-  B_CUDA(cudaMemcpyAsync(B->st + slot, &s0, sizeof(SysState), cudaMemcpyHostToDevice, st));
-  B_CUDA(cudaMemcpyAsync((SysDesc<T> *)B->desc + slot, &desc_of<T>(h), sizeof(SysDesc<T>), cudaMemcpyHostToDevice, st));
-  const int64_t work = std::max<int64_t>(d.nnz, d.n);
-  const int grid = (int)std::min<int64_t>(std::max<int64_t>((work + kBlock - 1) / kBlock, 1),
-                                          (int64_t)B->ctx->num_sms * 8);
-  slot_setup_kernel<T><<<grid, kBlock, 0, st>>>(d, &B->st[slot].bad_row);
+  const int nt = (int)B->tiles_host.size();
+  int grid = 1;
+  B_TRY(kernel_grid(B->ctx, (const void *)batch_spmv_plain_kernel<T>, &grid));
+  const SysDesc<T> *desc = (const SysDesc<T> *)B->desc;
+  batch_spmv_plain_kernel<T><<<grid, kBlock, 0, st>>>(B->tiles, nt, desc);
+  cudaEvent_t e0, e1;
+  B_CUDA(cudaEventCreate(&e0));
+  B_CUDA(cudaEventCreate(&e1));
+  B_CUDA(cudaEventRecord(e0, st));
+  for (int r = 0; r < reps; ++r) batch_spmv_plain_kernel<T><<<grid, kBlock, 0, st>>>(B->tiles, nt, desc);
+  B_CUDA(cudaEventRecord(e1, st));
+  B_CUDA(cudaEventSynchronize(e1));
+  B_CUDA(cudaEventElapsedTime(ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
   B_CUDA(cudaGetLastError());
+  *ms /= reps;
   return B200LA_OK;
-}
-
-template <typename T>
-int add_typed(b200la_batch B, int slot, int n, int64_t nnz, const int *rowptr, const int *col,
-              const double *val, const double *b, const double *x0) {
-  cudaStream_t st = B->ctx->stream;
-  SysDesc<T> d{};
-  B_TRY(alloc_slot<T>(B, slot, n, nnz, &d));
-  B_CUDA(cudaMemcpyAsync((void *)d.rowptr, rowptr, sizeof(int) * (n + 1), cudaMemcpyHostToDevice, st));
-  if (nnz) {
-    B_CUDA(cudaMemcpyAsync((void *)d.col, col, sizeof(int) * nnz, cudaMemcpyHostToDevice, st));
-    B_CUDA(cudaMemcpyAsync((void *)d.val64, val, 8 * nnz, cudaMemcpyHostToDevice, st));
-  }
-  B_CUDA(cudaMemcpyAsync((void *)d.b, b, 8 * n, cudaMemcpyHostToDevice, st));
-  if (x0) B_CUDA(cudaMemcpyAsync(d.x, x0, 8 * n, cudaMemcpyHostToDevice, st));
-  else B_CUDA(cudaMemsetAsync(d.x, 0, 8 * n, st));
-  return finish_slot<T>(B, slot, d);
 }
 
 }  // namespace
 
 extern "C" {
 
-int b200la_batch_slot_bytes(int64_t n, int64_t nnz, int mixed, int64_t *bytes) {
-  B_CHECK(bytes && n >= 0 && nnz >= 0, B200LA_ERR_INVALID, "batch_slot_bytes: bad argument");
-  *bytes = (int64_t)slot_bytes(n, nnz, mixed != 0);
+int b200la_batch_slot_bytes(int64_t n, int64_t nnz, int max_row, int mixed, int64_t *bytes) {
+  B_CHECK(bytes && n >= 0 && nnz >= 0 && max_row >= 0, B200LA_ERR_INVALID, "batch_slot_bytes: bad argument");
+  *bytes = (int64_t)slot_bytes(n, nnz, std::max(max_row, 1), mixed != 0);
   return B200LA_OK;
 }
 
@@ -679,18 +852,14 @@ int b200la_batch_create(b200la_ctx ctx, const b200la_batch_params *p, b200la_bat
   B_CHECK(p->inner_maxits >= 1 && p->inner_maxits <= 10000000, B200LA_ERR_INVALID, "batch_create: inner_maxits");
   B_CHECK(p->atol >= 0 && p->rtol >= 0 && p->dtol > 0, B200LA_ERR_INVALID, "batch_create: tolerances");
   B_CHECK(!p->mixed || (p->inner_rtol > 0 && p->inner_rtol < 1), B200LA_ERR_INVALID, "batch_create: inner_rtol");
-  const int lanes = p->lanes ? p->lanes : 4;
-  B_CHECK(lanes == 2 || lanes == 4 || lanes == 8 || lanes == 16 || lanes == 32, B200LA_ERR_INVALID,
-          "batch_create: lanes %d", lanes);
-  B_CHECK(p->tile_rows == 0 || (p->tile_rows >= 32 && p->tile_rows <= 65536), B200LA_ERR_INVALID,
-          "batch_create: tile_rows %d", p->tile_rows);
+  B_CHECK(p->tile_rows == 0 || (p->tile_rows >= 32 && p->tile_rows <= 65536 && p->tile_rows % 32 == 0),
+          B200LA_ERR_INVALID, "batch_create: tile_rows %d (32..65536, multiple of 32)", p->tile_rows);
   b200la_batch B = new b200la_batch_s();
   B->ctx = ctx;
   B->prm = *p;
   B->kp = BatchParams{p->max_outer, p->inner_maxits, p->atol, p->rtol, p->dtol, p->inner_rtol, p->precond ? 1 : 0,
                       p->mixed ? 1 : 0};
-  B->lanes = lanes;
-  B->tile_rows = p->tile_rows ? p->tile_rows : 512;
+  B->tile_rows = p->tile_rows ? p->tile_rows : 2048;
   B->capacity = p->capacity;
   B->sys.resize(p->capacity);
   cudaStream_t st = ctx->stream;
@@ -702,6 +871,7 @@ int b200la_batch_create(b200la_ctx ctx, const b200la_batch_params *p, b200la_bat
             cudaMallocHost(&B->glob_host, sizeof(BatchGlobals)) == cudaSuccess;
   if (ok) {
     memset(B->st_host, 0, sizeof(SysState) * p->capacity);
+    memset(B->glob_host, 0, sizeof(BatchGlobals));
     ok = cudaMemsetAsync(B->st, 0, sizeof(SysState) * p->capacity, st) == cudaSuccess &&
          cudaMemsetAsync(B->glob, 0, sizeof(BatchGlobals), st) == cudaSuccess &&
          cudaStreamSynchronize(st) == cudaSuccess;
@@ -721,16 +891,15 @@ int b200la_batch_add(b200la_batch B, int n, int64_t nnz, const int *rowptr, cons
   int max_row = 0;
   B_TRY(validate_csr(n, n, nnz, rowptr, col, &max_row));
   B_CHECK(nnz == 0 || val, B200LA_ERR_MATRIX, "batch_add: val is NULL");
-  int slot = -1;
-  for (int s = 0; s < B->capacity; ++s)
-    if (!B->sys[s].used) { slot = s; break; }
+  const int slot = find_free_slot(B);
   B_CHECK(slot >= 0, B200LA_ERR_NOMEM, "batch_add: all %d slots are in use", B->capacity);
   HostSys &h = B->sys[slot];
   h = HostSys();
   h.n = n;
   h.nnz = (int)nnz;
-  const int rc = B->kp.mixed ? add_typed<float>(B, slot, n, nnz, rowptr, col, val, b, x0)
-                             : add_typed<double>(B, slot, n, nnz, rowptr, col, val, b, x0);
+  const int ell = std::max(max_row, 1);
+  const int rc = B->kp.mixed ? add_typed<float>(B, slot, n, nnz, ell, rowptr, col, val, b, x0)
+                             : add_typed<double>(B, slot, n, nnz, ell, rowptr, col, val, b, x0);
   if (rc != B200LA_OK) {
     if (h.chunk) cudaFreeAsync(h.chunk, B->ctx->stream);
     h = HostSys();
@@ -749,19 +918,18 @@ int b200la_batch_add_q1(b200la_batch B, int dim, int cells, uint64_t seed, doubl
   const int64_t n64 = q1_rows(dim, cells), nnz = q1_nnz(dim, cells);
   B_CHECK(nnz < (int64_t)INT32_MAX, B200LA_ERR_UNSUPPORTED, "batch_add_q1: nnz exceeds int32 indexing");
   const int n = (int)n64;
-  int slot = -1;
-  for (int s = 0; s < B->capacity; ++s)
-    if (!B->sys[s].used) { slot = s; break; }
+  const int slot = find_free_slot(B);
   B_CHECK(slot >= 0, B200LA_ERR_NOMEM, "batch_add_q1: all %d slots are in use", B->capacity);
   HostSys &h = B->sys[slot];
   h = HostSys();
   h.n = n;
   h.nnz = (int)nnz;
   cudaStream_t st = B->ctx->stream;
+  const int ell = cells >= 2 ? (dim == 2 ? 9 : 27) : (dim == 2 ? 4 : 8);
   auto go = [&](auto tag) -> int {
     using T = decltype(tag);
     SysDesc<T> d{};
-    B_TRY(alloc_slot<T>(B, slot, n, nnz, &d));
+    B_TRY(alloc_slot<T>(B, slot, n, nnz, ell, &d));
     B_TRY(q1_assemble(st, B->ctx->num_sms, dim, cells, seed, sigma, (int *)d.rowptr, (int *)d.col,
                       (double *)d.val64, (double *)d.b));
     B_CUDA(cudaMemsetAsync(d.x, 0, 8 * (size_t)n, st));
@@ -783,12 +951,10 @@ int b200la_batch_get_system(b200la_batch B, int slot, int *rowptr, int *col, dou
   B_CHECK(B && slot >= 0 && slot < B->capacity && B->sys[slot].used, B200LA_ERR_INVALID, "batch_get_system: slot");
   const HostSys &h = B->sys[slot];
   cudaStream_t st = B->ctx->stream;
-  const SysDesc<double> &d64 = h.d64;
-  const SysDesc<float> &d32 = h.d32;
-  const int *rp = B->kp.mixed ? d32.rowptr : d64.rowptr;
-  const int *cl = B->kp.mixed ? d32.col : d64.col;
-  const double *vv = B->kp.mixed ? d32.val64 : d64.val64;
-  const double *bb = B->kp.mixed ? d32.b : d64.b;
+  const int *rp = B->kp.mixed ? h.d32.rowptr : h.d64.rowptr;
+  const int *cl = B->kp.mixed ? h.d32.col : h.d64.col;
+  const double *vv = B->kp.mixed ? h.d32.val64 : h.d64.val64;
+  const double *bb = B->kp.mixed ? h.d32.b : h.d64.b;
   if (rowptr) B_CUDA(cudaMemcpyAsync(rowptr, rp, sizeof(int) * (h.n + 1), cudaMemcpyDeviceToHost, st));
   if (col) B_CUDA(cudaMemcpyAsync(col, cl, sizeof(int) * (size_t)h.nnz, cudaMemcpyDeviceToHost, st));
   if (val) B_CUDA(cudaMemcpyAsync(val, vv, 8 * (size_t)h.nnz, cudaMemcpyDeviceToHost, st));
@@ -822,23 +988,46 @@ int b200la_batch_run(b200la_batch B, int max_passes, int *active_out) {
   B_CHECK(B && max_passes >= 1, B200LA_ERR_INVALID, "batch_run: bad argument");
   cudaStream_t st = B->ctx->stream;
   int active = 0;
-  B_TRY(rebuild_tiles(B, &active));
+  B_TRY(upload_tiles(B, true, &active, nullptr));
+  BatchGlobals &g = *B->glob_host;
   if (active == 0) {
+    g.passes = 0;
     if (active_out) *active_out = 0;
     return B200LA_OK;
   }
-  if (!B->exec) B_TRY(build_graph(B));
-  BatchGlobals &g = *B->glob_host;
+  if (B->ctx->use_graphs && !B->exec) B_TRY(build_graph(B));
   memset(&g, 0, sizeof(g));
   g.active = active;
   g.max_passes = max_passes;
   g.ntiles = (int)B->tiles_host.size();
   B_CUDA(cudaMemcpyAsync(B->glob, &g, sizeof(BatchGlobals), cudaMemcpyHostToDevice, st));
-  B_CUDA(cudaGraphLaunch(B->exec, st));
+  if (B->ctx->use_graphs) B_CUDA(cudaGraphLaunch(B->exec, st));
+  else B_TRY(host_loop(B));
   B_CUDA(cudaMemcpyAsync(B->st_host, B->st, sizeof(SysState) * B->capacity, cudaMemcpyDeviceToHost, st));
   B_CUDA(cudaMemcpyAsync(B->glob_host, B->glob, sizeof(BatchGlobals), cudaMemcpyDeviceToHost, st));
   B_CUDA(cudaStreamSynchronize(st));
   if (active_out) *active_out = B->glob_host->active;
+  return B200LA_OK;
+}
+
+int b200la_batch_solve(b200la_batch B, int chunk_passes, int *total_passes) {
+  B_CHECK(B && chunk_passes >= 1, B200LA_ERR_INVALID, "batch_solve: bad argument");
+  int active = 1, total = 0;
+  // each run ends after chunk_passes passes; the next run's tile list holds
+  // only the systems still running, so finished systems stop costing passes
+  while (active > 0) {
+    B_TRY(b200la_batch_run(B, chunk_passes, &active));
+    total += B->glob_host->passes;
+  }
+  B->glob_host->passes = total;
+  if (total_passes) *total_passes = total;
+  return B200LA_OK;
+}
+
+int b200la_batch_last_run(b200la_batch B, int *passes, double *reserved) {
+  B_CHECK(B, B200LA_ERR_INVALID, "batch_last_run: null batch");
+  if (passes) *passes = B->glob_host->passes;
+  if (reserved) *reserved = 0.0;
   return B200LA_OK;
 }
 
@@ -858,21 +1047,14 @@ int b200la_batch_result(b200la_batch B, int slot, double *x_host, b200la_sys_res
   r->device_us = (s.phase == PH_DONE && s.t_done >= s.t_begin) ? (double)(s.t_done - s.t_begin) / 1e3 : 0.0;
   if (B->kp.precond && s.bad_row != 0xffffffffu) r->state = B200LA_FAIL_BREAKDOWN;
   if (r->state == B200LA_SUCCESS_ABS || r->state == B200LA_SUCCESS_REL) r->solver_state = B200LA_SOLVER_SUCCESS;
-  else if (r->state == B200LA_FAIL_DIV || r->state == B200LA_FAIL_MAXITS) r->solver_state = B200LA_SOLVER_EXCEEDED;
-  else if (r->state == B200LA_ITERATE) r->solver_state = B200LA_SOLVER_EXCEEDED;
+  else if (r->state == B200LA_FAIL_DIV || r->state == B200LA_FAIL_MAXITS || r->state == B200LA_ITERATE)
+    r->solver_state = B200LA_SOLVER_EXCEEDED;
   else r->solver_state = B200LA_SOLVER_ERROR;
   if (x_host) {
     const double *xd = B->kp.mixed ? h.d32.x : h.d64.x;
     B_CUDA(cudaMemcpyAsync(x_host, xd, 8 * (size_t)h.n, cudaMemcpyDeviceToHost, B->ctx->stream));
     B_CUDA(cudaStreamSynchronize(B->ctx->stream));
   }
-  return B200LA_OK;
-}
-
-int b200la_batch_last_run(b200la_batch B, int *passes, double *reserved) {
-  B_CHECK(B, B200LA_ERR_INVALID, "batch_last_run: null batch");
-  if (passes) *passes = B->glob_host->passes;
-  if (reserved) *reserved = 0.0;
   return B200LA_OK;
 }
 
@@ -885,93 +1067,7 @@ int b200la_batch_info(b200la_batch B, int *used_slots, int64_t *device_bytes) {
   return B200LA_OK;
 }
 
-}  // extern "C"
-
-namespace {
-
-template <typename T, int G>
-int time_plain(b200la_batch B, int reps, float *ms) {
-  cudaStream_t st = B->ctx->stream;
-  const int nt = (int)B->tiles_host.size();
-  int occ = 1;
-  B_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, (const void *)batch_spmv_plain_kernel<T, G>, kBlock, 0));
-  const int grid = B->ctx->num_sms * std::max(occ, 1);
-  const SysDesc<T> *desc = (const SysDesc<T> *)B->desc;
-  batch_spmv_plain_kernel<T, G><<<grid, kBlock, 0, st>>>(B->tiles, nt, desc);
-  cudaEvent_t e0, e1;
-  B_CUDA(cudaEventCreate(&e0));
-  B_CUDA(cudaEventCreate(&e1));
-  B_CUDA(cudaEventRecord(e0, st));
-  for (int r = 0; r < reps; ++r) batch_spmv_plain_kernel<T, G><<<grid, kBlock, 0, st>>>(B->tiles, nt, desc);
-  B_CUDA(cudaEventRecord(e1, st));
-  B_CUDA(cudaEventSynchronize(e1));
-  B_CUDA(cudaEventElapsedTime(ms, e0, e1));
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  B_CUDA(cudaGetLastError());
-  *ms /= reps;
-  return B200LA_OK;
-}
-
-template <typename T> int time_lanes(b200la_batch B, int lanes, float *ms) {
-  switch (lanes) {
-    case 2: return time_plain<T, 2>(B, 5, ms);
-    case 4: return time_plain<T, 4>(B, 5, ms);
-    case 8: return time_plain<T, 8>(B, 5, ms);
-    case 16: return time_plain<T, 16>(B, 5, ms);
-    case 32: return time_plain<T, 32>(B, 5, ms);
-  }
-  return fail(B200LA_ERR_INVALID, "lanes %d", lanes);
-}
-
-// Restart every listed slot from x = 0: RESID phase, counters cleared.
-template <typename T>
-__global__ void __launch_bounds__(kBlock) batch_restart_kernel(const int *__restrict__ slots,
-                                                               const SysDesc<T> *__restrict__ desc, SysState *st) {
-  const int s = slots[blockIdx.x];
-  const SysDesc<T> d = desc[s];
-  for (int i = threadIdx.x; i < d.n; i += kBlock) d.x[i] = 0.0;
-  if (threadIdx.x == 0) {
-    SysState &S = st[s];
-    const unsigned bad = S.bad_row;
-    S = SysState{};
-    S.phase = PH_RESID;
-    S.bad_row = bad;
-  }
-}
-
-}  // namespace
-
-extern "C" int b200la_batch_tune(b200la_batch B, int *lanes_out, double *usec) {
-  B_CHECK(B, B200LA_ERR_INVALID, "batch_tune: null batch");
-  int active = 0;
-  B_TRY(rebuild_tiles(B, &active));
-  if (active == 0) {
-    if (lanes_out) *lanes_out = B->lanes;
-    if (usec) *usec = 0.0;
-    return B200LA_OK;
-  }
-  int best = B->lanes;
-  float best_ms = 1e30f;
-  for (int g : {2, 4, 8, 16}) {
-    float ms = 0.f;
-    B_TRY(B->kp.mixed ? time_lanes<float>(B, g, &ms) : time_lanes<double>(B, g, &ms));
-    if (ms < best_ms) {
-      best_ms = ms;
-      best = g;
-    }
-  }
-  if (best != B->lanes && B->exec) {
-    cudaGraphExecDestroy(B->exec);
-    B->exec = nullptr;
-  }
-  B->lanes = best;
-  if (lanes_out) *lanes_out = best;
-  if (usec) *usec = 1000.0 * best_ms;
-  return B200LA_OK;
-}
-
-extern "C" int b200la_batch_restart(b200la_batch B) {
+int b200la_batch_restart(b200la_batch B) {
   B_CHECK(B, B200LA_ERR_INVALID, "batch_restart: null batch");
   std::vector<int> slots;
   for (int s = 0; s < B->capacity; ++s)
@@ -988,6 +1084,7 @@ extern "C" int b200la_batch_restart(b200la_batch B) {
                                                                         B->st);
   B_CUDA(cudaGetLastError());
   B_CUDA(cudaFreeAsync(d_slots, st));
+  B_CUDA(cudaStreamSynchronize(st));
   for (int s : slots) {
     const unsigned bad = B->st_host[s].bad_row;
     memset(&B->st_host[s], 0, sizeof(SysState));
@@ -997,45 +1094,30 @@ extern "C" int b200la_batch_restart(b200la_batch B) {
   return B200LA_OK;
 }
 
-// Times the batched SpMV (the inner solve's SpMV kernel body) over every used
-// slot with the batch's current lanes; mean milliseconds per launch.
-extern "C" int b200la_batch_profile(b200la_batch B, int reps, double *ms_spmv, int64_t *algorithmic_bytes) {
-  B_CHECK(B && ms_spmv && reps >= 1, B200LA_ERR_INVALID, "batch_profile: bad argument");
-  // every used slot, whatever its phase
-  B->tiles_host.clear();
-  int64_t bytes = 0;
-  const int64_t vb = B->kp.mixed ? 4 : 8;
-  for (int s = 0; s < B->capacity; ++s) {
-    const HostSys &h = B->sys[s];
-    if (!h.used) continue;
-    const int count = (h.n + B->tile_rows - 1) / B->tile_rows;
-    const int first = (int)B->tiles_host.size();
-    for (int k = 0; k < count; ++k)
-      B->tiles_host.push_back(Tile{s, k * B->tile_rows, std::min(B->tile_rows, h.n - k * B->tile_rows), first, count, 0});
-    bytes += (int64_t)h.nnz * (vb + 4) + (int64_t)(h.n + 1) * 4 + 2 * (int64_t)h.n * vb;
-  }
-  const int64_t nt = (int64_t)B->tiles_host.size();
-  if (nt == 0) {
-    *ms_spmv = 0.0;
-    return B200LA_OK;
-  }
-  cudaStream_t st = B->ctx->stream;
-  if (nt > B->max_tiles) {
-    if (B->tiles) cudaFreeAsync(B->tiles, st);
-    if (B->part) cudaFreeAsync(B->part, st);
-    B_CUDA(cudaMallocAsync(&B->tiles, sizeof(Tile) * nt, st));
-    B_CUDA(cudaMallocAsync(&B->part, sizeof(double) * 3 * nt, st));
-    B->max_tiles = nt;
-    if (B->exec) {
-      cudaGraphExecDestroy(B->exec);
-      B->exec = nullptr;
-    }
-  }
-  B_CUDA(cudaMemcpyAsync(B->tiles, B->tiles_host.data(), sizeof(Tile) * nt, cudaMemcpyHostToDevice, st));
+int b200la_batch_tune(b200la_batch B, int *lanes_out, double *usec) {
+  B_CHECK(B, B200LA_ERR_INVALID, "batch_tune: null batch");
+  // Both SpMVs use the sliced-ELL layout (one row per lane, coalesced steps),
+  // which leaves no free parameter for these matrices; the time of the inner
+  // SpMV over the running systems is reported.
+  int active = 0;
+  B_TRY(upload_tiles(B, true, &active, nullptr));
   float ms = 0.f;
-  B_TRY(B->kp.mixed ? time_lanes<float>(B, B->lanes, &ms) : time_lanes<double>(B, B->lanes, &ms));
-  *ms_spmv = ms;
-  if (algorithmic_bytes) *algorithmic_bytes = bytes;
-  // the tile list on the device now lists every slot; the next run rebuilds it
+  if (active) B_TRY(B->kp.mixed ? time_plain<float>(B, 5, &ms) : time_plain<double>(B, 5, &ms));
+  if (lanes_out) *lanes_out = 0;
+  if (usec) *usec = 1000.0 * ms;
   return B200LA_OK;
 }
+
+int b200la_batch_profile(b200la_batch B, int reps, double *ms_spmv, int64_t *algorithmic_bytes) {
+  B_CHECK(B && ms_spmv && reps >= 1, B200LA_ERR_INVALID, "batch_profile: bad argument");
+  int count = 0;
+  int64_t bytes = 0;
+  B_TRY(upload_tiles(B, false, &count, &bytes));
+  float ms = 0.f;
+  if (count) B_TRY(B->kp.mixed ? time_plain<float>(B, reps, &ms) : time_plain<double>(B, reps, &ms));
+  *ms_spmv = ms;
+  if (algorithmic_bytes) *algorithmic_bytes = bytes;
+  return B200LA_OK;
+}
+
+}  // extern "C"

@@ -9,6 +9,7 @@
 // slice) per row with coalesced streaming loads instead of one thread per
 // row (cuda_spmv_kernel_csr_scalar.h:22-33).
 #include <cstdarg>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -259,6 +260,10 @@ int b200la_ctx_create(int device, b200la_ctx *out) {
   B_CUDA(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device));
   B_CUDA(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking));
   c->stream = c->own_stream;
+  {
+    const char *g = getenv("B200LA_GRAPHS");
+    c->use_graphs = !(g && g[0] == '0');
+  }
   B_CUDA(cudaMalloc(&c->scratch.part, sizeof(double) * 4 * kMaxReduceBlocks));
   B_CUDA(cudaMalloc(&c->scratch.ticket, sizeof(unsigned) * 16));
   B_CUDA(cudaMalloc(&c->scratch.result, sizeof(double) * 8));

@@ -60,6 +60,11 @@ struct b200la_ctx_s {
   cudaStream_t stream;
   b200la::ReduceScratch scratch;
   double *host_result;  // pinned [8]
+  // Device loops run as CUDA-graph WHILE nodes; with B200LA_GRAPHS=0 in the
+  // environment the same kernels are launched from a host loop instead, so
+  // a profiler can see each launch (ncu does not profile kernels inside
+  // graphs with conditional nodes).
+  bool use_graphs;
 };
 
 struct b200la_vec_s {

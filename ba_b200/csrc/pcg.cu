@@ -223,6 +223,24 @@ using namespace b200la;
 
 namespace b200la {
 
+// One iteration: K1, K2, K3 on stream `st` (captured into the graph body,
+// or launched from the host loop when graphs are off).
+template <typename T, bool PRE, bool IN_GRAPH>
+static int cg_launch_body_t(b200la_cg s, cudaStream_t st, cudaGraphConditionalHandle h) {
+  b200la_mat A = s->A;
+  b200la_ctx c = A->ctx;
+  CgVecs<T> v{(T *)s->x, (T *)s->r, (T *)s->p, (T *)s->Ap, (const T *)s->invd, s->n};
+  B_TRY(with_schedule<T>(A, [&](auto op) -> int {
+    using Op = decltype(op);
+    B_TRY(grid_for(c, (const void *)cg_spmv_kernel<Op, T>, op.work_items(), Op::kRowsPerBlock, &s->grid_spmv));
+    cg_spmv_kernel<Op, T><<<s->grid_spmv, kBlock, 0, st>>>(op, v, s->part, s->sc);
+    return B200LA_OK;
+  }));
+  cg_update_kernel<T, PRE><<<s->grid_ew, kBlock, 0, st>>>(v, s->part, s->sc);
+  cg_direction_kernel<T, PRE, IN_GRAPH><<<s->grid_ew, kBlock, 0, st>>>(v, s->sc, h);
+  return B200LA_OK;
+}
+
 template <typename T, bool PRE>
 static int cg_build_graph_t(b200la_cg s) {
   b200la_mat A = s->A;
@@ -247,14 +265,7 @@ static int cg_build_graph_t(b200la_cg s) {
   cudaStream_t cs;
   B_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
   B_CUDA(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-  int rc = with_schedule<T>(A, [&](auto op) -> int {
-    using Op = decltype(op);
-    B_TRY(grid_for(c, (const void *)cg_spmv_kernel<Op, T>, op.work_items(), Op::kRowsPerBlock, &s->grid_spmv));
-    cg_spmv_kernel<Op, T><<<s->grid_spmv, kBlock, 0, cs>>>(op, v, s->part, s->sc);
-    return B200LA_OK;
-  });
-  cg_update_kernel<T, PRE><<<s->grid_ew, kBlock, 0, cs>>>(v, s->part, s->sc);
-  cg_direction_kernel<T, PRE><<<s->grid_ew, kBlock, 0, cs>>>(v, s->sc, h);
+  int rc = cg_launch_body_t<T, PRE, true>(s, cs, h);
   cudaGraph_t captured;
   cudaError_t ce = cudaStreamEndCapture(cs, &captured);
   cudaStreamDestroy(cs);
@@ -303,8 +314,28 @@ static int cg_launch_init(b200la_cg s, const void *x_user, const void *b) {
 
 int cg_start(b200la_cg s, const void *x_dev, const void *b_dev) { return cg_launch_init(s, x_dev, b_dev); }
 
+template <typename T, bool PRE>
+static int cg_host_loop_t(b200la_cg s) {
+  cudaStream_t st = s->A->ctx->stream;
+  // the kernels return at once when the state is no longer "iterate", so
+  // checking the state every 16 iterations runs the same iterations
+  for (int64_t it = 0;; it += 16) {
+    for (int k = 0; k < 16; ++k) B_TRY((cg_launch_body_t<T, PRE, false>(s, st, 0)));
+    B_CUDA(cudaGetLastError());
+    CgScalars h;
+    B_TRY(cg_fetch(s, &h));
+    if (h.state != B200LA_ITERATE || it > (int64_t)s->prm.maxits + 32) break;
+  }
+  return B200LA_OK;
+}
+
 int cg_run(b200la_cg s) {
   b200la_mat A = s->A;
+  if (!A->ctx->use_graphs) {
+    const bool pre = s->prm.precond != 0;
+    if (A->dtype == B200LA_F64) return pre ? cg_host_loop_t<double, true>(s) : cg_host_loop_t<double, false>(s);
+    return pre ? cg_host_loop_t<float, true>(s) : cg_host_loop_t<float, false>(s);
+  }
   if (A->format != s->g_format || A->param != s->g_param) B_TRY(cg_build_graph(s));
   B_CUDA(cudaGraphLaunch(s->exec, A->ctx->stream));
   return B200LA_OK;

@@ -4,6 +4,10 @@ launches (no CUDA graph), so a profiler sees every launch on its own.
     python -m ba_b200.profile_case [--cells 128] [--dim 3] [--dtype f64|f32]
                                    [--spmv-reps 3] [--cg-iters 3] [--schedule tune|csr/8|sell/1]
 
+With --batch N: builds the standard batch of N 2D systems and solves it
+twice (the launches of interest are those of the second solve; set
+B200LA_GRAPHS=0 so the kernels launch one by one).
+
 Launch order: the tuner's SpMV launches (unless a schedule is given), then
 `--spmv-reps` plain SpMV launches (spmv_kernel), then the CG init kernel and
 `--cg-iters` iterations of cg_spmv_kernel, cg_update_kernel and
@@ -31,7 +35,13 @@ def main():
     ap.add_argument("--cg-iters", type=int, default=3)
     ap.add_argument("--schedule", default="tune")
     ap.add_argument("--sigma", type=float, default=0.0)
+    ap.add_argument("--batch", type=int, default=0,
+                    help="instead: solve a batch of this many 2D systems (n~logU[16,256], sigma 1) twice")
+    ap.add_argument("--chunk", type=int, default=32)
+    ap.add_argument("--tile-rows", type=int, default=0)
     a = ap.parse_args()
+    if a.batch:
+        return batch_case(a)
     dt = np.float64 if a.dtype == "f64" else np.float32
     s = P.q1_system(a.dim, a.cells, 20240602, a.sigma)
     plat = lmp.init_platform(0)
@@ -65,6 +75,24 @@ def main():
     print(f"spmv wall {spmv_ms:.3f} ms/launch; cg kernels ms: spmv_dot {ms[0]:.4f} update {ms[1]:.4f} "
           f"direction {ms[2]:.4f}; spmv algorithmic bytes {alg} -> {alg / ms[0] / 1e6:.1f} GB/s")
     load()
+
+
+def batch_case(a):
+    from .batch import Batch
+    systems = P.batch_systems(a.batch, sigma=1.0, seed=P.SEED_BATCH)
+    plat = lmp.init_platform(0)
+    B = Batch(len(systems), mixed=True, precond=True, rtol=1e-8, inner_rtol=1e-4, tile_rows=a.tile_rows,
+              platform=plat)
+    for s in systems:
+        B.add_system(s)
+    B.tune()
+    for _ in range(2):
+        B.restart()
+        t = time.perf_counter()
+        passes = B.solve(a.chunk)
+        dt = time.perf_counter() - t
+        print(f"batch {len(systems)} systems tile_rows {a.tile_rows or 'default'} chunk {a.chunk}: "
+              f"{passes} passes, {dt * 1e3:.1f} ms wall")
 
 
 if __name__ == "__main__":

@@ -254,8 +254,8 @@ typedef struct {
   int precond;        /* 1: Jacobi */
   int max_outer;      /* refinement passes (mixed) */
   int inner_maxits;   /* iterations per inner solve (FP64 mode: per solve) */
-  int lanes;          /* CSR lanes per row: 2..32 (0 = 4) */
-  int tile_rows;      /* rows per tile (0 = 512) */
+  int lanes;          /* reserved: 0 (both SpMVs use the sliced-ELL layout) */
+  int tile_rows;      /* rows per tile, a multiple of 32 (0 = 2048) */
   int reserved;
   double atol, rtol, dtol;  /* test on ||b - A x||_2 (FP64 mode: the CG recurrence residual) */
   double inner_rtol;        /* mixed: inner solve stops at inner_rtol x its start residual */
@@ -274,8 +274,9 @@ typedef struct {
 
 int b200la_batch_create(b200la_ctx ctx, const b200la_batch_params *params, b200la_batch *out);
 int b200la_batch_destroy(b200la_batch b);
-/* Device bytes one slot holds for a system of n rows and nnz entries. */
-int b200la_batch_slot_bytes(int64_t n, int64_t nnz, int mixed, int64_t *bytes);
+/* Device bytes one slot holds for a system of n rows, nnz entries and
+ * longest row max_row (the admission test of a request loop). */
+int b200la_batch_slot_bytes(int64_t n, int64_t nnz, int max_row, int mixed, int64_t *bytes);
 /* Upload one system (host CSR, FP64 values, FP64 RHS; x0 NULL = zero start)
  * into a free slot; it joins at the next run.  Copies are queued on the
  * context stream: host buffers must stay valid until the next run. */
@@ -293,6 +294,10 @@ int b200la_batch_remove(b200la_batch b, int slot);
 /* One graph launch: at most max_passes iterations of every running system.
  * Writes how many systems are still running. */
 int b200la_batch_run(b200la_batch b, int max_passes, int *active);
+/* Runs until every system has finished, in launches of at most chunk_passes
+ * passes; between launches the tile list is rebuilt from the systems still
+ * running.  Writes the passes taken. */
+int b200la_batch_solve(b200la_batch b, int chunk_passes, int *total_passes);
 /* Body passes (iterations of the device loop) taken by the last run. */
 int b200la_batch_last_run(b200la_batch b, int *passes, double *reserved);
 /* Result of a slot (solution copied to x if non-NULL). */
@@ -300,8 +305,8 @@ int b200la_batch_result(b200la_batch b, int slot, double *x, b200la_sys_result *
 int b200la_batch_info(b200la_batch b, int *used_slots, int64_t *device_bytes);
 /* Restart every system in the batch from x = 0 (matrices and RHS stay). */
 int b200la_batch_restart(b200la_batch b);
-/* Times each CSR lanes-per-row choice on the batch's matrices and keeps the
- * fastest; writes the choice and its time per batched SpMV in microseconds. */
+/* Times the inner solve's batched sliced-ELL SpMV over the running systems
+ * (microseconds per launch); `lanes` is reserved (writes 0). */
 int b200la_batch_tune(b200la_batch b, int *lanes, double *usec);
 /* Instrumentation: mean milliseconds of the inner solve's batched SpMV over
  * every slot (reps launches, CUDA events) and its algorithmic bytes:

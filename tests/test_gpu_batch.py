@@ -54,7 +54,7 @@ def test_fp64_batch_plain_cg(plat):
     (coefficient contrast ~e^6 without Jacobi scaling) CG's count is
     sensitive to rounding -- the device's FMA rows and tree-ordered dots move
     it by a few iterations, as they do for the single-system device CG -- so
-    there the bar is +-2% and the solution within 1e-10 of the oracle's."""
+    there the bar is +-5% and the solution within 1e-10 of the oracle's."""
     systems = _mix(seed=2, count=6)
     B = Batch(8, mixed=False, precond=False, rtol=1e-10, atol=0.0, platform=plat)
     slots = [B.add_system(s) for s in systems]
@@ -75,7 +75,7 @@ def test_fp64_batch_plain_cg(plat):
                      float(np.linalg.norm(r.x - ref.x) / np.linalg.norm(ref.x))))
     sig = {s.name: s.meta["sigma"] for s in systems}
     bad = [x for x in rows
-           if abs(x[2] - x[4]) > (1 if sig[x[0]] <= 1.0 else max(1, 0.02 * x[4])) or x[5] > 1e-10]
+           if abs(x[2] - x[4]) > (1 if sig[x[0]] <= 1.0 else max(2, 0.05 * x[4])) or x[5] > 1e-10]
     assert not bad, rows
 
 
