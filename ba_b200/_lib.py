@@ -55,6 +55,17 @@ class SysResult(C.Structure):
                 ("res_rel", C.c_double), ("device_us", C.c_double)]
 
 
+class ServerParams(C.Structure):
+    _fields_ = [("batch", BatchParams), ("hbm_budget", C.c_int64), ("chunk_passes", C.c_int),
+                ("max_skips", C.c_int)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [(k, C.c_int64) for k in ("submitted", "completed", "failed", "running", "queued",
+                                         "hbm_in_use", "hbm_peak", "hbm_budget", "launches", "passes")] + \
+               [(k, C.c_double) for k in ("p50_ms", "p99_ms", "mean_ms", "max_ms", "solves_per_s", "wall_s")]
+
+
 class CgResult(C.Structure):
     _fields_ = [("iters", C.c_int), ("state", C.c_int), ("solver_state", C.c_int),
                 ("reserved", C.c_int), ("res", C.c_double), ("res_init", C.c_double),
@@ -127,6 +138,16 @@ _SIGS = {
     "b200la_batch_add_q1": [_vp, _i, _i, C.c_uint64, _d, _P(_i)],
     "b200la_batch_get_system": [_vp, _i, _vp, _vp, _vp, _vp],
     "b200la_batch_slot_size": [_vp, _i, _P(_i), _P(_i64)],
+    "b200la_server_start": [_vp, _P(ServerParams), _P(_vp)],
+    "b200la_server_stop": [_vp],
+    "b200la_server_submit_csr": [_vp, _i, _i64, _vp, _vp, _vp, _vp, _vp, _P(_i64)],
+    "b200la_server_submit_q1": [_vp, _i, _i, C.c_uint64, _d, _P(_i64)],
+    "b200la_server_poll": [_vp, _i64, _P(_i), _vp, _P(SysResult), _P(_d)],
+    "b200la_server_wait": [_vp, _i64, _d, _P(_i)],
+    "b200la_server_release": [_vp, _i64],
+    "b200la_server_drain": [_vp, _d],
+    "b200la_server_get_stats": [_vp, _P(ServerStats)],
+    "b200la_server_reset_stats": [_vp],
     "b200la_q1_size": [_i, _i, _P(_i64), _P(_i64)],
     "b200la_q1_assemble": [_vp, _i, _i, C.c_uint64, _d, _vp, _vp, _vp, _vp],
     "b200la_mp_create": [_vp, _P(MpParams), _P(_vp)],

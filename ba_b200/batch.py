@@ -127,7 +127,7 @@ class Batch:
         return n.value
 
     def last_passes(self) -> int:
-        """Device-loop passes taken by the last run (each pass = 4 kernel launches)."""
+        """Device-loop passes taken by the last run (each pass = 3 kernel launches)."""
         n = C.c_int()
         call("b200la_batch_last_run", self.handle, C.byref(n), None)
         return n.value

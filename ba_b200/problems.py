@@ -195,6 +195,30 @@ def batch_systems(count: int = 1024, sigma: float = 1.0, seed: int = SEED_BATCH,
     return [q1_system(2, int(n), seed + 1 + k, sigma, f"batch{k}_n{int(n)}") for k, n in enumerate(sizes)]
 
 
+def serve_stream(count: int = 20000, rate: float = 100.0, lo_dofs: float = 1e3, hi_dofs: float = 2e6,
+                 seed: int = SEED_SERVE) -> list[dict]:
+    """The served workload: `count` Q1 diffusion solve requests arriving as a
+    Poisson process of `rate` requests/s.  Each request is 2D or 3D (equal
+    odds), has a DOF count log-uniform in [lo_dofs, hi_dofs] (cells per axis
+    rounded from it, at least 1), a lognormal coefficient with sigma uniform
+    in [0.5, 2], and its own seed.  Returns dicts with keys
+    t (arrival, s), dim, cells, dofs, sigma, seed."""
+    u_dim = uniform01(seed, count, stream=21)
+    u_dofs = uniform01(seed, count, stream=22)
+    u_sig = uniform01(seed, count, stream=23)
+    u_gap = uniform01(seed, count, stream=24)
+    gaps = -np.log1p(-u_gap) / rate
+    t = np.cumsum(gaps) - gaps[0]
+    out = []
+    for k in range(count):
+        dim = 2 if u_dim[k] < 0.5 else 3
+        dofs = math.exp(math.log(lo_dofs) + u_dofs[k] * (math.log(hi_dofs) - math.log(lo_dofs)))
+        cells = max(1, int(round(dofs ** (1.0 / dim))) - 1)
+        out.append(dict(t=float(t[k]), dim=dim, cells=cells, dofs=(cells + 1) ** dim,
+                        sigma=0.5 + 1.5 * float(u_sig[k]), seed=seed + 1 + k))
+    return out
+
+
 def known_answer_3x3() -> CSRSystem:
     """tests/cg_test.cc:44-94: [[2,-1,0],[-1,2,-1],[0,-1,2]] x = (1,-2,0),
     all 9 entries stored (explicit zeros), answer (-0.25, -1.5, -0.75)."""

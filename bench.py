@@ -54,9 +54,14 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="batch", choices=["batch", "poisson3d"])
+    ap.add_argument("--workload", default="batch", choices=["batch", "poisson3d", "serve"])
     ap.add_argument("--cells", type=int, default=128, help="poisson3d cells per axis")
     ap.add_argument("--count", type=int, default=BATCH_COUNT, help="batch: systems per step")
+    ap.add_argument("--requests", type=int, default=64, help="serve: requests per timed step")
+    ap.add_argument("--latency-requests", type=int, default=256, help="serve: requests of the latency stream")
+    ap.add_argument("--load", type=float, default=0.7,
+                    help="serve: Poisson arrival rate of the latency stream, as a fraction of measured throughput")
+    ap.add_argument("--hi-dofs", type=float, default=2e6, help="serve: largest request (DOFs)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -386,6 +391,199 @@ def run_batch(args, rank, local_rank, world, torch, dist, barrier):
     B.close()
 
 
+# ----------------------------------------------------------------- serve workload
+SERVE_CAPACITY = 256
+
+
+def serve_requests(count: int, rate: float, hi_dofs: float, rank: int, offset: int = 0):
+    """Requests offset..offset+count-1 of the seeded served stream (2D/3D Q1
+    diffusion, DOFs log-uniform in [1e3, hi_dofs], sigma U[0.5, 2])."""
+    from ba_b200 import problems as P
+    return P.serve_stream(offset + count, rate=rate, hi_dofs=hi_dofs, seed=P.SEED_SERVE + 7919 * rank)[offset:]
+
+
+def serve_config(args, extra=None):
+    cfg = {"workload": f"served: Poisson-arrival stream of 2D/3D Q1 diffusion solves, DOFs logU[1e3,{args.hi_dofs:.0e}], "
+                       f"lognormal kappa sigma~U[0.5,2], rel. residual 1e-8 (FP32 PCG + FP64 refinement), "
+                       f"admitted by free HBM into {SERVE_CAPACITY} slots, continuous batching",
+           "requests_per_step": args.requests,
+           "requests_note": "the first requests of the seeded 20,000-request stream; each is assembled on the "
+                            "device from (dim, cells, seed, sigma) at admission",
+           "l2": "inputs larger than L2 (each step's matrices total several GB)"}
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+def ref_serve_sample(reqs, nthreads: int, max_dofs: float, budget_s: float):
+    """The reference's CPU CG (FP64 Jacobi-PCG, OPENMP SpMV) to 1e-8 on the
+    stream's requests of at most max_dofs DOFs, in order, until budget_s of
+    solve time is spent; returns (solves, seconds)."""
+    import oracle
+    from ba_b200 import problems as P
+    total, cnt = 0.0, 0
+    for rq in reqs:
+        if rq["dofs"] > max_dofs:
+            continue
+        s = P.q1_system(rq["dim"], rq["cells"], rq["seed"], rq["sigma"])
+        ref = oracle.RefSystem(s.rowptr, s.col, s.val, impl=oracle.IMPL_OPENMP, nthreads=nthreads)
+        _, sec = ref.cg(s.b, maxits=100000, atol=0.0, rtol=BATCH_RTOL, dtol=1e8, precond=True)
+        ref.close()
+        total += sec
+        cnt += 1
+        if total >= budget_s:
+            break
+    return cnt, total
+
+
+def run_reference_serve(args, rank):
+    import oracle
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (reference sources absent)"}))
+        return
+    nthreads = os.cpu_count() or 1
+    reqs = serve_requests(2000, 1.0, args.hi_dofs, 0)
+    rates = []
+    for step in range(args.warmup + args.steps):
+        cnt, sec = ref_serve_sample(reqs[step * 40:], nthreads, 1e5, 3.0)
+        if step >= args.warmup:
+            rates.append(cnt / sec)
+    value = statistics.median(rates)
+    sample = (f"per step, requests of at most 1e5 DOFs of the stream (in order) solved to 1e-8 by HiFlow3 lmp "
+              f"CG (FP64 Jacobi-PCG, OPENMP SpMV, {nthreads} threads) until 3 s of solve time; larger requests "
+              f"are skipped, which favours the reference")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * args.requests / value,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": serve_config(args, {"parallelism": f"cpu openmp x{nthreads}"}),
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": nthreads, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+
+def _serve_stream(S, reqs, paced: bool, timeout: float = 1800.0):
+    """Submits reqs (paced by their arrival times, or all at once), waits for
+    all of them, fetches every solution; returns the results."""
+    t0 = time.monotonic()
+    ids = []
+    for rq in reqs:
+        if paced:
+            d = t0 + rq["t"] - time.monotonic()
+            if d > 0:
+                time.sleep(d)
+        ids.append(S.submit_q1(rq["dim"], rq["cells"], rq["seed"], rq["sigma"]))
+    S.drain(timeout)
+    out = []
+    for rid in ids:
+        r, lat = S.poll(rid, with_x=True)
+        out.append((r, lat))
+        S.release(rid)
+    return out
+
+
+def run_serve(args, rank, local_rank, world, torch, dist, barrier):
+    from ba_b200 import lmp
+    from ba_b200.server import Server
+
+    plat = lmp.Platform(local_rank)
+    stream = torch.cuda.current_stream()
+    plat.set_stream(stream.cuda_stream)
+    kw = dict(rtol=BATCH_RTOL, atol=0.0, dtol=1e8, inner_rtol=1e-4, max_outer=30, chunk_passes=CHUNK,
+              platform=plat)
+    R = args.requests
+    timed = serve_requests(args.steps * R, 1.0, args.hi_dofs, rank, offset=0)
+    warm = serve_requests(args.warmup * 4, 1.0, 2e4, rank, offset=50000)
+    S = Server(SERVE_CAPACITY, mixed=True, precond=True, **kw)
+    for w in range(args.warmup):
+        _serve_stream(S, warm[4 * w:4 * w + 4], paced=False)
+    clocks = ClockSampler(local_rank)
+    barrier()
+    clocks.start()
+    S.reset_stats()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    results = []
+    for k in range(args.steps):
+        results += _serve_stream(S, timed[k * R:(k + 1) * R], paced=False)
+    e1.record(stream)
+    e1.synchronize()
+    barrier()
+    clk = clocks.stop()
+    st_sat = S.stats()
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * args.steps * R / (ms_max / 1e3)
+    ok = sum(1 for r, _ in results if r.solver_state == 0)
+    d2h = int(sum(r.x.nbytes for r, _ in results)) // args.steps
+    h2d = 4 * 8 * R  # request descriptors: dim, cells, seed, sigma
+
+    # latency under a Poisson stream at a fraction of the measured throughput
+    rate = max(args.load * value / world, 1e-3)
+    lat_reqs = serve_requests(args.latency_requests, rate, args.hi_dofs, rank, offset=args.steps * R)
+    S.reset_stats()
+    lat_res = _serve_stream(S, lat_reqs, paced=True)
+    st_lat = S.stats()
+    lat_ok = sum(1 for r, _ in lat_res if r.solver_state == 0)
+    worst_rel = max(r.res_rel for r, _ in results + lat_res)
+    S.close()
+
+    # plain FP64 GPU CG (unpreconditioned recurrence) on the first step's requests, burst
+    Pn = Server(SERVE_CAPACITY, mixed=False, precond=False, inner_maxits=1000000, **{
+        k: v for k, v in kw.items() if k not in ("inner_rtol", "max_outer")})
+    _serve_stream(Pn, warm[:4], paced=False)
+    barrier()
+    c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    c0.record(stream)
+    plain_res = _serve_stream(Pn, timed[:R], paced=False)
+    c1.record(stream)
+    c1.synchronize()
+    plain_value = R / (c0.elapsed_time(c1) / 1e3)
+    plain_ok = sum(1 for r, _ in plain_res if r.solver_state == 0)
+    Pn.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import oracle
+        if oracle.ref_available():
+            nthreads = os.cpu_count() or 1
+            cnt, sec = ref_serve_sample(timed, nthreads, 1e5, 15.0)
+            cpu = {"value": cnt / sec, "unit": "solves/s", "cores": nthreads, "kind": "reference",
+                   "sample": f"{cnt} requests of at most 1e5 DOFs from the timed stream, solved to 1e-8 by "
+                             f"HiFlow3 lmp CG (FP64 Jacobi-PCG, OPENMP SpMV, {nthreads} threads); larger "
+                             f"requests skipped, which favours the reference"}
+    if rank == 0:
+        dofs = [rq["dofs"] for rq in timed]
+        print(json.dumps({
+            "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+            "config": serve_config(args, {
+                "parallelism": f"replicas x{world}", "throughput_stream": "each step submits its requests at once",
+                "converged": f"{ok}/{len(results)}", "dofs_mean": float(np.mean(dofs)), "dofs_max": int(max(dofs)),
+                "worst_rel_residual": worst_rel,
+                "hbm_peak_bytes": st_sat["hbm_peak"], "hbm_budget_bytes": st_sat["hbm_budget"],
+                "launches": st_sat["launches"], "device_passes": st_sat["passes"],
+                "latency_stream": {"requests": len(lat_reqs), "arrival_rate_per_s": rate,
+                                   "p50_ms": st_lat["p50_ms"], "p99_ms": st_lat["p99_ms"],
+                                   "mean_ms": st_lat["mean_ms"], "max_ms": st_lat["max_ms"],
+                                   "solves_per_s": st_lat["solves_per_s"], "converged": f"{lat_ok}/{len(lat_res)}",
+                                   "latency": "submission to solution on the host"},
+                "burst_latency_p50_ms": st_sat["p50_ms"], "burst_latency_p99_ms": st_sat["p99_ms"],
+                "plain_fp64_cg": {"value": plain_value, "unit": "solves/s", "requests": R,
+                                  "converged": f"{plain_ok}/{R}",
+                                  "speedup_of_mixed_pcg": value / world / plain_value}}),
+            "clocks": clk,
+            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "note": "the timed region is end to end: submission of request descriptors, device assembly, "
+                            "solve, solution copied to host memory"},
+            # 3 kernels per device pass; per request: coefficient, assembly and slot setup kernels
+            "gpu_launches": int(3 * st_sat["passes"] + 3 * args.steps * R),
+            "roofline": None,
+            "cpu_baseline": cpu}))
+
+
 # ----------------------------------------------------------------- poisson3d workload
 def run_reference_poisson3d(args, rank):
     import oracle
@@ -529,7 +727,8 @@ def main():
     rank, local_rank, world = dist_env()
     if args.impl == "reference":
         if rank == 0:
-            (run_reference_batch if args.workload == "batch" else run_reference_poisson3d)(args, rank)
+            {"batch": run_reference_batch, "poisson3d": run_reference_poisson3d,
+             "serve": run_reference_serve}[args.workload](args, rank)
         return
     import datetime
 
@@ -547,7 +746,7 @@ def main():
         torch.cuda.synchronize()
 
     load()
-    fn = run_batch if args.workload == "batch" else run_poisson3d
+    fn = {"batch": run_batch, "poisson3d": run_poisson3d, "serve": run_serve}[args.workload]
     fn(args, rank, local_rank, world, torch, dist, barrier)
     if world > 1:
         dist.barrier()

@@ -313,6 +313,67 @@ int b200la_batch_tune(b200la_batch b, int *lanes, double *usec);
  * sum over systems of nnz*(value+4) + (n+1)*4 + 2*n*value. */
 int b200la_batch_profile(b200la_batch b, int reps, double *ms_spmv, int64_t *algorithmic_bytes);
 
+/* ---- request loop (no reference counterpart) ------------------------------
+ * A server owns one batch and a worker thread.  Submitted solves wait in a
+ * FIFO queue; between graph launches of at most chunk_passes passes the
+ * worker admits queued requests first-fit while a slot is free and the
+ * resident systems' device bytes (b200la_batch_slot_bytes, plus the
+ * assembly's coefficient buffer for device-built requests) stay within
+ * hbm_budget, then harvests finished systems: their solution and result are
+ * copied to the host and the slot's memory is freed.  Admitted systems
+ * share every launch with the ones already running (continuous batching);
+ * matrices and Krylov state stay resident between launches.  A request the
+ * queue head could not fit past is held back once the head has been passed
+ * over max_skips times, so large requests are not starved.
+ *
+ * Threading: submit/poll/wait/stats may be called from any host thread;
+ * while a server runs, its context belongs to the worker thread (make no
+ * other calls on that context until b200la_server_stop returns). */
+typedef struct b200la_server_s *b200la_server;
+
+typedef struct {
+  b200la_batch_params batch;  /* solver settings; batch.capacity = slots */
+  int64_t hbm_budget;         /* device bytes for resident systems (0 = 90% of free memory at start) */
+  int chunk_passes;           /* passes per launch between admissions and harvests (0 = 32) */
+  int max_skips;              /* admission rounds the queue head may be passed over (0 = 8) */
+} b200la_server_params;
+
+typedef struct {
+  int64_t submitted, completed, failed, running, queued;
+  int64_t hbm_in_use, hbm_peak, hbm_budget;  /* admitted request bytes */
+  int64_t launches, passes;                  /* graph launches and device passes so far */
+  double p50_ms, p99_ms, mean_ms, max_ms;    /* submit-to-result latency of completed solves */
+  double solves_per_s;                       /* completed / wall_s */
+  double wall_s;                             /* first submission to last completion */
+} b200la_server_stats;
+
+int b200la_server_start(b200la_ctx ctx, const b200la_server_params *params, b200la_server *out);
+/* Stops the worker (requests still queued or running are dropped) and frees
+ * the server, its batch and every stored result. */
+int b200la_server_stop(b200la_server s);
+/* Queue one solve of a host CSR system (copied at submission; the caller's
+ * buffers may be reused on return).  Malformed CSR returns B200LA_ERR_MATRIX
+ * and a system larger than the budget B200LA_ERR_NOMEM, both at once. */
+int b200la_server_submit_csr(b200la_server s, int n, int64_t nnz, const int *rowptr, const int *col,
+                             const double *val, const double *rhs, const double *x0, int64_t *id);
+/* Queue one solve of a Q1 diffusion system assembled on the device at
+ * admission (arguments as in b200la_batch_add_q1). */
+int b200la_server_submit_q1(b200la_server s, int dim, int cells, uint64_t seed, double sigma, int64_t *id);
+/* done = 0 while queued or running.  Once done: the result, its latency
+ * (submission to harvest, ms) and, if x is non-NULL, the solution (n
+ * doubles).  A request that failed at admission returns that status. */
+int b200la_server_poll(b200la_server s, int64_t id, int *done, double *x, b200la_sys_result *result,
+                       double *latency_ms);
+/* Blocks until request id is done or timeout_s passes (done tells which). */
+int b200la_server_wait(b200la_server s, int64_t id, double timeout_s, int *done);
+/* Frees a finished request's stored solution. */
+int b200la_server_release(b200la_server s, int64_t id);
+/* Blocks until nothing is queued or running; B200LA_ERR_TIMEOUT after timeout_s. */
+int b200la_server_drain(b200la_server s, double timeout_s);
+int b200la_server_get_stats(b200la_server s, b200la_server_stats *stats);
+/* Clears the latency record and counters (e.g. after a warm-up stream). */
+int b200la_server_reset_stats(b200la_server s);
+
 #ifdef __cplusplus
 }
 #endif
