@@ -45,7 +45,7 @@ class MpResult(C.Structure):
 
 class BatchParams(C.Structure):
     _fields_ = [("capacity", C.c_int), ("mixed", C.c_int), ("precond", C.c_int), ("max_outer", C.c_int),
-                ("inner_maxits", C.c_int), ("lanes", C.c_int), ("tile_rows", C.c_int), ("reserved", C.c_int),
+                ("inner_maxits", C.c_int), ("lanes", C.c_int), ("tile_rows", C.c_int), ("index_bits", C.c_int),
                 ("atol", C.c_double), ("rtol", C.c_double), ("dtol", C.c_double), ("inner_rtol", C.c_double)]
 
 
@@ -131,10 +131,13 @@ _SIGS = {
     "b200la_batch_result": [_vp, _i, _vp, _P(SysResult)],
     "b200la_batch_info": [_vp, _P(_i), _P(_i64)],
     "b200la_batch_tune": [_vp, _P(_i), _P(_d)],
+    "b200la_batch_set_items": [_vp, _i, _i, _i, _i],
+    "b200la_batch_get_items": [_vp, _P(_i)],
     "b200la_batch_restart": [_vp],
     "b200la_batch_last_run": [_vp, _P(_i), _P(_d)],
     "b200la_batch_solve": [_vp, _i, _P(_i)],
     "b200la_batch_profile": [_vp, _i, _P(_d), _P(_i64)],
+    "b200la_batch_profile_pass": [_vp, _i, _P(_d), _P(_i64)],
     "b200la_batch_add_q1": [_vp, _i, _i, C.c_uint64, _d, _P(_i)],
     "b200la_batch_get_system": [_vp, _i, _vp, _vp, _vp, _vp],
     "b200la_batch_slot_size": [_vp, _i, _P(_i), _P(_i64)],

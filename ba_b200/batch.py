@@ -41,12 +41,12 @@ def slot_bytes(n: int, nnz: int, max_row: int, mixed: bool) -> int:
 class Batch:
     def __init__(self, capacity: int, *, mixed: bool = True, precond: bool = True, rtol: float = 1e-8,
                  atol: float = 0.0, dtol: float = 1e8, inner_rtol: float = 1e-4, max_outer: int = 30,
-                 inner_maxits: int = 100000, lanes: int = 0, tile_rows: int = 0,
+                 inner_maxits: int = 100000, lanes: int = 0, tile_rows: int = 0, index_bits: int = 0,
                  platform: Platform | None = None):
         self.platform = platform or init_platform()
         self.mixed = mixed
         prm = BatchParams(int(capacity), int(mixed), int(precond), int(max_outer), int(inner_maxits),
-                          int(lanes), int(tile_rows), 0, float(atol), float(rtol), float(dtol),
+                          int(lanes), int(tile_rows), int(index_bits), float(atol), float(rtol), float(dtol),
                           float(inner_rtol))
         self.handle = C.c_void_p()
         call("b200la_batch_create", self.platform.handle, C.byref(prm), C.byref(self.handle))
@@ -136,10 +136,31 @@ class Batch:
         """Restart every system from x = 0 (matrices and right-hand sides stay resident)."""
         call("b200la_batch_restart", self.handle)
 
-    def tune(self) -> tuple[int, float]:
-        lanes, us = C.c_int(), C.c_double()
-        call("b200la_batch_tune", self.handle, C.byref(lanes), C.byref(us))
-        return lanes.value, us.value
+    def tune(self) -> tuple[tuple[int, int, int], float]:
+        """Pick the warp item sizes (rows) of K1 (SpMV), K2 (update) and K3
+        (direction) by timing real passes (every system's state is
+        restored); returns ((k1, k2, k3), microseconds per pass)."""
+        rows, us = (C.c_int * 3)(), C.c_double()
+        call("b200la_batch_tune", self.handle, rows, C.byref(us))
+        return tuple(rows), us.value
+
+    def set_items(self, k1: int, k2: int, k3: int, adaptive: bool = True):
+        """Set the item sizes (rows, multiples of 32) of K1, K2, K3; with
+        adaptive, lightly loaded runs use smaller items."""
+        call("b200la_batch_set_items", self.handle, int(k1), int(k2), int(k3), int(adaptive))
+
+    def items(self) -> tuple[int, int, int]:
+        rows = (C.c_int * 3)()
+        call("b200la_batch_get_items", self.handle, rows)
+        return tuple(rows)
+
+    def profile_pass(self, reps: int = 5) -> tuple[list[float], list[int]]:
+        """Per-kernel ms of an inner pass (K1 SpMV + p.Ap, K2 update, K3
+        direction) and each kernel's algorithmic bytes.  Restarts every system."""
+        ms = (C.c_double * 3)()
+        nb = (C.c_int64 * 3)()
+        call("b200la_batch_profile_pass", self.handle, int(reps), ms, nb)
+        return list(ms), list(nb)
 
     def profile(self, reps: int = 5) -> tuple[float, int]:
         """(ms per batched SpMV over every slot, its algorithmic bytes)."""

@@ -7,14 +7,16 @@
 // (linear_solver/mpir.cc:52-230): FP64 residual, update and test around an
 // FP32 inner solve, or, in FP64 mode, a plain FP64 (P)CG.
 //
-// Work decomposition: every system is cut into tiles of consecutive rows (a
-// multiple of 32); a thread block handles one tile at a time (grid-stride
-// over the tile list), so large and small systems share every launch and the
-// load balances at tile granularity.  Per-system dot products are reduced
-// deterministically: each tile writes its partial sums, and the last tile of
-// the system to finish (per-system atomic ticket) adds the system's partials
-// in tile order.  A system's arithmetic therefore does not depend on what
-// else is in the batch.
+// Work decomposition: every system is cut into items of consecutive rows
+// (tile_rows, a multiple of 32, picked by the tuner); one warp handles one
+// item at a time (grid-stride over the item list across all warps of the
+// grid), so large and small systems share every launch, the load balances
+// at item granularity, and the warps of a block never wait on one another.
+// Per-system dot products are reduced deterministically: each item writes
+// its partial sums, and the warp of the system's last item to finish
+// (per-system atomic ticket) adds the system's partials in a fixed order.
+// A system's arithmetic therefore does not depend on what else is in the
+// batch or on the order its items ran in.
 //
 // Matrices are stored twice: CSR as uploaded (host-facing, setup), and a
 // sliced ELL copy used by both SpMVs: slices of 32 rows, every row padded to
@@ -22,11 +24,11 @@
 // (s*ell + k)*32 + l, so a warp reads 32 consecutive values per step and the
 // loads of one row do not depend on a row pointer.
 //
-// Each system walks through phases, advanced by the last tile of the kernel
-// that ends a phase, so all tiles of a system see one phase per launch:
+// Each system walks through phases, advanced by the last item of the kernel
+// that ends a phase, so all items of a system see one phase per launch:
 //   RESID   K1: r64 = b - A64 x (FP64), ||r64||, outer test; restart the inner
 //               solve from c = 0 with r = (T)r64, z = invD r, p = z -> START
-//   START   K3: opens the inner solve (-> INNER) once every tile saw START
+//   START   K3: opens the inner solve (-> INNER) once every item saw START
 //   INNER   K1: Ap = A p, p.Ap   K2: c += a p, r -= a Ap, r.r, r.z, inner test
 //               (-> CORRECT)     K3: p = b p + z
 //   CORRECT K3: x += (double)c -> RESID (mixed) or DONE (FP64 mode)
@@ -53,7 +55,8 @@ template <typename T> struct SysDesc {
   const int *col;
   const double *val64;
   int ell;            // sliced ELL width (longest row)
-  const int *scol;    // sliced ELL columns
+  int col16;          // 1: sliced ELL columns stored as int16 offsets from the row
+  const void *scol;   // sliced ELL columns: int32, or int16 (column - row) when col16
   const T *sval;      // sliced ELL values in the inner type
   const double *sval64;  // sliced ELL values in FP64 (== sval in FP64 mode)
   const double *b;
@@ -91,20 +94,33 @@ struct BatchGlobals {
   int active;          // systems not DONE (and not EMPTY)
   int passes;          // passes taken by this launch
   int max_passes;      // pass budget of this launch
-  int ntiles;          // tiles in the current tile list
   unsigned ticket;     // last block of K3
-  unsigned pad;
+  int ntiles[3];       // items in the K1, K2 and K3 lists
+  int tile_rows[3];    // rows per item of each list
+  int pad2;
   unsigned long long t_start;
 };
 
-struct Tile {
+// One warp's work item: rows row0 .. row0 + tile_rows - 1 of one system (the
+// last item of a system is shorter).  Items of a system are consecutive in
+// the list, so its first item is t - row0 / tile_rows and it has
+// ceil(n / tile_rows) items; tile_rows is uniform over the list.
+struct __align__(8) Tile {
   int sys;
-  int row0;   // a multiple of 32
-  int rows;
-  int first;  // index of the system's first tile (its partials start there)
-  int count;  // tiles of the system
-  int pad;
+  int row0;  // a multiple of tile_rows (itself a multiple of 32)
 };
+
+// Geometry of item t: rows, first item of the system, items of the system.
+struct ItemGeo {
+  int rows, first, count;
+};
+__device__ __forceinline__ ItemGeo item_geo(const Tile &tl, int t, int n, int tile_rows) {
+  ItemGeo g;
+  g.rows = min(tile_rows, n - tl.row0);
+  g.first = t - tl.row0 / tile_rows;
+  g.count = (n + tile_rows - 1) / tile_rows;
+  return g;
+}
 
 __device__ __forceinline__ unsigned long long globaltimer() {
   unsigned long long t;
@@ -112,33 +128,48 @@ __device__ __forceinline__ unsigned long long globaltimer() {
   return t;
 }
 
-// Deterministic per-system reduction: the block's sums go to part[k][tile];
-// the last tile of the system (ticket over `count` tiles) adds the system's
-// partials in tile order.  Returns true in that block; totals in v[] of
-// thread 0.  Must be called by every thread of the block.
+// Deterministic per-system reduction over warp items: the warp's sums go to
+// part[k][item]; the system's last item to finish (atomic ticket over
+// `count` items) adds the system's partials in a fixed order (lane-strided
+// sums, then a shuffle tree), whatever order the items finished in.
+// Returns true in every lane of that warp, with the totals in v[] of every
+// lane.  Must be called by all 32 lanes of the warp.
 template <int NV>
-__device__ __forceinline__ bool tile_sum_last(double (&v)[NV], double *part, int64_t ntiles, int tile, int first,
+__device__ __forceinline__ bool warp_sum_last(double (&v)[NV], double *part, int64_t stride, int item, int first,
                                               int count, unsigned *ticket) {
-  __shared__ double smem[NV * 32];
-  __shared__ bool is_last;
-  block_sum<NV>(v, smem);
-  if (threadIdx.x == 0) {
+  const int lane = threadIdx.x & 31;
 #pragma unroll
-    for (int k = 0; k < NV; ++k) part[k * ntiles + tile] = v[k];
+  for (int k = 0; k < NV; ++k) v[k] = warp_sum(v[k]);
+  unsigned t = 0;
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) part[k * stride + item] = v[k];
     __threadfence();
-    unsigned t = atomicInc(ticket, (unsigned)count - 1);
-    is_last = (t == (unsigned)count - 1);
+    t = atomicInc(ticket, (unsigned)count - 1);
   }
-  __syncthreads();
-  if (!is_last) return false;
+  t = __shfl_sync(0xffffffffu, t, 0);
+  if (t != (unsigned)count - 1) return false;
   __threadfence();
 #pragma unroll
   for (int k = 0; k < NV; ++k) {
     double a = 0.0;
-    for (int i = threadIdx.x; i < count; i += blockDim.x) a += __ldcg(&part[k * ntiles + first + i]);
-    v[k] = a;
+    for (int i = lane; i < count; i += 32) a += __ldcg(&part[k * stride + first + i]);
+    v[k] = warp_sum(a);
   }
-  block_sum<NV>(v, smem);
+  return true;
+}
+
+// Ticket only: true in every lane of the warp that handles the system's
+// last item to arrive.
+__device__ __forceinline__ bool warp_last(int count, unsigned *ticket) {
+  unsigned t = 0;
+  if ((threadIdx.x & 31) == 0) {
+    __threadfence();
+    t = atomicInc(ticket, (unsigned)count - 1);
+  }
+  t = __shfl_sync(0xffffffffu, t, 0);
+  if (t != (unsigned)count - 1) return false;
+  __threadfence();
   return true;
 }
 
@@ -159,39 +190,80 @@ __device__ __forceinline__ void finish_system(SysState &S, BatchGlobals *g, int 
 }
 
 // One row of y = A x per lane from the sliced ELL layout (V = value type of
-// the stored values, X = type of x).
-template <typename V, typename X>
-__device__ __forceinline__ V sell_row(const int *__restrict__ scol, const V *__restrict__ sval, int ell,
-                                      const X *__restrict__ x, int slice, int lane) {
+// the stored values, X = type of x, I = stored column type: int, or short
+// holding column - row).  The products are added in the row's stored order
+// whatever I is, so both column types give the same bits.
+template <typename V, typename X, typename I, int UNROLL>
+__device__ __forceinline__ V sell_row_t(const I *__restrict__ scol, const V *__restrict__ sval, int ell,
+                                        const X *__restrict__ x, int slice, int lane) {
   const int64_t base = (int64_t)slice * ell * 32 + lane;
-  const int *cp = scol + base;
+  const I *cp = scol + base;
   const V *vp = sval + base;
+  const int row = slice * 32 + lane;
   V sum = V(0);
-#pragma unroll 9
-  for (int k = 0; k < ell; ++k) sum = fma(ld_stream(vp + k * 32), (V)ld_keep(x + ld_stream(cp + k * 32)), sum);
+#pragma unroll UNROLL
+  for (int k = 0; k < ell; ++k) {
+    const int c = sizeof(I) == 2 ? row + (int)ld_stream(cp + k * 32) : (int)ld_stream(cp + k * 32);
+    sum = fma(ld_stream(vp + k * 32), (V)ld_keep(x + c), sum);
+  }
   return sum;
 }
+
+template <typename V, typename X, int UNROLL = 9>
+__device__ __forceinline__ V sell_row(const void *scol, int col16, const V *__restrict__ sval, int ell,
+                                      const X *__restrict__ x, int slice, int lane) {
+  return col16 ? sell_row_t<V, X, short, UNROLL>((const short *)scol, sval, ell, x, slice, lane)
+               : sell_row_t<V, X, int, UNROLL>((const int *)scol, sval, ell, x, slice, lane);
+}
+
+// Warp-item loop shared by the pass kernels: warp w of the grid (W warps)
+// takes items w, w + W, w + 2W, ... and loads the next item's record while
+// it works on the current one.  (Claiming items from an atomic counter
+// instead was measured slower: thousands of warps contend on one address.)
+template <typename F>
+__device__ __forceinline__ void for_each_item(const Tile *__restrict__ tiles, int ntiles, F &&body) {
+  const int nw = gridDim.x * (kBlock / 32);
+  int t = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
+  Tile tl = t < ntiles ? tiles[t] : Tile{};
+  while (t < ntiles) {
+    const int tn = t + nw;
+    const Tile nx = tn < ntiles ? tiles[tn] : Tile{};
+    body(tl, t);
+    tl = nx;
+    t = tn;
+  }
+}
+
+// Static variant (timing kernels): warp w takes items w, w + W, ...
+template <typename F>
+__device__ __forceinline__ void for_each_item_static(const Tile *__restrict__ tiles, int ntiles, F &&body) {
+  const int nw = gridDim.x * (kBlock / 32);
+  for (int t = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5); t < ntiles; t += nw) body(tiles[t], t);
+}
+
 
 }  // namespace b200la
 
 namespace b200la {
 
-// ---- RESID tiles (run by K1): FP64 residual, outer test, inner restart ------
+// ---- RESID items (run by K1): FP64 residual, outer test, inner restart ------
 // r64 = b - A64 x with the FP64 sliced-ELL values, ||r64||, then the inner
 // solve restarts from c = 0 with r = (T)r64, z = invD r, p = z.  The
-// system's last tile applies the outer test: DONE, or START.
+// system's last item applies the outer test: DONE, or START.
 template <typename T, bool PRE>
-__device__ __forceinline__ void resid_tile(const Tile &tl, int t, const SysDesc<T> &d, SysState &S, double *part,
-                                           int64_t part_stride, BatchGlobals *g, const BatchParams &prm) {
+__device__ __forceinline__ void resid_item(const Tile &tl, int t, const ItemGeo &ig, const SysDesc<T> &d, SysState &S,
+                                           double *part, int64_t part_stride, BatchGlobals *g,
+                                           const BatchParams &prm) {
   Acc<double> rr64;
   Acc<T> rrin, rzin;
   const int lane = threadIdx.x & 31;
-  const int nsl = (tl.rows + 31) >> 5;
-  for (int sl = (int)threadIdx.x >> 5; sl < nsl; sl += kBlock / 32) {
+  const int nsl = (ig.rows + 31) >> 5;
+  const int end = tl.row0 + ig.rows;
+  for (int sl = 0; sl < nsl; ++sl) {
     const int slice = (tl.row0 >> 5) + sl;
-    const double y = sell_row<double, double>(d.scol, d.sval64, d.ell, d.x, slice, lane);
+    const double y = sell_row<double, double, 3>(d.scol, d.col16, d.sval64, d.ell, d.x, slice, lane);
     const int row = slice * 32 + lane;
-    if (row < tl.row0 + tl.rows) {
+    if (row < end) {
       const double r64 = d.b[row] - y;
       rr64.add(r64 * r64);
       const T r = (T)r64;
@@ -204,7 +276,7 @@ __device__ __forceinline__ void resid_tile(const Tile &tl, int t, const SysDesc<
     }
   }
   double v[3] = {rr64.value(), rrin.value(), rzin.value()};
-  if (tile_sum_last<3>(v, part, part_stride, t, tl.first, tl.count, &S.ticket[3]) && threadIdx.x == 0) {
+  if (warp_sum_last<3>(v, part, part_stride, t, ig.first, ig.count, &S.ticket[3]) && lane == 0) {
     const double res = sqrt(v[0]);
     S.res = res;
     if (S.outer == 0) {
@@ -226,38 +298,99 @@ __device__ __forceinline__ void resid_tile(const Tile &tl, int t, const SysDesc<
   }
 }
 
+// Ap = A p over an item's rows and the item's share of p.Ap, for rows of
+// exactly E stored entries (E a compile-time width): software-pipelined, so
+// the next slice's values and columns stream in while the current slice's
+// gathers of p are in flight.  Same products, same order as sell_row.
+template <typename T, typename I, int E>
+__device__ __forceinline__ double spmv_item_fixed(int row0, int rows, const SysDesc<T> &d, int lane) {
+  Acc<T> acc;
+  const int nsl = (rows + 31) >> 5;
+  const int end = row0 + rows;
+  const I *__restrict__ scol = (const I *)d.scol;
+  const T *__restrict__ sval = d.sval;
+  const T *__restrict__ p = d.p;
+  int slice = row0 >> 5;
+  I cv[E];
+  T vv[E];
+  {
+    const int64_t base = (int64_t)slice * E * 32 + lane;
+#pragma unroll
+    for (int k = 0; k < E; ++k) {
+      cv[k] = ld_stream(scol + base + k * 32);
+      vv[k] = ld_stream(sval + base + k * 32);
+    }
+  }
+  for (int sl = 0; sl < nsl; ++sl, ++slice) {
+    const int row = slice * 32 + lane;
+    T xs[E];
+#pragma unroll
+    for (int k = 0; k < E; ++k) xs[k] = ld_keep(p + (sizeof(I) == 2 ? row + (int)cv[k] : (int)cv[k]));
+    T vc[E];
+#pragma unroll
+    for (int k = 0; k < E; ++k) vc[k] = vv[k];
+    if (sl + 1 < nsl) {
+      const int64_t base = (int64_t)(slice + 1) * E * 32 + lane;
+#pragma unroll
+      for (int k = 0; k < E; ++k) {
+        cv[k] = ld_stream(scol + base + k * 32);
+        vv[k] = ld_stream(sval + base + k * 32);
+      }
+    }
+    T y = T(0);
+#pragma unroll
+    for (int k = 0; k < E; ++k) y = fma(vc[k], xs[k], y);
+    if (row < end) {
+      d.Ap[row] = y;
+      acc.add(y * p[row]);
+    }
+  }
+  return acc.value();
+}
+
+// Ap = A p over an item's rows and the item's share of p.Ap.
+template <typename T, typename I>
+__device__ __forceinline__ double spmv_item(int row0, int rows, const SysDesc<T> &d, int lane) {
+  if (sizeof(T) == 4 && d.ell == 9) return spmv_item_fixed<T, I, 9>(row0, rows, d, lane);
+  Acc<T> acc;
+  const int nsl = (rows + 31) >> 5;
+  const int end = row0 + rows;
+  const I *scol = (const I *)d.scol;
+  for (int sl = 0; sl < nsl; ++sl) {
+    const int slice = (row0 >> 5) + sl;
+    const T y = sell_row_t<T, T, I, 9>(scol, d.sval, d.ell, d.p, slice, lane);
+    const int row = slice * 32 + lane;
+    if (row < end) {
+      d.Ap[row] = y;
+      acc.add(y * d.p[row]);
+    }
+  }
+  return acc.value();
+}
+
 // ---- K1: Ap = A p and p.Ap for INNER systems; RESID systems ------------------
 template <typename T, bool PRE>
-__global__ void __launch_bounds__(kBlock, 6) batch_spmv_kernel(const Tile *__restrict__ tiles,
+__global__ void __launch_bounds__(kBlock, 4) batch_spmv_kernel(const Tile *__restrict__ tiles,
                                                                const SysDesc<T> *__restrict__ desc, SysState *st,
                                                                double *part, int64_t part_stride, BatchGlobals *g,
                                                                BatchParams prm) {
-  const int ntiles = g->ntiles;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const Tile tl = tiles[t];
+  const int lane = threadIdx.x & 31;
+  const int tr = g->tile_rows[0];
+  for_each_item(tiles, g->ntiles[0], [&](const Tile &tl, int t) {
     SysState &S = st[tl.sys];
     const int ph = load_phase(&S);
-    if (ph != PH_INNER && ph != PH_RESID) continue;
+    if (ph != PH_INNER && ph != PH_RESID) return;
     const SysDesc<T> d = desc[tl.sys];
+    const ItemGeo ig = item_geo(tl, t, d.n, tr);
     if (ph == PH_RESID) {
-      resid_tile<T, PRE>(tl, t, d, S, part, part_stride, g, prm);
-      __syncthreads();
-      continue;
+      resid_item<T, PRE>(tl, t, ig, d, S, part, part_stride, g, prm);
+      return;
     }
-    Acc<T> acc;
-    const int nsl = (tl.rows + 31) >> 5;
-    for (int sl = warp; sl < nsl; sl += kBlock / 32) {
-      const int slice = (tl.row0 >> 5) + sl;
-      const T y = sell_row<T, T>(d.scol, d.sval, d.ell, d.p, slice, lane);
-      const int row = slice * 32 + lane;
-      if (row < tl.row0 + tl.rows) {
-        d.Ap[row] = y;
-        acc.add(y * d.p[row]);
-      }
-    }
-    double v[1] = {acc.value()};
-    if (tile_sum_last<1>(v, part, part_stride, t, tl.first, tl.count, &S.ticket[0]) && threadIdx.x == 0) {
+    // one column type per item, so each slice loop is a straight stream
+    const double pap = d.col16 ? spmv_item<T, short>(tl.row0, ig.rows, d, lane)
+                               : spmv_item<T, int>(tl.row0, ig.rows, d, lane);
+    double v[1] = {pap};
+    if (warp_sum_last<1>(v, part, part_stride, t, ig.first, ig.count, &S.ticket[0]) && lane == 0) {
       S.pAp = v[0];
       const double alpha = S.rz / v[0];
       S.alpha = alpha;
@@ -268,30 +401,31 @@ __global__ void __launch_bounds__(kBlock, 6) batch_spmv_kernel(const Tile *__res
         else finish_system(S, g, B200LA_FAIL_BREAKDOWN);
       }
     }
-    __syncthreads();
-  }
+  });
 }
+
 
 // ---- K2: c += alpha p, r -= alpha Ap, r.r and r.z; inner test ---------------
 template <typename T, bool PRE>
-__global__ void __launch_bounds__(kBlock, 6) batch_update_kernel(const Tile *__restrict__ tiles,
+__global__ void __launch_bounds__(kBlock, 4) batch_update_kernel(const Tile *__restrict__ tiles,
                                                                  const SysDesc<T> *__restrict__ desc, SysState *st,
                                                                  double *part, int64_t part_stride, BatchGlobals *g,
                                                                  BatchParams prm) {
-  const int ntiles = g->ntiles;
-  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const Tile tl = tiles[t];
+  const int lane = threadIdx.x & 31;
+  const int tr = g->tile_rows[1];
+  for_each_item(tiles, g->ntiles[1], [&](const Tile &tl, int t) {
     SysState &S = st[tl.sys];
-    if (load_phase(&S) != PH_INNER) continue;
+    if (load_phase(&S) != PH_INNER) return;
     const SysDesc<T> d = desc[tl.sys];
+    const ItemGeo ig = item_geo(tl, t, d.n, tr);
     const T alpha = (T)S.alpha;
     Acc<T> rr, rz;
-    // 16-byte vectors over the tile (tile starts are multiples of 32 rows and
-    // every slot vector is 256-byte aligned), then the ragged tail
+    // 16-byte vectors (item starts are multiples of 32 rows and every slot
+    // vector is 256-byte aligned), then the ragged tail
     using V = typename Vec16<T>::type;
     constexpr int W = Vec16<T>::n;
-    const int nv = tl.rows / W;
-    for (int q = threadIdx.x; q < nv; q += kBlock) {
+    const int nv = ig.rows / W;
+    for (int q = lane; q < nv; q += 32) {
       const int i = tl.row0 + q * W;
       V cv = *reinterpret_cast<const V *>(d.c + i);
       V rv = *reinterpret_cast<const V *>(d.r + i);
@@ -314,7 +448,8 @@ __global__ void __launch_bounds__(kBlock, 6) batch_update_kernel(const Tile *__r
       *reinterpret_cast<V *>(d.c + i) = cv;
       *reinterpret_cast<V *>(d.r + i) = rv;
     }
-    for (int i = tl.row0 + nv * W + threadIdx.x; i < tl.row0 + tl.rows; i += kBlock) {
+    const int end = tl.row0 + ig.rows;
+    for (int i = tl.row0 + nv * W + lane; i < end; i += 32) {
       d.c[i] = fma(alpha, d.p[i], d.c[i]);
       const T r = fma(-alpha, d.Ap[i], d.r[i]);
       d.r[i] = r;
@@ -322,7 +457,7 @@ __global__ void __launch_bounds__(kBlock, 6) batch_update_kernel(const Tile *__r
       if (PRE) rz.add(r * (r * d.invd[i]));
     }
     double v[2] = {rr.value(), rz.value()};
-    if (tile_sum_last<2>(v, part, part_stride, t, tl.first, tl.count, &S.ticket[1]) && threadIdx.x == 0) {
+    if (warp_sum_last<2>(v, part, part_stride, t, ig.first, ig.count, &S.ticket[1]) && lane == 0) {
       const double res = sqrt(v[0]);
       const double rz_new = PRE ? v[1] : v[0];
       S.res_in = res;
@@ -350,62 +485,71 @@ __global__ void __launch_bounds__(kBlock, 6) batch_update_kernel(const Tile *__r
       S.beta = rz_new / S.rz;
       S.rz = rz_new;
     }
-    __syncthreads();
-  }
+  });
 }
 
 // ---- K3: p = beta p + z (INNER); x += c (CORRECT); START -> INNER; end of pass
 template <typename T, bool PRE, bool IN_GRAPH = true>
-__global__ void __launch_bounds__(kBlock, 8) batch_direction_kernel(const Tile *__restrict__ tiles,
+__global__ void __launch_bounds__(kBlock, 5) batch_direction_kernel(const Tile *__restrict__ tiles,
                                                                     const SysDesc<T> *__restrict__ desc, SysState *st,
                                                                     double *part, int64_t part_stride, BatchGlobals *g,
                                                                     BatchParams prm, cudaGraphConditionalHandle loop) {
-  const int ntiles = g->ntiles;
-  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const Tile tl = tiles[t];
+  const int lane = threadIdx.x & 31;
+  const int tr = g->tile_rows[2];
+  for_each_item(tiles, g->ntiles[2], [&](const Tile &tl, int t) {
     SysState &S = st[tl.sys];
     const int ph = load_phase(&S);
+    if (ph != PH_INNER && ph != PH_CORRECT && ph != PH_START) return;
+    const SysDesc<T> d = desc[tl.sys];
+    const ItemGeo ig = item_geo(tl, t, d.n, tr);
+    const int end = tl.row0 + ig.rows;
     if (ph == PH_INNER) {
-      const SysDesc<T> d = desc[tl.sys];
       const T beta = (T)S.beta;
       using V = typename Vec16<T>::type;
       constexpr int W = Vec16<T>::n;
-      const int nv = tl.rows / W;
-      for (int q = threadIdx.x; q < nv; q += kBlock) {
-        const int i = tl.row0 + q * W;
-        V pv = *reinterpret_cast<const V *>(d.p + i);
-        const V rv = *reinterpret_cast<const V *>(d.r + i);
-        V dv;
-        if (PRE) dv = *reinterpret_cast<const V *>(d.invd + i);
-        T *ps = reinterpret_cast<T *>(&pv);
-        const T *rs = reinterpret_cast<const T *>(&rv);
-        const T *ds = reinterpret_cast<const T *>(&dv);
+      const int nv = ig.rows / W;
+      // two vectors per lane per step: six loads in flight before a store
+      for (int q = lane; q < nv; q += 64) {
+        const bool two = q + 32 < nv;
+        V pv[2], rv[2], dv[2];
 #pragma unroll
-        for (int k = 0; k < W; ++k) ps[k] = fma(beta, ps[k], PRE ? rs[k] * ds[k] : rs[k]);
-        *reinterpret_cast<V *>(d.p + i) = pv;
+        for (int u = 0; u < 2; ++u) {
+          if (u == 1 && !two) break;
+          const int i = tl.row0 + (q + 32 * u) * W;
+          pv[u] = *reinterpret_cast<const V *>(d.p + i);
+          rv[u] = *reinterpret_cast<const V *>(d.r + i);
+          if (PRE) dv[u] = *reinterpret_cast<const V *>(d.invd + i);
+        }
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          if (u == 1 && !two) break;
+          T *ps = reinterpret_cast<T *>(&pv[u]);
+          const T *rs = reinterpret_cast<const T *>(&rv[u]);
+          const T *ds = reinterpret_cast<const T *>(&dv[u]);
+#pragma unroll
+          for (int k = 0; k < W; ++k) ps[k] = fma(beta, ps[k], PRE ? rs[k] * ds[k] : rs[k]);
+          *reinterpret_cast<V *>(d.p + tl.row0 + (q + 32 * u) * W) = pv[u];
+        }
       }
-      for (int i = tl.row0 + nv * W + threadIdx.x; i < tl.row0 + tl.rows; i += kBlock)
+      for (int i = tl.row0 + nv * W + lane; i < end; i += 32)
         d.p[i] = fma(beta, d.p[i], PRE ? d.r[i] * d.invd[i] : d.r[i]);
     } else if (ph == PH_CORRECT) {
-      const SysDesc<T> d = desc[tl.sys];
-      for (int i = tl.row0 + threadIdx.x; i < tl.row0 + tl.rows; i += kBlock) d.x[i] += (double)d.c[i];
-      double v[1] = {0.0};
-      if (tile_sum_last<1>(v, part, part_stride, t, tl.first, tl.count, &S.ticket[2]) && threadIdx.x == 0) {
+      for (int i = tl.row0 + lane; i < end; i += 32) d.x[i] += (double)d.c[i];
+      // the phase moves on only after every item of the system saw CORRECT
+      if (warp_last(ig.count, &S.ticket[2]) && lane == 0) {
         if (prm.mixed) S.phase = PH_RESID;
         else finish_system(S, g, S.state);
       }
-    } else if (ph == PH_START) {
-      // K1 wrote the restart; open the inner solve once every tile of the
-      // system has passed this point
-      double v[1] = {0.0};
-      if (tile_sum_last<1>(v, part, part_stride, t, tl.first, tl.count, &S.ticket[2]) && threadIdx.x == 0)
-        S.phase = PH_INNER;
+    } else {
+      // START: K1 wrote the restart; open the inner solve once every item
+      // of the system has passed this point
+      if (warp_last(ig.count, &S.ticket[2]) && lane == 0) S.phase = PH_INNER;
     }
-    __syncthreads();
-  }
+  });
   // the last block of the launch ends the pass and decides whether the
   // device loop runs another one
   __shared__ bool last;
+  __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
     last = atomicInc(&g->ticket, gridDim.x - 1) == gridDim.x - 1;
@@ -443,7 +587,8 @@ __global__ void slot_setup_kernel(SysDesc<T> d, unsigned *bad) {
     for (int k = 0; k < d.ell; ++k) {
       const bool real = k < len;
       const int64_t pos = base + (int64_t)k * 32;
-      const_cast<int *>(d.scol)[pos] = real ? d.col[start + k] : pad;
+      if (d.col16) const_cast<short *>((const short *)d.scol)[pos] = real ? (short)(d.col[start + k] - (int)i) : 0;
+      else const_cast<int *>((const int *)d.scol)[pos] = real ? d.col[start + k] : pad;
       const_cast<T *>(d.sval)[pos] = real ? (T)d.val64[start + k] : T(0);
       if ((const void *)d.sval64 != (const void *)d.sval)
         const_cast<double *>(d.sval64)[pos] = real ? d.val64[start + k] : 0.0;
@@ -467,20 +612,48 @@ __global__ void slot_setup_kernel(SysDesc<T> d, unsigned *bad) {
   }
 }
 
-// Plain batched SpMV Ap = A p over every tile (timing only).
+// Plain batched SpMV Ap = A p over every item (timing only).
 template <typename T>
-__global__ void __launch_bounds__(kBlock, 8) batch_spmv_plain_kernel(const Tile *__restrict__ tiles, int ntiles,
+__global__ void __launch_bounds__(kBlock, 6) batch_spmv_plain_kernel(const Tile *__restrict__ tiles, int ntiles,
+                                                                     int tile_rows,
                                                                      const SysDesc<T> *__restrict__ desc) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const Tile tl = tiles[t];
+  const int lane = threadIdx.x & 31;
+  for_each_item_static(tiles, ntiles, [&](const Tile &tl, int) {
     const SysDesc<T> d = desc[tl.sys];
-    const int nsl = (tl.rows + 31) >> 5;
-    for (int sl = warp; sl < nsl; sl += kBlock / 32) {
+    const int rows = min(tile_rows, d.n - tl.row0);
+    const int nsl = (rows + 31) >> 5;
+    for (int sl = 0; sl < nsl; ++sl) {
       const int slice = (tl.row0 >> 5) + sl;
-      const T y = sell_row<T, T>(d.scol, d.sval, d.ell, d.p, slice, lane);
+      const T y = sell_row<T, T>(d.scol, d.col16, d.sval, d.ell, d.p, slice, lane);
       const int row = slice * 32 + lane;
-      if (row < tl.row0 + tl.rows) d.Ap[row] = y;
+      if (row < tl.row0 + rows) d.Ap[row] = y;
+    }
+  });
+}
+
+// Saves (save = 1) or restores the carried vectors x, c, r, p of the listed
+// slots: one block per slot; slot k's values start at offs[k] in xs and at
+// 3*offs[k] in vs.  Lets the tuner time real passes and leave every system
+// as it found it.
+template <typename T>
+__global__ void __launch_bounds__(kBlock) slot_snapshot_kernel(const int *__restrict__ slots,
+                                                               const int64_t *__restrict__ offs,
+                                                               const SysDesc<T> *__restrict__ desc, double *xs, T *vs,
+                                                               int save) {
+  const SysDesc<T> d = desc[slots[blockIdx.x]];
+  const int64_t o = offs[blockIdx.x];
+  T *vc = vs + 3 * o, *vr = vc + d.n, *vp = vr + d.n;
+  for (int i = threadIdx.x; i < d.n; i += kBlock) {
+    if (save) {
+      xs[o + i] = d.x[i];
+      vc[i] = d.c[i];
+      vr[i] = d.r[i];
+      vp[i] = d.p[i];
+    } else {
+      d.x[i] = xs[o + i];
+      d.c[i] = vc[i];
+      d.r[i] = vr[i];
+      d.p[i] = vp[i];
     }
   }
 }
@@ -520,26 +693,37 @@ struct HostSys {
 
 size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
 
+constexpr int kDefaultRows[3] = {256, 1024, 512};
+
+// One work-item list: host copy, device copy, per-item partial sums.
+struct ItemList {
+  int rows = 256;           // rows per item (upper bound when adaptive)
+  int used = 256;           // rows per item of the current list
+  int64_t cap = 0;          // device capacity (items)
+  Tile *dev = nullptr;      // [cap]
+  double *part = nullptr;   // [3][cap]
+  std::vector<Tile> host;
+};
+
 }  // namespace
 
 struct b200la_batch_s {
   b200la_ctx ctx;
   b200la_batch_params prm;
   BatchParams kp;
-  int tile_rows;
   int capacity;
-  int64_t max_tiles;
   std::vector<HostSys> sys;
+  // item lists of K1 (SpMV, residual), K2 (update + dots), K3 (direction)
+  ItemList lst[3];
+  bool adaptive;      // shrink items when few rows are running
+  int warps[3];       // resident warps of each pass kernel's grid (0 = not yet known)
   // device
   void *desc;         // SysDesc<T>[capacity]
   SysState *st;       // [capacity]
-  Tile *tiles;        // [max_tiles]
-  double *part;       // [3][max_tiles]
   BatchGlobals *glob;
   // host mirrors
   SysState *st_host;  // pinned [capacity]
   BatchGlobals *glob_host;
-  std::vector<Tile> tiles_host;
   int64_t device_bytes;
   cudaGraph_t graph;
   cudaGraphExec_t exec;
@@ -554,11 +738,11 @@ template <> SysDesc<double> &desc_of<double>(HostSys &h) { return h.d64; }
 template <> SysDesc<float> &desc_of<float>(HostSys &h) { return h.d32; }
 
 // Bytes one slot needs for a system (the admission test of the request loop).
-size_t slot_bytes(int64_t n, int64_t nnz, int64_t ell, bool mixed) {
+size_t slot_bytes(int64_t n, int64_t nnz, int64_t ell, bool mixed, bool col16 = false) {
   const size_t tb = mixed ? 4 : 8;
   const size_t padded = (size_t)((n + 31) / 32) * 32 * (size_t)ell;
   size_t b = align256(sizeof(int) * (n + 1)) + align256(sizeof(int) * nnz) + align256(8 * nnz);
-  b += align256(4 * padded) + align256(tb * padded);  // sliced-ELL columns and values
+  b += align256((col16 ? 2 : 4) * padded) + align256(tb * padded);  // sliced-ELL columns and values
   if (mixed) b += align256(8 * padded);               // and the FP64 values for the residual
   b += 2 * align256(8 * n);                            // b, x
   b += 5 * align256(tb * n);                           // c, r, p, Ap, invd
@@ -567,11 +751,11 @@ size_t slot_bytes(int64_t n, int64_t nnz, int64_t ell, bool mixed) {
 
 // Allocates a slot's buffers (one chunk) and carves them into a descriptor.
 template <typename T>
-int alloc_slot(BatchHandle B, int slot, int n, int64_t nnz, int ell, SysDesc<T> *out) {
+int alloc_slot(BatchHandle B, int slot, int n, int64_t nnz, int ell, bool col16, SysDesc<T> *out) {
   HostSys &h = B->sys[slot];
   cudaStream_t st = B->ctx->stream;
   const bool mixed = B->kp.mixed != 0;
-  h.bytes = slot_bytes(n, nnz, ell, mixed);
+  h.bytes = slot_bytes(n, nnz, ell, mixed, col16);
   B_CUDA(cudaMallocAsync(&h.chunk, h.bytes, st));
   char *p = (char *)h.chunk;
   auto take = [&](size_t bytes) { char *q = p; p += align256(bytes); return (void *)q; };
@@ -583,7 +767,8 @@ int alloc_slot(BatchHandle B, int slot, int n, int64_t nnz, int ell, SysDesc<T> 
   d.val64 = (const double *)take(8 * nnz);
   const size_t padded = (size_t)((n + 31) / 32) * 32 * (size_t)ell;
   d.ell = ell;
-  d.scol = (const int *)take(4 * padded);
+  d.col16 = col16 ? 1 : 0;
+  d.scol = take((col16 ? 2 : 4) * padded);
   d.sval = (const T *)take(sizeof(T) * padded);
   d.sval64 = mixed ? (const double *)take(8 * padded) : (const double *)d.sval;
   d.b = (const double *)take(8 * n);
@@ -620,11 +805,11 @@ int finish_slot(BatchHandle B, int slot, const SysDesc<T> &d) {
 }
 
 template <typename T>
-int add_typed(BatchHandle B, int slot, int n, int64_t nnz, int ell, const int *rowptr, const int *col,
+int add_typed(BatchHandle B, int slot, int n, int64_t nnz, int ell, bool col16, const int *rowptr, const int *col,
               const double *val, const double *b, const double *x0) {
   cudaStream_t st = B->ctx->stream;
   SysDesc<T> d{};
-  B_TRY(alloc_slot<T>(B, slot, n, nnz, ell, &d));
+  B_TRY(alloc_slot<T>(B, slot, n, nnz, ell, col16, &d));
   B_CUDA(cudaMemcpyAsync((void *)d.rowptr, rowptr, sizeof(int) * (n + 1), cudaMemcpyHostToDevice, st));
   if (nnz) {
     B_CUDA(cudaMemcpyAsync((void *)d.col, col, sizeof(int) * nnz, cudaMemcpyHostToDevice, st));
@@ -634,6 +819,25 @@ int add_typed(BatchHandle B, int slot, int n, int64_t nnz, int ell, const int *r
   if (x0) B_CUDA(cudaMemcpyAsync(d.x, x0, 8 * n, cudaMemcpyHostToDevice, st));
   else B_CUDA(cudaMemsetAsync(d.x, 0, 8 * n, st));
   return finish_slot<T>(B, slot, d);
+}
+
+// True when every column lies within int16 of its row: the sliced-ELL
+// columns are then stored as 2-byte offsets (FE orderings are banded).
+bool offsets_fit_int16(int n, const int *rowptr, const int *col) {
+  for (int i = 0; i < n; ++i)
+    for (int j = rowptr[i]; j < rowptr[i + 1]; ++j) {
+      const int d = col[j] - i;
+      if (d < -32768 || d > 32767) return false;
+    }
+  return true;
+}
+
+// Q1 rows couple nodes at most one cell away: offset (m + 1) + 1 in 2D,
+// m^2 + m + 1 in 3D, with m = cells + 1 nodes per axis.
+bool q1_col16(int dim, int cells) {
+  const int64_t m = (int64_t)cells + 1;
+  const int64_t d = dim == 2 ? m + 1 : m * m + m + 1;
+  return d <= 32767;
 }
 
 int kernel_grid(b200la_ctx c, const void *k, int *grid) {
@@ -652,15 +856,27 @@ int pass_grids(BatchHandle B, int g[3]) {
   return B200LA_OK;
 }
 
+// Resident warps of each pass kernel's grid (the adaptive item rule).
+int grid_warps(BatchHandle B) {
+  int g[3] = {1, 1, 1};
+  const bool pre = B->kp.precond != 0;
+  int rc;
+  if (B->kp.mixed) rc = pre ? pass_grids<float, true, true>(B, g) : pass_grids<float, false, true>(B, g);
+  else rc = pre ? pass_grids<double, true, true>(B, g) : pass_grids<double, false, true>(B, g);
+  B_TRY(rc);
+  for (int k = 0; k < 3; ++k) B->warps[k] = g[k] * (kBlock / 32);
+  return B200LA_OK;
+}
+
 // One pass (K1 K2 K3) on stream st: captured into the graph body, or
 // launched from the host loop when graphs are off.
 template <typename T, bool PRE, bool IN_GRAPH>
 void launch_pass(BatchHandle B, const int g[3], cudaStream_t st, cudaGraphConditionalHandle h) {
   const SysDesc<T> *desc = (const SysDesc<T> *)B->desc;
-  const int64_t ps = B->max_tiles;
-  batch_spmv_kernel<T, PRE><<<g[0], kBlock, 0, st>>>(B->tiles, desc, B->st, B->part, ps, B->glob, B->kp);
-  batch_update_kernel<T, PRE><<<g[1], kBlock, 0, st>>>(B->tiles, desc, B->st, B->part, ps, B->glob, B->kp);
-  batch_direction_kernel<T, PRE, IN_GRAPH><<<g[2], kBlock, 0, st>>>(B->tiles, desc, B->st, B->part, ps, B->glob,
+  const ItemList &a = B->lst[0], &b = B->lst[1], &c = B->lst[2];
+  batch_spmv_kernel<T, PRE><<<g[0], kBlock, 0, st>>>(a.dev, desc, B->st, a.part, a.cap, B->glob, B->kp);
+  batch_update_kernel<T, PRE><<<g[1], kBlock, 0, st>>>(b.dev, desc, B->st, b.part, b.cap, B->glob, B->kp);
+  batch_direction_kernel<T, PRE, IN_GRAPH><<<g[2], kBlock, 0, st>>>(c.dev, desc, B->st, c.part, c.cap, B->glob,
                                                                     B->kp, h);
 }
 
@@ -737,19 +953,21 @@ int host_loop(BatchHandle B) {
   return pre ? host_loop_t<double, true>(B) : host_loop_t<double, false>(B);
 }
 
-// Grows the tile and partial arrays to hold nt tiles (the graph bakes their
-// addresses in, so it is rebuilt after a reallocation).
-int ensure_tiles(BatchHandle B, int64_t nt) {
-  if (nt <= B->max_tiles) return B200LA_OK;
+// Grows list k's item and partial arrays to hold nt items (the graph bakes
+// their addresses in, so it is rebuilt after a reallocation).
+int ensure_items(BatchHandle B, int k, int64_t nt) {
+  ItemList &L = B->lst[k];
+  if (nt <= L.cap) return B200LA_OK;
   cudaStream_t st = B->ctx->stream;
-  const int64_t cap = std::max<int64_t>(nt, 2 * B->max_tiles);
-  if (B->tiles) cudaFreeAsync(B->tiles, st);
-  if (B->part) cudaFreeAsync(B->part, st);
-  B->tiles = nullptr;
-  B->part = nullptr;
-  B_CUDA(cudaMallocAsync(&B->tiles, sizeof(Tile) * cap, st));
-  B_CUDA(cudaMallocAsync(&B->part, sizeof(double) * 3 * cap, st));
-  B->max_tiles = cap;
+  const int64_t cap = std::max<int64_t>(nt, 2 * L.cap);
+  if (L.dev) cudaFreeAsync(L.dev, st);
+  if (L.part) cudaFreeAsync(L.part, st);
+  L.dev = nullptr;
+  L.part = nullptr;
+  L.cap = 0;
+  B_CUDA(cudaMallocAsync(&L.dev, sizeof(Tile) * cap, st));
+  B_CUDA(cudaMallocAsync(&L.part, sizeof(double) * 3 * cap, st));
+  L.cap = cap;
   if (B->exec) {
     cudaGraphExecDestroy(B->exec);
     B->exec = nullptr;
@@ -757,35 +975,65 @@ int ensure_tiles(BatchHandle B, int64_t nt) {
   return B200LA_OK;
 }
 
-// Tile list of the given slots (all used slots, or only those still running).
+// Both item lists over the given slots (all used slots, or only those still
+// running); writes the slot count and the SpMV's algorithmic bytes.
 int upload_tiles(BatchHandle B, bool running_only, int *count, int64_t *alg_bytes) {
-  B->tiles_host.clear();
+  for (ItemList &L : B->lst) L.host.clear();
   int act = 0;
   int64_t bytes = 0;
   const int64_t vb = B->kp.mixed ? 4 : 8;
+  std::vector<int> run;
   for (int s = 0; s < B->capacity; ++s) {
     const HostSys &h = B->sys[s];
     if (!h.used) continue;
     const int ph = B->st_host[s].phase;
     if (running_only && (ph == PH_DONE || ph == PH_EMPTY)) continue;
     ++act;
-    const int tiles = (h.n + B->tile_rows - 1) / B->tile_rows;
-    const int first = (int)B->tiles_host.size();
-    for (int k = 0; k < tiles; ++k) {
-      const int row0 = k * B->tile_rows;
-      B->tiles_host.push_back(Tile{s, row0, std::min(B->tile_rows, h.n - row0), first, tiles, 0});
-    }
+    run.push_back(s);
     bytes += (int64_t)h.nnz * (vb + 4) + (int64_t)(h.n + 1) * 4 + 2 * (int64_t)h.n * vb;
   }
-  const int64_t nt = (int64_t)B->tiles_host.size();
-  B_TRY(ensure_tiles(B, nt));
+  if (B->adaptive && !B->warps[0]) B_TRY(grid_warps(B));
+  for (int k = 0; k < 3; ++k) {
+    ItemList &L = B->lst[k];
+    // adaptive: halve the item (down to one 32-row slice) while the list
+    // would give the kernel's warps fewer than two items each, so a lightly
+    // loaded pass is not bound by one warp's long serial chain
+    int rows = L.rows;
+    if (B->adaptive)
+      while (rows > 32) {
+        int64_t items = 0;
+        for (int s : run) items += (B->sys[s].n + rows - 1) / rows;
+        if (items >= 2 * (int64_t)B->warps[k]) break;
+        rows = std::max(32, (rows / 2) & ~31);
+      }
+    L.used = rows;
+    for (int s : run)
+      for (int row0 = 0; row0 < B->sys[s].n; row0 += rows) L.host.push_back(Tile{s, row0});
+  }
   cudaStream_t st = B->ctx->stream;
-  if (nt) B_CUDA(cudaMemcpyAsync(B->tiles, B->tiles_host.data(), sizeof(Tile) * nt, cudaMemcpyHostToDevice, st));
-  // the staging vector must outlive the copy
+  for (int k = 0; k < 3; ++k) {
+    ItemList &L = B->lst[k];
+    const int64_t nt = (int64_t)L.host.size();
+    B_TRY(ensure_items(B, k, nt));
+    if (nt) B_CUDA(cudaMemcpyAsync(L.dev, L.host.data(), sizeof(Tile) * nt, cudaMemcpyHostToDevice, st));
+  }
+  // the staging vectors must outlive the copies
   B_CUDA(cudaStreamSynchronize(st));
   *count = act;
   if (alg_bytes) *alg_bytes = bytes;
   return B200LA_OK;
+}
+
+// Host globals of a launch over the current lists.
+void set_globals(BatchHandle B, int active, int max_passes) {
+  BatchGlobals &g = *B->glob_host;
+  memset(&g, 0, sizeof(g));
+  g.active = active;
+  g.max_passes = max_passes;
+  for (int k = 0; k < 3; ++k) {
+    g.ntiles[k] = (int)B->lst[k].host.size();
+    g.tile_rows[k] = B->lst[k].used;
+  }
 }
 
 int find_free_slot(BatchHandle B) {
@@ -797,16 +1045,17 @@ int find_free_slot(BatchHandle B) {
 template <typename T>
 int time_plain(BatchHandle B, int reps, float *ms) {
   cudaStream_t st = B->ctx->stream;
-  const int nt = (int)B->tiles_host.size();
+  const ItemList &L = B->lst[0];
+  const int nt = (int)L.host.size();
   int grid = 1;
   B_TRY(kernel_grid(B->ctx, (const void *)batch_spmv_plain_kernel<T>, &grid));
   const SysDesc<T> *desc = (const SysDesc<T> *)B->desc;
-  batch_spmv_plain_kernel<T><<<grid, kBlock, 0, st>>>(B->tiles, nt, desc);
+  batch_spmv_plain_kernel<T><<<grid, kBlock, 0, st>>>(L.dev, nt, L.used, desc);
   cudaEvent_t e0, e1;
   B_CUDA(cudaEventCreate(&e0));
   B_CUDA(cudaEventCreate(&e1));
   B_CUDA(cudaEventRecord(e0, st));
-  for (int r = 0; r < reps; ++r) batch_spmv_plain_kernel<T><<<grid, kBlock, 0, st>>>(B->tiles, nt, desc);
+  for (int r = 0; r < reps; ++r) batch_spmv_plain_kernel<T><<<grid, kBlock, 0, st>>>(L.dev, nt, L.used, desc);
   B_CUDA(cudaEventRecord(e1, st));
   B_CUDA(cudaEventSynchronize(e1));
   B_CUDA(cudaEventElapsedTime(ms, e0, e1));
@@ -814,6 +1063,123 @@ int time_plain(BatchHandle B, int reps, float *ms) {
   cudaEventDestroy(e1);
   B_CUDA(cudaGetLastError());
   *ms /= reps;
+  return B200LA_OK;
+}
+
+// Pass timing (instrumentation and the tuner): over the current item list,
+// one untimed pass, then `reps` passes timed kernel by kernel with CUDA
+// events on the context stream; ms[k] is the mean time of K1/K2/K3.  The
+// passes advance the systems like a run does.
+template <typename T, bool PRE>
+int time_passes_t(BatchHandle B, int reps, double ms[3]) {
+  cudaStream_t st = B->ctx->stream;
+  // `active` is only read by the end-of-pass test, which host mode ignores
+  set_globals(B, B->capacity, 1 << 30);
+  B_CUDA(cudaMemcpyAsync(B->glob, B->glob_host, sizeof(BatchGlobals), cudaMemcpyHostToDevice, st));
+  int grids[3] = {1, 1, 1};
+  B_TRY((pass_grids<T, PRE, false>(B, grids)));
+  const SysDesc<T> *desc = (const SysDesc<T> *)B->desc;
+  const ItemList &a = B->lst[0], &b = B->lst[1], &c = B->lst[2];
+  batch_start_kernel<<<1, 1, 0, st>>>(B->glob);
+  launch_pass<T, PRE, false>(B, grids, st, 0);
+  cudaEvent_t ev[4];
+  for (auto &e : ev) B_CUDA(cudaEventCreate(&e));
+  double acc[3] = {0.0, 0.0, 0.0};
+  int rc = B200LA_OK;
+  for (int r = 0; r < reps && rc == B200LA_OK; ++r) {
+    cudaEventRecord(ev[0], st);
+    batch_spmv_kernel<T, PRE><<<grids[0], kBlock, 0, st>>>(a.dev, desc, B->st, a.part, a.cap, B->glob, B->kp);
+    cudaEventRecord(ev[1], st);
+    batch_update_kernel<T, PRE><<<grids[1], kBlock, 0, st>>>(b.dev, desc, B->st, b.part, b.cap, B->glob, B->kp);
+    cudaEventRecord(ev[2], st);
+    batch_direction_kernel<T, PRE, false><<<grids[2], kBlock, 0, st>>>(c.dev, desc, B->st, c.part, c.cap, B->glob,
+                                                                        B->kp, 0);
+    cudaEventRecord(ev[3], st);
+    if (cudaEventSynchronize(ev[3]) != cudaSuccess) {
+      rc = fail(B200LA_ERR_CUDA, "batch pass timing: %s", cudaGetErrorString(cudaGetLastError()));
+      break;
+    }
+    for (int k = 0; k < 3; ++k) {
+      float t = 0.f;
+      cudaEventElapsedTime(&t, ev[k], ev[k + 1]);
+      acc[k] += t;
+    }
+  }
+  for (auto &e : ev) cudaEventDestroy(e);
+  B_TRY(rc);
+  B_CUDA(cudaGetLastError());
+  for (int k = 0; k < 3; ++k) ms[k] = acc[k] / reps;
+  return B200LA_OK;
+}
+
+// Device copy of every used slot's carried state (SysState array and the
+// x, c, r, p vectors), for the tuner.
+struct Snapshot {
+  SysState *st = nullptr;
+  void *buf = nullptr;  // [slots int][offs int64][x double][c r p T]
+  int nslots = 0;
+};
+
+template <typename T>
+int snapshot_copy_t(BatchHandle B, const Snapshot &sn, int save) {
+  const int *slots = (const int *)sn.buf;
+  const int64_t *offs = (const int64_t *)((char *)sn.buf + align256(sizeof(int) * sn.nslots));
+  double *xs = (double *)((char *)offs + align256(sizeof(int64_t) * sn.nslots));
+  int64_t n = 0;
+  for (const HostSys &h : B->sys)
+    if (h.used) n += h.n;
+  T *vs = (T *)((char *)xs + align256(sizeof(double) * n));
+  slot_snapshot_kernel<T><<<sn.nslots, kBlock, 0, B->ctx->stream>>>(slots, offs, (const SysDesc<T> *)B->desc, xs,
+                                                                      vs, save);
+  B_CUDA(cudaGetLastError());
+  return B200LA_OK;
+}
+
+void snapshot_free(BatchHandle B, Snapshot *sn) {
+  cudaStream_t st = B->ctx->stream;
+  if (sn->st) cudaFreeAsync(sn->st, st);
+  if (sn->buf) cudaFreeAsync(sn->buf, st);
+  cudaStreamSynchronize(st);
+  *sn = Snapshot();
+}
+
+int snapshot_save(BatchHandle B, Snapshot *sn) {
+  cudaStream_t st = B->ctx->stream;
+  std::vector<int> slots;
+  std::vector<int64_t> offs;
+  int64_t n = 0;
+  for (int s = 0; s < B->capacity; ++s)
+    if (B->sys[s].used) {
+      slots.push_back(s);
+      offs.push_back(n);
+      n += B->sys[s].n;
+    }
+  sn->nslots = (int)slots.size();
+  if (!sn->nslots) return B200LA_OK;
+  const size_t tb = B->kp.mixed ? 4 : 8;
+  const size_t bytes = align256(sizeof(int) * slots.size()) + align256(sizeof(int64_t) * slots.size()) +
+                       align256(sizeof(double) * n) + 3 * tb * (size_t)n;
+  if (cudaMallocAsync(&sn->st, sizeof(SysState) * B->capacity, st) != cudaSuccess ||
+      cudaMallocAsync(&sn->buf, bytes, st) != cudaSuccess) {
+    snapshot_free(B, sn);
+    return fail(B200LA_ERR_NOMEM, "batch_tune: no room for the state snapshot (%zu bytes)", bytes);
+  }
+  const int64_t *doffs = (const int64_t *)((char *)sn->buf + align256(sizeof(int) * slots.size()));
+  B_CUDA(cudaMemcpyAsync(sn->buf, slots.data(), sizeof(int) * slots.size(), cudaMemcpyHostToDevice, st));
+  B_CUDA(cudaMemcpyAsync((void *)doffs, offs.data(), sizeof(int64_t) * offs.size(), cudaMemcpyHostToDevice, st));
+  B_CUDA(cudaMemcpyAsync(sn->st, B->st, sizeof(SysState) * B->capacity, cudaMemcpyDeviceToDevice, st));
+  B_TRY(B->kp.mixed ? snapshot_copy_t<float>(B, *sn, 1) : snapshot_copy_t<double>(B, *sn, 1));
+  // the host vectors must outlive the copies
+  B_CUDA(cudaStreamSynchronize(st));
+  return B200LA_OK;
+}
+
+int snapshot_restore(BatchHandle B, const Snapshot &sn) {
+  if (!sn.nslots) return B200LA_OK;
+  cudaStream_t st = B->ctx->stream;
+  B_CUDA(cudaMemcpyAsync(B->st, sn.st, sizeof(SysState) * B->capacity, cudaMemcpyDeviceToDevice, st));
+  B_TRY(B->kp.mixed ? snapshot_copy_t<float>(B, sn, 0) : snapshot_copy_t<double>(B, sn, 0));
+  B_CUDA(cudaStreamSynchronize(st));
   return B200LA_OK;
 }
 
@@ -835,9 +1201,13 @@ int b200la_batch_destroy(b200la_batch B) {
   if (B->graph) cudaGraphDestroy(B->graph);
   for (HostSys &h : B->sys)
     if (h.chunk) cudaFreeAsync(h.chunk, st);
-  void *bufs[] = {B->desc, B->st, B->tiles, B->part, B->glob};
+  void *bufs[] = {B->desc, B->st, B->glob};
   for (void *p : bufs)
     if (p) cudaFreeAsync(p, st);
+  for (ItemList &L : B->lst) {
+    if (L.dev) cudaFreeAsync(L.dev, st);
+    if (L.part) cudaFreeAsync(L.part, st);
+  }
   if (B->st_host) cudaFreeHost(B->st_host);
   if (B->glob_host) cudaFreeHost(B->glob_host);
   cudaStreamSynchronize(st);
@@ -852,6 +1222,8 @@ int b200la_batch_create(b200la_ctx ctx, const b200la_batch_params *p, b200la_bat
   B_CHECK(p->inner_maxits >= 1 && p->inner_maxits <= 10000000, B200LA_ERR_INVALID, "batch_create: inner_maxits");
   B_CHECK(p->atol >= 0 && p->rtol >= 0 && p->dtol > 0, B200LA_ERR_INVALID, "batch_create: tolerances");
   B_CHECK(!p->mixed || (p->inner_rtol > 0 && p->inner_rtol < 1), B200LA_ERR_INVALID, "batch_create: inner_rtol");
+  B_CHECK(p->index_bits == 0 || p->index_bits == 32, B200LA_ERR_INVALID, "batch_create: index_bits %d (0 or 32)",
+          p->index_bits);
   B_CHECK(p->tile_rows == 0 || (p->tile_rows >= 32 && p->tile_rows <= 65536 && p->tile_rows % 32 == 0),
           B200LA_ERR_INVALID, "batch_create: tile_rows %d (32..65536, multiple of 32)", p->tile_rows);
   b200la_batch B = new b200la_batch_s();
@@ -859,7 +1231,10 @@ int b200la_batch_create(b200la_ctx ctx, const b200la_batch_params *p, b200la_bat
   B->prm = *p;
   B->kp = BatchParams{p->max_outer, p->inner_maxits, p->atol, p->rtol, p->dtol, p->inner_rtol, p->precond ? 1 : 0,
                       p->mixed ? 1 : 0};
-  B->tile_rows = p->tile_rows ? p->tile_rows : 2048;
+  // K1 sweeps 256-row items (8 slices per warp keep its gather chains
+  // short); K2 streams 1024-row items, K3 512; the tuner may change them
+  for (int k = 0; k < 3; ++k) B->lst[k].rows = p->tile_rows ? p->tile_rows : kDefaultRows[k];
+  B->adaptive = false;
   B->capacity = p->capacity;
   B->sys.resize(p->capacity);
   cudaStream_t st = ctx->stream;
@@ -898,8 +1273,9 @@ int b200la_batch_add(b200la_batch B, int n, int64_t nnz, const int *rowptr, cons
   h.n = n;
   h.nnz = (int)nnz;
   const int ell = std::max(max_row, 1);
-  const int rc = B->kp.mixed ? add_typed<float>(B, slot, n, nnz, ell, rowptr, col, val, b, x0)
-                             : add_typed<double>(B, slot, n, nnz, ell, rowptr, col, val, b, x0);
+  const bool col16 = B->prm.index_bits != 32 && offsets_fit_int16(n, rowptr, col);
+  const int rc = B->kp.mixed ? add_typed<float>(B, slot, n, nnz, ell, col16, rowptr, col, val, b, x0)
+                             : add_typed<double>(B, slot, n, nnz, ell, col16, rowptr, col, val, b, x0);
   if (rc != B200LA_OK) {
     if (h.chunk) cudaFreeAsync(h.chunk, B->ctx->stream);
     h = HostSys();
@@ -929,7 +1305,7 @@ int b200la_batch_add_q1(b200la_batch B, int dim, int cells, uint64_t seed, doubl
   auto go = [&](auto tag) -> int {
     using T = decltype(tag);
     SysDesc<T> d{};
-    B_TRY(alloc_slot<T>(B, slot, n, nnz, ell, &d));
+    B_TRY(alloc_slot<T>(B, slot, n, nnz, ell, B->prm.index_bits != 32 && q1_col16(dim, cells), &d));
     B_TRY(q1_assemble(st, B->ctx->num_sms, dim, cells, seed, sigma, (int *)d.rowptr, (int *)d.col,
                       (double *)d.val64, (double *)d.b));
     B_CUDA(cudaMemsetAsync(d.x, 0, 8 * (size_t)n, st));
@@ -996,10 +1372,7 @@ int b200la_batch_run(b200la_batch B, int max_passes, int *active_out) {
     return B200LA_OK;
   }
   if (B->ctx->use_graphs && !B->exec) B_TRY(build_graph(B));
-  memset(&g, 0, sizeof(g));
-  g.active = active;
-  g.max_passes = max_passes;
-  g.ntiles = (int)B->tiles_host.size();
+  set_globals(B, active, max_passes);
   B_CUDA(cudaMemcpyAsync(B->glob, &g, sizeof(BatchGlobals), cudaMemcpyHostToDevice, st));
   if (B->ctx->use_graphs) B_CUDA(cudaGraphLaunch(B->exec, st));
   else B_TRY(host_loop(B));
@@ -1094,18 +1467,115 @@ int b200la_batch_restart(b200la_batch B) {
   return B200LA_OK;
 }
 
-int b200la_batch_tune(b200la_batch B, int *lanes_out, double *usec) {
+int b200la_batch_set_items(b200la_batch B, int rows_spmv, int rows_update, int rows_direction, int adaptive) {
+  B_CHECK(B, B200LA_ERR_INVALID, "batch_set_items: null batch");
+  const int r[3] = {rows_spmv, rows_update, rows_direction};
+  for (int k = 0; k < 3; ++k)
+    B_CHECK(r[k] >= 32 && r[k] <= 65536 && r[k] % 32 == 0, B200LA_ERR_INVALID,
+            "batch_set_items: %d rows (32..65536, multiple of 32)", r[k]);
+  for (int k = 0; k < 3; ++k) B->lst[k].rows = r[k];
+  B->adaptive = adaptive != 0;
+  return B200LA_OK;
+}
+
+int b200la_batch_get_items(b200la_batch B, int *rows) {
+  B_CHECK(B && rows, B200LA_ERR_INVALID, "batch_get_items: null argument");
+  for (int k = 0; k < 3; ++k) rows[k] = B->lst[k].rows;
+  return B200LA_OK;
+}
+
+int b200la_batch_tune(b200la_batch B, int *rows, double *usec) {
   B_CHECK(B, B200LA_ERR_INVALID, "batch_tune: null batch");
-  // Both SpMVs use the sliced-ELL layout (one row per lane, coalesced steps),
-  // which leaves no free parameter for these matrices; the time of the inner
-  // SpMV over the running systems is reported.
+  // Both SpMVs use the sliced-ELL layout (one row per lane, 32-row slices,
+  // coalesced steps).  The free parameters are the item sizes: rows per
+  // warp work item of K1 (SpMV), K2 (update and dots) and K3 (direction).
+  // Small items give more independent warps, short serial chains and
+  // balance when few large systems run; large items amortise the per-item
+  // record, state and reduction.  Unless the batch was created with a fixed
+  // tile_rows, each candidate set is timed on real passes over the running
+  // systems (each kernel's time depends only on its own item size, so every
+  // kernel picks its own best), and every system's carried state (x, c, r,
+  // p and its scalars) is restored after each trial.  Each kernel keeps the
+  // smallest item within 3% of its best time: mid-solve passes, where
+  // finished systems and residual passes mix in, favour short items.
+  static const int cand[4][3] = {{128, 256, 256}, {256, 512, 512}, {512, 1024, 1024}, {1024, 2048, 2048}};
   int active = 0;
   B_TRY(upload_tiles(B, true, &active, nullptr));
-  float ms = 0.f;
-  if (active) B_TRY(B->kp.mixed ? time_plain<float>(B, 5, &ms) : time_plain<double>(B, 5, &ms));
-  if (lanes_out) *lanes_out = 0;
-  if (usec) *usec = 1000.0 * ms;
+  double best_ms = 0.0;
+  if (active) {
+    const bool pre = B->kp.precond != 0;
+    auto trial = [&](double *k) -> int {
+      if (B->kp.mixed) return pre ? time_passes_t<float, true>(B, 3, k) : time_passes_t<float, false>(B, 3, k);
+      return pre ? time_passes_t<double, true>(B, 3, k) : time_passes_t<double, false>(B, 3, k);
+    };
+    Snapshot snap;
+    B_TRY(snapshot_save(B, &snap));
+    int rc = B200LA_OK;
+    if (B->prm.tile_rows == 0) {
+      double t[4][3];
+      for (int c = 0; c < 4 && rc == B200LA_OK; ++c) {
+        for (int k = 0; k < 3; ++k) B->lst[k].rows = cand[c][k];
+        rc = upload_tiles(B, true, &active, nullptr);
+        if (rc == B200LA_OK) rc = trial(t[c]);
+        if (rc == B200LA_OK) rc = snapshot_restore(B, snap);
+      }
+      if (rc == B200LA_OK) {
+        for (int k = 0; k < 3; ++k) {
+          int best = 0;
+          for (int c = 1; c < 4; ++c)
+            if (t[c][k] < t[best][k]) best = c;
+          for (int c = 0; c < best; ++c)
+            if (t[c][k] <= 1.03 * t[best][k]) {
+              best = c;
+              break;
+            }
+          B->lst[k].rows = cand[best][k];
+          best_ms += t[best][k];
+        }
+        rc = upload_tiles(B, true, &active, nullptr);
+      }
+    } else {
+      double k[3] = {0, 0, 0};
+      rc = trial(k);
+      if (rc == B200LA_OK) rc = snapshot_restore(B, snap);
+      best_ms = k[0] + k[1] + k[2];
+    }
+    snapshot_free(B, &snap);
+    B_TRY(rc);
+  }
+  if (rows)
+    for (int k = 0; k < 3; ++k) rows[k] = B->lst[k].rows;
+  if (usec) *usec = 1000.0 * best_ms;
   return B200LA_OK;
+}
+
+int b200la_batch_profile_pass(b200la_batch B, int reps, double *ms, int64_t *algorithmic_bytes) {
+  B_CHECK(B && ms && reps >= 1 && reps <= 16, B200LA_ERR_INVALID, "batch_profile_pass: bad argument (reps 1..16)");
+  B_TRY(b200la_batch_restart(B));
+  int count = 0;
+  B_TRY(upload_tiles(B, false, &count, nullptr));
+  for (int k = 0; k < 3; ++k) ms[k] = 0.0;
+  int64_t n = 0, nnz = 0;
+  for (const HostSys &h : B->sys)
+    if (h.used) {
+      n += h.n;
+      nnz += h.nnz;
+    }
+  const int64_t tb = B->kp.mixed ? 4 : 8;
+  const int64_t vecs_k2 = B->kp.precond ? 7 : 6, vecs_k3 = B->kp.precond ? 4 : 3;
+  if (algorithmic_bytes) {
+    algorithmic_bytes[0] = nnz * (tb + 4) + (n + count) * 4 + 2 * n * tb;
+    algorithmic_bytes[1] = vecs_k2 * n * tb;
+    algorithmic_bytes[2] = vecs_k3 * n * tb;
+  }
+  if (count) {
+    const bool pre = B->kp.precond != 0;
+    int rc;
+    if (B->kp.mixed) rc = pre ? time_passes_t<float, true>(B, reps, ms) : time_passes_t<float, false>(B, reps, ms);
+    else rc = pre ? time_passes_t<double, true>(B, reps, ms) : time_passes_t<double, false>(B, reps, ms);
+    B_TRY(rc);
+  }
+  return b200la_batch_restart(B);
 }
 
 int b200la_batch_profile(b200la_batch B, int reps, double *ms_spmv, int64_t *algorithmic_bytes) {

@@ -6,7 +6,9 @@ launches (no CUDA graph), so a profiler sees every launch on its own.
 
 With --batch N: builds the standard batch of N 2D systems and solves it
 twice (the launches of interest are those of the second solve; set
-B200LA_GRAPHS=0 so the kernels launch one by one).
+B200LA_GRAPHS=0 so the kernels launch one by one).  With --profile-only the
+solves are skipped: one restart pass (K1 K2 K3) is followed by three timed
+inner passes (K1 K2 K3 each), the launches a profiler should capture.
 
 Launch order: the tuner's SpMV launches (unless a schedule is given), then
 `--spmv-reps` plain SpMV launches (spmv_kernel), then the CG init kernel and
@@ -39,6 +41,11 @@ def main():
                     help="instead: solve a batch of this many 2D systems (n~logU[16,256], sigma 1) twice")
     ap.add_argument("--chunk", type=int, default=32)
     ap.add_argument("--tile-rows", type=int, default=0)
+    ap.add_argument("--index-bits", type=int, default=0, choices=[0, 32],
+                    help="batch: sliced-ELL columns (0 = int16 offsets when they fit, 32 = int32)")
+    ap.add_argument("--items", default="", help="batch: K1,K2,K3 item rows instead of tuning")
+    ap.add_argument("--profile-only", action="store_true",
+                    help="batch: skip the solves; time one inner pass kernel by kernel (b200la_batch_profile_pass)")
     a = ap.parse_args()
     if a.batch:
         return batch_case(a)
@@ -82,10 +89,21 @@ def batch_case(a):
     systems = P.batch_systems(a.batch, sigma=1.0, seed=P.SEED_BATCH)
     plat = lmp.init_platform(0)
     B = Batch(len(systems), mixed=True, precond=True, rtol=1e-8, inner_rtol=1e-4, tile_rows=a.tile_rows,
-              platform=plat)
+              index_bits=a.index_bits, platform=plat)
     for s in systems:
         B.add_system(s)
-    B.tune()
+    if a.items:
+        B.set_items(*[int(v) for v in a.items.split(",")], adaptive=False)
+        print(f"item rows (K1, K2, K3) {B.items()}")
+    else:
+        rows, us = B.tune()
+        print(f"tuned item rows (K1, K2, K3) {rows}: pass {us:.1f} us")
+    if a.profile_only:
+        # launch order: K1 K2 K3 of the restart pass, then K1 K2 K3 per timed pass
+        ms, nb = B.profile_pass(3)
+        for name, t, b in zip(("K1 spmv+p.Ap", "K2 update", "K3 direction"), ms, nb):
+            print(f"{name}: {t * 1e3:.1f} us, algorithmic {b} bytes -> {b / t / 1e6:.1f} GB/s")
+        return
     for _ in range(2):
         B.restart()
         t = time.perf_counter()

@@ -255,8 +255,10 @@ typedef struct {
   int max_outer;      /* refinement passes (mixed) */
   int inner_maxits;   /* iterations per inner solve (FP64 mode: per solve) */
   int lanes;          /* reserved: 0 (both SpMVs use the sliced-ELL layout) */
-  int tile_rows;      /* rows per tile, a multiple of 32 (0 = 2048) */
-  int reserved;
+  int tile_rows;      /* rows per warp work item of every kernel, a multiple of 32
+                         (0 = 256 SpMV, 1024 update, 512 direction; tunable) */
+  int index_bits;     /* sliced-ELL column storage: 0 = int16 offsets from the row when
+                         every column is within int16 of its row, else int32; 32 = int32 */
   double atol, rtol, dtol;  /* test on ||b - A x||_2 (FP64 mode: the CG recurrence residual) */
   double inner_rtol;        /* mixed: inner solve stops at inner_rtol x its start residual */
 } b200la_batch_params;
@@ -305,13 +307,33 @@ int b200la_batch_result(b200la_batch b, int slot, double *x, b200la_sys_result *
 int b200la_batch_info(b200la_batch b, int *used_slots, int64_t *device_bytes);
 /* Restart every system in the batch from x = 0 (matrices and RHS stay). */
 int b200la_batch_restart(b200la_batch b);
-/* Times the inner solve's batched sliced-ELL SpMV over the running systems
- * (microseconds per launch); `lanes` is reserved (writes 0). */
-int b200la_batch_tune(b200la_batch b, int *lanes, double *usec);
+/* Work is split into warp items of consecutive rows; K1 (the SpMV), K2 (the
+ * update and its dot products) and K3 (the direction update) each have
+ * their own item size.  set_items sets them (multiples of 32 rows; they take
+ * effect at the next run); with adaptive = 1 each run halves a kernel's
+ * item, down to 32 rows, while the running systems would give its warps
+ * fewer than two items each (off by default: measured slower on the
+ * standard batch).  get_items writes the three sizes. */
+int b200la_batch_set_items(b200la_batch b, int rows_spmv, int rows_update, int rows_direction, int adaptive);
+int b200la_batch_get_items(b200la_batch b, int *rows /* [3] */);
+/* Autotuner: unless the batch was created with a fixed tile_rows, times
+ * candidate item sizes (K1 128..1024, K2/K3 256..2048 rows) on real passes
+ * over the running systems, whose carried state is restored after every
+ * trial, and keeps each kernel's fastest.  Writes the three item sizes and
+ * the pass time (microseconds, K1 + K2 + K3). */
+int b200la_batch_tune(b200la_batch b, int *rows /* [3] */, double *usec);
 /* Instrumentation: mean milliseconds of the inner solve's batched SpMV over
  * every slot (reps launches, CUDA events) and its algorithmic bytes:
  * sum over systems of nnz*(value+4) + (n+1)*4 + 2*n*value. */
 int b200la_batch_profile(b200la_batch b, int reps, double *ms_spmv, int64_t *algorithmic_bytes);
+/* Instrumentation of the solver's own kernels: restarts every system from
+ * x = 0, takes one pass, then times `reps` (1..16) inner passes kernel by
+ * kernel with CUDA events -- ms[0] K1 (SpMV + p.Ap), ms[1] K2 (c, r update
+ * + r.r, r.z), ms[2] K3 (direction update) -- and restarts again.  bytes[k]
+ * are each kernel's algorithmic bytes per launch over every slot:
+ * K1 nnz*(value+4) + (n+1)*4 + 2*n*value; K2 7*n*value (Jacobi) or 6;
+ * K3 4*n*value (Jacobi) or 3. */
+int b200la_batch_profile_pass(b200la_batch b, int reps, double *ms, int64_t *bytes);
 
 /* ---- request loop (no reference counterpart) ------------------------------
  * A server owns one batch and a worker thread.  Submitted solves wait in a
