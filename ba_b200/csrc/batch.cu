@@ -1498,7 +1498,10 @@ int b200la_batch_tune(b200la_batch B, int *rows, double *usec) {
   // p and its scalars) is restored after each trial.  Each kernel keeps the
   // smallest item within 3% of its best time: mid-solve passes, where
   // finished systems and residual passes mix in, favour short items.
-  static const int cand[4][3] = {{128, 256, 256}, {256, 512, 512}, {512, 1024, 1024}, {1024, 2048, 2048}};
+  // K1 is held to 128..256 rows: fresh passes (what a trial times) favour
+  // larger K1 items, but whole solves, where residual items (FP64, about
+  // twice the work) and finished systems mix in, were measured faster at 256
+  static const int cand[4][3] = {{128, 256, 256}, {256, 512, 512}, {256, 1024, 1024}, {256, 2048, 2048}};
   int active = 0;
   B_TRY(upload_tiles(B, true, &active, nullptr));
   double best_ms = 0.0;

@@ -1,0 +1,62 @@
+"""Host-side helpers for running the path on several GPUs, one process per
+GPU (torch.distributed; NCCL on GPUs, gloo in the CPU tests).
+
+Every workload of the path is a set of independent solves, so ranks never
+exchange solver data: each rank owns its share of the systems (or its own
+seeded batch / request stream) and only one scalar -- the step time -- is
+reduced, as the maximum over ranks.  The reference's multi-rank path
+(CoupledVector/CoupledMatrix halos, linear_algebra/coupled_vector.cc:890-973)
+partitions one system by rows; that split is not built here.
+"""
+from __future__ import annotations
+
+import heapq
+
+SEED_STRIDE = 7919  # a prime: per-rank seeds never collide with the per-system offsets (+1 .. +count)
+
+
+def rank_seed(base: int, rank: int) -> int:
+    """Seed of rank `rank`'s own batch or request stream."""
+    return int(base) + SEED_STRIDE * int(rank)
+
+
+def partition_by_cost(costs, world: int) -> list[list[int]]:
+    """Split items (e.g. systems weighted by nnz) over `world` ranks: longest
+    first, each to the least-loaded rank (ties to the lower rank), so every
+    rank gets a deterministic share within the largest item of the mean.
+    Returns the item indices of each rank in ascending order."""
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    order = sorted(range(len(costs)), key=lambda i: (-costs[i], i))
+    heap = [(0.0, r) for r in range(world)]
+    parts: list[list[int]] = [[] for _ in range(world)]
+    for i in order:
+        load, r = heapq.heappop(heap)
+        parts[r].append(i)
+        heapq.heappush(heap, (load + float(costs[i]), r))
+    return [sorted(p) for p in parts]
+
+
+def _reduce(value: float, op: str, device: str) -> float:
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(value)
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def max_over_ranks(value: float, device: str = "cuda") -> float:
+    """The maximum of `value` over all ranks (the value itself on one rank)."""
+    return _reduce(value, "max", device)
+
+
+def sum_over_ranks(value: float, device: str = "cuda") -> float:
+    return _reduce(value, "sum", device)
+
+
+def aggregate_rate(units_per_rank: float, world: int, max_ms: float) -> float:
+    """Whole-job throughput: every rank processed `units_per_rank` units and
+    the job took the slowest rank's time."""
+    return world * units_per_rank / (max_ms / 1e3)

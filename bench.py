@@ -41,6 +41,8 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from ba_b200 import dist as D  # noqa: E402  (host-side helpers only; no CUDA at import)
+
 METRIC = "PCG solves/s & p50/p99 latency at 1e-8 rel. residual vs plain FP64 GPU CG"
 COUNTS = os.path.join(ROOT, "tests", "golden", "workload_counts.json")
 BATCH_COUNT = 1024
@@ -142,7 +144,7 @@ def spmv_bytes(n: int, nnz: int, sv: int) -> int:
 # ----------------------------------------------------------------- batch workload
 def batch_seed(rank: int) -> int:
     from ba_b200 import problems as P
-    return P.SEED_BATCH + 7919 * rank
+    return D.rank_seed(P.SEED_BATCH, rank)
 
 
 def make_batch_systems(count: int, rank: int):
@@ -265,11 +267,7 @@ def run_batch(args, rank, local_rank, world, torch, dist, barrier):
     e1.synchronize()
     barrier()
     clk = clocks.stop()
-    ms = e0.elapsed_time(e1)
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    ms_max = D.max_over_ranks(e0.elapsed_time(e1))
     value = world * args.steps * len(systems) / (ms_max / 1e3)
 
     # per-system results of the last step: states, latency inside the step, accuracy
@@ -340,10 +338,7 @@ def run_batch(args, rank, local_rank, world, torch, dist, barrier):
         e2e_step()
     h1.record(stream)
     h1.synchronize()
-    te = torch.tensor([h0.elapsed_time(h1)], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * k_e2e * len(systems) / (float(te.item()) / 1e3)
+    e2e_value = D.aggregate_rate(k_e2e * len(systems), world, D.max_over_ranks(h0.elapsed_time(h1)))
     E.close()
 
     # roofline of the dominant kernel: K1 of the inner solve (batched FP32
@@ -405,7 +400,7 @@ def serve_requests(count: int, rate: float, hi_dofs: float, rank: int, offset: i
     """Requests offset..offset+count-1 of the seeded served stream (2D/3D Q1
     diffusion, DOFs log-uniform in [1e3, hi_dofs], sigma U[0.5, 2])."""
     from ba_b200 import problems as P
-    return P.serve_stream(offset + count, rate=rate, hi_dofs=hi_dofs, seed=P.SEED_SERVE + 7919 * rank)[offset:]
+    return P.serve_stream(offset + count, rate=rate, hi_dofs=hi_dofs, seed=D.rank_seed(P.SEED_SERVE, rank))[offset:]
 
 
 def serve_config(args, extra=None):
@@ -515,11 +510,7 @@ def run_serve(args, rank, local_rank, world, torch, dist, barrier):
     barrier()
     clk = clocks.stop()
     st_sat = S.stats()
-    ms = e0.elapsed_time(e1)
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    ms_max = D.max_over_ranks(e0.elapsed_time(e1))
     value = world * args.steps * R / (ms_max / 1e3)
     ok = sum(1 for r, _ in results if r.solver_state == 0)
     d2h = int(sum(r.x.nbytes for r, _ in results)) // args.steps
@@ -660,10 +651,7 @@ def run_poisson3d(args, rank, local_rank, world, torch, dist, barrier):
     e1.synchronize()
     barrier()
     clk = clocks.stop()
-    t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    ms_max = D.max_over_ranks(e0.elapsed_time(e1))
     value = world * args.steps / (ms_max / 1e3)
     step(plain)
     c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -686,10 +674,7 @@ def run_poisson3d(args, rank, local_rank, world, torch, dist, barrier):
         lib.b200la_vec_download(x.handle, C.c_void_p(xh.data_ptr()), n)
     h1.record(stream)
     h1.synchronize()
-    te = torch.tensor([h0.elapsed_time(h1)], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * args.steps / (float(te.item()) / 1e3)
+    e2e_value = D.aggregate_rate(args.steps, world, D.max_over_ranks(h0.elapsed_time(h1)))
     ms3 = (C.c_double * 3)()
     x.Zeros()
     lib.b200la_cg_profile(solver._solver, b.handle, x.handle, 20, ms3)

@@ -317,7 +317,7 @@ int b200la_batch_restart(b200la_batch b);
 int b200la_batch_set_items(b200la_batch b, int rows_spmv, int rows_update, int rows_direction, int adaptive);
 int b200la_batch_get_items(b200la_batch b, int *rows /* [3] */);
 /* Autotuner: unless the batch was created with a fixed tile_rows, times
- * candidate item sizes (K1 128..1024, K2/K3 256..2048 rows) on real passes
+ * candidate item sizes (K1 128..256, K2/K3 256..2048 rows) on real passes
  * over the running systems, whose carried state is restored after every
  * trial, and keeps each kernel's fastest.  Writes the three item sizes and
  * the pass time (microseconds, K1 + K2 + K3). */

@@ -1,0 +1,78 @@
+"""Multi-rank host logic on CPU: two gloo ranks, as bench.py runs one
+process per GPU.  Checks per-rank seeds, the cost-balanced partition, the
+max-over-ranks step time and the whole-job rate."""
+import json
+import os
+import socket
+
+import pytest
+import torch.multiprocessing as mp
+
+from ba_b200 import dist as D
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def _rank_main(rank, world, port, out_dir):
+    import datetime
+
+    import torch.distributed as dist
+
+    from ba_b200 import dist as D
+    from ba_b200 import problems as P
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        seed = D.rank_seed(P.SEED_BATCH, rank)
+        sizes = P.batch_sizes(64, seed=seed)
+        costs = [(int(n) + 1) ** 2 for n in sizes]
+        parts = D.partition_by_cost(costs, world)
+        my_ms = 100.0 + 25.0 * rank           # this rank's step time
+        mx = D.max_over_ranks(my_ms, device="cpu")
+        total = D.sum_over_ranks(len(sizes), device="cpu")
+        rate = D.aggregate_rate(len(sizes), world, mx)
+        dist.barrier()
+        with open(os.path.join(out_dir, f"rank{rank}.json"), "w") as f:
+            json.dump({"seed": seed, "sizes": [int(x) for x in sizes], "parts": parts, "max": mx,
+                       "total": total, "rate": rate}, f)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks(tmp_path):
+    world = 2
+    mp.start_processes(_rank_main, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True,
+                       start_method="spawn")
+    r = [json.load(open(tmp_path / f"rank{k}.json")) for k in range(world)]
+    # each rank has its own seeded batch
+    assert r[0]["seed"] != r[1]["seed"] and r[0]["sizes"] != r[1]["sizes"]
+    # the step time is the slowest rank's, on every rank
+    assert r[0]["max"] == r[1]["max"] == 125.0
+    assert r[0]["total"] == r[1]["total"] == 128
+    assert r[0]["rate"] == pytest.approx(2 * 64 / 0.125)
+
+
+def test_partition_by_cost_is_balanced_and_complete():
+    costs = [97, 5, 40, 40, 3, 61, 8, 22, 22, 1]
+    for world in (1, 2, 3, 4):
+        parts = D.partition_by_cost(costs, world)
+        flat = sorted(i for p in parts for i in p)
+        assert flat == list(range(len(costs)))
+        loads = [sum(costs[i] for i in p) for p in parts]
+        assert max(loads) - min(loads) <= max(costs)
+    assert D.partition_by_cost(costs, 2) == D.partition_by_cost(costs, 2)
+    with pytest.raises(ValueError):
+        D.partition_by_cost(costs, 0)
+
+
+def test_single_process_reductions_are_identity():
+    assert D.max_over_ranks(3.5, device="cpu") == 3.5
+    assert D.sum_over_ranks(2.0, device="cpu") == 2.0
+    assert D.rank_seed(10, 0) == 10 and D.rank_seed(10, 3) == 10 + 3 * D.SEED_STRIDE
