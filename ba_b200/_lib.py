@@ -13,7 +13,8 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libb200la.so")
 
 F64, F32 = 0, 1
-FMT_CSR, FMT_SELL = 1, 4
+FMT_CSR, FMT_SELL, FMT_SELL16 = 1, 4, 5
+FORMAT_NAMES = {FMT_CSR: "csr", FMT_SELL: "sell", FMT_SELL16: "sell16"}
 ITERATE, SUCCESS_ABS, SUCCESS_REL, FAIL_DIV, FAIL_MAXITS, FAIL_BREAKDOWN = range(6)
 SOLVER_SUCCESS, SOLVER_EXCEEDED, SOLVER_ERROR = range(3)
 STATUS_NAMES = {0: "OK", -1: "ERR_INVALID", -2: "ERR_CUDA", -3: "ERR_NOMEM", -4: "ERR_DTYPE",

@@ -577,7 +577,9 @@ __global__ void slot_setup_kernel(SysDesc<T> d, unsigned *bad) {
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   const int64_t padded_rows = (int64_t)(d.n + 31) / 32 * 32;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < padded_rows; i += stride) {
-    int start = 0, len = 0, pad = 0;
+    // padding repeats a column the row reads (an empty row: its own index);
+    // padding rows past n (last slice) read column n - 1
+    int start = 0, len = 0, pad = d.n - 1;
     if (i < d.n) {
       start = d.rowptr[i];
       len = d.rowptr[i + 1] - start;
@@ -587,7 +589,7 @@ __global__ void slot_setup_kernel(SysDesc<T> d, unsigned *bad) {
     for (int k = 0; k < d.ell; ++k) {
       const bool real = k < len;
       const int64_t pos = base + (int64_t)k * 32;
-      if (d.col16) const_cast<short *>((const short *)d.scol)[pos] = real ? (short)(d.col[start + k] - (int)i) : 0;
+      if (d.col16) const_cast<short *>((const short *)d.scol)[pos] = (short)((real ? d.col[start + k] : pad) - (int)i);
       else const_cast<int *>((const int *)d.scol)[pos] = real ? d.col[start + k] : pad;
       const_cast<T *>(d.sval)[pos] = real ? (T)d.val64[start + k] : T(0);
       if ((const void *)d.sval64 != (const void *)d.sval)

@@ -583,7 +583,7 @@ int b200la_mat_cast(b200la_mat src, int dtype, b200la_mat *out) {
       cast_kernel<double, float><<<grid, kBlock, 0, s>>>(src->nnz, (double *)m->val, (const float *)src->val);
     B_CUDA(cudaGetLastError());
   }
-  if (m->format == B200LA_FMT_SELL) B_TRY(sell_build(m, m->param));
+  if (is_sell(m->format)) B_TRY(sell_build(m, m->param, m->format == B200LA_FMT_SELL16));
   B_CUDA(cudaStreamSynchronize(s));
   *out = m;
   return B200LA_OK;
@@ -605,7 +605,13 @@ int b200la_mat_zero_rows(b200la_mat m, const int *rows, int size, double alpha) 
     zero_rows_kernel<float><<<grid, kBlock, 0, s>>>(size, d_rows, m->rowptr, m->col, (float *)m->val, (float)alpha);
   B_CUDA(cudaGetLastError());
   B_CUDA(cudaFreeAsync(d_rows, s));
-  if (m->format == B200LA_FMT_SELL) B_TRY(sell_build(m, m->param));
+  if (is_sell(m->format)) {
+    // the values changed: rebuild the sliced copy
+    const int w = m->param;
+    const bool c16 = m->format == B200LA_FMT_SELL16;
+    sell_free(m);
+    B_TRY(sell_build(m, w, c16));
+  }
   B_CUDA(cudaStreamSynchronize(s));
   return B200LA_OK;
 }
@@ -661,9 +667,9 @@ int b200la_mat_set_format(b200la_mat m, int format, int param) {
     m->param = param;
     return B200LA_OK;
   }
-  if (format == B200LA_FMT_SELL) {
+  if (is_sell(format)) {
     B_CHECK(param == 1 || param == 2 || param == 4, B200LA_ERR_INVALID, "mat_set_format: SELL width %d", param);
-    B_TRY(sell_build(m, param));
+    B_TRY(sell_build(m, param, format == B200LA_FMT_SELL16));
     m->format = format;
     m->param = param;
     return B200LA_OK;

@@ -81,7 +81,9 @@ struct SellData {
   int64_t padded = 0;   // stored entries incl. padding
   int *slice_ptr = nullptr;  // [nslices+1] offsets in entries
   int *slice_len = nullptr;  // [nslices] padded row length (multiple of width)
-  int *col = nullptr;
+  int *col = nullptr;        // int32 columns (col16 == 0)
+  short *col16p = nullptr;   // int16 offsets column - row (col16 == 1)
+  int col16 = 0;
   void *val = nullptr;
   int *perm = nullptr;       // row of each sorted position (sigma sorting)
 };

@@ -43,7 +43,7 @@ template <typename T>
 __global__ void sell_fill_kernel(int n, int nslices, int width, const int *__restrict__ rowptr,
                                  const int *__restrict__ col, const T *__restrict__ val,
                                  const int *__restrict__ slice_ptr, const int *__restrict__ slice_len,
-                                 int *__restrict__ scol, T *__restrict__ sval) {
+                                 int *__restrict__ scol, short *__restrict__ scol16, T *__restrict__ sval) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   int s = t >> 5, lane = t & 31;
   if (s >= nslices) return;
@@ -53,18 +53,27 @@ __global__ void sell_fill_kernel(int n, int nslices, int width, const int *__res
   if (row < n) {
     start = rowptr[row];
     len = rowptr[row + 1] - start;
-    if (len > 0) pad_col = col[start + len - 1];
+    // padding repeats a column the row reads; an empty row of the int16
+    // layout (square matrices only) pads with its own diagonal position
+    pad_col = len > 0 ? col[start + len - 1] : (scol16 ? row : 0);
   }
   for (int k = 0; k < L; ++k) {
     int pos = base + ((k / width) * 32 + lane) * width + (k % width);
-    if (k < len) {
-      scol[pos] = col[start + k];
-      sval[pos] = val[start + k];
-    } else {
-      scol[pos] = pad_col;
-      sval[pos] = T(0);
-    }
+    const int c = k < len ? col[start + k] : pad_col;
+    if (scol16) scol16[pos] = (short)(row < n ? c - row : 0);
+    else scol[pos] = c;
+    sval[pos] = k < len ? val[start + k] : T(0);
   }
+}
+
+// Largest |col - row| over the stored entries (atomicMax of each row's).
+__global__ void offset_range_kernel(int n, const int *__restrict__ rowptr, const int *__restrict__ col,
+                                    int *__restrict__ maxabs) {
+  const int stride = gridDim.x * blockDim.x;
+  int mx = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+    for (int j = rowptr[i]; j < rowptr[i + 1]; ++j) mx = max(mx, abs(col[j] - i));
+  if (mx) atomicMax(maxabs, mx);
 }
 
 void sell_free(b200la_mat m) {
@@ -73,17 +82,37 @@ void sell_free(b200la_mat m) {
   if (d.slice_ptr) cudaFreeAsync(d.slice_ptr, s);
   if (d.slice_len) cudaFreeAsync(d.slice_len, s);
   if (d.col) cudaFreeAsync(d.col, s);
+  if (d.col16p) cudaFreeAsync(d.col16p, s);
   if (d.val) cudaFreeAsync(d.val, s);
   if (d.perm) cudaFreeAsync(d.perm, s);
   d = SellData();
 }
 
-int sell_build(b200la_mat m, int width) {
-  if (m->sell.width == width && m->sell.col) return B200LA_OK;
-  sell_free(m);
+int sell_build(b200la_mat m, int width, bool col16) {
+  if (m->sell.width == width && m->sell.col16 == (int)col16 && (col16 ? (void *)m->sell.col16p : (void *)m->sell.col))
+    return B200LA_OK;
   cudaStream_t s = m->ctx->stream;
+  if (col16) {
+    B_CHECK(m->nrow == m->ncol, B200LA_ERR_UNSUPPORTED, "SELL16: square matrices only (%dx%d)", m->nrow, m->ncol);
+    // int16 offsets only when every stored column lies within int16 of its row
+    int *d_max = nullptr, h_max = 0;
+    B_CUDA(cudaMallocAsync(&d_max, sizeof(int), s));
+    B_CUDA(cudaMemsetAsync(d_max, 0, sizeof(int), s));
+    if (m->nrow) {
+      const int grid = std::min((m->nrow + kBlock - 1) / kBlock, m->ctx->num_sms * 8);
+      offset_range_kernel<<<grid, kBlock, 0, s>>>(m->nrow, m->rowptr, m->col, d_max);
+    }
+    B_CUDA(cudaGetLastError());
+    B_CUDA(cudaMemcpyAsync(&h_max, d_max, sizeof(int), cudaMemcpyDeviceToHost, s));
+    B_CUDA(cudaFreeAsync(d_max, s));
+    B_CUDA(cudaStreamSynchronize(s));
+    B_CHECK(h_max <= 32767, B200LA_ERR_UNSUPPORTED, "SELL16: a column lies %d rows from its row (int16 offsets)",
+            h_max);
+  }
+  sell_free(m);
   SellData &d = m->sell;
   d.width = width;
+  d.col16 = col16 ? 1 : 0;
   d.nslices = (m->nrow + 31) / 32;
   if (d.nslices == 0) return B200LA_OK;
   B_CUDA(cudaMallocAsync(&d.slice_len, sizeof(int) * d.nslices, s));
@@ -105,18 +134,19 @@ int sell_build(b200la_mat m, int width) {
   d.padded = acc;
   size_t pz = (size_t)(acc > 0 ? acc : 1);
   B_CUDA(cudaMemcpyAsync(d.slice_ptr, ptr.data(), sizeof(int) * (d.nslices + 1), cudaMemcpyHostToDevice, s));
-  B_CUDA(cudaMallocAsync(&d.col, sizeof(int) * pz, s));
+  if (col16) B_CUDA(cudaMallocAsync(&d.col16p, sizeof(short) * pz, s));
+  else B_CUDA(cudaMallocAsync(&d.col, sizeof(int) * pz, s));
   B_CUDA(cudaMallocAsync(&d.val, dtype_size(m->dtype) * pz, s));
   int threads = d.nslices * 32;
   int grid = (threads + kBlock - 1) / kBlock;
   if (m->dtype == B200LA_F64)
     sell_fill_kernel<double><<<grid, kBlock, 0, s>>>(m->nrow, d.nslices, width, m->rowptr, m->col,
                                                      (const double *)m->val, d.slice_ptr, d.slice_len, d.col,
-                                                     (double *)d.val);
+                                                     d.col16p, (double *)d.val);
   else
     sell_fill_kernel<float><<<grid, kBlock, 0, s>>>(m->nrow, d.nslices, width, m->rowptr, m->col,
                                                     (const float *)m->val, d.slice_ptr, d.slice_len, d.col,
-                                                    (float *)d.val);
+                                                    d.col16p, (float *)d.val);
   B_CUDA(cudaGetLastError());
   B_CUDA(cudaStreamSynchronize(s));
   return B200LA_OK;
@@ -130,8 +160,10 @@ extern "C" int b200la_mat_tune(b200la_mat m, int *format, int *param, double *us
   B_CHECK(m, B200LA_ERR_INVALID, "mat_tune: null matrix");
   b200la_ctx c = m->ctx;
   cudaStream_t s = c->stream;
-  const int fmts[][2] = {{B200LA_FMT_CSR, 2},  {B200LA_FMT_CSR, 4},  {B200LA_FMT_CSR, 8}, {B200LA_FMT_CSR, 16},
-                         {B200LA_FMT_CSR, 32}, {B200LA_FMT_SELL, 1}, {B200LA_FMT_SELL, 2}, {B200LA_FMT_SELL, 4}};
+  const int fmts[][2] = {{B200LA_FMT_CSR, 2},    {B200LA_FMT_CSR, 4},    {B200LA_FMT_CSR, 8},
+                         {B200LA_FMT_CSR, 16},   {B200LA_FMT_CSR, 32},   {B200LA_FMT_SELL, 1},
+                         {B200LA_FMT_SELL, 2},   {B200LA_FMT_SELL, 4},   {B200LA_FMT_SELL16, 1},
+                         {B200LA_FMT_SELL16, 2}, {B200LA_FMT_SELL16, 4}};
   size_t es = dtype_size(m->dtype);
   void *x = nullptr, *y = nullptr;
   B_CUDA(cudaMallocAsync(&x, es * (m->ncol > 0 ? m->ncol : 1), s));
@@ -144,7 +176,7 @@ extern "C" int b200la_mat_tune(b200la_mat m, int *format, int *param, double *us
   float best = 1e30f;
   const int reps = 10;
   for (auto &fp : fmts) {
-    if (fp[0] == B200LA_FMT_SELL) {
+    if (is_sell(fp[0])) {
       // SELL copies cost extra HBM; skip them when they would pad badly.
       if (b200la_mat_set_format(m, fp[0], fp[1]) != B200LA_OK) continue;
       if ((double)m->sell.padded > 1.25 * (double)m->nnz + 64.0 * m->sell.nslices) continue;
@@ -169,7 +201,7 @@ extern "C" int b200la_mat_tune(b200la_mat m, int *format, int *param, double *us
   cudaFreeAsync(x, s);
   cudaFreeAsync(y, s);
   B_TRY(b200la_mat_set_format(m, best_f, best_p));
-  if (best_f != B200LA_FMT_SELL) sell_free(m);
+  if (!is_sell(best_f)) sell_free(m);
   if (format) *format = best_f;
   if (param) *param = best_p;
   if (usec) *usec = 1000.0 * best / reps;

@@ -97,6 +97,53 @@ template <typename T, int W> struct SellOp {
   }
 };
 
+// ---- SELL-32 with int16 column offsets -------------------------------------
+// Same slices and value layout as SellOp; the stored column of entry k is
+// (column - row) as int16, so a warp reads 2*W bytes of indices per lane and
+// step instead of 4*W.  Products and their order are those of SellOp.
+template <int W> struct VecS;
+template <> struct VecS<1> { using i = short; };
+template <> struct VecS<2> { using i = short2; };
+template <> struct VecS<4> { using i = short4; };
+
+template <typename I> __device__ __forceinline__ int lane_gets(const I &v, int k) {
+  return (int)reinterpret_cast<const short *>(&v)[k];
+}
+
+template <typename T, int W> struct SellOp16 {
+  const int *__restrict__ slice_ptr;
+  const int *__restrict__ slice_len;
+  const short *__restrict__ col;
+  const T *__restrict__ val;
+  int n, nslices;
+  static constexpr int kRowsPerBlock = kBlock;
+  __host__ __device__ int64_t work_items() const { return n; }
+  template <typename Emit> __device__ __forceinline__ void run(const T *__restrict__ x, Emit &emit) const {
+    using VV = typename VecW<T, W>::v;
+    using VI = typename VecS<W>::i;
+    const int lane = threadIdx.x & 31;
+    const int wpb = kBlock / 32;
+    for (int s = blockIdx.x * wpb + ((int)threadIdx.x >> 5); s < nslices; s += gridDim.x * wpb) {
+      const int base = __ldg(slice_ptr + s);
+      const int chunks = __ldg(slice_len + s) / W;
+      const VI *ci = reinterpret_cast<const VI *>(col + base) + lane;
+      const VV *vi = reinterpret_cast<const VV *>(val + base) + lane;
+      const int row = s * 32 + lane;
+      // padding rows past n (last slice) hold offset 0 and gather x[0]
+      const int rb = row < n ? row : 0;
+      T sum = T(0);
+#pragma unroll 4
+      for (int c = 0; c < chunks; ++c) {
+        VI cc = __ldcs(ci + c * 32);
+        VV vv = ld_vec_stream(vi + c * 32);
+#pragma unroll
+        for (int k = 0; k < W; ++k) sum = fma(lane_get<VV, T, W>(vv, k), ld_keep(x + rb + lane_gets(cc, k)), sum);
+      }
+      if (row < n) emit(row, sum);
+    }
+  }
+};
+
 // ---- plain emitters --------------------------------------------------------
 template <typename T> struct StoreEmit {
   T *__restrict__ y;
@@ -131,6 +178,16 @@ template <typename T, typename F> int with_schedule(b200la_mat m, F &&f) {
     }
     return fail(B200LA_ERR_INVALID, "SELL width %d", m->param);
   }
+  if (m->format == B200LA_FMT_SELL16) {
+    const SellData &s = m->sell;
+    const T *sv = (const T *)s.val;
+    switch (m->param) {
+      case 1: return f(SellOp16<T, 1>{s.slice_ptr, s.slice_len, s.col16p, sv, m->nrow, s.nslices});
+      case 2: return f(SellOp16<T, 2>{s.slice_ptr, s.slice_len, s.col16p, sv, m->nrow, s.nslices});
+      case 4: return f(SellOp16<T, 4>{s.slice_ptr, s.slice_len, s.col16p, sv, m->nrow, s.nslices});
+    }
+    return fail(B200LA_ERR_INVALID, "SELL16 width %d", m->param);
+  }
   switch (m->param) {
     case 1: return f(CsrOp<T, 1>{m->rowptr, m->col, val, m->nrow});
     case 2: return f(CsrOp<T, 2>{m->rowptr, m->col, val, m->nrow});
@@ -143,7 +200,8 @@ template <typename T, typename F> int with_schedule(b200la_mat m, F &&f) {
 }
 
 int spmv_launch(b200la_mat m, const void *x, void *y, bool add, cudaStream_t s);
-int sell_build(b200la_mat m, int width);
+int sell_build(b200la_mat m, int width, bool col16 = false);
+inline bool is_sell(int format) { return format == B200LA_FMT_SELL || format == B200LA_FMT_SELL16; }
 void sell_free(b200la_mat m);
 
 }  // namespace b200la

@@ -25,7 +25,7 @@ import numpy as np
 
 from . import lmp
 from . import problems as P
-from ._lib import FMT_CSR, FMT_SELL, call, load
+from ._lib import FMT_CSR, FMT_SELL, FMT_SELL16, FORMAT_NAMES, call, load
 
 
 def main():
@@ -57,7 +57,7 @@ def main():
         fmt, prm, us = A.tune()
     else:
         kind, prm = a.schedule.split("/")
-        fmt, prm = (FMT_SELL if kind == "sell" else FMT_CSR), int(prm)
+        fmt, prm = {"sell": FMT_SELL, "sell16": FMT_SELL16, "csr": FMT_CSR}[kind], int(prm)
         A.set_format(fmt, prm)
         us = float("nan")
     x = lmp.B200_lVector.from_numpy(s.b.astype(dt), platform=plat, dtype=dt)
@@ -77,7 +77,7 @@ def main():
     call("b200la_cg_profile", solver._solver, b.handle, x0.handle, a.cg_iters, ms)
     sv = 8 if dt == np.float64 else 4
     alg = s.nnz * (sv + 4) + (s.n + 1) * 4 + 2 * s.n * sv
-    print(f"system n={s.n} nnz={s.nnz} dtype={a.dtype} schedule={'sell' if fmt == FMT_SELL else 'csr'}/{prm} "
+    print(f"system n={s.n} nnz={s.nnz} dtype={a.dtype} schedule={FORMAT_NAMES[fmt]}/{prm} "
           f"tuned_us={us:.1f}")
     print(f"spmv wall {spmv_ms:.3f} ms/launch; cg kernels ms: spmv_dot {ms[0]:.4f} update {ms[1]:.4f} "
           f"direction {ms[2]:.4f}; spmv algorithmic bytes {alg} -> {alg / ms[0] / 1e6:.1f} GB/s")

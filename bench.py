@@ -56,7 +56,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="batch", choices=["batch", "poisson3d", "serve"])
+    ap.add_argument("--workload", default="batch", choices=["batch", "poisson3d", "varcoef3d", "serve"])
     ap.add_argument("--cells", type=int, default=128, help="poisson3d cells per axis")
     ap.add_argument("--count", type=int, default=BATCH_COUNT, help="batch: systems per step")
     ap.add_argument("--requests", type=int, default=64, help="serve: requests per timed step")
@@ -616,7 +616,7 @@ def run_poisson3d(args, rank, local_rank, world, torch, dist, barrier):
 
     from ba_b200 import lmp
     from ba_b200 import problems as P
-    from ba_b200._lib import FMT_SELL, load
+    from ba_b200._lib import FORMAT_NAMES, load
 
     plat = lmp.Platform(local_rank)
     stream = torch.cuda.current_stream()
@@ -700,7 +700,7 @@ def run_poisson3d(args, rank, local_rank, world, torch, dist, barrier):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": f"fp64 jacobi-pcg 3d q1 poisson {args.cells}^3 cells, rel 1e-10", "n": n,
                        "nnz": nnz, "iters_per_solve": iters, "parallelism": f"replicas x{world}",
-                       "spmv_schedule": ("sell" if fmt == FMT_SELL else "csr") + f"/{prm}",
+                       "spmv_schedule": FORMAT_NAMES[fmt] + f"/{prm}",
                        "l2": "inputs larger than L2 (matrix 685 MB streamed per iteration)",
                        "plain_fp64_cg": {"value": plain_value, "unit": "solves/s", "iters_per_solve": plain.iter()}},
             "clocks": clk,
@@ -713,13 +713,189 @@ def run_poisson3d(args, rank, local_rank, world, torch, dist, barrier):
             "cpu_baseline": cpu}))
 
 
+# ----------------------------------------------------------------- varcoef3d workload (C3)
+def run_reference_varcoef3d(args, rank):
+    import oracle
+    from ba_b200 import problems as P
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (reference sources absent)"}))
+        return
+    s = P.varcoef_3d(args.cells, sigma=2.0)
+    counts = json.load(open(COUNTS)) if os.path.exists(COUNTS) else {}
+    full_iters = counts.get(f"varcoef3d_{args.cells}_s2/jacobi/rtol1e-10", {}).get("iters")
+    nthreads = os.cpu_count() or 1
+    ref = oracle.RefSystem(s.rowptr, s.col, s.val, impl=oracle.IMPL_OPENMP, nthreads=nthreads)
+    per_iter = []
+    for step in range(args.warmup + args.steps):
+        r, sec = ref.cg(s.b, maxits=20, atol=0.0, rtol=1e-10, dtol=1e8, precond=True)
+        if step >= args.warmup:
+            per_iter.append(sec / max(r.iters, 1))
+    scale = full_iters or VARCOEF_FP64_ITERS_FALLBACK
+    value = 1.0 / (statistics.median(per_iter) * scale)
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"3d q1 lognormal sigma=2 diffusion {args.cells}^3 cells, rel 1e-10", "n": s.n,
+                   "nnz": s.nnz, "parallelism": f"cpu openmp x{nthreads}"},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": nthreads, "kind": "reference",
+                         "sample": f"20 iterations of FP64 Jacobi-PCG per step (HiFlow3 lmp OPENMP SpMV, {nthreads} "
+                                   f"threads), scaled by {scale} iterations per solve"},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+
+
+# FP64 Jacobi-PCG iterations of the 128^3 sigma=2 system to 1e-10 on this
+# project's device CG (the reference's count to +-1), used to scale the CPU
+# sample when no recorded reference count exists
+VARCOEF_FP64_ITERS_FALLBACK = 2000
+
+
+def run_varcoef3d(args, rank, local_rank, world, torch, dist, barrier):
+    import ctypes as C
+
+    from ba_b200 import lmp
+    from ba_b200 import problems as P
+    from ba_b200._lib import load
+
+    plat = lmp.Platform(local_rank)
+    stream = torch.cuda.current_stream()
+    plat.set_stream(stream.cuda_stream)
+    s = P.varcoef_3d(args.cells, sigma=2.0)
+    n, nnz = s.n, s.nnz
+    A = lmp.B200_CSR_lMatrix(s.rowptr, s.col, s.val, platform=plat)
+    A.tune()
+    b = lmp.B200_lVector.from_numpy(s.b, platform=plat)
+    x = lmp.B200_lVector(n, platform=plat)
+    m = lmp.MPIR()
+    m.SetupOperator(A)
+    m.SetMpirParameters(0, 30, 0.0, 1e-10, 1e6)
+    m.SetLowPrecErrCorSolverParameters(200000, 0.0, 1e-5, 1e30)
+
+    def mp_step():
+        x.Zeros()
+        st = m.Solve(b, x)
+        assert st == lmp.kSolverSuccess, (m.state_, m.res_rel_)
+
+    for _ in range(args.warmup):
+        mp_step()
+    clocks = ClockSampler(local_rank)
+    barrier()
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        mp_step()
+    e1.record(stream)
+    e1.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms_max = D.max_over_ranks(e0.elapsed_time(e1))
+    value = world * args.steps / (ms_max / 1e3)
+    x_mp = x.numpy().copy()
+    outer, inner = m.outer_, m.iter()
+
+    # FP64 comparators on the same matrix: Jacobi-PCG and plain CG
+    def fp64_rate(precond, rtol, reps):
+        sv = lmp.setup_CG_solver(maxits=500000, atol=0.0, rtol=rtol, dtol=1e8, use_precond=precond)
+        sv.SetupOperator(A)
+        x.Zeros()
+        sv.Solve(b, x)
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for _ in range(reps):
+            x.Zeros()
+            st = sv.Solve(b, x)
+        f1.record(stream)
+        f1.synchronize()
+        return reps / (f0.elapsed_time(f1) / 1e3), sv.iter(), st
+
+    pcg_value, pcg_iters, _ = fp64_rate(True, 1e-10, 2)
+    plain_value, plain_iters, plain_state = fp64_rate(False, 1e-10, 1)
+    # the FP64 reference solution for the error: device FP64 Jacobi-PCG to 1e-13
+    # (parity-tested against the CPU oracle, which needs minutes at this size)
+    ref = lmp.setup_CG_solver(maxits=500000, atol=0.0, rtol=1e-13, dtol=1e8, use_precond=True)
+    ref.SetupOperator(A)
+    x.Zeros()
+    ref.Solve(b, x)
+    x_ref = x.numpy().copy()
+    err = float(np.linalg.norm(x_mp - x_ref) / np.linalg.norm(x_ref))
+    import scipy.sparse as sp
+    Ah = sp.csr_matrix((s.val, s.col, s.rowptr), shape=(n, n))
+    true_rel = float(np.linalg.norm(s.b - Ah @ x_mp) / np.linalg.norm(s.b))
+
+    # e2e through the public API: RHS up from pinned host memory, solve, solution down
+    lib = load()
+    bh = torch.from_numpy(s.b).pin_memory()
+    xh = torch.empty(n, dtype=torch.float64).pin_memory()
+    barrier()
+    h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    h0.record(stream)
+    for _ in range(args.steps):
+        lib.b200la_vec_upload(b.handle, C.c_void_p(bh.data_ptr()), n)
+        mp_step()
+        lib.b200la_vec_download(x.handle, C.c_void_p(xh.data_ptr()), n)
+    h1.record(stream)
+    h1.synchronize()
+    e2e_value = D.aggregate_rate(args.steps, world, D.max_over_ranks(h0.elapsed_time(h1)))
+
+    # roofline: the inner solve's FP32 K1 (SpMV + p.Ap) on the FP32 copy
+    A32 = A.CastTo(np.float32)  # the same FP32 copy the solver makes, tuned the same way
+    A32.tune()
+    b32 = lmp.B200_lVector.from_numpy(s.b.astype(np.float32), platform=plat, dtype=np.float32)
+    x32 = lmp.B200_lVector(n, platform=plat, dtype=np.float32)
+    sv32 = lmp.setup_CG_solver(maxits=1000, atol=0.0, rtol=1e-12, dtol=1e8, use_precond=True)
+    sv32.SetupOperator(A32)
+    sv32._ensure()
+    ms3 = (C.c_double * 3)()
+    lib.b200la_cg_profile(sv32._solver, b32.handle, x32.handle, 20, ms3)
+    bytes_spmv = spmv_bytes(n, nnz, 4)
+    peak, peak_kind = measured_peak_gbs()
+    achieved = bytes_spmv / (ms3[0] / 1e3) / 1e9
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import oracle
+        if oracle.ref_available():
+            nthreads = os.cpu_count() or 1
+            refc = oracle.RefSystem(s.rowptr, s.col, s.val, impl=oracle.IMPL_OPENMP, nthreads=nthreads)
+            r, sec = refc.cg(s.b, maxits=20, atol=0.0, rtol=1e-10, dtol=1e8, precond=True)
+            cpu = {"value": 1.0 / (sec / max(r.iters, 1) * pcg_iters), "unit": "solves/s", "cores": nthreads,
+                   "kind": "reference", "sample": f"20 of {pcg_iters} FP64 Jacobi-PCG iterations (HiFlow3 lmp "
+                                                  f"OPENMP SpMV, {nthreads} threads), scaled to a full solve"}
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": f"mixed-precision refinement, 3d q1 lognormal sigma=2 diffusion {args.cells}^3 "
+                                   f"cells, rel 1e-10 (FP32 Jacobi-PCG inner, FP64 outer)", "n": n, "nnz": nnz,
+                       "refinement_passes": outer, "inner_iters": inner, "parallelism": f"replicas x{world}",
+                       "true_rel_residual": true_rel,
+                       "error_vs_fp64": {"value": err, "reference": "device FP64 Jacobi-PCG to 1e-13"},
+                       "fp64_jacobi_pcg": {"value": pcg_value, "unit": "solves/s", "iters": pcg_iters},
+                       "plain_fp64_cg": {"value": plain_value, "unit": "solves/s", "iters": plain_iters,
+                                         "state": plain_state},
+                       "speedup_vs_plain_fp64_cg": value / world / plain_value,
+                       "speedup_vs_fp64_pcg": value / world / pcg_value,
+                       "l2": "inputs larger than L2 (FP32 matrix 456 MB + FP64 matrix 685 MB)"},
+            "clocks": clk,
+            "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": n * 8, "d2h_bytes_per_step": n * 8},
+            "gpu_launches": args.steps * (3 * inner + 8 * outer + 4),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": profile_traffic(f"varcoef3d_{args.cells}/f32/spmv"), "peak_source": peak_kind,
+                         "kernel": "cg_spmv_kernel<float> (inner SpMV fused with p.Ap)",
+                         "algorithmic_bytes": bytes_spmv,
+                         "kernel_ms": {"spmv_dot": ms3[0], "update": ms3[1], "direction": ms3[2]}},
+            "cpu_baseline": cpu}))
+
+
 def main():
     args = parse()
     rank, local_rank, world = dist_env()
     if args.impl == "reference":
         if rank == 0:
             {"batch": run_reference_batch, "poisson3d": run_reference_poisson3d,
-             "serve": run_reference_serve}[args.workload](args, rank)
+             "varcoef3d": run_reference_varcoef3d, "serve": run_reference_serve}[args.workload](args, rank)
         return
     import datetime
 
@@ -737,7 +913,8 @@ def main():
         torch.cuda.synchronize()
 
     load()
-    fn = {"batch": run_batch, "poisson3d": run_poisson3d, "serve": run_serve}[args.workload]
+    fn = {"batch": run_batch, "poisson3d": run_poisson3d, "varcoef3d": run_varcoef3d,
+          "serve": run_serve}[args.workload]
     fn(args, rank, local_rank, world, torch, dist, barrier)
     if world > 1:
         dist.barrier()

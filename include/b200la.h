@@ -65,6 +65,8 @@ typedef struct b200la_batch_s *b200la_batch;
 /* SpMV storage formats (la_global.h:56 MATRIX_FORMAT has DENSE, CSR, COO, ELL) */
 #define B200LA_FMT_CSR 1  /* CSR, a group of `lanes` threads per row */
 #define B200LA_FMT_SELL 4 /* SELL-C-sigma, C = 32 rows per slice */
+#define B200LA_FMT_SELL16 5 /* SELL-32 with columns stored as int16 offsets from the row
+                             (banded matrices: every |col - row| <= 32767) */
 
 /* ---- library / context ---------------------------------------------------
  * replaces init_platform_gpu (lmp/cuda/platform_management_gpu.cu:78-143) */

@@ -14,12 +14,13 @@ import pytest
 import oracle
 from ba_b200 import lmp
 from ba_b200 import problems as P
-from ba_b200._lib import FMT_CSR, FMT_SELL, B200LAError
+from ba_b200._lib import FMT_CSR, FMT_SELL, FMT_SELL16, B200LAError
 
 pytestmark = pytest.mark.gpu
 
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-SCHEDULES = [(FMT_CSR, g) for g in (1, 2, 4, 8, 16, 32)] + [(FMT_SELL, w) for w in (1, 2, 4)]
+SCHEDULES = ([(FMT_CSR, g) for g in (1, 2, 4, 8, 16, 32)] + [(FMT_SELL, w) for w in (1, 2, 4)]
+             + [(FMT_SELL16, w) for w in (1, 2, 4)])
 
 # FP64 SpMV tolerance: the device sums each row with FMA in a different order
 # than the oracle's sequential loop; bound by a few ulps of sum |a_ij x_j|.
@@ -202,7 +203,7 @@ def test_cg_matches_reference_runs(plat, case):
         same = oracle.cg(s.rowptr, s.col, s.val, s.b, maxits=20000, atol=0.0, rtol=run["rtol"],
                          dtol=1e8, precond=run["precond"], dtype=dt)
         assert same.iters == run["iters"]
-        for fmt, prm in ((FMT_CSR, 4), (FMT_CSR, 16), (FMT_SELL, 1)):
+        for fmt, prm in ((FMT_CSR, 4), (FMT_CSR, 16), (FMT_SELL, 1), (FMT_SELL16, 2)):
             A = _mat(plat, s, dt)
             A.set_format(fmt, prm)
             b = _vec(plat, s.b, dt)
@@ -318,3 +319,33 @@ def test_full_size_c2_properties(plat):
     xs_ = sol.numpy()
     true_res = np.linalg.norm(s.b - Ah @ xs_)
     assert true_res <= 2e-10 * np.linalg.norm(s.b)
+
+
+def test_sell16_matches_sell_bitwise_and_refuses_far_columns(plat):
+    """SELL16 stores (column - row) as int16: same products in the same order
+    as SELL, so the results are identical; a column more than 32767 rows away
+    is refused with B200LA_ERR_UNSUPPORTED (the tuner then skips SELL16)."""
+    s = P.q1_system(3, 20, 31, 1.0)
+    xs = np.random.default_rng(3).standard_normal(s.n)
+    for dt in (np.float64, np.float32):
+        ys = []
+        for fmt in (FMT_SELL, FMT_SELL16):
+            for w in (1, 2, 4):
+                A = _mat(plat, s, dt)
+                A.set_format(fmt, w)
+                x = _vec(plat, xs, dt)
+                y = x.CloneWithoutContent()
+                A.VectorMult(x, y)
+                ys.append((w, y.numpy()))
+        for (w1, a), (w2, b) in zip(ys[:3], ys[3:]):
+            np.testing.assert_array_equal(a, b)
+    n = 40000
+    rowptr = np.arange(n + 1, dtype=np.int32)
+    col = np.arange(n, dtype=np.int32)
+    col[0] = n - 1                      # row 0 reads column 39999
+    A = lmp.B200_CSR_lMatrix(rowptr, col, np.ones(n), platform=plat)
+    with pytest.raises(B200LAError) as e:
+        A.set_format(FMT_SELL16, 1)
+    assert e.value.status == -7
+    fmt, _, _ = A.tune()
+    assert fmt != FMT_SELL16
