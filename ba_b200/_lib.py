@@ -46,7 +46,7 @@ class MpResult(C.Structure):
 
 class BatchParams(C.Structure):
     _fields_ = [("capacity", C.c_int), ("mixed", C.c_int), ("precond", C.c_int), ("max_outer", C.c_int),
-                ("inner_maxits", C.c_int), ("lanes", C.c_int), ("tile_rows", C.c_int), ("index_bits", C.c_int),
+                ("inner_maxits", C.c_int), ("adaptive", C.c_int), ("tile_rows", C.c_int), ("index_bits", C.c_int),
                 ("atol", C.c_double), ("rtol", C.c_double), ("dtol", C.c_double), ("inner_rtol", C.c_double)]
 
 

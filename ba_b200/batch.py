@@ -41,12 +41,12 @@ def slot_bytes(n: int, nnz: int, max_row: int, mixed: bool) -> int:
 class Batch:
     def __init__(self, capacity: int, *, mixed: bool = True, precond: bool = True, rtol: float = 1e-8,
                  atol: float = 0.0, dtol: float = 1e8, inner_rtol: float = 1e-4, max_outer: int = 30,
-                 inner_maxits: int = 100000, lanes: int = 0, tile_rows: int = 0, index_bits: int = 0,
+                 inner_maxits: int = 100000, adaptive: bool = False, tile_rows: int = 0, index_bits: int = 0,
                  platform: Platform | None = None):
         self.platform = platform or init_platform()
         self.mixed = mixed
         prm = BatchParams(int(capacity), int(mixed), int(precond), int(max_outer), int(inner_maxits),
-                          int(lanes), int(tile_rows), int(index_bits), float(atol), float(rtol), float(dtol),
+                          int(adaptive), int(tile_rows), int(index_bits), float(atol), float(rtol), float(dtol),
                           float(inner_rtol))
         self.handle = C.c_void_p()
         call("b200la_batch_create", self.platform.handle, C.byref(prm), C.byref(self.handle))

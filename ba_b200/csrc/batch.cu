@@ -998,14 +998,14 @@ int upload_tiles(BatchHandle B, bool running_only, int *count, int64_t *alg_byte
   for (int k = 0; k < 3; ++k) {
     ItemList &L = B->lst[k];
     // adaptive: halve the item (down to one 32-row slice) while the list
-    // would give the kernel's warps fewer than two items each, so a lightly
+    // would give the kernel's warps fewer than one item each, so a lightly
     // loaded pass is not bound by one warp's long serial chain
     int rows = L.rows;
     if (B->adaptive)
       while (rows > 32) {
         int64_t items = 0;
         for (int s : run) items += (B->sys[s].n + rows - 1) / rows;
-        if (items >= 2 * (int64_t)B->warps[k]) break;
+        if (items >= (int64_t)B->warps[k]) break;
         rows = std::max(32, (rows / 2) & ~31);
       }
     L.used = rows;
@@ -1236,7 +1236,7 @@ int b200la_batch_create(b200la_ctx ctx, const b200la_batch_params *p, b200la_bat
   // K1 sweeps 256-row items (8 slices per warp keep its gather chains
   // short); K2 streams 1024-row items, K3 512; the tuner may change them
   for (int k = 0; k < 3; ++k) B->lst[k].rows = p->tile_rows ? p->tile_rows : kDefaultRows[k];
-  B->adaptive = false;
+  B->adaptive = p->adaptive != 0;
   B->capacity = p->capacity;
   B->sys.resize(p->capacity);
   cudaStream_t st = ctx->stream;

@@ -256,7 +256,8 @@ typedef struct {
   int precond;        /* 1: Jacobi */
   int max_outer;      /* refinement passes (mixed) */
   int inner_maxits;   /* iterations per inner solve (FP64 mode: per solve) */
-  int lanes;          /* reserved: 0 (both SpMVs use the sliced-ELL layout) */
+  int adaptive;       /* 1: each run shrinks work items (down to 32 rows) while the running
+                         systems would give a kernel's warps fewer than one item each */
   int tile_rows;      /* rows per warp work item of every kernel, a multiple of 32
                          (0 = 256 SpMV, 1024 update, 512 direction; tunable) */
   int index_bits;     /* sliced-ELL column storage: 0 = int16 offsets from the row when
@@ -314,8 +315,8 @@ int b200la_batch_restart(b200la_batch b);
  * their own item size.  set_items sets them (multiples of 32 rows; they take
  * effect at the next run); with adaptive = 1 each run halves a kernel's
  * item, down to 32 rows, while the running systems would give its warps
- * fewer than two items each (off by default: measured slower on the
- * standard batch).  get_items writes the three sizes. */
+ * fewer than one item each (as b200la_batch_params.adaptive).  get_items
+ * writes the three sizes. */
 int b200la_batch_set_items(b200la_batch b, int rows_spmv, int rows_update, int rows_direction, int adaptive);
 int b200la_batch_get_items(b200la_batch b, int *rows /* [3] */);
 /* Autotuner: unless the batch was created with a fixed tile_rows, times
