@@ -130,6 +130,7 @@ _SIGS = {
     "b200la_batch_remove": [_vp, _i],
     "b200la_batch_run": [_vp, _i, _P(_i)],
     "b200la_batch_result": [_vp, _i, _vp, _P(SysResult)],
+    "b200la_batch_results": [_vp, _i, _P(_i), _P(_vp), _P(SysResult)],
     "b200la_batch_info": [_vp, _P(_i), _P(_i64)],
     "b200la_batch_tune": [_vp, _P(_i), _P(_d)],
     "b200la_batch_set_items": [_vp, _i, _i, _i, _i],

@@ -115,6 +115,22 @@ class Batch:
         return SystemResult(r.state, r.solver_state, r.iters, r.outer, bool(r.phase_done), r.res, r.res_init,
                             r.res_rel, r.device_us, x)
 
+    def results(self, slots, with_x: bool = True, out=None) -> list[SystemResult]:
+        """Results of many slots with one wait for all the solution copies;
+        `out` may give preallocated float64 arrays (e.g. pinned) per slot."""
+        slots = [int(s) for s in slots]
+        k = len(slots)
+        rs = (SysResult * k)()
+        sl = (C.c_int * k)(*slots)
+        xs = None
+        ptrs = None
+        if with_x:
+            xs = list(out) if out is not None else [np.empty(self.slot_n(s), np.float64) for s in slots]
+            ptrs = (C.c_void_p * k)(*[x.ctypes.data for x in xs])
+        call("b200la_batch_results", self.handle, k, sl, ptrs, rs)
+        return [SystemResult(r.state, r.solver_state, r.iters, r.outer, bool(r.phase_done), r.res, r.res_init,
+                             r.res_rel, r.device_us, None if xs is None else xs[j]) for j, r in enumerate(rs)]
+
     def slot_n(self, slot: int) -> int:
         return self._sizes[slot]
 

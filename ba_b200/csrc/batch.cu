@@ -660,6 +660,48 @@ __global__ void __launch_bounds__(kBlock) slot_snapshot_kernel(const int *__rest
   }
 }
 
+// Checks of an uploaded CSR (those of the host validate_csr): rowptr[0] == 0,
+// rowptr[n] == nnz, non-decreasing, 0 <= col < n; also the longest row and
+// the largest |col - row|.  The first failing row (and why) is kept with a
+// 64-bit atomicMin on (row << 8 | code); columns are read only for rows
+// whose bounds lie inside [0, nnz].
+enum CsrCheckCode : int { kChkStart = 1, kChkDecrease = 2, kChkBounds = 3, kChkColumn = 4 };
+struct CsrCheck {
+  unsigned long long err;  // ~0: valid
+  int max_row;
+  int max_off;
+};
+
+__global__ void csr_check_kernel(int n, int nnz, const int *__restrict__ rowptr, const int *__restrict__ col,
+                                 CsrCheck *out) {
+  const int stride = gridDim.x * blockDim.x;
+  int mr = 0, mo = 0;
+  unsigned long long err = ~0ull;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const int a = rowptr[i], b = rowptr[i + 1];
+    unsigned long long e = ~0ull;
+    if ((i == 0 && a != 0) || (i == n - 1 && b != nnz)) e = ((unsigned long long)i << 8) | kChkStart;
+    else if (b < a) e = ((unsigned long long)i << 8) | kChkDecrease;
+    else if (a < 0 || b > nnz) e = ((unsigned long long)i << 8) | kChkBounds;
+    if (e != ~0ull) {
+      err = min(err, e);
+      continue;
+    }
+    mr = max(mr, b - a);
+    for (int j = a; j < b; ++j) {
+      const int c = col[j];
+      if (c < 0 || c >= n) {
+        err = min(err, ((unsigned long long)i << 8) | kChkColumn);
+        break;
+      }
+      mo = max(mo, abs(c - i));
+    }
+  }
+  if (err != ~0ull) atomicMin(&out->err, err);
+  if (mr) atomicMax(&out->max_row, mr);
+  if (mo) atomicMax(&out->max_off, mo);
+}
+
 // Restart every listed slot from x = 0: RESID phase, counters cleared.
 template <typename T>
 __global__ void __launch_bounds__(kBlock) batch_restart_kernel(const int *__restrict__ slots,
@@ -687,7 +729,8 @@ struct HostSys {
   bool used = false;
   int n = 0;
   int nnz = 0;
-  void *chunk = nullptr;  // one allocation holds all of the slot's buffers
+  void *chunk = nullptr;   // CSR as uploaded and the vectors
+  void *chunk2 = nullptr;  // the sliced-ELL copy (sized once the rows are known)
   size_t bytes = 0;
   SysDesc<double> d64{};
   SysDesc<float> d32{};
@@ -723,6 +766,8 @@ struct b200la_batch_s {
   void *desc;         // SysDesc<T>[capacity]
   SysState *st;       // [capacity]
   BatchGlobals *glob;
+  CsrCheck *chk;       // device result of csr_check_kernel
+  CsrCheck *chk_host;  // pinned mirror
   // host mirrors
   SysState *st_host;  // pinned [capacity]
   BatchGlobals *glob_host;
@@ -739,40 +784,44 @@ template <typename T> SysDesc<T> &desc_of(HostSys &h);
 template <> SysDesc<double> &desc_of<double>(HostSys &h) { return h.d64; }
 template <> SysDesc<float> &desc_of<float>(HostSys &h) { return h.d32; }
 
-// Bytes one slot needs for a system (the admission test of the request loop).
-size_t slot_bytes(int64_t n, int64_t nnz, int64_t ell, bool mixed, bool col16 = false) {
+// Bytes of a slot's two allocations: the CSR as uploaded plus the vectors,
+// and the sliced-ELL copy.  Their sum is the admission test of the request loop.
+size_t csr_part_bytes(int64_t n, int64_t nnz, bool mixed) {
   const size_t tb = mixed ? 4 : 8;
-  const size_t padded = (size_t)((n + 31) / 32) * 32 * (size_t)ell;
   size_t b = align256(sizeof(int) * (n + 1)) + align256(sizeof(int) * nnz) + align256(8 * nnz);
-  b += align256((col16 ? 2 : 4) * padded) + align256(tb * padded);  // sliced-ELL columns and values
-  if (mixed) b += align256(8 * padded);               // and the FP64 values for the residual
-  b += 2 * align256(8 * n);                            // b, x
-  b += 5 * align256(tb * n);                           // c, r, p, Ap, invd
+  b += 2 * align256(8 * n);   // b, x
+  b += 5 * align256(tb * n);  // c, r, p, Ap, invd
   return b;
 }
+size_t sell_part_bytes(int64_t n, int64_t ell, bool mixed, bool col16) {
+  const size_t tb = mixed ? 4 : 8;
+  const size_t padded = (size_t)((n + 31) / 32) * 32 * (size_t)ell;
+  size_t b = align256((col16 ? 2 : 4) * padded) + align256(tb * padded);  // columns and values
+  if (mixed) b += align256(8 * padded);                                     // FP64 values (residual)
+  return b;
+}
+size_t slot_bytes(int64_t n, int64_t nnz, int64_t ell, bool mixed, bool col16 = false) {
+  return csr_part_bytes(n, nnz, mixed) + sell_part_bytes(n, ell, mixed, col16);
+}
 
-// Allocates a slot's buffers (one chunk) and carves them into a descriptor.
+// Allocates a slot's CSR part (one chunk: CSR as uploaded, b, x and the
+// work vectors) and carves it into a descriptor.
 template <typename T>
-int alloc_slot(BatchHandle B, int slot, int n, int64_t nnz, int ell, bool col16, SysDesc<T> *out) {
+int alloc_csr_part(BatchHandle B, int slot, int n, int64_t nnz, SysDesc<T> *out) {
   HostSys &h = B->sys[slot];
   cudaStream_t st = B->ctx->stream;
   const bool mixed = B->kp.mixed != 0;
-  h.bytes = slot_bytes(n, nnz, ell, mixed, col16);
-  B_CUDA(cudaMallocAsync(&h.chunk, h.bytes, st));
+  const size_t bytes = csr_part_bytes(n, nnz, mixed);
+  B_CUDA(cudaMallocAsync(&h.chunk, bytes, st));
+  h.bytes = bytes;
   char *p = (char *)h.chunk;
-  auto take = [&](size_t bytes) { char *q = p; p += align256(bytes); return (void *)q; };
+  auto take = [&](size_t nb) { char *q = p; p += align256(nb); return (void *)q; };
   SysDesc<T> d{};
   d.n = n;
   d.nnz = (int)nnz;
   d.rowptr = (const int *)take(sizeof(int) * (n + 1));
   d.col = (const int *)take(sizeof(int) * nnz);
   d.val64 = (const double *)take(8 * nnz);
-  const size_t padded = (size_t)((n + 31) / 32) * 32 * (size_t)ell;
-  d.ell = ell;
-  d.col16 = col16 ? 1 : 0;
-  d.scol = take((col16 ? 2 : 4) * padded);
-  d.sval = (const T *)take(sizeof(T) * padded);
-  d.sval64 = mixed ? (const double *)take(8 * padded) : (const double *)d.sval;
   d.b = (const double *)take(8 * n);
   d.x = (double *)take(8 * n);
   d.c = (T *)take(sizeof(T) * n);
@@ -782,6 +831,34 @@ int alloc_slot(BatchHandle B, int slot, int n, int64_t nnz, int ell, bool col16,
   d.invd = (const T *)take(sizeof(T) * n);
   *out = d;
   return B200LA_OK;
+}
+
+// Allocates the sliced-ELL part (second chunk) once ell and the column type
+// are known.
+template <typename T>
+int alloc_sell_part(BatchHandle B, int slot, int ell, bool col16, SysDesc<T> &d) {
+  HostSys &h = B->sys[slot];
+  cudaStream_t st = B->ctx->stream;
+  const bool mixed = B->kp.mixed != 0;
+  const size_t bytes = sell_part_bytes(d.n, ell, mixed, col16);
+  B_CUDA(cudaMallocAsync(&h.chunk2, bytes, st));
+  h.bytes += bytes;
+  char *p = (char *)h.chunk2;
+  auto take = [&](size_t nb) { char *q = p; p += align256(nb); return (void *)q; };
+  const size_t padded = (size_t)((d.n + 31) / 32) * 32 * (size_t)ell;
+  d.ell = ell;
+  d.col16 = col16 ? 1 : 0;
+  d.scol = take((col16 ? 2 : 4) * padded);
+  d.sval = (const T *)take(sizeof(T) * padded);
+  d.sval64 = mixed ? (const double *)take(8 * padded) : (const double *)d.sval;
+  return B200LA_OK;
+}
+
+void free_slot_memory(BatchHandle B, HostSys &h) {
+  cudaStream_t st = B->ctx->stream;
+  if (h.chunk) cudaFreeAsync(h.chunk, st);
+  if (h.chunk2) cudaFreeAsync(h.chunk2, st);
+  h.chunk = h.chunk2 = nullptr;
 }
 
 // Uploads the descriptor and a fresh RESID state, then builds the sliced-ELL
@@ -806,12 +883,16 @@ int finish_slot(BatchHandle B, int slot, const SysDesc<T> &d) {
   return B200LA_OK;
 }
 
+// Uploads a host CSR system into a slot: the CSR part is copied, checked on
+// the device (the checks of validate_csr, plus the longest row and the
+// largest |column - row|), and only then is the sliced-ELL part sized and
+// built.  One 16-byte read-back per system replaces two O(nnz) host passes.
 template <typename T>
-int add_typed(BatchHandle B, int slot, int n, int64_t nnz, int ell, bool col16, const int *rowptr, const int *col,
-              const double *val, const double *b, const double *x0) {
+int add_typed(BatchHandle B, int slot, int n, int64_t nnz, const int *rowptr, const int *col, const double *val,
+              const double *b, const double *x0) {
   cudaStream_t st = B->ctx->stream;
   SysDesc<T> d{};
-  B_TRY(alloc_slot<T>(B, slot, n, nnz, ell, col16, &d));
+  B_TRY(alloc_csr_part<T>(B, slot, n, nnz, &d));
   B_CUDA(cudaMemcpyAsync((void *)d.rowptr, rowptr, sizeof(int) * (n + 1), cudaMemcpyHostToDevice, st));
   if (nnz) {
     B_CUDA(cudaMemcpyAsync((void *)d.col, col, sizeof(int) * nnz, cudaMemcpyHostToDevice, st));
@@ -820,18 +901,25 @@ int add_typed(BatchHandle B, int slot, int n, int64_t nnz, int ell, bool col16, 
   B_CUDA(cudaMemcpyAsync((void *)d.b, b, 8 * n, cudaMemcpyHostToDevice, st));
   if (x0) B_CUDA(cudaMemcpyAsync(d.x, x0, 8 * n, cudaMemcpyHostToDevice, st));
   else B_CUDA(cudaMemsetAsync(d.x, 0, 8 * n, st));
+  CsrCheck init{~0ull, 0, 0};
+  B_CUDA(cudaMemcpyAsync(B->chk, &init, sizeof(CsrCheck), cudaMemcpyHostToDevice, st));
+  const int grid = (int)std::min<int64_t>((n + kBlock - 1) / kBlock, (int64_t)B->ctx->num_sms * 8);
+  csr_check_kernel<<<grid, kBlock, 0, st>>>(n, (int)nnz, d.rowptr, d.col, B->chk);
+  B_CUDA(cudaGetLastError());
+  B_CUDA(cudaMemcpyAsync(B->chk_host, B->chk, sizeof(CsrCheck), cudaMemcpyDeviceToHost, st));
+  B_CUDA(cudaStreamSynchronize(st));
+  const CsrCheck c = *B->chk_host;
+  if (c.err != ~0ull) {
+    const int row = (int)(c.err >> 8), code = (int)(c.err & 0xff);
+    if (code == kChkStart) return fail(B200LA_ERR_MATRIX, "csr: rowptr[0] != 0 or rowptr[nrow] != nnz %lld",
+                                       (long long)nnz);
+    if (code == kChkDecrease) return fail(B200LA_ERR_MATRIX, "csr: rowptr decreases at row %d", row);
+    if (code == kChkBounds) return fail(B200LA_ERR_MATRIX, "csr: rowptr out of [0, nnz] at row %d", row);
+    return fail(B200LA_ERR_MATRIX, "csr: a column of row %d is out of range [0,%d)", row, n);
+  }
+  const bool col16 = B->prm.index_bits != 32 && c.max_off <= 32767;
+  B_TRY(alloc_sell_part<T>(B, slot, std::max(c.max_row, 1), col16, d));
   return finish_slot<T>(B, slot, d);
-}
-
-// True when every column lies within int16 of its row: the sliced-ELL
-// columns are then stored as 2-byte offsets (FE orderings are banded).
-bool offsets_fit_int16(int n, const int *rowptr, const int *col) {
-  for (int i = 0; i < n; ++i)
-    for (int j = rowptr[i]; j < rowptr[i + 1]; ++j) {
-      const int d = col[j] - i;
-      if (d < -32768 || d > 32767) return false;
-    }
-  return true;
 }
 
 // Q1 rows couple nodes at most one cell away: offset (m + 1) + 1 in 2D,
@@ -1201,9 +1289,8 @@ int b200la_batch_destroy(b200la_batch B) {
   cudaStreamSynchronize(st);
   if (B->exec) cudaGraphExecDestroy(B->exec);
   if (B->graph) cudaGraphDestroy(B->graph);
-  for (HostSys &h : B->sys)
-    if (h.chunk) cudaFreeAsync(h.chunk, st);
-  void *bufs[] = {B->desc, B->st, B->glob};
+  for (HostSys &h : B->sys) free_slot_memory(B, h);
+  void *bufs[] = {B->desc, B->st, B->glob, B->chk};
   for (void *p : bufs)
     if (p) cudaFreeAsync(p, st);
   for (ItemList &L : B->lst) {
@@ -1211,8 +1298,15 @@ int b200la_batch_destroy(b200la_batch B) {
     if (L.part) cudaFreeAsync(L.part, st);
   }
   if (B->st_host) cudaFreeHost(B->st_host);
+  if (B->chk_host) cudaFreeHost(B->chk_host);
   if (B->glob_host) cudaFreeHost(B->glob_host);
   cudaStreamSynchronize(st);
+  {
+    // return the pool's free blocks to the driver (the context keeps freed
+    // blocks while batches add and remove systems)
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, B->ctx->device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
+  }
   delete B;
   return B200LA_OK;
 }
@@ -1244,6 +1338,8 @@ int b200la_batch_create(b200la_ctx ctx, const b200la_batch_params *p, b200la_bat
   bool ok = cudaMallocAsync(&B->desc, dsz * p->capacity, st) == cudaSuccess &&
             cudaMallocAsync(&B->st, sizeof(SysState) * p->capacity, st) == cudaSuccess &&
             cudaMallocAsync(&B->glob, sizeof(BatchGlobals), st) == cudaSuccess &&
+            cudaMallocAsync(&B->chk, sizeof(CsrCheck), st) == cudaSuccess &&
+            cudaMallocHost(&B->chk_host, sizeof(CsrCheck)) == cudaSuccess &&
             cudaMallocHost(&B->st_host, sizeof(SysState) * p->capacity) == cudaSuccess &&
             cudaMallocHost(&B->glob_host, sizeof(BatchGlobals)) == cudaSuccess;
   if (ok) {
@@ -1265,8 +1361,10 @@ int b200la_batch_add(b200la_batch B, int n, int64_t nnz, const int *rowptr, cons
                      const double *b, const double *x0, int *slot_out) {
   B_CHECK(B && slot_out && b, B200LA_ERR_INVALID, "batch_add: null argument");
   B_CHECK(n > 0, B200LA_ERR_INVALID, "batch_add: empty system");
-  int max_row = 0;
-  B_TRY(validate_csr(n, n, nnz, rowptr, col, &max_row));
+  B_CHECK(nnz >= 0 && nnz < (int64_t)INT32_MAX, B200LA_ERR_MATRIX, "csr: nnz %lld exceeds int32 indexing",
+          (long long)nnz);
+  B_CHECK(rowptr, B200LA_ERR_MATRIX, "csr: rowptr is NULL");
+  B_CHECK(nnz == 0 || col, B200LA_ERR_MATRIX, "csr: col is NULL");
   B_CHECK(nnz == 0 || val, B200LA_ERR_MATRIX, "batch_add: val is NULL");
   const int slot = find_free_slot(B);
   B_CHECK(slot >= 0, B200LA_ERR_NOMEM, "batch_add: all %d slots are in use", B->capacity);
@@ -1274,12 +1372,11 @@ int b200la_batch_add(b200la_batch B, int n, int64_t nnz, const int *rowptr, cons
   h = HostSys();
   h.n = n;
   h.nnz = (int)nnz;
-  const int ell = std::max(max_row, 1);
-  const bool col16 = B->prm.index_bits != 32 && offsets_fit_int16(n, rowptr, col);
-  const int rc = B->kp.mixed ? add_typed<float>(B, slot, n, nnz, ell, col16, rowptr, col, val, b, x0)
-                             : add_typed<double>(B, slot, n, nnz, ell, col16, rowptr, col, val, b, x0);
+  // the structure is checked on the device after the upload (add_typed)
+  const int rc = B->kp.mixed ? add_typed<float>(B, slot, n, nnz, rowptr, col, val, b, x0)
+                             : add_typed<double>(B, slot, n, nnz, rowptr, col, val, b, x0);
   if (rc != B200LA_OK) {
-    if (h.chunk) cudaFreeAsync(h.chunk, B->ctx->stream);
+    free_slot_memory(B, h);
     h = HostSys();
     return rc;
   }
@@ -1307,7 +1404,8 @@ int b200la_batch_add_q1(b200la_batch B, int dim, int cells, uint64_t seed, doubl
   auto go = [&](auto tag) -> int {
     using T = decltype(tag);
     SysDesc<T> d{};
-    B_TRY(alloc_slot<T>(B, slot, n, nnz, ell, B->prm.index_bits != 32 && q1_col16(dim, cells), &d));
+    B_TRY(alloc_csr_part<T>(B, slot, n, nnz, &d));
+    B_TRY(alloc_sell_part<T>(B, slot, ell, B->prm.index_bits != 32 && q1_col16(dim, cells), d));
     B_TRY(q1_assemble(st, B->ctx->num_sms, dim, cells, seed, sigma, (int *)d.rowptr, (int *)d.col,
                       (double *)d.val64, (double *)d.b));
     B_CUDA(cudaMemsetAsync(d.x, 0, 8 * (size_t)n, st));
@@ -1315,7 +1413,7 @@ int b200la_batch_add_q1(b200la_batch B, int dim, int cells, uint64_t seed, doubl
   };
   const int rc = B->kp.mixed ? go(float()) : go(double());
   if (rc != B200LA_OK) {
-    if (h.chunk) cudaFreeAsync(h.chunk, st);
+    free_slot_memory(B, h);
     h = HostSys();
     return rc;
   }
@@ -1353,12 +1451,13 @@ int b200la_batch_remove(b200la_batch B, int slot) {
           slot);
   HostSys &h = B->sys[slot];
   cudaStream_t st = B->ctx->stream;
-  B_CUDA(cudaFreeAsync(h.chunk, st));
+  // stream-ordered: the slot's memory is released after the work queued
+  // before it, and its device state is cleared; no host wait
+  free_slot_memory(B, h);
   B->device_bytes -= (int64_t)h.bytes;
   h = HostSys();
   memset(&B->st_host[slot], 0, sizeof(SysState));
-  B_CUDA(cudaMemcpyAsync(B->st + slot, &B->st_host[slot], sizeof(SysState), cudaMemcpyHostToDevice, st));
-  B_CUDA(cudaStreamSynchronize(st));
+  B_CUDA(cudaMemsetAsync(B->st + slot, 0, sizeof(SysState), st));
   return B200LA_OK;
 }
 
@@ -1406,7 +1505,10 @@ int b200la_batch_last_run(b200la_batch B, int *passes, double *reserved) {
   return B200LA_OK;
 }
 
-int b200la_batch_result(b200la_batch B, int slot, double *x_host, b200la_sys_result *r) {
+namespace {
+// Host copy of a slot's result from the last run's state read-back; the
+// solution copy, if asked for, is queued on the context stream.
+int fill_result(b200la_batch B, int slot, double *x_host, b200la_sys_result *r) {
   B_CHECK(B && r && slot >= 0 && slot < B->capacity && B->sys[slot].used, B200LA_ERR_INVALID,
           "batch_result: slot %d", slot);
   const HostSys &h = B->sys[slot];
@@ -1428,8 +1530,27 @@ int b200la_batch_result(b200la_batch B, int slot, double *x_host, b200la_sys_res
   if (x_host) {
     const double *xd = B->kp.mixed ? h.d32.x : h.d64.x;
     B_CUDA(cudaMemcpyAsync(x_host, xd, 8 * (size_t)h.n, cudaMemcpyDeviceToHost, B->ctx->stream));
-    B_CUDA(cudaStreamSynchronize(B->ctx->stream));
   }
+  return B200LA_OK;
+}
+}  // namespace
+
+int b200la_batch_result(b200la_batch B, int slot, double *x_host, b200la_sys_result *r) {
+  B_TRY(fill_result(B, slot, x_host, r));
+  if (x_host) B_CUDA(cudaStreamSynchronize(B->ctx->stream));
+  return B200LA_OK;
+}
+
+int b200la_batch_results(b200la_batch B, int count, const int *slots, double *const *x_host,
+                         b200la_sys_result *results) {
+  B_CHECK(B && count >= 0 && (count == 0 || (slots && results)), B200LA_ERR_INVALID, "batch_results: bad argument");
+  bool any = false;
+  for (int k = 0; k < count; ++k) {
+    double *x = x_host ? x_host[k] : nullptr;
+    B_TRY(fill_result(B, slots[k], x, &results[k]));
+    any = any || x;
+  }
+  if (any) B_CUDA(cudaStreamSynchronize(B->ctx->stream));
   return B200LA_OK;
 }
 

@@ -269,6 +269,19 @@ int b200la_ctx_create(int device, b200la_ctx *out) {
   B_CUDA(cudaMalloc(&c->scratch.result, sizeof(double) * 8));
   B_CUDA(cudaMemset(c->scratch.ticket, 0, sizeof(unsigned) * 16));
   B_CUDA(cudaMallocHost(&c->host_result, sizeof(double) * 8));
+  // Stream-ordered allocations (batch slots, tile lists, scratch) come from
+  // the device's default pool.  Keep freed blocks in the pool instead of
+  // returning them to the driver at every synchronisation, so adding and
+  // removing systems in a loop reuses memory rather than remapping it.  The
+  // attribute lives only in this process; batches trim the pool when they
+  // are destroyed.
+  {
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+      uint64_t keep = UINT64_MAX;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+  }
   *out = c;
   return B200LA_OK;
 }

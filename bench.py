@@ -307,27 +307,19 @@ def run_batch(args, rank, local_rank, world, torch, dist, barrier):
     # end to end through the public API: upload every system from pinned host
     # memory, solve, download every solution, each step
     E = Batch(cap, **kw)
-    E.add(*host[0])
-    E.tune()
+    E.set_items(*B.items(), adaptive=False)  # the schedule tuned on the full batch
     xs = [torch.empty(s.n, dtype=torch.float64).pin_memory().numpy() for s in systems]
     h2d = int(sum(h[0].nbytes + h[1].nbytes + h[2].nbytes + h[3].nbytes for h in host))
     d2h = int(sum(x.nbytes for x in xs))
-    import ctypes as C
-    from ba_b200._lib import SysResult, load
-    lib = load()
-
     def e2e_step():
         for k in range(len(systems)):
             try:
                 E.remove(k)
             except Exception:
                 pass
-        for h in host:
-            E.add(*h)
+        slots = [E.add(*h) for h in host]
         E.solve(CHUNK)
-        r = SysResult()
-        for k, x in enumerate(xs):
-            lib.b200la_batch_result(E.handle, k, x.ctypes.data_as(C.c_void_p), C.byref(r))
+        E.results(slots, out=xs)
 
     e2e_step()
     barrier()

@@ -283,8 +283,10 @@ int b200la_batch_destroy(b200la_batch b);
  * longest row max_row (the admission test of a request loop). */
 int b200la_batch_slot_bytes(int64_t n, int64_t nnz, int max_row, int mixed, int64_t *bytes);
 /* Upload one system (host CSR, FP64 values, FP64 RHS; x0 NULL = zero start)
- * into a free slot; it joins at the next run.  Copies are queued on the
- * context stream: host buffers must stay valid until the next run. */
+ * into a free slot; it joins at the next run.  The structure is checked on
+ * the device after the copy (the checks of b200la_csr_upload; malformed CSR
+ * returns B200LA_ERR_MATRIX and leaves the slot free), so the call waits for
+ * its own copies: host buffers may be reused on return. */
 int b200la_batch_add(b200la_batch b, int n, int64_t nnz, const int *rowptr, const int *col,
                      const double *val, const double *rhs, const double *x0, int *slot);
 /* Assemble a Q1 diffusion system on the device directly into a free slot:
@@ -295,6 +297,7 @@ int b200la_batch_add_q1(b200la_batch b, int dim, int cells, uint64_t seed, doubl
 /* Copy a slot's system back to the host (any pointer may be NULL). */
 int b200la_batch_get_system(b200la_batch b, int slot, int *rowptr, int *col, double *val, double *rhs);
 int b200la_batch_slot_size(b200la_batch b, int slot, int *n, int64_t *nnz);
+/* Frees a slot (stream-ordered: after the work already queued; no wait). */
 int b200la_batch_remove(b200la_batch b, int slot);
 /* One graph launch: at most max_passes iterations of every running system.
  * Writes how many systems are still running. */
@@ -307,6 +310,10 @@ int b200la_batch_solve(b200la_batch b, int chunk_passes, int *total_passes);
 int b200la_batch_last_run(b200la_batch b, int *passes, double *reserved);
 /* Result of a slot (solution copied to x if non-NULL). */
 int b200la_batch_result(b200la_batch b, int slot, double *x, b200la_sys_result *result);
+/* Results of `count` slots at once; x[k] (or x itself) may be NULL.  The
+ * solution copies are queued together and waited for once. */
+int b200la_batch_results(b200la_batch b, int count, const int *slots, double *const *x,
+                         b200la_sys_result *results);
 int b200la_batch_info(b200la_batch b, int *used_slots, int64_t *device_bytes);
 /* Restart every system in the batch from x = 0 (matrices and RHS stay). */
 int b200la_batch_restart(b200la_batch b);

@@ -173,3 +173,27 @@ def test_device_assembly_matches_host_generator(plat, dim, cells, sigma):
     r = B.result(slot)
     assert r.done and r.solver_state == lmp.kSolverSuccess
     assert _true_rel_res(s, r.x) < 1.001e-8
+
+
+def test_malformed_csr_is_refused_on_the_device_check(plat):
+    """batch_add checks the uploaded structure on the device (the checks of
+    csr_upload): a bad system returns B200LA_ERR_MATRIX and leaves no slot
+    behind; the batch keeps working."""
+    B = Batch(4, mixed=True, rtol=1e-8, platform=plat)
+    good = P.q1_system(2, 12, 9, 1.0)
+    bad_cases = [
+        (np.array([0, 2, 3], np.int32), np.array([0, 5, 1], np.int32)),   # column out of range
+        (np.array([0, 3, 2], np.int32), np.array([0, 1, 1], np.int32)),   # rowptr decreases
+        (np.array([1, 2, 3], np.int32), np.array([0, 1, 1], np.int32)),   # rowptr[0] != 0
+        (np.array([0, 1, 7], np.int32), np.array([0, 1, 1], np.int32)),   # rowptr[n] != nnz
+    ]
+    for rp, cl in bad_cases:
+        with pytest.raises(lmp.B200LAError) as e:
+            B.add(rp, cl, np.ones(cl.shape[0]), np.ones(2))
+        assert e.value.status == -5, e.value
+        assert B.info()[0] == 0
+    s = B.add_system(good)
+    assert B.info()[0] == 1
+    B.solve()
+    r = B.results([s])[0]
+    assert r.solver_state == lmp.kSolverSuccess and _true_rel_res(good, r.x) < 1.001e-8
