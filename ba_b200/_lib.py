@@ -141,6 +141,7 @@ _SIGS = {
     "b200la_batch_profile": [_vp, _i, _P(_d), _P(_i64)],
     "b200la_batch_profile_pass": [_vp, _i, _P(_d), _P(_i64)],
     "b200la_batch_add_q1": [_vp, _i, _i, C.c_uint64, _d, _P(_i)],
+    "b200la_batch_add_many": [_vp, _i, _P(_i), _P(_i64), _P(_vp), _P(_vp), _P(_vp), _P(_vp), _P(_vp), _P(_i), _P(_i)],
     "b200la_batch_get_system": [_vp, _i, _vp, _vp, _vp, _vp],
     "b200la_batch_slot_size": [_vp, _i, _P(_i), _P(_i64)],
     "b200la_server_start": [_vp, _P(ServerParams), _P(_vp)],

@@ -68,6 +68,36 @@ class Batch:
         self._sizes[slot.value] = rp.shape[0] - 1
         return slot.value
 
+    def add_many(self, systems) -> list[int]:
+        """Add many systems, each (rowptr, col, val, rhs[, x0]), with one wait
+        for all the device checks; raises on the first failure (the others
+        that succeeded stay added: see `last_slots` and `last_status`)."""
+        arrs = []
+        for t in systems:
+            rp = np.ascontiguousarray(t[0], np.int32)
+            cl = np.ascontiguousarray(t[1], np.int32)
+            vv = np.ascontiguousarray(t[2], np.float64)
+            bb = np.ascontiguousarray(t[3], np.float64)
+            xx = None if len(t) < 5 or t[4] is None else np.ascontiguousarray(t[4], np.float64)
+            arrs.append((rp, cl, vv, bb, xx))
+        k = len(arrs)
+        ptr = lambda a: None if a is None else a.ctypes.data  # noqa: E731
+        n = (C.c_int * k)(*[a[0].shape[0] - 1 for a in arrs])
+        nnz = (C.c_int64 * k)(*[a[1].shape[0] for a in arrs])
+        P = C.c_void_p * k
+        slots, status = (C.c_int * k)(), (C.c_int * k)()
+        rc = load().b200la_batch_add_many(self.handle, k, n, nnz, P(*[ptr(a[0]) for a in arrs]),
+                                          P(*[ptr(a[1]) for a in arrs]), P(*[ptr(a[2]) for a in arrs]),
+                                          P(*[ptr(a[3]) for a in arrs]), P(*[ptr(a[4]) for a in arrs]), slots, status)
+        out = list(slots)
+        for j, sl in enumerate(out):
+            if sl >= 0:
+                self._sizes[sl] = arrs[j][0].shape[0] - 1
+        self.last_status = list(status)
+        self.last_slots = out
+        _lib.check(rc)
+        return out
+
     def add_system(self, s, x0=None) -> int:
         return self.add(s.rowptr, s.col, s.val, s.b, x0)
 

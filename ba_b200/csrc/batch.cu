@@ -672,6 +672,11 @@ struct CsrCheck {
   int max_off;
 };
 
+__global__ void csr_check_init_kernel(int count, CsrCheck *c) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x)
+    c[k] = CsrCheck{~0ull, 0, 0};
+}
+
 __global__ void csr_check_kernel(int n, int nnz, const int *__restrict__ rowptr, const int *__restrict__ col,
                                  CsrCheck *out) {
   const int stride = gridDim.x * blockDim.x;
@@ -766,8 +771,9 @@ struct b200la_batch_s {
   void *desc;         // SysDesc<T>[capacity]
   SysState *st;       // [capacity]
   BatchGlobals *glob;
-  CsrCheck *chk;       // device result of csr_check_kernel
+  CsrCheck *chk;       // device results of csr_check_kernel, one per system of an add
   CsrCheck *chk_host;  // pinned mirror
+  int chk_cap;
   // host mirrors
   SysState *st_host;  // pinned [capacity]
   BatchGlobals *glob_host;
@@ -883,43 +889,60 @@ int finish_slot(BatchHandle B, int slot, const SysDesc<T> &d) {
   return B200LA_OK;
 }
 
-// Uploads a host CSR system into a slot: the CSR part is copied, checked on
-// the device (the checks of validate_csr, plus the longest row and the
-// largest |column - row|), and only then is the sliced-ELL part sized and
-// built.  One 16-byte read-back per system replaces two O(nnz) host passes.
+// Uploading a host CSR system into a slot, in two stages: (1) the CSR part
+// is allocated and copied, and a device check (those of validate_csr, plus
+// the longest row and the largest |column - row|) writes its verdict to
+// `chk`; (2) after the caller has read the verdict back, the sliced-ELL part
+// is sized and built, or the error is reported.  One small read-back per
+// system (or per bulk add) replaces two O(nnz) host passes.
 template <typename T>
-int add_typed(BatchHandle B, int slot, int n, int64_t nnz, const int *rowptr, const int *col, const double *val,
-              const double *b, const double *x0) {
+int upload_stage(BatchHandle B, int slot, int n, int64_t nnz, const int *rowptr, const int *col, const double *val,
+                 const double *b, const double *x0, CsrCheck *chk, SysDesc<T> *d) {
   cudaStream_t st = B->ctx->stream;
-  SysDesc<T> d{};
-  B_TRY(alloc_csr_part<T>(B, slot, n, nnz, &d));
-  B_CUDA(cudaMemcpyAsync((void *)d.rowptr, rowptr, sizeof(int) * (n + 1), cudaMemcpyHostToDevice, st));
+  B_TRY(alloc_csr_part<T>(B, slot, n, nnz, d));
+  B_CUDA(cudaMemcpyAsync((void *)d->rowptr, rowptr, sizeof(int) * (n + 1), cudaMemcpyHostToDevice, st));
   if (nnz) {
-    B_CUDA(cudaMemcpyAsync((void *)d.col, col, sizeof(int) * nnz, cudaMemcpyHostToDevice, st));
-    B_CUDA(cudaMemcpyAsync((void *)d.val64, val, 8 * nnz, cudaMemcpyHostToDevice, st));
+    B_CUDA(cudaMemcpyAsync((void *)d->col, col, sizeof(int) * nnz, cudaMemcpyHostToDevice, st));
+    B_CUDA(cudaMemcpyAsync((void *)d->val64, val, 8 * nnz, cudaMemcpyHostToDevice, st));
   }
-  B_CUDA(cudaMemcpyAsync((void *)d.b, b, 8 * n, cudaMemcpyHostToDevice, st));
-  if (x0) B_CUDA(cudaMemcpyAsync(d.x, x0, 8 * n, cudaMemcpyHostToDevice, st));
-  else B_CUDA(cudaMemsetAsync(d.x, 0, 8 * n, st));
-  CsrCheck init{~0ull, 0, 0};
-  B_CUDA(cudaMemcpyAsync(B->chk, &init, sizeof(CsrCheck), cudaMemcpyHostToDevice, st));
+  B_CUDA(cudaMemcpyAsync((void *)d->b, b, 8 * n, cudaMemcpyHostToDevice, st));
+  if (x0) B_CUDA(cudaMemcpyAsync(d->x, x0, 8 * n, cudaMemcpyHostToDevice, st));
+  else B_CUDA(cudaMemsetAsync(d->x, 0, 8 * n, st));
   const int grid = (int)std::min<int64_t>((n + kBlock - 1) / kBlock, (int64_t)B->ctx->num_sms * 8);
-  csr_check_kernel<<<grid, kBlock, 0, st>>>(n, (int)nnz, d.rowptr, d.col, B->chk);
+  csr_check_kernel<<<grid, kBlock, 0, st>>>(n, (int)nnz, d->rowptr, d->col, chk);
   B_CUDA(cudaGetLastError());
-  B_CUDA(cudaMemcpyAsync(B->chk_host, B->chk, sizeof(CsrCheck), cudaMemcpyDeviceToHost, st));
-  B_CUDA(cudaStreamSynchronize(st));
-  const CsrCheck c = *B->chk_host;
+  return B200LA_OK;
+}
+
+template <typename T>
+int finish_stage(BatchHandle B, int slot, const CsrCheck &c, SysDesc<T> &d) {
   if (c.err != ~0ull) {
     const int row = (int)(c.err >> 8), code = (int)(c.err & 0xff);
-    if (code == kChkStart) return fail(B200LA_ERR_MATRIX, "csr: rowptr[0] != 0 or rowptr[nrow] != nnz %lld",
-                                       (long long)nnz);
+    if (code == kChkStart)
+      return fail(B200LA_ERR_MATRIX, "csr: rowptr[0] != 0 or rowptr[nrow] != nnz %d", d.nnz);
     if (code == kChkDecrease) return fail(B200LA_ERR_MATRIX, "csr: rowptr decreases at row %d", row);
     if (code == kChkBounds) return fail(B200LA_ERR_MATRIX, "csr: rowptr out of [0, nnz] at row %d", row);
-    return fail(B200LA_ERR_MATRIX, "csr: a column of row %d is out of range [0,%d)", row, n);
+    return fail(B200LA_ERR_MATRIX, "csr: a column of row %d is out of range [0,%d)", row, d.n);
   }
   const bool col16 = B->prm.index_bits != 32 && c.max_off <= 32767;
   B_TRY(alloc_sell_part<T>(B, slot, std::max(c.max_row, 1), col16, d));
   return finish_slot<T>(B, slot, d);
+}
+
+// Grows the per-batch check records (device and pinned host) to `count`.
+int ensure_checks(BatchHandle B, int count) {
+  if (count <= B->chk_cap) return B200LA_OK;
+  cudaStream_t st = B->ctx->stream;
+  const int cap = std::max(count, 2 * B->chk_cap);
+  if (B->chk) cudaFreeAsync(B->chk, st);
+  if (B->chk_host) cudaFreeHost(B->chk_host);
+  B->chk = nullptr;
+  B->chk_host = nullptr;
+  B->chk_cap = 0;
+  B_CUDA(cudaMallocAsync(&B->chk, sizeof(CsrCheck) * cap, st));
+  B_CUDA(cudaMallocHost(&B->chk_host, sizeof(CsrCheck) * cap));
+  B->chk_cap = cap;
+  return B200LA_OK;
 }
 
 // Q1 rows couple nodes at most one cell away: offset (m + 1) + 1 in 2D,
@@ -1273,6 +1296,82 @@ int snapshot_restore(BatchHandle B, const Snapshot &sn) {
   return B200LA_OK;
 }
 
+// Adds `count` host CSR systems: every system's copies and device check are
+// queued first, the verdicts are read back with one wait, then each valid
+// system gets its sliced-ELL part.  status[k] is each system's outcome; the
+// return value is the first failure's (its message stays in last_error).
+template <typename T>
+int add_many_t(BatchHandle B, int count, const int *n, const int64_t *nnz, const int *const *rowptr,
+               const int *const *col, const double *const *val, const double *const *rhs,
+               const double *const *x0, int *slots, int *status) {
+  cudaStream_t st = B->ctx->stream;
+  B_TRY(ensure_checks(B, count));
+  csr_check_init_kernel<<<std::max(1, std::min((count + kBlock - 1) / kBlock, 64)), kBlock, 0, st>>>(count, B->chk);
+  B_CUDA(cudaGetLastError());
+  std::vector<int> sl(count, -1);
+  std::vector<SysDesc<T>> d(count);
+  int first = B200LA_OK;
+  std::string first_msg;
+  auto note = [&](int k, int rc) {
+    status[k] = rc;
+    if (first == B200LA_OK && rc != B200LA_OK) {
+      first = rc;
+      first_msg = b200la_last_error();
+    }
+  };
+  for (int k = 0; k < count; ++k) {
+    slots[k] = -1;
+    status[k] = B200LA_OK;
+    int rc = B200LA_OK;
+    if (n[k] <= 0) rc = fail(B200LA_ERR_INVALID, "batch_add: empty system");
+    else if (nnz[k] < 0 || nnz[k] >= (int64_t)INT32_MAX)
+      rc = fail(B200LA_ERR_MATRIX, "csr: nnz %lld exceeds int32 indexing", (long long)nnz[k]);
+    else if (!rowptr[k]) rc = fail(B200LA_ERR_MATRIX, "csr: rowptr is NULL");
+    else if (nnz[k] && (!col[k] || !val[k])) rc = fail(B200LA_ERR_MATRIX, "csr: col or val is NULL");
+    else if (!rhs[k]) rc = fail(B200LA_ERR_INVALID, "batch_add: rhs is NULL");
+    if (rc != B200LA_OK) {
+      note(k, rc);
+      continue;
+    }
+    const int slot = find_free_slot(B);
+    if (slot < 0) {
+      note(k, fail(B200LA_ERR_NOMEM, "batch_add: all %d slots are in use", B->capacity));
+      continue;
+    }
+    HostSys &h = B->sys[slot];
+    h = HostSys();
+    h.n = n[k];
+    h.nnz = (int)nnz[k];
+    h.used = true;  // reserved while its copies and check are in flight
+    rc = upload_stage<T>(B, slot, n[k], nnz[k], rowptr[k], col[k], val[k], rhs[k], x0 ? x0[k] : nullptr,
+                         B->chk + k, &d[k]);
+    if (rc != B200LA_OK) {
+      free_slot_memory(B, h);
+      h = HostSys();
+      note(k, rc);
+      continue;
+    }
+    sl[k] = slot;
+  }
+  B_CUDA(cudaMemcpyAsync(B->chk_host, B->chk, sizeof(CsrCheck) * count, cudaMemcpyDeviceToHost, st));
+  B_CUDA(cudaStreamSynchronize(st));
+  for (int k = 0; k < count; ++k) {
+    if (sl[k] < 0) continue;
+    HostSys &h = B->sys[sl[k]];
+    const int rc = finish_stage<T>(B, sl[k], B->chk_host[k], d[k]);
+    if (rc != B200LA_OK) {
+      free_slot_memory(B, h);
+      h = HostSys();
+      note(k, rc);
+      continue;
+    }
+    B->device_bytes += (int64_t)h.bytes;
+    slots[k] = sl[k];
+  }
+  if (first != B200LA_OK) set_error(first_msg);
+  return first;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1338,8 +1437,7 @@ int b200la_batch_create(b200la_ctx ctx, const b200la_batch_params *p, b200la_bat
   bool ok = cudaMallocAsync(&B->desc, dsz * p->capacity, st) == cudaSuccess &&
             cudaMallocAsync(&B->st, sizeof(SysState) * p->capacity, st) == cudaSuccess &&
             cudaMallocAsync(&B->glob, sizeof(BatchGlobals), st) == cudaSuccess &&
-            cudaMallocAsync(&B->chk, sizeof(CsrCheck), st) == cudaSuccess &&
-            cudaMallocHost(&B->chk_host, sizeof(CsrCheck)) == cudaSuccess &&
+            ensure_checks(B, 64) == B200LA_OK &&
             cudaMallocHost(&B->st_host, sizeof(SysState) * p->capacity) == cudaSuccess &&
             cudaMallocHost(&B->glob_host, sizeof(BatchGlobals)) == cudaSuccess;
   if (ok) {
@@ -1360,30 +1458,20 @@ int b200la_batch_create(b200la_ctx ctx, const b200la_batch_params *p, b200la_bat
 int b200la_batch_add(b200la_batch B, int n, int64_t nnz, const int *rowptr, const int *col, const double *val,
                      const double *b, const double *x0, int *slot_out) {
   B_CHECK(B && slot_out && b, B200LA_ERR_INVALID, "batch_add: null argument");
-  B_CHECK(n > 0, B200LA_ERR_INVALID, "batch_add: empty system");
-  B_CHECK(nnz >= 0 && nnz < (int64_t)INT32_MAX, B200LA_ERR_MATRIX, "csr: nnz %lld exceeds int32 indexing",
-          (long long)nnz);
-  B_CHECK(rowptr, B200LA_ERR_MATRIX, "csr: rowptr is NULL");
-  B_CHECK(nnz == 0 || col, B200LA_ERR_MATRIX, "csr: col is NULL");
-  B_CHECK(nnz == 0 || val, B200LA_ERR_MATRIX, "batch_add: val is NULL");
-  const int slot = find_free_slot(B);
-  B_CHECK(slot >= 0, B200LA_ERR_NOMEM, "batch_add: all %d slots are in use", B->capacity);
-  HostSys &h = B->sys[slot];
-  h = HostSys();
-  h.n = n;
-  h.nnz = (int)nnz;
-  // the structure is checked on the device after the upload (add_typed)
-  const int rc = B->kp.mixed ? add_typed<float>(B, slot, n, nnz, rowptr, col, val, b, x0)
-                             : add_typed<double>(B, slot, n, nnz, rowptr, col, val, b, x0);
-  if (rc != B200LA_OK) {
-    free_slot_memory(B, h);
-    h = HostSys();
-    return rc;
-  }
-  h.used = true;
-  B->device_bytes += (int64_t)h.bytes;
-  *slot_out = slot;
-  return B200LA_OK;
+  int status = B200LA_OK;
+  const double *x0s[1] = {x0};
+  return B->kp.mixed ? add_many_t<float>(B, 1, &n, &nnz, &rowptr, &col, &val, &b, x0s, slot_out, &status)
+                     : add_many_t<double>(B, 1, &n, &nnz, &rowptr, &col, &val, &b, x0s, slot_out, &status);
+}
+
+int b200la_batch_add_many(b200la_batch B, int count, const int *n, const int64_t *nnz, const int *const *rowptr,
+                          const int *const *col, const double *const *val, const double *const *rhs,
+                          const double *const *x0, int *slots, int *status) {
+  B_CHECK(B && count >= 0 && (count == 0 || (n && nnz && rowptr && col && val && rhs && slots && status)),
+          B200LA_ERR_INVALID, "batch_add_many: null argument");
+  if (count == 0) return B200LA_OK;
+  return B->kp.mixed ? add_many_t<float>(B, count, n, nnz, rowptr, col, val, rhs, x0, slots, status)
+                     : add_many_t<double>(B, count, n, nnz, rowptr, col, val, rhs, x0, slots, status);
 }
 
 int b200la_batch_add_q1(b200la_batch B, int dim, int cells, uint64_t seed, double sigma, int *slot_out) {

@@ -317,7 +317,7 @@ def run_batch(args, rank, local_rank, world, torch, dist, barrier):
                 E.remove(k)
             except Exception:
                 pass
-        slots = [E.add(*h) for h in host]
+        slots = E.add_many(host)
         E.solve(CHUNK)
         E.results(slots, out=xs)
 

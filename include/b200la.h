@@ -294,6 +294,14 @@ int b200la_batch_add(b200la_batch b, int n, int64_t nnz, const int *rowptr, cons
  * exp(sigma * g) (sigma = 0: Poisson), homogeneous Dirichlet rows, RHS
  * U[0,1) on interior rows, from `seed` (see b200la_q1_assemble). */
 int b200la_batch_add_q1(b200la_batch b, int dim, int cells, uint64_t seed, double sigma, int *slot);
+/* Adds `count` systems (arrays of the arguments of b200la_batch_add; x0 may
+ * be NULL, or hold NULL entries): all copies and device checks are queued,
+ * then waited for once.  slots[k] is each system's slot (-1 if it failed),
+ * status[k] its status; returns the first failure's status (B200LA_OK if
+ * every system was added). */
+int b200la_batch_add_many(b200la_batch b, int count, const int *n, const int64_t *nnz, const int *const *rowptr,
+                          const int *const *col, const double *const *val, const double *const *rhs,
+                          const double *const *x0, int *slots, int *status);
 /* Copy a slot's system back to the host (any pointer may be NULL). */
 int b200la_batch_get_system(b200la_batch b, int slot, int *rowptr, int *col, double *val, double *rhs);
 int b200la_batch_slot_size(b200la_batch b, int slot, int *n, int64_t *nnz);

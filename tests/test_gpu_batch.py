@@ -197,3 +197,27 @@ def test_malformed_csr_is_refused_on_the_device_check(plat):
     B.solve()
     r = B.results([s])[0]
     assert r.solver_state == lmp.kSolverSuccess and _true_rel_res(good, r.x) < 1.001e-8
+
+
+def test_add_many_matches_single_adds_and_reports_per_system_status(plat):
+    """The bulk add gives each system the result it gets from a single add
+    (bit for bit) and reports a malformed one on its own."""
+    systems = _mix(seed=4, count=5)
+    A = Batch(8, mixed=True, rtol=1e-8, platform=plat)
+    one = [A.add_system(s) for s in systems]
+    A.solve()
+    M = Batch(8, mixed=True, rtol=1e-8, platform=plat)
+    bad = (np.array([0, 2, 3], np.int32), np.array([0, 9, 1], np.int32), np.ones(3), np.ones(2))
+    items = [(s.rowptr, s.col, s.val, s.b) for s in systems]
+    items.insert(2, bad)
+    with pytest.raises(lmp.B200LAError) as e:
+        M.add_many(items)
+    assert e.value.status == -5
+    assert M.last_status == [0, 0, -5, 0, 0, 0]
+    assert M.last_slots[2] == -1 and M.info()[0] == 5
+    M.solve()
+    good = [sl for sl in M.last_slots if sl >= 0]
+    for a_slot, rm in zip(one, M.results(good)):
+        ra = A.results([a_slot])[0]
+        assert rm.solver_state == lmp.kSolverSuccess
+        np.testing.assert_array_equal(ra.x, rm.x)
