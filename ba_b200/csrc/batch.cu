@@ -180,7 +180,12 @@ __device__ __forceinline__ int outer_check(double res, double res0, const BatchP
   return B200LA_ITERATE;
 }
 
-__device__ __forceinline__ int load_phase(const SysState *s) { return *(volatile const int *)&s->phase; }
+// A system's phase (and alpha, beta) can change inside a kernel only when its
+// last item to arrive writes them, after every other item of that system has
+// read them; kernel launches refresh the read-only cache.  So the read-only
+// path is safe, and it keeps the items of one large system from all asking
+// L2 for the same line.
+__device__ __forceinline__ int load_phase(const SysState *s) { return __ldg(&s->phase); }
 
 __device__ __forceinline__ void finish_system(SysState &S, BatchGlobals *g, int state) {
   S.state = state;

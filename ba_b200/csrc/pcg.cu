@@ -114,7 +114,7 @@ template <typename T> struct SpmvDotEmit {
 
 template <typename Op, typename T>
 __global__ void __launch_bounds__(kBlock) cg_spmv_kernel(Op op, CgVecs<T> v, double *part, CgScalars *sc) {
-  if (*(volatile int *)&sc->state != B200LA_ITERATE) return;
+  if (__ldg(&sc->state) != B200LA_ITERATE) return;
   SpmvDotEmit<T> e{v.Ap, v.p};
   op.run(v.p, e);
   double s[1] = {e.acc.value()};
@@ -129,7 +129,7 @@ __global__ void __launch_bounds__(kBlock) cg_spmv_kernel(Op op, CgVecs<T> v, dou
 // ---- K2: x += alpha p, r -= alpha Ap, sums r.r and r.z ----------------------------
 template <typename T, bool PRE>
 __global__ void __launch_bounds__(kBlock) cg_update_kernel(CgVecs<T> v, double *part, CgScalars *sc) {
-  if (*(volatile int *)&sc->state != B200LA_ITERATE) return;
+  if (__ldg(&sc->state) != B200LA_ITERATE) return;
   using V = typename Vec16<T>::type;
   constexpr int W = Vec16<T>::n;
   const T alpha = (T)sc->alpha;
@@ -184,7 +184,7 @@ __global__ void __launch_bounds__(kBlock) cg_update_kernel(CgVecs<T> v, double *
 template <typename T, bool PRE, bool IN_GRAPH = true>
 __global__ void __launch_bounds__(kBlock) cg_direction_kernel(CgVecs<T> v, CgScalars *sc,
                                                               cudaGraphConditionalHandle loop) {
-  const int state = *(volatile int *)&sc->state;
+  const int state = __ldg(&sc->state);
   if (IN_GRAPH && blockIdx.x == 0 && threadIdx.x == 0) {
     int g = sc->guard + 1;
     sc->guard = g;
