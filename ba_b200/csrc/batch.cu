@@ -29,9 +29,9 @@
 //   RESID   K1: r64 = b - A64 x (FP64), ||r64||, outer test; restart the inner
 //               solve from c = 0 with r = (T)r64, z = invD r, p = z -> START
 //   START   K3: opens the inner solve (-> INNER) once every item saw START
-//   INNER   K1: Ap = A p, p.Ap   K2: c += a p, r -= a Ap, r.r, r.z, inner test
-//               (-> CORRECT)     K3: p = b p + z
-//   CORRECT K3: x += (double)c -> RESID (mixed) or DONE (FP64 mode)
+//   INNER   K1: Ap = A p, p.Ap   K2: r -= a Ap, r.r, r.z, inner test
+//               (-> CORRECT)     K3: c += a p, then p = b p + z
+//   CORRECT K3: x += (double)(c + a p) -> RESID (mixed) or DONE (FP64 mode)
 //   DONE    skipped by every kernel
 // One pass of the device loop is K1 K2 K3; the last block of K3 ends the
 // pass and clears the graph's WHILE condition when no system is running or
@@ -402,8 +402,12 @@ __global__ void __launch_bounds__(kBlock, 4) batch_spmv_kernel(const Tile *__res
       if (!(v[0] != 0.0) || !isfinite(alpha)) {
         // breakdown: mixed mode keeps the correction so far and refines;
         // FP64 mode ends the system with an error state
-        if (prm.mixed) S.phase = PH_CORRECT;
-        else finish_system(S, g, B200LA_FAIL_BREAKDOWN);
+        if (prm.mixed) {
+          S.alpha = 0.0;  // no step this pass: K3 folds c into x as it stands
+          S.phase = PH_CORRECT;
+        } else {
+          finish_system(S, g, B200LA_FAIL_BREAKDOWN);
+        }
       }
     }
   });
@@ -412,7 +416,7 @@ __global__ void __launch_bounds__(kBlock, 4) batch_spmv_kernel(const Tile *__res
 
 // ---- K2: c += alpha p, r -= alpha Ap, r.r and r.z; inner test ---------------
 template <typename T, bool PRE>
-__global__ void __launch_bounds__(kBlock, 4) batch_update_kernel(const Tile *__restrict__ tiles,
+__global__ void __launch_bounds__(kBlock, 5) batch_update_kernel(const Tile *__restrict__ tiles,
                                                                  const SysDesc<T> *__restrict__ desc, SysState *st,
                                                                  double *part, int64_t part_stride, BatchGlobals *g,
                                                                  BatchParams prm) {
@@ -430,32 +434,27 @@ __global__ void __launch_bounds__(kBlock, 4) batch_update_kernel(const Tile *__r
     using V = typename Vec16<T>::type;
     constexpr int W = Vec16<T>::n;
     const int nv = ig.rows / W;
+    // (the correction c += alpha p of this step is applied by K3, which
+    // reads p anyway)
     for (int q = lane; q < nv; q += 32) {
       const int i = tl.row0 + q * W;
-      V cv = *reinterpret_cast<const V *>(d.c + i);
       V rv = *reinterpret_cast<const V *>(d.r + i);
-      const V pv = *reinterpret_cast<const V *>(d.p + i);
       const V av = *reinterpret_cast<const V *>(d.Ap + i);
       V dv;
       if (PRE) dv = *reinterpret_cast<const V *>(d.invd + i);
-      T *cs = reinterpret_cast<T *>(&cv);
       T *rs = reinterpret_cast<T *>(&rv);
-      const T *ps = reinterpret_cast<const T *>(&pv);
       const T *as = reinterpret_cast<const T *>(&av);
       const T *ds = reinterpret_cast<const T *>(&dv);
 #pragma unroll
       for (int k = 0; k < W; ++k) {
-        cs[k] = fma(alpha, ps[k], cs[k]);
         rs[k] = fma(-alpha, as[k], rs[k]);
         rr.add(rs[k] * rs[k]);
         if (PRE) rz.add(rs[k] * (rs[k] * ds[k]));
       }
-      *reinterpret_cast<V *>(d.c + i) = cv;
       *reinterpret_cast<V *>(d.r + i) = rv;
     }
     const int end = tl.row0 + ig.rows;
     for (int i = tl.row0 + nv * W + lane; i < end; i += 32) {
-      d.c[i] = fma(alpha, d.p[i], d.c[i]);
       const T r = fma(-alpha, d.Ap[i], d.r[i]);
       d.r[i] = r;
       rr.add(r * r);
@@ -509,37 +508,41 @@ __global__ void __launch_bounds__(kBlock, 5) batch_direction_kernel(const Tile *
     const ItemGeo ig = item_geo(tl, t, d.n, tr);
     const int end = tl.row0 + ig.rows;
     if (ph == PH_INNER) {
+      // this step's correction c += alpha p (with p before its update), then
+      // the new direction p = z + beta p
+      const T alpha = (T)S.alpha;
       const T beta = (T)S.beta;
       using V = typename Vec16<T>::type;
       constexpr int W = Vec16<T>::n;
       const int nv = ig.rows / W;
-      // two vectors per lane per step: six loads in flight before a store
-      for (int q = lane; q < nv; q += 64) {
-        const bool two = q + 32 < nv;
-        V pv[2], rv[2], dv[2];
+      for (int q = lane; q < nv; q += 32) {
+        const int i = tl.row0 + q * W;
+        V pv = *reinterpret_cast<const V *>(d.p + i);
+        V cv = *reinterpret_cast<const V *>(d.c + i);
+        const V rv = *reinterpret_cast<const V *>(d.r + i);
+        V dv;
+        if (PRE) dv = *reinterpret_cast<const V *>(d.invd + i);
+        T *ps = reinterpret_cast<T *>(&pv);
+        T *cs = reinterpret_cast<T *>(&cv);
+        const T *rs = reinterpret_cast<const T *>(&rv);
+        const T *ds = reinterpret_cast<const T *>(&dv);
 #pragma unroll
-        for (int u = 0; u < 2; ++u) {
-          if (u == 1 && !two) break;
-          const int i = tl.row0 + (q + 32 * u) * W;
-          pv[u] = *reinterpret_cast<const V *>(d.p + i);
-          rv[u] = *reinterpret_cast<const V *>(d.r + i);
-          if (PRE) dv[u] = *reinterpret_cast<const V *>(d.invd + i);
+        for (int k = 0; k < W; ++k) {
+          cs[k] = fma(alpha, ps[k], cs[k]);
+          ps[k] = fma(beta, ps[k], PRE ? rs[k] * ds[k] : rs[k]);
         }
-#pragma unroll
-        for (int u = 0; u < 2; ++u) {
-          if (u == 1 && !two) break;
-          T *ps = reinterpret_cast<T *>(&pv[u]);
-          const T *rs = reinterpret_cast<const T *>(&rv[u]);
-          const T *ds = reinterpret_cast<const T *>(&dv[u]);
-#pragma unroll
-          for (int k = 0; k < W; ++k) ps[k] = fma(beta, ps[k], PRE ? rs[k] * ds[k] : rs[k]);
-          *reinterpret_cast<V *>(d.p + tl.row0 + (q + 32 * u) * W) = pv[u];
-        }
+        *reinterpret_cast<V *>(d.c + i) = cv;
+        *reinterpret_cast<V *>(d.p + i) = pv;
       }
-      for (int i = tl.row0 + nv * W + lane; i < end; i += 32)
-        d.p[i] = fma(beta, d.p[i], PRE ? d.r[i] * d.invd[i] : d.r[i]);
+      for (int i = tl.row0 + nv * W + lane; i < end; i += 32) {
+        const T pi = d.p[i];
+        d.c[i] = fma(alpha, pi, d.c[i]);
+        d.p[i] = fma(beta, pi, PRE ? d.r[i] * d.invd[i] : d.r[i]);
+      }
     } else if (ph == PH_CORRECT) {
-      for (int i = tl.row0 + lane; i < end; i += 32) d.x[i] += (double)d.c[i];
+      // the last step's correction, then x += c (alpha is 0 after a breakdown)
+      const T alpha = (T)S.alpha;
+      for (int i = tl.row0 + lane; i < end; i += 32) d.x[i] += (double)fma(alpha, d.p[i], d.c[i]);
       // the phase moves on only after every item of the system saw CORRECT
       if (warp_last(ig.count, &S.ticket[2]) && lane == 0) {
         if (prm.mixed) S.phase = PH_RESID;
@@ -1781,7 +1784,7 @@ int b200la_batch_profile_pass(b200la_batch B, int reps, double *ms, int64_t *alg
       nnz += h.nnz;
     }
   const int64_t tb = B->kp.mixed ? 4 : 8;
-  const int64_t vecs_k2 = B->kp.precond ? 7 : 6, vecs_k3 = B->kp.precond ? 4 : 3;
+  const int64_t vecs_k2 = B->kp.precond ? 4 : 3, vecs_k3 = B->kp.precond ? 6 : 5;
   if (algorithmic_bytes) {
     algorithmic_bytes[0] = nnz * (tb + 4) + (n + count) * 4 + 2 * n * tb;
     algorithmic_bytes[1] = vecs_k2 * n * tb;

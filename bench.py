@@ -171,14 +171,14 @@ def ref_batch_sample(systems, k: int, sample: int, nthreads: int):
 def batch_solver_bytes(systems, results) -> int:
     """Algorithmic HBM bytes of the whole mixed-precision batch solve: per
     FP32 inner iteration 8*nnz + 4(n+1) (SpMV: values, indices, row pointer)
-    + 8n (p gathered once, Ap written) + 28n (update: read c,p,r,Ap,invD,
-    write c,r) + 16n (direction: read p,r,invD, write p); per refinement pass
-    12*nnz + 4(n+1) + 16n (FP64 residual SpMV: x once, b) + 16n (write r,c,p,
-    read invD) + 20n (x += c)."""
+    + 8n (p gathered once, Ap written) + 16n (update: read r,Ap,invD, write r)
+    + 24n (correction and direction: read p,c,r,invD, write c,p); per
+    refinement pass 12*nnz + 4(n+1) + 16n (FP64 residual SpMV: x once, b) +
+    16n (write r,c,p, read invD) + 20n (x += c)."""
     total = 0
     for s, r in zip(systems, results):
         n, nnz = s.n, s.nnz
-        total += r.iters * (8 * nnz + 4 * (n + 1) + 52 * n)
+        total += r.iters * (8 * nnz + 4 * (n + 1) + 48 * n)
         total += (r.outer + 1) * (12 * nnz + 4 * (n + 1) + 52 * n)
     return int(total)
 

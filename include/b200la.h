@@ -346,11 +346,11 @@ int b200la_batch_tune(b200la_batch b, int *rows /* [3] */, double *usec);
 int b200la_batch_profile(b200la_batch b, int reps, double *ms_spmv, int64_t *algorithmic_bytes);
 /* Instrumentation of the solver's own kernels: restarts every system from
  * x = 0, takes one pass, then times `reps` (1..16) inner passes kernel by
- * kernel with CUDA events -- ms[0] K1 (SpMV + p.Ap), ms[1] K2 (c, r update
- * + r.r, r.z), ms[2] K3 (direction update) -- and restarts again.  bytes[k]
- * are each kernel's algorithmic bytes per launch over every slot:
- * K1 nnz*(value+4) + (n+1)*4 + 2*n*value; K2 7*n*value (Jacobi) or 6;
- * K3 4*n*value (Jacobi) or 3. */
+ * kernel with CUDA events -- ms[0] K1 (SpMV + p.Ap), ms[1] K2 (r update +
+ * r.r, r.z), ms[2] K3 (correction c += alpha p and direction update) -- and
+ * restarts again.  bytes[k] are each kernel's algorithmic bytes per launch
+ * over every slot: K1 nnz*(value+4) + (n+1)*4 + 2*n*value; K2 4*n*value
+ * (Jacobi) or 3; K3 6*n*value (Jacobi) or 5. */
 int b200la_batch_profile_pass(b200la_batch b, int reps, double *ms, int64_t *bytes);
 
 /* ---- request loop (no reference counterpart) ------------------------------
