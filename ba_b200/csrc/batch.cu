@@ -436,22 +436,32 @@ __global__ void __launch_bounds__(kBlock, 5) batch_update_kernel(const Tile *__r
     const int nv = ig.rows / W;
     // (the correction c += alpha p of this step is applied by K3, which
     // reads p anyway)
-    for (int q = lane; q < nv; q += 32) {
-      const int i = tl.row0 + q * W;
-      V rv = *reinterpret_cast<const V *>(d.r + i);
-      const V av = *reinterpret_cast<const V *>(d.Ap + i);
-      V dv;
-      if (PRE) dv = *reinterpret_cast<const V *>(d.invd + i);
-      T *rs = reinterpret_cast<T *>(&rv);
-      const T *as = reinterpret_cast<const T *>(&av);
-      const T *ds = reinterpret_cast<const T *>(&dv);
+    // two vectors per lane per step: their six loads are in flight together
+    for (int q = lane; q < nv; q += 64) {
+      const bool two = q + 32 < nv;
+      V rv[2], av[2], dv[2];
 #pragma unroll
-      for (int k = 0; k < W; ++k) {
-        rs[k] = fma(-alpha, as[k], rs[k]);
-        rr.add(rs[k] * rs[k]);
-        if (PRE) rz.add(rs[k] * (rs[k] * ds[k]));
+      for (int u = 0; u < 2; ++u) {
+        if (u == 1 && !two) break;
+        const int i = tl.row0 + (q + 32 * u) * W;
+        rv[u] = *reinterpret_cast<const V *>(d.r + i);
+        av[u] = *reinterpret_cast<const V *>(d.Ap + i);
+        if (PRE) dv[u] = *reinterpret_cast<const V *>(d.invd + i);
       }
-      *reinterpret_cast<V *>(d.r + i) = rv;
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        if (u == 1 && !two) break;
+        T *rs = reinterpret_cast<T *>(&rv[u]);
+        const T *as = reinterpret_cast<const T *>(&av[u]);
+        const T *ds = reinterpret_cast<const T *>(&dv[u]);
+#pragma unroll
+        for (int k = 0; k < W; ++k) {
+          rs[k] = fma(-alpha, as[k], rs[k]);
+          rr.add(rs[k] * rs[k]);
+          if (PRE) rz.add(rs[k] * (rs[k] * ds[k]));
+        }
+        *reinterpret_cast<V *>(d.r + tl.row0 + (q + 32 * u) * W) = rv[u];
+      }
     }
     const int end = tl.row0 + ig.rows;
     for (int i = tl.row0 + nv * W + lane; i < end; i += 32) {
