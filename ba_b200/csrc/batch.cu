@@ -56,6 +56,7 @@ template <typename T> struct SysDesc {
   const double *val64;
   int ell;            // sliced ELL width (longest row)
   int col16;          // 1: sliced ELL columns stored as int16 offsets from the row
+  int max_off;        // largest |column - row| of the stored entries
   const void *scol;   // sliced ELL columns: int32, or int16 (column - row) when col16
   const T *sval;      // sliced ELL values in the inner type
   const double *sval64;  // sliced ELL values in FP64 (== sval in FP64 mode)
@@ -307,8 +308,15 @@ __device__ __forceinline__ void resid_item(const Tile &tl, int t, const ItemGeo 
 // exactly E stored entries (E a compile-time width): software-pipelined, so
 // the next slice's values and columns stream in while the current slice's
 // gathers of p are in flight.  Same products, same order as sell_row.
-template <typename T, typename I, int E>
-__device__ __forceinline__ double spmv_item_fixed(int row0, int rows, const SysDesc<T> &d, int lane) {
+//
+// STAGE (banded systems): the warp first copies the window of p its rows can
+// reach -- rows row0 - max_off .. row0 + rows + max_off, at most kWin values
+// -- into its slice of shared memory with coalesced loads, so the gathers of
+// every slice read shared memory instead of waiting on L1/L2.
+constexpr int kWin = 1280;  // values of p per warp window (FP32: 5 KB)
+
+template <typename T, typename I, int E, bool STAGE>
+__device__ __forceinline__ double spmv_item_fixed(int row0, int rows, const SysDesc<T> &d, int lane, T *win) {
   Acc<T> acc;
   const int nsl = (rows + 31) >> 5;
   const int end = row0 + rows;
@@ -326,11 +334,21 @@ __device__ __forceinline__ double spmv_item_fixed(int row0, int rows, const SysD
       vv[k] = ld_stream(sval + base + k * 32);
     }
   }
+  int lo = 0;
+  if (STAGE) {
+    lo = max(row0 - d.max_off, 0);
+    const int hi = min(end + d.max_off, d.n);
+    for (int i = lo + lane; i < hi; i += 32) win[i - lo] = ld_keep(p + i);
+    __syncwarp();
+  }
   for (int sl = 0; sl < nsl; ++sl, ++slice) {
     const int row = slice * 32 + lane;
     T xs[E];
 #pragma unroll
-    for (int k = 0; k < E; ++k) xs[k] = ld_keep(p + (sizeof(I) == 2 ? row + (int)cv[k] : (int)cv[k]));
+    for (int k = 0; k < E; ++k) {
+      const int c = sizeof(I) == 2 ? row + (int)cv[k] : (int)cv[k];
+      xs[k] = STAGE ? win[c - lo] : ld_keep(p + c);
+    }
     T vc[E];
 #pragma unroll
     for (int k = 0; k < E; ++k) vc[k] = vv[k];
@@ -347,16 +365,20 @@ __device__ __forceinline__ double spmv_item_fixed(int row0, int rows, const SysD
     for (int k = 0; k < E; ++k) y = fma(vc[k], xs[k], y);
     if (row < end) {
       d.Ap[row] = y;
-      acc.add(y * p[row]);
+      acc.add(y * (STAGE ? win[row - lo] : p[row]));
     }
   }
+  if (STAGE) __syncwarp();  // the window is rewritten by the warp's next item
   return acc.value();
 }
 
 // Ap = A p over an item's rows and the item's share of p.Ap.
 template <typename T, typename I>
-__device__ __forceinline__ double spmv_item(int row0, int rows, const SysDesc<T> &d, int lane) {
-  if (sizeof(T) == 4 && d.ell == 9) return spmv_item_fixed<T, I, 9>(row0, rows, d, lane);
+__device__ __forceinline__ double spmv_item(int row0, int rows, const SysDesc<T> &d, int lane, T *win) {
+  if (sizeof(T) == 4 && d.ell == 9) {
+    if (win && rows + 2 * d.max_off <= kWin) return spmv_item_fixed<T, I, 9, true>(row0, rows, d, lane, win);
+    return spmv_item_fixed<T, I, 9, false>(row0, rows, d, lane, nullptr);
+  }
   Acc<T> acc;
   const int nsl = (rows + 31) >> 5;
   const int end = row0 + rows;
@@ -380,6 +402,10 @@ __global__ void __launch_bounds__(kBlock, 4) batch_spmv_kernel(const Tile *__res
                                                                double *part, int64_t part_stride, BatchGlobals *g,
                                                                BatchParams prm) {
   const int lane = threadIdx.x & 31;
+  // per-warp window of p for banded FP32 systems (see spmv_item_fixed)
+  constexpr int kWinT = sizeof(T) == 4 ? kWin : 1;
+  __shared__ T win_all[kBlock / 32][kWinT];
+  T *win = sizeof(T) == 4 ? win_all[threadIdx.x >> 5] : nullptr;
   const int tr = g->tile_rows[0];
   for_each_item(tiles, g->ntiles[0], [&](const Tile &tl, int t) {
     SysState &S = st[tl.sys];
@@ -392,8 +418,8 @@ __global__ void __launch_bounds__(kBlock, 4) batch_spmv_kernel(const Tile *__res
       return;
     }
     // one column type per item, so each slice loop is a straight stream
-    const double pap = d.col16 ? spmv_item<T, short>(tl.row0, ig.rows, d, lane)
-                               : spmv_item<T, int>(tl.row0, ig.rows, d, lane);
+    const double pap = d.col16 ? spmv_item<T, short>(tl.row0, ig.rows, d, lane, win)
+                               : spmv_item<T, int>(tl.row0, ig.rows, d, lane, win);
     double v[1] = {pap};
     if (warp_sum_last<1>(v, part, part_stride, t, ig.first, ig.count, &S.ticket[0]) && lane == 0) {
       S.pAp = v[0];
@@ -944,6 +970,7 @@ int finish_stage(BatchHandle B, int slot, const CsrCheck &c, SysDesc<T> &d) {
   }
   const bool col16 = B->prm.index_bits != 32 && c.max_off <= 32767;
   B_TRY(alloc_sell_part<T>(B, slot, std::max(c.max_row, 1), col16, d));
+  d.max_off = c.max_off;
   return finish_slot<T>(B, slot, d);
 }
 
@@ -963,13 +990,13 @@ int ensure_checks(BatchHandle B, int count) {
   return B200LA_OK;
 }
 
-// Q1 rows couple nodes at most one cell away: offset (m + 1) + 1 in 2D,
-// m^2 + m + 1 in 3D, with m = cells + 1 nodes per axis.
-bool q1_col16(int dim, int cells) {
+// Q1 rows couple nodes at most one cell away: largest |column - row| is
+// m + 1 in 2D and m^2 + m + 1 in 3D, with m = cells + 1 nodes per axis.
+int64_t q1_max_off(int dim, int cells) {
   const int64_t m = (int64_t)cells + 1;
-  const int64_t d = dim == 2 ? m + 1 : m * m + m + 1;
-  return d <= 32767;
+  return dim == 2 ? m + 1 : m * m + m + 1;
 }
+bool q1_col16(int dim, int cells) { return q1_max_off(dim, cells) <= 32767; }
 
 int kernel_grid(b200la_ctx c, const void *k, int *grid) {
   int o = 0;
@@ -1512,6 +1539,7 @@ int b200la_batch_add_q1(b200la_batch B, int dim, int cells, uint64_t seed, doubl
     SysDesc<T> d{};
     B_TRY(alloc_csr_part<T>(B, slot, n, nnz, &d));
     B_TRY(alloc_sell_part<T>(B, slot, ell, B->prm.index_bits != 32 && q1_col16(dim, cells), d));
+    d.max_off = (int)std::min<int64_t>(q1_max_off(dim, cells), INT32_MAX);
     B_TRY(q1_assemble(st, B->ctx->num_sms, dim, cells, seed, sigma, (int *)d.rowptr, (int *)d.col,
                       (double *)d.val64, (double *)d.b));
     B_CUDA(cudaMemsetAsync(d.x, 0, 8 * (size_t)n, st));
