@@ -80,6 +80,11 @@ struct SysState {
   int state;                   // B200LA_* iterate state at the end
   unsigned bad_row;            // first row without a usable diagonal (Jacobi), else ~0u
   unsigned ticket[4];
+  double rzb[2];               // r.z of the current inner iteration, by pass parity
+  double alphab[2];            // this pass's step (K2 writes, K3 reads), by pass parity
+  int okb[2];                  // 0: this pass's step broke down
+  int itb[2];                  // inner iterations done, by pass parity
+  int totb[2];                 // inner iterations over all passes, by pass parity
 };
 
 struct BatchParams {
@@ -98,7 +103,7 @@ struct BatchGlobals {
   unsigned ticket;     // last block of K3
   int ntiles[3];       // items in the K1, K2 and K3 lists
   int tile_rows[3];    // rows per item of each list
-  int pad2;
+  unsigned pass_total; // passes since the batch was created (parity of the buffered scalars)
   unsigned long long t_start;
 };
 
@@ -252,14 +257,67 @@ __device__ __forceinline__ void for_each_item_static(const Tile *__restrict__ ti
 
 namespace b200la {
 
+// ---- deferred per-system reductions -----------------------------------------
+// K1 and K2 only store each item's partial sums.  The next kernel's items
+// re-add their system's partials -- every item the same values in the same
+// fixed order (lane-strided, then a shuffle tree), so all get the same bits --
+// and each makes the system's decision itself: K2 derives alpha from K1's
+// partials (its first item passes alpha on to K3), K3 the residual, rz and
+// the inner test from K2's.  Scalars
+// that K3 both reads and updates are double-buffered by pass parity: kernels
+// of pass P read slot P & 1; the one writer of each system (its first item)
+// writes slot (P + 1) & 1.  Phase changes still wait for every item of the
+// system (last-arriver ticket), because other items read the phase.
+
+// Lists of the three pass kernels as one kernel argument.
+struct PassLists {
+  const Tile *tiles[3];
+  double *part[3];           // [3][stride] partial sums per item
+  int64_t stride[3];
+  const int *sysfirst;       // [capacity][3]: each system's first item in each list
+};
+
+// Items of a system in list k: its first item and how many there are.
+__device__ __forceinline__ void sys_items(const PassLists &L, int k, int sys, int n, int tile_rows, int *first,
+                                          int *count) {
+  *first = __ldg(L.sysfirst + 3 * sys + k);
+  *count = (n + tile_rows - 1) / tile_rows;
+}
+
+// Sum of partial slot `slot` over a system's items in list k (all lanes).
+__device__ __forceinline__ double sum_partials(const PassLists &L, int k, int slot, int first, int count) {
+  const int lane = threadIdx.x & 31;
+  const double *p = L.part[k] + slot * L.stride[k] + first;
+  double a = 0.0;
+  for (int i = lane; i < count; i += 32) a += __ldg(p + i);
+  return warp_sum(a);
+}
+
+// The step size of the current inner iteration from K1's partials, as K2
+// and K3 both compute it.  False on breakdown (p.Ap == 0 or alpha not finite).
+__device__ __forceinline__ bool step_alpha(const PassLists &L, const BatchGlobals *g, int sys, int n, double rz,
+                                           double *alpha) {
+  int f, c;
+  sys_items(L, 0, sys, n, g->tile_rows[0], &f, &c);
+  const double pap = sum_partials(L, 0, 0, f, c);
+  const double a = rz / pap;
+  *alpha = a;
+  return pap != 0.0 && isfinite(a);
+}
+
+}  // namespace b200la
+
+namespace b200la {
+
 // ---- RESID items (run by K1): FP64 residual, outer test, inner restart ------
 // r64 = b - A64 x with the FP64 sliced-ELL values, ||r64||, then the inner
 // solve restarts from c = 0 with r = (T)r64, z = invD r, p = z.  The
-// system's last item applies the outer test: DONE, or START.
+// system's last item applies the outer test: DONE, or START.  It also seeds
+// the next pass's slot of the double-buffered scalars.
 template <typename T, bool PRE>
 __device__ __forceinline__ void resid_item(const Tile &tl, int t, const ItemGeo &ig, const SysDesc<T> &d, SysState &S,
                                            double *part, int64_t part_stride, BatchGlobals *g,
-                                           const BatchParams &prm) {
+                                           const BatchParams &prm, int q) {
   Acc<double> rr64;
   Acc<T> rrin, rzin;
   const int lane = threadIdx.x & 31;
@@ -298,7 +356,9 @@ __device__ __forceinline__ void resid_item(const Tile &tl, int t, const ItemGeo 
       S.outer += 1;
       S.inner_iter = 0;
       S.res_in = S.res_in0 = sqrt(v[1]);
-      S.rz = PRE ? v[2] : v[1];
+      S.rzb[q ^ 1] = PRE ? v[2] : v[1];
+      S.itb[q ^ 1] = 0;
+      S.totb[q ^ 1] = S.totb[q];
       S.phase = PH_START;
     }
   }
@@ -395,81 +455,70 @@ __device__ __forceinline__ double spmv_item(int row0, int rows, const SysDesc<T>
   return acc.value();
 }
 
-// ---- K1: Ap = A p and p.Ap for INNER systems; RESID systems ------------------
+// ---- K1: Ap = A p and the items' p.Ap partials (INNER); RESID systems -------
 template <typename T, bool PRE>
-__global__ void __launch_bounds__(kBlock, 4) batch_spmv_kernel(const Tile *__restrict__ tiles,
-                                                               const SysDesc<T> *__restrict__ desc, SysState *st,
-                                                               double *part, int64_t part_stride, BatchGlobals *g,
-                                                               BatchParams prm) {
+__global__ void __launch_bounds__(kBlock, 4) batch_spmv_kernel(PassLists L, const SysDesc<T> *__restrict__ desc,
+                                                               SysState *st, BatchGlobals *g, BatchParams prm) {
   const int lane = threadIdx.x & 31;
   // per-warp window of p for banded FP32 systems (see spmv_item_fixed)
   constexpr int kWinT = sizeof(T) == 4 ? kWin : 1;
   __shared__ T win_all[kBlock / 32][kWinT];
   T *win = sizeof(T) == 4 ? win_all[threadIdx.x >> 5] : nullptr;
   const int tr = g->tile_rows[0];
-  for_each_item(tiles, g->ntiles[0], [&](const Tile &tl, int t) {
+  const int q = (int)(__ldg(&g->pass_total) & 1u);
+  for_each_item(L.tiles[0], g->ntiles[0], [&](const Tile &tl, int t) {
     SysState &S = st[tl.sys];
     const int ph = load_phase(&S);
     if (ph != PH_INNER && ph != PH_RESID) return;
     const SysDesc<T> d = desc[tl.sys];
     const ItemGeo ig = item_geo(tl, t, d.n, tr);
     if (ph == PH_RESID) {
-      resid_item<T, PRE>(tl, t, ig, d, S, part, part_stride, g, prm);
+      resid_item<T, PRE>(tl, t, ig, d, S, L.part[0], L.stride[0], g, prm, q);
       return;
     }
     // one column type per item, so each slice loop is a straight stream
     const double pap = d.col16 ? spmv_item<T, short>(tl.row0, ig.rows, d, lane, win)
                                : spmv_item<T, int>(tl.row0, ig.rows, d, lane, win);
-    double v[1] = {pap};
-    if (warp_sum_last<1>(v, part, part_stride, t, ig.first, ig.count, &S.ticket[0]) && lane == 0) {
-      S.pAp = v[0];
-      const double alpha = S.rz / v[0];
-      S.alpha = alpha;
-      if (!(v[0] != 0.0) || !isfinite(alpha)) {
-        // breakdown: mixed mode keeps the correction so far and refines;
-        // FP64 mode ends the system with an error state
-        if (prm.mixed) {
-          S.alpha = 0.0;  // no step this pass: K3 folds c into x as it stands
-          S.phase = PH_CORRECT;
-        } else {
-          finish_system(S, g, B200LA_FAIL_BREAKDOWN);
-        }
-      }
-    }
+    const double s = warp_sum(pap);
+    if (lane == 0) L.part[0][t] = s;
   });
 }
 
-
-// ---- K2: c += alpha p, r -= alpha Ap, r.r and r.z; inner test ---------------
+// ---- K2: r -= alpha Ap and the items' r.r, r.z partials ----------------------
 template <typename T, bool PRE>
-__global__ void __launch_bounds__(kBlock, 5) batch_update_kernel(const Tile *__restrict__ tiles,
-                                                                 const SysDesc<T> *__restrict__ desc, SysState *st,
-                                                                 double *part, int64_t part_stride, BatchGlobals *g,
-                                                                 BatchParams prm) {
+__global__ void __launch_bounds__(kBlock, 4) batch_update_kernel(PassLists L, const SysDesc<T> *__restrict__ desc,
+                                                                 SysState *st, BatchGlobals *g, BatchParams prm) {
   const int lane = threadIdx.x & 31;
   const int tr = g->tile_rows[1];
-  for_each_item(tiles, g->ntiles[1], [&](const Tile &tl, int t) {
+  const int q = (int)(__ldg(&g->pass_total) & 1u);
+  for_each_item(L.tiles[1], g->ntiles[1], [&](const Tile &tl, int t) {
     SysState &S = st[tl.sys];
     if (load_phase(&S) != PH_INNER) return;
     const SysDesc<T> d = desc[tl.sys];
     const ItemGeo ig = item_geo(tl, t, d.n, tr);
-    const T alpha = (T)S.alpha;
+    double alpha_d;
+    const bool ok = step_alpha(L, g, tl.sys, d.n, __ldg(&S.rzb[q]), &alpha_d);
+    if (t == ig.first && lane == 0) {  // the step, for K3
+      S.alphab[q] = ok ? alpha_d : 0.0;
+      S.okb[q] = ok ? 1 : 0;
+    }
+    // breakdown: no update; K3 folds c into x as it stands
+    if (!ok) return;
+    const T alpha = (T)alpha_d;
     Acc<T> rr, rz;
     // 16-byte vectors (item starts are multiples of 32 rows and every slot
     // vector is 256-byte aligned), then the ragged tail
     using V = typename Vec16<T>::type;
     constexpr int W = Vec16<T>::n;
     const int nv = ig.rows / W;
-    // (the correction c += alpha p of this step is applied by K3, which
-    // reads p anyway)
     // two vectors per lane per step: their six loads are in flight together
-    for (int q = lane; q < nv; q += 64) {
-      const bool two = q + 32 < nv;
+    for (int qv = lane; qv < nv; qv += 64) {
+      const bool two = qv + 32 < nv;
       V rv[2], av[2], dv[2];
 #pragma unroll
       for (int u = 0; u < 2; ++u) {
         if (u == 1 && !two) break;
-        const int i = tl.row0 + (q + 32 * u) * W;
+        const int i = tl.row0 + (qv + 32 * u) * W;
         rv[u] = *reinterpret_cast<const V *>(d.r + i);
         av[u] = *reinterpret_cast<const V *>(d.Ap + i);
         if (PRE) dv[u] = *reinterpret_cast<const V *>(d.invd + i);
@@ -486,7 +535,7 @@ __global__ void __launch_bounds__(kBlock, 5) batch_update_kernel(const Tile *__r
           rr.add(rs[k] * rs[k]);
           if (PRE) rz.add(rs[k] * (rs[k] * ds[k]));
         }
-        *reinterpret_cast<V *>(d.r + tl.row0 + (q + 32 * u) * W) = rv[u];
+        *reinterpret_cast<V *>(d.r + tl.row0 + (qv + 32 * u) * W) = rv[u];
       }
     }
     const int end = tl.row0 + ig.rows;
@@ -496,63 +545,90 @@ __global__ void __launch_bounds__(kBlock, 5) batch_update_kernel(const Tile *__r
       rr.add(r * r);
       if (PRE) rz.add(r * (r * d.invd[i]));
     }
-    double v[2] = {rr.value(), rz.value()};
-    if (warp_sum_last<2>(v, part, part_stride, t, ig.first, ig.count, &S.ticket[1]) && lane == 0) {
-      const double res = sqrt(v[0]);
-      const double rz_new = PRE ? v[1] : v[0];
-      S.res_in = res;
-      S.inner_iter += 1;
-      S.total_iter += 1;
-      if (prm.mixed) {
-        // inner solve: stop at inner_rtol (strict, as IterateControl), no
-        // tighter than half the outer target (the last pass does not
-        // over-solve), or at its iteration budget
-        const double target = fmax(prm.inner_rtol * S.res_in0, 0.5 * prm.rtol * S.res0);
-        if (res < target || S.inner_iter >= prm.inner_maxits || !(res == res)) S.phase = PH_CORRECT;
-      } else {
-        // FP64 CG: IterateControl::Check on the recurrence residual (cg.h:214-225)
-        int s = B200LA_ITERATE;
-        if (res <= prm.atol) s = B200LA_SUCCESS_ABS;
-        else if (res < prm.rtol * S.res_in0) s = B200LA_SUCCESS_REL;
-        else if (res > prm.dtol * S.res_in0) s = B200LA_FAIL_DIV;
-        else if (S.inner_iter >= prm.inner_maxits) s = B200LA_FAIL_MAXITS;
-        if (s != B200LA_ITERATE) {
-          S.state = s;
-          S.res = res;
-          S.phase = PH_CORRECT;
-        }
-      }
-      S.beta = rz_new / S.rz;
-      S.rz = rz_new;
+    const double srr = warp_sum(rr.value()), srz = warp_sum(rz.value());
+    if (lane == 0) {
+      L.part[1][t] = srr;
+      L.part[1][L.stride[1] + t] = srz;
     }
   });
 }
 
-// ---- K3: p = beta p + z (INNER); x += c (CORRECT); START -> INNER; end of pass
+// ---- K3: the inner step's decision; c += alpha p, p = z + beta p, or x += c --
 template <typename T, bool PRE, bool IN_GRAPH = true>
-__global__ void __launch_bounds__(kBlock, 5) batch_direction_kernel(const Tile *__restrict__ tiles,
-                                                                    const SysDesc<T> *__restrict__ desc, SysState *st,
-                                                                    double *part, int64_t part_stride, BatchGlobals *g,
-                                                                    BatchParams prm, cudaGraphConditionalHandle loop) {
+__global__ void __launch_bounds__(kBlock, 4) batch_direction_kernel(PassLists L, const SysDesc<T> *__restrict__ desc,
+                                                                    SysState *st, BatchGlobals *g, BatchParams prm,
+                                                                    cudaGraphConditionalHandle loop) {
   const int lane = threadIdx.x & 31;
   const int tr = g->tile_rows[2];
-  for_each_item(tiles, g->ntiles[2], [&](const Tile &tl, int t) {
+  const int q = (int)(__ldg(&g->pass_total) & 1u);
+  for_each_item(L.tiles[2], g->ntiles[2], [&](const Tile &tl, int t) {
     SysState &S = st[tl.sys];
     const int ph = load_phase(&S);
-    if (ph != PH_INNER && ph != PH_CORRECT && ph != PH_START) return;
+    if (ph != PH_INNER && ph != PH_START) return;
     const SysDesc<T> d = desc[tl.sys];
     const ItemGeo ig = item_geo(tl, t, d.n, tr);
     const int end = tl.row0 + ig.rows;
-    if (ph == PH_INNER) {
+    if (ph == PH_START) {
+      // K1 wrote the restart; open the inner solve once every item of the
+      // system has passed this point
+      if (warp_last(ig.count, &S.ticket[2]) && lane == 0) S.phase = PH_INNER;
+      return;
+    }
+    // INNER: every item of the system makes the same decision from K1's and
+    // K2's partials (IterateControl for the FP64 recurrence, the inner
+    // tolerance for mixed precision)
+    const double rz_cur = __ldg(&S.rzb[q]);
+    const int it = __ldg(&S.itb[q]), tot = __ldg(&S.totb[q]);
+    double alpha_d = __ldg(&S.alphab[q]), res = 0.0, rz_new = 0.0;
+    const bool ok = __ldg(&S.okb[q]) != 0;
+    int state = B200LA_ITERATE;
+    bool done = true;
+    if (!ok) {
+      alpha_d = 0.0;  // breakdown: no step; x takes the correction so far
+      state = B200LA_FAIL_BREAKDOWN;
+    } else {
+      int f2, c2;
+      sys_items(L, 1, tl.sys, d.n, g->tile_rows[1], &f2, &c2);
+      const double rr = sum_partials(L, 1, 0, f2, c2);
+      const double rzs = sum_partials(L, 1, 1, f2, c2);
+      res = sqrt(rr);
+      rz_new = PRE ? rzs : rr;
+      const int it1 = it + 1;
+      const double res_in0 = __ldg(&S.res_in0);
+      if (prm.mixed) {
+        // inner solve: stop at inner_rtol (strict, as IterateControl), no
+        // tighter than half the outer target (the last pass does not
+        // over-solve), or at its iteration budget
+        const double target = fmax(prm.inner_rtol * res_in0, 0.5 * prm.rtol * __ldg(&S.res0));
+        done = res < target || it1 >= prm.inner_maxits || !(res == res);
+      } else {
+        // FP64 CG: IterateControl::Check on the recurrence residual (cg.h:214-225)
+        if (res <= prm.atol) state = B200LA_SUCCESS_ABS;
+        else if (res < prm.rtol * res_in0) state = B200LA_SUCCESS_REL;
+        else if (res > prm.dtol * res_in0) state = B200LA_FAIL_DIV;
+        else if (it1 >= prm.inner_maxits) state = B200LA_FAIL_MAXITS;
+        done = state != B200LA_ITERATE;
+      }
+    }
+    const T alpha = (T)alpha_d;
+    const int steps = ok ? 1 : 0;
+    if (t == ig.first && lane == 0) {
+      S.rzb[q ^ 1] = ok ? rz_new : rz_cur;
+      S.itb[q ^ 1] = it + steps;
+      S.totb[q ^ 1] = tot + steps;
+      S.inner_iter = it + steps;
+      S.total_iter = tot + steps;
+      if (ok) S.res_in = res;
+    }
+    if (!done) {
       // this step's correction c += alpha p (with p before its update), then
       // the new direction p = z + beta p
-      const T alpha = (T)S.alpha;
-      const T beta = (T)S.beta;
+      const T beta = (T)(rz_new / rz_cur);
       using V = typename Vec16<T>::type;
       constexpr int W = Vec16<T>::n;
       const int nv = ig.rows / W;
-      for (int q = lane; q < nv; q += 32) {
-        const int i = tl.row0 + q * W;
+      for (int qv = lane; qv < nv; qv += 32) {
+        const int i = tl.row0 + qv * W;
         V pv = *reinterpret_cast<const V *>(d.p + i);
         V cv = *reinterpret_cast<const V *>(d.c + i);
         const V rv = *reinterpret_cast<const V *>(d.r + i);
@@ -575,19 +651,18 @@ __global__ void __launch_bounds__(kBlock, 5) batch_direction_kernel(const Tile *
         d.c[i] = fma(alpha, pi, d.c[i]);
         d.p[i] = fma(beta, pi, PRE ? d.r[i] * d.invd[i] : d.r[i]);
       }
-    } else if (ph == PH_CORRECT) {
-      // the last step's correction, then x += c (alpha is 0 after a breakdown)
-      const T alpha = (T)S.alpha;
-      for (int i = tl.row0 + lane; i < end; i += 32) d.x[i] += (double)fma(alpha, d.p[i], d.c[i]);
-      // the phase moves on only after every item of the system saw CORRECT
-      if (warp_last(ig.count, &S.ticket[2]) && lane == 0) {
-        if (prm.mixed) S.phase = PH_RESID;
-        else finish_system(S, g, S.state);
+      return;
+    }
+    // the inner solve ends: the last step's correction, then x += c
+    for (int i = tl.row0 + lane; i < end; i += 32) d.x[i] += (double)fma(alpha, d.p[i], d.c[i]);
+    // the phase moves on only after every item of the system did its part
+    if (warp_last(ig.count, &S.ticket[2]) && lane == 0) {
+      if (prm.mixed) {
+        S.phase = PH_RESID;
+      } else {
+        if (ok) S.res = res;
+        finish_system(S, g, state);
       }
-    } else {
-      // START: K1 wrote the restart; open the inner solve once every item
-      // of the system has passed this point
-      if (warp_last(ig.count, &S.ticket[2]) && lane == 0) S.phase = PH_INNER;
     }
   });
   // the last block of the launch ends the pass and decides whether the
@@ -603,6 +678,7 @@ __global__ void __launch_bounds__(kBlock, 5) batch_direction_kernel(const Tile *
     __threadfence();
     const int passes = g->passes + 1;
     g->passes = passes;
+    g->pass_total = g->pass_total + 1;
     const int active = *(volatile int *)&g->active;
     if (IN_GRAPH) cudaGraphSetConditional(loop, (active > 0 && passes < g->max_passes) ? 1u : 0u);
   }
@@ -809,6 +885,9 @@ struct b200la_batch_s {
   std::vector<HostSys> sys;
   // item lists of K1 (SpMV, residual), K2 (update + dots), K3 (direction)
   ItemList lst[3];
+  int *sysfirst;      // device [capacity][3]: each system's first item in each list
+  std::vector<int> sysfirst_host;
+  unsigned pass_total; // passes since creation, as the device last reported it
   bool adaptive;      // shrink items when few rows are running
   int warps[3];       // resident warps of each pass kernel's grid (0 = not yet known)
   // device
@@ -1026,16 +1105,27 @@ int grid_warps(BatchHandle B) {
   return B200LA_OK;
 }
 
+// The three lists as the pass kernels' argument.
+PassLists pass_lists(BatchHandle B) {
+  PassLists L;
+  for (int k = 0; k < 3; ++k) {
+    L.tiles[k] = B->lst[k].dev;
+    L.part[k] = B->lst[k].part;
+    L.stride[k] = B->lst[k].cap;
+  }
+  L.sysfirst = B->sysfirst;
+  return L;
+}
+
 // One pass (K1 K2 K3) on stream st: captured into the graph body, or
 // launched from the host loop when graphs are off.
 template <typename T, bool PRE, bool IN_GRAPH>
 void launch_pass(BatchHandle B, const int g[3], cudaStream_t st, cudaGraphConditionalHandle h) {
   const SysDesc<T> *desc = (const SysDesc<T> *)B->desc;
-  const ItemList &a = B->lst[0], &b = B->lst[1], &c = B->lst[2];
-  batch_spmv_kernel<T, PRE><<<g[0], kBlock, 0, st>>>(a.dev, desc, B->st, a.part, a.cap, B->glob, B->kp);
-  batch_update_kernel<T, PRE><<<g[1], kBlock, 0, st>>>(b.dev, desc, B->st, b.part, b.cap, B->glob, B->kp);
-  batch_direction_kernel<T, PRE, IN_GRAPH><<<g[2], kBlock, 0, st>>>(c.dev, desc, B->st, c.part, c.cap, B->glob,
-                                                                    B->kp, h);
+  const PassLists L = pass_lists(B);
+  batch_spmv_kernel<T, PRE><<<g[0], kBlock, 0, st>>>(L, desc, B->st, B->glob, B->kp);
+  batch_update_kernel<T, PRE><<<g[1], kBlock, 0, st>>>(L, desc, B->st, B->glob, B->kp);
+  batch_direction_kernel<T, PRE, IN_GRAPH><<<g[2], kBlock, 0, st>>>(L, desc, B->st, B->glob, B->kp, h);
 }
 
 // Graph: start kernel -> WHILE(pass).
@@ -1165,8 +1255,10 @@ int upload_tiles(BatchHandle B, bool running_only, int *count, int64_t *alg_byte
         rows = std::max(32, (rows / 2) & ~31);
       }
     L.used = rows;
-    for (int s : run)
+    for (int s : run) {
+      B->sysfirst_host[3 * s + k] = (int)L.host.size();
       for (int row0 = 0; row0 < B->sys[s].n; row0 += rows) L.host.push_back(Tile{s, row0});
+    }
   }
   cudaStream_t st = B->ctx->stream;
   for (int k = 0; k < 3; ++k) {
@@ -1175,6 +1267,8 @@ int upload_tiles(BatchHandle B, bool running_only, int *count, int64_t *alg_byte
     B_TRY(ensure_items(B, k, nt));
     if (nt) B_CUDA(cudaMemcpyAsync(L.dev, L.host.data(), sizeof(Tile) * nt, cudaMemcpyHostToDevice, st));
   }
+  B_CUDA(cudaMemcpyAsync(B->sysfirst, B->sysfirst_host.data(), sizeof(int) * 3 * B->capacity,
+                         cudaMemcpyHostToDevice, st));
   // the staging vectors must outlive the copies
   B_CUDA(cudaStreamSynchronize(st));
   *count = act;
@@ -1188,6 +1282,7 @@ void set_globals(BatchHandle B, int active, int max_passes) {
   memset(&g, 0, sizeof(g));
   g.active = active;
   g.max_passes = max_passes;
+  g.pass_total = B->pass_total;
   for (int k = 0; k < 3; ++k) {
     g.ntiles[k] = (int)B->lst[k].host.size();
     g.tile_rows[k] = B->lst[k].used;
@@ -1237,7 +1332,7 @@ int time_passes_t(BatchHandle B, int reps, double ms[3]) {
   int grids[3] = {1, 1, 1};
   B_TRY((pass_grids<T, PRE, false>(B, grids)));
   const SysDesc<T> *desc = (const SysDesc<T> *)B->desc;
-  const ItemList &a = B->lst[0], &b = B->lst[1], &c = B->lst[2];
+  const PassLists L = pass_lists(B);
   batch_start_kernel<<<1, 1, 0, st>>>(B->glob);
   launch_pass<T, PRE, false>(B, grids, st, 0);
   cudaEvent_t ev[4];
@@ -1246,12 +1341,11 @@ int time_passes_t(BatchHandle B, int reps, double ms[3]) {
   int rc = B200LA_OK;
   for (int r = 0; r < reps && rc == B200LA_OK; ++r) {
     cudaEventRecord(ev[0], st);
-    batch_spmv_kernel<T, PRE><<<grids[0], kBlock, 0, st>>>(a.dev, desc, B->st, a.part, a.cap, B->glob, B->kp);
+    batch_spmv_kernel<T, PRE><<<grids[0], kBlock, 0, st>>>(L, desc, B->st, B->glob, B->kp);
     cudaEventRecord(ev[1], st);
-    batch_update_kernel<T, PRE><<<grids[1], kBlock, 0, st>>>(b.dev, desc, B->st, b.part, b.cap, B->glob, B->kp);
+    batch_update_kernel<T, PRE><<<grids[1], kBlock, 0, st>>>(L, desc, B->st, B->glob, B->kp);
     cudaEventRecord(ev[2], st);
-    batch_direction_kernel<T, PRE, false><<<grids[2], kBlock, 0, st>>>(c.dev, desc, B->st, c.part, c.cap, B->glob,
-                                                                        B->kp, 0);
+    batch_direction_kernel<T, PRE, false><<<grids[2], kBlock, 0, st>>>(L, desc, B->st, B->glob, B->kp, 0);
     cudaEventRecord(ev[3], st);
     if (cudaEventSynchronize(ev[3]) != cudaSuccess) {
       rc = fail(B200LA_ERR_CUDA, "batch pass timing: %s", cudaGetErrorString(cudaGetLastError()));
@@ -1434,7 +1528,7 @@ int b200la_batch_destroy(b200la_batch B) {
   if (B->exec) cudaGraphExecDestroy(B->exec);
   if (B->graph) cudaGraphDestroy(B->graph);
   for (HostSys &h : B->sys) free_slot_memory(B, h);
-  void *bufs[] = {B->desc, B->st, B->glob, B->chk};
+  void *bufs[] = {B->desc, B->st, B->glob, B->chk, B->sysfirst};
   for (void *p : bufs)
     if (p) cudaFreeAsync(p, st);
   for (ItemList &L : B->lst) {
@@ -1477,11 +1571,13 @@ int b200la_batch_create(b200la_ctx ctx, const b200la_batch_params *p, b200la_bat
   B->adaptive = p->adaptive != 0;
   B->capacity = p->capacity;
   B->sys.resize(p->capacity);
+  B->sysfirst_host.assign(3 * (size_t)p->capacity, 0);
   cudaStream_t st = ctx->stream;
   const size_t dsz = p->mixed ? sizeof(SysDesc<float>) : sizeof(SysDesc<double>);
   bool ok = cudaMallocAsync(&B->desc, dsz * p->capacity, st) == cudaSuccess &&
             cudaMallocAsync(&B->st, sizeof(SysState) * p->capacity, st) == cudaSuccess &&
             cudaMallocAsync(&B->glob, sizeof(BatchGlobals), st) == cudaSuccess &&
+            cudaMallocAsync(&B->sysfirst, sizeof(int) * 3 * p->capacity, st) == cudaSuccess &&
             ensure_checks(B, 64) == B200LA_OK &&
             cudaMallocHost(&B->st_host, sizeof(SysState) * p->capacity) == cudaSuccess &&
             cudaMallocHost(&B->glob_host, sizeof(BatchGlobals)) == cudaSuccess;
@@ -1614,6 +1710,7 @@ int b200la_batch_run(b200la_batch B, int max_passes, int *active_out) {
   B_CUDA(cudaMemcpyAsync(B->st_host, B->st, sizeof(SysState) * B->capacity, cudaMemcpyDeviceToHost, st));
   B_CUDA(cudaMemcpyAsync(B->glob_host, B->glob, sizeof(BatchGlobals), cudaMemcpyDeviceToHost, st));
   B_CUDA(cudaStreamSynchronize(st));
+  B->pass_total = B->glob_host->pass_total;
   if (active_out) *active_out = B->glob_host->active;
   return B200LA_OK;
 }
