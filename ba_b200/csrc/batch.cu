@@ -7,16 +7,19 @@
 // (linear_solver/mpir.cc:52-230): FP64 residual, update and test around an
 // FP32 inner solve, or, in FP64 mode, a plain FP64 (P)CG.
 //
-// Work decomposition: every system is cut into items of consecutive rows
-// (tile_rows, a multiple of 32, picked by the tuner); one warp handles one
-// item at a time (grid-stride over the item list across all warps of the
-// grid), so large and small systems share every launch, the load balances
-// at item granularity, and the warps of a block never wait on one another.
-// Per-system dot products are reduced deterministically: each item writes
-// its partial sums, and the warp of the system's last item to finish
-// (per-system atomic ticket) adds the system's partials in a fixed order.
-// A system's arithmetic therefore does not depend on what else is in the
-// batch or on the order its items ran in.
+// Work decomposition: every system is cut into items of consecutive rows (a
+// multiple of 32; each pass kernel has its own item size, picked by the
+// tuner); one warp handles one item at a time (round-robin over the item
+// list across all warps of the grid), so large and small systems share every
+// launch and the warps of a block never wait on one another.
+//
+// Per-system sums are deterministic and deferred: an item stores its partial
+// sums, and the next kernel's items each re-add their system's partials in a
+// fixed order and take the system's decision themselves (alpha in K2, the
+// residual, rz and the inner test in K3).  A system's arithmetic therefore
+// does not depend on what else is in the batch or on the order its items ran
+// in, and no item waits on a fence or an atomic ticket in K1 or K2.  Scalars
+// that one kernel both reads and updates are double-buffered by pass parity.
 //
 // Matrices are stored twice: CSR as uploaded (host-facing, setup), and a
 // sliced ELL copy used by both SpMVs: slices of 32 rows, every row padded to
@@ -24,14 +27,17 @@
 // (s*ell + k)*32 + l, so a warp reads 32 consecutive values per step and the
 // loads of one row do not depend on a row pointer.
 //
-// Each system walks through phases, advanced by the last item of the kernel
-// that ends a phase, so all items of a system see one phase per launch:
+// Each system walks through phases; a phase changes only after every item of
+// the system has passed (last-arriver ticket), so all items of a system see
+// one phase per launch:
 //   RESID   K1: r64 = b - A64 x (FP64), ||r64||, outer test; restart the inner
 //               solve from c = 0 with r = (T)r64, z = invD r, p = z -> START
 //   START   K3: opens the inner solve (-> INNER) once every item saw START
-//   INNER   K1: Ap = A p, p.Ap   K2: r -= a Ap, r.r, r.z, inner test
-//               (-> CORRECT)     K3: c += a p, then p = b p + z
-//   CORRECT K3: x += (double)(c + a p) -> RESID (mixed) or DONE (FP64 mode)
+//   INNER   K1: Ap = A p, p.Ap partials
+//           K2: alpha = rz / p.Ap; r -= alpha Ap; r.r, r.z partials
+//           K3: inner test on r.r; if it goes on, c += alpha p and
+//               p = z + beta p; if it ends, x += (double)(c + alpha p) and
+//               -> RESID (mixed) or DONE (FP64 mode)
 //   DONE    skipped by every kernel
 // One pass of the device loop is K1 K2 K3; the last block of K3 ends the
 // pass and clears the graph's WHILE condition when no system is running or
