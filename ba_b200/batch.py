@@ -164,7 +164,7 @@ class Batch:
     def slot_n(self, slot: int) -> int:
         return self._sizes[slot]
 
-    def solve(self, chunk_passes: int = 32) -> int:
+    def solve(self, chunk_passes: int = 64) -> int:
         """Run until every system has finished, compacting the tile list every
         chunk_passes passes; returns the passes taken."""
         n = C.c_int()

@@ -39,7 +39,7 @@ def main():
     ap.add_argument("--sigma", type=float, default=0.0)
     ap.add_argument("--batch", type=int, default=0,
                     help="instead: solve a batch of this many 2D systems (n~logU[16,256], sigma 1) twice")
-    ap.add_argument("--chunk", type=int, default=32)
+    ap.add_argument("--chunk", type=int, default=64)
     ap.add_argument("--tile-rows", type=int, default=0)
     ap.add_argument("--index-bits", type=int, default=0, choices=[0, 32],
                     help="batch: sliced-ELL columns (0 = int16 offsets when they fit, 32 = int32)")

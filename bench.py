@@ -47,7 +47,7 @@ METRIC = "PCG solves/s & p50/p99 latency at 1e-8 rel. residual vs plain FP64 GPU
 COUNTS = os.path.join(ROOT, "tests", "golden", "workload_counts.json")
 BATCH_COUNT = 1024
 BATCH_RTOL = 1e-8
-CHUNK = 32  # device-loop passes between tile-list compactions
+CHUNK = 64  # device-loop passes per graph launch (item lists compacted in between)
 
 
 def parse():
