@@ -18,8 +18,11 @@
 // fixed order and take the system's decision themselves (alpha in K2, the
 // residual, rz and the inner test in K3).  A system's arithmetic therefore
 // does not depend on what else is in the batch or on the order its items ran
-// in, and no item waits on a fence or an atomic ticket in K1 or K2.  Scalars
-// that one kernel both reads and updates are double-buffered by pass parity.
+// in, and no item waits on a fence or an atomic ticket in K1 or K2.  Systems
+// with more than kDirectItems items in a list (millions of rows) hand their
+// totals on through a last-arriver ticket instead, since re-adding costs
+// count^2 loads.  Scalars that one kernel both reads and updates are
+// double-buffered by pass parity.
 //
 // Matrices are stored twice: CSR as uploaded (host-facing, setup), and a
 // sliced ELL copy used by both SpMVs: slices of 32 rows, every row padded to
@@ -91,6 +94,7 @@ struct SysState {
   int okb[2];                  // 0: this pass's step broke down
   int itb[2];                  // inner iterations done, by pass parity
   int totb[2];                 // inner iterations over all passes, by pass parity
+  double tot[3];               // ticket path totals: K1 p.Ap; K2 r.r, r.z
 };
 
 struct BatchParams {
@@ -283,6 +287,13 @@ struct PassLists {
   const int *sysfirst;       // [capacity][3]: each system's first item in each list
 };
 
+// A system with more items than this in a list hands its totals on through a
+// last-arriver ticket (warp_sum_last into SysState::tot) instead: re-adding
+// every partial in every consumer item costs count^2 loads per kernel, which
+// for systems of millions of rows (thousands of items) exceeds the kernel's
+// own traffic.  Both paths add the partials in a fixed order.
+constexpr int kDirectItems = 1024;
+
 // Items of a system in list k: its first item and how many there are.
 __device__ __forceinline__ void sys_items(const PassLists &L, int k, int sys, int n, int tile_rows, int *first,
                                           int *count) {
@@ -299,13 +310,46 @@ __device__ __forceinline__ double sum_partials(const PassLists &L, int k, int sl
   return warp_sum(a);
 }
 
+// Total of partial slot `slot` of list k for a system: re-added from the
+// items' partials, or the ticket path's total.
+__device__ __forceinline__ double sys_total(const PassLists &L, const SysState &S, int k, int slot, int first,
+                                            int count) {
+  if (count <= kDirectItems) return sum_partials(L, k, slot, first, count);
+  return __ldcg(&S.tot[k == 0 ? 0 : 1 + slot]);
+}
+
+// Stores an item's partial sums v[] (one value per lane) for list k: as the
+// item's partials, or through the ticket into S.tot.  All 32 lanes call it.
+// The system's first item and item count are looked up here, after the
+// item's main loop, so they are not held in registers across it.
+template <int NV>
+__device__ __forceinline__ void put_partials(const PassLists &L, SysState *st, int k, double (&v)[NV], int item,
+                                             int sys, int n, int tile_rows) {
+  const int lane = threadIdx.x & 31;
+  const int count = (n + tile_rows - 1) / tile_rows;
+  if (count <= kDirectItems) {
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+      const double s = warp_sum(v[j]);
+      if (lane == 0) L.part[k][j * L.stride[k] + item] = s;
+    }
+    return;
+  }
+  const int first = __ldg(L.sysfirst + 3 * sys + k);
+  SysState &S = st[sys];
+  if (warp_sum_last<NV>(v, L.part[k], L.stride[k], item, first, count, &S.ticket[k]) && lane == 0) {
+#pragma unroll
+    for (int j = 0; j < NV; ++j) S.tot[k == 0 ? 0 : 1 + j] = v[j];
+  }
+}
+
 // The step size of the current inner iteration from K1's partials, as K2
-// and K3 both compute it.  False on breakdown (p.Ap == 0 or alpha not finite).
-__device__ __forceinline__ bool step_alpha(const PassLists &L, const BatchGlobals *g, int sys, int n, double rz,
-                                           double *alpha) {
+// computes it.  False on breakdown (p.Ap == 0 or alpha not finite).
+__device__ __forceinline__ bool step_alpha(const PassLists &L, const BatchGlobals *g, const SysState &S, int sys,
+                                           int n, double rz, double *alpha) {
   int f, c;
   sys_items(L, 0, sys, n, g->tile_rows[0], &f, &c);
-  const double pap = sum_partials(L, 0, 0, f, c);
+  const double pap = sys_total(L, S, 0, 0, f, c);
   const double a = rz / pap;
   *alpha = a;
   return pap != 0.0 && isfinite(a);
@@ -483,10 +527,9 @@ __global__ void __launch_bounds__(kBlock, 4) batch_spmv_kernel(PassLists L, cons
       return;
     }
     // one column type per item, so each slice loop is a straight stream
-    const double pap = d.col16 ? spmv_item<T, short>(tl.row0, ig.rows, d, lane, win)
-                               : spmv_item<T, int>(tl.row0, ig.rows, d, lane, win);
-    const double s = warp_sum(pap);
-    if (lane == 0) L.part[0][t] = s;
+    double pap[1] = {d.col16 ? spmv_item<T, short>(tl.row0, ig.rows, d, lane, win)
+                             : spmv_item<T, int>(tl.row0, ig.rows, d, lane, win)};
+    put_partials<1>(L, st, 0, pap, t, tl.sys, d.n, tr);
   });
 }
 
@@ -503,7 +546,7 @@ __global__ void __launch_bounds__(kBlock, 4) batch_update_kernel(PassLists L, co
     const SysDesc<T> d = desc[tl.sys];
     const ItemGeo ig = item_geo(tl, t, d.n, tr);
     double alpha_d;
-    const bool ok = step_alpha(L, g, tl.sys, d.n, __ldg(&S.rzb[q]), &alpha_d);
+    const bool ok = step_alpha(L, g, S, tl.sys, d.n, __ldg(&S.rzb[q]), &alpha_d);
     if (t == ig.first && lane == 0) {  // the step, for K3
       S.alphab[q] = ok ? alpha_d : 0.0;
       S.okb[q] = ok ? 1 : 0;
@@ -551,11 +594,8 @@ __global__ void __launch_bounds__(kBlock, 4) batch_update_kernel(PassLists L, co
       rr.add(r * r);
       if (PRE) rz.add(r * (r * d.invd[i]));
     }
-    const double srr = warp_sum(rr.value()), srz = warp_sum(rz.value());
-    if (lane == 0) {
-      L.part[1][t] = srr;
-      L.part[1][L.stride[1] + t] = srz;
-    }
+    double sums[2] = {rr.value(), rz.value()};
+    put_partials<2>(L, st, 1, sums, t, tl.sys, d.n, tr);
   });
 }
 
@@ -595,8 +635,8 @@ __global__ void __launch_bounds__(kBlock, 4) batch_direction_kernel(PassLists L,
     } else {
       int f2, c2;
       sys_items(L, 1, tl.sys, d.n, g->tile_rows[1], &f2, &c2);
-      const double rr = sum_partials(L, 1, 0, f2, c2);
-      const double rzs = sum_partials(L, 1, 1, f2, c2);
+      const double rr = sys_total(L, S, 1, 0, f2, c2);
+      const double rzs = sys_total(L, S, 1, 1, f2, c2);
       res = sqrt(rr);
       rz_new = PRE ? rzs : rr;
       const int it1 = it + 1;
@@ -1858,9 +1898,11 @@ int b200la_batch_tune(b200la_batch B, int *rows, double *usec) {
   // p and its scalars) is restored after each trial.  Each kernel keeps the
   // smallest item within 3% of its best time: mid-solve passes, where
   // finished systems and residual passes mix in, favour short items.
-  // K1 is held to 128..256 rows: fresh passes (what a trial times) favour
-  // larger K1 items, but whole solves, where residual items (FP64, about
-  // twice the work) and finished systems mix in, were measured faster at 256
+  // K1 is held to 128..256 rows and keeps 128 unless 256 is more than 8%
+  // faster: fresh passes (what a trial times) favour larger K1 items by up
+  // to ~2.5%, but whole solves, where residual items (FP64, about twice the
+  // work) and finished systems mix in, ran 204 ms at 128 rows against 220 ms
+  // at 256 (1,024-system batch).
   static const int cand[4][3] = {{128, 256, 256}, {256, 512, 512}, {256, 1024, 1024}, {256, 2048, 2048}};
   int active = 0;
   B_TRY(upload_tiles(B, true, &active, nullptr));
@@ -1887,8 +1929,9 @@ int b200la_batch_tune(b200la_batch B, int *rows, double *usec) {
           int best = 0;
           for (int c = 1; c < 4; ++c)
             if (t[c][k] < t[best][k]) best = c;
+          const double slack = k == 0 ? 1.08 : 1.03;
           for (int c = 0; c < best; ++c)
-            if (t[c][k] <= 1.03 * t[best][k]) {
+            if (t[c][k] <= slack * t[best][k]) {
               best = c;
               break;
             }

@@ -221,3 +221,31 @@ def test_add_many_matches_single_adds_and_reports_per_system_status(plat):
         ra = A.results([a_slot])[0]
         assert rm.solver_state == lmp.kSolverSuccess
         np.testing.assert_array_equal(ra.x, rm.x)
+
+
+def test_large_system_ticket_path_isolated_and_converged(plat):
+    # 128-row items: the 3D system has 2,350 items in K1 and K2 (more than
+    # kDirectItems = 1,024), so its p.Ap and r.r/r.z totals go through the
+    # last-arriver ticket, while the small systems re-add their partials.
+    big = P.q1_system(3, 66, 77, 1.0, "big3d_66")
+    small = [P.q1_system(2, c, 500 + c, 1.0, f"s{c}") for c in (9, 30, 64)]
+    kw = dict(mixed=True, precond=True, rtol=1e-8, inner_rtol=1e-4, platform=plat)
+    A = Batch(1, **kw)
+    A.set_items(128, 128, 256, adaptive=False)
+    a = A.add_system(big)
+    A.run()
+    alone = A.result(a)
+    M = Batch(8, **kw)
+    M.set_items(128, 128, 256, adaptive=False)
+    slots = [M.add_system(s) for s in small[:2]] + [M.add_system(big)] + [M.add_system(small[2])]
+    M.run()
+    mixed = M.result(slots[2])
+    assert alone.solver_state == lmp.kSolverSuccess
+    assert mixed.iters == alone.iters and mixed.outer == alone.outer
+    np.testing.assert_array_equal(mixed.x, alone.x)
+    res = np.linalg.norm(big.b - oracle.spmv(big.rowptr, big.col, big.val, alone.x))
+    assert res <= 1.001e-8 * np.linalg.norm(big.b)
+    for s, sl in zip(small[:2] + small[2:], slots[:2] + slots[3:]):
+        r = M.result(sl)
+        assert r.solver_state == lmp.kSolverSuccess
+        assert np.linalg.norm(s.b - oracle.spmv(s.rowptr, s.col, s.val, r.x)) <= 1.001e-8 * np.linalg.norm(s.b)
