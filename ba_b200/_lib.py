@@ -15,7 +15,8 @@ LIB_PATH = os.path.join(_HERE, "libb200la.so")
 F64, F32 = 0, 1
 FMT_CSR, FMT_SELL, FMT_SELL16 = 1, 4, 5
 FORMAT_NAMES = {FMT_CSR: "csr", FMT_SELL: "sell", FMT_SELL16: "sell16"}
-ITERATE, SUCCESS_ABS, SUCCESS_REL, FAIL_DIV, FAIL_MAXITS, FAIL_BREAKDOWN = range(6)
+ITERATE, SUCCESS_ABS, SUCCESS_REL, FAIL_DIV, FAIL_MAXITS, FAIL_BREAKDOWN, DONE_FIXED = range(7)
+METHOD_JACOBI, METHOD_BICGSTAB = 1, 2
 SOLVER_SUCCESS, SOLVER_EXCEEDED, SOLVER_ERROR = range(3)
 STATUS_NAMES = {0: "OK", -1: "ERR_INVALID", -2: "ERR_CUDA", -3: "ERR_NOMEM", -4: "ERR_DTYPE",
                 -5: "ERR_MATRIX", -6: "ERR_TIMEOUT", -7: "ERR_UNSUPPORTED"}
@@ -73,6 +74,18 @@ class CgResult(C.Structure):
                 ("res_rel", C.c_double)]
 
 
+class SolverParams(C.Structure):
+    _fields_ = [("method", C.c_int), ("maxits", C.c_int), ("atol", C.c_double), ("rtol", C.c_double),
+                ("dtol", C.c_double), ("precond", C.c_int), ("mode", C.c_int), ("inner_iter", C.c_int),
+                ("smooth_iter", C.c_int), ("w", C.c_double)]
+
+
+class SolverResult(C.Structure):
+    _fields_ = [("iters", C.c_int), ("state", C.c_int), ("solver_state", C.c_int),
+                ("restarts", C.c_int), ("res", C.c_double), ("res_init", C.c_double),
+                ("res_rel", C.c_double)]
+
+
 _vp = C.c_void_p
 _i = C.c_int
 _i64 = C.c_int64
@@ -123,6 +136,10 @@ _SIGS = {
     "b200la_cg_solve": [_vp, _vp, _vp, _P(CgResult)],
     "b200la_cg_profile": [_vp, _vp, _vp, _i, _P(_d)],
     "b200la_pcg_solve": [_vp, _vp, _vp, _P(CgParams), _P(CgResult)],
+    "b200la_solver_create": [_vp, _P(SolverParams), _P(_vp)],
+    "b200la_solver_destroy": [_vp],
+    "b200la_solver_solve": [_vp, _vp, _vp, _P(SolverResult)],
+    "b200la_solver_profile": [_vp, _vp, _vp, _i, _P(_d)],
     "b200la_batch_create": [_vp, _P(BatchParams), _P(_vp)],
     "b200la_batch_destroy": [_vp],
     "b200la_batch_slot_bytes": [_i64, _i64, _i, _i, _P(_i64)],

@@ -411,6 +411,190 @@ def setup_CG_solver(maxits: int = 1000, atol: float = 1e-12, rtol: float = 1e-10
     return s
 
 
+class _DeviceSolver:
+    """Common part of the solvers that run on b200la_solver (Jacobi, BiCGSTAB)."""
+
+    _name = "solver"
+
+    def __init__(self):
+        self.control = IterateControl()
+        self.op = None
+        self._s = C.c_void_p()
+        self.iter_ = 0
+        self.res_ = self.res_init_ = self.res_rel_ = 0.0
+        self.state_ = 0
+        self.restarts_ = 0
+
+    def InitControl(self, maxits: int, atol: float, rtol: float, dtol: float):
+        self.control = IterateControl(maxits, atol, rtol, dtol)
+        self._release()
+
+    def SetRelativeTolerance(self, reltol: float):
+        c = self.control
+        self.InitControl(c.maxits, c.atol, reltol, c.dtol)
+
+    def SetupOperator(self, op: B200_CSR_lMatrix):
+        self.op = op
+        self._release()
+
+    def _params(self) -> "_lib.SolverParams":
+        raise NotImplementedError
+
+    def _release(self):
+        if self._s:
+            load().b200la_solver_destroy(self._s)
+            self._s = C.c_void_p()
+
+    def _ensure(self):
+        if self._s:
+            return
+        if self.op is None:
+            raise B200LAError(-1, f"{self._name}: SetupOperator was not called")
+        prm = self._params()
+        call("b200la_solver_create", self.op.handle, C.byref(prm), C.byref(self._s))
+
+    def _solve(self, b: B200_lVector, x: B200_lVector) -> "_lib.SolverResult":
+        self._ensure()
+        r = _lib.SolverResult()
+        call("b200la_solver_solve", self._s, b.handle, x.handle, C.byref(r))
+        self.state_, self.restarts_ = r.state, r.restarts
+        self.res_, self.res_init_, self.res_rel_ = r.res, r.res_init, r.res_rel
+        return r
+
+    def profile(self, b: B200_lVector, x: B200_lVector, passes: int = 20) -> list[float]:
+        """Mean milliseconds per launch of each kernel of one pass."""
+        self._ensure()
+        ms = (C.c_double * 5)()
+        call("b200la_solver_profile", self._s, b.handle, x.handle, int(passes), ms)
+        return list(ms)
+
+    def iter(self) -> int:
+        return self.iter_
+
+    def res(self) -> float:
+        return self.res_
+
+    def res_init(self) -> float:
+        return self.res_init_
+
+    def res_rel(self) -> float:
+        return self.res_rel_
+
+    def __del__(self):
+        if sys.is_finalizing():
+            return
+        try:
+            self._release()
+        except Exception:
+            pass
+
+
+class Jacobi(_DeviceSolver):
+    """Jacobi<LAD> (linear_solver/jacobi.h:30-80, jacobi.cc): the stationary
+    Jacobi solver and smoother.  SetSolveMode(0 SolveNormal, 1 SolveDamped,
+    2 SmoothNormal, 3 SmoothDamped), SetNumIter (smoothing sweeps),
+    SetInnerIter (sweeps between residual tests), SetDampingParameter(w).
+    As in the reference, the smoothing modes add their sweeps to iter() and
+    the solve modes restart it from 0.  Prepare(op, sample) is SetupOperator;
+    the asynchronous ghost flag has no meaning on one device and is stored
+    only."""
+
+    _name = "Jacobi"
+
+    def __init__(self):
+        super().__init__()
+        self.solve_mode, self.smooth_iter, self.inner_iter, self.w, self.async_ = 0, 1, 1, 1.0, False
+
+    def Prepare(self, op: B200_CSR_lMatrix, sample: B200_lVector | None = None):
+        self.SetupOperator(op)
+
+    def SetSolveMode(self, mode: int):
+        if not 0 <= int(mode) <= 3:
+            raise B200LAError(-1, f"Jacobi: unknown solve mode {mode}")
+        self.solve_mode = int(mode)
+        self._release()
+
+    def SetNumIter(self, it: int):
+        if int(it) <= 0:
+            raise B200LAError(-1, "Jacobi: SetNumIter needs a positive count")
+        self.smooth_iter = int(it)
+        self._release()
+
+    def SetInnerIter(self, it: int):
+        if int(it) <= 0:
+            raise B200LAError(-1, "Jacobi: SetInnerIter needs a positive count")
+        self.inner_iter = int(it)
+        self._release()
+
+    def SetDampingParameter(self, w: float):
+        if not float(w) > 0.0:
+            raise B200LAError(-1, "Jacobi: the damping parameter must be positive")
+        self.w = float(w)
+        self._release()
+
+    def SetAsyncFlag(self, flag: bool):
+        self.async_ = bool(flag)
+
+    def _params(self):
+        c = self.control
+        return _lib.SolverParams(_lib.METHOD_JACOBI, c.maxits, c.atol, c.rtol, c.dtol, 1, self.solve_mode,
+                                 self.inner_iter, self.smooth_iter, self.w)
+
+    def Solve(self, b: B200_lVector, x: B200_lVector) -> int:
+        r = self._solve(b, x)
+        if self.solve_mode >= 2:
+            self.iter_ += r.iters
+        else:
+            self.iter_ = r.iters
+        return r.solver_state
+
+
+class BiCGSTAB(_DeviceSolver):
+    """BiCGSTAB<LAD> (linear_solver/bicgstab.h:37-473):
+    InitParameter("NoPreconditioning" | "RightPreconditioning" |
+    "LeftPreconditioning"), SetupPreconditioner (switches to right
+    preconditioning, linear_solver.h:97-100), Solve.  Left preconditioning
+    returns kSolverError as in the reference (bicgstab.h:485-495).  iter()
+    reports the iterations taken (the reference never stores its local
+    count in iter_); restarts() the restarts."""
+
+    _name = "BiCGSTAB"
+
+    def __init__(self):
+        super().__init__()
+        self.method = "NoPreconditioning"
+        self.precond = None
+
+    def InitParameter(self, method: str):
+        if method not in ("NoPreconditioning", "RightPreconditioning", "LeftPreconditioning"):
+            raise B200LAError(-1, f"BiCGSTAB: unknown method {method!r}")
+        self.method = method
+        self._release()
+
+    def SetupPreconditioner(self, precond: PreconditionerBlockJacobiStand):
+        self.precond = precond
+        self.method = "RightPreconditioning"
+        self._release()
+
+    def _params(self):
+        use_pc = self.method == "RightPreconditioning"
+        if use_pc and (self.precond is None or self.precond.kind != "Jacobi"):
+            raise B200LAError(-7, "BiCGSTAB: only the Jacobi preconditioner runs on this path")
+        c = self.control
+        return _lib.SolverParams(_lib.METHOD_BICGSTAB, c.maxits, c.atol, c.rtol, c.dtol, 1 if use_pc else 0,
+                                 0, 1, 1, 1.0)
+
+    def Solve(self, b: B200_lVector, x: B200_lVector) -> int:
+        if self.method == "LeftPreconditioning":
+            return kSolverError
+        r = self._solve(b, x)
+        self.iter_ = r.iters
+        return r.solver_state
+
+    def restarts(self) -> int:
+        return self.restarts_
+
+
 class MPIR:
     """MPIR<LADescriptorCoupledD, LADescriptorCoupledS> with an FP32 Jacobi-PCG
     as the low-precision error-correction solver (linear_solver/mpir.h:29-150):

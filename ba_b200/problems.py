@@ -238,6 +238,38 @@ def lmp_test_3x3() -> CSRSystem:
     return CSRSystem(0, 0, rowptr, col, val, b, np.zeros(3, dtype=bool), "lmp_test_3x3")
 
 
+def convdiff_2d(n: int, peclet: float = 20.0, seed: int = 7, name: str = "") -> CSRSystem:
+    """Non-symmetric test system for BiCGSTAB and Jacobi: -lap u + beta.grad u
+    on the n x n interior nodes of the unit square (h = 1/(n+1), Dirichlet
+    nodes eliminated), 5-point diffusion and first-order upwind convection,
+    scaled by h^2, beta = peclet (cos 0.3, sin 0.3).  The matrix is an
+    M-matrix (diagonally dominant, strictly in rows next to the boundary);
+    columns ascend within each row; b ~ U[0,1) from the seed's stream 0."""
+    h = 1.0 / (n + 1)
+    bx, by = peclet * np.cos(0.3), peclet * np.sin(0.3)
+    ix, iy = np.meshgrid(np.arange(n), np.arange(n), indexing="xy")
+    ix, iy = ix.ravel(), iy.ravel()
+    N = n * n
+    rows = np.arange(N)
+    # (offset, coefficient, neighbour exists) in ascending column order
+    nb = [(-n, -1.0 - h * max(by, 0.0), iy > 0), (-1, -1.0 - h * max(bx, 0.0), ix > 0),
+          (0, 4.0 + h * (abs(bx) + abs(by)), np.ones(N, bool)),
+          (1, -1.0 + h * min(bx, 0.0), ix < n - 1), (n, -1.0 + h * min(by, 0.0), iy < n - 1)]
+    cnt = sum(m.astype(np.int32) for _, _, m in nb)
+    rowptr = np.zeros(N + 1, dtype=np.int32)
+    np.cumsum(cnt, out=rowptr[1:])
+    col = np.empty(rowptr[-1], dtype=np.int32)
+    val = np.empty(rowptr[-1], dtype=np.float64)
+    pos = rowptr[:-1].copy()
+    for off, c, m in nb:
+        r = rows[m]
+        col[pos[m]] = r + off
+        val[pos[m]] = c
+        pos[m] += 1
+    b = uniform01(seed, N, stream=0)
+    return CSRSystem(2, n, rowptr, col, val, b, np.zeros(N, dtype=bool), name or f"convdiff2d_{n}_pe{peclet:g}")
+
+
 def random_spd(n: int, seed: int, density: float = 0.1, empty_rows: int = 0) -> CSRSystem:
     """Small random symmetric diagonally dominant matrix (ragged rows) for
     edge-case parity: the first `empty_rows` rows hold only their diagonal."""

@@ -4,6 +4,12 @@ launches (no CUDA graph), so a profiler sees every launch on its own.
     python -m ba_b200.profile_case [--cells 128] [--dim 3] [--dtype f64|f32]
                                    [--spmv-reps 3] [--cg-iters 3] [--schedule tune|csr/8|sell/1]
 
+With --solver jacobi|bicgstab: after the SpMV launches, runs `--cg-iters`
+passes of that solver's kernels as plain launches (b200la_solver_profile:
+one jacobi_sweep_kernel per pass; bicg_spmv_q, bicg_s, bicg_spmv_s,
+bicg_update, bicg_direction per pass, the first pass a restart) instead of
+the CG kernels.
+
 With --batch N: builds the standard batch of N 2D systems and solves it
 twice (the launches of interest are those of the second solve; set
 B200LA_GRAPHS=0 so the kernels launch one by one).  With --profile-only the
@@ -37,6 +43,7 @@ def main():
     ap.add_argument("--cg-iters", type=int, default=3)
     ap.add_argument("--schedule", default="tune")
     ap.add_argument("--sigma", type=float, default=0.0)
+    ap.add_argument("--solver", default="cg", choices=["cg", "jacobi", "bicgstab"])
     ap.add_argument("--batch", type=int, default=0,
                     help="instead: solve a batch of this many 2D systems (n~logU[16,256], sigma 1) twice")
     ap.add_argument("--chunk", type=int, default=64)
@@ -68,6 +75,10 @@ def main():
         A.VectorMult(x, y)
     plat.synchronize()
     spmv_ms = (time.perf_counter() - t) * 1e3 / max(a.spmv_reps, 1)
+    sv = 8 if dt == np.float64 else 4
+    alg = s.nnz * (sv + 4) + (s.n + 1) * 4 + 2 * s.n * sv
+    if a.solver != "cg":
+        return solver_case(a, s, A, dt, fmt, prm, us, alg, sv)
     solver = lmp.setup_CG_solver(maxits=100000, atol=0.0, rtol=1e-12, dtol=1e8)
     solver.SetupOperator(A)
     solver._ensure()
@@ -75,13 +86,38 @@ def main():
     x0 = lmp.B200_lVector(s.n, platform=plat, dtype=dt)
     ms = (C.c_double * 3)()
     call("b200la_cg_profile", solver._solver, b.handle, x0.handle, a.cg_iters, ms)
-    sv = 8 if dt == np.float64 else 4
-    alg = s.nnz * (sv + 4) + (s.n + 1) * 4 + 2 * s.n * sv
     print(f"system n={s.n} nnz={s.nnz} dtype={a.dtype} schedule={FORMAT_NAMES[fmt]}/{prm} "
           f"tuned_us={us:.1f}")
     print(f"spmv wall {spmv_ms:.3f} ms/launch; cg kernels ms: spmv_dot {ms[0]:.4f} update {ms[1]:.4f} "
           f"direction {ms[2]:.4f}; spmv algorithmic bytes {alg} -> {alg / ms[0] / 1e6:.1f} GB/s")
     load()
+
+
+def solver_case(a, s, A, dt, fmt, prm, us, alg, sv):
+    """Kernel times of the Jacobi sweep or the BiCGSTAB pass kernels."""
+    plat = A.platform
+    if a.solver == "jacobi":
+        sol = lmp.Jacobi()
+        sol.SetSolveMode(2)
+        sol.SetNumIter(max(a.cg_iters, 1))
+        names, extra = ["sweep"], [2 * s.n * sv]
+    else:
+        sol = lmp.BiCGSTAB()
+        pc = lmp.PreconditionerBlockJacobiStand()
+        pc.Init_Jacobi()
+        sol.SetupPreconditioner(pc)
+        names = ["spmv_q (A q, q.r0-type sums)", "s update", "spmv_s (A s, t.s, t.t)", "x/r update",
+                 "direction"]
+        extra = [s.n * sv, 5 * s.n * sv, s.n * sv, 8 * s.n * sv, 5 * s.n * sv]
+    sol.InitControl(100000, 0.0, 1e-12, 1e8)
+    sol.SetupOperator(A)
+    b = lmp.B200_lVector.from_numpy(s.b.astype(dt), platform=plat, dtype=dt)
+    x0 = lmp.B200_lVector(s.n, platform=plat, dtype=dt)
+    ms = sol.profile(b, x0, a.cg_iters)
+    print(f"system n={s.n} nnz={s.nnz} dtype={a.dtype} schedule={FORMAT_NAMES[fmt]}/{prm} tuned_us={us:.1f}")
+    for k, name in enumerate(names):
+        nbytes = extra[k] + (alg if name.startswith(("sweep", "spmv")) else 0)
+        print(f"{a.solver} {name}: {ms[k]:.4f} ms, algorithmic {nbytes} bytes -> {nbytes / ms[k] / 1e6:.1f} GB/s")
 
 
 def batch_case(a):

@@ -2,7 +2,7 @@
 """Benchmark of the PCG hot path on B200: one JSON line on rank 0.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload batch|poisson3d]
+                    [--workload batch|poisson3d|varcoef3d|serve|bicgstab|jacobi]
 
 Workload "batch" (default): 1,024 independent 2D Q1 diffusion systems, n x n
 cells with n log-uniform in [16, 256] from the seed, lognormal per-cell
@@ -16,6 +16,12 @@ of FP64 CSR) are larger than L2.
 
 Workload "poisson3d": FP64 Jacobi-PCG on 3D Q1 Poisson, 128^3 cells
 (2,146,689 DOFs, 57,066,625 nnz), rel. 1e-10; a step is one solve.
+Workload "varcoef3d": the same shape with a lognormal coefficient (sigma 2),
+FP32 PCG inside FP64 refinement to 1e-10.  Workload "serve": a seeded
+Poisson-arrival request stream through the request loop (p50/p99).
+Workloads "bicgstab" and "jacobi": the poisson3d matrix solved by FP64
+BiCGSTAB with right Jacobi preconditioning to 1e-10 (solves/s), and swept by
+the Jacobi smoother (100 sweeps per step, sweeps/s).
 
 Multi-GPU: every rank solves its own batch (seeded per rank): independent
 systems need no exchange, value = all ranks' solves / the slowest rank's time.
@@ -56,7 +62,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="batch", choices=["batch", "poisson3d", "varcoef3d", "serve"])
+    ap.add_argument("--workload", default="batch",
+                    choices=["batch", "poisson3d", "varcoef3d", "serve", "bicgstab", "jacobi"])
     ap.add_argument("--cells", type=int, default=128, help="poisson3d cells per axis")
     ap.add_argument("--count", type=int, default=BATCH_COUNT, help="batch: systems per step")
     ap.add_argument("--requests", type=int, default=64, help="serve: requests per timed step")
@@ -78,6 +85,17 @@ def measured_peak_gbs():
     if os.path.exists(p):
         return float(json.load(open(p))["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
+
+
+def dram_rate(traffic, kernel_ms, peak):
+    """The dominant kernel's physical DRAM rate: the ncu-measured traffic per
+    launch over the CUDA-event duration (null without a capture).  Compressed
+    storage (int16 column offsets, no row pointer) moves fewer bytes than the
+    algorithmic count, so this can sit below `frac`."""
+    if not traffic or not kernel_ms:
+        return {"traffic_gbs": None, "traffic_frac": None}
+    gbs = traffic / (kernel_ms * 1e-3) / 1e9
+    return {"traffic_gbs": gbs, "traffic_frac": gbs / peak}
 
 
 def profile_traffic(key):
@@ -377,7 +395,8 @@ def run_batch(args, rank, local_rank, world, torch, dist, barrier):
                          "kernel": "batch_spmv_kernel<float> (K1: sliced-ELL SpMV + p.Ap) over an inner pass of "
                                    "all 1024 systems",
                          "algorithmic_bytes": spmv_bytes_alg, "kernel_ms": spmv_ms, "pass_kernels": kernels,
-                         "item_rows": {"spmv": item_rows[0], "update": item_rows[1], "direction": item_rows[2]}},
+                         "item_rows": {"spmv": item_rows[0], "update": item_rows[1], "direction": item_rows[2]},
+                         **dram_rate(profile_traffic("batch1024/f32/spmv"), spmv_ms, peak)},
             "cpu_baseline": cpu,
         }
         print(json.dumps(out))
@@ -704,7 +723,8 @@ def run_poisson3d(args, rank, local_rank, world, torch, dist, barrier):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": profile_traffic(f"poisson3d_{args.cells}/f64/spmv"), "peak_source": peak_kind,
                          "kernel": "cg_spmv_kernel (SpMV fused with p.Ap)", "algorithmic_bytes": bytes_spmv,
-                         "kernel_ms": {"spmv_dot": ms3[0], "update": ms3[1], "direction": ms3[2]}},
+                         "kernel_ms": {"spmv_dot": ms3[0], "update": ms3[1], "direction": ms3[2]},
+                         **dram_rate(profile_traffic(f"poisson3d_{args.cells}/f64/spmv"), ms3[0], peak)},
             "cpu_baseline": cpu}))
 
 
@@ -880,7 +900,232 @@ def run_varcoef3d(args, rank, local_rank, world, torch, dist, barrier):
                          "traffic": profile_traffic(f"varcoef3d_{args.cells}/f32/spmv"), "peak_source": peak_kind,
                          "kernel": "cg_spmv_kernel<float> (inner SpMV fused with p.Ap)",
                          "algorithmic_bytes": bytes_spmv,
-                         "kernel_ms": {"spmv_dot": ms3[0], "update": ms3[1], "direction": ms3[2]}},
+                         "kernel_ms": {"spmv_dot": ms3[0], "update": ms3[1], "direction": ms3[2]},
+                         **dram_rate(profile_traffic(f"varcoef3d_{args.cells}/f32/spmv"), ms3[0], peak)},
+            "cpu_baseline": cpu}))
+
+
+# ----------------------------------------------------------------- more solvers on the C2 matrix
+BICG_METRIC = "BiCGSTAB (right Jacobi) solves/s at 1e-10 rel. residual, FP64, 3D Q1 Poisson"
+JACOBI_METRIC = "Jacobi smoother sweeps/s (SmoothNormal), FP64, 3D Q1 Poisson"
+JACOBI_SWEEPS = 100
+
+
+def _ref_unavailable():
+    import oracle
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (reference sources absent)"}))
+        return True
+    return False
+
+
+def run_reference_bicgstab(args, rank):
+    import oracle
+    from ba_b200 import problems as P
+    if _ref_unavailable():
+        return
+    s = P.poisson_3d(args.cells)
+    counts = json.load(open(COUNTS)) if os.path.exists(COUNTS) else {}
+    full = counts.get(f"poisson3d_{args.cells}/bicgstab_jacobi/rtol1e-10", {}).get("iters", 20)
+    nthreads = os.cpu_count() or 1
+    sample, per_iter = 10, []
+    for step in range(args.warmup + args.steps):
+        r, _ = oracle.ref_bicgstab(s.rowptr, s.col, s.val, s.b, maxits=sample, atol=0.0, rtol=1e-10,
+                                   dtol=1e8, precond=True, impl=oracle.IMPL_OPENMP, nthreads=nthreads)
+        if step >= args.warmup:
+            per_iter.append(r.seconds / max(r.iters, 1))
+    value = 1.0 / (statistics.median(per_iter) * full)
+    print(json.dumps({
+        "impl": "reference", "metric": BICG_METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"fp64 bicgstab + right jacobi, 3d q1 poisson {args.cells}^3 cells, rel 1e-10",
+                   "n": s.n, "nnz": s.nnz, "parallelism": f"cpu openmp x{nthreads}"},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": nthreads, "kind": "reference",
+                         "sample": f"{sample} of {full} iterations of one solve per step (HiFlow3 lmp OPENMP "
+                                   f"classes, BiCGSTAB<LAD> restated over them), scaled"},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+
+
+def run_reference_jacobi(args, rank):
+    import oracle
+    from ba_b200 import problems as P
+    if _ref_unavailable():
+        return
+    s = P.poisson_3d(args.cells)
+    nthreads = os.cpu_count() or 1
+    sample, rates = 5, []
+    for step in range(args.warmup + args.steps):
+        r = oracle.ref_jacobi(s.rowptr, s.col, s.val, s.b, mode=oracle.JACOBI_SMOOTH_NORMAL, smooth_iter=sample,
+                              impl=oracle.IMPL_OPENMP, nthreads=nthreads)
+        if step >= args.warmup:
+            rates.append(r.iters / r.seconds)
+    value = statistics.median(rates)
+    print(json.dumps({
+        "impl": "reference", "metric": JACOBI_METRIC, "value": value, "unit": "sweeps/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * JACOBI_SWEEPS / value,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"fp64 jacobi smoothing, 3d q1 poisson {args.cells}^3 cells", "n": s.n,
+                   "nnz": s.nnz, "parallelism": f"cpu openmp x{nthreads}"},
+        "cpu_baseline": {"value": value, "unit": "sweeps/s", "cores": nthreads, "kind": "reference",
+                         "sample": f"{sample} sweeps per step (HiFlow3 lmp OPENMP classes, Jacobi<LAD> "
+                                   f"DoNormalIteration restated over them)"},
+        "e2e": {"value": value, "unit": "sweeps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+
+
+def _c2_setup(args, local_rank, torch):
+    from ba_b200 import lmp
+    from ba_b200 import problems as P
+    plat = lmp.Platform(local_rank)
+    stream = torch.cuda.current_stream()
+    plat.set_stream(stream.cuda_stream)
+    s = P.poisson_3d(args.cells)
+    A = lmp.B200_CSR_lMatrix(s.rowptr, s.col, s.val, platform=plat)
+    fmt, prm, _ = A.tune()
+    b = lmp.B200_lVector.from_numpy(s.b, platform=plat)
+    x = lmp.B200_lVector(s.n, platform=plat)
+    return plat, stream, s, A, fmt, prm, b, x
+
+
+def _timed(args, stream, torch, barrier, local_rank, step):
+    for _ in range(args.warmup):
+        step()
+    clocks = ClockSampler(local_rank)
+    barrier()
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    e1.synchronize()
+    barrier()
+    return D.max_over_ranks(e0.elapsed_time(e1)), clocks.stop()
+
+
+def _timed_e2e(args, stream, torch, barrier, b, x, n, step):
+    import ctypes as C
+    from ba_b200._lib import load
+    lib = load()
+    bh = torch.from_numpy(np.zeros(n)).pin_memory()
+    bh.copy_(torch.from_numpy(b.numpy()))
+    xh = torch.empty(n, dtype=torch.float64).pin_memory()
+    barrier()
+    h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    h0.record(stream)
+    for _ in range(args.steps):
+        lib.b200la_vec_upload(b.handle, C.c_void_p(bh.data_ptr()), n)
+        step()
+        lib.b200la_vec_download(x.handle, C.c_void_p(xh.data_ptr()), n)
+    h1.record(stream)
+    h1.synchronize()
+    return D.max_over_ranks(h0.elapsed_time(h1))
+
+
+def run_bicgstab(args, rank, local_rank, world, torch, dist, barrier):
+    from ba_b200 import lmp
+    from ba_b200._lib import FORMAT_NAMES
+    plat, stream, s, A, fmt, prm, b, x = _c2_setup(args, local_rank, torch)
+    n, nnz = s.n, s.nnz
+    solver = lmp.BiCGSTAB()
+    solver.InitControl(20000, 0.0, 1e-10, 1e8)
+    solver.SetupOperator(A)
+    pc = lmp.PreconditionerBlockJacobiStand()
+    pc.Init_Jacobi()
+    solver.SetupPreconditioner(pc)
+
+    def step():
+        x.Zeros()
+        assert solver.Solve(b, x) == lmp.kSolverSuccess
+    ms_max, clk = _timed(args, stream, torch, barrier, local_rank, step)
+    iters = solver.iter()
+    value = D.aggregate_rate(args.steps, world, ms_max)
+    e2e_value = D.aggregate_rate(args.steps, world, _timed_e2e(args, stream, torch, barrier, b, x, n, step))
+    x.Zeros()
+    ms = solver.profile(b, x, 20)
+    bytes_b1 = spmv_bytes(n, nnz, 8) + n * 8
+    peak, peak_kind = measured_peak_gbs()
+    achieved = bytes_b1 / (ms[0] / 1e3) / 1e9
+    key = f"poisson3d_{args.cells}/f64/bicgstab_spmv_q"
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import oracle
+        if oracle.ref_available():
+            nthreads = os.cpu_count() or 1
+            r, _ = oracle.ref_bicgstab(s.rowptr, s.col, s.val, s.b, maxits=10, atol=0.0, rtol=1e-10, dtol=1e8,
+                                       precond=True, impl=oracle.IMPL_OPENMP, nthreads=nthreads)
+            cpu = {"value": 1.0 / (r.seconds / max(r.iters, 1) * iters), "unit": "solves/s", "cores": nthreads,
+                   "kind": "reference", "sample": f"10 of {iters} iterations of one solve (HiFlow3 lmp OPENMP "
+                                                  f"classes, {nthreads} threads), scaled to a full solve"}
+    if rank == 0:
+        print(json.dumps({
+            "metric": BICG_METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"fp64 bicgstab + right jacobi, 3d q1 poisson {args.cells}^3 cells, rel 1e-10",
+                       "n": n, "nnz": nnz, "iters_per_solve": iters, "restarts": solver.restarts(),
+                       "parallelism": f"replicas x{world}", "spmv_schedule": FORMAT_NAMES[fmt] + f"/{prm}",
+                       "l2": "inputs larger than L2 (matrix 685 MB streamed twice per iteration)"},
+            "clocks": clk,
+            "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": n * 8, "d2h_bytes_per_step": n * 8},
+            "gpu_launches": args.steps * 5 * (iters + 1),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": profile_traffic(key), "peak_source": peak_kind,
+                         "kernel": "bicg_spmv_q_kernel (A q fused with Ap.r0, Ap.Ap)", "algorithmic_bytes": bytes_b1,
+                         "kernel_ms": dict(zip(("spmv_q", "s_update", "spmv_s", "xr_update", "direction"), ms)),
+                         **dram_rate(profile_traffic(key), ms[0], peak)},
+            "cpu_baseline": cpu}))
+
+
+def run_jacobi(args, rank, local_rank, world, torch, dist, barrier):
+    from ba_b200 import lmp
+    from ba_b200._lib import FORMAT_NAMES
+    plat, stream, s, A, fmt, prm, b, x = _c2_setup(args, local_rank, torch)
+    n, nnz = s.n, s.nnz
+    j = lmp.Jacobi()
+    j.SetupOperator(A)
+    j.SetSolveMode(2)
+    j.SetNumIter(JACOBI_SWEEPS)
+
+    def step():
+        x.Zeros()
+        assert j.Solve(b, x) == lmp.kSolverSuccess
+    ms_max, clk = _timed(args, stream, torch, barrier, local_rank, step)
+    value = D.aggregate_rate(args.steps * JACOBI_SWEEPS, world, ms_max)
+    e2e_value = D.aggregate_rate(args.steps * JACOBI_SWEEPS, world,
+                                 _timed_e2e(args, stream, torch, barrier, b, x, n, step))
+    x.Zeros()
+    ms = j.profile(b, x, 20)
+    bytes_sweep = spmv_bytes(n, nnz, 8) + 2 * n * 8
+    peak, peak_kind = measured_peak_gbs()
+    achieved = bytes_sweep / (ms[0] / 1e3) / 1e9
+    key = f"poisson3d_{args.cells}/f64/jacobi_sweep"
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import oracle
+        if oracle.ref_available():
+            nthreads = os.cpu_count() or 1
+            r = oracle.ref_jacobi(s.rowptr, s.col, s.val, s.b, mode=oracle.JACOBI_SMOOTH_NORMAL, smooth_iter=5,
+                                  impl=oracle.IMPL_OPENMP, nthreads=nthreads)
+            cpu = {"value": r.iters / r.seconds, "unit": "sweeps/s", "cores": nthreads, "kind": "reference",
+                   "sample": f"5 sweeps (HiFlow3 lmp OPENMP classes, {nthreads} threads)"}
+    if rank == 0:
+        print(json.dumps({
+            "metric": JACOBI_METRIC, "value": value, "unit": "sweeps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"fp64 jacobi smoothing ({JACOBI_SWEEPS} sweeps per step), 3d q1 poisson "
+                                   f"{args.cells}^3 cells", "n": n, "nnz": nnz, "parallelism": f"replicas x{world}",
+                       "spmv_schedule": FORMAT_NAMES[fmt] + f"/{prm}",
+                       "l2": "inputs larger than L2 (matrix 685 MB streamed per sweep)"},
+            "clocks": clk,
+            "e2e": {"value": e2e_value, "unit": "sweeps/s", "h2d_bytes_per_step": n * 8, "d2h_bytes_per_step": n * 8},
+            "gpu_launches": args.steps * JACOBI_SWEEPS,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": profile_traffic(key), "peak_source": peak_kind,
+                         "kernel": "jacobi_sweep_kernel (r = b - A x_k, ||r||, x_k+1 = x_k + inv_D r)",
+                         "algorithmic_bytes": bytes_sweep, "kernel_ms": ms[0],
+                         **dram_rate(profile_traffic(key), ms[0], peak)},
             "cpu_baseline": cpu}))
 
 
@@ -890,7 +1135,8 @@ def main():
     if args.impl == "reference":
         if rank == 0:
             {"batch": run_reference_batch, "poisson3d": run_reference_poisson3d,
-             "varcoef3d": run_reference_varcoef3d, "serve": run_reference_serve}[args.workload](args, rank)
+             "varcoef3d": run_reference_varcoef3d, "serve": run_reference_serve,
+             "bicgstab": run_reference_bicgstab, "jacobi": run_reference_jacobi}[args.workload](args, rank)
         return
     import datetime
 
@@ -909,7 +1155,7 @@ def main():
 
     load()
     fn = {"batch": run_batch, "poisson3d": run_poisson3d, "varcoef3d": run_varcoef3d,
-          "serve": run_serve}[args.workload]
+          "serve": run_serve, "bicgstab": run_bicgstab, "jacobi": run_jacobi}[args.workload]
     fn(args, rank, local_rank, world, torch, dist, barrier)
     if world > 1:
         dist.barrier()

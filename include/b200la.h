@@ -193,6 +193,68 @@ int b200la_cg_profile(b200la_cg s, b200la_vec b, b200la_vec x, int iters, double
 int b200la_pcg_solve(b200la_mat A, b200la_vec b, b200la_vec x, const b200la_cg_params *params,
                      b200la_cg_result *result);
 
+/* ---- more solvers on the same kernels: the stationary Jacobi<LAD> solver /
+ * smoother (linear_solver/jacobi.cc:101-356) and BiCGSTAB<LAD>
+ * (linear_solver/bicgstab.h:104-473).  Like CG, each solve is one CUDA-graph
+ * launch whose WHILE node runs the iteration on the device.
+ *
+ * Jacobi: one fused kernel per sweep computes r = b - A x_k, its norm and
+ * x_{k+1} = x_k + w inv_D r (the same iterate as the reference's
+ * y = inv_D (b - A_nodiag x), x = (1 - w) x + w y, rounded differently) into a
+ * second buffer, so the residual test of x_k costs no extra SpMV; the test
+ * runs when k is a multiple of inner_iter, as SolveNormal/SolveDamped check
+ * after every inner_iter sweeps.  Smoothing modes run a fixed number of sweeps
+ * (SmoothNormal: smooth_iter * inner_iter; SmoothDamped: maxits * inner_iter,
+ * as jacobi.cc:276 loops to maxits_) and end in B200LA_DONE_FIXED.
+ *
+ * BiCGSTAB: per iteration A q with q.r0-type sums, s = r - alpha Ap, A s with
+ * t.s and t.t, the x/r update with r.r and r.r0 and IterateControl, and the
+ * direction update; restarts when |sigma| <= eps ||Ap|| ||r0|| and the short
+ * update when ||s|| <= eps follow the reference (eps 1e-15, or 5e-16 with
+ * right preconditioning).  With right Jacobi preconditioning the direction is
+ * kept as q = inv_D p, so A (P p) is one SpMV of q. */
+#define B200LA_METHOD_JACOBI 1
+#define B200LA_METHOD_BICGSTAB 2
+#define B200LA_JACOBI_SOLVE_NORMAL 0
+#define B200LA_JACOBI_SOLVE_DAMPED 1
+#define B200LA_JACOBI_SMOOTH_NORMAL 2
+#define B200LA_JACOBI_SMOOTH_DAMPED 3
+#define B200LA_DONE_FIXED 6 /* a fixed number of sweeps ran (no stopping test) */
+
+typedef struct {
+  int method;       /* B200LA_METHOD_JACOBI / _BICGSTAB */
+  int maxits;       /* IterateControl maxits */
+  double atol, rtol, dtol;
+  int precond;      /* BiCGSTAB: 0 "NoPreconditioning", 1 "RightPreconditioning" (Jacobi) */
+  int mode;         /* Jacobi SetSolveMode: B200LA_JACOBI_* */
+  int inner_iter;   /* Jacobi SetInnerIter (>= 1) */
+  int smooth_iter;  /* Jacobi SetNumIter (>= 1) */
+  double w;         /* Jacobi SetDampingParameter (> 0; 1 in the normal modes) */
+} b200la_solver_params;
+
+typedef struct {
+  int iters;        /* iterations (Jacobi: sweeps) */
+  int state;        /* B200LA_ITERATE .. B200LA_DONE_FIXED */
+  int solver_state; /* B200LA_SOLVER_SUCCESS / _EXCEEDED / _ERROR */
+  int restarts;     /* BiCGSTAB restarts after the first start */
+  double res;       /* ||r||_2 at the last test */
+  double res_init;  /* ||r||_2 at the (last re)start */
+  double res_rel;
+} b200la_solver_result;
+
+typedef struct b200la_solver_s *b200la_solver;
+
+int b200la_solver_create(b200la_mat A, const b200la_solver_params *params, b200la_solver *out);
+int b200la_solver_destroy(b200la_solver s);
+/* Solve(b, &x): x holds the start value on entry and the solution on exit. */
+int b200la_solver_solve(b200la_solver s, b200la_vec b, b200la_vec x, b200la_solver_result *result);
+/* Instrumentation: from the start value x, runs `passes` passes of the
+ * iteration as separate launches with CUDA events between the kernels and
+ * writes the mean milliseconds per launch of each kernel of a pass:
+ * Jacobi ms[0] = sweep; BiCGSTAB ms[0..4] = A q, s update, A s, x/r update,
+ * direction.  x is not modified. */
+int b200la_solver_profile(b200la_solver s, b200la_vec b, b200la_vec x, int passes, double *ms);
+
 /* ---- Q1 system assembly on the device (no reference counterpart: the
  * reference assembles on the host through its FE stack and uploads the CSR).
  * Builds the Q1 stiffness of -div(kappa grad u) on `cells`^dim uniform cells of

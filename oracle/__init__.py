@@ -6,10 +6,12 @@ The product library ba_b200 never imports it.
 
 Two checkers:
 * ``liboracle.so``: the C restatement in pcg_oracle.c (CG<LAD>, lmp cg(),
-  IterateControl, CSR SpMV, BLAS-1, Jacobi, MPIR-style refinement);
+  IterateControl, CSR SpMV, BLAS-1, Jacobi, MPIR-style refinement, the
+  stationary Jacobi<LAD> solver and BiCGSTAB<LAD>);
 * ``_ref/libhiflow_lmp_ref.so``: HiFlow3's own lmp CPU sources (NAIVE and
   OPENMP implementations, lPreconditioner_Jacobi, lmp cg()) compiled by
-  oracle/ref/Makefile, with a driver restating CG<LAD> over those objects.
+  oracle/ref/Makefile, with a driver restating CG<LAD>, Jacobi<LAD> and
+  BiCGSTAB<LAD> over those objects.
 """
 from .oracle import (  # noqa: F401
     CTRL_FAIL_DIV,
@@ -19,17 +21,26 @@ from .oracle import (  # noqa: F401
     CTRL_SUCCESS_REL,
     IMPL_NAIVE,
     IMPL_OPENMP,
+    JACOBI_SMOOTH_DAMPED,
+    JACOBI_SMOOTH_NORMAL,
+    JACOBI_SOLVE_DAMPED,
+    JACOBI_SOLVE_NORMAL,
     OracleResult,
     RefSystem,
+    bicgstab,
     cg,
     dot,
     invdiag,
     iterate_check,
+    jacobi,
     lmp_cg,
     mpir,
     ref_available,
+    ref_bicgstab,
     ref_cg,
+    ref_jacobi,
     ref_lmp_cg,
     ref_spmv,
     spmv,
+    spmv_nodiag,
 )

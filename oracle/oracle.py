@@ -44,6 +44,13 @@ def _load():
                 C.c_double, C.c_int, fp, fp, _ip, _dp, _dp]
             getattr(lib, f"orc_lmp_cg_{s}").argtypes = [
                 C.c_int, _i32p, _i32p, fp, fp, fp, T, T, _ip, fp]
+            getattr(lib, f"orc_spmv_nodiag_{s}").argtypes = [C.c_int, _i32p, _i32p, fp, fp, fp]
+            getattr(lib, f"orc_jacobi_{s}").argtypes = [
+                C.c_int, _i32p, _i32p, fp, fp, fp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
+                C.c_double, C.c_double, C.c_double, _ip, _dp, _dp]
+            getattr(lib, f"orc_bicgstab_{s}").argtypes = [
+                C.c_int, _i32p, _i32p, fp, fp, fp, C.c_int, fp, C.c_int, C.c_double, C.c_double,
+                C.c_double, _ip, _ip, _dp, _dp]
         lib.orc_iterate_check.argtypes = [C.c_int, C.c_double, C.c_int, C.c_double, C.c_double,
                                           C.c_double, _dp]
         lib.orc_mpir_d.argtypes = [C.c_int, _i32p, _i32p, _f64p, _f32p, _f64p, _f64p, C.c_int,
@@ -69,6 +76,12 @@ def _load_ref():
             getattr(lib, f"ref_cg_solve_{s}").argtypes = [
                 C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _i32p, _i32p, fp, fp, fp, C.c_int,
                 C.c_double, C.c_double, C.c_double, _ip, _dp, _dp, _dp]
+        lib.ref_jacobi_solve_d.argtypes = [
+            C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p, C.c_int,
+            C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, _ip, _dp, _dp, _dp]
+        lib.ref_bicgstab_solve_d.argtypes = [
+            C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p, C.c_int,
+            C.c_double, C.c_double, C.c_double, _ip, _ip, _dp, _dp, _dp]
         lib.ref_lmp_cg_d.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f64p, _f64p,
                                      _f64p, C.c_double, C.c_double, _ip]
         _ref = lib
@@ -96,6 +109,7 @@ class OracleResult:
     res: float
     res_init: float
     state: int
+    seconds: float = 0.0   # reference runs: time of the iteration loop alone
 
     @property
     def res_rel(self) -> float:
@@ -179,6 +193,82 @@ def mpir(rowptr, col, val, b, *, rtol=1e-10, inner_rtol=1e-4, inner_maxits=10000
                             np.empty(8 * n, np.float32), C.byref(outer), C.byref(inner),
                             C.byref(res), C.byref(res0))
     return OracleResult(x, inner.value, res.value, res0.value, st), outer.value
+
+
+def spmv_nodiag(rowptr, col, val, x, dtype=np.float64) -> np.ndarray:
+    """CPU_CSR_lMatrix::VectorMultNoDiag restated in C."""
+    s, T = _sfx(dtype)
+    rp, c, v = _csr(rowptr, col, val, T)
+    n = rp.shape[0] - 1
+    y = np.empty(n, T)
+    getattr(_load(), f"orc_spmv_nodiag_{s}")(n, rp, c, v, np.ascontiguousarray(x, T), y)
+    return y
+
+
+# Jacobi<LAD>::SetSolveMode values (linear_solver/jacobi.cc SolveImpl)
+JACOBI_SOLVE_NORMAL, JACOBI_SOLVE_DAMPED, JACOBI_SMOOTH_NORMAL, JACOBI_SMOOTH_DAMPED = range(4)
+
+
+def jacobi(rowptr, col, val, b, x0=None, *, mode=JACOBI_SOLVE_NORMAL, maxits=1000, inner_iter=1,
+           smooth_iter=1, w=1.0, atol=1e-12, rtol=1e-8, dtol=1e8, dtype=np.float64) -> OracleResult:
+    """Jacobi<LAD> (stationary solver / smoother) restated in C."""
+    s, T = _sfx(dtype)
+    rp, c, v = _csr(rowptr, col, val, T)
+    n = rp.shape[0] - 1
+    x = np.zeros(n, T) if x0 is None else np.array(x0, T)
+    it, res, res0 = C.c_int(), C.c_double(), C.c_double()
+    st = getattr(_load(), f"orc_jacobi_{s}")(n, rp, c, v, np.ascontiguousarray(b, T), x, int(mode),
+                                             int(maxits), int(inner_iter), int(smooth_iter), float(w),
+                                             atol, rtol, dtol, C.byref(it), C.byref(res),
+                                             C.byref(res0))
+    if st == -2:
+        raise ValueError("a row has no nonzero diagonal")
+    return OracleResult(x, it.value, res.value, res0.value, st)
+
+
+def bicgstab(rowptr, col, val, b, x0=None, *, maxits=1000, atol=1e-12, rtol=1e-8, dtol=1e8,
+             precond=True, dtype=np.float64) -> tuple[OracleResult, int]:
+    """BiCGSTAB<LAD> (no / right Jacobi preconditioning) restated in C.
+    Returns the result and the number of restarts."""
+    s, T = _sfx(dtype)
+    rp, c, v = _csr(rowptr, col, val, T)
+    n = rp.shape[0] - 1
+    x = np.zeros(n, T) if x0 is None else np.array(x0, T)
+    inv = invdiag(rp, c, v, T) if precond else np.zeros(1, T)
+    it, rs, res, res0 = C.c_int(), C.c_int(), C.c_double(), C.c_double()
+    st = getattr(_load(), f"orc_bicgstab_{s}")(n, rp, c, v, np.ascontiguousarray(b, T), x,
+                                               int(bool(precond)), inv, int(maxits), atol, rtol, dtol,
+                                               C.byref(it), C.byref(rs), C.byref(res), C.byref(res0))
+    return OracleResult(x, it.value, res.value, res0.value, st), rs.value
+
+
+def ref_jacobi(rowptr, col, val, b, x0=None, *, mode=JACOBI_SOLVE_NORMAL, maxits=1000, inner_iter=1,
+               smooth_iter=1, w=1.0, atol=1e-12, rtol=1e-8, dtol=1e8, impl=IMPL_NAIVE,
+               nthreads=1) -> OracleResult:
+    """Jacobi<LAD> restated over the reference's compiled lmp objects (FP64)."""
+    rp, c, v = _csr(rowptr, col, val, np.float64)
+    n = rp.shape[0] - 1
+    x = np.zeros(n) if x0 is None else np.array(x0, np.float64)
+    it, res, res0, sec = C.c_int(), C.c_double(), C.c_double(), C.c_double()
+    st = _load_ref().ref_jacobi_solve_d(impl, nthreads, int(mode), n, c.shape[0], rp, c, v,
+                                        np.ascontiguousarray(b, np.float64), x, int(maxits),
+                                        int(inner_iter), int(smooth_iter), float(w), atol, rtol, dtol,
+                                        C.byref(it), C.byref(res), C.byref(res0), C.byref(sec))
+    return OracleResult(x, it.value, res.value, res0.value, st, sec.value)
+
+
+def ref_bicgstab(rowptr, col, val, b, x0=None, *, maxits=1000, atol=1e-12, rtol=1e-8, dtol=1e8,
+                 precond=True, impl=IMPL_NAIVE, nthreads=1) -> tuple[OracleResult, int]:
+    """BiCGSTAB<LAD> restated over the reference's compiled lmp objects (FP64)."""
+    rp, c, v = _csr(rowptr, col, val, np.float64)
+    n = rp.shape[0] - 1
+    x = np.zeros(n) if x0 is None else np.array(x0, np.float64)
+    it, rs, res, res0, sec = C.c_int(), C.c_int(), C.c_double(), C.c_double(), C.c_double()
+    st = _load_ref().ref_bicgstab_solve_d(impl, nthreads, int(bool(precond)), n, c.shape[0], rp, c, v,
+                                          np.ascontiguousarray(b, np.float64), x, int(maxits), atol,
+                                          rtol, dtol, C.byref(it), C.byref(rs), C.byref(res),
+                                          C.byref(res0), C.byref(sec))
+    return OracleResult(x, it.value, res.value, res0.value, st, sec.value), rs.value
 
 
 def ref_spmv(rowptr, col, val, x, *, impl=IMPL_NAIVE, nthreads=1, dtype=np.float64) -> np.ndarray:

@@ -18,6 +18,8 @@
 #include <math.h>
 #include <stddef.h>
 #include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
 
 /* IterateControl states, numbered as the B200 library's solver status. */
 enum { CTRL_ITERATE = 0, CTRL_SUCCESS_ABS = 1, CTRL_SUCCESS_REL = 2,
@@ -181,6 +183,216 @@ int orc_iterate_check(int step, double value, int maxits, double atol,
 
 ORACLE_INSTANTIATE(double, d, sqrt)
 ORACLE_INSTANTIATE(float, f, sqrtf)
+
+/*
+ * Jacobi<LAD> and BiCGSTAB<LAD> on one rank, over the routines above.
+ */
+#define ORACLE_KRYLOV(T, S, SQRT, FABS)                                           \
+  /* CPU_CSR_lMatrix::SwapDiagElementsToRowFront (lmp/lmatrix_csr_cpu.cc:      \
+   * 430-454): in each row the first entry whose column is the row trades      \
+   * places (value and column) with the row's first entry. */                 \
+  static void orc_swap_diag_##S(int n, const int *rowptr, int *col, T *val) {  \
+    for (int i = 0; i < n; ++i)                                                \
+      for (int j = rowptr[i]; j < rowptr[i + 1]; ++j)                          \
+        if (col[j] == i) {                                                     \
+          const int j0 = rowptr[i];                                            \
+          T tv = val[j0]; val[j0] = val[j]; val[j] = tv;                       \
+          int tc = col[j0]; col[j0] = col[j]; col[j] = tc;                     \
+          break;                                                               \
+        }                                                                      \
+  }                                                                            \
+  /* CPU_CSR_lMatrix::VectorMultNoDiag (lmp/lmatrix_csr_cpu.cc:479-492):       \
+   * y_i = sum over stored j with col[j] != i, in stored order. */             \
+  void orc_spmv_nodiag_##S(int n, const int *rowptr, const int *col,           \
+                           const T *val, const T *x, T *y) {                   \
+    for (int i = 0; i < n; ++i) {                                              \
+      T res = 0;                                                               \
+      for (int j = rowptr[i]; j < rowptr[i + 1]; ++j)                          \
+        if (col[j] != i) res += val[j] * x[col[j]];                            \
+      y[i] = res;                                                              \
+    }                                                                          \
+  }                                                                            \
+  /* Jacobi<LAD> (linear_solver/jacobi.cc): Prepare (:35-63) moves each       \
+   * diagonal entry to the front of its row and takes inv_D = 1/a_ii;         \
+   * mode 0/1 = SolveNormal/SolveDamped (:145-254): Check(iter, ||b - A x||)   \
+   * before the loop and after every inner_iter sweeps; mode 2 = SmoothNormal \
+   * (smooth_iter * inner_iter sweeps), mode 3 = SmoothDamped (maxits *       \
+   * inner_iter sweeps; the reference loops to maxits_ there, :276).  A sweep \
+   * (:288-356): y = A_nodiag x; y = -y + b; y .*= inv_D; x = y, or           \
+   * x = (1 - w) x + w y.  Smoothing modes return CTRL_ITERATE; -2 if a       \
+   * diagonal entry is missing or zero; -3 if out of memory. */              \
+  int orc_jacobi_##S(int n, const int *rowptr, const int *col_in,              \
+                     const T *val_in, const T *b, T *x, int mode, int maxits,  \
+                     int inner_iter, int smooth_iter, double w, double atol,   \
+                     double rtol, double dtol, int *iters, double *res_out,    \
+                     double *res_init_out) {                                   \
+    const int nnz = rowptr[n];                                                 \
+    int *col = (int *)malloc(sizeof(int) * (size_t)(nnz > 0 ? nnz : 1));       \
+    T *val = (T *)malloc(sizeof(T) * (size_t)(nnz > 0 ? nnz : 1));             \
+    T *work = (T *)malloc(sizeof(T) * 3 * (size_t)(n > 0 ? n : 1));            \
+    if (!col || !val || !work) {                                               \
+      free(col); free(val); free(work);                                        \
+      return -3;                                                               \
+    }                                                                          \
+    T *invd = work, *y = work + n, *r = work + 2 * (size_t)n;                  \
+    memcpy(col, col_in, sizeof(int) * (size_t)nnz);                            \
+    memcpy(val, val_in, sizeof(T) * (size_t)nnz);                              \
+    orc_swap_diag_##S(n, rowptr, col, val);                                    \
+    int state = CTRL_ITERATE, iter = 0;                                        \
+    double res = 0., first = 0.;                                               \
+    *res_init_out = 0.;                                                        \
+    if (orc_invdiag_##S(n, rowptr, col, val, invd) >= 0) {                     \
+      state = -2;                                                              \
+      goto done;                                                               \
+    }                                                                          \
+    const int damped = mode == 1 || mode == 3;                                 \
+    const T tw = (T)w, keep = (T)(1.0 - tw);                                   \
+    for (int k = 0, outer = mode == 2 ? smooth_iter : maxits;; ++k) {          \
+      if (mode <= 1) {                                                         \
+        orc_spmv_##S(n, rowptr, col, val, x, r);                               \
+        orc_scaleadd_##S(n, r, (T)-1., b);                                     \
+        res = (double)SQRT(orc_dot_##S(n, r, r));                              \
+        if (iter == 0) *res_init_out = res;                                    \
+        state = orc_iterate_check(iter, res, maxits, atol, rtol, dtol,        \
+                                  &first);                                     \
+        if (state != CTRL_ITERATE) break;                                      \
+      } else if (k >= outer) {                                                 \
+        break;                                                                 \
+      }                                                                        \
+      for (int i = 0; i < inner_iter; ++i) {                                   \
+        ++iter;                                                                \
+        orc_spmv_nodiag_##S(n, rowptr, col, val, x, y);                        \
+        orc_scaleadd_##S(n, y, (T)-1., b);                                     \
+        orc_ewmult_##S(n, y, invd);                                            \
+        if (damped) {                                                          \
+          for (int q = 0; q < n; ++q) x[q] *= keep;                            \
+          orc_axpy_##S(n, x, y, tw);                                           \
+        } else {                                                               \
+          memcpy(x, y, sizeof(T) * (size_t)n);                                 \
+        }                                                                      \
+      }                                                                        \
+    }                                                                          \
+  done:                                                                        \
+    *iters = iter;                                                             \
+    *res_out = res;                                                            \
+    free(col); free(val); free(work);                                          \
+    return state;                                                              \
+  }                                                                            \
+  /* BiCGSTAB<LAD>::SolveNoPrecond / SolvePrecondRight (linear_solver/         \
+   * bicgstab.h:127-293, :297-473) with the Jacobi preconditioner h = copy(v) \
+   * .* inv_D.  A step: Ap = A (P) p; sigma = Ap.r0; restart (r0 = b - A x,    \
+   * r = p = r0, the count carried on) unless |sigma| > eps ||Ap|| ||r0||;    \
+   * alpha = rho / sigma; s = r - alpha Ap; if ||s|| > eps: t = A (P) s,       \
+   * omega = t.s / t.t, x += (P)(alpha p + omega s), r = s - omega t, check,  \
+   * rho = r.r0, beta = alpha rho / (omega rho_old), p = beta p + r - omega    \
+   * beta Ap; else x += (P)(alpha p), r = s, check.  eps = 1e-15 without,     \
+   * 5e-16 with preconditioner.  restarts counts the restarts after the       \
+   * first start; every restart follows a counted step, so IterateControl    \
+   * ends the loop at maxits.  Returns the IterateControl state, -3 if out of \
+   * memory. */                                                               \
+  int orc_bicgstab_##S(int n, const int *rowptr, const int *col, const T *val, \
+                       const T *b, T *x, int precond, const T *invd,           \
+                       int maxits, double atol, double rtol, double dtol,      \
+                       int *iters, int *restarts, double *res_out,             \
+                       double *res_init_out) {                                 \
+    T *w = (T *)malloc(sizeof(T) * 8 * (size_t)(n > 0 ? n : 1));               \
+    if (!w) return -3;                                                         \
+    T *r = w, *r0 = w + n, *p = w + 2 * (size_t)n, *Ap = w + 3 * (size_t)n;    \
+    T *s = w + 4 * (size_t)n, *t = w + 5 * (size_t)n, *h = w + 6 * (size_t)n;  \
+    T *h1 = w + 7 * (size_t)n;                                                 \
+    const T eps = precond ? (T)5.e-16 : (T)1.e-15;                             \
+    T alpha = 0, beta, ressq, rho, rho_old, omega, sigma, tol1;                \
+    int iter = 0, nrestart = -1, conv = CTRL_ITERATE, restart = 1;             \
+    double res = 0., first = 0.;                                               \
+    while (restart) {                                                          \
+      restart = 0;                                                             \
+      ++nrestart;                                                              \
+      memset(w, 0, sizeof(T) * 8 * (size_t)n);                                 \
+      orc_spmv_##S(n, rowptr, col, val, x, r0);                                \
+      orc_scaleadd_##S(n, r0, (T)-1., b);                                      \
+      memcpy(r, r0, sizeof(T) * (size_t)n);                                    \
+      ressq = orc_dot_##S(n, r, r);                                            \
+      rho = rho_old = ressq;                                                   \
+      res = (double)SQRT(ressq);                                               \
+      *res_init_out = res;                                                     \
+      conv = orc_iterate_check(iter, res, maxits, atol, rtol, dtol, &first);   \
+      memcpy(p, r, sizeof(T) * (size_t)n);                                     \
+      while (conv == CTRL_ITERATE && !restart) {                               \
+        ++iter;                                                                \
+        if (precond) {                                                         \
+          memcpy(h, p, sizeof(T) * (size_t)n);                                 \
+          orc_ewmult_##S(n, h, invd);                                          \
+          orc_spmv_##S(n, rowptr, col, val, h, Ap);                            \
+        } else {                                                               \
+          orc_spmv_##S(n, rowptr, col, val, p, Ap);                            \
+        }                                                                      \
+        sigma = orc_dot_##S(n, Ap, r0);                                        \
+        tol1 = eps * SQRT(orc_dot_##S(n, Ap, Ap)) * SQRT(orc_dot_##S(n, r0, r0)); \
+        if (!(FABS(sigma) > tol1)) {                                           \
+          restart = 1;                                                         \
+          break;                                                               \
+        }                                                                      \
+        alpha = rho / sigma;                                                   \
+        memcpy(s, r, sizeof(T) * (size_t)n);                                   \
+        orc_axpy_##S(n, s, Ap, -alpha);                                        \
+        if (SQRT(orc_dot_##S(n, s, s)) > eps) {                                \
+          if (precond) {                                                       \
+            memcpy(h, s, sizeof(T) * (size_t)n);                               \
+            orc_ewmult_##S(n, h, invd);                                        \
+            orc_spmv_##S(n, rowptr, col, val, h, t);                           \
+          } else {                                                             \
+            orc_spmv_##S(n, rowptr, col, val, s, t);                           \
+          }                                                                    \
+          omega = orc_dot_##S(n, t, s) / orc_dot_##S(n, t, t);                 \
+          if (precond) {                                                       \
+            memset(h1, 0, sizeof(T) * (size_t)n);                              \
+            orc_axpy_##S(n, h1, p, alpha);                                     \
+            orc_axpy_##S(n, h1, s, omega);                                     \
+            memcpy(h, h1, sizeof(T) * (size_t)n);                              \
+            orc_ewmult_##S(n, h, invd);                                        \
+            orc_axpy_##S(n, x, h, (T)1.);                                      \
+          } else {                                                             \
+            orc_axpy_##S(n, x, p, alpha);                                      \
+            orc_axpy_##S(n, x, s, omega);                                      \
+          }                                                                    \
+          memcpy(r, s, sizeof(T) * (size_t)n);                                 \
+          orc_axpy_##S(n, r, t, -omega);                                       \
+          ressq = orc_dot_##S(n, r, r);                                        \
+          res = (double)SQRT(ressq);                                           \
+          conv = orc_iterate_check(iter, res, maxits, atol, rtol, dtol, &first); \
+          if (conv != CTRL_ITERATE) break;                                     \
+          rho = orc_dot_##S(n, r, r0);                                         \
+          beta = (alpha * rho) / (omega * rho_old);                            \
+          rho_old = rho;                                                       \
+          orc_scaleadd_##S(n, p, beta, r);                                     \
+          orc_axpy_##S(n, p, Ap, -omega * beta);                               \
+        } else {                                                               \
+          if (precond) {                                                       \
+            memset(h1, 0, sizeof(T) * (size_t)n);                              \
+            orc_axpy_##S(n, h1, p, alpha);                                     \
+            memcpy(h, h1, sizeof(T) * (size_t)n);                              \
+            orc_ewmult_##S(n, h, invd);                                        \
+            orc_axpy_##S(n, x, h, (T)1.);                                      \
+          } else {                                                             \
+            orc_axpy_##S(n, x, p, alpha);                                      \
+          }                                                                    \
+          memcpy(r, s, sizeof(T) * (size_t)n);                                 \
+          ressq = orc_dot_##S(n, r, r);                                        \
+          res = (double)SQRT(ressq);                                           \
+          conv = orc_iterate_check(iter, res, maxits, atol, rtol, dtol, &first); \
+          if (conv != CTRL_ITERATE) break;                                     \
+        }                                                                      \
+      }                                                                        \
+    }                                                                          \
+    *iters = iter;                                                             \
+    *restarts = nrestart;                                                      \
+    *res_out = res;                                                            \
+    free(w);                                                                   \
+    return conv;                                                               \
+  }
+
+ORACLE_KRYLOV(double, d, sqrt, fabs)
+ORACLE_KRYLOV(float, f, sqrtf, fabsf)
 
 /*
  * Mixed-precision iterative refinement around a float inner CG, structured

@@ -21,6 +21,10 @@
 //                        the diagonal block's VectorMult, so the restatement
 //                        issues exactly the arithmetic the reference does.
 //   * ref_lmp_cg_*    -> the reference's own lmp cg() (lmp/solvers/cg.cc:35).
+//   * ref_jacobi_solve_d, ref_bicgstab_solve_d -> single-rank restatements of
+//                        Jacobi<LAD> (linear_solver/jacobi.cc:145-356) and
+//                        BiCGSTAB<LAD> (linear_solver/bicgstab.h:127-473) over
+//                        the same compiled lmp calls.
 #include <chrono>
 #include <cmath>
 #include <vector>
@@ -210,6 +214,208 @@ int lmp_cg(int impl, int nthreads, int n, int nnz, const int *rowptr,
   return rv;
 }
 
+// Jacobi<LAD> (linear_solver/jacobi.cc) on one rank: Prepare/BuildImpl
+// (:35-63: SwapDiagElementsToRowFront, extract_invdiagelements), then
+// SolveNormal/SolveDamped (:145-254: residual b - A x, Check(iter, ||r||) once
+// per inner_iter sweeps) or SmoothNormal (smooth_iter * inner_iter sweeps) /
+// SmoothDamped (maxits * inner_iter sweeps, :256-285).  One sweep is
+// DoNormalIteration/DoDampedIteration (:288-356): y = A_nodiag x,
+// y.ScaleAdd(-1, b), y .*= inv_D, then x = y or x = (1 - w) x + w y.
+// Smoothing modes return CTRL_ITERATE (no stopping test).
+template < typename T >
+int jacobi_solve(int impl, int nthreads, int mode, int n, int nnz,
+                 const int *rowptr, const int *col, const T *val, const T *bh,
+                 T *xh, int maxits, int inner_iter, int smooth_iter, double w,
+                 double atol, double rtol, double dtol, int *iters,
+                 double *res_out, double *res_init_out, double *seconds) {
+  CPU_CSR_lMatrix< T > *A = make_matrix< T >(impl, nthreads, n, nnz, rowptr,
+                                             col, val);
+  A->SwapDiagElementsToRowFront();
+  lVector< T > *b = make_vector< T >(impl, n, "b");
+  lVector< T > *x = make_vector< T >(impl, n, "x");
+  lVector< T > *y = make_vector< T >(impl, n, "y");
+  lVector< T > *r = make_vector< T >(impl, n, "res");
+  lVector< T > *invd = make_vector< T >(impl, n, "inv_diag");
+  b->SetBlockValues(0, n, bh);
+  x->SetBlockValues(0, n, xh);
+  A->extract_invdiagelements(0, n, invd);
+  const bool damped = mode == 1 || mode == 3;
+  int iter = 0;
+  auto sweep = [&]() {
+    ++iter;
+    A->VectorMultNoDiag(*x, y);
+    y->ScaleAdd(static_cast< T >(-1.0), *b);
+    y->ElementWiseMult(*invd);
+    if (damped) {
+      x->Scale(static_cast< T >(1.0 - static_cast< T >(w)));
+      x->Axpy(*y, static_cast< T >(w));
+    } else {
+      x->CopyFrom(*y);
+    }
+  };
+  auto residual = [&]() -> double {
+    A->VectorMult(*x, r);
+    r->ScaleAdd(static_cast< T >(-1.0), *b);
+    return r->Norm2();
+  };
+  int state = CTRL_ITERATE;
+  double res = 0., first = 0.;
+  *res_init_out = 0.;
+  const auto t0 = std::chrono::steady_clock::now();
+  if (mode <= 1) {
+    res = residual();
+    *res_init_out = res;
+    state = control_check(iter, res, maxits, atol, rtol, dtol, &first);
+    while (state == CTRL_ITERATE) {
+      for (int i = 0; i < inner_iter; ++i) sweep();
+      res = residual();
+      state = control_check(iter, res, maxits, atol, rtol, dtol, &first);
+    }
+  } else {
+    const int outer = mode == 2 ? smooth_iter : maxits;
+    for (int k = 0; k < outer; ++k)
+      for (int i = 0; i < inner_iter; ++i) sweep();
+  }
+  if (seconds)
+    *seconds = std::chrono::duration< double >(
+                   std::chrono::steady_clock::now() - t0).count();
+  x->GetBlockValues(0, n, xh);
+  *iters = iter;
+  *res_out = res;
+  delete invd; delete r; delete y; delete x; delete b; delete A;
+  return state;
+}
+
+// BiCGSTAB<LAD>::SolveNoPrecond / SolvePrecondRight (linear_solver/
+// bicgstab.h:127-293, :297-473) on one rank with the block-Jacobi(Jacobi)
+// preconditioner: the same sequence of compiled lVector/lMatrix calls,
+// including the restart when |sigma| <= tol1 (r0 recomputed from the current
+// x, the iteration count carried on) and the short update when ||s|| is at
+// rounding level.  The coupled calls map to the interior ones as
+// r0.ScaleAdd(b, -1) -> r0.ScaleAdd(-1, b) and p.ScaleAdd(r, beta) ->
+// p.ScaleAdd(beta, r) (coupled_vector.cc:353-358).
+template < typename T >
+int bicgstab_solve(int impl, int nthreads, int precond, int n, int nnz,
+                   const int *rowptr, const int *col, const T *val,
+                   const T *bh, T *xh, int maxits, double atol, double rtol,
+                   double dtol, int *iters, int *restarts, double *res_out,
+                   double *res_init_out, double *seconds) {
+  CPU_CSR_lMatrix< T > *A = make_matrix< T >(impl, nthreads, n, nnz, rowptr,
+                                             col, val);
+  const char *names[] = {"b", "x", "r", "r0", "p", "Ap", "s", "t", "h", "h1"};
+  lVector< T > *v[10];
+  for (int i = 0; i < 10; ++i) v[i] = make_vector< T >(impl, n, names[i]);
+  lVector< T > &b = *v[0], &x = *v[1], &r = *v[2], &r0 = *v[3], &p = *v[4];
+  lVector< T > &Ap = *v[5], &s = *v[6], &t = *v[7], &h = *v[8], &h1 = *v[9];
+  b.SetBlockValues(0, n, bh);
+  x.SetBlockValues(0, n, xh);
+  lPreconditioner_Jacobi< T > jac;
+  if (precond) {
+    jac.Init();
+    jac.SetupOperator(*A);
+    jac.SetReuse(true);
+    jac.Build(&r, &h);
+  }
+  const T eps = precond ? static_cast< T >(5.e-16) : static_cast< T >(1.e-15);
+  T alpha, beta, ressquared, rho, rho_old, omega, sigma, tol1;
+  int iter = 0, nrestart = -1, conv = CTRL_ITERATE;
+  double res = 0., first = 0.;
+  bool restart = true;
+  const auto t0 = std::chrono::steady_clock::now();
+  while (restart) {
+    restart = false;
+    ++nrestart;
+    r.Zeros(); r0.Zeros(); p.Zeros(); Ap.Zeros(); s.Zeros(); t.Zeros();
+    h.Zeros(); h1.Zeros();
+    A->VectorMult(x, &r0);
+    r0.ScaleAdd(static_cast< T >(-1.), b);
+    r.CopyFrom(r0);
+    ressquared = r.Dot(r);
+    rho = rho_old = ressquared;
+    res = std::sqrt(ressquared);
+    *res_init_out = res;
+    conv = control_check(iter, res, maxits, atol, rtol, dtol, &first);
+    p.CopyFrom(r);
+    while (conv == CTRL_ITERATE && !restart) {
+      ++iter;
+      if (precond) {
+        h.Zeros();
+        jac.ApplylPreconditioner(p, &h);
+        A->VectorMult(h, &Ap);
+      } else {
+        A->VectorMult(p, &Ap);
+      }
+      sigma = Ap.Dot(r0);
+      tol1 = eps * Ap.Norm2() * r0.Norm2();
+      if (std::abs(sigma) > tol1) {
+        alpha = rho / sigma;
+        s.CopyFrom(r);
+        s.Axpy(Ap, -alpha);
+        if (s.Norm2() > eps) {
+          if (precond) {
+            h.Zeros();
+            jac.ApplylPreconditioner(s, &h);
+            A->VectorMult(h, &t);
+          } else {
+            A->VectorMult(s, &t);
+          }
+          omega = t.Dot(s) / t.Dot(t);
+          if (precond) {
+            h.Zeros();
+            h1.Zeros();
+            h1.Axpy(p, alpha);
+            h1.Axpy(s, omega);
+            jac.ApplylPreconditioner(h1, &h);
+            x.Axpy(h, static_cast< T >(1.));
+          } else {
+            x.Axpy(p, alpha);
+            x.Axpy(s, omega);
+          }
+          r.CopyFrom(s);
+          r.Axpy(t, -omega);
+          ressquared = r.Dot(r);
+          res = std::sqrt(ressquared);
+          conv = control_check(iter, res, maxits, atol, rtol, dtol, &first);
+          if (conv != CTRL_ITERATE) break;
+          rho = r.Dot(r0);
+          beta = (alpha * rho) / (omega * rho_old);
+          rho_old = rho;
+          p.ScaleAdd(beta, r);
+          p.Axpy(Ap, -omega * beta);
+        } else {
+          if (precond) {
+            h1.Zeros();
+            h1.Axpy(p, alpha);
+            h.Zeros();
+            jac.ApplylPreconditioner(h1, &h);
+            x.Axpy(h, static_cast< T >(1.));
+          } else {
+            x.Axpy(p, alpha);
+          }
+          r.CopyFrom(s);
+          ressquared = r.Dot(r);
+          res = std::sqrt(ressquared);
+          conv = control_check(iter, res, maxits, atol, rtol, dtol, &first);
+          if (conv != CTRL_ITERATE) break;
+        }
+      } else {
+        restart = true;
+      }
+    }
+  }
+  if (seconds)
+    *seconds = std::chrono::duration< double >(
+                   std::chrono::steady_clock::now() - t0).count();
+  x.GetBlockValues(0, n, xh);
+  *iters = iter;
+  *restarts = nrestart;
+  *res_out = res;
+  if (precond) jac.Clear();
+  for (int i = 9; i >= 0; --i) delete v[i];
+  delete A;
+  return conv;
+}
+
 struct RefSystem {
   int impl;
   int n;
@@ -276,6 +482,27 @@ int ref_cg_solve_f(int impl, int nthreads, int precond, int n, int nnz,
   return cg_solve< float >(impl, nthreads, precond, n, nnz, rowptr, col, val,
                            b, x, maxits, atol, rtol, dtol, iters, res,
                            res_init, res_rel);
+}
+
+int ref_jacobi_solve_d(int impl, int nthreads, int mode, int n, int nnz,
+                       const int *rowptr, const int *col, const double *val,
+                       const double *b, double *x, int maxits, int inner_iter,
+                       int smooth_iter, double w, double atol, double rtol,
+                       double dtol, int *iters, double *res,
+                       double *res_init, double *seconds) {
+  return jacobi_solve< double >(impl, nthreads, mode, n, nnz, rowptr, col, val,
+                                b, x, maxits, inner_iter, smooth_iter, w, atol,
+                                rtol, dtol, iters, res, res_init, seconds);
+}
+
+int ref_bicgstab_solve_d(int impl, int nthreads, int precond, int n, int nnz,
+                         const int *rowptr, const int *col, const double *val,
+                         const double *b, double *x, int maxits, double atol,
+                         double rtol, double dtol, int *iters, int *restarts,
+                         double *res, double *res_init, double *seconds) {
+  return bicgstab_solve< double >(impl, nthreads, precond, n, nnz, rowptr, col,
+                                  val, b, x, maxits, atol, rtol, dtol, iters,
+                                  restarts, res, res_init, seconds);
 }
 
 int ref_lmp_cg_d(int impl, int nthreads, int n, int nnz, const int *rowptr,

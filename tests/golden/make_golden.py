@@ -7,6 +7,8 @@ reference's own unit tests are recorded beside them, verbatim from:
   tests/cg_test.cc:92-94     x = (-0.25, -1.5, -0.75) for cg() on the 3x3 stencil
   tests/lmp_test.cc:80-82    A*(1,-2,0) = (4,-5,2) (7-nnz CSR)
   tests/cuda_test.cc:76-78   A*(1.2,-2.3,0.7) = (4.7,-6.5,3.7) (dense-stored 3x3)
+and the reference's Jacobi<LAD> and BiCGSTAB<LAD> (restated over the same
+compiled objects) on further systems, in reference_krylov_runs.json.
 
 Usage (from the repository root, where oracle/_ref exists):
     python tests/golden/make_golden.py
@@ -84,6 +86,50 @@ def main():
     with open(os.path.join(OUT, "reference_cg_runs.json"), "w") as f:
         json.dump({"generator": "tests/golden/make_golden.py", "cases": solves}, f)
     print("wrote", len(solves), "cases")
+    krylov_runs()
+
+
+# Jacobi<LAD> runs: (mode, w, inner_iter, smooth_iter, maxits)
+JACOBI_RUNS = ((0, 1.0, 1, 1, 20000), (1, 0.7, 3, 1, 20000), (2, 1.0, 2, 7, 20000), (3, 0.6, 2, 1, 5))
+
+
+def krylov_cases():
+    yield P.poisson_2d(16)
+    yield P.q1_system(2, 33, 11, 1.0, "varcoef2d_33_s1")
+    yield P.convdiff_2d(24, 20.0)
+    yield P.convdiff_2d(16, 200.0)
+    yield P.q1_system(3, 8, 12, 0.0, "poisson3d_8")
+    yield P.random_spd(33, 2, empty_rows=3)
+
+
+def krylov_runs():
+    """Jacobi<LAD> and BiCGSTAB<LAD> restated over the compiled lmp objects
+    (oracle/ref/ref_driver.cc) -> reference_krylov_runs.json."""
+    out = []
+    for s in krylov_cases():
+        entry = {"name": s.name, "n": s.n, "nnz": s.nnz, "sha_val": sha(s.val), "sha_b": sha(s.b),
+                 "jacobi": [], "bicgstab": []}
+        for mode, w, inner, smooth, maxits in JACOBI_RUNS:
+            r = oracle.ref_jacobi(s.rowptr, s.col, s.val, s.b, mode=mode, maxits=maxits, inner_iter=inner,
+                                  smooth_iter=smooth, w=w, atol=0.0, rtol=1e-6, dtol=1e8)
+            run = {"mode": mode, "w": w, "inner_iter": inner, "smooth_iter": smooth, "maxits": maxits,
+                   "rtol": 1e-6, "iters": r.iters, "state": r.state, "res": r.res,
+                   "res_init": r.res_init, "sha_x": sha(r.x)}
+            if s.n <= 300:
+                run["x"] = [float(v) for v in r.x]
+            entry["jacobi"].append(run)
+        for precond in (False, True):
+            r, restarts = oracle.ref_bicgstab(s.rowptr, s.col, s.val, s.b, maxits=5000, atol=0.0,
+                                              rtol=1e-10, dtol=1e8, precond=precond)
+            run = {"precond": precond, "rtol": 1e-10, "maxits": 5000, "iters": r.iters, "state": r.state,
+                   "restarts": restarts, "res": r.res, "res_init": r.res_init, "sha_x": sha(r.x)}
+            if s.n <= 300:
+                run["x"] = [float(v) for v in r.x]
+            entry["bicgstab"].append(run)
+        out.append(entry)
+    with open(os.path.join(OUT, "reference_krylov_runs.json"), "w") as f:
+        json.dump({"generator": "tests/golden/make_golden.py", "cases": out}, f)
+    print("wrote", len(out), "Jacobi/BiCGSTAB cases")
 
 
 if __name__ == "__main__":

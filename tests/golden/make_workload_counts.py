@@ -1,7 +1,8 @@
-"""Records the reference's iteration counts on the full-size standard
-workloads (tests/golden/workload_counts.json), by running HiFlow3's own lmp
-CPU classes (oracle/_ref, NAIVE implementation, bit-identical to the C
-restatement) to convergence here.  bench.py's CPU legs time a bounded sample
+"""Records the reference's iteration counts (CG<LAD>, and BiCGSTAB<LAD> on the
+poisson3d matrix) on the full-size standard workloads
+(tests/golden/workload_counts.json), by running HiFlow3's own lmp CPU classes
+(oracle/_ref, NAIVE implementation, bit-identical to the C restatement) to
+convergence here.  bench.py's CPU legs time a bounded sample
 of iterations and scale it by these counts.
 
 Usage (repository root, oracle/_ref built):  python tests/golden/make_workload_counts.py
@@ -38,6 +39,17 @@ def main():
                         "solve_seconds_1core": sec, "n": s.n, "nnz": s.nnz}
             print(key, out[key], f"{time.time() - t:.1f}s", flush=True)
             json.dump(out, open(OUT, "w"), indent=1)
+    # BiCGSTAB<LAD> with right Jacobi preconditioning on the poisson3d matrix
+    key = "poisson3d_128/bicgstab_jacobi/rtol1e-10"
+    if key not in out:
+        s = P.poisson_3d(128)
+        t = time.time()
+        r, restarts = oracle.ref_bicgstab(s.rowptr, s.col, s.val, s.b, maxits=20000, atol=0.0, rtol=1e-10,
+                                          dtol=1e8, precond=True)
+        out[key] = {"iters": r.iters, "restarts": restarts, "res": r.res, "res_init": r.res_init,
+                    "state": r.state, "solve_seconds_1core": r.seconds, "n": s.n, "nnz": s.nnz}
+        print(key, out[key], f"{time.time() - t:.1f}s", flush=True)
+        json.dump(out, open(OUT, "w"), indent=1)
 
 
 if __name__ == "__main__":

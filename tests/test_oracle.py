@@ -154,3 +154,89 @@ def test_generator_shapes():
     assert np.all(s.b[s.boundary] == 0.0)
     sizes = P.batch_sizes(1024)
     assert sizes.min() >= 16 and sizes.max() <= 256
+
+
+# ---- Jacobi<LAD> and BiCGSTAB<LAD> ----------------------------------------------
+
+def _krylov_cases():
+    with open(os.path.join(GOLD, "reference_krylov_runs.json")) as f:
+        return json.load(f)["cases"]
+
+
+def _krylov_system(name):
+    import re
+    m = re.match(r"convdiff2d_(\d+)_pe([0-9.]+)$", name)
+    if m:
+        return P.convdiff_2d(int(m.group(1)), float(m.group(2)))
+    return _system(name)
+
+
+@pytest.mark.parametrize("case", _krylov_cases(), ids=lambda c: c["name"])
+def test_jacobi_bicgstab_oracle_matches_reference_runs(case):
+    s = _krylov_system(case["name"])
+    assert s.n == case["n"] and s.nnz == case["nnz"]
+    assert _sha(s.val) == case["sha_val"] and _sha(s.b) == case["sha_b"]
+    for run in case["jacobi"]:
+        r = oracle.jacobi(s.rowptr, s.col, s.val, s.b, mode=run["mode"], maxits=run["maxits"],
+                          inner_iter=run["inner_iter"], smooth_iter=run["smooth_iter"], w=run["w"],
+                          atol=0.0, rtol=run["rtol"], dtol=1e8)
+        assert (r.iters, r.state) == (run["iters"], run["state"])
+        assert r.res == run["res"] and r.res_init == run["res_init"]
+        assert _sha(r.x) == run["sha_x"]          # bit-identical to the reference
+    for run in case["bicgstab"]:
+        r, restarts = oracle.bicgstab(s.rowptr, s.col, s.val, s.b, maxits=run["maxits"], atol=0.0,
+                                      rtol=run["rtol"], dtol=1e8, precond=run["precond"])
+        assert (r.iters, r.state, restarts) == (run["iters"], run["state"], run["restarts"])
+        assert r.res == run["res"]
+        assert _sha(r.x) == run["sha_x"]
+
+
+def test_jacobi_bicgstab_known_answer():
+    # the 3x3 system of tests/cg_test.cc:44-94 (x = (-0.25, -1.5, -0.75))
+    kat = json.load(open(os.path.join(GOLD, "reference_known_answers.json")))
+    s = P.known_answer_3x3()
+    for precond in (False, True):
+        r, _ = oracle.bicgstab(s.rowptr, s.col, s.val, s.b, maxits=100, atol=0.0, rtol=1e-15,
+                               precond=precond)
+        np.testing.assert_allclose(r.x, kat["cg_test_3x3"]["x"], rtol=0, atol=1e-12)
+    r = oracle.jacobi(s.rowptr, s.col, s.val, s.b, maxits=5000, atol=0.0, rtol=1e-15)
+    np.testing.assert_allclose(r.x, kat["cg_test_3x3"]["x"], rtol=0, atol=1e-12)
+
+
+def indefinite_2x2():
+    return (np.array([0, 1, 2], np.int32), np.array([0, 1], np.int32), np.array([1.0, -1.0]),
+            np.array([1.0, 1.0]))
+
+
+def test_bicgstab_restart_and_short_update():
+    rp, c, v, b = indefinite_2x2()
+    # no preconditioner: sigma = (A r0).r0 = 0 at every step, so each step
+    # restarts (bicgstab.h:282-284) until IterateControl stops at maxits
+    r, restarts = oracle.bicgstab(rp, c, v, b, maxits=5, atol=0.0, rtol=1e-12, precond=False)
+    assert (r.iters, r.state, restarts) == (5, oracle.CTRL_FAIL_MAXITS, 5)
+    # Jacobi: q = (1, -1), A q = (1, 1), alpha = 1, s = 0 -> the short update
+    # lands on the exact solution (1, -1)
+    r, restarts = oracle.bicgstab(rp, c, v, b, maxits=5, atol=0.0, rtol=1e-12, precond=True)
+    assert (r.iters, r.state, restarts) == (1, oracle.CTRL_SUCCESS_ABS, 0)
+    np.testing.assert_array_equal(r.x, [1.0, -1.0])
+    if oracle.ref_available():
+        for pc in (False, True):
+            a, ra = oracle.bicgstab(rp, c, v, b, maxits=5, atol=0.0, rtol=1e-12, precond=pc)
+            e, re_ = oracle.ref_bicgstab(rp, c, v, b, maxits=5, atol=0.0, rtol=1e-12, precond=pc)
+            assert (a.iters, a.state, ra) == (e.iters, e.state, re_) and np.array_equal(a.x, e.x)
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="oracle/_ref not built")
+def test_jacobi_bicgstab_match_compiled_reference_live():
+    s = P.convdiff_2d(20, 50.0)
+    for mode, w in ((0, 1.0), (1, 0.8), (2, 1.0), (3, 0.5)):
+        kw = dict(mode=mode, maxits=50 if mode == 3 else 4000, inner_iter=2, smooth_iter=3, w=w,
+                  atol=0.0, rtol=1e-7, dtol=1e8)
+        a = oracle.jacobi(s.rowptr, s.col, s.val, s.b, **kw)
+        e = oracle.ref_jacobi(s.rowptr, s.col, s.val, s.b, **kw)
+        assert (a.iters, a.state) == (e.iters, e.state) and np.array_equal(a.x, e.x)
+    for pc in (False, True):
+        a, ra = oracle.bicgstab(s.rowptr, s.col, s.val, s.b, maxits=500, atol=0.0, rtol=1e-11, precond=pc)
+        e, re_ = oracle.ref_bicgstab(s.rowptr, s.col, s.val, s.b, maxits=500, atol=0.0, rtol=1e-11,
+                                     precond=pc)
+        assert (a.iters, ra) == (e.iters, re_) and np.array_equal(a.x, e.x)
