@@ -16,7 +16,7 @@ F64, F32 = 0, 1
 FMT_CSR, FMT_SELL, FMT_SELL16 = 1, 4, 5
 FORMAT_NAMES = {FMT_CSR: "csr", FMT_SELL: "sell", FMT_SELL16: "sell16"}
 ITERATE, SUCCESS_ABS, SUCCESS_REL, FAIL_DIV, FAIL_MAXITS, FAIL_BREAKDOWN, DONE_FIXED = range(7)
-METHOD_JACOBI, METHOD_BICGSTAB = 1, 2
+METHOD_JACOBI, METHOD_BICGSTAB, METHOD_GMRES = 1, 2, 3
 SOLVER_SUCCESS, SOLVER_EXCEEDED, SOLVER_ERROR = range(3)
 STATUS_NAMES = {0: "OK", -1: "ERR_INVALID", -2: "ERR_CUDA", -3: "ERR_NOMEM", -4: "ERR_DTYPE",
                 -5: "ERR_MATRIX", -6: "ERR_TIMEOUT", -7: "ERR_UNSUPPORTED"}
@@ -77,7 +77,7 @@ class CgResult(C.Structure):
 class SolverParams(C.Structure):
     _fields_ = [("method", C.c_int), ("maxits", C.c_int), ("atol", C.c_double), ("rtol", C.c_double),
                 ("dtol", C.c_double), ("precond", C.c_int), ("mode", C.c_int), ("inner_iter", C.c_int),
-                ("smooth_iter", C.c_int), ("w", C.c_double)]
+                ("smooth_iter", C.c_int), ("w", C.c_double), ("size_basis", C.c_int)]
 
 
 class SolverResult(C.Structure):

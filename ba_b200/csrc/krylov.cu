@@ -34,9 +34,9 @@
 // direction is stored as q = P p, so A P p is one SpMV of q.
 #include <cmath>
 #include <cstring>
-#include <type_traits>
 
 #include "internal.cuh"
+#include "krylov.cuh"
 #include "spmv.cuh"
 
 namespace b200la {
@@ -65,46 +65,6 @@ __device__ __forceinline__ int it_check(int step, double value, const ItScalars 
   if (value > s.dtol * s.first) return B200LA_FAIL_DIV;
   if (step >= s.maxits) return B200LA_FAIL_MAXITS;
   return B200LA_ITERATE;
-}
-
-// Grid-stride loop over [0, n) in 16-byte vectors, then the ragged tail:
-// f(i0, C) handles elements i0 .. i0+C-1 (C = Vec16<T>::n or 1, a
-// std::integral_constant).  Work vectors start 256-byte aligned.
-template <typename T, typename F>
-__device__ __forceinline__ void for_each_chunk(int64_t n, F &&f) {
-  constexpr int W = Vec16<T>::n;
-  const int64_t nv = n / W;
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  for (int64_t i = tid; i < nv; i += stride) f(i * W, std::integral_constant<int, W>{});
-  for (int64_t i = nv * W + tid; i < n; i += stride) f(i, std::integral_constant<int, 1>{});
-}
-
-template <int C, typename T> __device__ __forceinline__ void ld(const T *p, T (&a)[C]) {
-  if constexpr (C == Vec16<T>::n) {
-    using V = typename Vec16<T>::type;
-    const V v = *reinterpret_cast<const V *>(p);
-    const T *s = reinterpret_cast<const T *>(&v);
-#pragma unroll
-    for (int k = 0; k < C; ++k) a[k] = s[k];
-  } else {
-#pragma unroll
-    for (int k = 0; k < C; ++k) a[k] = p[k];
-  }
-}
-
-template <int C, typename T> __device__ __forceinline__ void st(T *p, const T (&a)[C]) {
-  if constexpr (C == Vec16<T>::n) {
-    using V = typename Vec16<T>::type;
-    V v;
-    T *d = reinterpret_cast<T *>(&v);
-#pragma unroll
-    for (int k = 0; k < C; ++k) d[k] = a[k];
-    *reinterpret_cast<V *>(p) = v;
-  } else {
-#pragma unroll
-    for (int k = 0; k < C; ++k) p[k] = a[k];
-  }
 }
 
 // ---- Jacobi sweep ------------------------------------------------------------
@@ -403,6 +363,7 @@ struct b200la_solver_s {
   cudaGraphExec_t exec;
   int g_format, g_param;     // schedule baked into the graph
   int grid_spmv, grid_ew;
+  b200la::GmresState *gm;    // GMRES keeps its own state (gmres.cu)
 };
 
 namespace b200la {
@@ -610,6 +571,11 @@ extern "C" {
 
 int b200la_solver_destroy(b200la_solver s) {
   if (!s) return B200LA_OK;
+  if (s->gm) {
+    gmres_destroy(s->gm);
+    delete s;
+    return B200LA_OK;
+  }
   cudaStream_t st = s->A->ctx->stream;
   cudaStreamSynchronize(st);
   if (s->exec) cudaGraphExecDestroy(s->exec);
@@ -627,13 +593,31 @@ int b200la_solver_destroy(b200la_solver s) {
 int b200la_solver_create(b200la_mat A, const b200la_solver_params *prm, b200la_solver *out) {
   B_CHECK(A && prm && out, B200LA_ERR_INVALID, "solver_create: null argument");
   B_CHECK(A->nrow == A->ncol, B200LA_ERR_INVALID, "solver_create: matrix is %dx%d, not square", A->nrow, A->ncol);
-  B_CHECK(prm->method == B200LA_METHOD_JACOBI || prm->method == B200LA_METHOD_BICGSTAB, B200LA_ERR_INVALID,
-          "solver_create: unknown method %d", prm->method);
+  B_CHECK(prm->method == B200LA_METHOD_JACOBI || prm->method == B200LA_METHOD_BICGSTAB ||
+              prm->method == B200LA_METHOD_GMRES,
+          B200LA_ERR_INVALID, "solver_create: unknown method %d", prm->method);
   B_CHECK(prm->maxits >= 0 && prm->maxits <= 10000000, B200LA_ERR_INVALID, "solver_create: maxits %d not in [0, 1e7]",
           prm->maxits);
   B_CHECK(prm->atol >= 0.0 && prm->rtol >= 0.0 && prm->dtol > 0.0, B200LA_ERR_INVALID,
           "solver_create: tolerances must be atol >= 0, rtol >= 0, dtol > 0");
   b200la_solver_params p = *prm;
+  if (p.method == B200LA_METHOD_GMRES) {
+    p.mode = 0;
+    p.inner_iter = 1;
+    p.smooth_iter = 1;
+    p.w = 1.0;
+    b200la_solver s = new b200la_solver_s();
+    s->A = A;
+    s->prm = p;
+    s->n = A->nrow;
+    const int rc = gmres_create(A, &p, &s->gm);
+    if (rc != B200LA_OK) {
+      delete s;
+      return rc;
+    }
+    *out = s;
+    return B200LA_OK;
+  }
   if (p.method == B200LA_METHOD_JACOBI) {
     B_CHECK(p.mode >= 0 && p.mode <= 3, B200LA_ERR_INVALID, "solver_create: Jacobi mode %d not in 0..3", p.mode);
     B_CHECK(p.inner_iter >= 1 && p.smooth_iter >= 1, B200LA_ERR_INVALID,
@@ -689,6 +673,7 @@ int b200la_solver_solve(b200la_solver s, b200la_vec b, b200la_vec x, b200la_solv
   B_CHECK(b->n == s->n && x->n == s->n, B200LA_ERR_INVALID, "solver_solve: vector sizes %lld/%lld vs %lld",
           (long long)b->n, (long long)x->n, (long long)s->n);
   B_CHECK(b->dtype == A->dtype && x->dtype == A->dtype, B200LA_ERR_DTYPE, "solver_solve: dtype mismatch");
+  if (s->gm) return gmres_solve(s->gm, b, x, res);
   memset(res, 0, sizeof(*res));
   const bool jac = s->prm.method == B200LA_METHOD_JACOBI;
   const bool smooth = jac && s->prm.mode >= B200LA_JACOBI_SMOOTH_NORMAL;
@@ -733,6 +718,7 @@ int b200la_solver_profile(b200la_solver s, b200la_vec b, b200la_vec x, int passe
   B_CHECK(s && b && x && ms && passes >= 0, B200LA_ERR_INVALID, "solver_profile: bad argument");
   B_CHECK(b->n == s->n && x->n == s->n && s->n > 0, B200LA_ERR_INVALID, "solver_profile: sizes");
   B_CHECK(b->dtype == s->A->dtype && x->dtype == s->A->dtype, B200LA_ERR_DTYPE, "solver_profile: dtype");
+  if (s->gm) return gmres_profile(s->gm, b, x, passes, ms);
   const bool pre = solver_pre(s);
   if (s->A->dtype == B200LA_F64)
     return pre ? solver_profile_t<double, true>(s, b->d, x->d, passes, ms)

@@ -1,0 +1,96 @@
+// Helpers shared by the device solvers of krylov.cu and gmres.cu.
+#pragma once
+
+#include <type_traits>
+
+#include "internal.cuh"
+
+namespace b200la {
+
+// Grid-stride loop over [0, n) in 16-byte vectors, then the ragged tail:
+// f(i0, C) handles elements i0 .. i0+C-1 (C = Vec16<T>::n or 1, a
+// std::integral_constant).  Work vectors start 256-byte aligned.
+template <typename T, typename F>
+__device__ __forceinline__ void for_each_chunk(int64_t n, F &&f) {
+  constexpr int W = Vec16<T>::n;
+  const int64_t nv = n / W;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (int64_t i = tid; i < nv; i += stride) f(i * W, std::integral_constant<int, W>{});
+  for (int64_t i = nv * W + tid; i < n; i += stride) f(i, std::integral_constant<int, 1>{});
+}
+
+template <int C, typename T> __device__ __forceinline__ void ld(const T *p, T (&a)[C]) {
+  if constexpr (C == Vec16<T>::n) {
+    using V = typename Vec16<T>::type;
+    const V v = *reinterpret_cast<const V *>(p);
+    const T *s = reinterpret_cast<const T *>(&v);
+#pragma unroll
+    for (int k = 0; k < C; ++k) a[k] = s[k];
+  } else {
+#pragma unroll
+    for (int k = 0; k < C; ++k) a[k] = p[k];
+  }
+}
+
+template <int C, typename T> __device__ __forceinline__ void st(T *p, const T (&a)[C]) {
+  if constexpr (C == Vec16<T>::n) {
+    using V = typename Vec16<T>::type;
+    V v;
+    T *d = reinterpret_cast<T *>(&v);
+#pragma unroll
+    for (int k = 0; k < C; ++k) d[k] = a[k];
+    *reinterpret_cast<V *>(p) = v;
+  } else {
+#pragma unroll
+    for (int k = 0; k < C; ++k) p[k] = a[k];
+  }
+}
+
+// Grid-wide barrier for kernels launched cooperatively (all blocks resident).
+// Sense by generation: a block's thread 0 reads the generation, arrives on
+// the counter, and the last to arrive resets the counter and advances the
+// generation; the others wait for the generation to move.  Every wait is
+// bounded: after kSpinLimit polls (about 0.3 s) the waiter sets *err and the
+// call returns false in every thread of the block; a waiter also gives up at
+// once when another block has set *err.  Callers end the kernel when it
+// returns false.  Must be called by every thread of every block.
+constexpr long long kSpinLimit = 1LL << 22;
+
+__device__ __forceinline__ bool grid_barrier(unsigned *arrive, unsigned *gen, unsigned *err) {
+  __shared__ bool ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    bool good = true;
+    const unsigned g = atomicAdd(gen, 0u);
+    __threadfence();
+    if (atomicAdd(arrive, 1u) == gridDim.x - 1) {
+      atomicExch(arrive, 0u);
+      __threadfence();
+      atomicAdd(gen, 1u);
+    } else {
+      long long spins = 0;
+      while (atomicAdd(gen, 0u) == g) {
+        if (++spins > kSpinLimit || atomicAdd(err, 0u) != 0u) {
+          atomicExch(err, 1u);
+          good = false;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    ok = good;
+  }
+  __syncthreads();
+  return ok;
+}
+
+// Restarted GMRES (gmres.cu), behind the b200la_solver_* entry points.
+struct GmresState;
+int gmres_create(b200la_mat A, const b200la_solver_params *prm, GmresState **out);
+int gmres_solve(GmresState *s, b200la_vec b, b200la_vec x, b200la_solver_result *res);
+int gmres_profile(GmresState *s, b200la_vec b, b200la_vec x, int passes, double *ms);
+void gmres_destroy(GmresState *s);
+
+}  // namespace b200la

@@ -538,7 +538,7 @@ class Jacobi(_DeviceSolver):
     def _params(self):
         c = self.control
         return _lib.SolverParams(_lib.METHOD_JACOBI, c.maxits, c.atol, c.rtol, c.dtol, 1, self.solve_mode,
-                                 self.inner_iter, self.smooth_iter, self.w)
+                                 self.inner_iter, self.smooth_iter, self.w, 0)
 
     def Solve(self, b: B200_lVector, x: B200_lVector) -> int:
         r = self._solve(b, x)
@@ -582,7 +582,7 @@ class BiCGSTAB(_DeviceSolver):
             raise B200LAError(-7, "BiCGSTAB: only the Jacobi preconditioner runs on this path")
         c = self.control
         return _lib.SolverParams(_lib.METHOD_BICGSTAB, c.maxits, c.atol, c.rtol, c.dtol, 1 if use_pc else 0,
-                                 0, 1, 1, 1.0)
+                                 0, 1, 1, 1.0, 0)
 
     def Solve(self, b: B200_lVector, x: B200_lVector) -> int:
         if self.method == "LeftPreconditioning":
@@ -593,6 +593,55 @@ class BiCGSTAB(_DeviceSolver):
 
     def restarts(self) -> int:
         return self.restarts_
+
+
+class GMRES(_DeviceSolver):
+    """GMRES<LAD, PreLAD> (linear_solver/gmres.h:46-746): InitParameter(size_basis,
+    "NoPreconditioning" | "RightPreconditioning" | "LeftPreconditioning"),
+    SetupPreconditioner (switches to right preconditioning), InitControl,
+    Solve.  Restarted after size_basis steps (default 100, gmres.h:145), modified
+    Gram-Schmidt; left preconditioning with a preconditioner set returns
+    kSolverError as in the reference (gmres.h:394-404), and without one the
+    solve is unpreconditioned (gmres.h:213-219)."""
+
+    _name = "GMRES"
+
+    def __init__(self):
+        super().__init__()
+        self.size_basis_ = 100
+        self.method = "NoPreconditioning"
+        self.precond = None
+
+    def InitParameter(self, size_basis: int, method: str):
+        if method not in ("NoPreconditioning", "RightPreconditioning", "LeftPreconditioning"):
+            raise B200LAError(-1, f"GMRES: unknown method {method!r}")
+        self.size_basis_, self.method = int(size_basis), method
+        self._release()
+
+    def size_basis(self) -> int:
+        return self.size_basis_
+
+    def SetupPreconditioner(self, precond: PreconditionerBlockJacobiStand):
+        self.precond = precond
+        self.method = "RightPreconditioning"
+        self._release()
+
+    def _params(self):
+        # SolveImpl (gmres.h:194-221): right preconditioning only with a
+        # preconditioner set, otherwise SolveNoPrecond
+        use_pc = self.method == "RightPreconditioning" and self.precond is not None
+        if use_pc and self.precond.kind != "Jacobi":
+            raise B200LAError(-7, "GMRES: only the Jacobi preconditioner runs on this path")
+        c = self.control
+        return _lib.SolverParams(_lib.METHOD_GMRES, c.maxits, c.atol, c.rtol, c.dtol, 1 if use_pc else 0,
+                                 0, 1, 1, 1.0, self.size_basis_)
+
+    def Solve(self, b: B200_lVector, x: B200_lVector) -> int:
+        if self.size_basis_ <= 0 or (self.method == "LeftPreconditioning" and self.precond is not None):
+            return kSolverError
+        r = self._solve(b, x)
+        self.iter_ = r.iters
+        return r.solver_state
 
 
 class MPIR:

@@ -4,11 +4,12 @@ launches (no CUDA graph), so a profiler sees every launch on its own.
     python -m ba_b200.profile_case [--cells 128] [--dim 3] [--dtype f64|f32]
                                    [--spmv-reps 3] [--cg-iters 3] [--schedule tune|csr/8|sell/1]
 
-With --solver jacobi|bicgstab: after the SpMV launches, runs `--cg-iters`
-passes of that solver's kernels as plain launches (b200la_solver_profile:
-one jacobi_sweep_kernel per pass; bicg_spmv_q, bicg_s, bicg_spmv_s,
-bicg_update, bicg_direction per pass, the first pass a restart) instead of
-the CG kernels.
+With --solver jacobi|bicgstab|gmres: after the SpMV launches, runs
+`--cg-iters` passes of that solver's kernels as plain launches
+(b200la_solver_profile: one jacobi_sweep_kernel per pass; bicg_spmv_q,
+bicg_s, bicg_spmv_s, bicg_update, bicg_direction per pass, the first pass a
+restart; gm_update, gm_restart, gm_spmv, gm_arnoldi per pass, the first
+pass's gm_restart building V0) instead of the CG kernels.
 
 With --batch N: builds the standard batch of N 2D systems and solves it
 twice (the launches of interest are those of the second solve; set
@@ -43,7 +44,8 @@ def main():
     ap.add_argument("--cg-iters", type=int, default=3)
     ap.add_argument("--schedule", default="tune")
     ap.add_argument("--sigma", type=float, default=0.0)
-    ap.add_argument("--solver", default="cg", choices=["cg", "jacobi", "bicgstab"])
+    ap.add_argument("--solver", default="cg", choices=["cg", "jacobi", "bicgstab", "gmres"])
+    ap.add_argument("--basis", type=int, default=100, help="gmres: Krylov basis size")
     ap.add_argument("--batch", type=int, default=0,
                     help="instead: solve a batch of this many 2D systems (n~logU[16,256], sigma 1) twice")
     ap.add_argument("--chunk", type=int, default=64)
@@ -101,7 +103,7 @@ def solver_case(a, s, A, dt, fmt, prm, us, alg, sv):
         sol.SetSolveMode(2)
         sol.SetNumIter(max(a.cg_iters, 1))
         names, extra = ["sweep"], [2 * s.n * sv]
-    else:
+    elif a.solver == "bicgstab":
         sol = lmp.BiCGSTAB()
         pc = lmp.PreconditionerBlockJacobiStand()
         pc.Init_Jacobi()
@@ -109,6 +111,14 @@ def solver_case(a, s, A, dt, fmt, prm, us, alg, sv):
         names = ["spmv_q (A q, q.r0-type sums)", "s update", "spmv_s (A s, t.s, t.t)", "x/r update",
                  "direction"]
         extra = [s.n * sv, 5 * s.n * sv, s.n * sv, 8 * s.n * sv, 5 * s.n * sv]
+    else:
+        sol = lmp.GMRES()
+        sol.InitParameter(a.basis, "RightPreconditioning")
+        pc = lmp.PreconditionerBlockJacobiStand()
+        pc.Init_Jacobi()
+        sol.SetupPreconditioner(pc)
+        names = ["cycle update", "restart", "spmv (A P v_j, w.V0)", "arnoldi step"]
+        extra = [0, 0, s.n * sv, 0]
     sol.InitControl(100000, 0.0, 1e-12, 1e8)
     sol.SetupOperator(A)
     b = lmp.B200_lVector.from_numpy(s.b.astype(dt), platform=plat, dtype=dt)
@@ -117,6 +127,9 @@ def solver_case(a, s, A, dt, fmt, prm, us, alg, sv):
     print(f"system n={s.n} nnz={s.nnz} dtype={a.dtype} schedule={FORMAT_NAMES[fmt]}/{prm} tuned_us={us:.1f}")
     for k, name in enumerate(names):
         nbytes = extra[k] + (alg if name.startswith(("sweep", "spmv")) else 0)
+        if not nbytes:
+            print(f"{a.solver} {name}: {ms[k]:.4f} ms")
+            continue
         print(f"{a.solver} {name}: {ms[k]:.4f} ms, algorithmic {nbytes} bytes -> {nbytes / ms[k] / 1e6:.1f} GB/s")
 
 

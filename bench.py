@@ -2,7 +2,7 @@
 """Benchmark of the PCG hot path on B200: one JSON line on rank 0.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload batch|poisson3d|varcoef3d|serve|bicgstab|jacobi]
+                    [--workload batch|poisson3d|varcoef3d|serve|bicgstab|jacobi|gmres]
 
 Workload "batch" (default): 1,024 independent 2D Q1 diffusion systems, n x n
 cells with n log-uniform in [16, 256] from the seed, lognormal per-cell
@@ -19,9 +19,10 @@ Workload "poisson3d": FP64 Jacobi-PCG on 3D Q1 Poisson, 128^3 cells
 Workload "varcoef3d": the same shape with a lognormal coefficient (sigma 2),
 FP32 PCG inside FP64 refinement to 1e-10.  Workload "serve": a seeded
 Poisson-arrival request stream through the request loop (p50/p99).
-Workloads "bicgstab" and "jacobi": the poisson3d matrix solved by FP64
-BiCGSTAB with right Jacobi preconditioning to 1e-10 (solves/s), and swept by
-the Jacobi smoother (100 sweeps per step, sweeps/s).
+Workloads "bicgstab", "gmres" and "jacobi": the poisson3d matrix solved by
+FP64 BiCGSTAB and by GMRES(100), both with right Jacobi preconditioning, to
+1e-10 (solves/s), and swept by the Jacobi smoother (100 sweeps per step,
+sweeps/s).
 
 Multi-GPU: every rank solves its own batch (seeded per rank): independent
 systems need no exchange, value = all ranks' solves / the slowest rank's time.
@@ -63,7 +64,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="batch",
-                    choices=["batch", "poisson3d", "varcoef3d", "serve", "bicgstab", "jacobi"])
+                    choices=["batch", "poisson3d", "varcoef3d", "serve", "bicgstab", "jacobi", "gmres"])
     ap.add_argument("--cells", type=int, default=128, help="poisson3d cells per axis")
     ap.add_argument("--count", type=int, default=BATCH_COUNT, help="batch: systems per step")
     ap.add_argument("--requests", type=int, default=64, help="serve: requests per timed step")
@@ -1129,6 +1130,102 @@ def run_jacobi(args, rank, local_rank, world, torch, dist, barrier):
             "cpu_baseline": cpu}))
 
 
+GMRES_METRIC = "GMRES(100) (right Jacobi) solves/s at 1e-10 rel. residual, FP64, 3D Q1 Poisson"
+GMRES_BASIS = 100
+
+
+def run_reference_gmres(args, rank):
+    import oracle
+    from ba_b200 import problems as P
+    if _ref_unavailable():
+        return
+    s = P.poisson_3d(args.cells)
+    counts = json.load(open(COUNTS)) if os.path.exists(COUNTS) else {}
+    full = counts.get(f"poisson3d_{args.cells}/gmres{GMRES_BASIS}_jacobi/rtol1e-10", {}).get("iters", GMRES_BASIS)
+    nthreads = os.cpu_count() or 1
+    per_iter = []
+    # one whole cycle per step: the Gram-Schmidt cost grows within a cycle
+    for step in range(max(1, args.warmup // 3) + args.steps):
+        r = oracle.ref_gmres(s.rowptr, s.col, s.val, s.b, size_basis=GMRES_BASIS, maxits=GMRES_BASIS, atol=0.0,
+                             rtol=1e-10, dtol=1e8, precond=True, impl=oracle.IMPL_OPENMP, nthreads=nthreads)
+        if step >= max(1, args.warmup // 3):
+            per_iter.append(r.seconds / max(r.iters, 1))
+    value = 1.0 / (statistics.median(per_iter) * full)
+    print(json.dumps({
+        "impl": "reference", "metric": GMRES_METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"fp64 gmres({GMRES_BASIS}) + right jacobi, 3d q1 poisson {args.cells}^3 cells, "
+                               f"rel 1e-10", "n": s.n, "nnz": s.nnz, "parallelism": f"cpu openmp x{nthreads}"},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": nthreads, "kind": "reference",
+                         "sample": f"the first {GMRES_BASIS}-step cycle of one solve per step (HiFlow3 lmp OPENMP "
+                                   f"classes, GMRES<LAD> restated over them), scaled to {full} steps"},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+
+
+def run_gmres(args, rank, local_rank, world, torch, dist, barrier):
+    from ba_b200 import lmp
+    from ba_b200._lib import FORMAT_NAMES
+    plat, stream, s, A, fmt, prm, b, x = _c2_setup(args, local_rank, torch)
+    n, nnz = s.n, s.nnz
+    solver = lmp.GMRES()
+    solver.InitParameter(GMRES_BASIS, "RightPreconditioning")
+    solver.InitControl(20000, 0.0, 1e-10, 1e8)
+    solver.SetupOperator(A)
+    pc = lmp.PreconditionerBlockJacobiStand()
+    pc.Init_Jacobi()
+    solver.SetupPreconditioner(pc)
+
+    def step():
+        x.Zeros()
+        assert solver.Solve(b, x) == lmp.kSolverSuccess
+    ms_max, clk = _timed(args, stream, torch, barrier, local_rank, step)
+    iters = solver.iter()
+    value = D.aggregate_rate(args.steps, world, ms_max)
+    e2e_value = D.aggregate_rate(args.steps, world, _timed_e2e(args, stream, torch, barrier, b, x, n, step))
+    # kernel times over the first cycle (the Arnoldi step grows with j)
+    x.Zeros()
+    ms = solver.profile(b, x, GMRES_BASIS)
+    bytes_spmv = spmv_bytes(n, nnz, 8) + n * 8
+    avg_j = (GMRES_BASIS - 1) / 2.0
+    bytes_arnoldi = int((avg_j + 1) * 4 * n * 8 + 3 * n * 8)
+    peak, peak_kind = measured_peak_gbs()
+    achieved = bytes_spmv / (ms[2] / 1e3) / 1e9
+    key = f"poisson3d_{args.cells}/f64/gmres_spmv"
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import oracle
+        if oracle.ref_available():
+            nthreads = os.cpu_count() or 1
+            r = oracle.ref_gmres(s.rowptr, s.col, s.val, s.b, size_basis=GMRES_BASIS, maxits=GMRES_BASIS, atol=0.0,
+                                 rtol=1e-10, dtol=1e8, precond=True, impl=oracle.IMPL_OPENMP, nthreads=nthreads)
+            cpu = {"value": 1.0 / (r.seconds / max(r.iters, 1) * iters), "unit": "solves/s", "cores": nthreads,
+                   "kind": "reference", "sample": f"the first {GMRES_BASIS}-step cycle (HiFlow3 lmp OPENMP classes, "
+                                                  f"{nthreads} threads), scaled to {iters} steps"}
+    if rank == 0:
+        print(json.dumps({
+            "metric": GMRES_METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"fp64 gmres({GMRES_BASIS}) + right jacobi, 3d q1 poisson {args.cells}^3 cells, "
+                                   f"rel 1e-10", "n": n, "nnz": nnz, "iters_per_solve": iters,
+                       "parallelism": f"replicas x{world}", "spmv_schedule": FORMAT_NAMES[fmt] + f"/{prm}",
+                       "l2": "inputs larger than L2 (matrix 685 MB streamed per step, basis 1.7 GB)"},
+            "clocks": clk,
+            "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": n * 8, "d2h_bytes_per_step": n * 8},
+            "gpu_launches": args.steps * (4 * iters + 5),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": profile_traffic(key), "peak_source": peak_kind,
+                         "kernel": "gm_spmv_kernel (w = A P v_j fused with w.V0)", "algorithmic_bytes": bytes_spmv,
+                         "kernel_ms": dict(zip(("cycle_update", "restart", "spmv", "arnoldi"), ms)),
+                         "arnoldi": {"algorithmic_bytes_mean": bytes_arnoldi,
+                                     "gbs": bytes_arnoldi / (ms[3] / 1e3) / 1e9,
+                                     "note": "mean over the first cycle: (j+1) passes of w, V_i read and w "
+                                             "written, V_{j+1} and z written"},
+                         **dram_rate(profile_traffic(key), ms[2], peak)},
+            "cpu_baseline": cpu}))
+
+
 def main():
     args = parse()
     rank, local_rank, world = dist_env()
@@ -1136,7 +1233,8 @@ def main():
         if rank == 0:
             {"batch": run_reference_batch, "poisson3d": run_reference_poisson3d,
              "varcoef3d": run_reference_varcoef3d, "serve": run_reference_serve,
-             "bicgstab": run_reference_bicgstab, "jacobi": run_reference_jacobi}[args.workload](args, rank)
+             "bicgstab": run_reference_bicgstab, "jacobi": run_reference_jacobi,
+             "gmres": run_reference_gmres}[args.workload](args, rank)
         return
     import datetime
 
@@ -1155,7 +1253,7 @@ def main():
 
     load()
     fn = {"batch": run_batch, "poisson3d": run_poisson3d, "varcoef3d": run_varcoef3d,
-          "serve": run_serve, "bicgstab": run_bicgstab, "jacobi": run_jacobi}[args.workload]
+          "serve": run_serve, "bicgstab": run_bicgstab, "jacobi": run_jacobi, "gmres": run_gmres}[args.workload]
     fn(args, rank, local_rank, world, torch, dist, barrier)
     if world > 1:
         dist.barrier()

@@ -212,9 +212,19 @@ int b200la_pcg_solve(b200la_mat A, b200la_vec b, b200la_vec x, const b200la_cg_p
  * direction update; restarts when |sigma| <= eps ||Ap|| ||r0|| and the short
  * update when ||s|| <= eps follow the reference (eps 1e-15, or 5e-16 with
  * right preconditioning).  With right Jacobi preconditioning the direction is
- * kept as q = inv_D p, so A (P p) is one SpMV of q. */
+ * kept as q = inv_D p, so A (P p) is one SpMV of q.
+ *
+ * GMRES<LAD, PreLAD> (linear_solver/gmres.h:143-746), restarted after
+ * size_basis steps, modified Gram-Schmidt, no or right (Jacobi)
+ * preconditioning: per step one SpMV (fused with w.V_0) and one cooperative
+ * kernel that runs the whole Gram-Schmidt sweep with grid barriers (every
+ * wait bounded: a wait that runs out ends the solve with B200LA_ERR_TIMEOUT),
+ * normalises the new basis vector and applies the Givens rotations and the
+ * test; at a cycle end one pass applies x += P V y.  The basis takes
+ * (size_basis + 1) vectors of device memory. */
 #define B200LA_METHOD_JACOBI 1
 #define B200LA_METHOD_BICGSTAB 2
+#define B200LA_METHOD_GMRES 3
 #define B200LA_JACOBI_SOLVE_NORMAL 0
 #define B200LA_JACOBI_SOLVE_DAMPED 1
 #define B200LA_JACOBI_SMOOTH_NORMAL 2
@@ -230,6 +240,7 @@ typedef struct {
   int inner_iter;   /* Jacobi SetInnerIter (>= 1) */
   int smooth_iter;  /* Jacobi SetNumIter (>= 1) */
   double w;         /* Jacobi SetDampingParameter (> 0; 1 in the normal modes) */
+  int size_basis;   /* GMRES InitParameter(size_basis, ...): Krylov basis before a restart, 1..512 */
 } b200la_solver_params;
 
 typedef struct {
@@ -252,7 +263,8 @@ int b200la_solver_solve(b200la_solver s, b200la_vec b, b200la_vec x, b200la_solv
  * iteration as separate launches with CUDA events between the kernels and
  * writes the mean milliseconds per launch of each kernel of a pass:
  * Jacobi ms[0] = sweep; BiCGSTAB ms[0..4] = A q, s update, A s, x/r update,
- * direction.  x is not modified. */
+ * direction; GMRES ms[0..3] = cycle update, restart, SpMV, Arnoldi step.
+ * x is not modified. */
 int b200la_solver_profile(b200la_solver s, b200la_vec b, b200la_vec x, int passes, double *ms);
 
 /* ---- Q1 system assembly on the device (no reference counterpart: the

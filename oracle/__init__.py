@@ -7,11 +7,11 @@ The product library ba_b200 never imports it.
 Two checkers:
 * ``liboracle.so``: the C restatement in pcg_oracle.c (CG<LAD>, lmp cg(),
   IterateControl, CSR SpMV, BLAS-1, Jacobi, MPIR-style refinement, the
-  stationary Jacobi<LAD> solver and BiCGSTAB<LAD>);
+  stationary Jacobi<LAD> solver, BiCGSTAB<LAD> and GMRES<LAD>);
 * ``_ref/libhiflow_lmp_ref.so``: HiFlow3's own lmp CPU sources (NAIVE and
   OPENMP implementations, lPreconditioner_Jacobi, lmp cg()) compiled by
-  oracle/ref/Makefile, with a driver restating CG<LAD>, Jacobi<LAD> and
-  BiCGSTAB<LAD> over those objects.
+  oracle/ref/Makefile, with a driver restating CG<LAD>, Jacobi<LAD>,
+  BiCGSTAB<LAD> and GMRES<LAD> over those objects.
 """
 from .oracle import (  # noqa: F401
     CTRL_FAIL_DIV,
@@ -30,6 +30,7 @@ from .oracle import (  # noqa: F401
     bicgstab,
     cg,
     dot,
+    gmres,
     invdiag,
     iterate_check,
     jacobi,
@@ -38,6 +39,7 @@ from .oracle import (  # noqa: F401
     ref_available,
     ref_bicgstab,
     ref_cg,
+    ref_gmres,
     ref_jacobi,
     ref_lmp_cg,
     ref_spmv,

@@ -51,6 +51,9 @@ def _load():
             getattr(lib, f"orc_bicgstab_{s}").argtypes = [
                 C.c_int, _i32p, _i32p, fp, fp, fp, C.c_int, fp, C.c_int, C.c_double, C.c_double,
                 C.c_double, _ip, _ip, _dp, _dp]
+            getattr(lib, f"orc_gmres_{s}").argtypes = [
+                C.c_int, _i32p, _i32p, fp, fp, fp, C.c_int, fp, C.c_int, C.c_int, C.c_double,
+                C.c_double, C.c_double, _ip, _dp, _dp]
         lib.orc_iterate_check.argtypes = [C.c_int, C.c_double, C.c_int, C.c_double, C.c_double,
                                           C.c_double, _dp]
         lib.orc_mpir_d.argtypes = [C.c_int, _i32p, _i32p, _f64p, _f32p, _f64p, _f64p, C.c_int,
@@ -82,6 +85,9 @@ def _load_ref():
         lib.ref_bicgstab_solve_d.argtypes = [
             C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p, C.c_int,
             C.c_double, C.c_double, C.c_double, _ip, _ip, _dp, _dp, _dp]
+        lib.ref_gmres_solve_d.argtypes = [
+            C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p, C.c_int,
+            C.c_int, C.c_double, C.c_double, C.c_double, _ip, _dp, _dp, _dp]
         lib.ref_lmp_cg_d.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f64p, _f64p,
                                      _f64p, C.c_double, C.c_double, _ip]
         _ref = lib
@@ -240,6 +246,36 @@ def bicgstab(rowptr, col, val, b, x0=None, *, maxits=1000, atol=1e-12, rtol=1e-8
                                                int(bool(precond)), inv, int(maxits), atol, rtol, dtol,
                                                C.byref(it), C.byref(rs), C.byref(res), C.byref(res0))
     return OracleResult(x, it.value, res.value, res0.value, st), rs.value
+
+
+def gmres(rowptr, col, val, b, x0=None, *, size_basis=100, maxits=1000, atol=1e-12, rtol=1e-8, dtol=1e8,
+          precond=True, dtype=np.float64) -> OracleResult:
+    """GMRES<LAD> (restarted, modified Gram-Schmidt; no / right Jacobi
+    preconditioning) restated in C."""
+    s, T = _sfx(dtype)
+    rp, c, v = _csr(rowptr, col, val, T)
+    n = rp.shape[0] - 1
+    x = np.zeros(n, T) if x0 is None else np.array(x0, T)
+    inv = invdiag(rp, c, v, T) if precond else np.zeros(1, T)
+    it, res, res0 = C.c_int(), C.c_double(), C.c_double()
+    st = getattr(_load(), f"orc_gmres_{s}")(n, rp, c, v, np.ascontiguousarray(b, T), x, int(bool(precond)), inv,
+                                            int(size_basis), int(maxits), atol, rtol, dtol, C.byref(it),
+                                            C.byref(res), C.byref(res0))
+    return OracleResult(x, it.value, res.value, res0.value, st)
+
+
+def ref_gmres(rowptr, col, val, b, x0=None, *, size_basis=100, maxits=1000, atol=1e-12, rtol=1e-8, dtol=1e8,
+              precond=True, impl=IMPL_NAIVE, nthreads=1) -> OracleResult:
+    """GMRES<LAD> restated over the reference's compiled lmp objects (FP64)."""
+    rp, c, v = _csr(rowptr, col, val, np.float64)
+    n = rp.shape[0] - 1
+    x = np.zeros(n) if x0 is None else np.array(x0, np.float64)
+    it, res, res0, sec = C.c_int(), C.c_double(), C.c_double(), C.c_double()
+    st = _load_ref().ref_gmres_solve_d(impl, nthreads, int(bool(precond)), n, c.shape[0], rp, c, v,
+                                       np.ascontiguousarray(b, np.float64), x, int(size_basis), int(maxits),
+                                       atol, rtol, dtol, C.byref(it), C.byref(res), C.byref(res0),
+                                       C.byref(sec))
+    return OracleResult(x, it.value, res.value, res0.value, st, sec.value)
 
 
 def ref_jacobi(rowptr, col, val, b, x0=None, *, mode=JACOBI_SOLVE_NORMAL, maxits=1000, inner_iter=1,

@@ -395,6 +395,127 @@ ORACLE_KRYLOV(double, d, sqrt, fabs)
 ORACLE_KRYLOV(float, f, sqrtf, fabsf)
 
 /*
+ * GMRES<LAD, PreLAD>::SolveNoPrecond / SolveRight (linear_solver/gmres.h:
+ * 229-389, 462-713) on one rank: restarted GMRES with modified Gram-Schmidt,
+ * Givens rotations (ApplyPlaneRotation / GeneratePlaneRotation, :97-115) and
+ * UpdateSolution (:727-746: back substitution, then x += V y; with right
+ * preconditioning z = V y, x += inv_D .* z).  The basis size is min(m,
+ * maxits).  After a restart V[0] = b - A x is scaled by 1 / res with res the
+ * recurrence residual |g[j+1]| (not the norm of the new V[0]), as the
+ * reference does.  Returns the IterateControl state, -3 if out of memory.
+ */
+#define ORACLE_GMRES(T, S, SQRT, FABS)                                            \
+  static void orc_gm_update_##S(int n, T **V, const T *H, int ld, const T *g,  \
+                                int k, T *y, T *x) {                           \
+    for (int i = 0; i <= k; ++i) y[i] = g[i];                                  \
+    for (int i = k + 1; (i--) != 0;) {                                         \
+      y[i] /= H[i * ld + i];                                                   \
+      const T temp = y[i];                                                     \
+      for (int j = 0; j < i; ++j) y[j] -= H[i * ld + j] * temp;                \
+    }                                                                          \
+    for (int j = 0; j <= k; ++j) orc_axpy_##S(n, x, V[j], y[j]);               \
+  }                                                                            \
+  static void orc_gm_rot_##S(T cs, T sn, T *dx, T *dy) {                       \
+    const T temp = cs * (*dx) + sn * (*dy);                                    \
+    *dy = -sn * (*dx) + cs * (*dy);                                            \
+    *dx = temp;                                                                \
+  }                                                                            \
+  int orc_gmres_##S(int n, const int *rowptr, const int *col, const T *val,    \
+                    const T *b, T *x, int precond, const T *invd,              \
+                    int size_basis, int maxits, double atol, double rtol,      \
+                    double dtol, int *iters, double *res_out,                  \
+                    double *res_init_out) {                                    \
+    const int m = size_basis < maxits ? size_basis : maxits;                   \
+    const int ld = m + 1;                                                      \
+    const size_t nn = (size_t)(n > 0 ? n : 1);                                 \
+    T *store = (T *)calloc(nn * (size_t)(m + 3), sizeof(T));                   \
+    T **V = (T **)calloc((size_t)(m + 1), sizeof(T *));                        \
+    T *H = (T *)calloc((size_t)(m > 0 ? m : 1) * (size_t)ld, sizeof(T));       \
+    T *gv = (T *)calloc((size_t)(4 * ld), sizeof(T));                          \
+    if (!store || !V || !H || !gv) {                                           \
+      free(store); free(V); free(H); free(gv);                                 \
+      return -3;                                                               \
+    }                                                                          \
+    for (int i = 0; i <= m; ++i) V[i] = store + (size_t)i * nn;                \
+    T *w = store + (size_t)(m + 1) * nn, *z = store + (size_t)(m + 2) * nn;    \
+    T *g = gv, *cs = gv + ld, *sn = gv + 2 * ld, *y = gv + 3 * ld;             \
+    int iter = 0, conv;                                                        \
+    double first = 0.;                                                         \
+    T res;                                                                     \
+    orc_spmv_##S(n, rowptr, col, val, x, V[0]);                                \
+    orc_scaleadd_##S(n, V[0], (T)-1., b);                                      \
+    res = SQRT(orc_dot_##S(n, V[0], V[0]));                                    \
+    *res_init_out = (double)res;                                               \
+    conv = orc_iterate_check(iter, (double)res, maxits, atol, rtol, dtol,      \
+                             &first);                                          \
+    while (conv == CTRL_ITERATE) {                                             \
+      for (int i = 0; i < ld; ++i) g[i] = 0;                                   \
+      memset(H, 0, sizeof(T) * (size_t)m * (size_t)ld);                        \
+      {                                                                        \
+        const T sc = (T)1. / res;                                              \
+        for (int q = 0; q < n; ++q) V[0][q] *= sc;                             \
+      }                                                                        \
+      g[0] = res;                                                              \
+      int j = 0;                                                               \
+      for (; j != m; ++j) {                                                    \
+        ++iter;                                                                \
+        if (precond) {                                                         \
+          memcpy(z, V[j], sizeof(T) * (size_t)n);                              \
+          orc_ewmult_##S(n, z, invd);                                          \
+          orc_spmv_##S(n, rowptr, col, val, z, w);                             \
+        } else {                                                               \
+          orc_spmv_##S(n, rowptr, col, val, V[j], w);                          \
+        }                                                                      \
+        for (int i = 0; i <= j; ++i) {                                         \
+          H[j * ld + i] = orc_dot_##S(n, w, V[i]);                             \
+          orc_axpy_##S(n, w, V[i], (T)-1. * H[j * ld + i]);                    \
+        }                                                                      \
+        H[j * ld + j + 1] = SQRT(orc_dot_##S(n, w, w));                        \
+        {                                                                      \
+          const T sc = (T)1. / H[j * ld + j + 1];                              \
+          for (int q = 0; q < n; ++q) w[q] *= sc;                              \
+        }                                                                      \
+        memcpy(V[j + 1], w, sizeof(T) * (size_t)n);                            \
+        for (int k = 0; k != j; ++k)                                           \
+          orc_gm_rot_##S(cs[k], sn[k], &H[j * ld + k], &H[j * ld + k + 1]);    \
+        {                                                                      \
+          const T dx = H[j * ld + j], dy = H[j * ld + j + 1];                  \
+          const T beta = SQRT(dx * dx + dy * dy);                              \
+          cs[j] = dx / beta;                                                   \
+          sn[j] = dy / beta;                                                   \
+        }                                                                      \
+        orc_gm_rot_##S(cs[j], sn[j], &H[j * ld + j], &H[j * ld + j + 1]);      \
+        orc_gm_rot_##S(cs[j], sn[j], &g[j], &g[j + 1]);                        \
+        res = FABS(g[j + 1]);                                                  \
+        conv = orc_iterate_check(iter, (double)res, maxits, atol, rtol, dtol,  \
+                                 &first);                                      \
+        if (conv != CTRL_ITERATE) break;                                       \
+      }                                                                        \
+      const int k = conv != CTRL_ITERATE ? j : m - 1;                          \
+      if (precond) {                                                           \
+        memset(z, 0, sizeof(T) * (size_t)n);                                   \
+        orc_gm_update_##S(n, V, H, ld, g, k, y, z);                            \
+        memcpy(w, z, sizeof(T) * (size_t)n);                                   \
+        orc_ewmult_##S(n, w, invd);                                            \
+        orc_axpy_##S(n, x, w, (T)1.);                                          \
+      } else {                                                                 \
+        orc_gm_update_##S(n, V, H, ld, g, k, y, x);                            \
+      }                                                                        \
+      if (conv == CTRL_ITERATE) {                                              \
+        orc_spmv_##S(n, rowptr, col, val, x, V[0]);                            \
+        orc_scaleadd_##S(n, V[0], (T)-1., b);                                  \
+      }                                                                        \
+    }                                                                          \
+    *iters = iter;                                                             \
+    *res_out = (double)res;                                                    \
+    free(store); free(V); free(H); free(gv);                                   \
+    return conv;                                                               \
+  }
+
+ORACLE_GMRES(double, d, sqrt, fabs)
+ORACLE_GMRES(float, f, sqrtf, fabsf)
+
+/*
  * Mixed-precision iterative refinement around a float inner CG, structured
  * like MPIR<LAD_high, LAD_low>::SolveImpl (linear_solver/mpir.cc:52-230)
  * without smoothers: double residual r = b - A x; loop { cast r to float;

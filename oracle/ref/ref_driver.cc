@@ -21,10 +21,13 @@
 //                        the diagonal block's VectorMult, so the restatement
 //                        issues exactly the arithmetic the reference does.
 //   * ref_lmp_cg_*    -> the reference's own lmp cg() (lmp/solvers/cg.cc:35).
-//   * ref_jacobi_solve_d, ref_bicgstab_solve_d -> single-rank restatements of
-//                        Jacobi<LAD> (linear_solver/jacobi.cc:145-356) and
-//                        BiCGSTAB<LAD> (linear_solver/bicgstab.h:127-473) over
-//                        the same compiled lmp calls.
+//   * ref_jacobi_solve_d, ref_bicgstab_solve_d, ref_gmres_solve_d ->
+//                        single-rank restatements of Jacobi<LAD>
+//                        (linear_solver/jacobi.cc:145-356), BiCGSTAB<LAD>
+//                        (linear_solver/bicgstab.h:127-473) and GMRES<LAD>
+//                        (linear_solver/gmres.h:229-746) over the same
+//                        compiled lmp calls.
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <vector>
@@ -416,6 +419,121 @@ int bicgstab_solve(int impl, int nthreads, int precond, int n, int nnz,
   return conv;
 }
 
+// GMRES<LAD, PreLAD>::SolveNoPrecond / SolveRight (linear_solver/gmres.h:
+// 229-389, 462-713) on one rank over the compiled lmp objects, with the
+// Givens helpers (:97-115) and UpdateSolution (:727-746).  H is the
+// reference's SeqDenseMatrix H(row j, column i) of m rows and m + 1 columns.
+template < typename T >
+int gmres_solve(int impl, int nthreads, int precond, int n, int nnz,
+                const int *rowptr, const int *col, const T *val, const T *bh,
+                T *xh, int size_basis, int maxits, double atol, double rtol,
+                double dtol, int *iters, double *res_out, double *res_init_out,
+                double *seconds) {
+  CPU_CSR_lMatrix< T > *A = make_matrix< T >(impl, nthreads, n, nnz, rowptr,
+                                             col, val);
+  const int m = std::min(size_basis, maxits);
+  std::vector< lVector< T > * > V(m + 1);
+  for (int i = 0; i <= m; ++i) V[i] = make_vector< T >(impl, n, "V");
+  lVector< T > *b = make_vector< T >(impl, n, "b");
+  lVector< T > *x = make_vector< T >(impl, n, "x");
+  lVector< T > *w = make_vector< T >(impl, n, "w");
+  lVector< T > *z = make_vector< T >(impl, n, "z");
+  b->SetBlockValues(0, n, bh);
+  x->SetBlockValues(0, n, xh);
+  lPreconditioner_Jacobi< T > jac;
+  if (precond) {
+    jac.Init();
+    jac.SetupOperator(*A);
+    jac.SetReuse(true);
+    jac.Build(w, z);
+  }
+  const int ld = m + 1;
+  std::vector< T > H((size_t)std::max(m, 1) * ld), g(ld), cs(ld), sn(ld);
+  auto rot = [](T c, T s_, T *dx, T *dy) {
+    const T temp = c * (*dx) + s_ * (*dy);
+    *dy = -s_ * (*dx) + c * (*dy);
+    *dx = temp;
+  };
+  auto update = [&](int k, lVector< T > *out) {
+    std::vector< T > y(g);
+    for (int i = k + 1; (i--) != 0;) {
+      y[i] /= H[i * ld + i];
+      const T temp = y[i];
+      for (int j = 0; j < i; ++j) y[j] -= H[i * ld + j] * temp;
+    }
+    for (int j = 0; j <= k; ++j) out->Axpy(*V[j], y[j]);
+  };
+  int iter = 0, conv;
+  double first = 0.;
+  const auto t0 = std::chrono::steady_clock::now();
+  A->VectorMult(*x, V[0]);
+  V[0]->ScaleAdd(static_cast< T >(-1.), *b);
+  T res = V[0]->Norm2();
+  *res_init_out = res;
+  conv = control_check(iter, res, maxits, atol, rtol, dtol, &first);
+  while (conv == CTRL_ITERATE) {
+    std::fill(g.begin(), g.end(), static_cast< T >(0.));
+    std::fill(H.begin(), H.end(), static_cast< T >(0.));
+    V[0]->Scale(static_cast< T >(1.) / res);
+    g[0] = res;
+    int j = 0;
+    for (; j != m; ++j) {
+      ++iter;
+      if (precond) {
+        z->Zeros();
+        jac.ApplylPreconditioner(*V[j], z);
+        A->VectorMult(*z, w);
+      } else {
+        A->VectorMult(*V[j], w);
+      }
+      for (int i = 0; i <= j; ++i) {
+        H[j * ld + i] = w->Dot(*V[i]);
+        w->Axpy(*V[i], static_cast< T >(-1.) * H[j * ld + i]);
+      }
+      H[j * ld + j + 1] = w->Norm2();
+      w->Scale(static_cast< T >(1.) / H[j * ld + j + 1]);
+      V[j + 1]->CopyFrom(*w);
+      for (int k = 0; k != j; ++k) rot(cs[k], sn[k], &H[j * ld + k], &H[j * ld + k + 1]);
+      {
+        const T dx = H[j * ld + j], dy = H[j * ld + j + 1];
+        const T beta = std::sqrt(dx * dx + dy * dy);
+        cs[j] = dx / beta;
+        sn[j] = dy / beta;
+      }
+      rot(cs[j], sn[j], &H[j * ld + j], &H[j * ld + j + 1]);
+      rot(cs[j], sn[j], &g[j], &g[j + 1]);
+      res = std::abs(g[j + 1]);
+      conv = control_check(iter, res, maxits, atol, rtol, dtol, &first);
+      if (conv != CTRL_ITERATE) break;
+    }
+    const int k = conv != CTRL_ITERATE ? j : m - 1;
+    if (precond) {
+      z->Zeros();
+      update(k, z);
+      w->Zeros();
+      jac.ApplylPreconditioner(*z, w);
+      x->Axpy(*w, static_cast< T >(1.));
+    } else {
+      update(k, x);
+    }
+    if (conv == CTRL_ITERATE) {
+      A->VectorMult(*x, V[0]);
+      V[0]->ScaleAdd(static_cast< T >(-1.), *b);
+    }
+  }
+  if (seconds)
+    *seconds = std::chrono::duration< double >(
+                   std::chrono::steady_clock::now() - t0).count();
+  x->GetBlockValues(0, n, xh);
+  *iters = iter;
+  *res_out = res;
+  if (precond) jac.Clear();
+  delete z; delete w; delete x; delete b;
+  for (int i = m; i >= 0; --i) delete V[i];
+  delete A;
+  return conv;
+}
+
 struct RefSystem {
   int impl;
   int n;
@@ -503,6 +621,16 @@ int ref_bicgstab_solve_d(int impl, int nthreads, int precond, int n, int nnz,
   return bicgstab_solve< double >(impl, nthreads, precond, n, nnz, rowptr, col,
                                   val, b, x, maxits, atol, rtol, dtol, iters,
                                   restarts, res, res_init, seconds);
+}
+
+int ref_gmres_solve_d(int impl, int nthreads, int precond, int n, int nnz,
+                      const int *rowptr, const int *col, const double *val,
+                      const double *b, double *x, int size_basis, int maxits,
+                      double atol, double rtol, double dtol, int *iters,
+                      double *res, double *res_init, double *seconds) {
+  return gmres_solve< double >(impl, nthreads, precond, n, nnz, rowptr, col,
+                               val, b, x, size_basis, maxits, atol, rtol, dtol,
+                               iters, res, res_init, seconds);
 }
 
 int ref_lmp_cg_d(int impl, int nthreads, int n, int nnz, const int *rowptr,

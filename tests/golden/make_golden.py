@@ -7,8 +7,8 @@ reference's own unit tests are recorded beside them, verbatim from:
   tests/cg_test.cc:92-94     x = (-0.25, -1.5, -0.75) for cg() on the 3x3 stencil
   tests/lmp_test.cc:80-82    A*(1,-2,0) = (4,-5,2) (7-nnz CSR)
   tests/cuda_test.cc:76-78   A*(1.2,-2.3,0.7) = (4.7,-6.5,3.7) (dense-stored 3x3)
-and the reference's Jacobi<LAD> and BiCGSTAB<LAD> (restated over the same
-compiled objects) on further systems, in reference_krylov_runs.json.
+and the reference's Jacobi<LAD>, BiCGSTAB<LAD> and GMRES<LAD> (restated over
+the same compiled objects) on further systems, in reference_krylov_runs.json.
 
 Usage (from the repository root, where oracle/_ref exists):
     python tests/golden/make_golden.py
@@ -89,6 +89,8 @@ def main():
     krylov_runs()
 
 
+# GMRES<LAD> restart lengths (basis sizes)
+GMRES_BASIS = (10, 30, 100)
 # Jacobi<LAD> runs: (mode, w, inner_iter, smooth_iter, maxits)
 JACOBI_RUNS = ((0, 1.0, 1, 1, 20000), (1, 0.7, 3, 1, 20000), (2, 1.0, 2, 7, 20000), (3, 0.6, 2, 1, 5))
 
@@ -103,8 +105,8 @@ def krylov_cases():
 
 
 def krylov_runs():
-    """Jacobi<LAD> and BiCGSTAB<LAD> restated over the compiled lmp objects
-    (oracle/ref/ref_driver.cc) -> reference_krylov_runs.json."""
+    """Jacobi<LAD>, BiCGSTAB<LAD> and GMRES<LAD> restated over the compiled lmp
+    objects (oracle/ref/ref_driver.cc) -> reference_krylov_runs.json."""
     out = []
     for s in krylov_cases():
         entry = {"name": s.name, "n": s.n, "nnz": s.nnz, "sha_val": sha(s.val), "sha_b": sha(s.b),
@@ -126,10 +128,20 @@ def krylov_runs():
             if s.n <= 300:
                 run["x"] = [float(v) for v in r.x]
             entry["bicgstab"].append(run)
+        entry["gmres"] = []
+        for precond in (False, True):
+            for m in GMRES_BASIS:
+                r = oracle.ref_gmres(s.rowptr, s.col, s.val, s.b, size_basis=m, maxits=3000, atol=0.0,
+                                     rtol=1e-10, dtol=1e8, precond=precond)
+                run = {"precond": precond, "size_basis": m, "rtol": 1e-10, "maxits": 3000, "iters": r.iters,
+                       "state": r.state, "res": r.res, "res_init": r.res_init, "sha_x": sha(r.x)}
+                if s.n <= 300:
+                    run["x"] = [float(v) for v in r.x]
+                entry["gmres"].append(run)
         out.append(entry)
     with open(os.path.join(OUT, "reference_krylov_runs.json"), "w") as f:
         json.dump({"generator": "tests/golden/make_golden.py", "cases": out}, f)
-    print("wrote", len(out), "Jacobi/BiCGSTAB cases")
+    print("wrote", len(out), "Jacobi/BiCGSTAB/GMRES cases")
 
 
 if __name__ == "__main__":

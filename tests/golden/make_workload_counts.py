@@ -1,5 +1,5 @@
-"""Records the reference's iteration counts (CG<LAD>, and BiCGSTAB<LAD> on the
-poisson3d matrix) on the full-size standard workloads
+"""Records the reference's iteration counts (CG<LAD>, and BiCGSTAB<LAD> and
+GMRES<LAD>(100) on the poisson3d matrix) on the full-size standard workloads
 (tests/golden/workload_counts.json), by running HiFlow3's own lmp CPU classes
 (oracle/_ref, NAIVE implementation, bit-identical to the C restatement) to
 convergence here.  bench.py's CPU legs time a bounded sample
@@ -48,6 +48,17 @@ def main():
                                           dtol=1e8, precond=True)
         out[key] = {"iters": r.iters, "restarts": restarts, "res": r.res, "res_init": r.res_init,
                     "state": r.state, "solve_seconds_1core": r.seconds, "n": s.n, "nnz": s.nnz}
+        print(key, out[key], f"{time.time() - t:.1f}s", flush=True)
+        json.dump(out, open(OUT, "w"), indent=1)
+    # GMRES<LAD>(100) with right Jacobi preconditioning on the poisson3d matrix
+    key = "poisson3d_128/gmres100_jacobi/rtol1e-10"
+    if key not in out:
+        s = P.poisson_3d(128)
+        t = time.time()
+        r = oracle.ref_gmres(s.rowptr, s.col, s.val, s.b, size_basis=100, maxits=20000, atol=0.0, rtol=1e-10,
+                             dtol=1e8, precond=True)
+        out[key] = {"iters": r.iters, "res": r.res, "res_init": r.res_init, "state": r.state,
+                    "solve_seconds_1core": r.seconds, "n": s.n, "nnz": s.nnz}
         print(key, out[key], f"{time.time() - t:.1f}s", flush=True)
         json.dump(out, open(OUT, "w"), indent=1)
 

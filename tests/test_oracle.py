@@ -156,7 +156,7 @@ def test_generator_shapes():
     assert sizes.min() >= 16 and sizes.max() <= 256
 
 
-# ---- Jacobi<LAD> and BiCGSTAB<LAD> ----------------------------------------------
+# ---- Jacobi<LAD>, BiCGSTAB<LAD> and GMRES<LAD> -----------------------------------
 
 def _krylov_cases():
     with open(os.path.join(GOLD, "reference_krylov_runs.json")) as f:
@@ -172,7 +172,7 @@ def _krylov_system(name):
 
 
 @pytest.mark.parametrize("case", _krylov_cases(), ids=lambda c: c["name"])
-def test_jacobi_bicgstab_oracle_matches_reference_runs(case):
+def test_jacobi_bicgstab_gmres_oracle_matches_reference_runs(case):
     s = _krylov_system(case["name"])
     assert s.n == case["n"] and s.nnz == case["nnz"]
     assert _sha(s.val) == case["sha_val"] and _sha(s.b) == case["sha_b"]
@@ -189,9 +189,15 @@ def test_jacobi_bicgstab_oracle_matches_reference_runs(case):
         assert (r.iters, r.state, restarts) == (run["iters"], run["state"], run["restarts"])
         assert r.res == run["res"]
         assert _sha(r.x) == run["sha_x"]
+    for run in case["gmres"]:
+        r = oracle.gmres(s.rowptr, s.col, s.val, s.b, size_basis=run["size_basis"], maxits=run["maxits"],
+                         atol=0.0, rtol=run["rtol"], dtol=1e8, precond=run["precond"])
+        assert (r.iters, r.state) == (run["iters"], run["state"])
+        assert r.res == run["res"] and r.res_init == run["res_init"]
+        assert _sha(r.x) == run["sha_x"]
 
 
-def test_jacobi_bicgstab_known_answer():
+def test_jacobi_bicgstab_gmres_known_answer():
     # the 3x3 system of tests/cg_test.cc:44-94 (x = (-0.25, -1.5, -0.75))
     kat = json.load(open(os.path.join(GOLD, "reference_known_answers.json")))
     s = P.known_answer_3x3()
@@ -201,6 +207,10 @@ def test_jacobi_bicgstab_known_answer():
         np.testing.assert_allclose(r.x, kat["cg_test_3x3"]["x"], rtol=0, atol=1e-12)
     r = oracle.jacobi(s.rowptr, s.col, s.val, s.b, maxits=5000, atol=0.0, rtol=1e-15)
     np.testing.assert_allclose(r.x, kat["cg_test_3x3"]["x"], rtol=0, atol=1e-12)
+    for precond in (False, True):
+        r = oracle.gmres(s.rowptr, s.col, s.val, s.b, size_basis=3, maxits=100, atol=0.0, rtol=1e-15,
+                         precond=precond)
+        np.testing.assert_allclose(r.x, kat["cg_test_3x3"]["x"], rtol=0, atol=1e-12)
 
 
 def indefinite_2x2():
@@ -227,7 +237,7 @@ def test_bicgstab_restart_and_short_update():
 
 
 @pytest.mark.skipif(not oracle.ref_available(), reason="oracle/_ref not built")
-def test_jacobi_bicgstab_match_compiled_reference_live():
+def test_jacobi_bicgstab_gmres_match_compiled_reference_live():
     s = P.convdiff_2d(20, 50.0)
     for mode, w in ((0, 1.0), (1, 0.8), (2, 1.0), (3, 0.5)):
         kw = dict(mode=mode, maxits=50 if mode == 3 else 4000, inner_iter=2, smooth_iter=3, w=w,
@@ -240,3 +250,10 @@ def test_jacobi_bicgstab_match_compiled_reference_live():
         e, re_ = oracle.ref_bicgstab(s.rowptr, s.col, s.val, s.b, maxits=500, atol=0.0, rtol=1e-11,
                                      precond=pc)
         assert (a.iters, ra) == (e.iters, re_) and np.array_equal(a.x, e.x)
+    for pc in (False, True):
+        for m in (7, 40):
+            a = oracle.gmres(s.rowptr, s.col, s.val, s.b, size_basis=m, maxits=800, atol=0.0, rtol=1e-11,
+                             precond=pc)
+            e = oracle.ref_gmres(s.rowptr, s.col, s.val, s.b, size_basis=m, maxits=800, atol=0.0, rtol=1e-11,
+                                 precond=pc)
+            assert (a.iters, a.state) == (e.iters, e.state) and np.array_equal(a.x, e.x)
