@@ -121,6 +121,8 @@ _SIGS = {
     "b200la_vec_elementwise_mult": [_vp, _vp],
     "b200la_dot_noalloc": [_vp, _vp, _i64, _i, _vp, _P(_d)],
     "b200la_csr_upload": [_vp, _i, _i, _i64, _vp, _vp, _vp, _i, _i, _P(_vp)],
+    "b200la_coo_upload": [_vp, _i, _i, _i64, _vp, _vp, _vp, _i, _i, _i, _P(_vp)],
+    "b200la_mat_download": [_vp, _vp, _vp, _vp],
     "b200la_mat_destroy": [_vp],
     "b200la_mat_info": [_vp, _P(_i), _P(_i), _P(_i64), _P(_i)],
     "b200la_mat_cast": [_vp, _i, _P(_vp)],

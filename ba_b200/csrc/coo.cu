@@ -1,0 +1,253 @@
+// COO -> CSR on the device: CPU_CSR_lMatrix::TransformFromCOO
+// (lmp/lmatrix_csr_cpu.cc:883-906), i.e. coo_2_csr (lmp/lmatrix_formats.h:
+// 320-452), for matrices assembled as coordinate triplets.
+//
+// The reference counts the entries of each row, scatters them in input order
+// and then sorts every row by column with a selection sort that keeps
+// duplicates (and, being a selection sort with swaps, does not keep them in
+// input order).  Here the same result comes from:
+//   1. a device check of every index (a bad triplet fails the upload),
+//   2. a stable radix sort of the triplets by row (input order kept within a
+//      row, as the reference's scatter keeps it),
+//   3. row offsets from the sorted rows (each row boundary writes its range),
+//   4. a gather of columns and values (cast to the storage type),
+//   5. the reference's selection sort, one thread per row (rows are short in
+//      FE matrices; the work per row is quadratic in its length),
+//   6. the diagonal positions and the longest row, as b200la_csr_upload does.
+// The result is the reference's CSR bit for bit, duplicates included.
+#include <cub/device/device_radix_sort.cuh>
+
+#include <climits>
+#include <cstring>
+
+#include "internal.cuh"
+
+namespace b200la {
+
+// First bad triplet (smallest index), or all ones when every index is in range.
+__global__ void coo_check_kernel(int64_t nnz, int nrow, int ncol, const int *__restrict__ rows,
+                                 const int *__restrict__ cols, unsigned long long *bad) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nnz; i += (int64_t)gridDim.x * blockDim.x) {
+    const int r = rows[i], c = cols[i];
+    if (r < 0 || r >= nrow || c < 0 || c >= ncol) atomicMin(bad, (unsigned long long)i);
+  }
+}
+
+__global__ void iota_kernel(int64_t n, int *out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = (int)i;
+}
+
+// rowptr from the rows sorted ascending: entry i starts rows prev+1 .. r.
+__global__ void coo_rowptr_kernel(int64_t nnz, int nrow, const int *__restrict__ srow, int *rowptr) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= nnz; i += (int64_t)gridDim.x * blockDim.x) {
+    const int prev = i == 0 ? -1 : srow[i - 1];
+    const int r = i == nnz ? nrow : srow[i];
+    for (int rr = prev + 1; rr <= r; ++rr) rowptr[rr] = (int)i;
+  }
+}
+
+template <typename T, typename S>
+__global__ void coo_gather_kernel(int64_t nnz, const int *__restrict__ perm, const int *__restrict__ cols,
+                                  const S *__restrict__ vals, int *col, T *val) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nnz; k += (int64_t)gridDim.x * blockDim.x) {
+    const int p = perm[k];
+    col[k] = cols[p];
+    val[k] = (T)vals[p];
+  }
+}
+
+// The reference's per-row selection sort (lmatrix_formats.h:405-431), one
+// thread per row; also the first diagonal entry and the longest row.
+template <typename T>
+__global__ void coo_rowsort_kernel(int nrow, const int *__restrict__ rowptr, int *col, T *val, int *diag,
+                                   int *max_row) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nrow; k += gridDim.x * blockDim.x) {
+    const int b = rowptr[k], e = rowptr[k + 1];
+    for (int i = b; i != e; ++i) {
+      int mi = i, mc = col[i];
+      for (int j = i + 1; j < e; ++j)
+        if (col[j] < mc) {
+          mi = j;
+          mc = col[j];
+        }
+      const int tc = col[i];
+      col[i] = col[mi];
+      col[mi] = tc;
+      const T tv = val[i];
+      val[i] = val[mi];
+      val[mi] = tv;
+    }
+    int d = -1;
+    for (int i = b; i != e; ++i)
+      if (col[i] == k) {
+        d = i;
+        break;
+      }
+    diag[k] = d;
+    atomicMax(max_row, e - b);
+  }
+}
+
+static int grid_1d(b200la_ctx c, int64_t work) {
+  int64_t g = (work + kBlock - 1) / kBlock;
+  const int64_t cap = (int64_t)c->num_sms * 16;
+  if (g > cap) g = cap;
+  return (int)(g < 1 ? 1 : g);
+}
+
+// Number of bits that hold values 0 .. n-1.
+static int bits_for(int n) {
+  int b = 1;
+  while (b < 31 && (1LL << b) < (long long)n) ++b;
+  return b;
+}
+
+}  // namespace b200la
+
+using namespace b200la;
+
+extern "C" int b200la_coo_upload(b200la_ctx c, int nrow, int ncol, int64_t nnz, const int *rows, const int *cols,
+                                 const void *val, int val_dtype, int dtype, int device_input, b200la_mat *out) {
+  B_CHECK(c && out, B200LA_ERR_INVALID, "coo_upload: null argument");
+  B_CHECK(nrow >= 0 && ncol >= 0, B200LA_ERR_INVALID, "coo_upload: negative size %d x %d", nrow, ncol);
+  B_CHECK(nnz >= 0 && nnz <= INT_MAX, B200LA_ERR_INVALID, "coo_upload: nnz %lld not in [0, 2^31)", (long long)nnz);
+  B_CHECK(dtype == B200LA_F64 || dtype == B200LA_F32, B200LA_ERR_DTYPE, "coo_upload: dtype %d", dtype);
+  B_CHECK(val_dtype == B200LA_F64 || val_dtype == B200LA_F32, B200LA_ERR_DTYPE, "coo_upload: value dtype %d",
+          val_dtype);
+  B_CHECK(nnz == 0 || (rows && cols && val), B200LA_ERR_INVALID, "coo_upload: null triplet arrays");
+  cudaStream_t s = c->stream;
+  const size_t nz = (size_t)(nnz > 0 ? nnz : 1);
+  const size_t vsz = dtype_size(val_dtype);
+  // scratch: device triplets (when given host arrays), sorted rows, permutation
+  int *d_rows = nullptr, *d_cols = nullptr, *srow = nullptr, *idx = nullptr, *perm = nullptr;
+  void *d_vals = nullptr, *cub_tmp = nullptr;
+  unsigned long long *bad = nullptr;
+  int *max_row_d = nullptr;
+  b200la_mat m = new b200la_mat_s();
+  m->ctx = c;
+  m->nrow = nrow;
+  m->ncol = ncol;
+  m->nnz = nnz;
+  m->dtype = dtype;
+  int rc = B200LA_OK;
+  auto cu = [&](cudaError_t e, const char *what) {
+    if (e != cudaSuccess && rc == B200LA_OK)
+      rc = fail(e == cudaErrorMemoryAllocation ? B200LA_ERR_NOMEM : B200LA_ERR_CUDA, "coo_upload: %s: %s", what,
+                cudaGetErrorString(e));
+    return rc == B200LA_OK;
+  };
+  do {
+    if (!cu(cudaMallocAsync(&m->rowptr, sizeof(int) * ((size_t)nrow + 1), s), "allocation") ||
+        !cu(cudaMallocAsync(&m->col, sizeof(int) * nz, s), "allocation") ||
+        !cu(cudaMallocAsync(&m->val, dtype_size(dtype) * nz, s), "allocation") ||
+        !cu(cudaMallocAsync(&m->diag, sizeof(int) * (size_t)(nrow > 0 ? nrow : 1), s), "allocation") ||
+        !cu(cudaMallocAsync(&bad, sizeof(unsigned long long) + sizeof(int), s), "allocation"))
+      break;
+    max_row_d = reinterpret_cast<int *>(bad + 1);
+    const unsigned long long none = ~0ull;
+    if (!cu(cudaMemcpyAsync(bad, &none, sizeof(none), cudaMemcpyHostToDevice, s), "copy") ||
+        !cu(cudaMemsetAsync(max_row_d, 0, sizeof(int), s), "memset"))
+      break;
+    if (nnz == 0) {
+      if (!cu(cudaMemsetAsync(m->rowptr, 0, sizeof(int) * ((size_t)nrow + 1), s), "memset")) break;
+      if (nrow > 0 && !cu(cudaMemsetAsync(m->diag, 0xff, sizeof(int) * (size_t)nrow, s), "memset")) break;
+      break;
+    }
+    const int *r_in = rows, *c_in = cols;
+    const void *v_in = val;
+    if (!device_input) {
+      if (!cu(cudaMallocAsync(&d_rows, sizeof(int) * nz, s), "allocation") ||
+          !cu(cudaMallocAsync(&d_cols, sizeof(int) * nz, s), "allocation") ||
+          !cu(cudaMallocAsync(&d_vals, vsz * nz, s), "allocation") ||
+          !cu(cudaMemcpyAsync(d_rows, rows, sizeof(int) * nnz, cudaMemcpyHostToDevice, s), "copy") ||
+          !cu(cudaMemcpyAsync(d_cols, cols, sizeof(int) * nnz, cudaMemcpyHostToDevice, s), "copy") ||
+          !cu(cudaMemcpyAsync(d_vals, val, vsz * nnz, cudaMemcpyHostToDevice, s), "copy"))
+        break;
+      r_in = d_rows;
+      c_in = d_cols;
+      v_in = d_vals;
+    }
+    const int g = grid_1d(c, nnz);
+    coo_check_kernel<<<g, kBlock, 0, s>>>(nnz, nrow, ncol, r_in, c_in, bad);
+    unsigned long long hbad = 0;
+    if (!cu(cudaGetLastError(), "check") ||
+        !cu(cudaMemcpyAsync(&hbad, bad, sizeof(hbad), cudaMemcpyDeviceToHost, s), "copy") ||
+        !cu(cudaStreamSynchronize(s), "check"))
+      break;
+    if (hbad != ~0ull) {
+      rc = fail(B200LA_ERR_MATRIX, "coo_upload: triplet %llu has an index out of range", hbad);
+      break;
+    }
+    // stable sort by row: keys rows, values input positions
+    if (!cu(cudaMallocAsync(&srow, sizeof(int) * nz, s), "allocation") ||
+        !cu(cudaMallocAsync(&idx, sizeof(int) * nz, s), "allocation") ||
+        !cu(cudaMallocAsync(&perm, sizeof(int) * nz, s), "allocation"))
+      break;
+    iota_kernel<<<g, kBlock, 0, s>>>(nnz, idx);
+    size_t tmp_bytes = 0;
+    const int end_bit = bits_for(nrow);
+    if (!cu(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, r_in, srow, idx, perm, (int)nnz, 0, end_bit, s),
+            "sort size") ||
+        !cu(cudaMallocAsync(&cub_tmp, tmp_bytes > 0 ? tmp_bytes : 1, s), "allocation") ||
+        !cu(cub::DeviceRadixSort::SortPairs(cub_tmp, tmp_bytes, r_in, srow, idx, perm, (int)nnz, 0, end_bit, s),
+            "sort"))
+      break;
+    coo_rowptr_kernel<<<grid_1d(c, nnz + 1), kBlock, 0, s>>>(nnz, nrow, srow, m->rowptr);
+    if (dtype == B200LA_F64) {
+      if (val_dtype == B200LA_F64)
+        coo_gather_kernel<double, double><<<g, kBlock, 0, s>>>(nnz, perm, c_in, (const double *)v_in, m->col,
+                                                               (double *)m->val);
+      else
+        coo_gather_kernel<double, float><<<g, kBlock, 0, s>>>(nnz, perm, c_in, (const float *)v_in, m->col,
+                                                              (double *)m->val);
+    } else {
+      if (val_dtype == B200LA_F64)
+        coo_gather_kernel<float, double><<<g, kBlock, 0, s>>>(nnz, perm, c_in, (const double *)v_in, m->col,
+                                                              (float *)m->val);
+      else
+        coo_gather_kernel<float, float><<<g, kBlock, 0, s>>>(nnz, perm, c_in, (const float *)v_in, m->col,
+                                                             (float *)m->val);
+    }
+    if (nrow > 0) {
+      const int gr = grid_1d(c, nrow);
+      if (dtype == B200LA_F64)
+        coo_rowsort_kernel<double><<<gr, kBlock, 0, s>>>(nrow, m->rowptr, m->col, (double *)m->val, m->diag, max_row_d);
+      else
+        coo_rowsort_kernel<float><<<gr, kBlock, 0, s>>>(nrow, m->rowptr, m->col, (float *)m->val, m->diag, max_row_d);
+    }
+    cu(cudaGetLastError(), "kernels");
+  } while (false);
+  int hmax = 0;
+  if (rc == B200LA_OK && bad) {
+    cu(cudaMemcpyAsync(&hmax, max_row_d, sizeof(int), cudaMemcpyDeviceToHost, s), "copy");
+    cu(cudaStreamSynchronize(s), "sync");
+  }
+  void *scratch[] = {d_rows, d_cols, d_vals, srow, idx, perm, cub_tmp, bad};
+  for (void *p : scratch)
+    if (p) cudaFreeAsync(p, s);
+  if (rc != B200LA_OK) {
+    cudaStreamSynchronize(s);
+    b200la_mat_destroy(m);
+    return rc;
+  }
+  m->max_row = hmax;
+  const double avg = nrow ? (double)nnz / nrow : 0.0;
+  m->format = B200LA_FMT_CSR;
+  m->param = avg <= 3 ? 2 : avg <= 6 ? 4 : avg <= 14 ? 8 : avg <= 40 ? 16 : 32;
+  *out = m;
+  return B200LA_OK;
+}
+
+// CopyTo a host CSR: the uploaded (or built) CSR arrays as stored.
+extern "C" int b200la_mat_download(b200la_mat m, int *rowptr, int *col, void *val) {
+  B_CHECK(m && rowptr && (m->nnz == 0 || (col && val)), B200LA_ERR_INVALID, "mat_download: null argument");
+  cudaStream_t s = m->ctx->stream;
+  B_CUDA(cudaMemcpyAsync(rowptr, m->rowptr, sizeof(int) * ((size_t)m->nrow + 1), cudaMemcpyDeviceToHost, s));
+  if (m->nnz) {
+    B_CUDA(cudaMemcpyAsync(col, m->col, sizeof(int) * (size_t)m->nnz, cudaMemcpyDeviceToHost, s));
+    B_CUDA(cudaMemcpyAsync(val, m->val, dtype_size(m->dtype) * (size_t)m->nnz, cudaMemcpyDeviceToHost, s));
+  }
+  B_CUDA(cudaStreamSynchronize(s));
+  return B200LA_OK;
+}

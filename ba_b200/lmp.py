@@ -230,6 +230,46 @@ class B200_CSR_lMatrix:
         self._shape = (nrow, ncol, int(cl.shape[0]))
 
     @classmethod
+    def TransformFromCOO(cls, rows, cols, data, num_rows: int, num_cols: int, name: str = "",
+                         platform: Platform | None = None, dtype=np.float64) -> "B200_CSR_lMatrix":
+        """CPU_CSR_lMatrix::TransformFromCOO (lmp/lmatrix_csr_cpu.cc:883-906) on
+        the device: triplets in any order (host arrays, or torch CUDA tensors
+        int32/int32/float, read in place), duplicates kept, the reference's CSR
+        order bit for bit."""
+        platform = platform or init_platform()
+        dev = all(hasattr(a, "is_cuda") and a.is_cuda for a in (rows, cols, data))
+        if dev:
+            import torch
+            assert rows.dtype == torch.int32 and cols.dtype == torch.int32
+            nnz = int(rows.numel())
+            vdt = F64 if data.dtype == torch.float64 else F32
+            ptrs = [C.c_void_p(t.data_ptr()) for t in (rows, cols, data)]
+        else:
+            r = np.ascontiguousarray(rows, np.int32)
+            c = np.ascontiguousarray(cols, np.int32)
+            v = np.ascontiguousarray(data)
+            if v.dtype not in (np.float64, np.float32):
+                v = v.astype(np.float64)
+            nnz = int(r.shape[0])
+            vdt = _dt(v.dtype)
+            keep = (r, c, v)
+            ptrs = [a.ctypes.data_as(C.c_void_p) for a in keep]
+        h = C.c_void_p()
+        call("b200la_coo_upload", platform.handle, int(num_rows), int(num_cols), nnz, *ptrs, vdt, _dt(dtype),
+             1 if dev else 0, C.byref(h))
+        return cls._from_handle(h, platform, _dt(dtype), (int(num_rows), int(num_cols), nnz), name)
+
+    def csr(self) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+        """The stored CSR arrays (rowptr, col, val) copied to host memory."""
+        nrow, _, nnz = self._shape
+        rp = np.empty(nrow + 1, np.int32)
+        cl = np.empty(max(nnz, 1), np.int32)
+        vv = np.empty(max(nnz, 1), np.float64 if self.dtype == F64 else np.float32)
+        call("b200la_mat_download", self.handle, rp.ctypes.data_as(C.c_void_p), cl.ctypes.data_as(C.c_void_p),
+             vv.ctypes.data_as(C.c_void_p))
+        return rp, cl[:nnz], vv[:nnz]
+
+    @classmethod
     def _from_handle(cls, handle, platform, dtype, shape, name=""):
         m = cls.__new__(cls)
         m.platform, m.name, m.dtype, m.handle, m._shape = platform, name, dtype, handle, shape

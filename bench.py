@@ -2,7 +2,7 @@
 """Benchmark of the PCG hot path on B200: one JSON line on rank 0.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload batch|poisson3d|varcoef3d|serve|bicgstab|jacobi|gmres]
+                    [--workload batch|poisson3d|varcoef3d|serve|bicgstab|jacobi|gmres|coo]
 
 Workload "batch" (default): 1,024 independent 2D Q1 diffusion systems, n x n
 cells with n log-uniform in [16, 256] from the seed, lognormal per-cell
@@ -22,7 +22,8 @@ Poisson-arrival request stream through the request loop (p50/p99).
 Workloads "bicgstab", "gmres" and "jacobi": the poisson3d matrix solved by
 FP64 BiCGSTAB and by GMRES(100), both with right Jacobi preconditioning, to
 1e-10 (solves/s), and swept by the Jacobi smoother (100 sweeps per step,
-sweeps/s).
+sweeps/s).  Workload "coo": TransformFromCOO of the same matrix from 57M
+shuffled triplets (conversions/s).
 
 Multi-GPU: every rank solves its own batch (seeded per rank): independent
 systems need no exchange, value = all ranks' solves / the slowest rank's time.
@@ -64,7 +65,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="batch",
-                    choices=["batch", "poisson3d", "varcoef3d", "serve", "bicgstab", "jacobi", "gmres"])
+                    choices=["batch", "poisson3d", "varcoef3d", "serve", "bicgstab", "jacobi", "gmres", "coo"])
     ap.add_argument("--cells", type=int, default=128, help="poisson3d cells per axis")
     ap.add_argument("--count", type=int, default=BATCH_COUNT, help="batch: systems per step")
     ap.add_argument("--requests", type=int, default=64, help="serve: requests per timed step")
@@ -1226,6 +1227,101 @@ def run_gmres(args, rank, local_rank, world, torch, dist, barrier):
             "cpu_baseline": cpu}))
 
 
+COO_METRIC = "TransformFromCOO conversions/s (device COO -> CSR), 3D Q1 Poisson triplets in random order"
+
+
+def _coo_triplets(cells):
+    from ba_b200 import problems as P
+    s = P.poisson_3d(cells)
+    rows = np.repeat(np.arange(s.n, dtype=np.int32), np.diff(s.rowptr))
+    perm = np.random.default_rng(20240603).permutation(s.nnz)
+    return s, rows[perm], s.col[perm], s.val[perm]
+
+
+def run_reference_coo(args, rank):
+    import oracle
+    if _ref_unavailable():
+        return
+    s, r, c, v = _coo_triplets(args.cells)
+    secs = []
+    for step in range(1 + args.steps):
+        t = time.perf_counter()
+        oracle.ref_coo_to_csr(s.n, s.n, r, c, v)
+        if step >= 1:
+            secs.append(time.perf_counter() - t)
+    value = 1.0 / statistics.median(secs)
+    print(json.dumps({
+        "impl": "reference", "metric": COO_METRIC, "value": value, "unit": "conversions/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": 1, "ms_per_step": 1e3 / value, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"TransformFromCOO of the 3d q1 poisson {args.cells}^3 matrix, triplets shuffled",
+                   "n": s.n, "nnz": s.nnz, "parallelism": "cpu, 1 thread (the reference's coo_2_csr is serial)"},
+        "cpu_baseline": {"value": value, "unit": "conversions/s", "cores": 1, "kind": "reference",
+                         "sample": "whole conversions, host arrays in, CSR out (copied from the matrix)"},
+        "e2e": {"value": value, "unit": "conversions/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+
+
+def run_coo(args, rank, local_rank, world, torch, dist, barrier):
+    from ba_b200 import lmp
+    plat = lmp.Platform(local_rank)
+    stream = torch.cuda.current_stream()
+    plat.set_stream(stream.cuda_stream)
+    s, r, c, v = _coo_triplets(args.cells)
+    dev = [torch.from_numpy(a).cuda() for a in (r, c, v)]
+    torch.cuda.synchronize()
+
+    def step():
+        A = lmp.B200_CSR_lMatrix.TransformFromCOO(*dev, s.n, s.n, platform=plat)
+        A.Clear()
+    ms_max, clk = _timed(args, stream, torch, barrier, local_rank, step)
+    value = D.aggregate_rate(args.steps, world, ms_max)
+    # e2e: host triplets in, CSR back in host memory
+    barrier()
+    h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    h0.record(stream)
+    for _ in range(args.steps):
+        A = lmp.B200_CSR_lMatrix.TransformFromCOO(r, c, v, s.n, s.n, platform=plat)
+        A.csr()
+        A.Clear()
+    h1.record(stream)
+    h1.synchronize()
+    e2e_value = D.aggregate_rate(args.steps, world, D.max_over_ranks(h0.elapsed_time(h1)))
+    A = lmp.B200_CSR_lMatrix.TransformFromCOO(*dev, s.n, s.n, platform=plat)
+    ok = all(np.array_equal(a, b) for a, b in zip(A.csr(), (s.rowptr, s.col, s.val)))
+    A.Clear()
+    # algorithmic bytes: read the triplets (16 B), write col + val (12 B) and the row pointer
+    alg = s.nnz * (4 + 4 + 8) + s.nnz * (4 + 8) + (s.n + 1) * 4
+    peak, peak_kind = measured_peak_gbs()
+    achieved = alg / (ms_max / args.steps / 1e3) / 1e9
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import oracle
+        if oracle.ref_available():
+            t = time.perf_counter()
+            oracle.ref_coo_to_csr(s.n, s.n, r, c, v)
+            cpu = {"value": 1.0 / (time.perf_counter() - t), "unit": "conversions/s", "cores": 1,
+                   "kind": "reference", "sample": "one whole conversion (the reference's coo_2_csr is serial)"}
+    if rank == 0:
+        print(json.dumps({
+            "metric": COO_METRIC, "value": value, "unit": "conversions/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"TransformFromCOO of the 3d q1 poisson {args.cells}^3 matrix, triplets shuffled",
+                       "n": s.n, "nnz": s.nnz, "matches_generator_csr": ok, "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (913 MB of triplets)"},
+            "clocks": clk,
+            "e2e": {"value": e2e_value, "unit": "conversions/s", "h2d_bytes_per_step": s.nnz * 16,
+                    "d2h_bytes_per_step": s.nnz * 12 + (s.n + 1) * 4},
+            "gpu_launches": args.steps * 7,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None, "peak_source": peak_kind,
+                         "kernel": "whole conversion (check, radix sort by row, row offsets, gather, row sort)",
+                         "algorithmic_bytes": alg,
+                         "note": "the radix sort moves the keys and positions several times; the algorithmic "
+                                 "bytes count one read of the triplets and one write of the CSR"},
+            "cpu_baseline": cpu}))
+
+
 def main():
     args = parse()
     rank, local_rank, world = dist_env()
@@ -1234,7 +1330,7 @@ def main():
             {"batch": run_reference_batch, "poisson3d": run_reference_poisson3d,
              "varcoef3d": run_reference_varcoef3d, "serve": run_reference_serve,
              "bicgstab": run_reference_bicgstab, "jacobi": run_reference_jacobi,
-             "gmres": run_reference_gmres}[args.workload](args, rank)
+             "gmres": run_reference_gmres, "coo": run_reference_coo}[args.workload](args, rank)
         return
     import datetime
 
@@ -1253,7 +1349,8 @@ def main():
 
     load()
     fn = {"batch": run_batch, "poisson3d": run_poisson3d, "varcoef3d": run_varcoef3d,
-          "serve": run_serve, "bicgstab": run_bicgstab, "jacobi": run_jacobi, "gmres": run_gmres}[args.workload]
+          "serve": run_serve, "bicgstab": run_bicgstab, "jacobi": run_jacobi, "gmres": run_gmres,
+          "coo": run_coo}[args.workload]
     fn(args, rank, local_rank, world, torch, dist, barrier)
     if world > 1:
         dist.barrier()

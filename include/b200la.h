@@ -131,6 +131,19 @@ int b200la_dot_noalloc(const void *x, const void *y, int64_t n, int dtype, void 
 int b200la_csr_upload(b200la_ctx ctx, int nrow, int ncol, int64_t nnz, const int *rowptr,
                       const int *col, const void *val, int val_dtype, int dtype,
                       b200la_mat *out);
+/* COO -> CSR on the device: CPU_CSR_lMatrix::TransformFromCOO
+ * (lmp/lmatrix_csr_cpu.cc:883-906, coo_2_csr in lmp/lmatrix_formats.h:320-452).
+ * Triplets (rows[k], cols[k], val[k]) in any order, duplicates kept; the result
+ * is the reference's CSR bit for bit: entries grouped by row in input order,
+ * then each row sorted by column with the reference's selection sort.
+ * device_input = 1: rows, cols and val are device buffers (for example from a
+ * device assembler); 0: host arrays.  Every index is checked on the device; a
+ * triplet out of range fails with B200LA_ERR_MATRIX.  nnz < 2^31. */
+int b200la_coo_upload(b200la_ctx ctx, int nrow, int ncol, int64_t nnz, const int *rows, const int *cols,
+                      const void *val, int val_dtype, int dtype, int device_input, b200la_mat *out);
+/* CopyTo a host CSR (lmp/lmatrix.h CopyTo): rowptr int32[nrow+1], col
+ * int32[nnz], val of the matrix's dtype [nnz], as stored. */
+int b200la_mat_download(b200la_mat m, int *rowptr, int *col, void *val);
 int b200la_mat_destroy(b200la_mat m);
 int b200la_mat_info(b200la_mat m, int *nrow, int *ncol, int64_t *nnz, int *dtype);
 /* CastFrom: a new matrix of the same structure holding the values as dtype. */

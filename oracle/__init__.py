@@ -29,6 +29,7 @@ from .oracle import (  # noqa: F401
     RefSystem,
     bicgstab,
     cg,
+    coo_to_csr,
     dot,
     gmres,
     invdiag,
@@ -39,6 +40,7 @@ from .oracle import (  # noqa: F401
     ref_available,
     ref_bicgstab,
     ref_cg,
+    ref_coo_to_csr,
     ref_gmres,
     ref_jacobi,
     ref_lmp_cg,

@@ -54,6 +54,7 @@ def _load():
             getattr(lib, f"orc_gmres_{s}").argtypes = [
                 C.c_int, _i32p, _i32p, fp, fp, fp, C.c_int, fp, C.c_int, C.c_int, C.c_double,
                 C.c_double, C.c_double, _ip, _dp, _dp]
+        lib.orc_coo2csr_d.argtypes = [C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f64p, _i32p, _i32p, _f64p, _i32p]
         lib.orc_iterate_check.argtypes = [C.c_int, C.c_double, C.c_int, C.c_double, C.c_double,
                                           C.c_double, _dp]
         lib.orc_mpir_d.argtypes = [C.c_int, _i32p, _i32p, _f64p, _f32p, _f64p, _f64p, C.c_int,
@@ -88,6 +89,7 @@ def _load_ref():
         lib.ref_gmres_solve_d.argtypes = [
             C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p, C.c_int,
             C.c_int, C.c_double, C.c_double, C.c_double, _ip, _dp, _dp, _dp]
+        lib.ref_coo_to_csr_d.argtypes = [C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f64p, _i32p, _i32p, _f64p]
         lib.ref_lmp_cg_d.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f64p, _f64p,
                                      _f64p, C.c_double, C.c_double, _ip]
         _ref = lib
@@ -276,6 +278,34 @@ def ref_gmres(rowptr, col, val, b, x0=None, *, size_basis=100, maxits=1000, atol
                                        atol, rtol, dtol, C.byref(it), C.byref(res), C.byref(res0),
                                        C.byref(sec))
     return OracleResult(x, it.value, res.value, res0.value, st, sec.value)
+
+
+def coo_to_csr(nrow, ncol, rows, cols, vals):
+    """coo_2_csr / TransformFromCOO restated in C: (rowptr, col, val)."""
+    rows = np.ascontiguousarray(rows, np.int32)
+    cols = np.ascontiguousarray(cols, np.int32)
+    vals = np.ascontiguousarray(vals, np.float64)
+    nnz = rows.shape[0]
+    rp = np.empty(nrow + 1, np.int32)
+    c = np.empty(max(nnz, 1), np.int32)
+    v = np.empty(max(nnz, 1), np.float64)
+    if _load().orc_coo2csr_d(int(nrow), int(ncol), nnz, rows, cols, vals, rp, c, v,
+                             np.empty(max(nrow, 1), np.int32)) != 0:
+        raise ValueError("COO index out of range")
+    return rp, c[:nnz], v[:nnz]
+
+
+def ref_coo_to_csr(nrow, ncol, rows, cols, vals):
+    """The reference's own CPU_CSR_lMatrix::TransformFromCOO: (rowptr, col, val)."""
+    rows = np.ascontiguousarray(rows, np.int32)
+    cols = np.ascontiguousarray(cols, np.int32)
+    vals = np.ascontiguousarray(vals, np.float64)
+    nnz = rows.shape[0]
+    rp = np.empty(nrow + 1, np.int32)
+    c = np.empty(max(nnz, 1), np.int32)
+    v = np.empty(max(nnz, 1), np.float64)
+    _load_ref().ref_coo_to_csr_d(int(nrow), int(ncol), nnz, rows, cols, vals, rp, c, v)
+    return rp, c[:nnz], v[:nnz]
 
 
 def ref_jacobi(rowptr, col, val, b, x0=None, *, mode=JACOBI_SOLVE_NORMAL, maxits=1000, inner_iter=1,

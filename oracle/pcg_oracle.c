@@ -562,3 +562,52 @@ int orc_mpir_d(int n, const int *rowptr, const int *col, const double *val,
   *res_out = res;
   return res <= rtol * res0 ? 0 : 1;
 }
+
+/*
+ * coo_2_csr (lmp/lmatrix_formats.h:320-452), as CPU_CSR_lMatrix::
+ * TransformFromCOO (lmp/lmatrix_csr_cpu.cc:883-906) calls it: count the
+ * entries of each row, turn the counts into row offsets, scatter the entries
+ * in input order, then sort each row by column with a selection sort (first
+ * minimum by strict <, swapped into place; duplicates are kept and are not
+ * kept in input order).  work holds nrow ints.  Returns 0, or -1 if an index
+ * is out of range.
+ */
+int orc_coo2csr_d(int nrow, int ncol, int nnz, const int *rows, const int *cols,
+                  const double *vals, int *rowptr, int *col, double *val,
+                  int *work) {
+  for (int i = 0; i < nnz; ++i)
+    if (rows[i] < 0 || rows[i] >= nrow || cols[i] < 0 || cols[i] >= ncol)
+      return -1;
+  memset(rowptr, 0, sizeof(int) * (size_t)(nrow + 1));
+  for (int i = 0; i < nnz; ++i) ++rowptr[rows[i]];
+  rowptr[nrow] = nnz;
+  int acc = 0;
+  for (int i = 0; i < nrow; ++i) {
+    const int c = rowptr[i];
+    rowptr[i] = acc;
+    work[i] = acc;
+    acc += c;
+  }
+  for (int i = 0; i < nnz; ++i) {
+    const int t = work[rows[i]]++;
+    col[t] = cols[i];
+    val[t] = vals[i];
+  }
+  for (int k = 0; k < nrow; ++k) {
+    for (int i = rowptr[k], ie = rowptr[k + 1]; i != ie; ++i) {
+      int mi = i, mc = col[i];
+      for (int j = i + 1; j < ie; ++j)
+        if (col[j] < mc) {
+          mi = j;
+          mc = col[j];
+        }
+      const int tc = col[i];
+      col[i] = col[mi];
+      col[mi] = tc;
+      const double tv = val[i];
+      val[i] = val[mi];
+      val[mi] = tv;
+    }
+  }
+  return 0;
+}

@@ -27,6 +27,7 @@
 //                        (linear_solver/bicgstab.h:127-473) and GMRES<LAD>
 //                        (linear_solver/gmres.h:229-746) over the same
 //                        compiled lmp calls.
+//   * ref_coo_to_csr_d -> CPU_CSR_lMatrix::TransformFromCOO.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -631,6 +632,22 @@ int ref_gmres_solve_d(int impl, int nthreads, int precond, int n, int nnz,
   return gmres_solve< double >(impl, nthreads, precond, n, nnz, rowptr, col,
                                val, b, x, size_basis, maxits, atol, rtol, dtol,
                                iters, res, res_init, seconds);
+}
+
+// CPU_CSR_lMatrix::TransformFromCOO (lmp/lmatrix_csr_cpu.cc:883-906, which
+// calls coo_2_csr, lmp/lmatrix_formats.h:320-452) on host COO arrays; the CSR
+// arrays are copied out of the matrix's storage.
+int ref_coo_to_csr_d(int nrow, int ncol, int nnz, const int *rows,
+                     const int *cols, const double *vals, int *rowptr_out,
+                     int *col_out, double *val_out) {
+  CPUsimple_CSR_lMatrix< double > m(nnz, nrow, ncol, "coo");
+  m.TransformFromCOO(rows, cols, vals, nrow, ncol, nnz);
+  for (int i = 0; i <= nrow; ++i) rowptr_out[i] = m.matrix.row[i];
+  for (int k = 0; k < nnz; ++k) {
+    col_out[k] = m.matrix.col[k];
+    val_out[k] = m.matrix.val[k];
+  }
+  return 0;
 }
 
 int ref_lmp_cg_d(int impl, int nthreads, int n, int nnz, const int *rowptr,

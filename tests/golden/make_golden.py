@@ -89,6 +89,17 @@ def main():
     krylov_runs()
 
 
+# TransformFromCOO cases: (rows, cols, triplets, seed); duplicates, empty rows
+COO_CASES = ((50, 60, 400, 1), (300, 300, 5000, 2), (1000, 800, 3000, 3))
+
+
+def coo_triplets(nrow, ncol, nnz, seed):
+    """Seeded random triplets in random order, with duplicate positions."""
+    rng = np.random.default_rng(seed)
+    return (rng.integers(0, nrow, nnz).astype(np.int32), rng.integers(0, ncol, nnz).astype(np.int32),
+            rng.standard_normal(nnz))
+
+
 # GMRES<LAD> restart lengths (basis sizes)
 GMRES_BASIS = (10, 30, 100)
 # Jacobi<LAD> runs: (mode, w, inner_iter, smooth_iter, maxits)
@@ -139,8 +150,14 @@ def krylov_runs():
                     run["x"] = [float(v) for v in r.x]
                 entry["gmres"].append(run)
         out.append(entry)
+    coo = []
+    for nrow, ncol, nnz, seed in COO_CASES:
+        rows, cols, vals = coo_triplets(nrow, ncol, nnz, seed)
+        rp, c, v = oracle.ref_coo_to_csr(nrow, ncol, rows, cols, vals)
+        coo.append({"nrow": nrow, "ncol": ncol, "nnz": nnz, "seed": seed, "sha_rowptr": sha(rp),
+                    "sha_col": sha(c), "sha_val": sha(v)})
     with open(os.path.join(OUT, "reference_krylov_runs.json"), "w") as f:
-        json.dump({"generator": "tests/golden/make_golden.py", "cases": out}, f)
+        json.dump({"generator": "tests/golden/make_golden.py", "cases": out, "coo_to_csr": coo}, f)
     print("wrote", len(out), "Jacobi/BiCGSTAB/GMRES cases")
 
 

@@ -257,3 +257,34 @@ def test_jacobi_bicgstab_gmres_match_compiled_reference_live():
             e = oracle.ref_gmres(s.rowptr, s.col, s.val, s.b, size_basis=m, maxits=800, atol=0.0, rtol=1e-11,
                                  precond=pc)
             assert (a.iters, a.state) == (e.iters, e.state) and np.array_equal(a.x, e.x)
+
+
+# ---- TransformFromCOO -----------------------------------------------------------
+
+LMP_TEST_COO = ([0, 0, 1, 1, 1, 2, 2], [0, 1, 0, 1, 2, 1, 2], [2.0, -1.0, -1.0, 2.0, -1.0, -1.0, 2.0])
+
+
+def test_coo_to_csr_known_answer():
+    # tests/lmp_test.cc:42-89: the 7 triplets through TransformFromCOO, then
+    # A (1, -2, 0) = (4, -5, 2); here also in reversed order
+    kat = json.load(open(os.path.join(GOLD, "reference_known_answers.json")))
+    s7 = P.lmp_test_3x3()
+    for order in (slice(None), slice(None, None, -1)):
+        rows, cols, vals = (np.asarray(a)[order] for a in LMP_TEST_COO)
+        rp, c, v = oracle.coo_to_csr(3, 3, rows, cols, vals)
+        np.testing.assert_array_equal(rp, s7.rowptr)
+        np.testing.assert_array_equal(c, s7.col)
+        np.testing.assert_array_equal(v, s7.val)
+        np.testing.assert_array_equal(oracle.spmv(rp, c, v, kat["lmp_test_spmv"]["x"]), kat["lmp_test_spmv"]["y"])
+
+
+def test_coo_to_csr_matches_reference_runs():
+    from tests.golden.make_golden import coo_triplets
+    with open(os.path.join(GOLD, "reference_krylov_runs.json")) as f:
+        cases = json.load(f)["coo_to_csr"]
+    for case in cases:
+        rows, cols, vals = coo_triplets(case["nrow"], case["ncol"], case["nnz"], case["seed"])
+        rp, c, v = oracle.coo_to_csr(case["nrow"], case["ncol"], rows, cols, vals)
+        assert (_sha(rp), _sha(c), _sha(v)) == (case["sha_rowptr"], case["sha_col"], case["sha_val"])
+    with pytest.raises(ValueError):
+        oracle.coo_to_csr(3, 3, [0, 3], [0, 0], [1.0, 1.0])
