@@ -29,6 +29,7 @@ struct CgScalars {
 
 struct b200la_cg_s {
   b200la_mat A;
+  b200la_ctx ctx;              // kept for destroy, which may come after A's
   b200la_cg_params prm;
   int64_t n;
   void *x, *r, *p, *Ap, *invd;

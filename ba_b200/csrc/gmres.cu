@@ -346,6 +346,7 @@ namespace b200la {
 
 struct GmresState {
   b200la_mat A;
+  b200la_ctx ctx;            // kept for destroy, which may come after A's
   b200la_solver_params prm;
   int64_t n, ldv;
   int m;
@@ -557,7 +558,7 @@ static int gm_profile_t(GmresState *s, const void *b_dev, const void *x_dev, int
 
 void gmres_destroy(GmresState *s) {
   if (!s) return;
-  cudaStream_t st = s->A->ctx->stream;
+  cudaStream_t st = s->ctx->stream;
   cudaStreamSynchronize(st);
   if (s->exec) cudaGraphExecDestroy(s->exec);
   if (s->graph) cudaGraphDestroy(s->graph);
@@ -575,6 +576,7 @@ int gmres_create(b200la_mat A, const b200la_solver_params *prm, GmresState **out
   cudaStream_t st = c->stream;
   GmresState *s = new GmresState();
   s->A = A;
+  s->ctx = c;
   s->prm = *prm;
   s->n = A->nrow;
   s->m = prm->size_basis < prm->maxits ? prm->size_basis : prm->maxits;

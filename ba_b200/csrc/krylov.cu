@@ -350,6 +350,7 @@ using namespace b200la;
 
 struct b200la_solver_s {
   b200la_mat A;
+  b200la_ctx ctx;            // kept for destroy, which may come after A's
   b200la_solver_params prm;
   int64_t n;
   // Jacobi: v[0], v[1] = the iterate pair.  BiCGSTAB: x r r0 q Ap s sh t.
@@ -576,7 +577,7 @@ int b200la_solver_destroy(b200la_solver s) {
     delete s;
     return B200LA_OK;
   }
-  cudaStream_t st = s->A->ctx->stream;
+  cudaStream_t st = s->ctx->stream;
   cudaStreamSynchronize(st);
   if (s->exec) cudaGraphExecDestroy(s->exec);
   if (s->graph) cudaGraphDestroy(s->graph);
@@ -608,6 +609,7 @@ int b200la_solver_create(b200la_mat A, const b200la_solver_params *prm, b200la_s
     p.w = 1.0;
     b200la_solver s = new b200la_solver_s();
     s->A = A;
+    s->ctx = A->ctx;
     s->prm = p;
     s->n = A->nrow;
     const int rc = gmres_create(A, &p, &s->gm);
@@ -635,6 +637,7 @@ int b200la_solver_create(b200la_mat A, const b200la_solver_params *prm, b200la_s
   cudaStream_t st = c->stream;
   b200la_solver s = new b200la_solver_s();
   s->A = A;
+  s->ctx = A->ctx;
   s->prm = p;
   s->n = A->nrow;
   const size_t vb = dtype_size(A->dtype) * (size_t)(s->n > 0 ? s->n : 1);

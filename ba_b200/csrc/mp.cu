@@ -70,6 +70,7 @@ using namespace b200la;
 
 struct b200la_mp_s {
   b200la_mat A64;
+  b200la_ctx ctx;            // kept for destroy, which may come after A64's
   b200la_mat A32;
   b200la_mp_params prm;
   b200la_cg inner;
@@ -105,7 +106,7 @@ extern "C" {
 
 int b200la_mp_destroy(b200la_mp s) {
   if (!s) return B200LA_OK;
-  cudaStream_t st = s->A64->ctx->stream;
+  cudaStream_t st = s->ctx->stream;
   cudaStreamSynchronize(st);
   if (s->inner) b200la_cg_destroy(s->inner);
   if (s->A32) b200la_mat_destroy(s->A32);
@@ -128,6 +129,7 @@ int b200la_mp_create(b200la_mat A64, const b200la_mp_params *prm, b200la_mp *out
   B_CHECK(prm->atol >= 0.0 && prm->rtol >= 0.0 && prm->dtol > 0.0, B200LA_ERR_INVALID, "mp_create: tolerances");
   b200la_mp s = new b200la_mp_s();
   s->A64 = A64;
+  s->ctx = A64->ctx;
   s->prm = *prm;
   s->n = A64->nrow;
   cudaStream_t st = A64->ctx->stream;

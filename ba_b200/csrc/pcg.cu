@@ -413,6 +413,7 @@ int b200la_cg_create(b200la_mat A, const b200la_cg_params *prm, b200la_cg *out) 
   cudaStream_t st = c->stream;
   b200la_cg s = new b200la_cg_s();
   s->A = A;
+  s->ctx = c;
   s->prm = *prm;
   s->n = A->nrow;
   size_t es = dtype_size(A->dtype);
@@ -451,7 +452,7 @@ int b200la_cg_create(b200la_mat A, const b200la_cg_params *prm, b200la_cg *out) 
 
 int b200la_cg_destroy(b200la_cg s) {
   if (!s) return B200LA_OK;
-  cudaStream_t st = s->A->ctx->stream;
+  cudaStream_t st = s->ctx->stream;
   cudaStreamSynchronize(st);
   if (s->exec) cudaGraphExecDestroy(s->exec);
   if (s->graph) cudaGraphDestroy(s->graph);

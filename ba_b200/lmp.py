@@ -685,16 +685,32 @@ class GMRES(_DeviceSolver):
 
 
 class MPIR:
-    """MPIR<LADescriptorCoupledD, LADescriptorCoupledS> with an FP32 Jacobi-PCG
-    as the low-precision error-correction solver (linear_solver/mpir.h:29-150):
-    SetupOperator(A64), SetMpirParameters(max_ech, max_ecl, abs_tol, rel_tol,
-    div_tol), SetLowPrecErrCorSolverParameters(max_iter, abs_tol, rel_tol,
-    div_tol), Solve(b, x).  Only low-precision correction passes run
-    (max_ech is accepted for interface parity and must be 0)."""
+    """MPIR<LADescriptorCoupledD, LADescriptorCoupledS> (linear_solver/mpir.h:29-150,
+    mpir.cc:52-250) with B200 operands.
+
+    Generic form, as in the reference: SetHighPrecMatrix / SetLowPrecMatrix
+    (or SetupOperator(A64), which makes the FP32 copy), the work vectors
+    (made on first use if not set), SetLowPrecErrCorSolver /
+    SetHighPrecErrCorSolver and the four smoothers (any of CG, Jacobi,
+    BiCGSTAB, GMRES here, each running on the device), their
+    Set*Parameters, Use*Smoother and SetMpirParameters(max_ech, max_ecl,
+    abs_tol, rel_tol, div_tol); Solve runs SolveImpl's loop: FP64 residual,
+    then while ContinueIteration(): high pre-smoothing, a low-precision
+    error-correction pass (cast, low pre-smoothing, correction solve, low
+    post-smoothing, cast back) while max_ecl allows, else a high-precision
+    one, x += correction, high post-smoothing, FP64 residual, res0 = res.
+    Kept from the reference: res0_ moves to the latest residual after every
+    pass (mpir.cc:240), the component parameters default to 0 iterations,
+    and the pass counters n_ech_, n_ecl_ are not reset by Solve.
+
+    Fast form (no error-correction solver set): one fused device solve
+    (b200la_mp) with an FP32 Jacobi-PCG as the low-precision solver, outer
+    test relative to the initial residual, SetLowPrecErrCorSolverParameters
+    applying to that PCG; max_ech must be 0 there."""
 
     def __init__(self):
         self.op = None
-        self.max_ecl, self.abs_tol, self.rel_tol, self.div_tol = 50, 0.0, 1e-10, 1e6
+        self.max_ech, self.max_ecl, self.abs_tol, self.rel_tol, self.div_tol = 0, 50, 0.0, 1e-10, 1e6
         self.inner_maxits, self.inner_rtol = 100000, 1e-5
         self.precond = True
         self.tune = True
@@ -702,21 +718,109 @@ class MPIR:
         self.iter_ = 0
         self.outer_ = 0
         self.res_ = self.res_init_ = self.res_rel_ = 0.0
+        # generic form
+        self.Ah = self.Al = None
+        self.resh = self.corh = self.resl = self.corl = None
+        self.solvers = {}                 # role -> solver; roles: ech, ecl, preh, posth, prel, postl
+        self.params = {r: (0, 0.0, 0.0, 0.0) for r in ("ech", "ecl", "preh", "posth", "prel", "postl")}
+        self.use = {"preh": False, "posth": False, "prel": False, "postl": False}
+        self.n_ech = self.n_ecl = 0
+        self.accu = {r: 0 for r in self.params}
+        self.res0_ = 0.0
 
+    # ---- operators and work vectors
     def SetupOperator(self, op: B200_CSR_lMatrix):
         self.op = op
+        self.Ah = op
         self._release()
+
+    def SetHighPrecMatrix(self, mh: B200_CSR_lMatrix):
+        self.SetupOperator(mh)
+
+    def SetLowPrecMatrix(self, ml: B200_CSR_lMatrix):
+        self.Al = ml
+
+    def SetHighPrecResVector(self, v: B200_lVector):
+        self.resh = v
+
+    def SetHighPrecCorVector(self, v: B200_lVector):
+        self.corh = v
+
+    def SetLowPrecResVector(self, v: B200_lVector):
+        self.resl = v
+
+    def SetLowPrecCorVector(self, v: B200_lVector):
+        self.corl = v
+
+    def SetupPreconditioner(self, precond):
+        pass  # MPIR::SetupPreconditioner does nothing (mpir.cc:47-50)
+
+    # ---- components
+    def SetHighPrecPreSmoother(self, s):
+        self.solvers["preh"] = s
+
+    def SetHighPrecPostSmoother(self, s):
+        self.solvers["posth"] = s
+
+    def SetLowPrecPreSmoother(self, s):
+        self.solvers["prel"] = s
+
+    def SetLowPrecPostSmoother(self, s):
+        self.solvers["postl"] = s
+
+    def SetHighPrecErrCorSolver(self, s):
+        self.solvers["ech"] = s
+
+    def SetLowPrecErrCorSolver(self, s):
+        self.solvers["ecl"] = s
+
+    def UseHighPrecPreSmoother(self, use: bool):
+        self.use["preh"] = bool(use)
+
+    def UseHighPrecPostSmoother(self, use: bool):
+        self.use["posth"] = bool(use)
+
+    def UseLowPrecPreSmoother(self, use: bool):
+        self.use["prel"] = bool(use)
+
+    def UseLowPrecPostSmoother(self, use: bool):
+        self.use["postl"] = bool(use)
 
     def SetMpirParameters(self, max_ech: int, max_ecl: int, abs_tol: float, rel_tol: float, div_tol: float):
-        if max_ech != 0:
-            raise B200LAError(-7, "MPIR: high-precision correction passes are not on this path")
-        self.max_ecl, self.abs_tol, self.rel_tol, self.div_tol = int(max_ecl), abs_tol, rel_tol, div_tol
+        self.max_ech, self.max_ecl = int(max_ech), int(max_ecl)
+        self.abs_tol, self.rel_tol, self.div_tol = float(abs_tol), float(rel_tol), float(div_tol)
         self._release()
 
+    def _set_params(self, role, max_iter, abs_tol, rel_tol, div_tol):
+        self.params[role] = (int(max_iter), float(abs_tol), float(rel_tol), float(div_tol))
+        self._reset(role)
+
+    def _reset(self, role):
+        sv = self.solvers.get(role)
+        if sv is not None:
+            sv.InitControl(*self.params[role])
+
+    def SetHighPrecPreSmootherParameters(self, max_iter, abs_tol, rel_tol, div_tol):
+        self._set_params("preh", max_iter, abs_tol, rel_tol, div_tol)
+
+    def SetHighPrecPostSmootherParameters(self, max_iter, abs_tol, rel_tol, div_tol):
+        self._set_params("posth", max_iter, abs_tol, rel_tol, div_tol)
+
+    def SetLowPrecPreSmootherParameters(self, max_iter, abs_tol, rel_tol, div_tol):
+        self._set_params("prel", max_iter, abs_tol, rel_tol, div_tol)
+
+    def SetLowPrecPostSmootherParameters(self, max_iter, abs_tol, rel_tol, div_tol):
+        self._set_params("postl", max_iter, abs_tol, rel_tol, div_tol)
+
+    def SetHighPrecErrCorSolverParameters(self, max_iter, abs_tol, rel_tol, div_tol):
+        self._set_params("ech", max_iter, abs_tol, rel_tol, div_tol)
+
     def SetLowPrecErrCorSolverParameters(self, max_iter: int, abs_tol: float, rel_tol: float, div_tol: float):
+        self._set_params("ecl", max_iter, abs_tol, rel_tol, div_tol)
         self.inner_maxits, self.inner_rtol = int(max_iter), float(rel_tol)
         self._release()
 
+    # ---- fast form
     def _release(self):
         if self._s:
             load().b200la_mp_destroy(self._s)
@@ -727,11 +831,91 @@ class MPIR:
             return
         if self.op is None:
             raise B200LAError(-1, "MPIR: SetupOperator was not called")
+        if self.max_ech != 0:
+            raise B200LAError(-7, "MPIR: high-precision correction passes need SetHighPrecErrCorSolver")
         prm = _lib.MpParams(self.max_ecl, self.abs_tol, self.rel_tol, self.div_tol, self.inner_maxits,
                             self.inner_rtol, 1 if self.precond else 0, 1 if self.tune else 0)
         call("b200la_mp_create", self.op.handle, C.byref(prm), C.byref(self._s))
 
+    # ---- generic form: SolveImpl (mpir.cc:52-285), ContinueIteration (:288-297)
+    def _continue(self) -> bool:
+        r, r0 = self.res_, self.res0_
+        return (r > self.abs_tol and r > r0 * self.rel_tol and r < self.div_tol and
+                ((self.n_ech < self.max_ech and r > self.params["ech"][1] and r > r0 * self.params["ech"][2]
+                  and r < self.params["ech"][3]) or
+                 (self.n_ecl < self.max_ecl and r > self.params["ecl"][1] and r > r0 * self.params["ecl"][2]
+                  and r < self.params["ecl"][3])))
+
+    def _residual(self, b, x):
+        self.Ah.VectorMult(x, self.resh)
+        self.resh.ScaleAdd(-1.0, b)        # coupled resh.ScaleAdd(b, -1)
+        self.res_ = self.resh.Norm2()
+
+    def _run(self, role, b, x):
+        sv = self.solvers[role]
+        sv.Solve(b, x)
+        self.accu[role] += sv.iter()
+        self.iter_ += sv.iter()
+
+    def _solve_generic(self, b: B200_lVector, x: B200_lVector) -> int:
+        if self.Ah is None:
+            raise B200LAError(-1, "MPIR: SetupOperator was not called")
+        n = self.Ah.get_num_row()
+        plat = self.Ah.platform
+        if self.Al is None:
+            self.Al = self.Ah.CastTo(np.float32)
+        for name, dt in (("resh", np.float64), ("corh", np.float64), ("resl", np.float32), ("corl", np.float32)):
+            if getattr(self, name) is None:
+                setattr(self, name, B200_lVector(n, name, platform=plat, dtype=dt))
+        self.iter_ = 0
+        self.accu = {r: 0 for r in self.params}
+        for role, mat in (("preh", self.Ah), ("prel", self.Al), ("ecl", self.Al), ("postl", self.Al),
+                          ("ech", self.Ah), ("posth", self.Ah)):
+            if role in self.solvers and (role in ("ecl", "ech") or self.use.get(role)):
+                self._reset(role)
+                self.solvers[role].SetupOperator(mat)
+            elif self.use.get(role):
+                raise B200LAError(-1, f"MPIR: smoother {role} is used but not set")
+        self._residual(b, x)
+        self.res_init_ = self.res_
+        self.res0_ = self.res_
+        passes = 0
+        while self._continue():
+            passes += 1
+            if self.use["preh"]:
+                self._run("preh", b, x)
+                self._residual(b, x)
+            r, r0 = self.res_, self.res0_
+            pe = self.params["ecl"]
+            ph = self.params["ech"]
+            if "ecl" in self.solvers and self.n_ecl < self.max_ecl and r > pe[1] and r > r0 * pe[2] and r < pe[3]:
+                self.n_ecl += 1
+                self.resl.CastFrom(self.resh)
+                self.corl.Zeros()
+                if self.use["prel"]:
+                    self._run("prel", self.resl, self.corl)
+                self._run("ecl", self.resl, self.corl)
+                if self.use["postl"]:
+                    self._run("postl", self.resl, self.corl)
+                self.corh.CastFrom(self.corl)
+            elif "ech" in self.solvers and self.n_ech < self.max_ech and r > ph[1] and r > r0 * ph[2] and r < ph[3]:
+                self.n_ech += 1
+                self.corh.Zeros()
+                self._run("ech", self.resh, self.corh)
+            x.Axpy(self.corh, 1.0)
+            if self.use["posth"]:
+                self._run("posth", b, x)
+            self._residual(b, x)
+            self.res0_ = self.res_
+        self.outer_ = passes
+        self.res_rel_ = self.res_ / self.res_init_ if self.res_init_ > 0 else 0.0
+        if self.res_ < self.abs_tol or self.res_ < self.res0_ * self.rel_tol:
+            return kSolverSuccess
+        return kSolverExceeded
+
     def Solve(self, b: B200_lVector, x: B200_lVector) -> int:
+        if "ecl" in self.solvers or "ech" in self.solvers:
+            return self._solve_generic(b, x)
         self._ensure()
         r = _lib.MpResult()
         call("b200la_mp_solve", self._s, b.handle, x.handle, C.byref(r))

@@ -268,6 +268,9 @@ typedef struct {
 
 typedef struct b200la_solver_s *b200la_solver;
 
+/* Solver objects (b200la_cg, b200la_mp, b200la_solver) keep a pointer to their
+ * matrix: solve only while it lives; destroying a solver after its matrix is
+ * fine (destroy touches only the context). */
 int b200la_solver_create(b200la_mat A, const b200la_solver_params *params, b200la_solver *out);
 int b200la_solver_destroy(b200la_solver s);
 /* Solve(b, &x): x holds the start value on entry and the solution on exit. */

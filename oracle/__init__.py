@@ -37,6 +37,7 @@ from .oracle import (  # noqa: F401
     jacobi,
     lmp_cg,
     mpir,
+    mpir_generic,
     ref_available,
     ref_bicgstab,
     ref_cg,

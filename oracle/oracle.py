@@ -410,3 +410,99 @@ class RefSystem:
             self.close()
         except Exception:
             pass
+
+
+def _component(kind, opts, rowptr, col, val, b, x0, maxits, atol, rtol, dtol, dtype):
+    """One LinearSolver component of MPIR, solved by the oracle from x0."""
+    kw = dict(maxits=maxits, atol=atol, rtol=rtol, dtol=dtol, dtype=dtype)
+    if kind == "cg":
+        return cg(rowptr, col, val, b, x0, precond=opts.get("precond", True), **kw)
+    if kind == "bicgstab":
+        return bicgstab(rowptr, col, val, b, x0, precond=opts.get("precond", True), **kw)[0]
+    if kind == "gmres":
+        return gmres(rowptr, col, val, b, x0, precond=opts.get("precond", True),
+                     size_basis=opts.get("size_basis", 100), **kw)
+    if kind == "jacobi":
+        return jacobi(rowptr, col, val, b, x0, mode=opts.get("mode", 0), inner_iter=opts.get("inner_iter", 1),
+                      smooth_iter=opts.get("smooth_iter", 1), w=opts.get("w", 1.0), **kw)
+    raise ValueError(kind)
+
+
+def mpir_generic(rowptr, col, val, b, x0=None, *, max_ech=0, max_ecl=0, abs_tol=0.0, rel_tol=0.0, div_tol=0.0,
+                 components=None, use=None):
+    """MPIR<LAD_high, LAD_low>::SolveImpl (linear_solver/mpir.cc:52-285) with
+    ContinueIteration (:288-297), restated over the oracle's solvers: the
+    high-precision parts in float64, the low-precision parts in float32 on
+    the float32 copy of the matrix.  components: role -> (kind, options,
+    (max_iter, abs_tol, rel_tol, div_tol)) for the roles ech, ecl, preh,
+    posth, prel, postl; use: role -> bool for the four smoothers.  As in the
+    reference, res0 moves to the latest residual after every pass.  Returns
+    a dict with x, res, res_init, iters, n_ecl, n_ech, passes, success."""
+    rp, c, v = _csr(rowptr, col, val, np.float64)
+    v32 = v.astype(np.float32)
+    b = np.ascontiguousarray(b, np.float64)
+    n = rp.shape[0] - 1
+    x = np.zeros(n) if x0 is None else np.array(x0, np.float64)
+    components = components or {}
+    use = use or {}
+    zero = (0, 0.0, 0.0, 0.0)
+    par = {r: (components[r][2] if r in components else zero) for r in ("ech", "ecl", "preh", "posth", "prel",
+                                                                          "postl")}
+    it = 0
+    # Jacobi<LAD> in a smoothing mode never resets iter_ (jacobi.cc:256-285), so
+    # the iter() that MPIR adds after each call is that smoother's running total
+    smooth_total = {}
+
+    def run(role, bb, xx, low):
+        nonlocal it
+        kind, opts, (mi, at, rt, dt) = components[role]
+        r = _component(kind, opts, rp, c, v32 if low else v, bb, xx, mi, at, rt, dt,
+                       np.float32 if low else np.float64)
+        if kind == "jacobi" and opts.get("mode", 0) >= 2:
+            smooth_total[role] = smooth_total.get(role, 0) + r.iters
+            it += smooth_total[role]
+        else:
+            it += r.iters
+        return r.x
+
+    def residual(xx):
+        r = b - spmv(rp, c, v, xx)          # VectorMult, ScaleAdd(b, -1): -Ax + b
+        return r, float(np.sqrt(dot(r, r)))
+
+    resh, res = residual(x)
+    res_init = res0 = res
+    n_ech = n_ecl = passes = 0
+
+    def cont():
+        pe, ph = par["ecl"], par["ech"]
+        return (res > abs_tol and res > res0 * rel_tol and res < div_tol and
+                ((n_ech < max_ech and res > ph[1] and res > res0 * ph[2] and res < ph[3]) or
+                 (n_ecl < max_ecl and res > pe[1] and res > res0 * pe[2] and res < pe[3])))
+
+    while cont():
+        passes += 1
+        if use.get("preh"):
+            x = run("preh", b, x, False)
+            resh, res = residual(x)
+        pe, ph = par["ecl"], par["ech"]
+        if "ecl" in components and n_ecl < max_ecl and res > pe[1] and res > res0 * pe[2] and res < pe[3]:
+            n_ecl += 1
+            resl = resh.astype(np.float32)
+            corl = np.zeros(n, np.float32)
+            if use.get("prel"):
+                corl = run("prel", resl, corl, True)
+            corl = run("ecl", resl, corl, True)
+            if use.get("postl"):
+                corl = run("postl", resl, corl, True)
+            corh = corl.astype(np.float64)
+        elif "ech" in components and n_ech < max_ech and res > ph[1] and res > res0 * ph[2] and res < ph[3]:
+            n_ech += 1
+            corh = run("ech", resh, np.zeros(n), False)
+        x = x + corh
+        if use.get("posth"):
+            x = run("posth", b, x, False)
+        resh, res = residual(x)
+        res0 = res
+    success = res < abs_tol or res < res0 * rel_tol
+    return {"x": x, "res": res, "res_init": res_init, "iters": it, "n_ecl": n_ecl, "n_ech": n_ech,
+            "passes": passes, "success": success}

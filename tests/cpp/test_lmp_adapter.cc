@@ -2,7 +2,8 @@
 // like the reference's Boost tests: tests/lmp_test.cc (CSR SpMV known answer),
 // tests/cuda_test.cc (GPU SpMV known answer), tests/cg_test.cc (CG known
 // answer), plus a 2D Q1 Poisson Jacobi-PCG checked against the CPU oracle
-// (oracle/liboracle.so, test infrastructure) and the mixed-precision solver.
+// (oracle/liboracle.so, test infrastructure), the mixed-precision solver,
+// Jacobi/BiCGSTAB/GMRES on the CG known answer and a generic MPIR.
 #include <cmath>
 #include <cstdio>
 #include <vector>
@@ -124,13 +125,75 @@ int main() {
     // mixed precision to 1e-10 relative FP64 residual
     B200_lVector<double> xm(plat, n);
     xm.Zeros();
-    B200_MPIR mp;
+    B200_MPIR mp(plat);
     mp.SetupOperator(A);
     mp.SetMpirParameters(0, 20, 0.0, 1e-10, 1e6);
     mp.SetLowPrecErrCorSolverParameters(100000, 0.f, 1e-5f, 1e30f);
     CHECK(mp.Solve(b, &xm) == kSolverSuccess);
     CHECK(mp.res_rel() < 1e-10);
     std::printf("mpir: outer %d inner iters %d res_rel %.2e\n", mp.outer(), mp.iter(), mp.res_rel());
+  }
+  {  // Jacobi, BiCGSTAB and GMRES on the cg_test.cc system: x = (-0.25, -1.5, -0.75)
+    double bin[] = {1, -2, 0}, zero[] = {0, 0, 0}, xs[3];
+    B200_CSR_lMatrix<double> A(plat, 3, 3, 9, rp9, cl9, va9);
+    B200_lVector<double> b(plat, 3), x(plat, 3);
+    b.SetBlockValues(0, 3, bin);
+    B200_Jacobi<double> jac;
+    B200_BiCGSTAB<double> bicg;
+    bicg.InitParameter("RightPreconditioning");
+    B200_GMRES<double> gm;
+    gm.InitParameter(3, "RightPreconditioning");
+    B200_LinearSolver<double> *solvers[] = {&jac, &bicg, &gm};
+    for (B200_LinearSolver<double> *s : solvers) {
+      x.SetBlockValues(0, 3, zero);
+      s->InitControl(5000, 0.0, 1e-15, 1e8);
+      s->SetupOperator(A);
+      CHECK(s->Solve(b, &x) == kSolverSuccess);
+      x.GetBlockValues(0, 3, xs);
+      CHECK(std::fabs(xs[0] + 0.25) < 1e-12 && std::fabs(xs[1] + 1.5) < 1e-12 && std::fabs(xs[2] + 0.75) < 1e-12);
+    }
+  }
+  {  // generic MPIR: FP32 GMRES error correction with FP32 Jacobi smoothing,
+     // FP64 BiCGSTAB correction once the low passes are spent
+    std::vector<int> rp, cl;
+    std::vector<double> va, bh;
+    poisson2d(48, rp, cl, va, bh);
+    const int n = (int)bh.size();
+    B200_CSR_lMatrix<double> A(plat, n, n, (int64_t)cl.size(), rp.data(), cl.data(), va.data());
+    B200_lVector<double> b(plat, n), x(plat, n);
+    b.SetBlockValues(0, n, bh.data());
+    x.Zeros();
+    B200_GMRES<float> ecl;
+    ecl.InitParameter(30, "RightPreconditioning");
+    B200_Jacobi<float> smooth;
+    smooth.SetSolveMode(2);
+    smooth.SetNumIter(3);
+    B200_BiCGSTAB<double> ech;
+    ech.InitParameter("RightPreconditioning");
+    B200_MPIR mp(plat);
+    mp.SetupOperator(A);
+    mp.SetLowPrecErrCorSolver(ecl);
+    mp.SetHighPrecErrCorSolver(ech);
+    mp.SetLowPrecPreSmoother(smooth);
+    mp.UseLowPrecPreSmoother(true);
+    mp.SetMpirParameters(2, 2, 1e-9, 1e-14, 1e8);
+    mp.SetLowPrecErrCorSolverParameters(2000, 0.0, 1e-4, 1e8);
+    mp.SetLowPrecPreSmootherParameters(3, 0.0, 0.0, 1e8);
+    mp.SetHighPrecErrCorSolverParameters(2000, 1e-12, 1e-6, 1e8);
+    CHECK(mp.Solve(b, &x) == kSolverSuccess);
+    CHECK(mp.n_ecl() == 2 && mp.n_ech() >= 1);
+    std::vector<double> xg(n), r(n);
+    x.GetBlockValues(0, n, xg.data());
+    double rr = 0, bb = 0;
+    for (int i = 0; i < n; ++i) {
+      double y = 0;
+      for (int k = rp[i]; k < rp[i + 1]; ++k) y += va[k] * xg[cl[k]];
+      rr += (bh[i] - y) * (bh[i] - y);
+      bb += bh[i] * bh[i];
+    }
+    CHECK(std::sqrt(rr) <= 1e-9 * 1.001);
+    std::printf("generic mpir: passes %d (low %d, high %d) iters %d res %.2e\n", mp.outer(), mp.n_ecl(), mp.n_ech(),
+                mp.iter(), mp.res());
   }
   {  // errors are reported, not exit(-1)
     int rp2[] = {0, 2, 1};

@@ -70,3 +70,60 @@ def test_mp_pass_limit_reports_exceeded(plat):
     st, m, x = _solve_mp(plat, s, 1e-12, inner_rtol=1e-2, max_outer=2)
     assert st == lmp.kSolverExceeded
     assert m.outer_ == 2
+
+
+# ---- generic MPIR (mpir.cc:52-297) over the device solvers -------------------------
+
+def _mpir_generic(plat, s, cfg):
+    A = lmp.B200_CSR_lMatrix(s.rowptr, s.col, s.val, platform=plat)
+    mp = lmp.MPIR()
+    mp.SetupOperator(A)
+    ecl = lmp.GMRES()
+    ecl.InitParameter(30, "RightPreconditioning")
+    pc = lmp.PreconditionerBlockJacobiStand()
+    pc.Init_Jacobi()
+    ecl.SetupPreconditioner(pc)
+    ech = lmp.BiCGSTAB()
+    ech.SetupPreconditioner(pc)
+    prel = lmp.Jacobi()
+    prel.SetSolveMode(2)
+    prel.SetNumIter(3)
+    posth = lmp.Jacobi()
+    posth.SetSolveMode(3)
+    posth.SetDampingParameter(0.8)
+    mp.SetLowPrecErrCorSolver(ecl)
+    mp.SetHighPrecErrCorSolver(ech)
+    mp.SetLowPrecPreSmoother(prel)
+    mp.SetHighPrecPostSmoother(posth)
+    mp.UseLowPrecPreSmoother(True)
+    mp.UseHighPrecPostSmoother(True)
+    mp.SetMpirParameters(cfg["max_ech"], cfg["max_ecl"], cfg["abs_tol"], cfg["rel_tol"], 1e8)
+    mp.SetLowPrecErrCorSolverParameters(*cfg["ecl"])
+    mp.SetHighPrecErrCorSolverParameters(*cfg["ech"])
+    mp.SetLowPrecPreSmootherParameters(*cfg["prel"])
+    mp.SetHighPrecPostSmootherParameters(*cfg["posth"])
+    b = lmp.B200_lVector.from_numpy(s.b, platform=plat)
+    x = lmp.B200_lVector.from_numpy(np.zeros(s.n), platform=plat)
+    st = mp.Solve(b, x)
+    return mp, st, x.numpy()
+
+
+@pytest.mark.parametrize("max_ecl,max_ech", [(3, 0), (1, 2), (0, 2)])
+def test_generic_mpir_matches_oracle_loop(plat, max_ecl, max_ech):
+    s = P.q1_system(2, 40, 3, 1.0, "mp_generic")
+    cfg = {"max_ecl": max_ecl, "max_ech": max_ech, "abs_tol": 1e-9, "rel_tol": 1e-14,
+           "ecl": (2000, 0.0, 1e-4, 1e8), "ech": (2000, 1e-12, 1e-6, 1e8), "prel": (3, 0.0, 0.0, 1e8),
+           "posth": (2, 0.0, 0.0, 1e8)}
+    comps = {"ecl": ("gmres", {"precond": True, "size_basis": 30}, cfg["ecl"]),
+             "ech": ("bicgstab", {"precond": True}, cfg["ech"]),
+             "prel": ("jacobi", {"mode": 2, "smooth_iter": 3}, cfg["prel"]),
+             "posth": ("jacobi", {"mode": 3, "w": 0.8}, cfg["posth"])}
+    ref = oracle.mpir_generic(s.rowptr, s.col, s.val, s.b, max_ech=max_ech, max_ecl=max_ecl, abs_tol=1e-9,
+                              rel_tol=1e-14, div_tol=1e8, components=comps, use={"prel": True, "posth": True})
+    mp, st, x = _mpir_generic(plat, s, cfg)
+    assert (mp.n_ecl, mp.n_ech, mp.outer_) == (ref["n_ecl"], ref["n_ech"], ref["passes"])
+    assert (st == lmp.kSolverSuccess) == ref["success"]
+    assert abs(mp.iter() - ref["iters"]) <= max(3, int(0.1 * ref["iters"]))
+    true_res = np.linalg.norm(s.b - oracle.spmv(s.rowptr, s.col, s.val, x))
+    if ref["success"]:
+        assert true_res <= 1e-9 * 1.001
