@@ -147,6 +147,7 @@ _SIGS = {
     "b200la_batch_slot_bytes": [_i64, _i64, _i, _i, _P(_i64)],
     "b200la_batch_add": [_vp, _i, _i64, _vp, _vp, _vp, _vp, _vp, _P(_i)],
     "b200la_batch_remove": [_vp, _i],
+    "b200la_batch_launch": [_vp, _i],
     "b200la_batch_run": [_vp, _i, _P(_i)],
     "b200la_batch_result": [_vp, _i, _vp, _P(SysResult)],
     "b200la_batch_results": [_vp, _i, _P(_i), _P(_vp), _P(SysResult)],

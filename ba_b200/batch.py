@@ -15,7 +15,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import BatchParams, SysResult, call, load
-from .lmp import Platform, init_platform
+from .lmp import Platform, _finalizing, init_platform
 
 
 @dataclass
@@ -164,6 +164,11 @@ class Batch:
     def slot_n(self, slot: int) -> int:
         return self._sizes[slot]
 
+    def launch(self, max_passes: int = 64):
+        """Start up to max_passes passes over the running systems and return at
+        once; adds made meanwhile overlap the launch and join the next one."""
+        call("b200la_batch_launch", self.handle, int(max_passes))
+
     def solve(self, chunk_passes: int = 64) -> int:
         """Run until every system has finished, compacting the tile list every
         chunk_passes passes; returns the passes taken."""
@@ -225,7 +230,7 @@ class Batch:
             self.handle = C.c_void_p()
 
     def __del__(self):
-        if sys.is_finalizing():
+        if _finalizing():
             return
         try:
             self.close()

@@ -949,6 +949,11 @@ struct b200la_batch_s {
   int64_t device_bytes;
   cudaGraph_t graph;
   cudaGraphExec_t exec;
+  // adds run on their own stream, so they overlap a launch in flight on the
+  // context stream; the context stream waits for xfer_done before later work
+  cudaStream_t xfer;
+  cudaEvent_t xfer_done;
+  bool in_flight;     // a b200la_batch_launch not yet completed
 };
 
 namespace {
@@ -984,7 +989,7 @@ size_t slot_bytes(int64_t n, int64_t nnz, int64_t ell, bool mixed, bool col16 = 
 template <typename T>
 int alloc_csr_part(BatchHandle B, int slot, int n, int64_t nnz, SysDesc<T> *out) {
   HostSys &h = B->sys[slot];
-  cudaStream_t st = B->ctx->stream;
+  cudaStream_t st = B->xfer;
   const bool mixed = B->kp.mixed != 0;
   const size_t bytes = csr_part_bytes(n, nnz, mixed);
   B_CUDA(cudaMallocAsync(&h.chunk, bytes, st));
@@ -1011,9 +1016,8 @@ int alloc_csr_part(BatchHandle B, int slot, int n, int64_t nnz, SysDesc<T> *out)
 // Allocates the sliced-ELL part (second chunk) once ell and the column type
 // are known.
 template <typename T>
-int alloc_sell_part(BatchHandle B, int slot, int ell, bool col16, SysDesc<T> &d) {
+int alloc_sell_part(BatchHandle B, int slot, int ell, bool col16, SysDesc<T> &d, cudaStream_t st) {
   HostSys &h = B->sys[slot];
-  cudaStream_t st = B->ctx->stream;
   const bool mixed = B->kp.mixed != 0;
   const size_t bytes = sell_part_bytes(d.n, ell, mixed, col16);
   B_CUDA(cudaMallocAsync(&h.chunk2, bytes, st));
@@ -1039,9 +1043,8 @@ void free_slot_memory(BatchHandle B, HostSys &h) {
 // Uploads the descriptor and a fresh RESID state, then builds the sliced-ELL
 // copies, the inverse diagonal and zero work vectors on the device.
 template <typename T>
-int finish_slot(BatchHandle B, int slot, const SysDesc<T> &d) {
+int finish_slot(BatchHandle B, int slot, const SysDesc<T> &d, cudaStream_t st) {
   HostSys &h = B->sys[slot];
-  cudaStream_t st = B->ctx->stream;
   desc_of<T>(h) = d;
   SysState &s0 = B->st_host[slot];
   memset(&s0, 0, sizeof(SysState));
@@ -1067,7 +1070,7 @@ int finish_slot(BatchHandle B, int slot, const SysDesc<T> &d) {
 template <typename T>
 int upload_stage(BatchHandle B, int slot, int n, int64_t nnz, const int *rowptr, const int *col, const double *val,
                  const double *b, const double *x0, CsrCheck *chk, SysDesc<T> *d) {
-  cudaStream_t st = B->ctx->stream;
+  cudaStream_t st = B->xfer;
   B_TRY(alloc_csr_part<T>(B, slot, n, nnz, d));
   B_CUDA(cudaMemcpyAsync((void *)d->rowptr, rowptr, sizeof(int) * (n + 1), cudaMemcpyHostToDevice, st));
   if (nnz) {
@@ -1094,15 +1097,15 @@ int finish_stage(BatchHandle B, int slot, const CsrCheck &c, SysDesc<T> &d) {
     return fail(B200LA_ERR_MATRIX, "csr: a column of row %d is out of range [0,%d)", row, d.n);
   }
   const bool col16 = B->prm.index_bits != 32 && c.max_off <= 32767;
-  B_TRY(alloc_sell_part<T>(B, slot, std::max(c.max_row, 1), col16, d));
+  B_TRY(alloc_sell_part<T>(B, slot, std::max(c.max_row, 1), col16, d, B->xfer));
   d.max_off = c.max_off;
-  return finish_slot<T>(B, slot, d);
+  return finish_slot<T>(B, slot, d, B->xfer);
 }
 
 // Grows the per-batch check records (device and pinned host) to `count`.
 int ensure_checks(BatchHandle B, int count) {
   if (count <= B->chk_cap) return B200LA_OK;
-  cudaStream_t st = B->ctx->stream;
+  cudaStream_t st = B->xfer;
   const int cap = std::max(count, 2 * B->chk_cap);
   if (B->chk) cudaFreeAsync(B->chk, st);
   if (B->chk_host) cudaFreeHost(B->chk_host);
@@ -1489,7 +1492,8 @@ template <typename T>
 int add_many_t(BatchHandle B, int count, const int *n, const int64_t *nnz, const int *const *rowptr,
                const int *const *col, const double *const *val, const double *const *rhs,
                const double *const *x0, int *slots, int *status) {
-  cudaStream_t st = B->ctx->stream;
+  // all of an add runs on the transfer stream: it overlaps a launch in flight
+  cudaStream_t st = B->xfer;
   B_TRY(ensure_checks(B, count));
   csr_check_init_kernel<<<std::max(1, std::min((count + kBlock - 1) / kBlock, 64)), kBlock, 0, st>>>(count, B->chk);
   B_CUDA(cudaGetLastError());
@@ -1553,6 +1557,9 @@ int add_many_t(BatchHandle B, int count, const int *n, const int64_t *nnz, const
     B->device_bytes += (int64_t)h.bytes;
     slots[k] = sl[k];
   }
+  // later work on the context stream (runs, results, removals) follows the add
+  B_CUDA(cudaEventRecord(B->xfer_done, st));
+  B_CUDA(cudaStreamWaitEvent(B->ctx->stream, B->xfer_done, 0));
   if (first != B200LA_OK) set_error(first_msg);
   return first;
 }
@@ -1570,6 +1577,7 @@ int b200la_batch_slot_bytes(int64_t n, int64_t nnz, int max_row, int mixed, int6
 int b200la_batch_destroy(b200la_batch B) {
   if (!B) return B200LA_OK;
   cudaStream_t st = B->ctx->stream;
+  if (B->xfer) cudaStreamSynchronize(B->xfer);
   cudaStreamSynchronize(st);
   if (B->exec) cudaGraphExecDestroy(B->exec);
   if (B->graph) cudaGraphDestroy(B->graph);
@@ -1585,6 +1593,8 @@ int b200la_batch_destroy(b200la_batch B) {
   if (B->chk_host) cudaFreeHost(B->chk_host);
   if (B->glob_host) cudaFreeHost(B->glob_host);
   cudaStreamSynchronize(st);
+  if (B->xfer_done) cudaEventDestroy(B->xfer_done);
+  if (B->xfer) cudaStreamDestroy(B->xfer);
   {
     // return the pool's free blocks to the driver (the context keeps freed
     // blocks while batches add and remove systems)
@@ -1620,7 +1630,9 @@ int b200la_batch_create(b200la_ctx ctx, const b200la_batch_params *p, b200la_bat
   B->sysfirst_host.assign(3 * (size_t)p->capacity, 0);
   cudaStream_t st = ctx->stream;
   const size_t dsz = p->mixed ? sizeof(SysDesc<float>) : sizeof(SysDesc<double>);
-  bool ok = cudaMallocAsync(&B->desc, dsz * p->capacity, st) == cudaSuccess &&
+  bool ok = cudaStreamCreateWithFlags(&B->xfer, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaEventCreateWithFlags(&B->xfer_done, cudaEventDisableTiming) == cudaSuccess &&
+            cudaMallocAsync(&B->desc, dsz * p->capacity, st) == cudaSuccess &&
             cudaMallocAsync(&B->st, sizeof(SysState) * p->capacity, st) == cudaSuccess &&
             cudaMallocAsync(&B->glob, sizeof(BatchGlobals), st) == cudaSuccess &&
             cudaMallocAsync(&B->sysfirst, sizeof(int) * 3 * p->capacity, st) == cudaSuccess &&
@@ -1632,7 +1644,7 @@ int b200la_batch_create(b200la_ctx ctx, const b200la_batch_params *p, b200la_bat
     memset(B->glob_host, 0, sizeof(BatchGlobals));
     ok = cudaMemsetAsync(B->st, 0, sizeof(SysState) * p->capacity, st) == cudaSuccess &&
          cudaMemsetAsync(B->glob, 0, sizeof(BatchGlobals), st) == cudaSuccess &&
-         cudaStreamSynchronize(st) == cudaSuccess;
+         cudaStreamSynchronize(B->xfer) == cudaSuccess && cudaStreamSynchronize(st) == cudaSuccess;
   }
   if (!ok) {
     b200la_batch_destroy(B);
@@ -1674,20 +1686,26 @@ int b200la_batch_add_q1(b200la_batch B, int dim, int cells, uint64_t seed, doubl
   h = HostSys();
   h.n = n;
   h.nnz = (int)nnz;
-  cudaStream_t st = B->ctx->stream;
+  cudaStream_t st = B->xfer;  // like every add: overlaps a launch in flight
   const int ell = cells >= 2 ? (dim == 2 ? 9 : 27) : (dim == 2 ? 4 : 8);
   auto go = [&](auto tag) -> int {
     using T = decltype(tag);
     SysDesc<T> d{};
     B_TRY(alloc_csr_part<T>(B, slot, n, nnz, &d));
-    B_TRY(alloc_sell_part<T>(B, slot, ell, B->prm.index_bits != 32 && q1_col16(dim, cells), d));
+    B_TRY(alloc_sell_part<T>(B, slot, ell, B->prm.index_bits != 32 && q1_col16(dim, cells), d, st));
     d.max_off = (int)std::min<int64_t>(q1_max_off(dim, cells), INT32_MAX);
     B_TRY(q1_assemble(st, B->ctx->num_sms, dim, cells, seed, sigma, (int *)d.rowptr, (int *)d.col,
                       (double *)d.val64, (double *)d.b));
     B_CUDA(cudaMemsetAsync(d.x, 0, 8 * (size_t)n, st));
-    return finish_slot<T>(B, slot, d);
+    return finish_slot<T>(B, slot, d, st);
   };
   const int rc = B->kp.mixed ? go(float()) : go(double());
+  if (cudaEventRecord(B->xfer_done, st) != cudaSuccess ||
+      cudaStreamWaitEvent(B->ctx->stream, B->xfer_done, 0) != cudaSuccess) {
+    free_slot_memory(B, h);
+    h = HostSys();
+    return fail(B200LA_ERR_CUDA, "batch_add_q1: stream ordering failed");
+  }
   if (rc != B200LA_OK) {
     free_slot_memory(B, h);
     h = HostSys();
@@ -1737,8 +1755,48 @@ int b200la_batch_remove(b200la_batch B, int slot) {
   return B200LA_OK;
 }
 
+}  // extern "C"
+
+namespace {
+// Completes a b200la_batch_launch: the states and globals come back after the
+// launch (and after any add queued since, which the context stream waits for).
+int complete_inflight(b200la_batch B) {
+  if (!B->in_flight) return B200LA_OK;
+  cudaStream_t st = B->ctx->stream;
+  B->in_flight = false;
+  B_CUDA(cudaMemcpyAsync(B->st_host, B->st, sizeof(SysState) * B->capacity, cudaMemcpyDeviceToHost, st));
+  B_CUDA(cudaMemcpyAsync(B->glob_host, B->glob, sizeof(BatchGlobals), cudaMemcpyDeviceToHost, st));
+  B_CUDA(cudaStreamSynchronize(st));
+  B->pass_total = B->glob_host->pass_total;
+  return B200LA_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int b200la_batch_launch(b200la_batch B, int max_passes) {
+  B_CHECK(B && max_passes >= 1, B200LA_ERR_INVALID, "batch_launch: bad argument");
+  B_TRY(complete_inflight(B));
+  cudaStream_t st = B->ctx->stream;
+  int active = 0;
+  B_TRY(upload_tiles(B, true, &active, nullptr));
+  BatchGlobals &g = *B->glob_host;
+  if (active == 0) return B200LA_OK;
+  if (!B->ctx->use_graphs) {  // the host loop waits on the device anyway
+    int a = 0;
+    return b200la_batch_run(B, max_passes, &a);
+  }
+  if (!B->exec) B_TRY(build_graph(B));
+  set_globals(B, active, max_passes);
+  B_CUDA(cudaMemcpyAsync(B->glob, &g, sizeof(BatchGlobals), cudaMemcpyHostToDevice, st));
+  B_CUDA(cudaGraphLaunch(B->exec, st));
+  B->in_flight = true;
+  return B200LA_OK;
+}
+
 int b200la_batch_run(b200la_batch B, int max_passes, int *active_out) {
   B_CHECK(B && max_passes >= 1, B200LA_ERR_INVALID, "batch_run: bad argument");
+  B_TRY(complete_inflight(B));
   cudaStream_t st = B->ctx->stream;
   int active = 0;
   B_TRY(upload_tiles(B, true, &active, nullptr));
@@ -1813,6 +1871,8 @@ int fill_result(b200la_batch B, int slot, double *x_host, b200la_sys_result *r) 
 }  // namespace
 
 int b200la_batch_result(b200la_batch B, int slot, double *x_host, b200la_sys_result *r) {
+  B_CHECK(B, B200LA_ERR_INVALID, "batch_result: null batch");
+  B_TRY(complete_inflight(B));
   B_TRY(fill_result(B, slot, x_host, r));
   if (x_host) B_CUDA(cudaStreamSynchronize(B->ctx->stream));
   return B200LA_OK;
@@ -1821,6 +1881,7 @@ int b200la_batch_result(b200la_batch B, int slot, double *x_host, b200la_sys_res
 int b200la_batch_results(b200la_batch B, int count, const int *slots, double *const *x_host,
                          b200la_sys_result *results) {
   B_CHECK(B && count >= 0 && (count == 0 || (slots && results)), B200LA_ERR_INVALID, "batch_results: bad argument");
+  B_TRY(complete_inflight(B));
   bool any = false;
   for (int k = 0; k < count; ++k) {
     double *x = x_host ? x_host[k] : nullptr;
@@ -1842,6 +1903,7 @@ int b200la_batch_info(b200la_batch B, int *used_slots, int64_t *device_bytes) {
 
 int b200la_batch_restart(b200la_batch B) {
   B_CHECK(B, B200LA_ERR_INVALID, "batch_restart: null batch");
+  B_TRY(complete_inflight(B));
   std::vector<int> slots;
   for (int s = 0; s < B->capacity; ++s)
     if (B->sys[s].used) slots.push_back(s);
@@ -1886,6 +1948,7 @@ int b200la_batch_get_items(b200la_batch B, int *rows) {
 
 int b200la_batch_tune(b200la_batch B, int *rows, double *usec) {
   B_CHECK(B, B200LA_ERR_INVALID, "batch_tune: null batch");
+  B_TRY(complete_inflight(B));
   // Both SpMVs use the sliced-ELL layout (one row per lane, 32-row slices,
   // coalesced steps).  The free parameters are the item sizes: rows per
   // warp work item of K1 (SpMV), K2 (update and dots) and K3 (direction).
@@ -1986,6 +2049,7 @@ int b200la_batch_profile_pass(b200la_batch B, int reps, double *ms, int64_t *alg
 
 int b200la_batch_profile(b200la_batch B, int reps, double *ms_spmv, int64_t *algorithmic_bytes) {
   B_CHECK(B && ms_spmv && reps >= 1, B200LA_ERR_INVALID, "batch_profile: bad argument");
+  B_TRY(complete_inflight(B));
   int count = 0;
   int64_t bytes = 0;
   B_TRY(upload_tiles(B, false, &count, &bytes));

@@ -27,6 +27,7 @@ from . import _lib
 from ._lib import F32, F64, FMT_CSR, FMT_SELL, B200LAError, CgParams, CgResult, call, load
 
 kSolverSuccess, kSolverExceeded, kSolverError = 0, 1, 2
+_finalizing = sys.is_finalizing  # held: sys may be torn down before __del__ runs at exit
 
 _NP = {F64: np.float64, F32: np.float32}
 
@@ -70,7 +71,7 @@ class Platform:
     def __del__(self):
         # at interpreter exit the process teardown releases device memory;
         # destroying contexts in arbitrary finalization order is unsafe
-        if sys.is_finalizing():
+        if _finalizing():
             return
         try:
             self.close()
@@ -181,7 +182,7 @@ class B200_lVector:
             self.handle = C.c_void_p()
 
     def __del__(self):
-        if sys.is_finalizing():
+        if _finalizing():
             return
         try:
             self.Clear()
@@ -321,7 +322,7 @@ class B200_CSR_lMatrix:
             self.handle = C.c_void_p()
 
     def __del__(self):
-        if sys.is_finalizing():
+        if _finalizing():
             return
         try:
             self.Clear()
@@ -431,7 +432,7 @@ class CG:
         return self.res_rel_
 
     def __del__(self):
-        if sys.is_finalizing():
+        if _finalizing():
             return
         try:
             self._release()
@@ -521,7 +522,7 @@ class _DeviceSolver:
         return self.res_rel_
 
     def __del__(self):
-        if sys.is_finalizing():
+        if _finalizing():
             return
         try:
             self._release()
@@ -931,7 +932,7 @@ class MPIR:
         return self.res_
 
     def __del__(self):
-        if sys.is_finalizing():
+        if _finalizing():
             return
         try:
             self._release()

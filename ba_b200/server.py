@@ -22,7 +22,7 @@ import numpy as np
 
 from ._lib import BatchParams, ServerParams, ServerStats, SysResult, call, load
 from .batch import SystemResult
-from .lmp import Platform, init_platform
+from .lmp import Platform, _finalizing, init_platform
 
 
 class Server:
@@ -117,7 +117,7 @@ class Server:
         self.close()
 
     def __del__(self):
-        if sys.is_finalizing():
+        if _finalizing():
             return
         try:
             self.close()

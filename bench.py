@@ -331,15 +331,31 @@ def run_batch(args, rank, local_rank, world, torch, dist, barrier):
     xs = [torch.empty(s.n, dtype=torch.float64).pin_memory().numpy() for s in systems]
     h2d = int(sum(h[0].nbytes + h[1].nbytes + h[2].nbytes + h[3].nbytes for h in host))
     d2h = int(sum(x.nbytes for x in xs))
+    # the systems go up in chunks, largest first, each chunk's upload overlapping
+    # the passes already running on the chunks before it (adds run on the
+    # batch's transfer stream, launches are asynchronous)
+    order = sorted(range(len(systems)), key=lambda k: -systems[k].n)
+    chunks, at = [], 0
+    for size in E2E_CHUNKS:
+        chunks.append(order[at:at + size])
+        at += size
+    if at < len(order):
+        chunks.append(order[at:])
+    chunks = [c for c in chunks if c]
+
     def e2e_step():
         for k in range(len(systems)):
             try:
                 E.remove(k)
             except Exception:
                 pass
-        slots = E.add_many(host)
+        slot_of = {}
+        for ch in chunks:
+            for k, sl in zip(ch, E.add_many([host[k] for k in ch])):
+                slot_of[k] = sl
+            E.launch(E2E_LAUNCH_PASSES)
         E.solve(CHUNK)
-        E.results(slots, out=xs)
+        E.results([slot_of[k] for k in range(len(systems))], out=xs)
 
     e2e_step()
     barrier()
@@ -403,6 +419,12 @@ def run_batch(args, rank, local_rank, world, torch, dist, barrier):
         }
         print(json.dumps(out))
     B.close()
+
+
+# e2e: upload chunks (largest systems first: the first, small chunk starts the
+# slowest systems after a few ms) and passes per overlapping launch
+E2E_CHUNKS = (32, 64, 128, 256)
+E2E_LAUNCH_PASSES = 128
 
 
 # ----------------------------------------------------------------- serve workload

@@ -399,6 +399,12 @@ int b200la_batch_slot_size(b200la_batch b, int slot, int *n, int64_t *nnz);
 int b200la_batch_remove(b200la_batch b, int slot);
 /* One graph launch: at most max_passes iterations of every running system.
  * Writes how many systems are still running. */
+/* Asynchronous b200la_batch_run: enqueues one launch of at most max_passes
+ * passes over the running systems and returns at once.  Systems added
+ * meanwhile (b200la_batch_add* run on the batch's own transfer stream) join
+ * at the next launch; the next run, solve, result(s), restart, tune or
+ * profile call completes the launch first. */
+int b200la_batch_launch(b200la_batch B, int max_passes);
 int b200la_batch_run(b200la_batch b, int max_passes, int *active);
 /* Runs until every system has finished, in launches of at most chunk_passes
  * passes; between launches the tile list is rebuilt from the systems still

@@ -249,3 +249,33 @@ def test_large_system_ticket_path_isolated_and_converged(plat):
         r = M.result(sl)
         assert r.solver_state == lmp.kSolverSuccess
         assert np.linalg.norm(s.b - oracle.spmv(s.rowptr, s.col, s.val, r.x)) <= 1.001e-8 * np.linalg.norm(s.b)
+
+
+def test_adds_overlapping_launches_match_the_plain_solve(plat):
+    # systems added in chunks while earlier chunks already iterate (adds on the
+    # batch's transfer stream, launches asynchronous) end bit for bit as when
+    # all are added first: a system's arithmetic does not depend on when it
+    # joined or on what else runs
+    systems = _mix(seed=5, count=12)
+    kw = dict(mixed=True, precond=True, rtol=1e-9, inner_rtol=1e-4, platform=plat)
+    A = Batch(16, **kw)
+    A.set_items(128, 512, 512, adaptive=False)
+    slots_a = A.add_many([(s.rowptr, s.col, s.val, s.b) for s in systems])
+    A.solve(16)
+    ref = A.results(slots_a)
+    B = Batch(16, **kw)
+    B.set_items(128, 512, 512, adaptive=False)
+    order = sorted(range(len(systems)), key=lambda k: -systems[k].n)
+    slot_of = {}
+    for c in range(0, len(order), 4):
+        chunk = order[c:c + 4]
+        for k, sl in zip(chunk, B.add_many([(systems[k].rowptr, systems[k].col, systems[k].val, systems[k].b)
+                                            for k in chunk])):
+            slot_of[k] = sl
+        B.launch(8)
+    B.solve(16)
+    got = B.results([slot_of[k] for k in range(len(systems))])
+    for k, (r, g) in enumerate(zip(ref, got)):
+        assert g.solver_state == lmp.kSolverSuccess, (k, g)
+        assert (g.iters, g.outer) == (r.iters, r.outer)
+        np.testing.assert_array_equal(g.x, r.x)
