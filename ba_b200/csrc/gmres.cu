@@ -14,12 +14,15 @@
 //       them in the same order), w -= h_ij V_i fused with the next dot
 //       (w.V_{i+1}, or w.w at the end), one grid barrier per i; then
 //       V_{j+1} = w / ||w||, z = P V_{j+1}; block 0 applies the Givens
-//       rotations, the test, and at a cycle end solves H y = g.
+//       rotations, the test, and at a cycle end solves H y = g.  When w
+//       fits in the SMs' shared memory (up to ~4.3 M FP64 rows on 148
+//       SMs) it stays there for the whole step.
 // The reference runs the Gram-Schmidt loop as 2 (j+1) separate BLAS-1 calls
 // with a blocking scalar read each; here one launch covers it and the host
 // never waits.  As in the reference, a restart normalises V0 by the
 // recurrence residual |g[j+1]|, not by V0's own norm.
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 #include "internal.cuh"
@@ -43,6 +46,7 @@ struct GmScalars {
   int guard;         // body passes
   unsigned arrive, gen, err;  // G4's grid barrier
   unsigned ticket[2];
+  int stall_block;            // test hook: this block of the resident G4 never reaches its barrier (-1: none)
 };
 
 enum { kGmRestart = 0, kGmStep = 1, kGmUpdate = 2, kGmDone = 3 };
@@ -205,22 +209,103 @@ __device__ __forceinline__ void gm_rotate(double cs, double sn, double *dx, doub
 }
 
 // ---- G4: the Arnoldi step (cooperative launch: every block resident) -------------
-// part4 holds [2][gridDim.x] partial sums, by parity of i, so a block that is
-// one barrier ahead never overwrites partials another block still adds.
+// A pass outside an Arnoldi step only advances the guard and the loop
+// condition (lead thread).
+template <bool IN_GRAPH>
+__device__ __forceinline__ void gm_idle(GmScalars *sc, int phase, cudaGraphConditionalHandle loop) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    int g = sc->guard + 1;
+    sc->guard = g;
+    const bool go = phase != kGmDone;
+    if (IN_GRAPH) cudaGraphSetConditional(loop, go ? 1u : 0u);
+  }
+}
+
+// A grid barrier wait ran out (no block should ever be missing under a
+// cooperative launch): end the solve, and clear the loop condition from the
+// lead thread, which fails the same barrier.
+template <bool IN_GRAPH>
+__device__ __forceinline__ void gm_abort(GmScalars *sc, cudaGraphConditionalHandle loop) {
+  if (threadIdx.x == 0) {
+    sc->state = B200LA_FAIL_BREAKDOWN;
+    sc->phase = kGmDone;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0 && IN_GRAPH) cudaGraphSetConditional(loop, 0u);
+}
+
+// Block 0's end of step j (all its threads): H(j, j+1) = ||w||, the Givens
+// rotations, the test, at a cycle end the back substitution H y = g, then the
+// guard and the loop condition.
+template <bool IN_GRAPH>
+__device__ __noinline__ void gm_step_end(double *H, double *g, double *cs, double *sn, double *y, GmScalars *sc, int j, int m,
+                            double hn, cudaGraphConditionalHandle loop) {
+  __shared__ double ysh[kMaxBasis + 1];
+  __shared__ int finish;
+  const int ldh = m + 1;
+  if (threadIdx.x == 0) {
+    double *Hj = H + j * ldh;
+    Hj[j + 1] = hn;
+    for (int k = 0; k != j; ++k) gm_rotate(cs[k], sn[k], &Hj[k], &Hj[k + 1]);
+    const double dx = Hj[j], dy = Hj[j + 1];
+    const double beta = sqrt(dx * dx + dy * dy);
+    cs[j] = dx / beta;
+    sn[j] = dy / beta;
+    gm_rotate(cs[j], sn[j], &Hj[j], &Hj[j + 1]);
+    gm_rotate(cs[j], sn[j], &g[j], &g[j + 1]);
+    const double res = fabs(g[j + 1]);
+    const int it = sc->iter + 1;
+    sc->iter = it;
+    sc->res = res;
+    const int st8 = gm_check(it, res, *sc);
+    sc->state = st8;
+    finish = (st8 != B200LA_ITERATE || j + 1 == m) ? 1 : 0;
+    if (!finish) sc->j = j + 1;
+  }
+  __syncthreads();
+  if (finish) {
+    // UpdateSolution's back substitution (gmres.h:731-740): the per-element
+    // order of the reference (i descending) with the j < i updates in parallel
+    for (int i = threadIdx.x; i <= j; i += blockDim.x) ysh[i] = g[i];
+    __syncthreads();
+    for (int i = j; i >= 0; --i) {
+      if (threadIdx.x == 0) ysh[i] /= H[i * ldh + i];
+      __syncthreads();
+      const double temp = ysh[i];
+      for (int q = threadIdx.x; q < i; q += blockDim.x) ysh[q] -= H[i * ldh + q] * temp;
+      __syncthreads();
+    }
+    for (int i = threadIdx.x; i <= j; i += blockDim.x) y[i] = ysh[i];
+    if (threadIdx.x == 0) {
+      sc->kend = j;
+      sc->phase = kGmUpdate;
+    }
+  }
+  if (threadIdx.x == 0) {
+    // one pass per Arnoldi step (G1 and G2 ride along in the next pass), so
+    // IterateControl's maxits ends the loop first; the bound only guards
+    // against a broken reduction
+    const int gd = sc->guard + 1;
+    sc->guard = gd;
+    bool go = true;
+    if (gd > sc->maxits + 4) {
+      sc->state = B200LA_FAIL_BREAKDOWN;
+      sc->phase = kGmDone;
+      go = false;
+    }
+    if (IN_GRAPH) cudaGraphSetConditional(loop, go ? 1u : 0u);
+  }
+}
+
+// Streaming form, for any n: w lives in global memory (the L2 keeps most of
+// it).  part4 holds [2][gridDim.x] partial sums, by parity of i, so a block
+// that is one barrier ahead never overwrites partials another block still adds.
 template <typename T, bool PRE, bool IN_GRAPH>
 __global__ void __launch_bounds__(kBlock) gm_arnoldi_kernel(GmBufs<T> v, const double *part3, int n3, double *part4,
                                                             GmScalars *sc, cudaGraphConditionalHandle loop) {
   __shared__ double red[32];
-  __shared__ double ysh[kMaxBasis + 1];
   const int phase = __ldg(&sc->phase);
-  const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
   if (phase != kGmStep) {
-    if (lead) {
-      int g = sc->guard + 1;
-      sc->guard = g;
-      const bool go = phase != kGmDone;
-      if (IN_GRAPH) cudaGraphSetConditional(loop, go ? 1u : 0u);
-    }
+    gm_idle<IN_GRAPH>(sc, phase, loop);
     return;
   }
   const int j = __ldg(&sc->j);
@@ -230,7 +315,7 @@ __global__ void __launch_bounds__(kBlock) gm_arnoldi_kernel(GmBufs<T> v, const d
   // next dot (w.V_{i+1}, or w.w after the last i)
   double h = block_total(part3, n3);
   for (int i = 0; i <= j; ++i) {
-    if (lead) v.H[j * ldh + i] = h;
+    if (blockIdx.x == 0 && threadIdx.x == 0) v.H[j * ldh + i] = h;
     const T hi = (T)h;
     const T *vi = v.V + (int64_t)i * v.ldv;
     const T *vn = i < j ? v.V + (int64_t)(i + 1) * v.ldv : nullptr;
@@ -253,14 +338,7 @@ __global__ void __launch_bounds__(kBlock) gm_arnoldi_kernel(GmBufs<T> v, const d
     double *slot = part4 + (i & 1) * gridDim.x;
     if (threadIdx.x == 0) slot[blockIdx.x] = s[0];
     if (!grid_barrier(&sc->arrive, &sc->gen, &sc->err)) {
-      // a wait ran out (no block should ever be missing under a cooperative
-      // launch): end the solve, and clear the loop condition from the lead
-      // thread, which fails the same barrier
-      if (threadIdx.x == 0) {
-        sc->state = B200LA_FAIL_BREAKDOWN;
-        sc->phase = kGmDone;
-      }
-      if (lead && IN_GRAPH) cudaGraphSetConditional(loop, 0u);
+      gm_abort<IN_GRAPH>(sc, loop);
       return;
     }
     h = block_total(slot, gridDim.x);
@@ -282,60 +360,151 @@ __global__ void __launch_bounds__(kBlock) gm_arnoldi_kernel(GmBufs<T> v, const d
     if (PRE) st<C>(v.z + e, d);
   });
   if (blockIdx.x != 0) return;
-  // block 0: Givens rotations, the test, and at a cycle end H y = g
-  __shared__ int finish;
-  if (threadIdx.x == 0) {
-    double *Hj = v.H + j * ldh;
-    Hj[j + 1] = (double)hn;
-    for (int k = 0; k != j; ++k) gm_rotate(v.cs[k], v.sn[k], &Hj[k], &Hj[k + 1]);
-    const double dx = Hj[j], dy = Hj[j + 1];
-    const double beta = sqrt(dx * dx + dy * dy);
-    v.cs[j] = dx / beta;
-    v.sn[j] = dy / beta;
-    gm_rotate(v.cs[j], v.sn[j], &Hj[j], &Hj[j + 1]);
-    gm_rotate(v.cs[j], v.sn[j], &v.g[j], &v.g[j + 1]);
-    const double res = fabs(v.g[j + 1]);
-    const int it = sc->iter + 1;
-    sc->iter = it;
-    sc->res = res;
-    const int st8 = gm_check(it, res, *sc);
-    sc->state = st8;
-    finish = (st8 != B200LA_ITERATE || j + 1 == m) ? 1 : 0;
-    if (!finish) sc->j = j + 1;
+  gm_step_end<IN_GRAPH>(v.H, v.g, v.cs, v.sn, v.y, sc, j, m, (double)hn, loop);
+}
+
+// Resident form: one block of kResBlock threads per SM, block b owning the
+// slice [b S, b S + S) of w (S a multiple of the 16-byte vector) in shared
+// memory for the whole step.  w is read from global memory once (G3 wrote
+// it) and V_{j+1} (and z) written once at the end; in between, projection i
+// reads only V_i, already in L2 since projection i-1's dot, and V_{i+1},
+// which projection i-1 prefetched into L2 before its grid barrier, so the
+// barrier's wait overlaps the DRAM read.  Each thread owns the 16-byte
+// chunks k = threadIdx.x + t kResBlock of the slice in every pass (so the
+// slice needs no block barrier of its own) and walks them kResUnroll at a
+// time, loads first, to keep that many loads in flight.  Same arithmetic per
+// element as the streaming form, and the same per-thread order; only the
+// partition of the dot products into partial sums differs.  (Measured on
+// the 2.1 M-row Poisson matrix: 1024 threads with 2 loads in flight beat
+// 1024 x 1 and 512 x 4, and a barrier-free all-gather of tagged partials
+// was slower than this barrier.)
+constexpr int kResBlock = 1024;
+constexpr int kResUnroll = 2;
+
+template <typename T>
+__device__ __forceinline__ void prefetch_slice_l2(const T *p, int64_t len) {
+  const char *c = reinterpret_cast<const char *>(p);
+  const int64_t bytes = len * (int64_t)sizeof(T);
+  for (int64_t o = (int64_t)threadIdx.x * 128; o < bytes; o += (int64_t)blockDim.x * 128)
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(c + o));
+}
+
+template <typename T, bool PRE, bool IN_GRAPH>
+__global__ void __launch_bounds__(kResBlock, 1) gm_arnoldi_res_kernel(GmBufs<T> v, const double *part3, int n3,
+                                                                      double *part4, GmScalars *sc, int64_t S,
+                                                                      cudaGraphConditionalHandle loop) {
+  constexpr int W = Vec16<T>::n, U = kResUnroll;
+  extern __shared__ __align__(16) unsigned char gm_dyn[];
+  T *ws = reinterpret_cast<T *>(gm_dyn);
+  __shared__ double red[32];
+  const int phase = __ldg(&sc->phase);
+  if (phase != kGmStep) {
+    gm_idle<IN_GRAPH>(sc, phase, loop);
+    return;
   }
-  __syncthreads();
-  if (finish) {
-    // UpdateSolution's back substitution (gmres.h:731-740): the per-element
-    // order of the reference (i descending) with the j < i updates in parallel
-    for (int i = threadIdx.x; i <= j; i += blockDim.x) ysh[i] = v.g[i];
-    __syncthreads();
-    for (int i = j; i >= 0; --i) {
-      if (threadIdx.x == 0) ysh[i] /= v.H[i * ldh + i];
-      __syncthreads();
-      const double temp = ysh[i];
-      for (int q = threadIdx.x; q < i; q += blockDim.x) ysh[q] -= v.H[i * ldh + q] * temp;
-      __syncthreads();
+  const int j = __ldg(&sc->j);
+  const int m = __ldg(&sc->m), ldh = m + 1;
+  const int64_t lo = (int64_t)blockIdx.x * S;
+  const int64_t len = lo < v.n ? (v.n - lo < S ? v.n - lo : S) : 0;
+  const int64_t nv = len / W;               // whole chunks; elements nv W .. len-1 are the tail
+  const int64_t bd = blockDim.x;
+  const bool stall = (int)blockIdx.x == __ldg(&sc->stall_block);
+  prefetch_slice_l2(v.V + lo, len);
+  if (j > 0) prefetch_slice_l2(v.V + v.ldv + lo, len);
+  // w's slice into shared memory
+  for (int64_t k0 = threadIdx.x; k0 < nv; k0 += U * bd) {
+    T t[U][W];
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+      if (k0 + u * bd < nv) ld<W>(v.w + lo + (k0 + u * bd) * W, t[u]);
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+      if (k0 + u * bd < nv) st<W>(ws + (k0 + u * bd) * W, t[u]);
+  }
+  for (int64_t e = nv * W + threadIdx.x; e < len; e += bd) ws[e] = v.w[lo + e];
+  double h = block_total(part3, n3);
+  for (int i = 0; i <= j; ++i) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) v.H[j * ldh + i] = h;
+    const T hi = (T)h;
+    const T *vi = v.V + (int64_t)i * v.ldv + lo;
+    const T *vn = i < j ? v.V + (int64_t)(i + 1) * v.ldv + lo : nullptr;
+    Acc<T> acc;
+    for (int64_t k0 = threadIdx.x; k0 < nv; k0 += U * bd) {
+      T a[U][W], bn[U][W];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int64_t k = k0 + u * bd;
+        if (k < nv) {
+          ld<W>(vi + k * W, a[u]);
+          if (vn) ld<W>(vn + k * W, bn[u]);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int64_t k = k0 + u * bd;
+        if (k < nv) {
+          T wv[W];
+          ld<W>(ws + k * W, wv);
+#pragma unroll
+          for (int q = 0; q < W; ++q) {
+            wv[q] = fma(-hi, a[u][q], wv[q]);
+            acc.add(wv[q] * (vn ? bn[u][q] : wv[q]));
+          }
+          st<W>(ws + k * W, wv);
+        }
+      }
     }
-    for (int i = threadIdx.x; i <= j; i += blockDim.x) v.y[i] = ysh[i];
-    if (threadIdx.x == 0) {
-      sc->kend = j;
-      sc->phase = kGmUpdate;
+    for (int64_t e = nv * W + threadIdx.x; e < len; e += bd) {
+      const T wv = fma(-hi, vi[e], ws[e]);
+      acc.add(wv * (vn ? vn[e] : wv));
+      ws[e] = wv;
+    }
+    if (i + 2 <= j) prefetch_slice_l2(v.V + (int64_t)(i + 2) * v.ldv + lo, len);
+    double s[1] = {acc.value()};
+    block_sum<1>(s, red);
+    double *slot = part4 + (i & 1) * gridDim.x;
+    if (threadIdx.x == 0) slot[blockIdx.x] = s[0];
+    if (stall) return;  // test hook: this block never reaches the barrier
+    if (!grid_barrier(&sc->arrive, &sc->gen, &sc->err)) {
+      gm_abort<IN_GRAPH>(sc, loop);
+      return;
+    }
+    h = block_total(slot, gridDim.x);
+  }
+  // V_{j+1} = w / ||w||, z = P V_{j+1}
+  const T hn = sqrt((T)h);
+  const T inv = T(1) / hn;
+  T *vj1 = v.V + (int64_t)(j + 1) * v.ldv + lo;
+  for (int64_t k0 = threadIdx.x; k0 < nv; k0 += U * bd) {
+    T d[U][W];
+    if (PRE) {
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+        if (k0 + u * bd < nv) ld<W>(v.invd + lo + (k0 + u * bd) * W, d[u]);
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int64_t k = k0 + u * bd;
+      if (k < nv) {
+        T wv[W];
+        ld<W>(ws + k * W, wv);
+#pragma unroll
+        for (int q = 0; q < W; ++q) {
+          wv[q] = wv[q] * inv;
+          if (PRE) d[u][q] = wv[q] * d[u][q];
+        }
+        st<W>(vj1 + k * W, wv);
+        if (PRE) st<W>(v.z + lo + k * W, d[u]);
+      }
     }
   }
-  if (threadIdx.x == 0) {
-    // one pass per Arnoldi step (G1 and G2 ride along in the next pass), so
-    // IterateControl's maxits ends the loop first; the bound only guards
-    // against a broken reduction
-    const int g = sc->guard + 1;
-    sc->guard = g;
-    bool go = true;
-    if (g > sc->maxits + 4) {
-      sc->state = B200LA_FAIL_BREAKDOWN;
-      sc->phase = kGmDone;
-      go = false;
-    }
-    if (IN_GRAPH) cudaGraphSetConditional(loop, go ? 1u : 0u);
+  for (int64_t e = nv * W + threadIdx.x; e < len; e += bd) {
+    const T wv = ws[e] * inv;
+    vj1[e] = wv;
+    if (PRE) v.z[lo + e] = wv * v.invd[lo + e];
   }
+  if (blockIdx.x != 0) return;
+  gm_step_end<IN_GRAPH>(v.H, v.g, v.cs, v.sn, v.y, sc, j, m, (double)hn, loop);
 }
 
 }  // namespace b200la
@@ -358,6 +527,8 @@ struct GmresState {
   cudaGraphExec_t exec;
   int g_format, g_param;     // schedule baked into the graph
   int grid_start, grid_restart, grid_spmv, grid_ew, grid_coop;
+  int grid_res;              // blocks of the resident Arnoldi kernel (0: streaming form)
+  int64_t res_slice;         // elements of w per block there
 };
 
 template <typename T> static GmBufs<T> gm_bufs(const GmresState *s) {
@@ -373,9 +544,6 @@ template <typename T> static GmBufs<T> gm_bufs(const GmresState *s) {
 template <typename T, bool PRE, bool IN_GRAPH>
 static int gm_launch_arnoldi(GmresState *s, cudaStream_t st, cudaGraphConditionalHandle h) {
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3((unsigned)s->grid_coop);
-  cfg.blockDim = dim3(kBlock);
-  cfg.dynamicSmemBytes = 0;
   cfg.stream = st;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeCooperative;
@@ -383,8 +551,56 @@ static int gm_launch_arnoldi(GmresState *s, cudaStream_t st, cudaGraphConditiona
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   const GmBufs<T> v = gm_bufs<T>(s);
+  if (s->grid_res > 0) {
+    cfg.gridDim = dim3((unsigned)s->grid_res);
+    cfg.blockDim = dim3(kResBlock);
+    cfg.dynamicSmemBytes = (size_t)s->res_slice * sizeof(T);
+    B_CUDA(cudaLaunchKernelEx(&cfg, gm_arnoldi_res_kernel<T, PRE, IN_GRAPH>, v, (const double *)s->part3,
+                              s->grid_spmv, s->part4, s->sc, s->res_slice, h));
+    return B200LA_OK;
+  }
+  cfg.gridDim = dim3((unsigned)s->grid_coop);
+  cfg.blockDim = dim3(kBlock);
+  cfg.dynamicSmemBytes = 0;
   B_CUDA(cudaLaunchKernelEx(&cfg, gm_arnoldi_kernel<T, PRE, IN_GRAPH>, v, (const double *)s->part3, s->grid_spmv,
                             s->part4, s->sc, h));
+  return B200LA_OK;
+}
+
+// Sizes the resident Arnoldi kernel: one block per SM at most, each holding
+// its slice of w in shared memory.  Leaves grid_res = 0 (the streaming form)
+// when the slice does not fit, when a block cannot be resident, or when
+// B200LA_GMRES_RESIDENT=0 is in the environment.
+template <typename T, bool PRE>
+static int gm_size_resident(GmresState *s) {
+  s->grid_res = 0;
+  s->res_slice = 0;
+  const char *env = getenv("B200LA_GMRES_RESIDENT");
+  if (env && env[0] == '0') return B200LA_OK;
+  b200la_ctx c = s->A->ctx;
+  constexpr int W = Vec16<T>::n;
+  const int64_t want = (s->n + (int64_t)kResBlock * W - 1) / ((int64_t)kResBlock * W);
+  const int grid = (int)(want < c->num_sms ? (want < 1 ? 1 : want) : c->num_sms);
+  int64_t S = (s->n + grid - 1) / grid;
+  S = (S + W - 1) / W * W;
+  int optin = 0;
+  B_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
+  const void *kern[2] = {(const void *)gm_arnoldi_res_kernel<T, PRE, true>,
+                         (const void *)gm_arnoldi_res_kernel<T, PRE, false>};
+  const int64_t bytes = S * (int64_t)sizeof(T);
+  for (const void *k : kern) {
+    cudaFuncAttributes fa;
+    B_CUDA(cudaFuncGetAttributes(&fa, k));
+    if (bytes + (int64_t)fa.sharedSizeBytes > (int64_t)optin) return B200LA_OK;
+  }
+  for (const void *k : kern) {
+    B_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    int per_sm = 0;
+    B_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kResBlock, (size_t)bytes));
+    if (per_sm < 1) return B200LA_OK;
+  }
+  s->grid_res = grid;
+  s->res_slice = S;
   return B200LA_OK;
 }
 
@@ -426,7 +642,7 @@ static int gm_grids_t(GmresState *s) {
   int64_t cap = (int64_t)c->num_sms * per_sm;
   if (cap > kMaxReduceBlocks) cap = kMaxReduceBlocks;
   s->grid_coop = (int)(need < 1 ? 1 : (need < cap ? need : cap));
-  return B200LA_OK;
+  return gm_size_resident<T, PRE>(s);
 }
 
 template <typename T, bool PRE>
@@ -486,6 +702,12 @@ static GmScalars gm_initial(const GmresState *s) {
   init.m = s->m;
   init.state = B200LA_ITERATE;
   init.phase = kGmDone;
+  // B200LA_TEST_STALL_BARRIER=b makes block b of the resident Arnoldi
+  // kernel leave before its first grid barrier, so that the other blocks'
+  // waits run out: the solve then ends with B200LA_ERR_TIMEOUT and the
+  // context stays usable (the failure-path test; never set in normal use)
+  const char *stall = getenv("B200LA_TEST_STALL_BARRIER");
+  init.stall_block = stall && stall[0] ? atoi(stall) : -1;
   return init;
 }
 
@@ -638,7 +860,7 @@ int gmres_solve(GmresState *s, b200la_vec b, b200la_vec x, b200la_solver_result 
   B_TRY(gm_fetch(s, &h));
   B_CUDA(cudaMemcpyAsync(x->d, s->x, (size_t)s->n * dtype_size(A->dtype), cudaMemcpyDeviceToDevice, st));
   B_CUDA(cudaStreamSynchronize(st));
-  B_CHECK(h.err == 0, B200LA_ERR_TIMEOUT, "gmres: a grid barrier wait ran out");
+  B_CHECK(h.err == 0, B200LA_ERR_TIMEOUT, "gmres: a wait of the Arnoldi kernel ran out");
   res->iters = h.iter;
   res->state = h.state;
   res->res = h.res;
