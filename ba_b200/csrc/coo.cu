@@ -11,8 +11,11 @@
 //      row, as the reference's scatter keeps it),
 //   3. row offsets from the sorted rows (each row boundary writes its range),
 //   4. a gather of columns and values (cast to the storage type),
-//   5. the reference's selection sort, one thread per row (rows are short in
-//      FE matrices; the work per row is quadratic in its length),
+//   5. the row sort, one warp per row: ranks by shuffles when the row's
+//      columns are distinct (the sorted row is then unique), the
+//      reference's selection sort itself when a column repeats or the row
+//      is longer than 256 entries (rows above 32 entries go through a
+//      worklist to a second kernel),
 //   6. the diagonal positions and the longest row, as b200la_csr_upload does.
 // The result is the reference's CSR bit for bit, duplicates included.
 #include <cub/device/device_radix_sort.cuh>
@@ -47,45 +50,184 @@ __global__ void coo_rowptr_kernel(int64_t nnz, int nrow, const int *__restrict__
   }
 }
 
+// The reference's per-row selection sort (lmatrix_formats.h:405-431) on
+// col[b, e) / val[b, e) in place, then the first diagonal entry.
+template <typename T>
+__device__ void row_selection_sort(int k, int b, int e, int *col, T *val, int *diag) {
+  for (int i = b; i != e; ++i) {
+    int mi = i, mc = col[i];
+    for (int j = i + 1; j < e; ++j)
+      if (col[j] < mc) {
+        mi = j;
+        mc = col[j];
+      }
+    const int tc = col[i];
+    col[i] = col[mi];
+    col[mi] = tc;
+    const T tv = val[i];
+    val[i] = val[mi];
+    val[mi] = tv;
+  }
+  int d = -1;
+  for (int i = b; i != e; ++i)
+    if (col[i] == k) {
+      d = i;
+      break;
+    }
+  diag[k] = d;
+}
+
+// Gather of columns and values into the row-sorted order (cast to the
+// storage type).  The source positions are random, so each thread keeps
+// kGatherUnroll independent loads in flight.
+constexpr int kGatherUnroll = 4;
+
 template <typename T, typename S>
-__global__ void coo_gather_kernel(int64_t nnz, const int *__restrict__ perm, const int *__restrict__ cols,
-                                  const S *__restrict__ vals, int *col, T *val) {
-  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nnz; k += (int64_t)gridDim.x * blockDim.x) {
-    const int p = perm[k];
-    col[k] = cols[p];
-    val[k] = (T)vals[p];
+__global__ void __launch_bounds__(kBlock) coo_gather_kernel(int64_t nnz, const int *__restrict__ perm,
+                                                            const int *__restrict__ cols, const S *__restrict__ vals,
+                                                            int *col, T *val) {
+  constexpr int U = kGatherUnroll;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t k0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k0 < nnz; k0 += U * stride) {
+    int p[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) p[u] = k0 + u * stride < nnz ? perm[k0 + u * stride] : -1;
+    int cc[U];
+    S vv[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+      if (p[u] >= 0) {
+        cc[u] = cols[p[u]];
+        vv[u] = vals[p[u]];
+      }
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+      if (p[u] >= 0) {
+        col[k0 + u * stride] = cc[u];
+        val[k0 + u * stride] = (T)vv[u];
+      }
   }
 }
 
-// The reference's per-row selection sort (lmatrix_formats.h:405-431), one
-// thread per row; also the first diagonal entry and the longest row.
+// Row sort, one warp per row of up to 32 entries (lane l holds entry l, in
+// input order as gathered).  When the row's columns are distinct the sorted
+// row is unique, so each entry goes straight to b + (number of smaller
+// columns), ranks taken with shuffles; that equals the reference's selection
+// sort.  A row with a repeated column (found by __match_any_sync) is sorted
+// by the selection sort itself (lane 0), because there the order of equal
+// columns depends on its swaps.  Longer rows are appended to a worklist for
+// coo_long_rows_kernel.  Also the diagonal positions and the longest row.
 template <typename T>
-__global__ void coo_rowsort_kernel(int nrow, const int *__restrict__ rowptr, int *col, T *val, int *diag,
-                                   int *max_row) {
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nrow; k += gridDim.x * blockDim.x) {
-    const int b = rowptr[k], e = rowptr[k + 1];
-    for (int i = b; i != e; ++i) {
-      int mi = i, mc = col[i];
-      for (int j = i + 1; j < e; ++j)
-        if (col[j] < mc) {
-          mi = j;
-          mc = col[j];
-        }
-      const int tc = col[i];
-      col[i] = col[mi];
-      col[mi] = tc;
-      const T tv = val[i];
-      val[i] = val[mi];
-      val[mi] = tv;
+__global__ void __launch_bounds__(kBlock) coo_rowsort_kernel(int nrow, const int *__restrict__ rowptr, int *col,
+                                                             T *val, int *diag, int *max_row, int *long_rows,
+                                                             int *n_long) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  int longest = 0;
+  for (int64_t kk = warp; kk < nrow; kk += nwarps) {
+    const int k = (int)kk;
+    const int b = rowptr[k], e = rowptr[k + 1], L = e - b;
+    longest = L > longest ? L : longest;
+    if (L > 32) {
+      if (lane == 0) long_rows[atomicAdd(n_long, 1)] = k;
+      continue;
     }
-    int d = -1;
-    for (int i = b; i != e; ++i)
-      if (col[i] == k) {
-        d = i;
-        break;
+    const bool valid = lane < L;
+    const int c = valid ? col[b + lane] : INT_MAX;  // columns are < ncol <= INT_MAX
+    T v = T(0);
+    if (valid) v = val[b + lane];
+    const unsigned same = __match_any_sync(0xffffffffu, c);
+    if (__any_sync(0xffffffffu, valid && __popc(same) > 1)) {
+      if (lane == 0) row_selection_sort(k, b, e, col, val, diag);
+      __syncwarp();
+      continue;
+    }
+    int r = 0;
+    for (int j = 0; j < L; ++j) r += __shfl_sync(0xffffffffu, c, j) < c ? 1 : 0;
+    if (valid) {
+      col[b + r] = c;
+      val[b + r] = v;
+    }
+    // columns are distinct here, so at most one lane holds the diagonal
+    const unsigned dm = __ballot_sync(0xffffffffu, valid && c == k);
+    int rd = -1;
+    if (dm) rd = __shfl_sync(0xffffffffu, r, __ffs(dm) - 1);
+    if (lane == 0) diag[k] = dm ? b + rd : -1;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) longest = max(longest, __shfl_xor_sync(0xffffffffu, longest, o));
+  if (lane == 0 && longest > 0) atomicMax(max_row, longest);
+}
+
+// Rows longer than 32 entries (from coo_rowsort_kernel's worklist), one warp
+// per row: lane l holds entries l, l + 32, ... (up to kMaxQ * 32 = 256) and
+// the ranks come from shuffles as above; a repeated column or a longer row
+// takes the selection sort (lane 0).
+constexpr int kMaxQ = 8;
+
+template <typename T>
+__global__ void __launch_bounds__(kBlock) coo_long_rows_kernel(const int *__restrict__ rowptr, int *col, T *val,
+                                                               int *diag, const int *__restrict__ long_rows,
+                                                               const int *__restrict__ n_long) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int count = *n_long;
+  for (int64_t w = warp; w < count; w += nwarps) {
+    const int k = long_rows[w];
+    const int b = rowptr[k], e = rowptr[k + 1], L = e - b;
+    if (L > kMaxQ * 32) {
+      if (lane == 0) row_selection_sort(k, b, e, col, val, diag);
+      __syncwarp();
+      continue;
+    }
+    const int nq = (L + 31) >> 5;
+    int c[kMaxQ], rank[kMaxQ];
+    T v[kMaxQ];
+#pragma unroll
+    for (int q = 0; q < kMaxQ; ++q) {
+      const int i = q * 32 + lane;
+      const bool ok = q < nq && i < L;
+      c[q] = ok ? col[b + i] : INT_MAX;
+      v[q] = ok ? val[b + i] : T(0);
+      rank[q] = 0;
+    }
+    bool dup = false;
+#pragma unroll
+    for (int qj = 0; qj < kMaxQ; ++qj) {
+      if (qj >= nq) break;
+      const int jn = L - qj * 32 < 32 ? L - qj * 32 : 32;
+      for (int jl = 0; jl < jn; ++jl) {
+        const int cj = __shfl_sync(0xffffffffu, c[qj], jl);
+#pragma unroll
+        for (int q = 0; q < kMaxQ; ++q)
+          if (q < nq && q * 32 + lane < L) {
+            rank[q] += cj < c[q] ? 1 : 0;
+            dup |= cj == c[q] && !(qj == q && jl == lane);
+          }
       }
-    diag[k] = d;
-    atomicMax(max_row, e - b);
+    }
+    if (__any_sync(0xffffffffu, dup)) {
+      __syncwarp();
+      if (lane == 0) row_selection_sort(k, b, e, col, val, diag);
+      __syncwarp();
+      continue;
+    }
+    __syncwarp();
+    int d = INT_MAX;
+#pragma unroll
+    for (int q = 0; q < kMaxQ; ++q) {
+      const int i = q * 32 + lane;
+      if (q < nq && i < L) {
+        col[b + rank[q]] = c[q];
+        val[b + rank[q]] = v[q];
+        if (c[q] == k) d = b + rank[q];
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) d = min(d, __shfl_xor_sync(0xffffffffu, d, o));
+    if (lane == 0) diag[k] = d == INT_MAX ? -1 : d;
   }
 }
 
@@ -123,7 +265,7 @@ extern "C" int b200la_coo_upload(b200la_ctx c, int nrow, int ncol, int64_t nnz, 
   int *d_rows = nullptr, *d_cols = nullptr, *srow = nullptr, *idx = nullptr, *perm = nullptr;
   void *d_vals = nullptr, *cub_tmp = nullptr;
   unsigned long long *bad = nullptr;
-  int *max_row_d = nullptr;
+  int *max_row_d = nullptr, *n_long_d = nullptr, *long_rows = nullptr;
   b200la_mat m = new b200la_mat_s();
   m->ctx = c;
   m->nrow = nrow;
@@ -142,12 +284,13 @@ extern "C" int b200la_coo_upload(b200la_ctx c, int nrow, int ncol, int64_t nnz, 
         !cu(cudaMallocAsync(&m->col, sizeof(int) * nz, s), "allocation") ||
         !cu(cudaMallocAsync(&m->val, dtype_size(dtype) * nz, s), "allocation") ||
         !cu(cudaMallocAsync(&m->diag, sizeof(int) * (size_t)(nrow > 0 ? nrow : 1), s), "allocation") ||
-        !cu(cudaMallocAsync(&bad, sizeof(unsigned long long) + sizeof(int), s), "allocation"))
+        !cu(cudaMallocAsync(&bad, sizeof(unsigned long long) + 2 * sizeof(int), s), "allocation"))
       break;
     max_row_d = reinterpret_cast<int *>(bad + 1);
+    n_long_d = max_row_d + 1;
     const unsigned long long none = ~0ull;
     if (!cu(cudaMemcpyAsync(bad, &none, sizeof(none), cudaMemcpyHostToDevice, s), "copy") ||
-        !cu(cudaMemsetAsync(max_row_d, 0, sizeof(int), s), "memset"))
+        !cu(cudaMemsetAsync(max_row_d, 0, 2 * sizeof(int), s), "memset"))
       break;
     if (nnz == 0) {
       if (!cu(cudaMemsetAsync(m->rowptr, 0, sizeof(int) * ((size_t)nrow + 1), s), "memset")) break;
@@ -210,11 +353,19 @@ extern "C" int b200la_coo_upload(b200la_ctx c, int nrow, int ncol, int64_t nnz, 
                                                              (float *)m->val);
     }
     if (nrow > 0) {
-      const int gr = grid_1d(c, nrow);
-      if (dtype == B200LA_F64)
-        coo_rowsort_kernel<double><<<gr, kBlock, 0, s>>>(nrow, m->rowptr, m->col, (double *)m->val, m->diag, max_row_d);
-      else
-        coo_rowsort_kernel<float><<<gr, kBlock, 0, s>>>(nrow, m->rowptr, m->col, (float *)m->val, m->diag, max_row_d);
+      if (!cu(cudaMallocAsync(&long_rows, sizeof(int) * (size_t)nrow, s), "allocation")) break;
+      const int gr = grid_1d(c, (int64_t)nrow * 32);
+      if (dtype == B200LA_F64) {
+        coo_rowsort_kernel<double><<<gr, kBlock, 0, s>>>(nrow, m->rowptr, m->col, (double *)m->val, m->diag,
+                                                         max_row_d, long_rows, n_long_d);
+        coo_long_rows_kernel<double><<<c->num_sms * 8, kBlock, 0, s>>>(m->rowptr, m->col, (double *)m->val,
+                                                                       m->diag, long_rows, n_long_d);
+      } else {
+        coo_rowsort_kernel<float><<<gr, kBlock, 0, s>>>(nrow, m->rowptr, m->col, (float *)m->val, m->diag,
+                                                        max_row_d, long_rows, n_long_d);
+        coo_long_rows_kernel<float><<<c->num_sms * 8, kBlock, 0, s>>>(m->rowptr, m->col, (float *)m->val, m->diag,
+                                                                      long_rows, n_long_d);
+      }
     }
     cu(cudaGetLastError(), "kernels");
   } while (false);
@@ -223,7 +374,7 @@ extern "C" int b200la_coo_upload(b200la_ctx c, int nrow, int ncol, int64_t nnz, 
     cu(cudaMemcpyAsync(&hmax, max_row_d, sizeof(int), cudaMemcpyDeviceToHost, s), "copy");
     cu(cudaStreamSynchronize(s), "sync");
   }
-  void *scratch[] = {d_rows, d_cols, d_vals, srow, idx, perm, cub_tmp, bad};
+  void *scratch[] = {d_rows, d_cols, d_vals, srow, idx, perm, cub_tmp, bad, long_rows};
   for (void *p : scratch)
     if (p) cudaFreeAsync(p, s);
   if (rc != B200LA_OK) {

@@ -44,7 +44,11 @@ struct GmScalars {
   int phase;         // kGmRestart / kGmStep / kGmUpdate / kGmDone
   int maxits;
   int guard;         // body passes
-  unsigned arrive, gen, err;  // G4's grid barrier
+  // G4's grid barrier: arrivals, generation (polled by the waiters) and
+  // error flag, each on its own 128-byte line
+  alignas(128) unsigned arrive;
+  alignas(128) unsigned gen;
+  alignas(128) unsigned err;
   unsigned ticket[2];
   int stall_block;            // test hook: this block of the resident G4 never reaches its barrier (-1: none)
 };

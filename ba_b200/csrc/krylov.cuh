@@ -50,19 +50,30 @@ template <int C, typename T> __device__ __forceinline__ void st(T *p, const T (&
 // Grid-wide barrier for kernels launched cooperatively (all blocks resident).
 // Sense by generation: a block's thread 0 reads the generation, arrives on
 // the counter, and the last to arrive resets the counter and advances the
-// generation; the others wait for the generation to move.  Every wait is
-// bounded: after kSpinLimit polls (about 0.3 s) the waiter sets *err and the
-// call returns false in every thread of the block; a waiter also gives up at
-// once when another block has set *err.  Callers end the kernel when it
-// returns false.  Must be called by every thread of every block.
+// generation; the others wait for the generation to move.  The waiters poll
+// with plain (relaxed) loads, not atomics, so the arrivals' atomics do not
+// queue behind them; callers keep arrive, gen and err on separate 128-byte
+// lines.  Every wait is bounded: after kSpinLimit polls (a few seconds at
+// most) the waiter sets *err and the call returns false in every thread of
+// the block; a waiter also gives up when another block has set *err (checked
+// every 64 polls).  Callers end the kernel when it returns false.  Must be
+// called by every thread of every block.
 constexpr long long kSpinLimit = 1LL << 22;
+
+__device__ __forceinline__ unsigned ld_relaxed_u32(const unsigned *p) {
+  unsigned v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
 
 __device__ __forceinline__ bool grid_barrier(unsigned *arrive, unsigned *gen, unsigned *err) {
   __shared__ bool ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     bool good = true;
-    const unsigned g = atomicAdd(gen, 0u);
+    // a block passed the previous barrier only after seeing this generation,
+    // so the read cannot return an older one
+    const unsigned g = ld_relaxed_u32(gen);
     __threadfence();
     if (atomicAdd(arrive, 1u) == gridDim.x - 1) {
       atomicExch(arrive, 0u);
@@ -70,13 +81,14 @@ __device__ __forceinline__ bool grid_barrier(unsigned *arrive, unsigned *gen, un
       atomicAdd(gen, 1u);
     } else {
       long long spins = 0;
-      while (atomicAdd(gen, 0u) == g) {
-        if (++spins > kSpinLimit || atomicAdd(err, 0u) != 0u) {
+      while (ld_relaxed_u32(gen) == g) {
+        ++spins;
+        if (spins > kSpinLimit || ((spins & 63) == 0 && ld_relaxed_u32(err) != 0u)) {
           atomicExch(err, 1u);
           good = false;
           break;
         }
-        __nanosleep(64);
+        __nanosleep(32);
       }
     }
     __threadfence();

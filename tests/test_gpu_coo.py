@@ -66,6 +66,36 @@ def test_random_triplets_match_oracle(plat, nrow, ncol, nnz, seed):
     np.testing.assert_array_equal(v, ref[2].astype(np.float32))
 
 
+def test_long_and_distinct_rows(plat):
+    # the warp-per-row kernel ranks distinct columns with shuffles for rows
+    # of up to 256 entries and falls back to the selection sort for longer
+    # rows or repeated columns; cover each side of both limits
+    rng = np.random.default_rng(11)
+    lengths = [0, 1, 31, 32, 33, 64, 100, 255, 256, 257, 600, 27, 125]
+    ncol = 1000
+    rows, cols = [], []
+    for r, L in enumerate(lengths):
+        rows.append(np.full(L, r, np.int32))
+        cols.append(rng.permutation(ncol)[:L].astype(np.int32))   # distinct columns
+    # two rows with one repeated column each (short and long)
+    for L in (40, 300):
+        r = len(lengths)
+        lengths.append(L)
+        cc = rng.permutation(ncol)[:L].astype(np.int32)
+        cc[L // 2] = cc[3]
+        rows.append(np.full(L, r, np.int32))
+        cols.append(cc)
+    rows, cols = np.concatenate(rows), np.concatenate(cols)
+    perm = rng.permutation(rows.size)
+    rows, cols = rows[perm], cols[perm]
+    vals = rng.standard_normal(rows.size)
+    nrow = len(lengths)
+    ref = oracle.coo_to_csr(nrow, ncol, rows, cols, vals)
+    A = lmp.B200_CSR_lMatrix.TransformFromCOO(rows, cols, vals, nrow, ncol, platform=plat)
+    for got, want in zip(A.csr(), ref):
+        np.testing.assert_array_equal(got, want)
+
+
 def test_device_triplets_and_scrambled_fe_matrix(plat):
     import torch
     s = P.q1_system(3, 40, 21, 1.0, "q1_40")
