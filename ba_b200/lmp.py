@@ -260,15 +260,25 @@ class B200_CSR_lMatrix:
              1 if dev else 0, C.byref(h))
         return cls._from_handle(h, platform, _dt(dtype), (int(num_rows), int(num_cols), nnz), name)
 
-    def csr(self) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
-        """The stored CSR arrays (rowptr, col, val) copied to host memory."""
+    def csr(self, out=None) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+        """The stored CSR arrays (rowptr, col, val) copied to host memory, into
+        out = (rowptr, col, val) when given (contiguous arrays of at least
+        nrow + 1, nnz and nnz elements of int32, int32 and the value type,
+        e.g. views of pinned buffers)."""
         nrow, _, nnz = self._shape
-        rp = np.empty(nrow + 1, np.int32)
-        cl = np.empty(max(nnz, 1), np.int32)
-        vv = np.empty(max(nnz, 1), np.float64 if self.dtype == F64 else np.float32)
+        vdt = np.float64 if self.dtype == F64 else np.float32
+        if out is None:
+            rp = np.empty(nrow + 1, np.int32)
+            cl = np.empty(max(nnz, 1), np.int32)
+            vv = np.empty(max(nnz, 1), vdt)
+        else:
+            rp, cl, vv = out
+            for a, need, dt in ((rp, nrow + 1, np.int32), (cl, nnz, np.int32), (vv, nnz, vdt)):
+                if a.dtype != dt or not a.flags.c_contiguous or a.size < need:
+                    raise B200LAError(-1, "csr: out arrays of the wrong type, layout or size")
         call("b200la_mat_download", self.handle, rp.ctypes.data_as(C.c_void_p), cl.ctypes.data_as(C.c_void_p),
              vv.ctypes.data_as(C.c_void_p))
-        return rp, cl[:nnz], vv[:nnz]
+        return rp[:nrow + 1], cl[:nnz], vv[:nnz]
 
     @classmethod
     def _from_handle(cls, handle, platform, dtype, shape, name=""):

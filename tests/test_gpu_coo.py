@@ -120,6 +120,24 @@ def test_device_triplets_and_scrambled_fe_matrix(plat):
     assert abs(solver.iter() - ref.iters) <= 1
 
 
+def test_csr_download_into_given_buffers(plat):
+    import torch
+    rows, cols, vals = _triplets(300, 300, 5000, 2)
+    ref = oracle.coo_to_csr(300, 300, rows, cols, vals)
+    pin = [torch.from_numpy(a).pin_memory().numpy() for a in (rows, cols, vals)]
+    A = lmp.B200_CSR_lMatrix.TransformFromCOO(*pin, 300, 300, platform=plat)
+    out = (np.empty(301, np.int32), torch.empty(5000, dtype=torch.int32, pin_memory=True).numpy(),
+           np.empty(5000, np.float64))
+    got = A.csr(out=out)
+    for g, o, w in zip(got, out, ref):
+        assert np.shares_memory(g, o)
+        np.testing.assert_array_equal(g, w)
+    with pytest.raises(B200LAError):
+        A.csr(out=(np.empty(301, np.int32), np.empty(4999, np.int32), np.empty(5000, np.float64)))
+    with pytest.raises(B200LAError):
+        A.csr(out=(np.empty(301, np.int32), np.empty(5000, np.int32), np.empty(5000, np.float32)))
+
+
 def test_bad_triplets_are_refused(plat):
     with pytest.raises(B200LAError):
         lmp.B200_CSR_lMatrix.TransformFromCOO([0, 3], [0, 0], [1.0, 1.0], 3, 3, platform=plat)
