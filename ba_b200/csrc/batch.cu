@@ -739,10 +739,9 @@ __global__ void batch_start_kernel(BatchGlobals *g) {
 // Slot set-up after the CSR arrived: sliced-ELL copies (inner type and
 // FP64), the inverse diagonal in the inner type, zero work vectors.
 template <typename T>
-__global__ void slot_setup_kernel(SysDesc<T> d, unsigned *bad) {
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+__device__ void slot_setup_rows(const SysDesc<T> &d, unsigned *bad, int64_t first, int64_t stride, bool zero_x) {
   const int64_t padded_rows = (int64_t)(d.n + 31) / 32 * 32;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < padded_rows; i += stride) {
+  for (int64_t i = first; i < padded_rows; i += stride) {
     // padding repeats a column the row reads (an empty row: its own index);
     // padding rows past n (last slice) read column n - 1
     int start = 0, len = 0, pad = d.n - 1;
@@ -762,7 +761,7 @@ __global__ void slot_setup_kernel(SysDesc<T> d, unsigned *bad) {
         const_cast<double *>(d.sval64)[pos] = real ? d.val64[start + k] : 0.0;
     }
   }
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < d.n; i += stride) {
+  for (int64_t i = first; i < d.n; i += stride) {
     int k = -1;
     for (int j = d.rowptr[i]; j < d.rowptr[i + 1]; ++j)
       if (d.col[j] == i) { k = j; break; }
@@ -777,6 +776,46 @@ __global__ void slot_setup_kernel(SysDesc<T> d, unsigned *bad) {
     d.r[i] = T(0);
     d.p[i] = T(0);
     d.Ap[i] = T(0);
+    if (zero_x) d.x[i] = 0.0;
+  }
+}
+
+// One system's sliced-ELL copy, inverse diagonal and zero work vectors.
+template <typename T>
+__global__ void slot_setup_kernel(SysDesc<T> d, unsigned *bad) {
+  slot_setup_rows(d, bad, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, (int64_t)gridDim.x * blockDim.x, false);
+}
+
+// The systems of one add_many call: job k is system k's descriptor, slot and
+// whether x starts at zero.
+template <typename T> struct SetupJob {
+  SysDesc<T> d;
+  int slot;
+  int zero_x;
+};
+
+// Descriptor and fresh RESID state of every job's slot (thread per job).
+template <typename T>
+__global__ void slot_init_many_kernel(const SetupJob<T> *__restrict__ jobs, int count, SysDesc<T> *desc,
+                                      SysState *st) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
+    const int s = jobs[k].slot;
+    desc[s] = jobs[k].d;
+    SysState z{};
+    z.phase = PH_RESID;
+    z.bad_row = 0xffffffffu;
+    st[s] = z;
+  }
+}
+
+// slot_setup_kernel for every job: blockIdx.y walks the jobs, blockIdx.x
+// and the threads the rows of one system.
+template <typename T>
+__global__ void slot_setup_many_kernel(const SetupJob<T> *__restrict__ jobs, int count, SysState *st) {
+  for (int k = blockIdx.y; k < count; k += gridDim.y) {
+    const SetupJob<T> &j = jobs[k];
+    slot_setup_rows(j.d, &st[j.slot].bad_row, (int64_t)blockIdx.x * blockDim.x + threadIdx.x,
+                    (int64_t)gridDim.x * blockDim.x, j.zero_x != 0);
   }
 }
 
@@ -843,12 +882,11 @@ __global__ void csr_check_init_kernel(int count, CsrCheck *c) {
     c[k] = CsrCheck{~0ull, 0, 0};
 }
 
-__global__ void csr_check_kernel(int n, int nnz, const int *__restrict__ rowptr, const int *__restrict__ col,
-                                 CsrCheck *out) {
-  const int stride = gridDim.x * blockDim.x;
+__device__ void csr_check_rows(int n, int nnz, const int *__restrict__ rowptr, const int *__restrict__ col,
+                               CsrCheck *out, int first, int stride) {
   int mr = 0, mo = 0;
   unsigned long long err = ~0ull;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+  for (int i = first; i < n; i += stride) {
     const int a = rowptr[i], b = rowptr[i + 1];
     unsigned long long e = ~0ull;
     if ((i == 0 && a != 0) || (i == n - 1 && b != nnz)) e = ((unsigned long long)i << 8) | kChkStart;
@@ -871,6 +909,24 @@ __global__ void csr_check_kernel(int n, int nnz, const int *__restrict__ rowptr,
   if (err != ~0ull) atomicMin(&out->err, err);
   if (mr) atomicMax(&out->max_row, mr);
   if (mo) atomicMax(&out->max_off, mo);
+}
+
+// The uploaded CSR arrays of one add_many call, one job per system (n = 0:
+// nothing to check, the system was refused on the host).
+struct CheckJob {
+  const int *rowptr, *col;
+  int n, nnz;
+};
+
+// csr_check for every job: blockIdx.y walks the jobs, blockIdx.x and the
+// threads the rows of one system; out[k] collects job k's verdict.
+__global__ void csr_check_many_kernel(const CheckJob *__restrict__ jobs, int count, CsrCheck *out) {
+  for (int k = blockIdx.y; k < count; k += gridDim.y) {
+    const CheckJob j = jobs[k];
+    if (j.n > 0)
+      csr_check_rows(j.n, j.nnz, j.rowptr, j.col, out + k, blockIdx.x * blockDim.x + threadIdx.x,
+                     gridDim.x * blockDim.x);
+  }
 }
 
 // Restart every listed slot from x = 0: RESID phase, counters cleared.
@@ -940,9 +996,13 @@ struct b200la_batch_s {
   void *desc;         // SysDesc<T>[capacity]
   SysState *st;       // [capacity]
   BatchGlobals *glob;
-  CsrCheck *chk;       // device results of csr_check_kernel, one per system of an add
+  CsrCheck *chk;       // device verdicts of the checks, one per system of an add
   CsrCheck *chk_host;  // pinned mirror
   int chk_cap;
+  // per-add job lists (check jobs, then setup jobs): pinned host staging and
+  // its device copy, chk_cap entries of each
+  void *jobs_host;
+  void *jobs_dev;
   // host mirrors
   SysState *st_host;  // pinned [capacity]
   BatchGlobals *glob_host;
@@ -1067,9 +1127,11 @@ int finish_slot(BatchHandle B, int slot, const SysDesc<T> &d, cudaStream_t st) {
 // `chk`; (2) after the caller has read the verdict back, the sliced-ELL part
 // is sized and built, or the error is reported.  One small read-back per
 // system (or per bulk add) replaces two O(nnz) host passes.
+// Allocates a slot's CSR part and queues the copies of its arrays (x stays
+// for the setup kernel to zero when no x0 is given).
 template <typename T>
 int upload_stage(BatchHandle B, int slot, int n, int64_t nnz, const int *rowptr, const int *col, const double *val,
-                 const double *b, const double *x0, CsrCheck *chk, SysDesc<T> *d) {
+                 const double *b, const double *x0, SysDesc<T> *d) {
   cudaStream_t st = B->xfer;
   B_TRY(alloc_csr_part<T>(B, slot, n, nnz, d));
   B_CUDA(cudaMemcpyAsync((void *)d->rowptr, rowptr, sizeof(int) * (n + 1), cudaMemcpyHostToDevice, st));
@@ -1079,10 +1141,6 @@ int upload_stage(BatchHandle B, int slot, int n, int64_t nnz, const int *rowptr,
   }
   B_CUDA(cudaMemcpyAsync((void *)d->b, b, 8 * n, cudaMemcpyHostToDevice, st));
   if (x0) B_CUDA(cudaMemcpyAsync(d->x, x0, 8 * n, cudaMemcpyHostToDevice, st));
-  else B_CUDA(cudaMemsetAsync(d->x, 0, 8 * n, st));
-  const int grid = (int)std::min<int64_t>((n + kBlock - 1) / kBlock, (int64_t)B->ctx->num_sms * 8);
-  csr_check_kernel<<<grid, kBlock, 0, st>>>(n, (int)nnz, d->rowptr, d->col, chk);
-  B_CUDA(cudaGetLastError());
   return B200LA_OK;
 }
 
@@ -1099,21 +1157,32 @@ int finish_stage(BatchHandle B, int slot, const CsrCheck &c, SysDesc<T> &d) {
   const bool col16 = B->prm.index_bits != 32 && c.max_off <= 32767;
   B_TRY(alloc_sell_part<T>(B, slot, std::max(c.max_row, 1), col16, d, B->xfer));
   d.max_off = c.max_off;
-  return finish_slot<T>(B, slot, d, B->xfer);
+  return B200LA_OK;
 }
 
 // Grows the per-batch check records (device and pinned host) to `count`.
+size_t jobs_bytes(int cap) {
+  return align256(sizeof(CheckJob) * cap) + sizeof(SetupJob<double>) * (size_t)cap;
+}
+
 int ensure_checks(BatchHandle B, int count) {
   if (count <= B->chk_cap) return B200LA_OK;
   cudaStream_t st = B->xfer;
   const int cap = std::max(count, 2 * B->chk_cap);
+  // pinned buffers are freed only after the copies queued from them
+  B_CUDA(cudaStreamSynchronize(st));
   if (B->chk) cudaFreeAsync(B->chk, st);
   if (B->chk_host) cudaFreeHost(B->chk_host);
+  if (B->jobs_dev) cudaFreeAsync(B->jobs_dev, st);
+  if (B->jobs_host) cudaFreeHost(B->jobs_host);
   B->chk = nullptr;
   B->chk_host = nullptr;
+  B->jobs_dev = B->jobs_host = nullptr;
   B->chk_cap = 0;
   B_CUDA(cudaMallocAsync(&B->chk, sizeof(CsrCheck) * cap, st));
   B_CUDA(cudaMallocHost(&B->chk_host, sizeof(CsrCheck) * cap));
+  B_CUDA(cudaMallocAsync(&B->jobs_dev, jobs_bytes(cap), st));
+  B_CUDA(cudaMallocHost(&B->jobs_host, jobs_bytes(cap)));
   B->chk_cap = cap;
   return B200LA_OK;
 }
@@ -1532,8 +1601,7 @@ int add_many_t(BatchHandle B, int count, const int *n, const int64_t *nnz, const
     h.n = n[k];
     h.nnz = (int)nnz[k];
     h.used = true;  // reserved while its copies and check are in flight
-    rc = upload_stage<T>(B, slot, n[k], nnz[k], rowptr[k], col[k], val[k], rhs[k], x0 ? x0[k] : nullptr,
-                         B->chk + k, &d[k]);
+    rc = upload_stage<T>(B, slot, n[k], nnz[k], rowptr[k], col[k], val[k], rhs[k], x0 ? x0[k] : nullptr, &d[k]);
     if (rc != B200LA_OK) {
       free_slot_memory(B, h);
       h = HostSys();
@@ -1542,8 +1610,25 @@ int add_many_t(BatchHandle B, int count, const int *n, const int64_t *nnz, const
     }
     sl[k] = slot;
   }
+  // one check kernel over every uploaded system (the previous add's copies
+  // out of the staging buffer finished at its wait below)
+  CheckJob *cj = (CheckJob *)B->jobs_host;
+  int max_n = 1;
+  for (int k = 0; k < count; ++k) {
+    cj[k] = sl[k] < 0 ? CheckJob{nullptr, nullptr, 0, 0} : CheckJob{d[k].rowptr, d[k].col, d[k].n, d[k].nnz};
+    if (sl[k] >= 0) max_n = std::max(max_n, d[k].n);
+  }
+  B_CUDA(cudaMemcpyAsync(B->jobs_dev, cj, sizeof(CheckJob) * count, cudaMemcpyHostToDevice, st));
+  {
+    const dim3 grid((unsigned)std::min((max_n + kBlock - 1) / kBlock, 64), (unsigned)std::min(count, 65535));
+    csr_check_many_kernel<<<grid, kBlock, 0, st>>>((const CheckJob *)B->jobs_dev, count, B->chk);
+    B_CUDA(cudaGetLastError());
+  }
   B_CUDA(cudaMemcpyAsync(B->chk_host, B->chk, sizeof(CsrCheck) * count, cudaMemcpyDeviceToHost, st));
   B_CUDA(cudaStreamSynchronize(st));
+  SetupJob<T> *sj = (SetupJob<T> *)((char *)B->jobs_host + align256(sizeof(CheckJob) * B->chk_cap));
+  int nsetup = 0;
+  max_n = 1;
   for (int k = 0; k < count; ++k) {
     if (sl[k] < 0) continue;
     HostSys &h = B->sys[sl[k]];
@@ -1554,8 +1639,26 @@ int add_many_t(BatchHandle B, int count, const int *n, const int64_t *nnz, const
       note(k, rc);
       continue;
     }
+    desc_of<T>(h) = d[k];
+    SysState &s0 = B->st_host[sl[k]];
+    memset(&s0, 0, sizeof(SysState));
+    s0.phase = PH_RESID;
+    s0.bad_row = 0xffffffffu;
+    sj[nsetup++] = SetupJob<T>{d[k], sl[k], (x0 && x0[k]) ? 0 : 1};
+    max_n = std::max(max_n, d[k].n);
     B->device_bytes += (int64_t)h.bytes;
     slots[k] = sl[k];
+  }
+  if (nsetup) {
+    // descriptors, fresh states, sliced-ELL copies, inverse diagonals and
+    // zero vectors of every added system in two launches
+    void *sj_dev = (char *)B->jobs_dev + align256(sizeof(CheckJob) * B->chk_cap);
+    B_CUDA(cudaMemcpyAsync(sj_dev, sj, sizeof(SetupJob<T>) * nsetup, cudaMemcpyHostToDevice, st));
+    slot_init_many_kernel<T><<<(nsetup + kBlock - 1) / kBlock, kBlock, 0, st>>>(
+        (const SetupJob<T> *)sj_dev, nsetup, (SysDesc<T> *)B->desc, B->st);
+    const dim3 grid((unsigned)std::min((max_n + 32 + kBlock - 1) / kBlock, 256), (unsigned)std::min(nsetup, 65535));
+    slot_setup_many_kernel<T><<<grid, kBlock, 0, st>>>((const SetupJob<T> *)sj_dev, nsetup, B->st);
+    B_CUDA(cudaGetLastError());
   }
   // later work on the context stream (runs, results, removals) follows the add
   B_CUDA(cudaEventRecord(B->xfer_done, st));
@@ -1589,8 +1692,10 @@ int b200la_batch_destroy(b200la_batch B) {
     if (L.dev) cudaFreeAsync(L.dev, st);
     if (L.part) cudaFreeAsync(L.part, st);
   }
+  if (B->jobs_dev) cudaFreeAsync(B->jobs_dev, st);
   if (B->st_host) cudaFreeHost(B->st_host);
   if (B->chk_host) cudaFreeHost(B->chk_host);
+  if (B->jobs_host) cudaFreeHost(B->jobs_host);
   if (B->glob_host) cudaFreeHost(B->glob_host);
   cudaStreamSynchronize(st);
   if (B->xfer_done) cudaEventDestroy(B->xfer_done);
