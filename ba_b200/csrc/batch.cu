@@ -1453,27 +1453,32 @@ int time_passes_t(BatchHandle B, int reps, double ms[3]) {
   const PassLists L = pass_lists(B);
   batch_start_kernel<<<1, 1, 0, st>>>(B->glob);
   launch_pass<T, PRE, false>(B, grids, st, 0);
-  cudaEvent_t ev[4];
+  // every timed pass is queued before the wait (behind the untimed pass
+  // above), so the kernels run back to back and no host launch gap falls
+  // between an event pair
+  std::vector<cudaEvent_t> ev((size_t)reps * 4);
   for (auto &e : ev) B_CUDA(cudaEventCreate(&e));
   double acc[3] = {0.0, 0.0, 0.0};
   int rc = B200LA_OK;
-  for (int r = 0; r < reps && rc == B200LA_OK; ++r) {
-    cudaEventRecord(ev[0], st);
+  for (int r = 0; r < reps; ++r) {
+    cudaEvent_t *e = &ev[(size_t)r * 4];
+    cudaEventRecord(e[0], st);
     batch_spmv_kernel<T, PRE><<<grids[0], kBlock, 0, st>>>(L, desc, B->st, B->glob, B->kp);
-    cudaEventRecord(ev[1], st);
+    cudaEventRecord(e[1], st);
     batch_update_kernel<T, PRE><<<grids[1], kBlock, 0, st>>>(L, desc, B->st, B->glob, B->kp);
-    cudaEventRecord(ev[2], st);
+    cudaEventRecord(e[2], st);
     batch_direction_kernel<T, PRE, false><<<grids[2], kBlock, 0, st>>>(L, desc, B->st, B->glob, B->kp, 0);
-    cudaEventRecord(ev[3], st);
-    if (cudaEventSynchronize(ev[3]) != cudaSuccess) {
-      rc = fail(B200LA_ERR_CUDA, "batch pass timing: %s", cudaGetErrorString(cudaGetLastError()));
-      break;
-    }
-    for (int k = 0; k < 3; ++k) {
-      float t = 0.f;
-      cudaEventElapsedTime(&t, ev[k], ev[k + 1]);
-      acc[k] += t;
-    }
+    cudaEventRecord(e[3], st);
+  }
+  if (cudaStreamSynchronize(st) != cudaSuccess) {
+    rc = fail(B200LA_ERR_CUDA, "batch pass timing: %s", cudaGetErrorString(cudaGetLastError()));
+  } else {
+    for (int r = 0; r < reps; ++r)
+      for (int k = 0; k < 3; ++k) {
+        float t = 0.f;
+        cudaEventElapsedTime(&t, ev[(size_t)r * 4 + k], ev[(size_t)r * 4 + k + 1]);
+        acc[k] += t;
+      }
   }
   for (auto &e : ev) cudaEventDestroy(e);
   B_TRY(rc);

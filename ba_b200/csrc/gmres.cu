@@ -24,6 +24,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <vector>
 
 #include "internal.cuh"
 #include "krylov.cuh"
@@ -751,32 +752,38 @@ static int gm_profile_t(GmresState *s, const void *b_dev, const void *x_dev, int
   cudaStream_t st = s->A->ctx->stream;
   B_TRY(gm_begin_t<T>(s, b_dev, x_dev));
   const GmBufs<T> v = gm_bufs<T>(s);
-  cudaEvent_t ev[5];
+  // every pass is queued before the first wait, so the timed kernels run
+  // back to back and no host launch gap falls between an event pair (the
+  // first pass starts behind the start kernel)
+  std::vector<cudaEvent_t> ev((size_t)(passes > 0 ? passes : 0) * 5);
   for (auto &e : ev) B_CUDA(cudaEventCreate(&e));
   float acc[4] = {0.f, 0.f, 0.f, 0.f};
   int rc = B200LA_OK;
   for (int it = 0; it < passes && rc == B200LA_OK; ++it) {
-    cudaEventRecord(ev[0], st);
+    cudaEvent_t *e = &ev[(size_t)it * 5];
+    cudaEventRecord(e[0], st);
     gm_update_kernel<T, PRE><<<s->grid_ew, kBlock, 0, st>>>(v, s->sc);
-    cudaEventRecord(ev[1], st);
+    cudaEventRecord(e[1], st);
     rc = with_schedule<T>(s->A, [&](auto op) -> int {
       using Op = decltype(op);
       gm_restart_kernel<Op, T, PRE><<<s->grid_restart, kBlock, 0, st>>>(op, v, s->part, s->sc);
-      cudaEventRecord(ev[2], st);
+      cudaEventRecord(e[2], st);
       gm_spmv_kernel<Op, T, PRE><<<s->grid_spmv, kBlock, 0, st>>>(op, v, s->part3, s->sc);
-      cudaEventRecord(ev[3], st);
+      cudaEventRecord(e[3], st);
       return B200LA_OK;
     });
     if (rc == B200LA_OK) rc = gm_launch_arnoldi<T, PRE, false>(s, st, 0);
-    cudaEventRecord(ev[4], st);
-    B_CUDA(cudaEventSynchronize(ev[4]));
+    cudaEventRecord(e[4], st);
+  }
+  const cudaError_t se = cudaStreamSynchronize(st);
+  for (int it = 0; it < passes && rc == B200LA_OK && se == cudaSuccess; ++it)
     for (int k = 0; k < 4; ++k) {
       float t = 0.f;
-      cudaEventElapsedTime(&t, ev[k], ev[k + 1]);
+      cudaEventElapsedTime(&t, ev[(size_t)it * 5 + k], ev[(size_t)it * 5 + k + 1]);
       acc[k] += t;
     }
-  }
   for (auto &e : ev) cudaEventDestroy(e);
+  B_CUDA(se);
   B_CUDA(cudaGetLastError());
   for (int k = 0; k < 4; ++k) ms[k] = passes > 0 ? acc[k] / passes : 0.0;
   return rc;

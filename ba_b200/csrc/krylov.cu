@@ -34,6 +34,7 @@
 // direction is stored as q = P p, so A P p is one SpMV of q.
 #include <cmath>
 #include <cstring>
+#include <vector>
 
 #include "internal.cuh"
 #include "krylov.cuh"
@@ -525,42 +526,51 @@ static int solver_profile_t(b200la_solver s, const void *b_dev, const void *x_de
   const bool jac = s->prm.method == B200LA_METHOD_JACOBI;
   const int nk = jac ? 1 : 5;
   const BiVecs<T> v = bi_vecs<T>(s);
-  cudaEvent_t ev[6];
+  // every pass is queued before the first wait, after one untimed pass, so
+  // the timed kernels run back to back and no host launch gap falls between
+  // an event pair
+  const int ne = nk + 1;
+  std::vector<cudaEvent_t> ev((size_t)(passes > 0 ? passes : 0) * ne);
   for (auto &e : ev) B_CUDA(cudaEventCreate(&e));
   float acc[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
   int rc = B200LA_OK;
-  for (int it = 0; it < passes && rc == B200LA_OK; ++it) {
-    cudaEventRecord(ev[0], st);
-    rc = with_schedule<T>(A, [&](auto op) -> int {
+  auto pass = [&](cudaEvent_t *e) -> int {
+    if (e) cudaEventRecord(e[0], st);
+    B_TRY(with_schedule<T>(A, [&](auto op) -> int {
       using Op = decltype(op);
       if (jac) {
         jacobi_sweep_kernel<Op, T, false><<<s->grid_spmv, kBlock, 0, st>>>(
             op, (T *)s->v[0], (T *)s->v[1], (const T *)s->bown, (const T *)s->invd, s->part, s->sc, 0);
-        cudaEventRecord(ev[1], st);
+        if (e) cudaEventRecord(e[1], st);
         return B200LA_OK;
       }
       bicg_spmv_q_kernel<Op, T, PRE><<<s->grid_spmv, kBlock, 0, st>>>(op, v, s->part, s->sc);
-      cudaEventRecord(ev[1], st);
+      if (e) cudaEventRecord(e[1], st);
       bicg_s_kernel<T, PRE><<<s->grid_ew, kBlock, 0, st>>>(v, s->part, s->sc);
-      cudaEventRecord(ev[2], st);
+      if (e) cudaEventRecord(e[2], st);
       bicg_spmv_s_kernel<Op, T, PRE><<<s->grid_spmv, kBlock, 0, st>>>(op, v, s->part, s->sc);
-      cudaEventRecord(ev[3], st);
+      if (e) cudaEventRecord(e[3], st);
       return B200LA_OK;
-    });
+    }));
     if (!jac) {
       bicg_update_kernel<T, PRE><<<s->grid_ew, kBlock, 0, st>>>(v, s->part, s->sc);
-      cudaEventRecord(ev[4], st);
+      if (e) cudaEventRecord(e[4], st);
       bicg_direction_kernel<T, PRE, false><<<s->grid_ew, kBlock, 0, st>>>(v, s->sc, 0);
-      cudaEventRecord(ev[5], st);
+      if (e) cudaEventRecord(e[5], st);
     }
-    B_CUDA(cudaEventSynchronize(ev[nk]));
+    return B200LA_OK;
+  };
+  if (passes > 0) rc = pass(nullptr);
+  for (int it = 0; it < passes && rc == B200LA_OK; ++it) rc = pass(&ev[(size_t)it * ne]);
+  const cudaError_t se = cudaStreamSynchronize(st);
+  for (int it = 0; it < passes && rc == B200LA_OK && se == cudaSuccess; ++it)
     for (int k = 0; k < nk; ++k) {
       float t = 0.f;
-      cudaEventElapsedTime(&t, ev[k], ev[k + 1]);
+      cudaEventElapsedTime(&t, ev[(size_t)it * ne + k], ev[(size_t)it * ne + k + 1]);
       acc[k] += t;
     }
-  }
   for (auto &e : ev) cudaEventDestroy(e);
+  B_CUDA(se);
   B_CUDA(cudaGetLastError());
   for (int k = 0; k < nk; ++k) ms[k] = passes > 0 ? acc[k] / passes : 0.0;
   return rc;
