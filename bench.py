@@ -372,6 +372,7 @@ def run_batch(args, rank, local_rank, world, torch, dist, barrier):
     # roofline of the dominant kernel: K1 of the inner solve (batched FP32
     # sliced-ELL SpMV fused with p.Ap), timed launch by launch with CUDA
     # events on the solve stream over a full inner pass of every system
+    B.profile_pass(5)  # warms the GPU up after the host-bound e2e loop
     pass_ms, pass_bytes = B.profile_pass(5)
     spmv_ms, spmv_bytes_alg = pass_ms[0], pass_bytes[0]
     peak, peak_kind = measured_peak_gbs()
@@ -714,8 +715,9 @@ def run_poisson3d(args, rank, local_rank, world, torch, dist, barrier):
     h1.synchronize()
     e2e_value = D.aggregate_rate(args.steps, world, D.max_over_ranks(h0.elapsed_time(h1)))
     ms3 = (C.c_double * 3)()
-    x.Zeros()
-    lib.b200la_cg_profile(solver._solver, b.handle, x.handle, 20, ms3)
+    for _ in range(2):  # the first call warms the GPU up after the host-bound e2e loop
+        x.Zeros()
+        lib.b200la_cg_profile(solver._solver, b.handle, x.handle, 20, ms3)
     bytes_spmv = spmv_bytes(n, nnz, 8)
     peak, peak_kind = measured_peak_gbs()
     achieved = bytes_spmv / (ms3[0] / 1e3) / 1e9
@@ -886,7 +888,9 @@ def run_varcoef3d(args, rank, local_rank, world, torch, dist, barrier):
     sv32.SetupOperator(A32)
     sv32._ensure()
     ms3 = (C.c_double * 3)()
-    lib.b200la_cg_profile(sv32._solver, b32.handle, x32.handle, 20, ms3)
+    for _ in range(2):  # the first call warms the GPU up after the host-bound e2e loop
+        x32.Zeros()
+        lib.b200la_cg_profile(sv32._solver, b32.handle, x32.handle, 20, ms3)
     bytes_spmv = spmv_bytes(n, nnz, 4)
     peak, peak_kind = measured_peak_gbs()
     achieved = bytes_spmv / (ms3[0] / 1e3) / 1e9
@@ -1065,8 +1069,9 @@ def run_bicgstab(args, rank, local_rank, world, torch, dist, barrier):
     iters = solver.iter()
     value = D.aggregate_rate(args.steps, world, ms_max)
     e2e_value = D.aggregate_rate(args.steps, world, _timed_e2e(args, stream, torch, barrier, b, x, n, step))
-    x.Zeros()
-    ms = solver.profile(b, x, 20)
+    for _ in range(2):  # the first call warms the GPU up after the host-bound e2e loop
+        x.Zeros()
+        ms = solver.profile(b, x, 20)
     bytes_b1 = spmv_bytes(n, nnz, 8) + n * 8
     peak, peak_kind = measured_peak_gbs()
     achieved = bytes_b1 / (ms[0] / 1e3) / 1e9
@@ -1118,8 +1123,9 @@ def run_jacobi(args, rank, local_rank, world, torch, dist, barrier):
     value = D.aggregate_rate(args.steps * JACOBI_SWEEPS, world, ms_max)
     e2e_value = D.aggregate_rate(args.steps * JACOBI_SWEEPS, world,
                                  _timed_e2e(args, stream, torch, barrier, b, x, n, step))
-    x.Zeros()
-    ms = j.profile(b, x, 20)
+    for _ in range(2):  # the first call warms the GPU up after the host-bound e2e loop
+        x.Zeros()
+        ms = j.profile(b, x, 20)
     bytes_sweep = spmv_bytes(n, nnz, 8) + 2 * n * 8
     peak, peak_kind = measured_peak_gbs()
     achieved = bytes_sweep / (ms[0] / 1e3) / 1e9
