@@ -279,3 +279,33 @@ def test_adds_overlapping_launches_match_the_plain_solve(plat):
         assert g.solver_state == lmp.kSolverSuccess, (k, g)
         assert (g.iters, g.outer) == (r.iters, r.outer)
         np.testing.assert_array_equal(g.x, r.x)
+
+
+def test_initial_guesses_in_one_add_many(plat):
+    # one add_many call mixing systems with an initial guess (copied to x) and
+    # without (x zeroed by the setup kernel): the latter repeat a plain run bit
+    # for bit, the former start from their guess (res_init is its residual)
+    # and reach the tolerance relative to it
+    sizes = P.batch_sizes(8, lo=16, hi=48, seed=9)
+    systems = [P.q1_system(2, int(n), 900 + k, 1.0, f"g{k}") for k, n in enumerate(sizes)]
+    kw = dict(mixed=True, precond=True, rtol=1e-8, inner_rtol=1e-4, platform=plat)
+    A = Batch(8, **kw)
+    sa = A.add_many([(s.rowptr, s.col, s.val, s.b) for s in systems])
+    A.solve(16)
+    ra = A.results(sa)
+    guesses = [r.x * (1.0 + 1e-3) if k % 2 == 0 else None for k, r in enumerate(ra)]
+    B = Batch(8, **kw)
+    sb = B.add_many([(s.rowptr, s.col, s.val, s.b, g) for s, g in zip(systems, guesses)])
+    B.solve(16)
+    rb = B.results(sb)
+    for k, (s, a, b, g) in enumerate(zip(systems, ra, rb, guesses)):
+        assert b.done and b.solver_state == lmp.kSolverSuccess, (s.name, b)
+        if g is None:
+            assert b.iters == a.iters and np.array_equal(b.x, a.x), s.name
+            continue
+        r0 = np.linalg.norm(s.b - oracle.spmv(s.rowptr, s.col, s.val, g))
+        assert abs(b.res_init - r0) <= 1e-9 * r0, (s.name, b.res_init, r0)
+        assert b.res_init < 1e-2 * a.res_init
+        assert np.linalg.norm(s.b - oracle.spmv(s.rowptr, s.col, s.val, b.x)) <= 1.0001e-8 * r0, s.name
+    A.close()
+    B.close()
