@@ -7,10 +7,12 @@
 // duplicates (and, being a selection sort with swaps, does not keep them in
 // input order).  Here the same result comes from:
 //   1. a device check of every index (a bad triplet fails the upload),
-//   2. a stable radix sort of the triplets by row (input order kept within a
-//      row, as the reference's scatter keeps it),
+//   2. a stable radix sort of the triplets by row carrying (column, input
+//      position) pairs (input order kept within a row, as the reference's
+//      scatter keeps it),
 //   3. row offsets from the sorted rows (each row boundary writes its range),
-//   4. a gather of columns and values (cast to the storage type),
+//   4. a gather of the values from their input positions (cast to the
+//      storage type), the columns coming with the sorted pairs,
 //   5. the row sort, one warp per row: ranks by shuffles when the row's
 //      columns are distinct (the sorted row is then unique), the
 //      reference's selection sort itself when a column repeats or the row
@@ -36,9 +38,12 @@ __global__ void coo_check_kernel(int64_t nnz, int nrow, int ncol, const int *__r
   }
 }
 
-__global__ void iota_kernel(int64_t n, int *out) {
+// Sort payload of each triplet: its column in the high word and its input
+// position in the low word, so that the sort carries the column along and
+// the gather reads only the value from a random position.
+__global__ void coo_pack_kernel(int64_t n, const int *__restrict__ cols, unsigned long long *out) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    out[i] = (int)i;
+    out[i] = ((unsigned long long)(unsigned)cols[i] << 32) | (unsigned long long)(unsigned)i;
 }
 
 // rowptr from the rows sorted ascending: entry i starts rows prev+1 .. r.
@@ -77,33 +82,28 @@ __device__ void row_selection_sort(int k, int b, int e, int *col, T *val, int *d
   diag[k] = d;
 }
 
-// Gather of columns and values into the row-sorted order (cast to the
-// storage type).  The source positions are random, so each thread keeps
-// kGatherUnroll independent loads in flight.
+// Columns and values into the row-sorted order: the column comes with the
+// sorted payload, the value (cast to the storage type) from its input
+// position, a random read; each thread keeps kGatherUnroll of those in flight.
 constexpr int kGatherUnroll = 4;
 
 template <typename T, typename S>
-__global__ void __launch_bounds__(kBlock) coo_gather_kernel(int64_t nnz, const int *__restrict__ perm,
-                                                            const int *__restrict__ cols, const S *__restrict__ vals,
-                                                            int *col, T *val) {
+__global__ void __launch_bounds__(kBlock) coo_gather_kernel(int64_t nnz, const unsigned long long *__restrict__ packed,
+                                                            const S *__restrict__ vals, int *col, T *val) {
   constexpr int U = kGatherUnroll;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t k0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k0 < nnz; k0 += U * stride) {
-    int p[U];
+    unsigned long long q[U];
 #pragma unroll
-    for (int u = 0; u < U; ++u) p[u] = k0 + u * stride < nnz ? perm[k0 + u * stride] : -1;
-    int cc[U];
+    for (int u = 0; u < U; ++u) q[u] = k0 + u * stride < nnz ? packed[k0 + u * stride] : 0ull;
     S vv[U];
 #pragma unroll
     for (int u = 0; u < U; ++u)
-      if (p[u] >= 0) {
-        cc[u] = cols[p[u]];
-        vv[u] = vals[p[u]];
-      }
+      if (k0 + u * stride < nnz) vv[u] = vals[(unsigned)q[u]];
 #pragma unroll
     for (int u = 0; u < U; ++u)
-      if (p[u] >= 0) {
-        col[k0 + u * stride] = cc[u];
+      if (k0 + u * stride < nnz) {
+        col[k0 + u * stride] = (int)(q[u] >> 32);
         val[k0 + u * stride] = (T)vv[u];
       }
   }
@@ -262,7 +262,8 @@ extern "C" int b200la_coo_upload(b200la_ctx c, int nrow, int ncol, int64_t nnz, 
   const size_t nz = (size_t)(nnz > 0 ? nnz : 1);
   const size_t vsz = dtype_size(val_dtype);
   // scratch: device triplets (when given host arrays), sorted rows, permutation
-  int *d_rows = nullptr, *d_cols = nullptr, *srow = nullptr, *idx = nullptr, *perm = nullptr;
+  int *d_rows = nullptr, *d_cols = nullptr, *srow = nullptr;
+  unsigned long long *idx = nullptr, *perm = nullptr;  // sort payload in and out
   void *d_vals = nullptr, *cub_tmp = nullptr;
   unsigned long long *bad = nullptr;
   int *max_row_d = nullptr, *n_long_d = nullptr, *long_rows = nullptr;
@@ -324,10 +325,10 @@ extern "C" int b200la_coo_upload(b200la_ctx c, int nrow, int ncol, int64_t nnz, 
     }
     // stable sort by row: keys rows, values input positions
     if (!cu(cudaMallocAsync(&srow, sizeof(int) * nz, s), "allocation") ||
-        !cu(cudaMallocAsync(&idx, sizeof(int) * nz, s), "allocation") ||
-        !cu(cudaMallocAsync(&perm, sizeof(int) * nz, s), "allocation"))
+        !cu(cudaMallocAsync(&idx, sizeof(unsigned long long) * nz, s), "allocation") ||
+        !cu(cudaMallocAsync(&perm, sizeof(unsigned long long) * nz, s), "allocation"))
       break;
-    iota_kernel<<<g, kBlock, 0, s>>>(nnz, idx);
+    coo_pack_kernel<<<g, kBlock, 0, s>>>(nnz, c_in, idx);
     size_t tmp_bytes = 0;
     const int end_bit = bits_for(nrow);
     if (!cu(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, r_in, srow, idx, perm, (int)nnz, 0, end_bit, s),
@@ -339,17 +340,17 @@ extern "C" int b200la_coo_upload(b200la_ctx c, int nrow, int ncol, int64_t nnz, 
     coo_rowptr_kernel<<<grid_1d(c, nnz + 1), kBlock, 0, s>>>(nnz, nrow, srow, m->rowptr);
     if (dtype == B200LA_F64) {
       if (val_dtype == B200LA_F64)
-        coo_gather_kernel<double, double><<<g, kBlock, 0, s>>>(nnz, perm, c_in, (const double *)v_in, m->col,
+        coo_gather_kernel<double, double><<<g, kBlock, 0, s>>>(nnz, perm, (const double *)v_in, m->col,
                                                                (double *)m->val);
       else
-        coo_gather_kernel<double, float><<<g, kBlock, 0, s>>>(nnz, perm, c_in, (const float *)v_in, m->col,
+        coo_gather_kernel<double, float><<<g, kBlock, 0, s>>>(nnz, perm, (const float *)v_in, m->col,
                                                               (double *)m->val);
     } else {
       if (val_dtype == B200LA_F64)
-        coo_gather_kernel<float, double><<<g, kBlock, 0, s>>>(nnz, perm, c_in, (const double *)v_in, m->col,
+        coo_gather_kernel<float, double><<<g, kBlock, 0, s>>>(nnz, perm, (const double *)v_in, m->col,
                                                               (float *)m->val);
       else
-        coo_gather_kernel<float, float><<<g, kBlock, 0, s>>>(nnz, perm, c_in, (const float *)v_in, m->col,
+        coo_gather_kernel<float, float><<<g, kBlock, 0, s>>>(nnz, perm, (const float *)v_in, m->col,
                                                              (float *)m->val);
     }
     if (nrow > 0) {
