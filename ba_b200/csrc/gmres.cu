@@ -45,13 +45,13 @@ struct GmScalars {
   int phase;         // kGmRestart / kGmStep / kGmUpdate / kGmDone
   int maxits;
   int guard;         // body passes
-  // G4's grid barrier: arrivals, generation (polled by the waiters) and
-  // error flag, each on its own 128-byte line
-  alignas(128) unsigned arrive;
-  alignas(128) unsigned gen;
-  alignas(128) unsigned err;
+  alignas(128) unsigned err;  // a G4 barrier wait ran out
   unsigned ticket[2];
   int stall_block;            // test hook: this block of the resident G4 never reaches its barrier (-1: none)
+  // G4's grid barrier: arrivals since the solve started (own line) and the
+  // barriers its launches have passed (written by block 0 at the end)
+  alignas(128) unsigned long long bar_count;
+  unsigned long long bar_done;
 };
 
 enum { kGmRestart = 0, kGmStep = 1, kGmUpdate = 2, kGmDone = 3 };
@@ -315,6 +315,7 @@ __global__ void __launch_bounds__(kBlock) gm_arnoldi_kernel(GmBufs<T> v, const d
   }
   const int j = __ldg(&sc->j);
   const int m = __ldg(&sc->m), ldh = m + 1;
+  const unsigned long long bar0 = __ldg(&sc->bar_done);
   T *vj1 = v.V + (int64_t)(j + 1) * v.ldv;
   // h_0j from G3's partials; then for each i: w -= h_ij V_i, fused with the
   // next dot (w.V_{i+1}, or w.w after the last i)
@@ -342,7 +343,7 @@ __global__ void __launch_bounds__(kBlock) gm_arnoldi_kernel(GmBufs<T> v, const d
     block_sum<1>(s, red);
     double *slot = part4 + (i & 1) * gridDim.x;
     if (threadIdx.x == 0) slot[blockIdx.x] = s[0];
-    if (!grid_barrier(&sc->arrive, &sc->gen, &sc->err)) {
+    if (!grid_barrier_count(&sc->bar_count, (bar0 + (unsigned long long)i + 1ull) * gridDim.x, &sc->err)) {
       gm_abort<IN_GRAPH>(sc, loop);
       return;
     }
@@ -365,6 +366,7 @@ __global__ void __launch_bounds__(kBlock) gm_arnoldi_kernel(GmBufs<T> v, const d
     if (PRE) st<C>(v.z + e, d);
   });
   if (blockIdx.x != 0) return;
+  if (threadIdx.x == 0) sc->bar_done = bar0 + (unsigned long long)j + 1ull;
   gm_step_end<IN_GRAPH>(v.H, v.g, v.cs, v.sn, v.y, sc, j, m, (double)hn, loop);
 }
 
@@ -414,6 +416,7 @@ __global__ void __launch_bounds__(kResBlock, 1) gm_arnoldi_res_kernel(GmBufs<T> 
   const int64_t nv = len / W;               // whole chunks; elements nv W .. len-1 are the tail
   const int64_t bd = blockDim.x;
   const bool stall = (int)blockIdx.x == __ldg(&sc->stall_block);
+  const unsigned long long bar0 = __ldg(&sc->bar_done);
   prefetch_slice_l2(v.V + lo, len);
   if (j > 0) prefetch_slice_l2(v.V + v.ldv + lo, len);
   // w's slice into shared memory
@@ -470,7 +473,7 @@ __global__ void __launch_bounds__(kResBlock, 1) gm_arnoldi_res_kernel(GmBufs<T> 
     double *slot = part4 + (i & 1) * gridDim.x;
     if (threadIdx.x == 0) slot[blockIdx.x] = s[0];
     if (stall) return;  // test hook: this block never reaches the barrier
-    if (!grid_barrier(&sc->arrive, &sc->gen, &sc->err)) {
+    if (!grid_barrier_count(&sc->bar_count, (bar0 + (unsigned long long)i + 1ull) * gridDim.x, &sc->err)) {
       gm_abort<IN_GRAPH>(sc, loop);
       return;
     }
@@ -509,6 +512,9 @@ __global__ void __launch_bounds__(kResBlock, 1) gm_arnoldi_res_kernel(GmBufs<T> 
     if (PRE) v.z[lo + e] = wv * v.invd[lo + e];
   }
   if (blockIdx.x != 0) return;
+  // every block read bar_done at its start, and block 0 gets here only after
+  // all arrived at barrier j
+  if (threadIdx.x == 0) sc->bar_done = bar0 + (unsigned long long)j + 1ull;
   gm_step_end<IN_GRAPH>(v.H, v.g, v.cs, v.sn, v.y, sc, j, m, (double)hn, loop);
 }
 

@@ -47,17 +47,8 @@ template <int C, typename T> __device__ __forceinline__ void st(T *p, const T (&
   }
 }
 
-// Grid-wide barrier for kernels launched cooperatively (all blocks resident).
-// Sense by generation: a block's thread 0 reads the generation, arrives on
-// the counter, and the last to arrive resets the counter and advances the
-// generation; the others wait for the generation to move.  The waiters poll
-// with plain (relaxed) loads, not atomics, so the arrivals' atomics do not
-// queue behind them; callers keep arrive, gen and err on separate 128-byte
-// lines.  Every wait is bounded: after kSpinLimit polls (a few seconds at
-// most) the waiter sets *err and the call returns false in every thread of
-// the block; a waiter also gives up when another block has set *err (checked
-// every 64 polls).  Callers end the kernel when it returns false.  Must be
-// called by every thread of every block.
+// Bound on every spin-wait of the cooperative kernels: after kSpinLimit
+// polls (a few seconds at most) a waiter gives up and reports an error.
 constexpr long long kSpinLimit = 1LL << 22;
 
 __device__ __forceinline__ unsigned ld_relaxed_u32(const unsigned *p) {
@@ -66,22 +57,33 @@ __device__ __forceinline__ unsigned ld_relaxed_u32(const unsigned *p) {
   return v;
 }
 
-__device__ __forceinline__ bool grid_barrier(unsigned *arrive, unsigned *gen, unsigned *err) {
+// Grid-wide barrier on a monotonic 64-bit arrival counter, for kernels
+// launched cooperatively that pass several barriers: every block's thread 0
+// adds one and waits (relaxed loads) until the counter reaches `target` =
+// gridDim.x times the barriers passed so far including this one, so the last
+// arrival itself releases the waiters (no reset, no second counter).  Callers
+// derive `target` from a count that all blocks read alike (e.g. kept in
+// device memory by the previous launch) and zero the counter when that count
+// restarts.  Waits are bounded (kSpinLimit polls, *err checked every 64);
+// returns false in every thread of the block after a timeout or when *err is
+// set, and the caller ends the kernel.  Must be called by every thread of
+// every block.
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long *p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ bool grid_barrier_count(unsigned long long *count, unsigned long long target,
+                                                   unsigned *err) {
   __shared__ bool ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     bool good = true;
-    // a block passed the previous barrier only after seeing this generation,
-    // so the read cannot return an older one
-    const unsigned g = ld_relaxed_u32(gen);
     __threadfence();
-    if (atomicAdd(arrive, 1u) == gridDim.x - 1) {
-      atomicExch(arrive, 0u);
-      __threadfence();
-      atomicAdd(gen, 1u);
-    } else {
+    if (atomicAdd(count, 1ull) + 1ull < target) {
       long long spins = 0;
-      while (ld_relaxed_u32(gen) == g) {
+      while (ld_relaxed_u64(count) < target) {
         ++spins;
         if (spins > kSpinLimit || ((spins & 63) == 0 && ld_relaxed_u32(err) != 0u)) {
           atomicExch(err, 1u);
