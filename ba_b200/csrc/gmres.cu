@@ -388,6 +388,58 @@ __global__ void __launch_bounds__(kBlock) gm_arnoldi_kernel(GmBufs<T> v, const d
 constexpr int kResBlock = 1024;
 constexpr int kResUnroll = 2;
 
+// The end of one projection in the resident kernel: the block's partial
+// (the threads' v summed) goes to set[blockIdx.x]; after the grid barrier
+// warp 0 adds the gridDim partials in the same order in every block (lane l:
+// blocks l, l + 32, ..., then a shuffle tree), so all blocks hold the same
+// total.  Two block barriers in all (the block sum, the barrier wait and the
+// re-read of the partials each took their own before).  Returns false in
+// every thread when a wait ran out.
+__device__ __forceinline__ bool projection_total(double v, double *set, unsigned long long *count,
+                                                 unsigned long long target, unsigned *err, double *out) {
+  __shared__ double red[32];
+  __shared__ double tot;
+  __shared__ int okf;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  v = warp_sum(v);
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  if (warp == 0) {
+    double t = warp_sum(lane < nw ? red[lane] : 0.0);
+    int good = 1;
+    if (lane == 0) {
+      set[blockIdx.x] = t;
+      __threadfence();
+      if (atomicAdd(count, 1ull) + 1ull < target) {
+        long long spins = 0;
+        while (ld_relaxed_u64(count) < target) {
+          ++spins;
+          if (spins > kSpinLimit || ((spins & 63) == 0 && ld_relaxed_u32(err) != 0u)) {
+            atomicExch(err, 1u);
+            good = 0;
+            break;
+          }
+          __nanosleep(32);
+        }
+      }
+      __threadfence();
+    }
+    good = __shfl_sync(0xffffffffu, good, 0);
+    double a = 0.0;
+    if (good) {
+      for (int b = lane; b < (int)gridDim.x; b += 32) a += __ldcg(set + b);
+      a = warp_sum(a);
+    }
+    if (lane == 0) {
+      tot = a;
+      okf = good;
+    }
+  }
+  __syncthreads();
+  *out = tot;
+  return okf != 0;
+}
+
 template <typename T>
 __device__ __forceinline__ void prefetch_slice_l2(const T *p, int64_t len) {
   const char *c = reinterpret_cast<const char *>(p);
@@ -403,7 +455,6 @@ __global__ void __launch_bounds__(kResBlock, 1) gm_arnoldi_res_kernel(GmBufs<T> 
   constexpr int W = Vec16<T>::n, U = kResUnroll;
   extern __shared__ __align__(16) unsigned char gm_dyn[];
   T *ws = reinterpret_cast<T *>(gm_dyn);
-  __shared__ double red[32];
   const int phase = __ldg(&sc->phase);
   if (phase != kGmStep) {
     gm_idle<IN_GRAPH>(sc, phase, loop);
@@ -468,16 +519,12 @@ __global__ void __launch_bounds__(kResBlock, 1) gm_arnoldi_res_kernel(GmBufs<T> 
       ws[e] = wv;
     }
     if (i + 2 <= j) prefetch_slice_l2(v.V + (int64_t)(i + 2) * v.ldv + lo, len);
-    double s[1] = {acc.value()};
-    block_sum<1>(s, red);
-    double *slot = part4 + (i & 1) * gridDim.x;
-    if (threadIdx.x == 0) slot[blockIdx.x] = s[0];
     if (stall) return;  // test hook: this block never reaches the barrier
-    if (!grid_barrier_count(&sc->bar_count, (bar0 + (unsigned long long)i + 1ull) * gridDim.x, &sc->err)) {
+    if (!projection_total(acc.value(), part4 + (i & 1) * gridDim.x, &sc->bar_count,
+                          (bar0 + (unsigned long long)i + 1ull) * gridDim.x, &sc->err, &h)) {
       gm_abort<IN_GRAPH>(sc, loop);
       return;
     }
-    h = block_total(slot, gridDim.x);
   }
   // V_{j+1} = w / ||w||, z = P V_{j+1}
   const T hn = sqrt((T)h);
