@@ -424,7 +424,7 @@ def run_batch(args, rank, local_rank, world, torch, dist, barrier):
 
 # e2e: upload chunks (largest systems first: the first, small chunk starts the
 # slowest systems after a few ms) and passes per overlapping launch
-E2E_CHUNKS = (32, 64, 128, 256)
+E2E_CHUNKS = (8, 24, 64, 160, 256)
 E2E_LAUNCH_PASSES = 128
 
 
