@@ -52,6 +52,7 @@ class Batch:
         call("b200la_batch_create", self.platform.handle, C.byref(prm), C.byref(self.handle))
         self._keep = {}
         self._sizes = {}
+        self._outs = {}  # registered output arrays, kept alive until read
 
     def add(self, rowptr, col, val, rhs, x0=None) -> int:
         rp = np.ascontiguousarray(rowptr, np.int32)
@@ -127,6 +128,7 @@ class Batch:
         call("b200la_batch_remove", self.handle, int(slot))
         self._keep.pop(slot, None)
         self._sizes.pop(slot, None)
+        self._outs.pop(slot, None)
 
     def run(self, max_passes: int = 1 << 30) -> int:
         active = C.c_int()
@@ -142,8 +144,30 @@ class Batch:
             x = np.empty(self.slot_n(slot), np.float64)
             ptr = x.ctypes.data_as(C.c_void_p)
         call("b200la_batch_result", self.handle, int(slot), ptr, C.byref(r))
+        if with_x:
+            self._outs.pop(int(slot), None)
         return SystemResult(r.state, r.solver_state, r.iters, r.outer, bool(r.phase_done), r.res, r.res_init,
                             r.res_rel, r.device_us, x)
+
+    def set_outputs(self, slots, arrays):
+        """Register float64 host arrays (contiguous, at least n elements; pinned
+        ones keep the copies asynchronous) to receive the slots' solutions as
+        soon as runs see them finished, overlapping the passes still running;
+        `results(slots, out=arrays)` then only waits for those copies.  The
+        arrays are kept alive here until the results are read."""
+        slots = [int(s) for s in slots]
+        arrays = list(arrays)
+        if len(arrays) != len(slots):
+            raise _lib.B200LAError(-1, "set_outputs: one array per slot")
+        for s, a in zip(slots, arrays):
+            n = self._sizes.get(s)
+            if n is None or a.dtype != np.float64 or not a.flags.c_contiguous or a.size < n:
+                raise _lib.B200LAError(-1, f"set_outputs: slot {s} needs a contiguous float64 array of {n}")
+        k = len(slots)
+        call("b200la_batch_set_outputs", self.handle, k, (C.c_int * k)(*slots),
+             (C.c_void_p * k)(*[a.ctypes.data for a in arrays]))
+        for s, a in zip(slots, arrays):
+            self._outs[s] = a
 
     def results(self, slots, with_x: bool = True, out=None) -> list[SystemResult]:
         """Results of many slots with one wait for all the solution copies;
@@ -158,6 +182,9 @@ class Batch:
             xs = list(out) if out is not None else [np.empty(self.slot_n(s), np.float64) for s in slots]
             ptrs = (C.c_void_p * k)(*[x.ctypes.data for x in xs])
         call("b200la_batch_results", self.handle, k, sl, ptrs, rs)
+        if with_x:
+            for sl_ in slots:
+                self._outs.pop(sl_, None)  # registrations end with a read of x
         return [SystemResult(r.state, r.solver_state, r.iters, r.outer, bool(r.phase_done), r.res, r.res_init,
                              r.res_rel, r.device_us, None if xs is None else xs[j]) for j, r in enumerate(rs)]
 
@@ -186,6 +213,7 @@ class Batch:
     def restart(self):
         """Restart every system from x = 0 (matrices and right-hand sides stay resident)."""
         call("b200la_batch_restart", self.handle)
+        self._outs.clear()
 
     def tune(self) -> tuple[tuple[int, int, int], float]:
         """Pick the warp item sizes (rows) of K1 (SpMV), K2 (update) and K3

@@ -961,6 +961,8 @@ struct HostSys {
   size_t bytes = 0;
   SysDesc<double> d64{};
   SysDesc<float> d32{};
+  double *out = nullptr;   // registered host destination of the solution
+  bool out_copied = false; // its copy is queued on the transfer stream
 };
 
 size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
@@ -1013,6 +1015,7 @@ struct b200la_batch_s {
   // context stream; the context stream waits for xfer_done before later work
   cudaStream_t xfer;
   cudaEvent_t xfer_done;
+  bool xfer_copies;   // solution copies queued on xfer since its last wait
   bool in_flight;     // a b200la_batch_launch not yet completed
 };
 
@@ -1672,6 +1675,8 @@ int add_many_t(BatchHandle B, int count, const int *n, const int64_t *nnz, const
   return first;
 }
 
+int wait_early_copies(b200la_batch B);
+
 }  // namespace
 
 extern "C" {
@@ -1853,6 +1858,7 @@ int b200la_batch_slot_size(b200la_batch B, int slot, int *n, int64_t *nnz) {
 int b200la_batch_remove(b200la_batch B, int slot) {
   B_CHECK(B && slot >= 0 && slot < B->capacity && B->sys[slot].used, B200LA_ERR_INVALID, "batch_remove: slot %d",
           slot);
+  B_TRY(wait_early_copies(B));  // a queued solution copy may still read the slot
   HostSys &h = B->sys[slot];
   cudaStream_t st = B->ctx->stream;
   // stream-ordered: the slot's memory is released after the work queued
@@ -1868,6 +1874,32 @@ int b200la_batch_remove(b200la_batch B, int slot) {
 }  // extern "C"
 
 namespace {
+// Queues, on the transfer stream, the solution copy of every registered
+// system that the last state read-back shows finished.  A finished system's
+// x is no longer written (the item lists hold running systems only), so the
+// copy may overlap the passes that follow.
+int issue_early_copies(b200la_batch B) {
+  const bool mixed = B->kp.mixed != 0;
+  for (int s = 0; s < B->capacity; ++s) {
+    HostSys &h = B->sys[s];
+    if (!h.used || !h.out || h.out_copied || B->st_host[s].phase != PH_DONE) continue;
+    const double *xd = mixed ? h.d32.x : h.d64.x;
+    B_CUDA(cudaMemcpyAsync(h.out, xd, 8 * (size_t)h.n, cudaMemcpyDeviceToHost, B->xfer));
+    h.out_copied = true;
+    B->xfer_copies = true;
+  }
+  return B200LA_OK;
+}
+
+// Waits for the queued solution copies (before x is reset or freed, and
+// before results are handed out).
+int wait_early_copies(b200la_batch B) {
+  if (!B->xfer_copies) return B200LA_OK;
+  B_CUDA(cudaStreamSynchronize(B->xfer));
+  B->xfer_copies = false;
+  return B200LA_OK;
+}
+
 // Completes a b200la_batch_launch: the states and globals come back after the
 // launch (and after any add queued since, which the context stream waits for).
 int complete_inflight(b200la_batch B) {
@@ -1878,7 +1910,7 @@ int complete_inflight(b200la_batch B) {
   B_CUDA(cudaMemcpyAsync(B->glob_host, B->glob, sizeof(BatchGlobals), cudaMemcpyDeviceToHost, st));
   B_CUDA(cudaStreamSynchronize(st));
   B->pass_total = B->glob_host->pass_total;
-  return B200LA_OK;
+  return issue_early_copies(B);
 }
 }  // namespace
 
@@ -1926,7 +1958,7 @@ int b200la_batch_run(b200la_batch B, int max_passes, int *active_out) {
   B_CUDA(cudaStreamSynchronize(st));
   B->pass_total = B->glob_host->pass_total;
   if (active_out) *active_out = B->glob_host->active;
-  return B200LA_OK;
+  return issue_early_copies(B);
 }
 
 int b200la_batch_solve(b200la_batch B, int chunk_passes, int *total_passes) {
@@ -1956,7 +1988,7 @@ namespace {
 int fill_result(b200la_batch B, int slot, double *x_host, b200la_sys_result *r) {
   B_CHECK(B && r && slot >= 0 && slot < B->capacity && B->sys[slot].used, B200LA_ERR_INVALID,
           "batch_result: slot %d", slot);
-  const HostSys &h = B->sys[slot];
+  HostSys &h = B->sys[slot];
   const SysState &s = B->st_host[slot];
   memset(r, 0, sizeof(*r));
   r->phase_done = s.phase == PH_DONE;
@@ -1972,9 +2004,15 @@ int fill_result(b200la_batch B, int slot, double *x_host, b200la_sys_result *r) 
   else if (r->state == B200LA_FAIL_DIV || r->state == B200LA_FAIL_MAXITS || r->state == B200LA_ITERATE)
     r->solver_state = B200LA_SOLVER_EXCEEDED;
   else r->solver_state = B200LA_SOLVER_ERROR;
+  // a registered destination that already has its copy queued needs none;
+  // a read with a destination ends the registration (a status-only read not)
   if (x_host) {
-    const double *xd = B->kp.mixed ? h.d32.x : h.d64.x;
-    B_CUDA(cudaMemcpyAsync(x_host, xd, 8 * (size_t)h.n, cudaMemcpyDeviceToHost, B->ctx->stream));
+    if (!(x_host == h.out && h.out_copied)) {
+      const double *xd = B->kp.mixed ? h.d32.x : h.d64.x;
+      B_CUDA(cudaMemcpyAsync(x_host, xd, 8 * (size_t)h.n, cudaMemcpyDeviceToHost, B->ctx->stream));
+    }
+    h.out = nullptr;
+    h.out_copied = false;
   }
   return B200LA_OK;
 }
@@ -1985,7 +2023,7 @@ int b200la_batch_result(b200la_batch B, int slot, double *x_host, b200la_sys_res
   B_TRY(complete_inflight(B));
   B_TRY(fill_result(B, slot, x_host, r));
   if (x_host) B_CUDA(cudaStreamSynchronize(B->ctx->stream));
-  return B200LA_OK;
+  return wait_early_copies(B);
 }
 
 int b200la_batch_results(b200la_batch B, int count, const int *slots, double *const *x_host,
@@ -1999,6 +2037,20 @@ int b200la_batch_results(b200la_batch B, int count, const int *slots, double *co
     any = any || x;
   }
   if (any) B_CUDA(cudaStreamSynchronize(B->ctx->stream));
+  return wait_early_copies(B);
+}
+
+int b200la_batch_set_outputs(b200la_batch B, int count, const int *slots, double *const *x) {
+  B_CHECK(B && count >= 0 && (count == 0 || (slots && x)), B200LA_ERR_INVALID, "batch_set_outputs: bad argument");
+  for (int k = 0; k < count; ++k)
+    B_CHECK(slots[k] >= 0 && slots[k] < B->capacity && B->sys[slots[k]].used, B200LA_ERR_INVALID,
+            "batch_set_outputs: slot %d", slots[k]);
+  for (int k = 0; k < count; ++k) {
+    HostSys &h = B->sys[slots[k]];
+    if (h.out_copied && h.out != x[k]) B_TRY(wait_early_copies(B));  // the old destination's copy
+    h.out = x[k];
+    h.out_copied = false;
+  }
   return B200LA_OK;
 }
 
@@ -2014,6 +2066,12 @@ int b200la_batch_info(b200la_batch B, int *used_slots, int64_t *device_bytes) {
 int b200la_batch_restart(b200la_batch B) {
   B_CHECK(B, B200LA_ERR_INVALID, "batch_restart: null batch");
   B_TRY(complete_inflight(B));
+  // queued solution copies read x, which the restart zeroes; registrations end
+  B_TRY(wait_early_copies(B));
+  for (HostSys &h : B->sys) {
+    h.out = nullptr;
+    h.out_copied = false;
+  }
   std::vector<int> slots;
   for (int s = 0; s < B->capacity; ++s)
     if (B->sys[s].used) slots.push_back(s);
@@ -2059,6 +2117,7 @@ int b200la_batch_get_items(b200la_batch B, int *rows) {
 int b200la_batch_tune(b200la_batch B, int *rows, double *usec) {
   B_CHECK(B, B200LA_ERR_INVALID, "batch_tune: null batch");
   B_TRY(complete_inflight(B));
+  B_TRY(wait_early_copies(B));  // the passes below rewrite x
   // Both SpMVs use the sliced-ELL layout (one row per lane, 32-row slices,
   // coalesced steps).  The free parameters are the item sizes: rows per
   // warp work item of K1 (SpMV), K2 (update and dots) and K3 (direction).
@@ -2160,6 +2219,7 @@ int b200la_batch_profile_pass(b200la_batch B, int reps, double *ms, int64_t *alg
 int b200la_batch_profile(b200la_batch B, int reps, double *ms_spmv, int64_t *algorithmic_bytes) {
   B_CHECK(B && ms_spmv && reps >= 1, B200LA_ERR_INVALID, "batch_profile: bad argument");
   B_TRY(complete_inflight(B));
+  B_TRY(wait_early_copies(B));  // the passes below rewrite x
   int count = 0;
   int64_t bytes = 0;
   B_TRY(upload_tiles(B, false, &count, &bytes));

@@ -351,8 +351,11 @@ def run_batch(args, rank, local_rank, world, torch, dist, barrier):
                 pass
         slot_of = {}
         for ch in chunks:
-            for k, sl in zip(ch, E.add_many([host[k] for k in ch])):
+            sls = E.add_many([host[k] for k in ch])
+            for k, sl in zip(ch, sls):
                 slot_of[k] = sl
+            # each solution is copied out as soon as its system finishes
+            E.set_outputs(sls, [xs[k] for k in ch])
             E.launch(E2E_LAUNCH_PASSES)
         E.solve(CHUNK)
         E.results([slot_of[k] for k in range(len(systems))], out=xs)

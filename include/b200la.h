@@ -397,15 +397,25 @@ int b200la_batch_get_system(b200la_batch b, int slot, int *rowptr, int *col, dou
 int b200la_batch_slot_size(b200la_batch b, int slot, int *n, int64_t *nnz);
 /* Frees a slot (stream-ordered: after the work already queued; no wait). */
 int b200la_batch_remove(b200la_batch b, int slot);
-/* One graph launch: at most max_passes iterations of every running system.
- * Writes how many systems are still running. */
 /* Asynchronous b200la_batch_run: enqueues one launch of at most max_passes
  * passes over the running systems and returns at once.  Systems added
  * meanwhile (b200la_batch_add* run on the batch's own transfer stream) join
  * at the next launch; the next run, solve, result(s), restart, tune or
  * profile call completes the launch first. */
 int b200la_batch_launch(b200la_batch B, int max_passes);
+/* One graph launch: at most max_passes iterations of every running system.
+ * Writes how many systems are still running. */
 int b200la_batch_run(b200la_batch b, int max_passes, int *active);
+/* Registers host destinations x[k] for the solutions of slots[k]: each
+ * registered system's solution is copied there as soon as a run, solve or
+ * launch completion sees it finished, on the batch's transfer stream, so the
+ * copies overlap the passes of the systems still running.  A later
+ * b200la_batch_result(s) with the same destination only waits for the copy.
+ * Destinations must stay valid until that call (pinned memory keeps the
+ * copies asynchronous).  A registration ends when the slot's result is read
+ * with a destination, at its removal or at a restart; x[k] = NULL cancels
+ * one. */
+int b200la_batch_set_outputs(b200la_batch b, int count, const int *slots, double *const *x);
 /* Runs until every system has finished, in launches of at most chunk_passes
  * passes; between launches the tile list is rebuilt from the systems still
  * running.  Writes the passes taken. */

@@ -309,3 +309,38 @@ def test_initial_guesses_in_one_add_many(plat):
         assert np.linalg.norm(s.b - oracle.spmv(s.rowptr, s.col, s.val, b.x)) <= 1.0001e-8 * r0, s.name
     A.close()
     B.close()
+
+
+def test_registered_outputs_are_copied_as_systems_finish(plat):
+    # solutions registered with set_outputs are copied out on the transfer
+    # stream when a run sees their system finished; results(out=...) then
+    # only waits.  They equal the plain read bit for bit; status-only reads
+    # keep a registration, a restart ends them all.
+    import torch
+    sizes = P.batch_sizes(12, lo=16, hi=96, seed=21)
+    systems = [P.q1_system(2, int(n), 40 + k, 1.0, f"o{k}") for k, n in enumerate(sizes)]
+    kw = dict(mixed=True, precond=True, rtol=1e-8, inner_rtol=1e-4, platform=plat)
+    A = Batch(12, **kw)
+    sa = A.add_many([(s.rowptr, s.col, s.val, s.b) for s in systems])
+    A.solve(8)
+    ra = A.results(sa)
+    B = Batch(12, **kw)
+    sb = B.add_many([(s.rowptr, s.col, s.val, s.b) for s in systems])
+    outs = [torch.empty(s.n, dtype=torch.float64).pin_memory().numpy() for s in systems]
+    B.set_outputs(sb, outs)
+    B.run(20)
+    for sl in sb:
+        B.result(sl, with_x=False)  # status-only reads keep the registrations
+    B.solve(8)  # small launches: most systems finish, and are copied, before the last one
+    rb = B.results(sb, out=outs)
+    for a, b, o in zip(ra, rb, outs):
+        assert b.x is o and np.array_equal(b.x, a.x) and b.iters == a.iters
+    B.restart()
+    B.solve(8)
+    rc = B.results(sb)
+    for a, c in zip(ra, rc):
+        assert np.array_equal(c.x, a.x)
+    with pytest.raises(lmp.B200LAError):
+        B.set_outputs([sb[0]], [np.empty(3)])
+    A.close()
+    B.close()
