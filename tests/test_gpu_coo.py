@@ -66,6 +66,19 @@ def test_random_triplets_match_oracle(plat, nrow, ncol, nnz, seed):
     np.testing.assert_array_equal(v, ref[2].astype(np.float32))
 
 
+def test_float32_values_into_both_storage_types(plat):
+    # float32 triplet values: cast to FP64 storage exactly, kept as FP32
+    rows, cols, vals = _triplets(400, 300, 6000, 7)
+    v32 = vals.astype(np.float32)
+    ref = oracle.coo_to_csr(400, 300, rows, cols, v32.astype(np.float64))
+    for dt in (np.float64, np.float32):
+        A = lmp.B200_CSR_lMatrix.TransformFromCOO(rows, cols, v32, 400, 300, platform=plat, dtype=dt)
+        rp, c, v = A.csr()
+        np.testing.assert_array_equal(rp, ref[0])
+        np.testing.assert_array_equal(c, ref[1])
+        np.testing.assert_array_equal(v, ref[2].astype(dt))
+
+
 def test_long_and_distinct_rows(plat):
     # the warp-per-row kernel ranks distinct columns with shuffles for rows
     # of up to 256 entries and falls back to the selection sort for longer
