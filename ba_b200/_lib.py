@@ -149,6 +149,7 @@ _SIGS = {
     "b200la_batch_remove": [_vp, _i],
     "b200la_batch_launch": [_vp, _i],
     "b200la_batch_set_outputs": [_vp, _i, _P(_i), _P(_vp)],
+    "b200la_batch_remove_many": [_vp, _i, _P(_i)],
     "b200la_batch_run": [_vp, _i, _P(_i)],
     "b200la_batch_result": [_vp, _i, _vp, _P(SysResult)],
     "b200la_batch_results": [_vp, _i, _P(_i), _P(_vp), _P(SysResult)],

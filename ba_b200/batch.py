@@ -130,6 +130,16 @@ class Batch:
         self._sizes.pop(slot, None)
         self._outs.pop(slot, None)
 
+    def remove_many(self, slots):
+        """Free many slots with one call (all in use and distinct, else none is freed)."""
+        slots = [int(s) for s in slots]
+        k = len(slots)
+        call("b200la_batch_remove_many", self.handle, k, (C.c_int * k)(*slots))
+        for s in slots:
+            self._keep.pop(s, None)
+            self._sizes.pop(s, None)
+            self._outs.pop(s, None)
+
     def run(self, max_passes: int = 1 << 30) -> int:
         active = C.c_int()
         call("b200la_batch_run", self.handle, int(max_passes), C.byref(active))

@@ -1871,6 +1871,36 @@ int b200la_batch_remove(b200la_batch B, int slot) {
   return B200LA_OK;
 }
 
+int b200la_batch_remove_many(b200la_batch B, int count, const int *slots) {
+  B_CHECK(B && count >= 0 && (count == 0 || slots), B200LA_ERR_INVALID, "batch_remove_many: bad argument");
+  std::vector<char> seen(B->capacity, 0);
+  for (int k = 0; k < count; ++k) {
+    const int s = slots[k];
+    B_CHECK(s >= 0 && s < B->capacity && B->sys[s].used && !seen[s], B200LA_ERR_INVALID,
+            "batch_remove_many: slot %d (out of range, free or listed twice)", s);
+    seen[s] = 1;
+  }
+  if (count == 0) return B200LA_OK;
+  B_TRY(wait_early_copies(B));  // a queued solution copy may still read a slot
+  cudaStream_t st = B->ctx->stream;
+  for (int k = 0; k < count; ++k) {
+    HostSys &h = B->sys[slots[k]];
+    free_slot_memory(B, h);
+    B->device_bytes -= (int64_t)h.bytes;
+    h = HostSys();
+    memset(&B->st_host[slots[k]], 0, sizeof(SysState));
+  }
+  // device states cleared in runs of consecutive slots, one memset per run
+  for (int s = 0; s < B->capacity;) {
+    if (!seen[s]) { ++s; continue; }
+    int e = s;
+    while (e < B->capacity && seen[e]) ++e;
+    B_CUDA(cudaMemsetAsync(B->st + s, 0, sizeof(SysState) * (size_t)(e - s), st));
+    s = e;
+  }
+  return B200LA_OK;
+}
+
 }  // extern "C"
 
 namespace {

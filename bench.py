@@ -343,13 +343,12 @@ def run_batch(args, rank, local_rank, world, torch, dist, barrier):
         chunks.append(order[at:])
     chunks = [c for c in chunks if c]
 
+    slot_of = {}
+
     def e2e_step():
-        for k in range(len(systems)):
-            try:
-                E.remove(k)
-            except Exception:
-                pass
-        slot_of = {}
+        if slot_of:
+            E.remove_many(list(slot_of.values()))
+        slot_of.clear()
         for ch in chunks:
             sls = E.add_many([host[k] for k in ch])
             for k, sl in zip(ch, sls):

@@ -397,6 +397,10 @@ int b200la_batch_get_system(b200la_batch b, int slot, int *rowptr, int *col, dou
 int b200la_batch_slot_size(b200la_batch b, int slot, int *n, int64_t *nnz);
 /* Frees a slot (stream-ordered: after the work already queued; no wait). */
 int b200la_batch_remove(b200la_batch b, int slot);
+/* Frees `count` slots at once (all must be in use and distinct, else nothing
+ * is freed); their device states are cleared with one memset per run of
+ * consecutive slots. */
+int b200la_batch_remove_many(b200la_batch b, int count, const int *slots);
 /* Asynchronous b200la_batch_run: enqueues one launch of at most max_passes
  * passes over the running systems and returns at once.  Systems added
  * meanwhile (b200la_batch_add* run on the batch's own transfer stream) join

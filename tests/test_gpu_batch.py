@@ -344,3 +344,29 @@ def test_registered_outputs_are_copied_as_systems_finish(plat):
         B.set_outputs([sb[0]], [np.empty(3)])
     A.close()
     B.close()
+
+
+def test_remove_many(plat):
+    sizes = P.batch_sizes(6, lo=16, hi=32, seed=3)
+    systems = [P.q1_system(2, int(n), 70 + k, 1.0, f"r{k}") for k, n in enumerate(sizes)]
+    B = Batch(6, mixed=True, precond=True, rtol=1e-8, inner_rtol=1e-4, platform=plat)
+    sl = B.add_many([(s.rowptr, s.col, s.val, s.b) for s in systems])
+    used0, bytes0 = B.info()
+    # a bad list frees nothing: a repeated slot, a free slot
+    for bad in ([sl[0], sl[0]], [sl[1], 99]):
+        with pytest.raises(lmp.B200LAError):
+            B.remove_many(bad)
+    assert B.info() == (used0, bytes0)
+    B.remove_many([sl[1], sl[2], sl[4]])
+    used1, bytes1 = B.info()
+    assert used1 == used0 - 3 and bytes1 < bytes0
+    # the freed slots take new systems, and every system still solves alone
+    again = B.add_many([(systems[k].rowptr, systems[k].col, systems[k].val, systems[k].b) for k in (1, 2, 4)])
+    B.solve(16)
+    ref = Batch(1, mixed=True, precond=True, rtol=1e-8, inner_rtol=1e-4, platform=plat)
+    one = ref.add_system(systems[2])
+    ref.solve(16)
+    r = B.results([again[1]])[0]
+    assert np.array_equal(r.x, ref.result(one).x)
+    B.close()
+    ref.close()
