@@ -36,7 +36,7 @@ class CgParams(C.Structure):
 class MpParams(C.Structure):
     _fields_ = [("max_outer", C.c_int), ("atol", C.c_double), ("rtol", C.c_double),
                 ("dtol", C.c_double), ("inner_maxits", C.c_int), ("inner_rtol", C.c_double),
-                ("precond", C.c_int), ("tune", C.c_int)]
+                ("precond", C.c_int), ("tune", C.c_int), ("inner_storage", C.c_int)]
 
 
 class MpResult(C.Structure):
@@ -101,6 +101,7 @@ _SIGS = {
     "b200la_ctx_set_stream": [_vp, _vp],
     "b200la_ctx_get_stream": [_vp, _P(_vp)],
     "b200la_ctx_synchronize": [_vp],
+    "b200la_ctx_set_graphs": [_vp, _i],
     "b200la_ctx_num_sms": [_vp, _P(_i)],
     "b200la_vec_create": [_vp, _i64, _i, _P(_vp)],
     "b200la_vec_wrap": [_vp, _i64, _i, _vp, _P(_vp)],

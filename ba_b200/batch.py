@@ -267,8 +267,8 @@ class Batch:
             load().b200la_batch_destroy(self.handle)
             self.handle = C.c_void_p()
 
-    def __del__(self):
-        if _finalizing():
+    def __del__(self, _fin=_finalizing):  # bound at definition: globals are gone at exit
+        if _fin():
             return
         try:
             self.close()

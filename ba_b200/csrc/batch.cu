@@ -1015,6 +1015,11 @@ struct b200la_batch_s {
   // context stream; the context stream waits for xfer_done before later work
   cudaStream_t xfer;
   cudaEvent_t xfer_done;
+  // a removal clears slot states on the context stream, after any launch in
+  // flight that may still read them; the next add (on xfer) waits for it
+  // before it writes a reused slot's descriptor and fresh state
+  cudaEvent_t rm_done;
+  bool rm_pending;
   bool xfer_copies;   // solution copies queued on xfer since its last wait
   bool in_flight;     // a b200la_batch_launch not yet completed
 };
@@ -1561,6 +1566,24 @@ int snapshot_restore(BatchHandle B, const Snapshot &sn) {
   return B200LA_OK;
 }
 
+// Removals clear slot states on the context stream (after a launch in flight
+// that may still read them); adds run on the transfer stream.  A removal
+// records rm_done, and the next add makes the transfer stream wait for it, so
+// a reused slot's descriptor and fresh state are written after the removed
+// system's state was cleared and after every kernel that could read it.
+int note_removal(BatchHandle B) {
+  B_CUDA(cudaEventRecord(B->rm_done, B->ctx->stream));
+  B->rm_pending = true;
+  return B200LA_OK;
+}
+
+int order_after_removals(BatchHandle B) {
+  if (!B->rm_pending) return B200LA_OK;
+  B_CUDA(cudaStreamWaitEvent(B->xfer, B->rm_done, 0));
+  B->rm_pending = false;
+  return B200LA_OK;
+}
+
 // Adds `count` host CSR systems: every system's copies and device check are
 // queued first, the verdicts are read back with one wait, then each valid
 // system gets its sliced-ELL part.  status[k] is each system's outcome; the
@@ -1571,6 +1594,7 @@ int add_many_t(BatchHandle B, int count, const int *n, const int64_t *nnz, const
                const double *const *x0, int *slots, int *status) {
   // all of an add runs on the transfer stream: it overlaps a launch in flight
   cudaStream_t st = B->xfer;
+  B_TRY(order_after_removals(B));
   B_TRY(ensure_checks(B, count));
   csr_check_init_kernel<<<std::max(1, std::min((count + kBlock - 1) / kBlock, 64)), kBlock, 0, st>>>(count, B->chk);
   B_CUDA(cudaGetLastError());
@@ -1709,6 +1733,7 @@ int b200la_batch_destroy(b200la_batch B) {
   if (B->glob_host) cudaFreeHost(B->glob_host);
   cudaStreamSynchronize(st);
   if (B->xfer_done) cudaEventDestroy(B->xfer_done);
+  if (B->rm_done) cudaEventDestroy(B->rm_done);
   if (B->xfer) cudaStreamDestroy(B->xfer);
   {
     // return the pool's free blocks to the driver (the context keeps freed
@@ -1747,6 +1772,7 @@ int b200la_batch_create(b200la_ctx ctx, const b200la_batch_params *p, b200la_bat
   const size_t dsz = p->mixed ? sizeof(SysDesc<float>) : sizeof(SysDesc<double>);
   bool ok = cudaStreamCreateWithFlags(&B->xfer, cudaStreamNonBlocking) == cudaSuccess &&
             cudaEventCreateWithFlags(&B->xfer_done, cudaEventDisableTiming) == cudaSuccess &&
+            cudaEventCreateWithFlags(&B->rm_done, cudaEventDisableTiming) == cudaSuccess &&
             cudaMallocAsync(&B->desc, dsz * p->capacity, st) == cudaSuccess &&
             cudaMallocAsync(&B->st, sizeof(SysState) * p->capacity, st) == cudaSuccess &&
             cudaMallocAsync(&B->glob, sizeof(BatchGlobals), st) == cudaSuccess &&
@@ -1797,6 +1823,7 @@ int b200la_batch_add_q1(b200la_batch B, int dim, int cells, uint64_t seed, doubl
   const int n = (int)n64;
   const int slot = find_free_slot(B);
   B_CHECK(slot >= 0, B200LA_ERR_NOMEM, "batch_add_q1: all %d slots are in use", B->capacity);
+  B_TRY(order_after_removals(B));
   HostSys &h = B->sys[slot];
   h = HostSys();
   h.n = n;
@@ -1868,7 +1895,7 @@ int b200la_batch_remove(b200la_batch B, int slot) {
   h = HostSys();
   memset(&B->st_host[slot], 0, sizeof(SysState));
   B_CUDA(cudaMemsetAsync(B->st + slot, 0, sizeof(SysState), st));
-  return B200LA_OK;
+  return note_removal(B);
 }
 
 int b200la_batch_remove_many(b200la_batch B, int count, const int *slots) {
@@ -1898,7 +1925,7 @@ int b200la_batch_remove_many(b200la_batch B, int count, const int *slots) {
     B_CUDA(cudaMemsetAsync(B->st + s, 0, sizeof(SysState) * (size_t)(e - s), st));
     s = e;
   }
-  return B200LA_OK;
+  return note_removal(B);
 }
 
 }  // extern "C"

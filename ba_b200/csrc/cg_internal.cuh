@@ -31,6 +31,8 @@ struct b200la_cg_s {
   b200la_mat A;
   b200la_ctx ctx;              // kept for destroy, which may come after A's
   b200la_cg_params prm;
+  int vdtype;                  // type of the work vectors and scalars' arithmetic: A's own, or FP64
+                               // over an FP32 matrix (mixed storage)
   int64_t n;
   void *x, *r, *p, *Ap, *invd;
   double *part;                // [2][kMaxReduceBlocks]
@@ -43,6 +45,12 @@ struct b200la_cg_s {
 };
 
 namespace b200la {
+
+// Creates a CG solver whose work vectors have type vdtype: A->dtype (as
+// b200la_cg_create), or FP64 over an FP32 matrix, whose values are then
+// widened to FP64 in the SpMV; the Jacobi inverse diagonal then comes from
+// invd_src (an FP64 matrix of A's structure).
+int cg_create_ex(b200la_mat A, const b200la_cg_params *prm, int vdtype, b200la_mat invd_src, b200la_cg *out);
 
 // Start a solve on the context stream: r = b - A x0 (x0, b device buffers of
 // the solver's value type), or r = b with x0 = 0 when x_dev is nullptr.

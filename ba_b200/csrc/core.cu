@@ -311,6 +311,12 @@ int b200la_ctx_get_stream(b200la_ctx c, void **stream) {
   return B200LA_OK;
 }
 
+int b200la_ctx_set_graphs(b200la_ctx c, int on) {
+  B_CHECK(c, B200LA_ERR_INVALID, "ctx_set_graphs: null ctx");
+  c->use_graphs = on != 0;
+  return B200LA_OK;
+}
+
 int b200la_ctx_synchronize(b200la_ctx c) {
   B_CHECK(c, B200LA_ERR_INVALID, "ctx_synchronize: null ctx");
   B_CUDA(cudaStreamSynchronize(c->stream));

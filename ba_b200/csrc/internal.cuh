@@ -214,16 +214,19 @@ template <typename T> __device__ __forceinline__ T ld_keep(const T *p) { return 
 // All 32 lanes must call it (the shuffles use the full mask); lanes whose row
 // is out of range pass valid = false and contribute nothing.  The total is
 // returned in every lane of the group.
-template <typename T, int G>
-__device__ __forceinline__ T csr_row_group(const int *__restrict__ rowptr, const int *__restrict__ col,
-                                           const T *__restrict__ val, const T *__restrict__ x, int row,
+// X is the type of x and of the sum (the stored values T are widened to it:
+// FP32 values times FP64 vectors in the mixed-storage inner solve).
+template <typename T, int G, typename X = T>
+__device__ __forceinline__ X csr_row_group(const int *__restrict__ rowptr, const int *__restrict__ col,
+                                           const T *__restrict__ val, const X *__restrict__ x, int row,
                                            bool valid) {
   const int lane = threadIdx.x & (G - 1);
-  T sum = T(0);
+  X sum = X(0);
   if (valid) {
     const int start = __ldg(rowptr + row), end = __ldg(rowptr + row + 1);
 #pragma unroll 4
-    for (int j = start + lane; j < end; j += G) sum = fma(ld_stream(val + j), ld_keep(x + ld_stream(col + j)), sum);
+    for (int j = start + lane; j < end; j += G)
+      sum = fma((X)ld_stream(val + j), ld_keep(x + ld_stream(col + j)), sum);
   }
 #pragma unroll
   for (int o = G / 2; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);

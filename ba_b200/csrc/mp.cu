@@ -5,6 +5,12 @@
 //   loop: c = PCG32(A32, r32) from c = 0 to inner_rtol   (device graph)
 //         x += c             (FP64 update, fused cast)
 //         r = b - A64 x; stop on the FP64 residual
+// With inner_storage = B200LA_MP_F32_VALUES the inner PCG keeps its vectors,
+// dot products and Jacobi scaling in FP64 over the FP32 matrix values (each
+// widened before its FMA): the matrix, most of an iteration's bytes, still
+// moves at 4 bytes per value, while the Krylov recurrence no longer loses
+// accuracy to FP32 rounding -- on ill-conditioned systems the FP32 recurrence
+// needs far more iterations than FP64 PCG to reach the same inner tolerance.
 // The outer test is relative to the initial residual; the reference resets
 // res0_ to the latest residual after every pass (mpir.cc:239), which would
 // make a relative tolerance relative to the previous pass instead.
@@ -22,22 +28,24 @@ struct MpScalars {
   unsigned ticket[2];
 };
 
-template <typename Op> struct ResidualEmit {
+// R = type of the inner solve's right-hand side (float, or double under
+// mixed storage)
+template <typename Op, typename R> struct ResidualEmit {
   const double *__restrict__ b;
-  float *__restrict__ r32;
+  R *__restrict__ rin;
   Acc<double> rr;
   __device__ __forceinline__ void operator()(int row, double y) {
     const double r = b[row] - y;
-    r32[row] = (float)r;
+    rin[row] = (R)r;
     rr.add(r * r);
   }
 };
 
-template <typename Op>
+template <typename Op, typename R>
 __global__ void __launch_bounds__(kBlock) mp_residual_kernel(Op op, const double *__restrict__ x,
-                                                             const double *__restrict__ b, float *__restrict__ r32,
+                                                             const double *__restrict__ b, R *__restrict__ rin,
                                                              double *part, MpScalars *sc) {
-  ResidualEmit<Op> e{b, r32};
+  ResidualEmit<Op, R> e{b, rin};
   op.run(x, e);
   double s[1] = {e.rr.value()};
   if (grid_sum_last<1>(s, part, &sc->ticket[0]) && threadIdx.x == 0) {
@@ -64,6 +72,21 @@ __global__ void __launch_bounds__(kBlock) mp_correct_kernel(int64_t n, double *_
   for (int64_t i = n4 * 4 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) x[i] += (double)c[i];
 }
 
+// x += c with an FP64 correction (mixed storage)
+__global__ void __launch_bounds__(kBlock) mp_correct64_kernel(int64_t n, double *__restrict__ x,
+                                                              const double *__restrict__ c) {
+  const int64_t n2 = n / 2;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n2; i += stride) {
+    double2 a = reinterpret_cast<double2 *>(x)[i];
+    const double2 cv = reinterpret_cast<const double2 *>(c)[i];
+    a.x += cv.x;
+    a.y += cv.y;
+    reinterpret_cast<double2 *>(x)[i] = a;
+  }
+  for (int64_t i = n2 * 2 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) x[i] += c[i];
+}
+
 }  // namespace b200la
 
 using namespace b200la;
@@ -75,7 +98,7 @@ struct b200la_mp_s {
   b200la_mp_params prm;
   b200la_cg inner;
   int64_t n;
-  float *r32;
+  void *rin;         // the inner solve's right-hand side: float, or double under mixed storage
   double *part;
   MpScalars *sc;
   MpScalars *sc_host;
@@ -86,11 +109,19 @@ namespace b200la {
 static int mp_residual(b200la_mp s, const double *x, const double *b, double *res) {
   b200la_mat A = s->A64;
   cudaStream_t st = A->ctx->stream;
+  const bool f64in = s->prm.inner_storage == B200LA_MP_F32_VALUES;
   B_TRY(with_schedule<double>(A, [&](auto op) -> int {
     using Op = decltype(op);
     int grid;
-    B_TRY(grid_for(A->ctx, (const void *)mp_residual_kernel<Op>, op.work_items(), Op::kRowsPerBlock, &grid));
-    mp_residual_kernel<Op><<<grid, kBlock, 0, st>>>(op, x, b, s->r32, s->part, s->sc);
+    if (f64in) {
+      B_TRY(grid_for(A->ctx, (const void *)mp_residual_kernel<Op, double>, op.work_items(), Op::kRowsPerBlock,
+                     &grid));
+      mp_residual_kernel<Op, double><<<grid, kBlock, 0, st>>>(op, x, b, (double *)s->rin, s->part, s->sc);
+    } else {
+      B_TRY(grid_for(A->ctx, (const void *)mp_residual_kernel<Op, float>, op.work_items(), Op::kRowsPerBlock,
+                     &grid));
+      mp_residual_kernel<Op, float><<<grid, kBlock, 0, st>>>(op, x, b, (float *)s->rin, s->part, s->sc);
+    }
     B_CUDA(cudaGetLastError());
     return B200LA_OK;
   }));
@@ -110,7 +141,7 @@ int b200la_mp_destroy(b200la_mp s) {
   cudaStreamSynchronize(st);
   if (s->inner) b200la_cg_destroy(s->inner);
   if (s->A32) b200la_mat_destroy(s->A32);
-  if (s->r32) cudaFreeAsync(s->r32, st);
+  if (s->rin) cudaFreeAsync(s->rin, st);
   if (s->part) cudaFreeAsync(s->part, st);
   if (s->sc) cudaFreeAsync(s->sc, st);
   if (s->sc_host) cudaFreeHost(s->sc_host);
@@ -127,6 +158,9 @@ int b200la_mp_create(b200la_mat A64, const b200la_mp_params *prm, b200la_mp *out
   B_CHECK(prm->inner_rtol > 0.0 && prm->inner_rtol < 1.0, B200LA_ERR_INVALID, "mp_create: inner_rtol %g",
           prm->inner_rtol);
   B_CHECK(prm->atol >= 0.0 && prm->rtol >= 0.0 && prm->dtol > 0.0, B200LA_ERR_INVALID, "mp_create: tolerances");
+  B_CHECK(prm->inner_storage == B200LA_MP_F32 || prm->inner_storage == B200LA_MP_F32_VALUES, B200LA_ERR_INVALID,
+          "mp_create: inner_storage %d", prm->inner_storage);
+  const bool f64in = prm->inner_storage == B200LA_MP_F32_VALUES;
   b200la_mp s = new b200la_mp_s();
   s->A64 = A64;
   s->ctx = A64->ctx;
@@ -137,10 +171,11 @@ int b200la_mp_create(b200la_mat A64, const b200la_mp_params *prm, b200la_mp *out
   if (rc == B200LA_OK && prm->tune) rc = b200la_mat_tune(s->A32, nullptr, nullptr, nullptr);
   if (rc == B200LA_OK) {
     b200la_cg_params ip = {prm->inner_maxits, 0.0, prm->inner_rtol, 1e30, prm->precond};
-    rc = b200la_cg_create(s->A32, &ip, &s->inner);
+    rc = f64in ? cg_create_ex(s->A32, &ip, B200LA_F64, A64, &s->inner) : b200la_cg_create(s->A32, &ip, &s->inner);
   }
   if (rc == B200LA_OK &&
-      (cudaMallocAsync(&s->r32, sizeof(float) * (s->n > 0 ? s->n : 1), st) != cudaSuccess ||
+      (cudaMallocAsync(&s->rin, (f64in ? sizeof(double) : sizeof(float)) * (s->n > 0 ? s->n : 1), st) !=
+           cudaSuccess ||
        cudaMallocAsync(&s->part, sizeof(double) * kMaxReduceBlocks, st) != cudaSuccess ||
        cudaMallocAsync(&s->sc, sizeof(MpScalars), st) != cudaSuccess ||
        cudaMallocHost(&s->sc_host, sizeof(MpScalars)) != cudaSuccess ||
@@ -177,14 +212,17 @@ int b200la_mp_solve(b200la_mp s, b200la_vec b, b200la_vec x, b200la_mp_result *r
   B_TRY(mp_residual(s, (const double *)x->d, (const double *)b->d, &r));
   const double r0 = r;
   int outer = 0, inner_total = 0;
+  const bool f64in = p.inner_storage == B200LA_MP_F32_VALUES;
   int grid_c;
-  B_TRY(grid_for(c, (const void *)mp_correct_kernel, (s->n + 3) / 4, kBlock, &grid_c));
+  if (f64in) B_TRY(grid_for(c, (const void *)mp_correct64_kernel, (s->n + 1) / 2, kBlock, &grid_c));
+  else B_TRY(grid_for(c, (const void *)mp_correct_kernel, (s->n + 3) / 4, kBlock, &grid_c));
   auto done = [&](double v) { return v <= p.atol || v < p.rtol * r0 || !(v <= p.dtol * r0); };
   while (!done(r) && outer < p.max_outer) {
     ++outer;
-    B_TRY(cg_start(s->inner, nullptr, s->r32));
+    B_TRY(cg_start(s->inner, nullptr, s->rin));
     B_TRY(cg_run(s->inner));
-    mp_correct_kernel<<<grid_c, kBlock, 0, st>>>(s->n, (double *)x->d, (const float *)s->inner->x);
+    if (f64in) mp_correct64_kernel<<<grid_c, kBlock, 0, st>>>(s->n, (double *)x->d, (const double *)s->inner->x);
+    else mp_correct_kernel<<<grid_c, kBlock, 0, st>>>(s->n, (double *)x->d, (const float *)s->inner->x);
     B_CUDA(cudaGetLastError());
     B_TRY(mp_residual(s, (const double *)x->d, (const double *)b->d, &r));
     CgScalars h;

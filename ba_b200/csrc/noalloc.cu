@@ -16,6 +16,8 @@
 // All calls share the one array and it keeps the last call's contents; the
 // ticket is cleared at the start of every call.  Calls whose kernels overlap
 // on the GPU (several streams or host threads at once) race on the array.
+#include <cuda.h>
+
 #include <mutex>
 
 #include "internal.cuh"
@@ -37,9 +39,16 @@ struct NoAllocScratch {
 
 static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
 
-// Host-side cache of the scratch's device address, one per device.  The
-// symbol name itself is a host-side stand-in and must never reach a kernel.
-static NoAllocScratch *g_noalloc_addr[kNoAllocMaxDevices];
+// Host-side cache of the scratch's device address, one entry per device,
+// tagged with the id of the CUDA context it was looked up in.  The symbol
+// name itself is a host-side stand-in and must never reach a kernel.  After
+// cudaDeviceReset the device gets a new primary context (a new id) in which
+// the array has a new address, so a changed id triggers a new lookup.
+struct NoAllocEntry {
+  unsigned long long ctx_id;
+  NoAllocScratch *addr;
+};
+static NoAllocEntry g_noalloc_addr[kNoAllocMaxDevices];
 static std::mutex g_noalloc_mu;
 
 template <typename T>
@@ -56,19 +65,54 @@ __global__ void __launch_bounds__(kBlock) dot_noalloc_kernel(int64_t n, const T 
   if (grid_sum_last<1>(v, scr->part, &scr->ticket) && threadIdx.x == 0) scr->total = v[0];
 }
 
-// First call on a device: look up the scratch's device address with that
-// device current and cache it.
+// Id of the context current on this thread (0 if none is current yet, or if
+// the driver entry points cannot be had, in which case every call looks the
+// address up again -- the lookup allocates nothing).  The driver functions
+// come through the runtime's entry-point query, so the library does not link
+// libcuda itself.
+typedef CUresult (*CtxGetCurrentFn)(CUcontext *);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long *);
+
+static unsigned long long current_ctx_id() {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static bool tried = false;
+  if (!tried) {  // called under g_noalloc_mu
+    tried = true;
+    void *f1 = nullptr, *f2 = nullptr;
+    cudaDriverEntryPointQueryResult q1, q2;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f1, 12000, cudaEnableDefault, &q1) == cudaSuccess &&
+        cudaGetDriverEntryPointByVersion("cuCtxGetId", &f2, 12000, cudaEnableDefault, &q2) == cudaSuccess &&
+        q1 == cudaDriverEntryPointSuccess && q2 == cudaDriverEntryPointSuccess) {
+      get_current = (CtxGetCurrentFn)f1;
+      get_id = (CtxGetIdFn)f2;
+    }
+  }
+  if (!get_current || !get_id) return 0;
+  CUcontext c = nullptr;
+  unsigned long long id = 0;
+  if (get_current(&c) != CUDA_SUCCESS || !c || get_id(c, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
+
+// Set-up on a device (its first call there, or the first after the device's
+// context was replaced): look up the scratch's device address with that
+// device current and cache it with the context's id.
 static int noalloc_scratch(int device, NoAllocScratch **out) {
   B_CHECK(device >= 0 && device < kNoAllocMaxDevices, B200LA_ERR_UNSUPPORTED,
           "dot_noalloc: device %d beyond the %d supported", device, kNoAllocMaxDevices);
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_addr[device]) {
+  NoAllocEntry &e = g_noalloc_addr[device];
+  unsigned long long id = current_ctx_id();
+  if (!e.addr || id == 0 || e.ctx_id != id) {
     void *p = nullptr;
     B_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
     B_CHECK(p != nullptr, B200LA_ERR_CUDA, "dot_noalloc: scratch address lookup returned NULL");
-    g_noalloc_addr[device] = static_cast<NoAllocScratch *>(p);
+    id = current_ctx_id();  // the lookup makes the device's primary context current
+    e.ctx_id = id;
+    e.addr = static_cast<NoAllocScratch *>(p);
   }
-  *out = g_noalloc_addr[device];
+  *out = e.addr;
   return B200LA_OK;
 }
 

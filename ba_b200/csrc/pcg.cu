@@ -17,6 +17,7 @@
 // the device loop ends even if a reduction misbehaves.
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "cg_internal.cuh"
@@ -226,23 +227,35 @@ namespace b200la {
 
 // One iteration: K1, K2, K3 on stream `st` (captured into the graph body,
 // or launched from the host loop when graphs are off).
-template <typename T, bool PRE, bool IN_GRAPH>
+// M = stored matrix value type, T = vector type (M == T, or FP32 values over
+// FP64 vectors).
+template <typename M, typename T, bool PRE, bool IN_GRAPH>
 static int cg_launch_body_t(b200la_cg s, cudaStream_t st, cudaGraphConditionalHandle h) {
   b200la_mat A = s->A;
   b200la_ctx c = A->ctx;
   CgVecs<T> v{(T *)s->x, (T *)s->r, (T *)s->p, (T *)s->Ap, (const T *)s->invd, s->n};
-  B_TRY(with_schedule<T>(A, [&](auto op) -> int {
+  B_TRY((with_schedule<M, T>(A, [&](auto op) -> int {
     using Op = decltype(op);
     B_TRY(grid_for(c, (const void *)cg_spmv_kernel<Op, T>, op.work_items(), Op::kRowsPerBlock, &s->grid_spmv));
     cg_spmv_kernel<Op, T><<<s->grid_spmv, kBlock, 0, st>>>(op, v, s->part, s->sc);
     return B200LA_OK;
-  }));
+  })));
   cg_update_kernel<T, PRE><<<s->grid_ew, kBlock, 0, st>>>(v, s->part, s->sc);
   cg_direction_kernel<T, PRE, IN_GRAPH><<<s->grid_ew, kBlock, 0, st>>>(v, s->sc, h);
   return B200LA_OK;
 }
 
-template <typename T, bool PRE>
+// Calls f(M(), T(), std::bool_constant<PRE>()) with the solver's matrix value
+// type M, vector type T and preconditioning.
+template <typename F> static int cg_types(b200la_cg s, F &&f) {
+  const bool pre = s->prm.precond != 0;
+  auto go = [&](auto m, auto t) -> int { return pre ? f(m, t, std::true_type()) : f(m, t, std::false_type()); };
+  if (s->A->dtype == B200LA_F64) return go(double(), double());
+  if (s->vdtype == B200LA_F64) return go(float(), double());
+  return go(float(), float());
+}
+
+template <typename M, typename T, bool PRE>
 static int cg_build_graph_t(b200la_cg s) {
   b200la_mat A = s->A;
   b200la_ctx c = A->ctx;
@@ -266,7 +279,7 @@ static int cg_build_graph_t(b200la_cg s) {
   cudaStream_t cs;
   B_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
   B_CUDA(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-  int rc = cg_launch_body_t<T, PRE, true>(s, cs, h);
+  int rc = cg_launch_body_t<M, T, PRE, true>(s, cs, h);
   cudaGraph_t captured;
   cudaError_t ce = cudaStreamEndCapture(cs, &captured);
   cudaStreamDestroy(cs);
@@ -279,12 +292,12 @@ static int cg_build_graph_t(b200la_cg s) {
 }
 
 static int cg_build_graph(b200la_cg s) {
-  bool pre = s->prm.precond != 0;
-  if (s->A->dtype == B200LA_F64) return pre ? cg_build_graph_t<double, true>(s) : cg_build_graph_t<double, false>(s);
-  return pre ? cg_build_graph_t<float, true>(s) : cg_build_graph_t<float, false>(s);
+  return cg_types(s, [&](auto m, auto t, auto pre) -> int {
+    return cg_build_graph_t<decltype(m), decltype(t), decltype(pre)::value>(s);
+  });
 }
 
-template <typename T, bool PRE>
+template <typename M, typename T, bool PRE>
 static int cg_launch_init_t(b200la_cg s, const void *x_user, const void *b) {
   b200la_mat A = s->A;
   CgVecs<T> v{(T *)s->x, (T *)s->r, (T *)s->p, (T *)s->Ap, (const T *)s->invd, s->n};
@@ -296,7 +309,7 @@ static int cg_launch_init_t(b200la_cg s, const void *x_user, const void *b) {
     B_CUDA(cudaGetLastError());
     return B200LA_OK;
   }
-  return with_schedule<T>(A, [&](auto op) -> int {
+  return with_schedule<M, T>(A, [&](auto op) -> int {
     using Op = decltype(op);
     int grid;
     B_TRY(grid_for(A->ctx, (const void *)cg_init_kernel<Op, T, PRE>, op.work_items(), Op::kRowsPerBlock, &grid));
@@ -307,21 +320,20 @@ static int cg_launch_init_t(b200la_cg s, const void *x_user, const void *b) {
 }
 
 static int cg_launch_init(b200la_cg s, const void *x_user, const void *b) {
-  bool pre = s->prm.precond != 0;
-  if (s->A->dtype == B200LA_F64)
-    return pre ? cg_launch_init_t<double, true>(s, x_user, b) : cg_launch_init_t<double, false>(s, x_user, b);
-  return pre ? cg_launch_init_t<float, true>(s, x_user, b) : cg_launch_init_t<float, false>(s, x_user, b);
+  return cg_types(s, [&](auto m, auto t, auto pre) -> int {
+    return cg_launch_init_t<decltype(m), decltype(t), decltype(pre)::value>(s, x_user, b);
+  });
 }
 
 int cg_start(b200la_cg s, const void *x_dev, const void *b_dev) { return cg_launch_init(s, x_dev, b_dev); }
 
-template <typename T, bool PRE>
+template <typename M, typename T, bool PRE>
 static int cg_host_loop_t(b200la_cg s) {
   cudaStream_t st = s->A->ctx->stream;
   // the kernels return at once when the state is no longer "iterate", so
   // checking the state every 16 iterations runs the same iterations
   for (int64_t it = 0;; it += 16) {
-    for (int k = 0; k < 16; ++k) B_TRY((cg_launch_body_t<T, PRE, false>(s, st, 0)));
+    for (int k = 0; k < 16; ++k) B_TRY((cg_launch_body_t<M, T, PRE, false>(s, st, 0)));
     B_CUDA(cudaGetLastError());
     CgScalars h;
     B_TRY(cg_fetch(s, &h));
@@ -333,9 +345,9 @@ static int cg_host_loop_t(b200la_cg s) {
 int cg_run(b200la_cg s) {
   b200la_mat A = s->A;
   if (!A->ctx->use_graphs) {
-    const bool pre = s->prm.precond != 0;
-    if (A->dtype == B200LA_F64) return pre ? cg_host_loop_t<double, true>(s) : cg_host_loop_t<double, false>(s);
-    return pre ? cg_host_loop_t<float, true>(s) : cg_host_loop_t<float, false>(s);
+    return cg_types(s, [&](auto m, auto t, auto pre) -> int {
+      return cg_host_loop_t<decltype(m), decltype(t), decltype(pre)::value>(s);
+    });
   }
   if (A->format != s->g_format || A->param != s->g_param) B_TRY(cg_build_graph(s));
   B_CUDA(cudaGraphLaunch(s->exec, A->ctx->stream));
@@ -354,12 +366,12 @@ int cg_fetch(b200la_cg s, CgScalars *out) {
 // CUDA events between the kernels; adds the mean time per launch of K1, K2
 // and K3 to ms[0..2].  Same kernels as the graph body (K3 without the loop
 // condition).
-template <typename T, bool PRE>
+template <typename M, typename T, bool PRE>
 static int cg_profile_t(b200la_cg s, const void *x_user, const void *b, int iters, double *ms) {
   b200la_mat A = s->A;
   cudaStream_t st = A->ctx->stream;
   CgVecs<T> v{(T *)s->x, (T *)s->r, (T *)s->p, (T *)s->Ap, (const T *)s->invd, s->n};
-  B_TRY((cg_launch_init_t<T, PRE>(s, x_user, b)));
+  B_TRY((cg_launch_init_t<M, T, PRE>(s, x_user, b)));
   // every pass is queued before the first wait, after one untimed pass, so
   // the timed kernels run back to back and no host launch gap falls between
   // an event pair
@@ -368,11 +380,11 @@ static int cg_profile_t(b200la_cg s, const void *x_user, const void *b, int iter
   int rc = B200LA_OK;
   auto pass = [&](cudaEvent_t *e) -> int {
     if (e) cudaEventRecord(e[0], st);
-    B_TRY(with_schedule<T>(A, [&](auto op) -> int {
+    B_TRY((with_schedule<M, T>(A, [&](auto op) -> int {
       using Op = decltype(op);
       cg_spmv_kernel<Op, T><<<s->grid_spmv, kBlock, 0, st>>>(op, v, s->part, s->sc);
       return B200LA_OK;
-    }));
+    })));
     if (e) cudaEventRecord(e[1], st);
     cg_update_kernel<T, PRE><<<s->grid_ew, kBlock, 0, st>>>(v, s->part, s->sc);
     if (e) cudaEventRecord(e[2], st);
@@ -404,15 +416,27 @@ extern "C" {
 int b200la_cg_profile(b200la_cg s, b200la_vec b, b200la_vec x, int iters, double *ms) {
   B_CHECK(s && b && x && ms && iters >= 0, B200LA_ERR_INVALID, "cg_profile: bad argument");
   B_CHECK(b->n == s->n && x->n == s->n && s->n > 0, B200LA_ERR_INVALID, "cg_profile: sizes");
-  B_CHECK(b->dtype == s->A->dtype && x->dtype == s->A->dtype, B200LA_ERR_DTYPE, "cg_profile: dtype");
-  bool pre = s->prm.precond != 0;
-  if (s->A->dtype == B200LA_F64)
-    return pre ? cg_profile_t<double, true>(s, x->d, b->d, iters, ms) : cg_profile_t<double, false>(s, x->d, b->d, iters, ms);
-  return pre ? cg_profile_t<float, true>(s, x->d, b->d, iters, ms) : cg_profile_t<float, false>(s, x->d, b->d, iters, ms);
+  B_CHECK(b->dtype == s->vdtype && x->dtype == s->vdtype, B200LA_ERR_DTYPE, "cg_profile: dtype");
+  return cg_types(s, [&](auto m, auto t, auto pre) -> int {
+    return cg_profile_t<decltype(m), decltype(t), decltype(pre)::value>(s, x->d, b->d, iters, ms);
+  });
 }
 
 int b200la_cg_create(b200la_mat A, const b200la_cg_params *prm, b200la_cg *out) {
+  B_CHECK(A, B200LA_ERR_INVALID, "cg_create: null argument");
+  return cg_create_ex(A, prm, A->dtype, nullptr, out);
+}
+
+}  // extern "C"
+
+int b200la::cg_create_ex(b200la_mat A, const b200la_cg_params *prm, int vdtype, b200la_mat invd_src,
+                         b200la_cg *out) {
   B_CHECK(A && prm && out, B200LA_ERR_INVALID, "cg_create: null argument");
+  B_CHECK(vdtype == A->dtype || (A->dtype == B200LA_F32 && vdtype == B200LA_F64), B200LA_ERR_DTYPE,
+          "cg_create: vectors of dtype %d over a matrix of dtype %d", vdtype, A->dtype);
+  B_CHECK(vdtype == A->dtype || !prm->precond ||
+              (invd_src && invd_src->dtype == vdtype && invd_src->nrow == A->nrow && invd_src->nnz == A->nnz),
+          B200LA_ERR_INVALID, "cg_create: mixed storage with Jacobi needs an FP64 matrix of the same structure");
   B_CHECK(A->nrow == A->ncol, B200LA_ERR_INVALID, "cg_create: matrix is %dx%d, not square", A->nrow, A->ncol);
   B_CHECK(prm->maxits >= 0 && prm->maxits <= kMaxIts, B200LA_ERR_INVALID, "cg_create: maxits %d not in [0, %d]",
           prm->maxits, kMaxIts);
@@ -424,8 +448,9 @@ int b200la_cg_create(b200la_mat A, const b200la_cg_params *prm, b200la_cg *out) 
   s->A = A;
   s->ctx = c;
   s->prm = *prm;
+  s->vdtype = vdtype;
   s->n = A->nrow;
-  size_t es = dtype_size(A->dtype);
+  size_t es = dtype_size(vdtype);
   size_t vb = es * (size_t)(s->n > 0 ? s->n : 1);
   int rc = B200LA_OK;
   auto cleanup = [&](int code) { b200la_cg_destroy(s); return code; };
@@ -447,8 +472,8 @@ int b200la_cg_create(b200la_mat A, const b200la_cg_params *prm, b200la_cg *out) 
   if (prm->precond) {
     if (cudaMallocAsync(&s->invd, vb, st) != cudaSuccess)
       return cleanup(fail(B200LA_ERR_NOMEM, "cg_create: allocation of the inverse diagonal failed"));
-    b200la_vec_s dv{c, s->n, A->dtype, s->invd, false};
-    rc = b200la_mat_inv_diag(A, &dv);
+    b200la_vec_s dv{c, s->n, vdtype, s->invd, false};
+    rc = b200la_mat_inv_diag(vdtype == A->dtype ? A : invd_src, &dv);
     if (rc != B200LA_OK) return cleanup(rc);
   }
   if (s->n > 0) {
@@ -458,6 +483,8 @@ int b200la_cg_create(b200la_mat A, const b200la_cg_params *prm, b200la_cg *out) 
   *out = s;
   return B200LA_OK;
 }
+
+extern "C" {
 
 int b200la_cg_destroy(b200la_cg s) {
   if (!s) return B200LA_OK;
@@ -478,7 +505,7 @@ int b200la_cg_solve(b200la_cg s, b200la_vec b, b200la_vec x, b200la_cg_result *r
   b200la_mat A = s->A;
   B_CHECK(b->n == s->n && x->n == s->n, B200LA_ERR_INVALID, "cg_solve: vector sizes %lld/%lld vs %lld",
           (long long)b->n, (long long)x->n, (long long)s->n);
-  B_CHECK(b->dtype == A->dtype && x->dtype == A->dtype, B200LA_ERR_DTYPE, "cg_solve: dtype mismatch");
+  B_CHECK(b->dtype == s->vdtype && x->dtype == s->vdtype, B200LA_ERR_DTYPE, "cg_solve: dtype mismatch");
   memset(res, 0, sizeof(*res));
   if (s->n == 0) {
     res->state = B200LA_SUCCESS_ABS;
@@ -487,7 +514,7 @@ int b200la_cg_solve(b200la_cg s, b200la_vec b, b200la_vec x, b200la_cg_result *r
   cudaStream_t st = A->ctx->stream;
   B_TRY(cg_start(s, x->d, b->d));
   B_TRY(cg_run(s));
-  B_CUDA(cudaMemcpyAsync(x->d, s->x, (size_t)s->n * dtype_size(A->dtype), cudaMemcpyDeviceToDevice, st));
+  B_CUDA(cudaMemcpyAsync(x->d, s->x, (size_t)s->n * dtype_size(s->vdtype), cudaMemcpyDeviceToDevice, st));
   CgScalars h;
   B_TRY(cg_fetch(s, &h));
   res->iters = h.iter;

@@ -15,18 +15,23 @@ namespace b200la {
 // ---- CSR, G lanes per row (G = 1..32) -------------------------------------
 // Each warp covers 32/G consecutive rows, so a warp's loads of val/col fall
 // in one contiguous span of the CSR arrays; x is gathered through L1/L2.
-template <typename T, int G> struct CsrOp {
+//
+// Every schedule takes the stored value type T and the vector type X (x, y
+// and the row sums; X = T except in the mixed-storage inner solve, where
+// FP32 values meet FP64 vectors and each value is widened before its FMA).
+template <typename T, int G, typename X = T> struct CsrOp {
+  using XT = X;
   const int *__restrict__ rowptr;
   const int *__restrict__ col;
   const T *__restrict__ val;
   int n;
   static constexpr int kRowsPerBlock = kBlock / G;
   __host__ __device__ int64_t work_items() const { return n; }
-  template <typename Emit> __device__ __forceinline__ void run(const T *__restrict__ x, Emit &emit) const {
+  template <typename Emit> __device__ __forceinline__ void run(const X *__restrict__ x, Emit &emit) const {
     for (int base = blockIdx.x * kRowsPerBlock; base < n; base += gridDim.x * kRowsPerBlock) {
       const int row = base + (int)threadIdx.x / G;
       const bool valid = row < n;
-      T y = csr_row_group<T, G>(rowptr, col, val, x, row, valid);
+      X y = csr_row_group<T, G, X>(rowptr, col, val, x, row, valid);
       if (valid && (threadIdx.x & (G - 1)) == 0) emit(row, y);
     }
   }
@@ -64,7 +69,8 @@ template <> __device__ __forceinline__ double4 ld_vec_stream<double4>(const doub
   return ld_stream4<double>(p);
 }
 
-template <typename T, int W> struct SellOp {
+template <typename T, int W, typename X = T> struct SellOp {
+  using XT = X;
   const int *__restrict__ slice_ptr;
   const int *__restrict__ slice_len;
   const int *__restrict__ col;
@@ -72,7 +78,7 @@ template <typename T, int W> struct SellOp {
   int n, nslices;
   static constexpr int kRowsPerBlock = kBlock;
   __host__ __device__ int64_t work_items() const { return n; }
-  template <typename Emit> __device__ __forceinline__ void run(const T *__restrict__ x, Emit &emit) const {
+  template <typename Emit> __device__ __forceinline__ void run(const X *__restrict__ x, Emit &emit) const {
     using VV = typename VecW<T, W>::v;
     using VI = typename VecW<T, W>::i;
     const int lane = threadIdx.x & 31;
@@ -82,14 +88,14 @@ template <typename T, int W> struct SellOp {
       const int chunks = __ldg(slice_len + s) / W;
       const VI *ci = reinterpret_cast<const VI *>(col + base) + lane;
       const VV *vi = reinterpret_cast<const VV *>(val + base) + lane;
-      T sum = T(0);
+      X sum = X(0);
 #pragma unroll 4
       for (int c = 0; c < chunks; ++c) {
         VI cc = ld_vec_stream(ci + c * 32);
         VV vv = ld_vec_stream(vi + c * 32);
 #pragma unroll
         for (int k = 0; k < W; ++k)
-          sum = fma(lane_get<VV, T, W>(vv, k), ld_keep(x + lane_geti<VI, W>(cc, k)), sum);
+          sum = fma((X)lane_get<VV, T, W>(vv, k), ld_keep(x + lane_geti<VI, W>(cc, k)), sum);
       }
       const int row = s * 32 + lane;
       if (row < n) emit(row, sum);
@@ -110,7 +116,8 @@ template <typename I> __device__ __forceinline__ int lane_gets(const I &v, int k
   return (int)reinterpret_cast<const short *>(&v)[k];
 }
 
-template <typename T, int W> struct SellOp16 {
+template <typename T, int W, typename X = T> struct SellOp16 {
+  using XT = X;
   const int *__restrict__ slice_ptr;
   const int *__restrict__ slice_len;
   const short *__restrict__ col;
@@ -118,7 +125,7 @@ template <typename T, int W> struct SellOp16 {
   int n, nslices;
   static constexpr int kRowsPerBlock = kBlock;
   __host__ __device__ int64_t work_items() const { return n; }
-  template <typename Emit> __device__ __forceinline__ void run(const T *__restrict__ x, Emit &emit) const {
+  template <typename Emit> __device__ __forceinline__ void run(const X *__restrict__ x, Emit &emit) const {
     using VV = typename VecW<T, W>::v;
     using VI = typename VecS<W>::i;
     const int lane = threadIdx.x & 31;
@@ -131,13 +138,14 @@ template <typename T, int W> struct SellOp16 {
       const int row = s * 32 + lane;
       // padding rows past n (last slice) hold offset 0 and gather x[0]
       const int rb = row < n ? row : 0;
-      T sum = T(0);
+      X sum = X(0);
 #pragma unroll 4
       for (int c = 0; c < chunks; ++c) {
         VI cc = __ldcs(ci + c * 32);
         VV vv = ld_vec_stream(vi + c * 32);
 #pragma unroll
-        for (int k = 0; k < W; ++k) sum = fma(lane_get<VV, T, W>(vv, k), ld_keep(x + rb + lane_gets(cc, k)), sum);
+        for (int k = 0; k < W; ++k)
+          sum = fma((X)lane_get<VV, T, W>(vv, k), ld_keep(x + rb + lane_gets(cc, k)), sum);
       }
       if (row < n) emit(row, sum);
     }
@@ -165,16 +173,17 @@ __global__ void __launch_bounds__(kBlock) spmv_kernel(Op op, const T *__restrict
   }
 }
 
-// Calls f(op) with the schedule selected on the matrix.
-template <typename T, typename F> int with_schedule(b200la_mat m, F &&f) {
+// Calls f(op) with the schedule selected on the matrix (stored values T,
+// vectors X).
+template <typename T, typename X = T, typename F> int with_schedule(b200la_mat m, F &&f) {
   const T *val = (const T *)m->val;
   if (m->format == B200LA_FMT_SELL) {
     const SellData &s = m->sell;
     const T *sv = (const T *)s.val;
     switch (m->param) {
-      case 1: return f(SellOp<T, 1>{s.slice_ptr, s.slice_len, s.col, sv, m->nrow, s.nslices});
-      case 2: return f(SellOp<T, 2>{s.slice_ptr, s.slice_len, s.col, sv, m->nrow, s.nslices});
-      case 4: return f(SellOp<T, 4>{s.slice_ptr, s.slice_len, s.col, sv, m->nrow, s.nslices});
+      case 1: return f(SellOp<T, 1, X>{s.slice_ptr, s.slice_len, s.col, sv, m->nrow, s.nslices});
+      case 2: return f(SellOp<T, 2, X>{s.slice_ptr, s.slice_len, s.col, sv, m->nrow, s.nslices});
+      case 4: return f(SellOp<T, 4, X>{s.slice_ptr, s.slice_len, s.col, sv, m->nrow, s.nslices});
     }
     return fail(B200LA_ERR_INVALID, "SELL width %d", m->param);
   }
@@ -182,19 +191,19 @@ template <typename T, typename F> int with_schedule(b200la_mat m, F &&f) {
     const SellData &s = m->sell;
     const T *sv = (const T *)s.val;
     switch (m->param) {
-      case 1: return f(SellOp16<T, 1>{s.slice_ptr, s.slice_len, s.col16p, sv, m->nrow, s.nslices});
-      case 2: return f(SellOp16<T, 2>{s.slice_ptr, s.slice_len, s.col16p, sv, m->nrow, s.nslices});
-      case 4: return f(SellOp16<T, 4>{s.slice_ptr, s.slice_len, s.col16p, sv, m->nrow, s.nslices});
+      case 1: return f(SellOp16<T, 1, X>{s.slice_ptr, s.slice_len, s.col16p, sv, m->nrow, s.nslices});
+      case 2: return f(SellOp16<T, 2, X>{s.slice_ptr, s.slice_len, s.col16p, sv, m->nrow, s.nslices});
+      case 4: return f(SellOp16<T, 4, X>{s.slice_ptr, s.slice_len, s.col16p, sv, m->nrow, s.nslices});
     }
     return fail(B200LA_ERR_INVALID, "SELL16 width %d", m->param);
   }
   switch (m->param) {
-    case 1: return f(CsrOp<T, 1>{m->rowptr, m->col, val, m->nrow});
-    case 2: return f(CsrOp<T, 2>{m->rowptr, m->col, val, m->nrow});
-    case 4: return f(CsrOp<T, 4>{m->rowptr, m->col, val, m->nrow});
-    case 8: return f(CsrOp<T, 8>{m->rowptr, m->col, val, m->nrow});
-    case 16: return f(CsrOp<T, 16>{m->rowptr, m->col, val, m->nrow});
-    case 32: return f(CsrOp<T, 32>{m->rowptr, m->col, val, m->nrow});
+    case 1: return f(CsrOp<T, 1, X>{m->rowptr, m->col, val, m->nrow});
+    case 2: return f(CsrOp<T, 2, X>{m->rowptr, m->col, val, m->nrow});
+    case 4: return f(CsrOp<T, 4, X>{m->rowptr, m->col, val, m->nrow});
+    case 8: return f(CsrOp<T, 8, X>{m->rowptr, m->col, val, m->nrow});
+    case 16: return f(CsrOp<T, 16, X>{m->rowptr, m->col, val, m->nrow});
+    case 32: return f(CsrOp<T, 32, X>{m->rowptr, m->col, val, m->nrow});
   }
   return fail(B200LA_ERR_INVALID, "CSR lanes per row %d", m->param);
 }

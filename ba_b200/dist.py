@@ -1,12 +1,13 @@
 """Host-side helpers for running the path on several GPUs, one process per
 GPU (torch.distributed; NCCL on GPUs, gloo in the CPU tests).
 
-Every workload of the path is a set of independent solves, so ranks never
-exchange solver data: each rank owns its share of the systems (or its own
-seeded batch / request stream) and only one scalar -- the step time -- is
-reduced, as the maximum over ranks.  The reference's multi-rank path
-(CoupledVector/CoupledMatrix halos, linear_algebra/coupled_vector.cc:890-973)
-partitions one system by rows; that split is not built here.
+The batched and served workloads are sets of independent solves, so their
+ranks never exchange solver data: each rank owns its share of the systems (its
+own seeded batch or request stream, or a cost-balanced part of one batch from
+partition_by_cost) and only one scalar -- the step time -- is reduced, as the
+maximum over ranks.  The reference's multi-rank path, one system partitioned
+by rows with a ghost halo (CoupledVector/CoupledMatrix,
+linear_algebra/coupled_vector.cc:890-973), lives in ba_b200/coupled.py.
 """
 from __future__ import annotations
 

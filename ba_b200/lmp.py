@@ -57,6 +57,11 @@ class Platform:
     def set_stream(self, stream_ptr: int | None):
         call("b200la_ctx_set_stream", self.handle, C.c_void_p(stream_ptr or 0))
 
+    def set_graphs(self, on: bool):
+        """Run device loops as CUDA-graph WHILE nodes (default) or, with
+        False, launch the same kernels one by one from a host loop."""
+        call("b200la_ctx_set_graphs", self.handle, 1 if on else 0)
+
     @property
     def num_sms(self) -> int:
         n = C.c_int()
@@ -68,10 +73,10 @@ class Platform:
             load().b200la_ctx_destroy(self.handle)
             self.handle = C.c_void_p()
 
-    def __del__(self):
+    def __del__(self, _fin=_finalizing):  # bound at definition: globals are gone at exit
         # at interpreter exit the process teardown releases device memory;
         # destroying contexts in arbitrary finalization order is unsafe
-        if _finalizing():
+        if _fin():
             return
         try:
             self.close()
@@ -181,8 +186,8 @@ class B200_lVector:
             load().b200la_vec_destroy(self.handle)
             self.handle = C.c_void_p()
 
-    def __del__(self):
-        if _finalizing():
+    def __del__(self, _fin=_finalizing):  # bound at definition: globals are gone at exit
+        if _fin():
             return
         try:
             self.Clear()
@@ -331,8 +336,8 @@ class B200_CSR_lMatrix:
             load().b200la_mat_destroy(self.handle)
             self.handle = C.c_void_p()
 
-    def __del__(self):
-        if _finalizing():
+    def __del__(self, _fin=_finalizing):  # bound at definition: globals are gone at exit
+        if _fin():
             return
         try:
             self.Clear()
@@ -441,8 +446,8 @@ class CG:
     def res_rel(self) -> float:
         return self.res_rel_
 
-    def __del__(self):
-        if _finalizing():
+    def __del__(self, _fin=_finalizing):  # bound at definition: globals are gone at exit
+        if _fin():
             return
         try:
             self._release()
@@ -531,8 +536,8 @@ class _DeviceSolver:
     def res_rel(self) -> float:
         return self.res_rel_
 
-    def __del__(self):
-        if _finalizing():
+    def __del__(self, _fin=_finalizing):  # bound at definition: globals are gone at exit
+        if _fin():
             return
         try:
             self._release()
@@ -725,6 +730,8 @@ class MPIR:
         self.inner_maxits, self.inner_rtol = 100000, 1e-5
         self.precond = True
         self.tune = True
+        # fast form: 0 = FP32 inner PCG; 1 = FP32 matrix values under FP64 vectors and dots
+        self.inner_storage = 0
         self._s = C.c_void_p()
         self.iter_ = 0
         self.outer_ = 0
@@ -743,6 +750,13 @@ class MPIR:
     def SetupOperator(self, op: B200_CSR_lMatrix):
         self.op = op
         self.Ah = op
+        self._release()
+
+    def SetInnerStorage(self, f64_vectors: bool):
+        """Fast form: keep the FP32 matrix values but run the inner PCG's
+        vectors, dot products and Jacobi scaling in FP64 (True), or all in
+        FP32 (False, the default)."""
+        self.inner_storage = 1 if f64_vectors else 0
         self._release()
 
     def SetHighPrecMatrix(self, mh: B200_CSR_lMatrix):
@@ -845,7 +859,8 @@ class MPIR:
         if self.max_ech != 0:
             raise B200LAError(-7, "MPIR: high-precision correction passes need SetHighPrecErrCorSolver")
         prm = _lib.MpParams(self.max_ecl, self.abs_tol, self.rel_tol, self.div_tol, self.inner_maxits,
-                            self.inner_rtol, 1 if self.precond else 0, 1 if self.tune else 0)
+                            self.inner_rtol, 1 if self.precond else 0, 1 if self.tune else 0,
+                            int(self.inner_storage))
         call("b200la_mp_create", self.op.handle, C.byref(prm), C.byref(self._s))
 
     # ---- generic form: SolveImpl (mpir.cc:52-285), ContinueIteration (:288-297)
@@ -941,8 +956,8 @@ class MPIR:
     def res(self) -> float:
         return self.res_
 
-    def __del__(self):
-        if _finalizing():
+    def __del__(self, _fin=_finalizing):  # bound at definition: globals are gone at exit
+        if _fin():
             return
         try:
             self._release()

@@ -195,6 +195,54 @@ def batch_systems(count: int = 1024, sigma: float = 1.0, seed: int = SEED_BATCH,
     return [q1_system(2, int(n), seed + 1 + k, sigma, f"batch{k}_n{int(n)}") for k, n in enumerate(sizes)]
 
 
+def stratified_sample(sizes, m: int) -> list[int]:
+    """Indices of m items spread evenly over the items ranked by size (the
+    middle item of each of m equal-count strata), in ascending index order:
+    a fixed sample whose mean cost tracks the whole set's."""
+    order = sorted(range(len(sizes)), key=lambda i: (int(sizes[i]), i))
+    m = min(int(m), len(order))
+    return sorted(order[int((j + 0.5) * len(order) / m)] for j in range(m))
+
+
+# Solution fingerprints: comparing solutions of multi-million-row systems
+# without storing them.
+PROBE_SEED = 20240610
+PROBE_VECTORS = 64
+PROBE_SAMPLES = 2048
+
+
+def solution_probe(x) -> dict:
+    """Fingerprint of a solution vector: its 2-norm, its projections on
+    PROBE_VECTORS seeded Rademacher (+-1) vectors and its values at
+    PROBE_SAMPLES seeded positions.  For e = x - y and Rademacher v,
+    E[(e.v)^2] = ||e||^2, so probe_error() estimates ||x - y|| / ||y|| from
+    two fingerprints alone (64 draws: within about +-20%)."""
+    x = np.ascontiguousarray(x, np.float64)
+    n = x.shape[0]
+    proj = []
+    for k in range(PROBE_VECTORS):
+        v = 1.0 - 2.0 * (splitmix64(PROBE_SEED, n, stream=100 + k) >> np.uint64(63)).astype(np.float64)
+        proj.append(float(np.sum(x * v)))  # pairwise summation
+    idx = (splitmix64(PROBE_SEED, PROBE_SAMPLES, stream=99) % np.uint64(n)).astype(np.int64)
+    return {"n": int(n), "norm": float(np.linalg.norm(x)), "proj": proj, "sample": x[idx].tolist()}
+
+
+def probe_error(got: dict, ref: dict) -> dict:
+    """Relative error of a solution against a reference solution, from their
+    fingerprints: `proj` = sqrt(mean (p_got - p_ref)^2) / ||x_ref|| (an
+    unbiased estimate of ||x_got - x_ref||^2 under the square root), `sample`
+    = the same estimate from the sampled entries, `max_sample` = the largest
+    sampled |x_got - x_ref| over the largest sampled |x_ref|."""
+    if got["n"] != ref["n"]:
+        raise ValueError("fingerprints of different sizes")
+    dp = np.asarray(got["proj"]) - np.asarray(ref["proj"])
+    ds = np.asarray(got["sample"]) - np.asarray(ref["sample"])
+    m = ds.shape[0]
+    return {"proj": float(np.sqrt(np.mean(dp * dp)) / ref["norm"]),
+            "sample": float(np.sqrt(ref["n"] / m * np.sum(ds * ds)) / ref["norm"]),
+            "max_sample": float(np.max(np.abs(ds)) / max(np.max(np.abs(ref["sample"])), 1e-300))}
+
+
 def serve_stream(count: int = 20000, rate: float = 100.0, lo_dofs: float = 1e3, hi_dofs: float = 2e6,
                  seed: int = SEED_SERVE) -> list[dict]:
     """The served workload: `count` Q1 diffusion solve requests arriving as a

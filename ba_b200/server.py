@@ -116,8 +116,8 @@ class Server:
     def __exit__(self, *exc):
         self.close()
 
-    def __del__(self):
-        if _finalizing():
+    def __del__(self, _fin=_finalizing):  # bound at definition: globals are gone at exit
+        if _fin():
             return
         try:
             self.close()

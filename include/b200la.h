@@ -6,7 +6,7 @@
  * Each entry point names the reference interface it replaces
  * (paths relative to the HiFlow3 source tree, src/).  A reference binding
  * registers these behind lmp's lVector / lMatrix / lPreconditioner and the
- * linear_solver CG interface; see INTEGRATION.md.
+ * linear_solver CG interface.
  *
  * Threading: a context is used by one host thread at a time (the reference's
  * lmp objects are not thread-safe either, common/timer.h:28).  All device
@@ -77,6 +77,13 @@ int b200la_ctx_destroy(b200la_ctx ctx);
 /* Use an external cudaStream_t (NULL: the context's own stream). */
 int b200la_ctx_set_stream(b200la_ctx ctx, void *stream);
 int b200la_ctx_get_stream(b200la_ctx ctx, void **stream);
+/* Device loops (the solvers' iterations, the batch's passes) run as CUDA-graph
+ * WHILE nodes; with on = 0 the same kernels launch one by one from a host
+ * loop on this context (the environment variable B200LA_GRAPHS=0 sets the
+ * default of new contexts).  Results are the same bits either way; a host
+ * loop lets a profiler or a launch record see every kernel.  Takes effect at
+ * the next solve or run. */
+int b200la_ctx_set_graphs(b200la_ctx ctx, int on);
 int b200la_ctx_synchronize(b200la_ctx ctx);
 int b200la_ctx_num_sms(b200la_ctx ctx, int *out);
 
@@ -114,10 +121,11 @@ int b200la_vec_elementwise_mult(b200la_vec y, b200la_vec x);       /* ElementWis
  * cudaStream_t, NULL = legacy default stream) is synchronised.  The reduction
  * scratch is one fixed ~32 KB __device__ array that every GPU loading the
  * library keeps until exit, so n is limited to 16,777,216 elements; larger n
- * is rejected with B200LA_ERR_UNSUPPORTED.  The first call on a device looks
- * up the array's device address and caches it; make that first call before
- * any stream capture.  All calls share the array: calls that overlap on the
- * GPU race and must be serialised by the caller. */
+ * is rejected with B200LA_ERR_UNSUPPORTED.  The first call on a device (and
+ * the first after cudaDeviceReset replaced its context) looks up the array's
+ * device address and caches it; make that first call before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU race and
+ * must be serialised by the caller. */
 int b200la_dot_noalloc(const void *x, const void *y, int64_t n, int dtype, void *stream,
                        double *out);
 
@@ -312,7 +320,12 @@ typedef struct {
   double inner_rtol;  /* the FP32 solve stops at inner_rtol times its start residual */
   int precond;        /* 1: Jacobi in the FP32 solve */
   int tune;           /* 1: autotune the FP32 matrix's SpMV schedule at create */
+  int inner_storage;  /* B200LA_MP_F32 (0): the inner PCG keeps FP32 vectors; B200LA_MP_F32_VALUES (1):
+                         FP32 matrix values (the bulk of the bytes) under FP64 vectors, dot products
+                         and Jacobi scaling, which keeps the inner iteration count near FP64 PCG's */
 } b200la_mp_params;
+#define B200LA_MP_F32 0
+#define B200LA_MP_F32_VALUES 1
 
 typedef struct {
   int outer;          /* refinement passes taken */
@@ -324,7 +337,10 @@ typedef struct {
   double res_rel;
 } b200la_mp_result;
 
-/* A64 must be FP64; an FP32 copy is made (CastFrom) and kept with the solver. */
+/* A64 must be FP64; an FP32 copy is made (CastFrom) and kept with the solver.
+ * inner_storage = B200LA_MP_F32_VALUES runs the inner PCG in FP64 arithmetic
+ * over that FP32 copy (each value widened before its FMA); the FP64 matrix
+ * then also supplies the Jacobi inverse diagonal. */
 int b200la_mp_create(b200la_mat A64, const b200la_mp_params *params, b200la_mp *out);
 int b200la_mp_destroy(b200la_mp s);
 /* The FP32 copy, e.g. to pick its SpMV schedule (owned by the solver). */

@@ -370,3 +370,43 @@ def test_remove_many(plat):
     assert np.array_equal(r.x, ref.result(one).x)
     B.close()
     ref.close()
+
+
+def test_remove_and_reuse_slots_while_a_launch_is_in_flight(plat):
+    # running systems are removed while an asynchronous launch is in flight and
+    # new systems are added into the freed slots at once.  The removal clears
+    # the slots' states on the solve stream after the launch; the adds run on
+    # the transfer stream and must be ordered after that, or a new system's
+    # fresh state would be cleared (it would never solve) and the running
+    # kernels would read its descriptor.  Each new system, and the survivor,
+    # must end with the bits it gets when solved alone.
+    first = [P.q1_system(2, c, 300 + k, 1.0, f"f{k}") for k, c in enumerate((160, 200, 180, 220))]
+    second = [P.q1_system(2, c, 400 + k, 1.0, f"s{k}") for k, c in enumerate((40, 64, 90))]
+    kw = dict(mixed=True, precond=True, rtol=1e-8, inner_rtol=1e-4, platform=plat)
+
+    def alone(s):
+        A = Batch(1, **kw)
+        A.set_items(128, 512, 512, adaptive=False)
+        a = A.add_system(s)
+        A.solve(16)
+        r = A.result(a)
+        A.close()
+        return r
+
+    B = Batch(4, **kw)
+    B.set_items(128, 512, 512, adaptive=False)
+    sl = B.add_many([(s.rowptr, s.col, s.val, s.b) for s in first])
+    B.launch(200)  # returns at once: the launch is still running below
+    gone = [sl[0], sl[1], sl[3]]
+    B.remove_many(gone)
+    new = B.add_many([(s.rowptr, s.col, s.val, s.b) for s in second])
+    assert sorted(new) == sorted(gone)
+    B.solve(16)
+    got = B.results(new + [sl[2]])
+    for s, g in zip(second + [first[2]], got):
+        ref = alone(s)
+        assert g.done and g.solver_state == lmp.kSolverSuccess, (s.name, g)
+        assert (g.iters, g.outer) == (ref.iters, ref.outer), s.name
+        np.testing.assert_array_equal(g.x, ref.x)
+    assert B.info()[0] == 4
+    B.close()

@@ -65,6 +65,39 @@ def test_mp_1e8_and_zero_rhs(plat):
     assert st == lmp.kSolverSuccess and m.outer_ == 0 and not x.any()
 
 
+@pytest.mark.parametrize("case", [("2d", 2, 48, 1.0), ("3d", 3, 20, 2.0)])
+def test_mp_fp32_values_fp64_vectors(plat, case):
+    """Mixed storage: FP32 matrix values under FP64 inner vectors and dots.
+    Same bars as the FP32 inner solve (FP64 residual at the tolerance, error
+    against the converged FP64 oracle), and the inner iteration count of the
+    first pass is close to the FP64 PCG's own count to that inner tolerance."""
+    _, dim, n, sigma = case
+    s = P.q1_system(dim, n, 77 + n, sigma)
+    A = lmp.B200_CSR_lMatrix(s.rowptr, s.col, s.val, platform=plat)
+    b = lmp.B200_lVector.from_numpy(s.b, platform=plat)
+    x = lmp.B200_lVector(s.n, platform=plat)
+    m = lmp.MPIR()
+    m.SetupOperator(A)
+    m.SetInnerStorage(True)
+    m.SetMpirParameters(0, 20, 0.0, 1e-10, 1e6)
+    m.SetLowPrecErrCorSolverParameters(100000, 0.0, 1e-5, 1e30)
+    assert m.Solve(b, x) == lmp.kSolverSuccess
+    xs = x.numpy()
+    assert np.linalg.norm(s.b - oracle.spmv(s.rowptr, s.col, s.val, xs)) < 1.05e-10 * np.linalg.norm(s.b)
+    ref = oracle.cg(s.rowptr, s.col, s.val, s.b, maxits=100000, atol=0.0, rtol=1e-13)
+    assert np.linalg.norm(xs - ref.x) / np.linalg.norm(ref.x) < 1e-8
+    # first pass against the FP64 PCG to the same inner tolerance
+    m1 = lmp.MPIR()
+    m1.SetupOperator(A)
+    m1.SetInnerStorage(True)
+    m1.SetMpirParameters(0, 1, 0.0, 1e-30, 1e6)
+    m1.SetLowPrecErrCorSolverParameters(100000, 0.0, 1e-5, 1e30)
+    x1 = lmp.B200_lVector(s.n, platform=plat)
+    m1.Solve(b, x1)
+    r64 = oracle.cg(s.rowptr, s.col, s.val, s.b, maxits=100000, atol=0.0, rtol=1e-5)
+    assert m1.outer_ == 1 and abs(m1.iter() - r64.iters) <= max(2, 0.05 * r64.iters), (m1.iter(), r64.iters)
+
+
 def test_mp_pass_limit_reports_exceeded(plat):
     s = P.q1_system(3, 16, 9, 2.0)
     st, m, x = _solve_mp(plat, s, 1e-12, inner_rtol=1e-2, max_outer=2)
