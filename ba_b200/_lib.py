@@ -36,7 +36,8 @@ class CgParams(C.Structure):
 class MpParams(C.Structure):
     _fields_ = [("max_outer", C.c_int), ("atol", C.c_double), ("rtol", C.c_double),
                 ("dtol", C.c_double), ("inner_maxits", C.c_int), ("inner_rtol", C.c_double),
-                ("precond", C.c_int), ("tune", C.c_int), ("inner_storage", C.c_int)]
+                ("precond", C.c_int), ("tune", C.c_int), ("inner_storage", C.c_int),
+                ("restart_inner", C.c_int)]
 
 
 class MpResult(C.Structure):
@@ -48,7 +49,8 @@ class MpResult(C.Structure):
 class BatchParams(C.Structure):
     _fields_ = [("capacity", C.c_int), ("mixed", C.c_int), ("precond", C.c_int), ("max_outer", C.c_int),
                 ("inner_maxits", C.c_int), ("adaptive", C.c_int), ("tile_rows", C.c_int), ("index_bits", C.c_int),
-                ("atol", C.c_double), ("rtol", C.c_double), ("dtol", C.c_double), ("inner_rtol", C.c_double)]
+                ("atol", C.c_double), ("rtol", C.c_double), ("dtol", C.c_double), ("inner_rtol", C.c_double),
+                ("restart_inner", C.c_int)]
 
 
 class SysResult(C.Structure):

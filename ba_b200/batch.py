@@ -40,14 +40,19 @@ def slot_bytes(n: int, nnz: int, max_row: int, mixed: bool) -> int:
 
 class Batch:
     def __init__(self, capacity: int, *, mixed: bool = True, precond: bool = True, rtol: float = 1e-8,
-                 atol: float = 0.0, dtol: float = 1e8, inner_rtol: float = 1e-4, max_outer: int = 30,
+                 atol: float = 0.0, dtol: float = 1e8, inner_rtol: float = 0.1, max_outer: int = 30,
                  inner_maxits: int = 100000, adaptive: bool = False, tile_rows: int = 0, index_bits: int = 0,
-                 platform: Platform | None = None):
+                 restart_inner: bool = False, platform: Platform | None = None):
+        """Mixed mode: each FP32 inner pass ends once its residual has fallen
+        by inner_rtol; the FP64 residual then replaces it and the inner PCG
+        goes on with its search direction (restart_inner=True restarts it
+        from p = z each pass instead, as MPIR does; give it a tighter
+        inner_rtol such as 1e-4)."""
         self.platform = platform or init_platform()
         self.mixed = mixed
         prm = BatchParams(int(capacity), int(mixed), int(precond), int(max_outer), int(inner_maxits),
                           int(adaptive), int(tile_rows), int(index_bits), float(atol), float(rtol), float(dtol),
-                          float(inner_rtol))
+                          float(inner_rtol), 1 if restart_inner else 0)
         self.handle = C.c_void_p()
         call("b200la_batch_create", self.platform.handle, C.byref(prm), C.byref(self.handle))
         self._keep = {}

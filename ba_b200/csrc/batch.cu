@@ -33,9 +33,14 @@
 // Each system walks through phases; a phase changes only after every item of
 // the system has passed (last-arriver ticket), so all items of a system see
 // one phase per launch:
-//   RESID   K1: r64 = b - A64 x (FP64), ||r64||, outer test; restart the inner
-//               solve from c = 0 with r = (T)r64, z = invD r, p = z -> START
-//   START   K3: opens the inner solve (-> INNER) once every item saw START
+//   RESID   K1: r64 = b - A64 x (FP64), ||r64||, outer test; the inner solve
+//               goes on from c = 0 with its residual replaced: r = (T)r64 -> START
+//   START   K3: the search direction from the new residual, z = invD r and
+//               p = z + beta p with beta = r.z / (r.z before the last step)
+//               (the direction is kept: residual replacement, "reliable
+//               updates"), or p = z on the first pass, after a breakdown, or
+//               when the batch restarts its inner solves as MPIR does; then
+//               opens the inner solve (-> INNER) once every item has passed
 //   INNER   K1: Ap = A p, p.Ap partials
 //           K2: alpha = rz / p.Ap; r -= alpha Ap; r.r, r.z partials
 //           K3: inner test on r.r; if it goes on, c += alpha p and
@@ -90,6 +95,8 @@ struct SysState {
   unsigned bad_row;            // first row without a usable diagonal (Jacobi), else ~0u
   unsigned ticket[4];
   double rzb[2];               // r.z of the current inner iteration, by pass parity
+  double rz_keep;              // r.z before the last step of the previous inner solve
+  int keep_p;                  // 1: the next START keeps the search direction
   double alphab[2];            // this pass's step (K2 writes, K3 reads), by pass parity
   int okb[2];                  // 0: this pass's step broke down
   int itb[2];                  // inner iterations done, by pass parity
@@ -104,6 +111,7 @@ struct BatchParams {
   double inner_rtol;        // inner test relative to its start residual
   int precond;
   int mixed;                // 1: FP32 inner + FP64 refinement; 0: FP64 CG
+  int restart_inner;        // 1: every inner solve restarts from p = z
 };
 
 struct BatchGlobals {
@@ -361,9 +369,10 @@ namespace b200la {
 
 // ---- RESID items (run by K1): FP64 residual, outer test, inner restart ------
 // r64 = b - A64 x with the FP64 sliced-ELL values, ||r64||, then the inner
-// solve restarts from c = 0 with r = (T)r64, z = invD r, p = z.  The
-// system's last item applies the outer test: DONE, or START.  It also seeds
-// the next pass's slot of the double-buffered scalars.
+// solve goes on from c = 0 with r = (T)r64 (K3's START items form the new
+// direction from it).  The system's last item applies the outer test: DONE,
+// or START.  It also seeds the next pass's slot of the double-buffered
+// scalars.
 template <typename T, bool PRE>
 __device__ __forceinline__ void resid_item(const Tile &tl, int t, const ItemGeo &ig, const SysDesc<T> &d, SysState &S,
                                            double *part, int64_t part_stride, BatchGlobals *g,
@@ -384,7 +393,6 @@ __device__ __forceinline__ void resid_item(const Tile &tl, int t, const ItemGeo 
       d.r[row] = r;
       d.c[row] = T(0);
       const T z = PRE ? r * d.invd[row] : r;
-      d.p[row] = z;
       rrin.add(r * r);
       rzin.add(r * z);
     }
@@ -399,6 +407,10 @@ __device__ __forceinline__ void resid_item(const Tile &tl, int t, const ItemGeo 
     }
     int s = outer_check(res, S.res0, prm);
     if (s == B200LA_ITERATE && S.outer >= prm.max_outer) s = B200LA_FAIL_MAXITS;
+    // a replaced residual more than twice the recurrence's last one: the
+    // inner recurrence drifted from the true residual, so START restarts the
+    // direction (p = z) instead of keeping it
+    if (S.outer > 0 && sqrt(v[1]) > 2.0 * S.res_in) S.keep_p = 0;
     if (prm.precond && S.bad_row != 0xffffffffu) s = B200LA_FAIL_BREAKDOWN;  // Jacobi needs every diagonal
     if (s != B200LA_ITERATE) {
       finish_system(S, g, s);
@@ -615,8 +627,16 @@ __global__ void __launch_bounds__(kBlock, 4) batch_direction_kernel(PassLists L,
     const ItemGeo ig = item_geo(tl, t, d.n, tr);
     const int end = tl.row0 + ig.rows;
     if (ph == PH_START) {
-      // K1 wrote the restart; open the inner solve once every item of the
-      // system has passed this point
+      // K1 replaced the residual: the new direction p = z + beta p (or z),
+      // then the inner solve opens once every item of the system has passed
+      const bool keep = __ldg(&S.keep_p) != 0;
+      const double beta_d = keep ? __ldg(&S.rzb[q ^ 1]) / __ldg(&S.rz_keep) : 0.0;
+      const bool use = keep && isfinite(beta_d);
+      const T beta = (T)beta_d;
+      for (int i = tl.row0 + lane; i < end; i += 32) {
+        const T z = PRE ? d.r[i] * d.invd[i] : d.r[i];
+        d.p[i] = use ? fma(beta, d.p[i], z) : z;
+      }
       if (warp_last(ig.count, &S.ticket[2]) && lane == 0) S.phase = PH_INNER;
       return;
     }
@@ -665,6 +685,12 @@ __global__ void __launch_bounds__(kBlock, 4) batch_direction_kernel(PassLists L,
       S.inner_iter = it + steps;
       S.total_iter = tot + steps;
       if (ok) S.res_in = res;
+      if (done) {
+        // the next inner solve continues this direction (p is left as the
+        // direction of this last step) unless it broke down
+        S.rz_keep = rz_cur;
+        S.keep_p = (ok && isfinite(res) && !prm.restart_inner) ? 1 : 0;
+      }
     }
     if (!done) {
       // this step's correction c += alpha p (with p before its update), then
@@ -1760,7 +1786,7 @@ int b200la_batch_create(b200la_ctx ctx, const b200la_batch_params *p, b200la_bat
   B->ctx = ctx;
   B->prm = *p;
   B->kp = BatchParams{p->max_outer, p->inner_maxits, p->atol, p->rtol, p->dtol, p->inner_rtol, p->precond ? 1 : 0,
-                      p->mixed ? 1 : 0};
+                      p->mixed ? 1 : 0, p->restart_inner ? 1 : 0};
   // K1 sweeps 256-row items (8 slices per warp keep its gather chains
   // short); K2 streams 1024-row items, K3 512; the tuner may change them
   for (int k = 0; k < 3; ++k) B->lst[k].rows = p->tile_rows ? p->tile_rows : kDefaultRows[k];

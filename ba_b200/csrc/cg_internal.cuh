@@ -11,6 +11,7 @@ constexpr int kMaxIts = 10000000;
 // Device-resident scalars of one CG solve.
 struct CgScalars {
   double rz;        // r.z of the current residual (r.r without preconditioner)
+  double rz_prev;   // r.z before the last step (the denominator of the next beta)
   double pAp;
   double alpha;
   double beta;
@@ -55,6 +56,12 @@ int cg_create_ex(b200la_mat A, const b200la_cg_params *prm, int vdtype, b200la_m
 // Start a solve on the context stream: r = b - A x0 (x0, b device buffers of
 // the solver's value type), or r = b with x0 = 0 when x_dev is nullptr.
 int cg_start(b200la_cg s, const void *x_dev, const void *b_dev);
+// Continue a solve from a new residual already written to s->r (an outer
+// refinement pass replaced the recurrence residual by the true one): x = 0,
+// z = invD r, and p = z + beta p with beta = rz_new / rz_prev (the search
+// direction is kept), or p = z when `restart`.  sums = {r.r, r.z} of the new
+// residual (device; r.r twice without preconditioner).
+int cg_resume(b200la_cg s, const double *sums, bool restart);
 // Run the device loop (one graph launch); the solution stays in s->x.
 int cg_run(b200la_cg s);
 // Copy the scalars to the host (synchronises the context stream).

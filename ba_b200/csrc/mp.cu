@@ -15,7 +15,9 @@
 // res0_ to the latest residual after every pass (mpir.cc:239), which would
 // make a relative tolerance relative to the previous pass instead.
 #include <cmath>
+#include <cstddef>
 #include <cstring>
+#include <type_traits>
 
 #include "cg_internal.cuh"
 #include "spmv.cuh"
@@ -25,32 +27,43 @@ namespace b200la {
 struct MpScalars {
   double rr;
   double res;
+  double in[2];     // r.r and r.z of the residual in the inner type (the inner solve's new start)
   unsigned ticket[2];
 };
 
-// R = type of the inner solve's right-hand side (float, or double under
-// mixed storage)
-template <typename Op, typename R> struct ResidualEmit {
+// The FP64 residual r = b - A64 x, its norm, and its copy in the inner
+// solve's type R (float, or double under mixed storage) written straight into
+// the inner solve's r, with that copy's r.r and r.z (Jacobi) in the inner
+// arithmetic, as the inner solve's own kernels form them.
+template <typename Op, typename R, bool PRE> struct ResidualEmit {
   const double *__restrict__ b;
   R *__restrict__ rin;
+  const R *__restrict__ invd;
   Acc<double> rr;
+  Acc<R> rr_in, rz_in;
   __device__ __forceinline__ void operator()(int row, double y) {
     const double r = b[row] - y;
-    rin[row] = (R)r;
+    const R ri = (R)r;
+    rin[row] = ri;
     rr.add(r * r);
+    rr_in.add(ri * ri);
+    if (PRE) rz_in.add(ri * (ri * invd[row]));
   }
 };
 
-template <typename Op, typename R>
+template <typename Op, typename R, bool PRE>
 __global__ void __launch_bounds__(kBlock) mp_residual_kernel(Op op, const double *__restrict__ x,
                                                              const double *__restrict__ b, R *__restrict__ rin,
-                                                             double *part, MpScalars *sc) {
-  ResidualEmit<Op, R> e{b, rin};
+                                                             const R *__restrict__ invd, double *part,
+                                                             MpScalars *sc) {
+  ResidualEmit<Op, R, PRE> e{b, rin, invd};
   op.run(x, e);
-  double s[1] = {e.rr.value()};
-  if (grid_sum_last<1>(s, part, &sc->ticket[0]) && threadIdx.x == 0) {
+  double s[3] = {e.rr.value(), e.rr_in.value(), e.rz_in.value()};
+  if (grid_sum_last<3>(s, part, &sc->ticket[0]) && threadIdx.x == 0) {
     sc->rr = s[0];
     sc->res = sqrt(s[0]);
+    sc->in[0] = s[1];
+    sc->in[1] = PRE ? s[2] : s[1];
   }
 }
 
@@ -98,7 +111,6 @@ struct b200la_mp_s {
   b200la_mp_params prm;
   b200la_cg inner;
   int64_t n;
-  void *rin;         // the inner solve's right-hand side: float, or double under mixed storage
   double *part;
   MpScalars *sc;
   MpScalars *sc_host;
@@ -110,20 +122,22 @@ static int mp_residual(b200la_mp s, const double *x, const double *b, double *re
   b200la_mat A = s->A64;
   cudaStream_t st = A->ctx->stream;
   const bool f64in = s->prm.inner_storage == B200LA_MP_F32_VALUES;
-  B_TRY(with_schedule<double>(A, [&](auto op) -> int {
+  auto launch = [&](auto op, auto rtag, auto pre) -> int {
     using Op = decltype(op);
+    using R = decltype(rtag);
+    constexpr bool PRE = decltype(pre)::value;
     int grid;
-    if (f64in) {
-      B_TRY(grid_for(A->ctx, (const void *)mp_residual_kernel<Op, double>, op.work_items(), Op::kRowsPerBlock,
-                     &grid));
-      mp_residual_kernel<Op, double><<<grid, kBlock, 0, st>>>(op, x, b, (double *)s->rin, s->part, s->sc);
-    } else {
-      B_TRY(grid_for(A->ctx, (const void *)mp_residual_kernel<Op, float>, op.work_items(), Op::kRowsPerBlock,
-                     &grid));
-      mp_residual_kernel<Op, float><<<grid, kBlock, 0, st>>>(op, x, b, (float *)s->rin, s->part, s->sc);
-    }
+    B_TRY(grid_for(A->ctx, (const void *)mp_residual_kernel<Op, R, PRE>, op.work_items(), Op::kRowsPerBlock,
+                   &grid));
+    mp_residual_kernel<Op, R, PRE><<<grid, kBlock, 0, st>>>(op, x, b, (R *)s->inner->r, (const R *)s->inner->invd,
+                                                            s->part, s->sc);
     B_CUDA(cudaGetLastError());
     return B200LA_OK;
+  };
+  const bool pre = s->prm.precond != 0;
+  B_TRY(with_schedule<double>(A, [&](auto op) -> int {
+    if (f64in) return pre ? launch(op, double(), std::true_type()) : launch(op, double(), std::false_type());
+    return pre ? launch(op, float(), std::true_type()) : launch(op, float(), std::false_type());
   }));
   B_CUDA(cudaMemcpyAsync(s->sc_host, s->sc, sizeof(MpScalars), cudaMemcpyDeviceToHost, st));
   B_CUDA(cudaStreamSynchronize(st));
@@ -141,7 +155,6 @@ int b200la_mp_destroy(b200la_mp s) {
   cudaStreamSynchronize(st);
   if (s->inner) b200la_cg_destroy(s->inner);
   if (s->A32) b200la_mat_destroy(s->A32);
-  if (s->rin) cudaFreeAsync(s->rin, st);
   if (s->part) cudaFreeAsync(s->part, st);
   if (s->sc) cudaFreeAsync(s->sc, st);
   if (s->sc_host) cudaFreeHost(s->sc_host);
@@ -174,9 +187,7 @@ int b200la_mp_create(b200la_mat A64, const b200la_mp_params *prm, b200la_mp *out
     rc = f64in ? cg_create_ex(s->A32, &ip, B200LA_F64, A64, &s->inner) : b200la_cg_create(s->A32, &ip, &s->inner);
   }
   if (rc == B200LA_OK &&
-      (cudaMallocAsync(&s->rin, (f64in ? sizeof(double) : sizeof(float)) * (s->n > 0 ? s->n : 1), st) !=
-           cudaSuccess ||
-       cudaMallocAsync(&s->part, sizeof(double) * kMaxReduceBlocks, st) != cudaSuccess ||
+      (cudaMallocAsync(&s->part, sizeof(double) * 3 * kMaxReduceBlocks, st) != cudaSuccess ||
        cudaMallocAsync(&s->sc, sizeof(MpScalars), st) != cudaSuccess ||
        cudaMallocHost(&s->sc_host, sizeof(MpScalars)) != cudaSuccess ||
        cudaMemsetAsync(s->sc, 0, sizeof(MpScalars), st) != cudaSuccess))
@@ -217,9 +228,16 @@ int b200la_mp_solve(b200la_mp s, b200la_vec b, b200la_vec x, b200la_mp_result *r
   if (f64in) B_TRY(grid_for(c, (const void *)mp_correct64_kernel, (s->n + 1) / 2, kBlock, &grid_c));
   else B_TRY(grid_for(c, (const void *)mp_correct_kernel, (s->n + 3) / 4, kBlock, &grid_c));
   auto done = [&](double v) { return v <= p.atol || v < p.rtol * r0 || !(v <= p.dtol * r0); };
+  // every pass continues the inner solve from the true residual the last
+  // residual kernel wrote into it; its search direction is kept unless
+  // restart_inner is set, this is the first pass, or the last pass took no
+  // step or broke down
+  bool restart = true;
   while (!done(r) && outer < p.max_outer) {
     ++outer;
-    B_TRY(cg_start(s->inner, nullptr, s->rin));
+    const double *sums = reinterpret_cast<const double *>(reinterpret_cast<const char *>(s->sc) +
+                                                          offsetof(MpScalars, in));  // device address
+    B_TRY(cg_resume(s->inner, sums, restart || p.restart_inner != 0));
     B_TRY(cg_run(s->inner));
     if (f64in) mp_correct64_kernel<<<grid_c, kBlock, 0, st>>>(s->n, (double *)x->d, (const double *)s->inner->x);
     else mp_correct_kernel<<<grid_c, kBlock, 0, st>>>(s->n, (double *)x->d, (const float *)s->inner->x);
@@ -228,6 +246,10 @@ int b200la_mp_solve(b200la_mp s, b200la_vec b, b200la_vec x, b200la_mp_result *r
     CgScalars h;
     B_TRY(cg_fetch(s->inner, &h));
     inner_total += h.iter;
+    // restart the direction when the pass took no step or broke down, or when
+    // the replaced residual is more than twice the recurrence's last one (the
+    // inner recurrence drifted far from the true residual)
+    restart = h.iter == 0 || h.state == B200LA_FAIL_BREAKDOWN || !(sqrt(s->sc_host->in[0]) <= 2.0 * h.res);
   }
   res->outer = outer;
   res->inner_iters = inner_total;

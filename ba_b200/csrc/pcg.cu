@@ -177,6 +177,7 @@ __global__ void __launch_bounds__(kBlock) cg_update_kernel(CgVecs<T> v, double *
     int st = iterate_check(it, res, *sc, sc->res_init);
     double rz_new = PRE ? s[1] : s[0];
     sc->beta = rz_new / sc->rz;
+    sc->rz_prev = sc->rz;
     sc->rz = rz_new;
     sc->state = st;
   }
@@ -217,6 +218,35 @@ __global__ void __launch_bounds__(kBlock) cg_direction_kernel(CgVecs<T> v, CgSca
   }
   for (int64_t i = nv * W + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
     v.p[i] = fma(beta, v.p[i], PRE ? v.r[i] * v.invd[i] : v.r[i]);
+}
+
+// ---- resume after a residual replacement: x = 0, p = z + beta p ------------------
+// Every block derives beta from the same two scalars; block 0 then resets the
+// solve's scalars for the new start (none of which the other blocks read).
+template <typename T, bool PRE>
+__global__ void __launch_bounds__(kBlock) cg_resume_kernel(CgVecs<T> v, const double *__restrict__ sums,
+                                                           CgScalars *sc, int restart) {
+  const double rr = sums[0], rz_new = PRE ? sums[1] : sums[0];
+  const double beta_d = rz_new / __ldg(&sc->rz_prev);
+  const bool keep = !restart && isfinite(beta_d);
+  const T beta = keep ? (T)beta_d : T(0);
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < v.n; i += stride) {
+    const T r = v.r[i];
+    const T z = PRE ? r * v.invd[i] : r;
+    v.x[i] = T(0);
+    v.p[i] = keep ? fma(beta, v.p[i], z) : z;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    const double res = sqrt(rr);
+    sc->rr = rr;
+    sc->rz = rz_new;
+    sc->res = res;
+    sc->res_init = res;
+    sc->iter = 0;
+    sc->guard = 0;
+    sc->state = iterate_check(0, res, *sc, res);
+  }
 }
 
 }  // namespace b200la
@@ -326,6 +356,20 @@ static int cg_launch_init(b200la_cg s, const void *x_user, const void *b) {
 }
 
 int cg_start(b200la_cg s, const void *x_dev, const void *b_dev) { return cg_launch_init(s, x_dev, b_dev); }
+
+int cg_resume(b200la_cg s, const double *sums, bool restart) {
+  cudaStream_t st = s->A->ctx->stream;
+  return cg_types(s, [&](auto m, auto t, auto pre) -> int {
+    using T = decltype(t);
+    constexpr bool PRE = decltype(pre)::value;
+    CgVecs<T> v{(T *)s->x, (T *)s->r, (T *)s->p, (T *)s->Ap, (const T *)s->invd, s->n};
+    int grid;
+    B_TRY(grid_for(s->A->ctx, (const void *)cg_resume_kernel<T, PRE>, s->n, kBlock, &grid));
+    cg_resume_kernel<T, PRE><<<grid, kBlock, 0, st>>>(v, sums, s->sc, restart ? 1 : 0);
+    B_CUDA(cudaGetLastError());
+    return B200LA_OK;
+  });
+}
 
 template <typename M, typename T, bool PRE>
 static int cg_host_loop_t(b200la_cg s) {

@@ -732,6 +732,9 @@ class MPIR:
         self.tune = True
         # fast form: 0 = FP32 inner PCG; 1 = FP32 matrix values under FP64 vectors and dots
         self.inner_storage = 0
+        # fast form: False = each pass continues the inner PCG from the FP64 residual with
+        # its search direction kept; True = restart it each pass (as MPIR restarts its solver)
+        self.restart_inner = False
         self._s = C.c_void_p()
         self.iter_ = 0
         self.outer_ = 0
@@ -750,6 +753,13 @@ class MPIR:
     def SetupOperator(self, op: B200_CSR_lMatrix):
         self.op = op
         self.Ah = op
+        self._release()
+
+    def SetInnerRestart(self, restart: bool):
+        """Fast form: restart the inner PCG from p = z at every refinement
+        pass (True, as MPIR restarts its error-correction solver) or keep its
+        search direction across passes (False, the default)."""
+        self.restart_inner = bool(restart)
         self._release()
 
     def SetInnerStorage(self, f64_vectors: bool):
@@ -860,7 +870,7 @@ class MPIR:
             raise B200LAError(-7, "MPIR: high-precision correction passes need SetHighPrecErrCorSolver")
         prm = _lib.MpParams(self.max_ecl, self.abs_tol, self.rel_tol, self.div_tol, self.inner_maxits,
                             self.inner_rtol, 1 if self.precond else 0, 1 if self.tune else 0,
-                            int(self.inner_storage))
+                            int(self.inner_storage), 1 if self.restart_inner else 0)
         call("b200la_mp_create", self.op.handle, C.byref(prm), C.byref(self._s))
 
     # ---- generic form: SolveImpl (mpir.cc:52-285), ContinueIteration (:288-297)

@@ -27,12 +27,14 @@ from .lmp import Platform, _finalizing, init_platform
 
 class Server:
     def __init__(self, capacity: int = 256, *, mixed: bool = True, precond: bool = True, rtol: float = 1e-8,
-                 atol: float = 0.0, dtol: float = 1e8, inner_rtol: float = 1e-4, max_outer: int = 30,
+                 atol: float = 0.0, dtol: float = 1e8, inner_rtol: float = 0.1, max_outer: int = 30,
                  inner_maxits: int = 100000, tile_rows: int = 0, hbm_budget: int = 0, chunk_passes: int = 32,
-                 max_skips: int = 8, adaptive: bool = True, platform: Platform | None = None):
+                 max_skips: int = 8, adaptive: bool = True, restart_inner: bool = False,
+                 platform: Platform | None = None):
         self.platform = platform or init_platform()
         bp = BatchParams(int(capacity), int(mixed), int(precond), int(max_outer), int(inner_maxits), int(adaptive),
-                         int(tile_rows), 0, float(atol), float(rtol), float(dtol), float(inner_rtol))
+                         int(tile_rows), 0, float(atol), float(rtol), float(dtol), float(inner_rtol),
+                         1 if restart_inner else 0)
         prm = ServerParams(bp, int(hbm_budget), int(chunk_passes), int(max_skips))
         self.handle = C.c_void_p()
         call("b200la_server_start", self.platform.handle, C.byref(prm), C.byref(self.handle))

@@ -310,7 +310,11 @@ int b200la_q1_assemble(b200la_ctx ctx, int dim, int cells, uint64_t seed, double
  * solve runs SpMV and vector updates in FP32 (FP32 matrix values, int32
  * indices, dot products accumulated in FP32 with compensated summation).
  * The outer test is relative to the initial residual (the reference resets
- * res0_ every pass, mpir.cc:239). */
+ * res0_ every pass, mpir.cc:239).  By default a pass does not restart the
+ * inner PCG: the FP64 residual replaces its recurrence residual and the
+ * search direction carries on (restart_inner = 1 restarts it as MPIR does;
+ * restarting discards the Krylov space built so far, which on the 128^3
+ * lognormal case costs ~1.5x the FP64 PCG's iterations). */
 typedef struct {
   int max_outer;      /* refinement passes (MPIR max_ecl) */
   double atol;        /* success if ||r||_2 <= atol */
@@ -322,7 +326,11 @@ typedef struct {
   int tune;           /* 1: autotune the FP32 matrix's SpMV schedule at create */
   int inner_storage;  /* B200LA_MP_F32 (0): the inner PCG keeps FP32 vectors; B200LA_MP_F32_VALUES (1):
                          FP32 matrix values (the bulk of the bytes) under FP64 vectors, dot products
-                         and Jacobi scaling, which keeps the inner iteration count near FP64 PCG's */
+                         and Jacobi scaling */
+  int restart_inner;  /* 0: every pass after the first continues the inner PCG from the new FP64
+                         residual with its search direction kept (p = z + beta p, the residual
+                         replacement of "reliable updates"); 1: restart it from p = z each pass, as
+                         MPIR restarts its error-correction solver */
 } b200la_mp_params;
 #define B200LA_MP_F32 0
 #define B200LA_MP_F32_VALUES 1
@@ -369,7 +377,10 @@ typedef struct {
   int index_bits;     /* sliced-ELL column storage: 0 = int16 offsets from the row when
                          every column is within int16 of its row, else int32; 32 = int32 */
   double atol, rtol, dtol;  /* test on ||b - A x||_2 (FP64 mode: the CG recurrence residual) */
-  double inner_rtol;        /* mixed: inner solve stops at inner_rtol x its start residual */
+  double inner_rtol;        /* mixed: an inner pass ends at inner_rtol x its start residual */
+  int restart_inner;        /* mixed: 0 = each pass continues the inner PCG from the replaced FP64
+                               residual with its search direction kept (residual replacement;
+                               inner_rtol ~0.1); 1 = restart it from p = z as MPIR does */
 } b200la_batch_params;
 
 typedef struct {

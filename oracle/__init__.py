@@ -36,6 +36,7 @@ from .oracle import (  # noqa: F401
     iterate_check,
     jacobi,
     lmp_cg,
+    mpcg_kept,
     mpir,
     mpir_generic,
     ref_available,

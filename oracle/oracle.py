@@ -58,8 +58,11 @@ def _load():
         lib.orc_iterate_check.argtypes = [C.c_int, C.c_double, C.c_int, C.c_double, C.c_double,
                                           C.c_double, _dp]
         lib.orc_mpir_d.argtypes = [C.c_int, _i32p, _i32p, _f64p, _f32p, _f64p, _f64p, C.c_int,
-                                   C.c_double, C.c_double, C.c_int, _f64p, _f32p, _f64p, _f32p,
+                                   C.c_double, C.c_double, C.c_double, C.c_int, _f64p, _f32p, _f64p, _f32p,
                                    _ip, _ip, _dp, _dp]
+        lib.orc_mpcg_kept_d.argtypes = [C.c_int, _i32p, _i32p, _f64p, _f32p, _f64p, _f64p, C.c_int,
+                                        C.c_double, C.c_double, C.c_double, C.c_int, _f32p, _f64p, _f32p,
+                                        _ip, _ip, _dp, _dp]
         _lib = lib
     return _lib
 
@@ -187,7 +190,7 @@ def lmp_cg(rowptr, col, val, b, x0=None, *, rel_eps=1e-10, abs_eps=0.0, max_iter
 
 
 def mpir(rowptr, col, val, b, *, rtol=1e-10, inner_rtol=1e-4, inner_maxits=100000,
-         max_outer=50) -> tuple[OracleResult, int]:
+         max_outer=50, floor=0.0) -> tuple[OracleResult, int]:
     """FP64 refinement around a float Jacobi-PCG (MPIR structure)."""
     rp, c, v = _csr(rowptr, col, val, np.float64)
     v32 = v.astype(np.float32)
@@ -197,9 +200,29 @@ def mpir(rowptr, col, val, b, *, rtol=1e-10, inner_rtol=1e-4, inner_maxits=10000
     inv32 = invdiag(rp, c, v32, np.float32)
     outer, inner, res, res0 = C.c_int(), C.c_int(), C.c_double(), C.c_double()
     st = _load().orc_mpir_d(n, rp, c, v, v32, np.ascontiguousarray(b, np.float64), x, max_outer,
-                            rtol, inner_rtol, inner_maxits, inv, inv32, np.empty(3 * n),
+                            rtol, inner_rtol, floor, inner_maxits, inv, inv32, np.empty(3 * n),
                             np.empty(8 * n, np.float32), C.byref(outer), C.byref(inner),
                             C.byref(res), C.byref(res0))
+    return OracleResult(x, inner.value, res.value, res0.value, st), outer.value
+
+
+def mpcg_kept(rowptr, col, val, b, *, rtol=1e-10, inner_rtol=0.1, inner_maxits=100000,
+              max_outer=50, floor=0.0) -> tuple[OracleResult, int]:
+    """Mixed-precision Jacobi-PCG with residual replacement (the device's
+    default fused refinement: float inner PCG whose recurrence residual is
+    replaced by the double b - A x every inner_rtol reduction, search
+    direction kept).  Returns (result with the total inner iterations,
+    passes)."""
+    rp, c, v = _csr(rowptr, col, val, np.float64)
+    v32 = v.astype(np.float32)
+    n = rp.shape[0] - 1
+    x = np.zeros(n, np.float64)
+    inv32 = invdiag(rp, c, v32, np.float32)
+    outer, inner, res, res0 = C.c_int(), C.c_int(), C.c_double(), C.c_double()
+    st = _load().orc_mpcg_kept_d(n, rp, c, v, v32, np.ascontiguousarray(b, np.float64), x, max_outer,
+                                 rtol, inner_rtol, floor, inner_maxits, inv32, np.empty(n),
+                                 np.empty(6 * n, np.float32),
+                                 C.byref(outer), C.byref(inner), C.byref(res), C.byref(res0))
     return OracleResult(x, inner.value, res.value, res0.value, st), outer.value
 
 

@@ -524,13 +524,15 @@ ORACLE_GMRES(float, f, sqrtf, fabsf)
  * outer stopping test is relative to the INITIAL residual.  (The reference
  * overwrites res0_ with the latest residual after every pass, mpir.cc:239,
  * so its relative test compares against the previous pass instead; the
- * north-star tolerance is stated relative to the initial residual.)
- * work must hold 3n doubles + 6n floats.  Returns 0 on success, 1 if
+ * north-star tolerance is stated relative to the initial residual.)  An
+ * inner solve also stops once its residual is at or below floor_frac * rtol
+ * * (initial residual), as the batch's last pass does (floor_frac 0.5; 0 for
+ * none).  work must hold 3n doubles + 6n floats.  Returns 0 on success, 1 if
  * max_outer passes did not reach the tolerance.
  */
 int orc_mpir_d(int n, const int *rowptr, const int *col, const double *val,
                const float *val32, const double *b, double *x, int max_outer,
-               double rtol, double inner_rtol, int inner_maxits,
+               double rtol, double inner_rtol, double floor_frac, int inner_maxits,
                const double *invd, const float *invd32, double *work64,
                float *work32, int *outer_iters, int *inner_iters_total,
                double *res_out, double *res_init_out) {
@@ -548,8 +550,8 @@ int orc_mpir_d(int n, const int *rowptr, const int *col, const double *val,
     for (int i = 0; i < n; ++i) { r32[i] = (float)r[i]; c32[i] = 0.f; }
     int it = 0;
     double ires, ires0;
-    orc_cg_f(n, rowptr, col, val32, r32, c32, inner_maxits, 0., inner_rtol,
-             1e30, 1, invd32, w32, &it, &ires, &ires0);
+    orc_cg_f(n, rowptr, col, val32, r32, c32, inner_maxits, floor_frac * rtol * res0,
+             inner_rtol, 1e30, 1, invd32, w32, &it, &ires, &ires0);
     inner_total += it;
     for (int i = 0; i < n; ++i) c[i] = (double)c32[i];
     orc_axpy_d(n, x, c, 1.);
@@ -561,6 +563,90 @@ int orc_mpir_d(int n, const int *rowptr, const int *col, const double *val,
   *inner_iters_total = inner_total;
   *res_out = res;
   return res <= rtol * res0 ? 0 : 1;
+}
+
+/*
+ * Mixed-precision CG with residual replacement -- the B200 library's default
+ * fused refinement (b200la_mp with restart_inner = 0, and the batch's mixed
+ * mode), not a reference algorithm: the reference's MPIR restarts its inner
+ * solver every pass (orc_mpir_d above).  A float Jacobi-PCG runs on the float
+ * copy of the matrix; once its recurrence residual has fallen below
+ * inner_rtol times its value at the last replacement (IterateControl with
+ * rtol = inner_rtol, strict), its correction goes into x in double, the
+ * recurrence residual is replaced by the float copy of b - A x computed in
+ * double, and the search direction carries on: p = z + beta p with
+ * beta = (r.z of the new residual) / (r.z before the last step).  The first
+ * pass, a pass after one that took no step, and a pass whose new residual is
+ * more than twice the recurrence's last one start from p = z.  The
+ * outer test (strict, relative to the first residual) is as orc_mpir_d's.
+ * An inner pass never aims below floor_frac * rtol * (first residual): the
+ * batch stops its last pass at half the outer target (floor_frac = 0.5), the
+ * single-system solver does not (0).  work64 holds n doubles, work32 6n
+ * floats.
+ */
+int orc_mpcg_kept_d(int n, const int *rowptr, const int *col, const double *val,
+                    const float *val32, const double *b, double *x, int max_outer,
+                    double rtol, double inner_rtol, double floor_frac, int inner_maxits,
+                    const float *invd32, double *work64, float *work32,
+                    int *outer_iters, int *inner_iters_total, double *res_out,
+                    double *res_init_out) {
+  double *r = work64;
+  float *r32 = work32, *c32 = work32 + n, *p32 = work32 + 2 * (size_t)n;
+  float *ap32 = work32 + 3 * (size_t)n, *z32 = work32 + 4 * (size_t)n;
+  orc_spmv_d(n, rowptr, col, val, x, r);
+  orc_scaleadd_d(n, r, -1., b);
+  double res = sqrt(orc_dot_d(n, r, r));
+  const double res0 = res;
+  *res_init_out = res0;
+  int k = 0, inner_total = 0, restart = 1;
+  float rz_prev = 0.f;
+  double rec_res = 0.; /* recurrence residual at the end of the last pass */
+  while (!(res < rtol * res0) && k < max_outer) {
+    ++k;
+    for (int i = 0; i < n; ++i) {
+      r32[i] = (float)r[i];
+      c32[i] = 0.f;
+      z32[i] = r32[i] * invd32[i];
+    }
+    float rz = orc_dot_f(n, r32, z32);
+    const float beta0 = rz / rz_prev;
+    const double rr_new = (double)orc_dot_f(n, r32, r32);
+    /* a replaced residual more than twice the recurrence's last one means
+     * the float recurrence drifted far from the true residual: the old
+     * direction is then restarted (p = z) rather than kept */
+    const int keep = !restart && isfinite(beta0) && !(sqrt(rr_new) > 2. * rec_res);
+    for (int i = 0; i < n; ++i) p32[i] = keep ? beta0 * p32[i] + z32[i] : z32[i];
+    const double ires0 = (double)sqrtf(orc_dot_f(n, r32, r32));
+    int it = 0, broke = 0;
+    while (!(ires0 <= 0.) && it < inner_maxits) {
+      orc_spmv_f(n, rowptr, col, val32, p32, ap32);
+      const float pap = orc_dot_f(n, p32, ap32);
+      const float alpha = rz / pap;
+      if (pap == 0.f || !isfinite(alpha)) { broke = 1; break; }
+      orc_axpy_f(n, c32, p32, alpha);
+      orc_axpy_f(n, r32, ap32, -alpha);
+      ++it;
+      for (int i = 0; i < n; ++i) z32[i] = r32[i] * invd32[i];
+      const float rz_new = orc_dot_f(n, r32, z32);
+      const double ires = (double)sqrtf(orc_dot_f(n, r32, r32));
+      rz_prev = rz;
+      rz = rz_new;
+      rec_res = ires;
+      if (ires < fmax(inner_rtol * ires0, floor_frac * rtol * res0)) break;
+      const float beta = rz_new / rz_prev;
+      orc_scaleadd_f(n, p32, beta, z32);
+    }
+    inner_total += it;
+    restart = it == 0 || broke;
+    for (int i = 0; i < n; ++i) x[i] += (double)c32[i];
+    orc_spmv_d(n, rowptr, col, val, x, r);
+    orc_scaleadd_d(n, r, -1., b);
+    res = sqrt(orc_dot_d(n, r, r));
+  }
+  *outer_iters = k;
+  *inner_iters_total = inner_total;
+  *res_out = res;
+  return res < rtol * res0 ? 0 : 1;
 }
 
 /*

@@ -86,7 +86,7 @@ def _true_rel_res(s, x):
 def test_mixed_batch_reaches_tolerance(plat):
     sizes = P.batch_sizes(24, lo=16, hi=64, seed=5)
     systems = [P.q1_system(2, int(n), 500 + k, 1.0, f"b{k}") for k, n in enumerate(sizes)]
-    B = Batch(32, mixed=True, precond=True, rtol=1e-8, inner_rtol=1e-4, platform=plat)
+    B = Batch(32, mixed=True, precond=True, rtol=1e-8, platform=plat)
     B.tune()
     slots = [B.add_system(s) for s in systems]
     assert B.run() == 0
@@ -102,10 +102,39 @@ def test_mixed_batch_reaches_tolerance(plat):
         assert r.outer >= 2 and r.device_us > 0
 
 
+@pytest.mark.parametrize("restart", [False, True])
+def test_mixed_batch_passes_match_oracle(plat, restart):
+    """Mixed mode per system against the oracle's restatement of the same
+    refinement: with kept directions (default; oracle.mpcg_kept) and
+    restarted per pass (oracle.mpir, MPIR's form), both with the batch's
+    last-pass floor (an inner pass stops at half the outer target).  Passes within one, inner iterations within 10% (the device's
+    FP32 dots are compensated and tree-ordered, the oracle's are the
+    reference's grouped sums), FP64 true residual at the tolerance."""
+    systems = _mix(seed=7, count=9)
+    irt = 1e-4 if restart else 0.1
+    B = Batch(16, mixed=True, precond=True, rtol=1e-9, inner_rtol=irt, restart_inner=restart, max_outer=40,
+              platform=plat)
+    slots = B.add_many([(s.rowptr, s.col, s.val, s.b) for s in systems])
+    B.solve()
+    rows = []
+    for s, r in zip(systems, B.results(slots)):
+        if restart:
+            ref, passes = oracle.mpir(s.rowptr, s.col, s.val, s.b, rtol=1e-9, inner_rtol=irt, max_outer=40,
+                                      floor=0.5)
+        else:
+            ref, passes = oracle.mpcg_kept(s.rowptr, s.col, s.val, s.b, rtol=1e-9, inner_rtol=irt, max_outer=40,
+                                           floor=0.5)
+        assert r.solver_state == lmp.kSolverSuccess and ref.state == 0, (s.name, r)
+        assert _true_rel_res(s, r.x) < 1.0001e-9, s.name
+        rows.append((s.name, r.outer, passes, r.iters, ref.iters))
+    bad = [x for x in rows if abs(x[1] - x[2]) > 1 or abs(x[3] - x[4]) > max(3, 0.1 * x[4])]
+    assert not bad, rows
+
+
 def test_isolation_alone_vs_mix_vs_late_admission(plat):
     systems = _mix(seed=3, count=9)
     probe = systems[4]
-    kw = dict(mixed=True, precond=True, rtol=1e-9, inner_rtol=1e-4, platform=plat)
+    kw = dict(mixed=True, precond=True, rtol=1e-9, platform=plat)
     # alone
     A = Batch(1, **kw)
     a = A.add_system(probe)
@@ -229,7 +258,7 @@ def test_large_system_ticket_path_isolated_and_converged(plat):
     # last-arriver ticket, while the small systems re-add their partials.
     big = P.q1_system(3, 66, 77, 1.0, "big3d_66")
     small = [P.q1_system(2, c, 500 + c, 1.0, f"s{c}") for c in (9, 30, 64)]
-    kw = dict(mixed=True, precond=True, rtol=1e-8, inner_rtol=1e-4, platform=plat)
+    kw = dict(mixed=True, precond=True, rtol=1e-8, platform=plat)
     A = Batch(1, **kw)
     A.set_items(128, 128, 256, adaptive=False)
     a = A.add_system(big)
@@ -257,7 +286,7 @@ def test_adds_overlapping_launches_match_the_plain_solve(plat):
     # all are added first: a system's arithmetic does not depend on when it
     # joined or on what else runs
     systems = _mix(seed=5, count=12)
-    kw = dict(mixed=True, precond=True, rtol=1e-9, inner_rtol=1e-4, platform=plat)
+    kw = dict(mixed=True, precond=True, rtol=1e-9, platform=plat)
     A = Batch(16, **kw)
     A.set_items(128, 512, 512, adaptive=False)
     slots_a = A.add_many([(s.rowptr, s.col, s.val, s.b) for s in systems])
@@ -288,7 +317,7 @@ def test_initial_guesses_in_one_add_many(plat):
     # and reach the tolerance relative to it
     sizes = P.batch_sizes(8, lo=16, hi=48, seed=9)
     systems = [P.q1_system(2, int(n), 900 + k, 1.0, f"g{k}") for k, n in enumerate(sizes)]
-    kw = dict(mixed=True, precond=True, rtol=1e-8, inner_rtol=1e-4, platform=plat)
+    kw = dict(mixed=True, precond=True, rtol=1e-8, platform=plat)
     A = Batch(8, **kw)
     sa = A.add_many([(s.rowptr, s.col, s.val, s.b) for s in systems])
     A.solve(16)
@@ -319,7 +348,7 @@ def test_registered_outputs_are_copied_as_systems_finish(plat):
     import torch
     sizes = P.batch_sizes(12, lo=16, hi=96, seed=21)
     systems = [P.q1_system(2, int(n), 40 + k, 1.0, f"o{k}") for k, n in enumerate(sizes)]
-    kw = dict(mixed=True, precond=True, rtol=1e-8, inner_rtol=1e-4, platform=plat)
+    kw = dict(mixed=True, precond=True, rtol=1e-8, platform=plat)
     A = Batch(12, **kw)
     sa = A.add_many([(s.rowptr, s.col, s.val, s.b) for s in systems])
     A.solve(8)
@@ -349,7 +378,7 @@ def test_registered_outputs_are_copied_as_systems_finish(plat):
 def test_remove_many(plat):
     sizes = P.batch_sizes(6, lo=16, hi=32, seed=3)
     systems = [P.q1_system(2, int(n), 70 + k, 1.0, f"r{k}") for k, n in enumerate(sizes)]
-    B = Batch(6, mixed=True, precond=True, rtol=1e-8, inner_rtol=1e-4, platform=plat)
+    B = Batch(6, mixed=True, precond=True, rtol=1e-8, platform=plat)
     sl = B.add_many([(s.rowptr, s.col, s.val, s.b) for s in systems])
     used0, bytes0 = B.info()
     # a bad list frees nothing: a repeated slot, a free slot
@@ -363,7 +392,7 @@ def test_remove_many(plat):
     # the freed slots take new systems, and every system still solves alone
     again = B.add_many([(systems[k].rowptr, systems[k].col, systems[k].val, systems[k].b) for k in (1, 2, 4)])
     B.solve(16)
-    ref = Batch(1, mixed=True, precond=True, rtol=1e-8, inner_rtol=1e-4, platform=plat)
+    ref = Batch(1, mixed=True, precond=True, rtol=1e-8, platform=plat)
     one = ref.add_system(systems[2])
     ref.solve(16)
     r = B.results([again[1]])[0]
@@ -382,7 +411,7 @@ def test_remove_and_reuse_slots_while_a_launch_is_in_flight(plat):
     # must end with the bits it gets when solved alone.
     first = [P.q1_system(2, c, 300 + k, 1.0, f"f{k}") for k, c in enumerate((160, 200, 180, 220))]
     second = [P.q1_system(2, c, 400 + k, 1.0, f"s{k}") for k, c in enumerate((40, 64, 90))]
-    kw = dict(mixed=True, precond=True, rtol=1e-8, inner_rtol=1e-4, platform=plat)
+    kw = dict(mixed=True, precond=True, rtol=1e-8, platform=plat)
 
     def alone(s):
         A = Batch(1, **kw)

@@ -17,12 +17,13 @@ def plat():
     return lmp.init_platform(0)
 
 
-def _solve_mp(plat, s, rtol, inner_rtol=1e-5, max_outer=20):
+def _solve_mp(plat, s, rtol, inner_rtol=1e-5, max_outer=20, restart=True):
     A = lmp.B200_CSR_lMatrix(s.rowptr, s.col, s.val, platform=plat)
     b = lmp.B200_lVector.from_numpy(s.b, platform=plat)
     x = lmp.B200_lVector(s.n, platform=plat)
     m = lmp.MPIR()
     m.SetupOperator(A)
+    m.SetInnerRestart(restart)
     m.SetMpirParameters(0, max_outer, 0.0, rtol, 1e6)
     m.SetLowPrecErrCorSolverParameters(100000, 0.0, inner_rtol, 1e30)
     st = m.Solve(b, x)
@@ -79,6 +80,7 @@ def test_mp_fp32_values_fp64_vectors(plat, case):
     m = lmp.MPIR()
     m.SetupOperator(A)
     m.SetInnerStorage(True)
+    m.SetInnerRestart(True)
     m.SetMpirParameters(0, 20, 0.0, 1e-10, 1e6)
     m.SetLowPrecErrCorSolverParameters(100000, 0.0, 1e-5, 1e30)
     assert m.Solve(b, x) == lmp.kSolverSuccess
@@ -96,6 +98,26 @@ def test_mp_fp32_values_fp64_vectors(plat, case):
     m1.Solve(b, x1)
     r64 = oracle.cg(s.rowptr, s.col, s.val, s.b, maxits=100000, atol=0.0, rtol=1e-5)
     assert m1.outer_ == 1 and abs(m1.iter() - r64.iters) <= max(2, 0.05 * r64.iters), (m1.iter(), r64.iters)
+
+
+@pytest.mark.parametrize("case", [("2d", 2, 48, 1.0), ("3d", 3, 20, 2.0), ("2d_s2", 2, 64, 2.0), ("3d40", 3, 40, 2.0)])
+def test_mp_kept_direction_matches_oracle(plat, case):
+    """The default fused refinement: the inner FP32 PCG's residual is
+    replaced by the FP64 residual every 10x reduction and its search
+    direction kept.  Same passes as the oracle's restatement
+    (oracle.mpcg_kept) within one, total inner iterations within 10%, the
+    FP64 residual at the tolerance, and fewer iterations than restarting."""
+    _, dim, n, sigma = case
+    s = P.q1_system(dim, n, 77 + n, sigma)
+    st, m, x = _solve_mp(plat, s, 1e-10, inner_rtol=0.1, max_outer=40, restart=False)
+    ref, passes = oracle.mpcg_kept(s.rowptr, s.col, s.val, s.b, rtol=1e-10, inner_rtol=0.1, max_outer=40)
+    assert st == lmp.kSolverSuccess and ref.state == 0
+    assert abs(m.outer_ - passes) <= 1, (m.outer_, passes)
+    assert abs(m.iter() - ref.iters) <= max(3, 0.1 * ref.iters), (m.iter(), ref.iters)
+    assert np.linalg.norm(s.b - oracle.spmv(s.rowptr, s.col, s.val, x)) < 1.05e-10 * np.linalg.norm(s.b)
+    f64 = oracle.cg(s.rowptr, s.col, s.val, s.b, maxits=100000, atol=0.0, rtol=1e-10)
+    rst, _ = oracle.mpir(s.rowptr, s.col, s.val, s.b, rtol=1e-10, inner_rtol=1e-5)
+    assert m.iter() < rst.iters and m.iter() <= 1.3 * f64.iters, (m.iter(), rst.iters, f64.iters)
 
 
 def test_mp_pass_limit_reports_exceeded(plat):

@@ -288,3 +288,19 @@ def test_coo_to_csr_matches_reference_runs():
         assert (_sha(rp), _sha(c), _sha(v)) == (case["sha_rowptr"], case["sha_col"], case["sha_val"])
     with pytest.raises(ValueError):
         oracle.coo_to_csr(3, 3, [0, 3], [0, 0], [1.0, 1.0])
+
+
+def test_kept_direction_refinement_restatement():
+    # the device's default fused refinement restated: FP32 PCG whose residual
+    # is replaced by the FP64 one every 10x reduction, direction kept.  It
+    # reaches the FP64 tolerance in fewer inner iterations than restarting the
+    # inner solve every pass (MPIR's form), close to the FP64 PCG's count
+    for dim, n, sigma in ((2, 48, 1.0), (3, 20, 2.0)):
+        s = P.q1_system(dim, n, 77 + n, sigma)
+        kept, passes = oracle.mpcg_kept(s.rowptr, s.col, s.val, s.b, rtol=1e-10, inner_rtol=0.1)
+        rst, _ = oracle.mpir(s.rowptr, s.col, s.val, s.b, rtol=1e-10, inner_rtol=1e-5)
+        f64 = oracle.cg(s.rowptr, s.col, s.val, s.b, maxits=100000, atol=0.0, rtol=1e-10)
+        assert kept.state == 0 and passes >= 5
+        r = s.b - oracle.spmv(s.rowptr, s.col, s.val, kept.x)
+        assert np.linalg.norm(r) < 1e-10 * np.linalg.norm(s.b)
+        assert kept.iters < rst.iters and kept.iters <= 1.3 * f64.iters, (kept.iters, rst.iters, f64.iters)
