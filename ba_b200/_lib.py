@@ -30,7 +30,7 @@ class B200LAError(RuntimeError):
 
 class CgParams(C.Structure):
     _fields_ = [("maxits", C.c_int), ("atol", C.c_double), ("rtol", C.c_double),
-                ("dtol", C.c_double), ("precond", C.c_int)]
+                ("dtol", C.c_double), ("precond", C.c_int), ("stop_rule", C.c_int)]
 
 
 class MpParams(C.Structure):
@@ -122,6 +122,7 @@ _SIGS = {
     "b200la_vec_scaleadd": [_vp, _d, _vp],
     "b200la_vec_scale": [_vp, _d],
     "b200la_vec_elementwise_mult": [_vp, _vp],
+    "b200la_vec_range_update": [_vp, _i64, _vp, _i64, _i64, _i, _d],
     "b200la_dot_noalloc": [_vp, _vp, _i64, _i, _vp, _P(_d)],
     "b200la_csr_upload": [_vp, _i, _i, _i64, _vp, _vp, _vp, _i, _i, _P(_vp)],
     "b200la_coo_upload": [_vp, _i, _i, _i64, _vp, _vp, _vp, _i, _i, _i, _P(_vp)],
@@ -132,6 +133,7 @@ _SIGS = {
     "b200la_mat_zero_rows": [_vp, _vp, _i, _d],
     "b200la_spmv": [_vp, _vp, _vp],
     "b200la_spmv_add": [_vp, _vp, _vp],
+    "b200la_spmv_nodiag": [_vp, _vp, _vp],
     "b200la_mat_inv_diag": [_vp, _vp],
     "b200la_mat_set_format": [_vp, _i, _i],
     "b200la_mat_get_format": [_vp, _P(_i), _P(_i)],

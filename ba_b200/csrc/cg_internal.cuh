@@ -23,6 +23,7 @@ struct CgScalars {
   int state;
   int maxits;
   int guard;        // body passes, counted by the direction kernel
+  int stop_rule;    // B200LA_STOP_ITERATE_CONTROL or B200LA_STOP_LMP_CG
   unsigned ticket[4];
 };
 

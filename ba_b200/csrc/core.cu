@@ -127,6 +127,16 @@ __global__ void __launch_bounds__(kBlock) cast_kernel(int64_t n, D *__restrict__
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) d[i] = (D)s[i];
 }
 
+// dst[i] = src[i] (add = 0) or dst[i] += w * src[i] over a sub-range at
+// arbitrary offsets (no vector loads: the ranges need not be aligned)
+template <typename T>
+__global__ void __launch_bounds__(kBlock) range_kernel(int64_t n, T *__restrict__ dst, const T *__restrict__ src,
+                                                       int add, T w) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+    dst[i] = add ? fma(w, src[i], dst[i]) : src[i];
+}
+
 // Dot product: per-thread accumulation (Acc<T>), then the deterministic grid
 // sum; the last block writes the total to result[0].
 template <typename T>
@@ -491,6 +501,30 @@ int b200la_vec_scaleadd(b200la_vec y, double a, b200la_vec x) {
   return launch_ew<float>(y->ctx, y->n, ScaleAddF<float>{(float *)y->d, (const float *)x->d, (float)a});
 }
 
+int b200la_vec_range_update(b200la_vec dst, int64_t dst_start, b200la_vec src, int64_t src_start, int64_t n,
+                            int add, double weight) {
+  B_CHECK(dst && src, B200LA_ERR_INVALID, "vec_range_update: null vector");
+  B_CHECK(dst->dtype == src->dtype, B200LA_ERR_DTYPE, "vec_range_update: dtype mismatch");
+  B_CHECK(n >= 0 && dst_start >= 0 && src_start >= 0 && dst_start + n <= dst->n && src_start + n <= src->n,
+          B200LA_ERR_INVALID, "vec_range_update: range [%lld,+%lld) / [%lld,+%lld) outside %lld / %lld",
+          (long long)dst_start, (long long)n, (long long)src_start, (long long)n, (long long)dst->n,
+          (long long)src->n);
+  if (n == 0) return B200LA_OK;
+  b200la_ctx c = dst->ctx;
+  int grid;
+  if (dst->dtype == B200LA_F64) {
+    B_TRY(grid_for(c, (const void *)range_kernel<double>, n, kBlock, &grid));
+    range_kernel<double><<<grid, kBlock, 0, c->stream>>>(n, (double *)dst->d + dst_start,
+                                                         (const double *)src->d + src_start, add, weight);
+  } else {
+    B_TRY(grid_for(c, (const void *)range_kernel<float>, n, kBlock, &grid));
+    range_kernel<float><<<grid, kBlock, 0, c->stream>>>(n, (float *)dst->d + dst_start,
+                                                        (const float *)src->d + src_start, add, (float)weight);
+  }
+  B_CUDA(cudaGetLastError());
+  return B200LA_OK;
+}
+
 int b200la_vec_scale(b200la_vec y, double a) {
   B_CHECK(y, B200LA_ERR_INVALID, "vec_scale: null vector");
   if (y->dtype == B200LA_F64) return launch_ew<double>(y->ctx, y->n, ScaleF<double>{(double *)y->d, a});
@@ -652,6 +686,11 @@ int b200la_spmv(b200la_mat m, b200la_vec x, b200la_vec y) {
 int b200la_spmv_add(b200la_mat m, b200la_vec x, b200la_vec y) {
   B_TRY(check_spmv(m, x, y, "spmv_add"));
   return spmv_launch(m, x->d, y->d, true, m->ctx->stream);
+}
+
+int b200la_spmv_nodiag(b200la_mat m, b200la_vec x, b200la_vec y) {
+  B_TRY(check_spmv(m, x, y, "spmv_nodiag"));
+  return spmv_nodiag_launch(m, x->d, y->d, m->ctx->stream);
 }
 
 int b200la_mat_inv_diag(b200la_mat m, b200la_vec out) {

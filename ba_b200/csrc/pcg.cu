@@ -26,7 +26,14 @@
 namespace b200la {
 
 // IterateControl::Check; step 0 records the initial residual (res_init).
+// Under the lmp cg() rule: no test before the first iteration, success once
+// ||r|| <= max(rtol ||r0||, atol), no divergence test.
 __device__ __forceinline__ int iterate_check(int step, double value, const CgScalars &s, double first) {
+  if (s.stop_rule == B200LA_STOP_LMP_CG) {
+    if (step > 0 && value <= fmax(s.rtol * first, s.atol)) return B200LA_SUCCESS_REL;
+    if (step >= s.maxits) return B200LA_FAIL_MAXITS;
+    return B200LA_ITERATE;
+  }
   if (value <= s.atol) return B200LA_SUCCESS_ABS;
   if (value < s.rtol * first) return B200LA_SUCCESS_REL;
   if (value > s.dtol * first) return B200LA_FAIL_DIV;
@@ -486,6 +493,8 @@ int b200la::cg_create_ex(b200la_mat A, const b200la_cg_params *prm, int vdtype, 
           prm->maxits, kMaxIts);
   B_CHECK(prm->atol >= 0.0 && prm->rtol >= 0.0 && prm->dtol > 0.0, B200LA_ERR_INVALID,
           "cg_create: tolerances must be atol >= 0, rtol >= 0, dtol > 0");
+  B_CHECK(prm->stop_rule == B200LA_STOP_ITERATE_CONTROL || (prm->stop_rule == B200LA_STOP_LMP_CG && !prm->precond),
+          B200LA_ERR_INVALID, "cg_create: stop_rule %d (the lmp cg() rule takes no preconditioner)", prm->stop_rule);
   b200la_ctx c = A->ctx;
   cudaStream_t st = c->stream;
   b200la_cg s = new b200la_cg_s();
@@ -509,6 +518,7 @@ int b200la::cg_create_ex(b200la_mat A, const b200la_cg_params *prm, int vdtype, 
   init.rtol = prm->rtol;
   init.dtol = prm->dtol;
   init.maxits = prm->maxits;
+  init.stop_rule = prm->stop_rule;
   init.state = B200LA_ITERATE;
   if (cudaMemcpyAsync(s->sc, &init, sizeof(init), cudaMemcpyHostToDevice, st) != cudaSuccess ||
       cudaStreamSynchronize(st) != cudaSuccess)
@@ -562,6 +572,8 @@ int b200la_cg_solve(b200la_cg s, b200la_vec b, b200la_vec x, b200la_cg_result *r
   CgScalars h;
   B_TRY(cg_fetch(s, &h));
   res->iters = h.iter;
+  // the lmp cg() returns the 0-based index of the iteration that met its test
+  if (s->prm.stop_rule == B200LA_STOP_LMP_CG && h.state == B200LA_SUCCESS_REL) res->iters = h.iter - 1;
   res->state = h.state;
   res->res = h.res;
   res->res_init = h.res_init;

@@ -30,6 +30,48 @@ int spmv_launch(b200la_mat m, const void *x, void *y, bool add, cudaStream_t s) 
   return spmv_launch_t<float>(m, (const float *)x, (float *)y, add, s);
 }
 
+// ---- y = (A - diag(A)) x: CPU_CSR_lMatrix::VectorMultNoDiag
+// (lmp/lmatrix_csr_cpu.cc:479-493): every stored entry whose column is not
+// the row, in stored order; 8 lanes per row over the CSR as uploaded (the
+// stationary Jacobi path, not the PCG's hot loop).
+template <typename T>
+__global__ void __launch_bounds__(kBlock) spmv_nodiag_kernel(int n, const int *__restrict__ rowptr,
+                                                             const int *__restrict__ col,
+                                                             const T *__restrict__ val, const T *__restrict__ x,
+                                                             T *__restrict__ y) {
+  constexpr int G = 8;
+  const int lane = threadIdx.x & (G - 1);
+  for (int base = blockIdx.x * (kBlock / G); base < n; base += gridDim.x * (kBlock / G)) {
+    const int row = base + (int)threadIdx.x / G;
+    T sum = T(0);
+    if (row < n) {
+      for (int j = __ldg(rowptr + row) + lane; j < __ldg(rowptr + row + 1); j += G) {
+        const int c = __ldg(col + j);
+        if (c != row) sum = fma(__ldg(val + j), __ldg(x + c), sum);
+      }
+    }
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    if (row < n && lane == 0) y[row] = sum;
+  }
+}
+
+int spmv_nodiag_launch(b200la_mat m, const void *x, void *y, cudaStream_t s) {
+  if (m->nrow == 0) return B200LA_OK;
+  int grid;
+  if (m->dtype == B200LA_F64) {
+    B_TRY(grid_for(m->ctx, (const void *)spmv_nodiag_kernel<double>, m->nrow, kBlock / 8, &grid));
+    spmv_nodiag_kernel<double><<<grid, kBlock, 0, s>>>(m->nrow, m->rowptr, m->col, (const double *)m->val,
+                                                       (const double *)x, (double *)y);
+  } else {
+    B_TRY(grid_for(m->ctx, (const void *)spmv_nodiag_kernel<float>, m->nrow, kBlock / 8, &grid));
+    spmv_nodiag_kernel<float><<<grid, kBlock, 0, s>>>(m->nrow, m->rowptr, m->col, (const float *)m->val,
+                                                      (const float *)x, (float *)y);
+  }
+  B_CUDA(cudaGetLastError());
+  return B200LA_OK;
+}
+
 // ---- SELL construction -----------------------------------------------------
 __global__ void sell_len_kernel(int n, int nslices, int width, const int *__restrict__ rowptr, int *__restrict__ len) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;

@@ -209,6 +209,8 @@ template <typename T, typename X = T, typename F> int with_schedule(b200la_mat m
 }
 
 int spmv_launch(b200la_mat m, const void *x, void *y, bool add, cudaStream_t s);
+// y = (A - diag(A)) x from the CSR as uploaded (VectorMultNoDiag)
+int spmv_nodiag_launch(b200la_mat m, const void *x, void *y, cudaStream_t s);
 int sell_build(b200la_mat m, int width, bool col16 = false);
 inline bool is_sell(int format) { return format == B200LA_FMT_SELL || format == B200LA_FMT_SELL16; }
 void sell_free(b200la_mat m);

@@ -306,6 +306,10 @@ class B200_CSR_lMatrix:
     def VectorMultAdd(self, invec: B200_lVector, outvec: B200_lVector):
         call("b200la_spmv_add", self.handle, invec.handle, outvec.handle)
 
+    def VectorMultNoDiag(self, invec: B200_lVector, outvec: B200_lVector):
+        """outvec = (A - diag(A)) invec (CPU_CSR_lMatrix::VectorMultNoDiag)."""
+        call("b200la_spmv_nodiag", self.handle, invec.handle, outvec.handle)
+
     def extract_invdiagelements(self, vec: B200_lVector):
         call("b200la_mat_inv_diag", self.handle, vec.handle)
 
@@ -423,7 +427,7 @@ class CG:
         if use_pc and (self.precond is None or self.precond.kind != "Jacobi"):
             raise B200LAError(-7, "CG: only the Jacobi preconditioner runs on this path")
         c = self.control
-        prm = CgParams(c.maxits, c.atol, c.rtol, c.dtol, 1 if use_pc else 0)
+        prm = CgParams(c.maxits, c.atol, c.rtol, c.dtol, 1 if use_pc else 0, 0)
         call("b200la_cg_create", self.op.handle, C.byref(prm), C.byref(self._solver))
 
     def Solve(self, b: B200_lVector, x: B200_lVector) -> int:
@@ -453,6 +457,27 @@ class CG:
             self._release()
         except Exception:
             pass
+
+
+def cg(x: B200_lVector, b: B200_lVector, matrix: B200_CSR_lMatrix, rel_eps: float, abs_eps: float, max_iter: int,
+       print_level: int = -1, lPrecond=None) -> tuple[int, int]:
+    """The lmp cg() (lmp/solvers/cg.cc:35-41, CGFunctor, lmp/solvers/cg.h:93-209)
+    as one device solve: plain CG from x, stop after an iteration once
+    ||r|| <= max(rel_eps ||r0||, abs_eps), at most max_iter iterations.
+    Returns (0, index) where index is what cg() leaves in max_iter: the
+    0-based index of the breaking iteration, or max_iter.  lPrecond is
+    accepted and, as in the reference (which computes z but never uses it,
+    cg.h:153 vs :157), has no effect on the iterates."""
+    del print_level, lPrecond
+    prm = CgParams(int(max_iter), float(abs_eps), float(rel_eps), 1e300, 0, 1)
+    s = C.c_void_p()
+    call("b200la_cg_create", matrix.handle, C.byref(prm), C.byref(s))
+    try:
+        r = CgResult()
+        call("b200la_cg_solve", s, b.handle, x.handle, C.byref(r))
+    finally:
+        load().b200la_cg_destroy(s)
+    return 0, r.iters
 
 
 def setup_CG_solver(maxits: int = 1000, atol: float = 1e-12, rtol: float = 1e-10, dtol: float = 1e6,

@@ -110,6 +110,11 @@ int b200la_vec_axpy(b200la_vec y, b200la_vec x, double alpha);     /* y.Axpy(x, 
 int b200la_vec_scaleadd(b200la_vec y, double alpha, b200la_vec x); /* y.ScaleAdd(a, x): y = a y + x */
 int b200la_vec_scale(b200la_vec v, double alpha);                  /* Scale */
 int b200la_vec_elementwise_mult(b200la_vec y, b200la_vec x);       /* ElementWiseMult: y .*= x */
+/* partial_replace_subvector / partial_add_subvector (lvector.h:175-190):
+ * dst[dst_start + i] = src[src_start + i] (add = 0) or += weight * src[...]
+ * (add = 1) for i < n; the ranges may start anywhere. */
+int b200la_vec_range_update(b200la_vec dst, int64_t dst_start, b200la_vec src, int64_t src_start, int64_t n,
+                            int add, double weight);
 
 /* Dot product that allocates nothing (no counterpart in the reference; its
  * lmp Dot is the entry above).  For callers that cannot call cudaMalloc:
@@ -163,6 +168,9 @@ int b200la_mat_zero_rows(b200la_mat m, const int *rows, int size, double alpha);
 int b200la_spmv(b200la_mat m, b200la_vec x, b200la_vec y);
 /* VectorMultAdd: y += A x (lmatrix_csr_cpu.cc:1404-1440) */
 int b200la_spmv_add(b200la_mat m, b200la_vec x, b200la_vec y);
+/* VectorMultNoDiag: y = (A - diag(A)) x, every stored entry off the diagonal
+ * (lmp/lmatrix_csr_cpu.cc:479-493) */
+int b200la_spmv_nodiag(b200la_mat m, b200la_vec x, b200la_vec y);
 /* extract_invdiagelements(0, nrow, out) (lmatrix_csr_cpu.cc:2426-2441);
  * B200LA_ERR_MATRIX if a row has no stored nonzero diagonal. */
 int b200la_mat_inv_diag(b200la_mat m, b200la_vec out);
@@ -185,7 +193,17 @@ typedef struct {
   double rtol;   /* success if res < rtol * res_init */
   double dtol;   /* divergence if res > dtol * res_init */
   int precond;   /* 0: SolveNoPrecond; 1: SolvePrecond with Jacobi */
+  int stop_rule; /* B200LA_STOP_ITERATE_CONTROL (0): CG<LAD> with IterateControl::Check.
+                    B200LA_STOP_LMP_CG (1): the lmp cg() (lmp/solvers/cg.h:93-209,
+                    cg.cc:35-41): plain CG (that function computes a preconditioned z
+                    but never uses it, cg.h:153 vs :157, so precond must be 0), stop
+                    after an iteration once ||r|| <= max(rtol * ||r0||, atol) (:149,
+                    :193), no divergence test, at most maxits iterations; the result's
+                    iters is then the 0-based index of the breaking iteration, or maxits,
+                    as cg() returns it in max_iter (:201) */
 } b200la_cg_params;
+#define B200LA_STOP_ITERATE_CONTROL 0
+#define B200LA_STOP_LMP_CG 1
 
 typedef struct {
   int iters;        /* CG::iter_ */

@@ -112,6 +112,24 @@ def test_spmv_all_schedules_vs_oracle(plat, dtype):
             assert np.all(err2 <= 2 * bound + 1e-300), (s.name, fmt, prm)
 
 
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_spmv_nodiag_vs_oracle(plat, dtype):
+    # VectorMultNoDiag against the oracle's restatement of the reference loop
+    # (every stored entry off the diagonal), including rows without a stored
+    # diagonal and empty rows
+    rtol = SPMV_RTOL_F64 if dtype == np.float64 else SPMV_RTOL_F32
+    for s in _spmv_cases():
+        xs = P.uniform01(6, s.n, stream=9) - 0.5
+        ref = oracle.spmv_nodiag(s.rowptr, s.col, s.val, xs, dtype=np.float64)
+        bound = _abs_rowsum(s, xs) * rtol + 1e-300
+        A = _mat(plat, s, dtype)
+        x = _vec(plat, xs, dtype)
+        y = x.CloneWithoutContent()
+        A.VectorMultNoDiag(x, y)
+        err = np.abs(y.numpy().astype(np.float64) - ref)
+        assert np.all(err <= bound), (s.name, float(err.max()))
+
+
 def test_blas1_vs_oracle(plat):
     rng = np.random.default_rng(7)
     for n in (1, 2, 3, 5, 31, 1000, 4097, 123457):
@@ -349,3 +367,34 @@ def test_sell16_matches_sell_bitwise_and_refuses_far_columns(plat):
     assert e.value.status == -7
     fmt, _, _ = A.tune()
     assert fmt != FMT_SELL16
+
+
+@pytest.mark.parametrize("case", ["3x3", "2d", "3d_s1", "spd_empty"])
+def test_lmp_cg_entry_matches_reference_lmp_cg(plat, case):
+    """lmp.cg(): the reference's own lmp cg() (lmp/solvers/cg.h:93-209) as one
+    device solve -- its stop rule norm <= max(rel*norm0, abs) and the 0-based
+    index it returns in max_iter -- against that function compiled from the
+    reference sources (oracle/_ref) and its restatement (oracle.lmp_cg): the
+    same returned index +-1 and the solution within 1e-10 relative; the
+    tests/cg_test.cc known answer within 1e-12."""
+    s = {"3x3": P.known_answer_3x3, "2d": lambda: P.q1_system(2, 40, 5, 0.0),
+         "3d_s1": lambda: P.q1_system(3, 12, 7, 1.0), "spd_empty": lambda: P.random_spd(60, 9, empty_rows=3)}[case]()
+    rel = 0.0 if case == "3x3" else 1e-10
+    A = _mat(plat, s)
+    x = _vec(plat, np.zeros(s.n))
+    rc, idx = lmp.cg(x, _vec(plat, s.b), A, rel, 0.0, 100 if case == "3x3" else 5000)
+    xs = x.numpy()
+    ref = oracle.lmp_cg(s.rowptr, s.col, s.val, s.b, rel_eps=rel, abs_eps=0.0, max_iter=100 if case == "3x3" else 5000)
+    assert rc == 0
+    if oracle.ref_available():
+        real = oracle.ref_lmp_cg(s.rowptr, s.col, s.val, s.b, rel_eps=rel, abs_eps=0.0,
+                                 max_iter=100 if case == "3x3" else 5000)
+        assert real.iters == ref.iters and np.array_equal(real.x, ref.x)
+    if case == "3x3":
+        # rel = abs = 0 (as cg_test.cc sets them): the reference iterates until
+        # ||r|| is exactly 0 (31 iterations in its arithmetic); only the
+        # known answer is the bar here, as in cg_test.cc
+        np.testing.assert_allclose(xs, [-0.25, -1.5, -0.75], rtol=0, atol=1e-12)
+        return
+    assert abs(idx - ref.iters) <= 1, (idx, ref.iters)
+    assert np.linalg.norm(xs - ref.x) <= 1e-10 * np.linalg.norm(ref.x)
