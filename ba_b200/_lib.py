@@ -123,6 +123,8 @@ _SIGS = {
     "b200la_vec_scale": [_vp, _d],
     "b200la_vec_elementwise_mult": [_vp, _vp],
     "b200la_vec_range_update": [_vp, _i64, _vp, _i64, _i64, _i, _d],
+    "b200la_vec_gather": [_vp, _vp, _i64, _vp],
+    "b200la_vec_scatter": [_vp, _vp, _i64, _vp],
     "b200la_dot_noalloc": [_vp, _vp, _i64, _i, _vp, _P(_d)],
     "b200la_csr_upload": [_vp, _i, _i, _i64, _vp, _vp, _vp, _i, _i, _P(_vp)],
     "b200la_coo_upload": [_vp, _i, _i, _i64, _vp, _vp, _vp, _i, _i, _i, _P(_vp)],

@@ -20,10 +20,18 @@ coupled_matrix.cc) lay them out, with the CG<LAD> recurrence over them.
 
 The local work runs on the backend's vectors and matrices (ba_b200.lmp's B200
 classes on the device); the communicator carries the halo and the sums.
-TorchComm uses a torch.distributed process group (one process per rank; the
-halo goes through host buffers over a gloo group, as the reference stages its
-MPI halo through the host); ThreadComm runs the ranks as threads of one
-process, each with its own device context, for tests on one device.
+TorchComm uses a torch.distributed process group (one process per rank);
+ThreadComm runs the ranks as threads of one process, each with its own device
+context, for tests on one device.
+
+The halo has two forms.  Host-staged (as the reference stages its MPI halo
+through host buffers): GetValues / SetValues of the device vectors around a
+host exchange.  Device-resident (device_halo=True): the owned values every
+peer reads are gathered on the device into one send buffer (b200la_vec_gather),
+the buffers move device to device -- NCCL send/recv on an NCCL group, or
+device copies between thread ranks -- and the received values are scattered
+into the ghost vector on the device (b200la_vec_scatter).  The CG's two dot
+products after the update (r.r and r.z) go to the ranks in one all-reduce.
 """
 from __future__ import annotations
 
@@ -45,11 +53,12 @@ class ThreadComm:
             self.box = {}
             self.lock = threading.Lock()
 
-        def comm(self, rank: int) -> "ThreadComm":
-            return ThreadComm(self, rank)
+        def comm(self, rank: int, device_halo: bool = False) -> "ThreadComm":
+            return ThreadComm(self, rank, device_halo)
 
-    def __init__(self, world: "ThreadComm.World", rank: int):
+    def __init__(self, world: "ThreadComm.World", rank: int, device_halo: bool = False):
         self.world, self.rank, self.size = world, rank, world.size
+        self.device_halo = bool(device_halo)
 
     def _post(self, key, value):
         with self.world.lock:
@@ -71,6 +80,32 @@ class ThreadComm:
         # every rank adds the same values in rank order: identical results
         return float(sum(self.allgather(float(value), "sum")))
 
+    def allreduce_sum_many(self, values) -> list:
+        parts = self.allgather([float(v) for v in values], "sums")
+        return [float(sum(p[k] for p in parts)) for k in range(len(values))]
+
+    def exchange_device(self, halo: "DeviceHalo"):
+        """Device halo between thread ranks on one device: each rank's send
+        buffer is complete (its context stream synchronised) before any peer
+        copies from it, and stays untouched until every peer has copied."""
+        import torch
+        halo.sync()
+        self._post(("dh", self.rank), halo)
+        self.world.barrier.wait()
+        with self.world.lock:
+            peers = {q: self.world.box[("dh", q)] for q in halo.recv_seg}
+        for q, (o, n) in halo.recv_seg.items():
+            so, sn = peers[q].send_seg[self.rank]
+            assert sn == n
+            halo.recv_buf[o:o + n].copy_(peers[q].send_buf[so:so + sn])
+        torch.cuda.synchronize()
+        self.world.barrier.wait()
+        if self.rank == 0:
+            with self.world.lock:
+                for r in range(self.size):
+                    self.world.box.pop(("dh", r), None)
+        self.world.barrier.wait()
+
     def exchange(self, send: dict, recv_sizes: dict) -> dict:
         for q, arr in send.items():
             self._post(("x", self.rank, q), np.asarray(arr))
@@ -90,7 +125,7 @@ class TorchComm:
     halo is exchanged through host buffers with point-to-point sends on a gloo
     group (`halo_group`, default: the world group when it is gloo)."""
 
-    def __init__(self, group=None, halo_group=None, device=None):
+    def __init__(self, group=None, halo_group=None, device=None, device_halo=False):
         import torch.distributed as dist
         self.dist = dist
         self.group = group
@@ -98,6 +133,26 @@ class TorchComm:
         self.rank = dist.get_rank(group)
         self.size = dist.get_world_size(group)
         self.device = device
+        # device_halo: buffers move device to device over `group` (NCCL), and
+        # the B200 contexts must run on torch's current stream, so the gather
+        # kernel precedes the sends and the scatter follows the receives
+        self.device_halo = bool(device_halo)
+
+    def allreduce_sum_many(self, values) -> list:
+        import torch
+        t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=self.device)
+        self.dist.all_reduce(t, group=self.group)
+        return [float(v) for v in t.tolist()]
+
+    def exchange_device(self, halo: "DeviceHalo"):
+        ops = []
+        for q, (o, n) in halo.send_seg.items():
+            ops.append(self.dist.P2POp(self.dist.isend, halo.send_buf[o:o + n], q, group=self.group))
+        for q, (o, n) in halo.recv_seg.items():
+            ops.append(self.dist.P2POp(self.dist.irecv, halo.recv_buf[o:o + n], q, group=self.group))
+        if ops:
+            for w in self.dist.batch_isend_irecv(ops):
+                w.wait()
 
     def allgather(self, obj, tag="ag"):
         out = [None] * self.size
@@ -172,6 +227,7 @@ class HaloPlan:
     values rank q owns; send[q] = local indices of owned values rank q reads."""
     recv: dict = field(default_factory=dict)
     send: dict = field(default_factory=dict)
+    device: "DeviceHalo | None" = None  # the device form, built at the first device exchange
 
     @staticmethod
     def build(comm, couplings: LaCouplings, ghosts: np.ndarray) -> "HaloPlan":
@@ -190,6 +246,50 @@ class HaloPlan:
         return plan
 
 
+class DeviceHalo:
+    """A rank's halo plan on the device: device int32 indices of the owned
+    values each peer reads (one segment per peer, peers in ascending order)
+    and of the ghost positions each peer fills, with one device send and one
+    device receive buffer of float64."""
+
+    def __init__(self, plan: HaloPlan, platform):
+        import torch
+        from . import _lib
+        dev = torch.device("cuda", platform.device)
+        self.platform = platform
+        self.send_seg, self.recv_seg = {}, {}
+        send_idx, recv_idx = [], []
+        o = 0
+        for q in sorted(plan.send):
+            self.send_seg[q] = (o, len(plan.send[q]))
+            send_idx.append(np.asarray(plan.send[q], np.int32))
+            o += len(plan.send[q])
+        self.send_idx = torch.from_numpy(np.concatenate(send_idx) if send_idx else np.zeros(0, np.int32)).to(dev)
+        self.send_buf = torch.empty(o, dtype=torch.float64, device=dev)
+        o = 0
+        for q in sorted(plan.recv):
+            self.recv_seg[q] = (o, len(plan.recv[q]))
+            recv_idx.append(np.asarray(plan.recv[q], np.int32))
+            o += len(plan.recv[q])
+        self.recv_idx = torch.from_numpy(np.concatenate(recv_idx) if recv_idx else np.zeros(0, np.int32)).to(dev)
+        self.recv_buf = torch.empty(o, dtype=torch.float64, device=dev)
+        torch.cuda.synchronize(dev)
+        self._lib = _lib
+
+    def sync(self):
+        self._lib.call("b200la_ctx_synchronize", self.platform.handle)
+
+    def pack(self, interior):
+        import ctypes as C
+        self._lib.call("b200la_vec_gather", interior.handle, C.c_void_p(self.send_idx.data_ptr()),
+                       int(self.send_idx.numel()), C.c_void_p(self.send_buf.data_ptr()))
+
+    def unpack(self, ghost):
+        import ctypes as C
+        self._lib.call("b200la_vec_scatter", ghost.handle, C.c_void_p(self.recv_idx.data_ptr()),
+                       int(self.recv_idx.numel()), C.c_void_p(self.recv_buf.data_ptr()))
+
+
 # ---------------------------------------------------------------- coupled objects
 class CoupledVector:
     """Owned values (interior) and ghost values of one rank."""
@@ -206,6 +306,14 @@ class CoupledVector:
         return CoupledVector(self.comm, self.couplings, self.plan, self.n_ghost, self._make)
 
     def UpdateGhost(self):
+        if getattr(self.comm, "device_halo", False):
+            if self.plan.device is None:
+                self.plan.device = DeviceHalo(self.plan, self.interior.platform)
+            self.plan.device.pack(self.interior)
+            self.comm.exchange_device(self.plan.device)
+            if self.ghost is not None:
+                self.plan.device.unpack(self.ghost)
+            return
         send = {q: self.interior.GetValues(idx) for q, idx in self.plan.send.items()}
         recv = self.comm.exchange(send, {q: len(pos) for q, pos in self.plan.recv.items()})
         for q, pos in self.plan.recv.items():
@@ -213,6 +321,10 @@ class CoupledVector:
 
     def Dot(self, other: "CoupledVector") -> float:
         return self.comm.allreduce_sum(self.interior.Dot(other.interior))
+
+    def DotMany(self, pairs) -> list:
+        """Several dot products summed over the ranks in one all-reduce."""
+        return self.comm.allreduce_sum_many([a.interior.Dot(b.interior) for a, b in pairs])
 
     def Norm2(self) -> float:
         return float(np.sqrt(self.Dot(self)))
@@ -307,15 +419,18 @@ def coupled_cg(A: CoupledMatrix, b: CoupledVector, x: CoupledVector, *, maxits=1
         alpha = beta / Ap.Dot(p)
         x.Axpy(p, alpha)
         r.Axpy(Ap, -alpha)
-        ressq = r.Dot(r)
+        if precond:
+            # r.r (the test) and r.z (the next beta) in one all-reduce
+            z.CopyFrom(r)
+            z.interior.ElementWiseMult(invd.interior)
+            ressq, gamma = r.DotMany([(r, r), (r, z)])
+        else:
+            ressq = r.Dot(r)
         res = float(np.sqrt(ressq))
         state = check(it, res, first)
         if state != 0:
             break
         if precond:
-            z.CopyFrom(r)
-            z.interior.ElementWiseMult(invd.interior)
-            gamma = r.Dot(z)
             p.ScaleAdd(z, gamma / beta)      # p = (gamma / beta) p + z
             beta = gamma
         else:

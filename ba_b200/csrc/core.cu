@@ -137,6 +137,24 @@ __global__ void __launch_bounds__(kBlock) range_kernel(int64_t n, T *__restrict_
     dst[i] = add ? fma(w, src[i], dst[i]) : src[i];
 }
 
+// Halo exchange of a row-partitioned vector (CoupledVector::SendBorder /
+// ReceiveGhost, linear_algebra/coupled_vector.cc:890-973): gather the owned
+// values peers read into a contiguous device buffer, scatter received values
+// into the ghost vector.  idx is a device int32 array of n positions.
+template <typename T>
+__global__ void __launch_bounds__(kBlock) gather_kernel(int64_t n, const int *__restrict__ idx,
+                                                        const T *__restrict__ src, T *__restrict__ out) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) out[k] = src[__ldg(idx + k)];
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kBlock) scatter_kernel(int64_t n, const int *__restrict__ idx,
+                                                         const T *__restrict__ in, T *__restrict__ dst) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) dst[__ldg(idx + k)] = in[k];
+}
+
 // Dot product: per-thread accumulation (Acc<T>), then the deterministic grid
 // sum; the last block writes the total to result[0].
 template <typename T>
@@ -520,6 +538,38 @@ int b200la_vec_range_update(b200la_vec dst, int64_t dst_start, b200la_vec src, i
     B_TRY(grid_for(c, (const void *)range_kernel<float>, n, kBlock, &grid));
     range_kernel<float><<<grid, kBlock, 0, c->stream>>>(n, (float *)dst->d + dst_start,
                                                         (const float *)src->d + src_start, add, (float)weight);
+  }
+  B_CUDA(cudaGetLastError());
+  return B200LA_OK;
+}
+
+int b200la_vec_gather(b200la_vec src, const int *idx, int64_t n, void *out) {
+  B_CHECK(src && (n == 0 || (idx && out)) && n >= 0, B200LA_ERR_INVALID, "vec_gather: bad argument");
+  if (n == 0) return B200LA_OK;
+  b200la_ctx c = src->ctx;
+  int grid;
+  if (src->dtype == B200LA_F64) {
+    B_TRY(grid_for(c, (const void *)gather_kernel<double>, n, kBlock, &grid));
+    gather_kernel<double><<<grid, kBlock, 0, c->stream>>>(n, idx, (const double *)src->d, (double *)out);
+  } else {
+    B_TRY(grid_for(c, (const void *)gather_kernel<float>, n, kBlock, &grid));
+    gather_kernel<float><<<grid, kBlock, 0, c->stream>>>(n, idx, (const float *)src->d, (float *)out);
+  }
+  B_CUDA(cudaGetLastError());
+  return B200LA_OK;
+}
+
+int b200la_vec_scatter(b200la_vec dst, const int *idx, int64_t n, const void *in) {
+  B_CHECK(dst && (n == 0 || (idx && in)) && n >= 0, B200LA_ERR_INVALID, "vec_scatter: bad argument");
+  if (n == 0) return B200LA_OK;
+  b200la_ctx c = dst->ctx;
+  int grid;
+  if (dst->dtype == B200LA_F64) {
+    B_TRY(grid_for(c, (const void *)scatter_kernel<double>, n, kBlock, &grid));
+    scatter_kernel<double><<<grid, kBlock, 0, c->stream>>>(n, idx, (const double *)in, (double *)dst->d);
+  } else {
+    B_TRY(grid_for(c, (const void *)scatter_kernel<float>, n, kBlock, &grid));
+    scatter_kernel<float><<<grid, kBlock, 0, c->stream>>>(n, idx, (const float *)in, (float *)dst->d);
   }
   B_CUDA(cudaGetLastError());
   return B200LA_OK;

@@ -115,6 +115,16 @@ int b200la_vec_elementwise_mult(b200la_vec y, b200la_vec x);       /* ElementWis
  * (add = 1) for i < n; the ranges may start anywhere. */
 int b200la_vec_range_update(b200la_vec dst, int64_t dst_start, b200la_vec src, int64_t src_start, int64_t n,
                             int add, double weight);
+/* Device halo of a row-partitioned vector (CoupledVector::SendBorder /
+ * ReceiveGhost, linear_algebra/coupled_vector.cc:890-973, which stage the
+ * values through host buffers and MPI): gather out[k] = src[idx[k]] into a
+ * device send buffer, scatter dst[idx[k]] = in[k] from a device receive
+ * buffer; idx is a device int32 array of n indices (in range: not checked on
+ * the device), out/in device buffers of n values of the vector's dtype.
+ * Stream-ordered on the context stream, so a collective on the same stream
+ * (or one that waits on it) moves the buffers in between. */
+int b200la_vec_gather(b200la_vec src, const int *idx, int64_t n, void *out);
+int b200la_vec_scatter(b200la_vec dst, const int *idx, int64_t n, const void *in);
 
 /* Dot product that allocates nothing (no counterpart in the reference; its
  * lmp Dot is the entry above).  For callers that cannot call cudaMalloc:

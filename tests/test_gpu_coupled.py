@@ -1,11 +1,13 @@
 """Multi-rank CoupledMatrix / CoupledVector / CG (ba_b200.coupled) with the
 B200 backend on one GPU: the ranks run as threads of this process, each with
-its own device context and stream; the halo and the sums go through the host
-(ThreadComm), so no kernel waits on another rank's kernel.  The diagonal and
-off-diagonal blocks are B200 CSR matrices, the ghost exchange uses the
-device vectors' GetValues/SetValues.  Bar: the single-rank reference CG's
-iteration count (+-1) and solution within 1e-10; the coupled SpMV equal to the
-global product up to summation order."""
+its own device context and stream (ThreadComm), so no kernel waits on another
+rank's kernel.  The diagonal and off-diagonal blocks are B200 CSR matrices.
+The halo runs host-staged (the device vectors' GetValues/SetValues around a
+host exchange) or device-resident (gather kernel into a device send buffer,
+device-to-device copies between the ranks' buffers, scatter kernel into the
+ghost vector).  Bar: the single-rank reference CG's iteration count (+-1) and
+solution within 1e-10; the coupled SpMV equal to the global product up to
+summation order; both halo forms give the same bits."""
 import threading
 
 import numpy as np
@@ -34,16 +36,13 @@ def _rank(comm, s, out, precond):
     out[comm.rank] = (y.interior.numpy(), sol.interior.numpy(), r)
 
 
-@pytest.mark.parametrize("size", [2, 3])
-@pytest.mark.parametrize("precond", [True, False])
-def test_device_ranks_match_single_rank_cg(size, precond):
-    s = P.q1_system(3, 12, 31, 1.0, "coupled3d")
+def _run(size, s, precond, device_halo):
     world = CP.ThreadComm.World(size)
     out, errors = {}, []
 
     def run(r):
         try:
-            _rank(world.comm(r), s, out, precond)
+            _rank(world.comm(r, device_halo=device_halo), s, out, precond)
         except BaseException as e:  # surface the rank's error in the test
             errors.append(e)
             world.barrier.abort()
@@ -54,6 +53,15 @@ def test_device_ranks_match_single_rank_cg(size, precond):
     for t in threads:
         t.join(timeout=300)
     assert not errors, errors
+    return out
+
+
+@pytest.mark.parametrize("size", [2, 3])
+@pytest.mark.parametrize("precond", [True, False])
+@pytest.mark.parametrize("device_halo", [False, True])
+def test_device_ranks_match_single_rank_cg(size, precond, device_halo):
+    s = P.q1_system(3, 12, 31, 1.0, "coupled3d")
+    out = _run(size, s, precond, device_halo)
     y = np.concatenate([out[r][0] for r in range(size)])
     x = np.concatenate([out[r][1] for r in range(size)])
     yg = oracle.spmv(s.rowptr, s.col, s.val, P.uniform01(5, s.n, stream=3))
@@ -62,3 +70,13 @@ def test_device_ranks_match_single_rank_cg(size, precond):
     its = {out[r][2].iters for r in range(size)}
     assert len(its) == 1 and abs(its.pop() - ref.iters) <= 1
     assert np.linalg.norm(x - ref.x) <= 1e-10 * np.linalg.norm(ref.x)
+
+
+def test_device_halo_gives_the_host_halos_bits():
+    s = P.q1_system(2, 30, 17, 1.0, "coupled2d")
+    a = _run(3, s, True, False)
+    b = _run(3, s, True, True)
+    for r in range(3):
+        np.testing.assert_array_equal(a[r][0], b[r][0])
+        np.testing.assert_array_equal(a[r][1], b[r][1])
+        assert a[r][2].iters == b[r][2].iters

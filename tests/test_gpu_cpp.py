@@ -32,5 +32,6 @@ def test_hiflow_lmp_on_b200_classes():
     lines = [ln for ln in p.stdout.splitlines() if ln.startswith(("PASS", "FAIL"))]
     names = {ln.split()[1] for ln in lines}
     assert {"cg_test_known_answer", "lmp_test_spmv", "lmp_test_spmv_from_coo", "laplace_cg_f64",
-            "laplace_cg_f64_jacobi", "laplace_cg_f32", "laplace_cg_f32_jacobi", "vector_semantics"} <= names, p.stdout
+            "laplace_cg_f64_jacobi", "laplace_cg_f32", "laplace_cg_f32_jacobi", "vector_dot_norm2", "vector_updates",
+            "vector_casts", "matrix_nodiag_invdiag"} <= names, p.stdout
     assert p.returncode == 0 and not any(ln.startswith("FAIL") for ln in lines), p.stdout + p.stderr
