@@ -139,6 +139,8 @@ _SIGS = {
     "b200la_mat_inv_diag": [_vp, _vp],
     "b200la_mat_set_format": [_vp, _i, _i],
     "b200la_mat_get_format": [_vp, _P(_i), _P(_i)],
+    "b200la_mat_to_sell": [_vp, _i, _i, _i, _i],
+    "b200la_mat_get_sell": [_vp, _P(_i), _P(_i), _P(_i64)],
     "b200la_mat_tune": [_vp, _P(_i), _P(_i), _P(_d)],
     "b200la_cg_create": [_vp, _P(CgParams), _P(_vp)],
     "b200la_cg_destroy": [_vp],

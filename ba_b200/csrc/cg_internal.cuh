@@ -43,6 +43,7 @@ struct b200la_cg_s {
   cudaGraph_t graph;
   cudaGraphExec_t exec;
   int g_format, g_param;       // schedule baked into the graph
+  int g_gen;                   // the matrix's schedule generation at capture
   int grid_spmv, grid_ew;
 };
 

@@ -773,6 +773,7 @@ int b200la_mat_set_format(b200la_mat m, int format, int param) {
             "mat_set_format: CSR lanes per row %d (1..32, power of two)", param);
     m->format = format;
     m->param = param;
+    m->sched_gen += 1;
     return B200LA_OK;
   }
   if (is_sell(format)) {
@@ -780,9 +781,29 @@ int b200la_mat_set_format(b200la_mat m, int format, int param) {
     B_TRY(sell_build(m, param, format == B200LA_FMT_SELL16));
     m->format = format;
     m->param = param;
+    m->sched_gen += 1;
     return B200LA_OK;
   }
   return fail(B200LA_ERR_UNSUPPORTED, "mat_set_format: format %d", format);
+}
+
+int b200la_mat_to_sell(b200la_mat m, int C, int sigma, int width, int col16) {
+  B_CHECK(m, B200LA_ERR_INVALID, "mat_to_sell: null matrix");
+  B_CHECK(width == 1 || width == 2 || width == 4, B200LA_ERR_INVALID, "mat_to_sell: width %d (1, 2 or 4)", width);
+  B_TRY(sell_build(m, width, col16 != 0, C, sigma));
+  m->format = col16 ? B200LA_FMT_SELL16 : B200LA_FMT_SELL;
+  m->param = width;
+  m->sched_gen += 1;
+  return B200LA_OK;
+}
+
+int b200la_mat_get_sell(b200la_mat m, int *C, int *sigma, int64_t *padded) {
+  B_CHECK(m && C && sigma, B200LA_ERR_INVALID, "mat_get_sell: null argument");
+  B_CHECK(is_sell(m->format), B200LA_ERR_INVALID, "mat_get_sell: the matrix's schedule is not sliced");
+  *C = m->sell.c;
+  *sigma = m->sell.sigma;
+  if (padded) *padded = m->sell.padded;
+  return B200LA_OK;
 }
 
 int b200la_mat_get_format(b200la_mat m, int *format, int *param) {

@@ -584,6 +584,7 @@ struct GmresState {
   cudaGraph_t graph;
   cudaGraphExec_t exec;
   int g_format, g_param;     // schedule baked into the graph
+  int g_gen;                 // the matrix's schedule generation at capture
   int grid_start, grid_restart, grid_spmv, grid_ew, grid_coop;
   int grid_res;              // blocks of the resident Arnoldi kernel (0: streaming form)
   int64_t res_slice;         // elements of w per block there
@@ -734,6 +735,7 @@ static int gm_build_graph_t(GmresState *s) {
   B_CUDA(cudaGraphInstantiate(&s->exec, g, 0));
   s->g_format = A->format;
   s->g_param = A->param;
+  s->g_gen = A->sched_gen;
   return B200LA_OK;
 }
 
@@ -913,7 +915,7 @@ int gmres_solve(GmresState *s, b200la_vec b, b200la_vec x, b200la_solver_result 
   if (A->dtype == B200LA_F64) B_TRY(gm_begin_t<double>(s, b->d, x->d));
   else B_TRY(gm_begin_t<float>(s, b->d, x->d));
   if (A->ctx->use_graphs) {
-    if (A->format != s->g_format || A->param != s->g_param) B_TRY(gm_build_graph(s));
+    if (A->format != s->g_format || A->param != s->g_param || A->sched_gen != s->g_gen) B_TRY(gm_build_graph(s));
     B_CUDA(cudaGraphLaunch(s->exec, st));
   } else if (A->dtype == B200LA_F64) {
     B_TRY((pre ? gm_host_loop_t<double, true>(s) : gm_host_loop_t<double, false>(s)));

@@ -85,7 +85,10 @@ struct SellData {
   short *col16p = nullptr;   // int16 offsets column - row (col16 == 1)
   int col16 = 0;
   void *val = nullptr;
-  int *perm = nullptr;       // row of each sorted position (sigma sorting)
+  int *perm = nullptr;       // row of each sorted position (sigma sorting; nullptr: rows keep their order)
+  int c = 32;                // rows per slice (SELL-C-sigma's C: 8, 16 or 32)
+  int log2c = 5;
+  int sigma = 1;             // rows per sorting window (1: no sorting)
 };
 
 struct b200la_mat_s {
@@ -101,6 +104,7 @@ struct b200la_mat_s {
   int format;         // B200LA_FMT_CSR / B200LA_FMT_SELL
   int param;          // CSR lanes per row / SELL width
   SellData sell;
+  int sched_gen;      // bumped whenever the schedule or its device data change (graphs re-capture)
 };
 
 namespace b200la {

@@ -364,6 +364,7 @@ struct b200la_solver_s {
   cudaGraph_t graph;
   cudaGraphExec_t exec;
   int g_format, g_param;     // schedule baked into the graph
+  int g_gen;                 // the matrix's schedule generation at capture
   int grid_spmv, grid_ew;
   b200la::GmresState *gm;    // GMRES keeps its own state (gmres.cu)
 };
@@ -439,6 +440,7 @@ static int solver_build_graph_t(b200la_solver s) {
   B_CUDA(cudaGraphInstantiate(&s->exec, g, 0));
   s->g_format = A->format;
   s->g_param = A->param;
+  s->g_gen = A->sched_gen;
   return B200LA_OK;
 }
 
@@ -701,7 +703,7 @@ int b200la_solver_solve(b200la_solver s, b200la_vec b, b200la_vec x, b200la_solv
   B_CUDA(cudaMemcpyAsync(s->bown, b->d, vb, cudaMemcpyDeviceToDevice, st));
   B_CUDA(cudaMemcpyAsync(s->v[0], x->d, vb, cudaMemcpyDeviceToDevice, st));
   if (A->ctx->use_graphs) {
-    if (A->format != s->g_format || A->param != s->g_param) B_TRY(solver_build_graph(s));
+    if (A->format != s->g_format || A->param != s->g_param || A->sched_gen != s->g_gen) B_TRY(solver_build_graph(s));
     B_CUDA(cudaGraphLaunch(s->exec, st));
   } else {
     B_TRY(solver_host_loop(s));

@@ -325,6 +325,7 @@ static int cg_build_graph_t(b200la_cg s) {
   B_CUDA(cudaGraphInstantiate(&s->exec, g, 0));
   s->g_format = A->format;
   s->g_param = A->param;
+  s->g_gen = A->sched_gen;
   return B200LA_OK;
 }
 
@@ -400,7 +401,7 @@ int cg_run(b200la_cg s) {
       return cg_host_loop_t<decltype(m), decltype(t), decltype(pre)::value>(s);
     });
   }
-  if (A->format != s->g_format || A->param != s->g_param) B_TRY(cg_build_graph(s));
+  if (A->format != s->g_format || A->param != s->g_param || A->sched_gen != s->g_gen) B_TRY(cg_build_graph(s));
   B_CUDA(cudaGraphLaunch(s->exec, A->ctx->stream));
   return B200LA_OK;
 }

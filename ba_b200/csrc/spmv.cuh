@@ -37,12 +37,17 @@ template <typename T, int G, typename X = T> struct CsrOp {
   }
 };
 
-// ---- SELL-C-sigma with C = 32, sigma = 1 (rows keep their order) ---------
-// Slice s holds rows 32s..32s+31, padded to slice_len[s] entries per row (a
-// multiple of W).  Chunk c of lane r starts at slice_ptr[s] + (c*32 + r)*W:
-// lane r reads W consecutive entries of its own row with one vector load and
-// a warp reads 32*W*sizeof(T) contiguous bytes per step.  Padding entries
-// hold value 0 and repeat a column the row already reads.
+// ---- SELL-C-sigma ----------------------------------------------------------
+// Rows are sorted by length, longest first, within windows of sigma rows
+// (perm[position] = row; sigma = 1 keeps the order and perm is null), then
+// cut into slices of C rows (C = 8, 16 or 32), each padded to its longest
+// row rounded up to W entries.  Entry k of the row at position r of slice s
+// sits at slice_ptr[s] + ((k/W)*C + r)*W + k%W: a row's W consecutive
+// entries are one vector load, and the C rows of a slice read C*W contiguous
+// values per step.  A warp handles 32/C slices at a time (lane = slice in
+// the warp * C + r).  Padding entries hold value 0 and repeat a column the
+// row already reads.  Every row's products are added in its stored order
+// whatever C, sigma and W are, so all SELL variants give the same bits.
 template <typename T, int W> struct VecW;
 template <> struct VecW<double, 1> { using v = double; using i = int; };
 template <> struct VecW<double, 2> { using v = double2; using i = int2; };
@@ -76,6 +81,8 @@ template <typename T, int W, typename X = T> struct SellOp {
   const int *__restrict__ col;
   const T *__restrict__ val;
   int n, nslices;
+  int log2c;                 // C = 1 << log2c rows per slice
+  const int *__restrict__ perm;  // row of each position, or null (identity)
   static constexpr int kRowsPerBlock = kBlock;
   __host__ __device__ int64_t work_items() const { return n; }
   template <typename Emit> __device__ __forceinline__ void run(const X *__restrict__ x, Emit &emit) const {
@@ -83,22 +90,26 @@ template <typename T, int W, typename X = T> struct SellOp {
     using VI = typename VecW<T, W>::i;
     const int lane = threadIdx.x & 31;
     const int wpb = kBlock / 32;
-    for (int s = blockIdx.x * wpb + ((int)threadIdx.x >> 5); s < nslices; s += gridDim.x * wpb) {
-      const int base = __ldg(slice_ptr + s);
-      const int chunks = __ldg(slice_len + s) / W;
-      const VI *ci = reinterpret_cast<const VI *>(col + base) + lane;
-      const VV *vi = reinterpret_cast<const VV *>(val + base) + lane;
+    const int C = 1 << log2c, spw = 32 >> log2c;
+    const int r = lane & (C - 1), sub = lane >> log2c;
+    for (int s0 = (blockIdx.x * wpb + ((int)threadIdx.x >> 5)) * spw; s0 < nslices; s0 += gridDim.x * wpb * spw) {
+      const int s = s0 + sub;
+      const bool live = s < nslices;
+      const int base = live ? __ldg(slice_ptr + s) : 0;
+      const int chunks = live ? __ldg(slice_len + s) / W : 0;
+      const VI *ci = reinterpret_cast<const VI *>(col + base) + r;
+      const VV *vi = reinterpret_cast<const VV *>(val + base) + r;
       X sum = X(0);
 #pragma unroll 4
       for (int c = 0; c < chunks; ++c) {
-        VI cc = ld_vec_stream(ci + c * 32);
-        VV vv = ld_vec_stream(vi + c * 32);
+        VI cc = ld_vec_stream(ci + c * C);
+        VV vv = ld_vec_stream(vi + c * C);
 #pragma unroll
         for (int k = 0; k < W; ++k)
           sum = fma((X)lane_get<VV, T, W>(vv, k), ld_keep(x + lane_geti<VI, W>(cc, k)), sum);
       }
-      const int row = s * 32 + lane;
-      if (row < n) emit(row, sum);
+      const int pos = s * C + r;
+      if (live && pos < n) emit(perm ? __ldg(perm + pos) : pos, sum);
     }
   }
 };
@@ -123,6 +134,8 @@ template <typename T, int W, typename X = T> struct SellOp16 {
   const short *__restrict__ col;
   const T *__restrict__ val;
   int n, nslices;
+  int log2c;                 // C = 1 << log2c rows per slice
+  const int *__restrict__ perm;  // row of each position, or null (identity)
   static constexpr int kRowsPerBlock = kBlock;
   __host__ __device__ int64_t work_items() const { return n; }
   template <typename Emit> __device__ __forceinline__ void run(const X *__restrict__ x, Emit &emit) const {
@@ -130,24 +143,30 @@ template <typename T, int W, typename X = T> struct SellOp16 {
     using VI = typename VecS<W>::i;
     const int lane = threadIdx.x & 31;
     const int wpb = kBlock / 32;
-    for (int s = blockIdx.x * wpb + ((int)threadIdx.x >> 5); s < nslices; s += gridDim.x * wpb) {
-      const int base = __ldg(slice_ptr + s);
-      const int chunks = __ldg(slice_len + s) / W;
-      const VI *ci = reinterpret_cast<const VI *>(col + base) + lane;
-      const VV *vi = reinterpret_cast<const VV *>(val + base) + lane;
-      const int row = s * 32 + lane;
-      // padding rows past n (last slice) hold offset 0 and gather x[0]
-      const int rb = row < n ? row : 0;
+    const int C = 1 << log2c, spw = 32 >> log2c;
+    const int r = lane & (C - 1), sub = lane >> log2c;
+    for (int s0 = (blockIdx.x * wpb + ((int)threadIdx.x >> 5)) * spw; s0 < nslices; s0 += gridDim.x * wpb * spw) {
+      const int s = s0 + sub;
+      const bool live = s < nslices;
+      const int base = live ? __ldg(slice_ptr + s) : 0;
+      const int chunks = live ? __ldg(slice_len + s) / W : 0;
+      const VI *ci = reinterpret_cast<const VI *>(col + base) + r;
+      const VV *vi = reinterpret_cast<const VV *>(val + base) + r;
+      const int pos = s * C + r;
+      const bool real = live && pos < n;
+      // the stored offsets are relative to the row itself; padding rows
+      // past n (last slice) hold offset 0 and gather x[0]
+      const int row = real ? (perm ? __ldg(perm + pos) : pos) : 0;
       X sum = X(0);
 #pragma unroll 4
       for (int c = 0; c < chunks; ++c) {
-        VI cc = __ldcs(ci + c * 32);
-        VV vv = ld_vec_stream(vi + c * 32);
+        VI cc = __ldcs(ci + c * C);
+        VV vv = ld_vec_stream(vi + c * C);
 #pragma unroll
         for (int k = 0; k < W; ++k)
-          sum = fma((X)lane_get<VV, T, W>(vv, k), ld_keep(x + rb + lane_gets(cc, k)), sum);
+          sum = fma((X)lane_get<VV, T, W>(vv, k), ld_keep(x + row + lane_gets(cc, k)), sum);
       }
-      if (row < n) emit(row, sum);
+      if (real) emit(row, sum);
     }
   }
 };
@@ -181,9 +200,9 @@ template <typename T, typename X = T, typename F> int with_schedule(b200la_mat m
     const SellData &s = m->sell;
     const T *sv = (const T *)s.val;
     switch (m->param) {
-      case 1: return f(SellOp<T, 1, X>{s.slice_ptr, s.slice_len, s.col, sv, m->nrow, s.nslices});
-      case 2: return f(SellOp<T, 2, X>{s.slice_ptr, s.slice_len, s.col, sv, m->nrow, s.nslices});
-      case 4: return f(SellOp<T, 4, X>{s.slice_ptr, s.slice_len, s.col, sv, m->nrow, s.nslices});
+      case 1: return f(SellOp<T, 1, X>{s.slice_ptr, s.slice_len, s.col, sv, m->nrow, s.nslices, s.log2c, s.perm});
+      case 2: return f(SellOp<T, 2, X>{s.slice_ptr, s.slice_len, s.col, sv, m->nrow, s.nslices, s.log2c, s.perm});
+      case 4: return f(SellOp<T, 4, X>{s.slice_ptr, s.slice_len, s.col, sv, m->nrow, s.nslices, s.log2c, s.perm});
     }
     return fail(B200LA_ERR_INVALID, "SELL width %d", m->param);
   }
@@ -191,9 +210,12 @@ template <typename T, typename X = T, typename F> int with_schedule(b200la_mat m
     const SellData &s = m->sell;
     const T *sv = (const T *)s.val;
     switch (m->param) {
-      case 1: return f(SellOp16<T, 1, X>{s.slice_ptr, s.slice_len, s.col16p, sv, m->nrow, s.nslices});
-      case 2: return f(SellOp16<T, 2, X>{s.slice_ptr, s.slice_len, s.col16p, sv, m->nrow, s.nslices});
-      case 4: return f(SellOp16<T, 4, X>{s.slice_ptr, s.slice_len, s.col16p, sv, m->nrow, s.nslices});
+      case 1:
+        return f(SellOp16<T, 1, X>{s.slice_ptr, s.slice_len, s.col16p, sv, m->nrow, s.nslices, s.log2c, s.perm});
+      case 2:
+        return f(SellOp16<T, 2, X>{s.slice_ptr, s.slice_len, s.col16p, sv, m->nrow, s.nslices, s.log2c, s.perm});
+      case 4:
+        return f(SellOp16<T, 4, X>{s.slice_ptr, s.slice_len, s.col16p, sv, m->nrow, s.nslices, s.log2c, s.perm});
     }
     return fail(B200LA_ERR_INVALID, "SELL16 width %d", m->param);
   }
@@ -211,7 +233,10 @@ template <typename T, typename X = T, typename F> int with_schedule(b200la_mat m
 int spmv_launch(b200la_mat m, const void *x, void *y, bool add, cudaStream_t s);
 // y = (A - diag(A)) x from the CSR as uploaded (VectorMultNoDiag)
 int spmv_nodiag_launch(b200la_mat m, const void *x, void *y, cudaStream_t s);
-int sell_build(b200la_mat m, int width, bool col16 = false);
+// Builds the sliced copy: `width` entries per vector load, int16 column
+// offsets (col16), C rows per slice, rows sorted by length within windows of
+// sigma rows (1 = no sorting; otherwise rounded up to a multiple of C).
+int sell_build(b200la_mat m, int width, bool col16 = false, int C = 32, int sigma = 1);
 inline bool is_sell(int format) { return format == B200LA_FMT_SELL || format == B200LA_FMT_SELL16; }
 void sell_free(b200la_mat m);
 

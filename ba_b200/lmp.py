@@ -325,6 +325,24 @@ class B200_CSR_lMatrix:
     def set_format(self, fmt: int, param: int):
         call("b200la_mat_set_format", self.handle, fmt, param)
 
+    def set_sell(self, C: int = 32, sigma: int = 1, width: int = 1, col16: bool = False):
+        """SELL-C-sigma schedule: slices of C (8/16/32) rows, rows sorted by
+        length within windows of sigma rows, width entries per vector load,
+        int16 column offsets with col16."""
+        call("b200la_mat_to_sell", self.handle, int(C), int(sigma), int(width), 1 if col16 else 0)
+
+    def get_sell(self) -> tuple[int, int]:
+        """(C, sigma) of the current sliced schedule."""
+        c, sg = C.c_int(), C.c_int()
+        call("b200la_mat_get_sell", self.handle, C.byref(c), C.byref(sg), None)
+        return c.value, sg.value
+
+    def sell_padded(self) -> int:
+        """Stored entries of the current sliced copy, padding included."""
+        c, sg, pd = C.c_int(), C.c_int(), C.c_int64()
+        call("b200la_mat_get_sell", self.handle, C.byref(c), C.byref(sg), C.byref(pd))
+        return pd.value
+
     def get_format(self) -> tuple[int, int]:
         f, p = C.c_int(), C.c_int()
         call("b200la_mat_get_format", self.handle, C.byref(f), C.byref(p))

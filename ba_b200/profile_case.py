@@ -3,6 +3,7 @@ launches (no CUDA graph), so a profiler sees every launch on its own.
 
     python -m ba_b200.profile_case [--cells 128] [--dim 3] [--dtype f64|f32]
                                    [--spmv-reps 3] [--cg-iters 3] [--schedule tune|csr/8|sell/1]
+    python -m ba_b200.profile_case --sell-table [--dtype f64|f32]
 
 With --solver jacobi|bicgstab|gmres: after the SpMV launches, runs
 `--cg-iters` passes of that solver's kernels as plain launches
@@ -55,7 +56,12 @@ def main():
     ap.add_argument("--items", default="", help="batch: K1,K2,K3 item rows instead of tuning")
     ap.add_argument("--profile-only", action="store_true",
                     help="batch: skip the solves; time one inner pass kernel by kernel (b200la_batch_profile_pass)")
+    ap.add_argument("--sell-table", action="store_true",
+                    help="instead: time every SpMV schedule (CSR lane groups, SELL-C-sigma with C 8/16/32, sigma "
+                         "1/1024, widths 1/2/4, int32/int16 columns) on three matrices and print a table")
     a = ap.parse_args()
+    if a.sell_table:
+        return sell_table(a)
     if a.batch:
         return batch_case(a)
     dt = np.float64 if a.dtype == "f64" else np.float32
@@ -93,6 +99,83 @@ def main():
     print(f"spmv wall {spmv_ms:.3f} ms/launch; cg kernels ms: spmv_dot {ms[0]:.4f} update {ms[1]:.4f} "
           f"direction {ms[2]:.4f}; spmv algorithmic bytes {alg} -> {alg / ms[0] / 1e6:.1f} GB/s")
     load()
+
+
+def ragged_system(n: int, seed: int = 11):
+    """A banded matrix with power-law row lengths (1..200 entries, mean ~7,
+    a few long rows among many short ones, columns within 5,000 of the row):
+    the case SELL-C-sigma's sorting is for."""
+    u = P.uniform01(seed, n, stream=1)
+    deg = np.minimum(1 + (3.0 * ((1.0 - u) ** (-1.0 / 1.5) - 1.0)).astype(np.int64), 200)
+    rowptr = np.zeros(n + 1, np.int64)
+    np.cumsum(deg, out=rowptr[1:])
+    nnz = int(rowptr[-1])
+    rows = np.repeat(np.arange(n, dtype=np.int64), deg)
+    off = (P.uniform01(seed, nnz, stream=2) * 10001).astype(np.int64) - 5000
+    cols = np.clip(rows + off, 0, n - 1)
+    order = np.lexsort((cols, rows))
+    cols = cols[order]
+    val = P.uniform01(seed, nnz, stream=3) - 0.5
+    return P.CSRSystem(0, 0, rowptr.astype(np.int32), cols.astype(np.int32), val, P.uniform01(seed, n, stream=4),
+                       np.zeros(n, bool), f"ragged_{n}")
+
+
+def sell_table(a):
+    """Every SpMV schedule on three matrices, CUDA-event timed (20 launches
+    after 3 warm-ups), as a markdown table: microseconds per SpMV, padding of
+    the sliced copy, algorithmic GB/s; then the tuner's pick."""
+    import torch
+    dt = np.float64 if a.dtype == "f64" else np.float32
+    sv = 8 if dt == np.float64 else 4
+    plat = lmp.init_platform(0)
+    st = torch.cuda.current_stream()
+    plat.set_stream(st.cuda_stream)
+    cases = [P.q1_system(2, 1024, 20240601, 1.0, "q1_2d_1024_s1"), P.q1_system(3, 128, 20240602, 2.0, "q1_3d_128_s2"),
+             ragged_system(2_000_000)]
+    print(f"| matrix | schedule | C | sigma | us | padding | GB/s |")
+    print(f"|---|---|---:|---:|---:|---:|---:|")
+    for s in cases:
+        A = lmp.B200_CSR_lMatrix(s.rowptr, s.col, s.val, platform=plat, dtype=dt)
+        x = lmp.B200_lVector.from_numpy(s.b.astype(dt), platform=plat, dtype=dt)
+        y = x.CloneWithoutContent()
+        alg = s.nnz * (sv + 4) + (s.n + 1) * 4 + 2 * s.n * sv
+        rows = []
+
+        def timed():
+            for _ in range(3):
+                A.VectorMult(x, y)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            for _ in range(20):
+                A.VectorMult(x, y)
+            e1.record(st)
+            e1.synchronize()
+            return e0.elapsed_time(e1) * 1e3 / 20
+        for g in (2, 4, 8, 16, 32):
+            A.set_format(FMT_CSR, g)
+            rows.append((f"csr/{g}", "", "", timed(), ""))
+        for col16 in (False, True):
+            for sigma in (1, 1024):
+                for c in (32, 16, 8):
+                    for w in (1, 2, 4):
+                        try:
+                            A.set_sell(c, sigma, w, col16)
+                        except lmp.B200LAError:
+                            continue
+                        padded = A.sell_padded()
+                        rows.append((f"{'sell16' if col16 else 'sell'}/{w}", c, sigma, timed(),
+                                     f"{padded / s.nnz - 1:.1%}"))
+        best = min(rows, key=lambda r: r[3])
+        for r in rows:
+            mark = " **" if r is best else ""
+            print(f"| {s.name} (n={s.n}, nnz={s.nnz}) | {r[0]}{mark} | {r[1]} | {r[2]} | {r[3]:.1f} | {r[4]} | "
+                  f"{alg / (r[3] * 1e-6) / 1e9:.0f} |")
+        fmt, prm, us = A.tune()
+        cs = A.get_sell() if fmt != FMT_CSR else ("", "")
+        print(f"| {s.name} | tuner pick: {FORMAT_NAMES[fmt]}/{prm} | {cs[0]} | {cs[1]} | {us:.1f} | | "
+              f"{alg / (us * 1e-6) / 1e9:.0f} |")
+        del A, x, y
+        plat.synchronize()
 
 
 def solver_case(a, s, A, dt, fmt, prm, us, alg, sv):

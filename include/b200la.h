@@ -64,7 +64,7 @@ typedef struct b200la_batch_s *b200la_batch;
 
 /* SpMV storage formats (la_global.h:56 MATRIX_FORMAT has DENSE, CSR, COO, ELL) */
 #define B200LA_FMT_CSR 1  /* CSR, a group of `lanes` threads per row */
-#define B200LA_FMT_SELL 4 /* SELL-C-sigma, C = 32 rows per slice */
+#define B200LA_FMT_SELL 4 /* SELL-C-sigma (C = 32 and sigma = 1 unless b200la_mat_to_sell says otherwise) */
 #define B200LA_FMT_SELL16 5 /* SELL-32 with columns stored as int16 offsets from the row
                              (banded matrices: every |col - row| <= 32767) */
 
@@ -189,8 +189,24 @@ int b200la_mat_inv_diag(b200la_mat m, b200la_vec out);
  * chunk width (1, 2 or 4); builds the SELL copy on first use. */
 int b200la_mat_set_format(b200la_mat m, int format, int param);
 int b200la_mat_get_format(b200la_mat m, int *format, int *param);
-/* Autotuner: times every schedule on this matrix and keeps the fastest.
- * Writes the chosen format/param and its time per SpMV in microseconds. */
+/* SELL-C-sigma (no reference counterpart: la_global.h:56 lists an ELL format
+ * the reference never implements, lmatrix_formats.h:101-110): rows sorted by
+ * length, longest first, within windows of `sigma` rows (1 = rows keep their
+ * order; otherwise rounded up to a multiple of C), cut into slices of C = 8,
+ * 16 or 32 rows, each padded to its longest row rounded up to `width` (1, 2
+ * or 4) entries per vector load; col16 = 1 stores int16 column offsets as
+ * SELL16 does.  Selects the copy as the matrix's schedule (format SELL or
+ * SELL16, param width).  Every variant adds each row's products in stored
+ * order, so all give the same bits as SELL-32.  get_sell writes C, sigma
+ * and the stored entries including padding (padded may be NULL) of the
+ * current sliced schedule. */
+int b200la_mat_to_sell(b200la_mat m, int C, int sigma, int width, int col16);
+int b200la_mat_get_sell(b200la_mat m, int *C, int *sigma, int64_t *padded);
+/* Autotuner: times every schedule on this matrix (CSR lane groups 2..32;
+ * SELL and SELL16 with width 1/2/4, C = 32/16/8 and sigma 1 or 1,024,
+ * sliced copies padding more than 25% skipped) and keeps the fastest.
+ * Writes the chosen format/param and its time per SpMV in microseconds;
+ * b200la_mat_get_sell gives the chosen C and sigma. */
 int b200la_mat_tune(b200la_mat m, int *format, int *param, double *usec);
 
 /* ---- preconditioned CG: CG<LAD> + PreconditionerBlockJacobiStand<LAD>

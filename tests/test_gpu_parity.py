@@ -398,3 +398,84 @@ def test_lmp_cg_entry_matches_reference_lmp_cg(plat, case):
         return
     assert abs(idx - ref.iters) <= 1, (idx, ref.iters)
     assert np.linalg.norm(xs - ref.x) <= 1e-10 * np.linalg.norm(ref.x)
+
+
+def _ragged(n, seed):
+    """Symmetric diagonally dominant matrix with power-law row lengths (a
+    few long rows among many short ones): where sorting rows by length in
+    SELL-C-sigma removes padding."""
+    rng = np.random.default_rng(seed)
+    deg = np.minimum((rng.pareto(1.5, n) * 3).astype(int) + 1, 200)
+    rows, cols = [], []
+    for i in range(n):
+        c = rng.choice(n, size=min(deg[i], n), replace=False)
+        rows.append(np.full(c.shape[0], i))
+        cols.append(c)
+    r = np.concatenate(rows)
+    c = np.concatenate(cols)
+    import scipy.sparse as sp
+    A = sp.coo_matrix((rng.standard_normal(r.shape[0]), (r, c)), shape=(n, n)).tocsr()
+    A = A + A.T
+    A = A + sp.diags(np.asarray(abs(A).sum(axis=1)).ravel() + 1.0)
+    A = A.tocsr()
+    A.sort_indices()
+    return P.CSRSystem(0, 0, A.indptr.astype(np.int32), A.indices.astype(np.int32), A.data.astype(np.float64),
+                       rng.random(n), np.zeros(n, bool), f"ragged_{n}")
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_sell_c_sigma_gives_the_sell32_bits(plat, dtype):
+    """SELL-C-sigma (C = 8/16/32 rows per slice, rows sorted by length within
+    windows of sigma rows, widths 1/2/4, int32 or int16 columns) adds each
+    row's products in stored order like SELL-32, so every variant gives its
+    bits; on the ragged matrix sorting cuts the padding."""
+    cases = [P.poisson_2d(100), P.q1_system(3, 10, 3, 2.0), P.random_spd(257, 3, density=0.02, empty_rows=5),
+             P.random_spd(33, 2, empty_rows=3), _ragged(3000, 5)]
+    for s in cases:
+        xs = P.uniform01(8, s.n, stream=9) - 0.5
+        A = _mat(plat, s, dtype)
+        A.set_format(FMT_SELL, 1)
+        x = _vec(plat, xs, dtype)
+        y0 = x.CloneWithoutContent()
+        A.VectorMult(x, y0)
+        ref = y0.numpy()
+        for col16 in (False, True):
+            for C in (8, 16, 32):
+                for sigma in (1, 64, 1024):
+                    for w in (1, 2, 4):
+                        try:
+                            A.set_sell(C, sigma, w, col16)
+                        except B200LAError as e:
+                            assert col16 and e.status == -7  # far columns: int16 offsets refused
+                            continue
+                        assert A.get_sell() == (C, sigma if sigma == 1 else -(-sigma // C) * C)
+                        y = x.CloneWithoutContent()
+                        A.VectorMult(x, y)
+                        np.testing.assert_array_equal(y.numpy(), ref, err_msg=f"{s.name} C{C} s{sigma} w{w} {col16}")
+                        # y += A x through the same schedule
+                        A.VectorMultAdd(x, y)
+                        np.testing.assert_array_equal(y.numpy(), (ref + ref).astype(ref.dtype))
+
+
+def test_sell_c_sigma_in_the_solver_and_the_tuner(plat):
+    s = _ragged(4000, 7)
+    A = _mat(plat, s)
+    A.set_sell(16, 512, 2, False)
+    b = _vec(plat, s.b)
+    x = _vec(plat, np.zeros(s.n))
+    cg = lmp.setup_CG_solver(maxits=5000, atol=0.0, rtol=1e-10, dtol=1e8)
+    cg.SetupOperator(A)
+    assert cg.Solve(b, x) == lmp.kSolverSuccess
+    ref = oracle.cg(s.rowptr, s.col, s.val, s.b, maxits=5000, atol=0.0, rtol=1e-10)
+    assert abs(cg.iter() - ref.iters) <= 1
+    assert np.linalg.norm(x.numpy() - ref.x) <= 1e-10 * np.linalg.norm(ref.x)
+    # the schedule changes under the solver: its graph is captured again
+    A.set_sell(8, 1, 1, False)
+    x2 = _vec(plat, np.zeros(s.n))
+    assert cg.Solve(b, x2) == lmp.kSolverSuccess
+    assert np.linalg.norm(x2.numpy() - ref.x) <= 1e-10 * np.linalg.norm(ref.x)
+    fmt, prm, us = A.tune()
+    assert us > 0 and fmt in (FMT_CSR, FMT_SELL, FMT_SELL16)
+    if fmt != FMT_CSR:
+        C, sigma = A.get_sell()
+        assert C in (8, 16, 32) and sigma in (1, 1024)
