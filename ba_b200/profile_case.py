@@ -128,7 +128,8 @@ def sell_table(a):
     dt = np.float64 if a.dtype == "f64" else np.float32
     sv = 8 if dt == np.float64 else 4
     plat = lmp.init_platform(0)
-    st = torch.cuda.current_stream()
+    st = torch.cuda.Stream()  # not the legacy default stream: handle 0 selects the context's own stream
+    torch.cuda.set_stream(st)
     plat.set_stream(st.cuda_stream)
     cases = [P.q1_system(2, 1024, 20240601, 1.0, "q1_2d_1024_s1"), P.q1_system(3, 128, 20240602, 2.0, "q1_3d_128_s2"),
              ragged_system(2_000_000)]

@@ -85,6 +85,17 @@ def parse():
     return ap.parse_args()
 
 
+def work_stream(torch):
+    """A non-default CUDA stream made torch's current one: the library's
+    context runs its work on it (b200la_ctx_set_stream), so the CUDA events
+    recorded on it time the device work itself.  (Handing the library the
+    legacy default stream, handle 0, would select the context's own stream,
+    which the events on stream 0 do not wait for.)"""
+    st = torch.cuda.Stream()
+    torch.cuda.set_stream(st)
+    return st
+
+
 def dist_env():
     return (int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0")),
             int(os.environ.get("WORLD_SIZE", "1")))
@@ -318,7 +329,7 @@ def run_batch(args, rank, local_rank, world, torch, dist, barrier):
     from ba_b200.batch import Batch
 
     plat = lmp.Platform(local_rank)
-    stream = torch.cuda.current_stream()
+    stream = work_stream(torch)
     plat.set_stream(stream.cuda_stream)
     all_systems = make_batch_systems(args.count, 0 if args.split else rank)
     systems = all_systems
@@ -640,7 +651,7 @@ def run_serve(args, rank, local_rank, world, torch, dist, barrier):
     from ba_b200.server import Server
 
     plat = lmp.Platform(local_rank)
-    stream = torch.cuda.current_stream()
+    stream = work_stream(torch)
     plat.set_stream(stream.cuda_stream)
     inner_rtol = args.inner_rtol if args.inner_rtol is not None else BATCH_INNER
     kw = dict(rtol=BATCH_RTOL, atol=0.0, dtol=1e8, inner_rtol=inner_rtol, max_outer=60, chunk_passes=CHUNK,
@@ -830,7 +841,7 @@ def run_poisson3d(args, rank, local_rank, world, torch, dist, barrier):
     from ba_b200._lib import FORMAT_NAMES, load
 
     plat = lmp.Platform(local_rank)
-    stream = torch.cuda.current_stream()
+    stream = work_stream(torch)
     plat.set_stream(stream.cuda_stream)
     s = P.poisson_3d(args.cells)
     n, nnz = s.n, s.nnz
@@ -988,7 +999,7 @@ def run_varcoef3d(args, rank, local_rank, world, torch, dist, barrier):
     from ba_b200._lib import load
 
     plat = lmp.Platform(local_rank)
-    stream = torch.cuda.current_stream()
+    stream = work_stream(torch)
     plat.set_stream(stream.cuda_stream)
     s = P.varcoef_3d(args.cells, sigma=2.0)
     n, nnz = s.n, s.nnz
@@ -1229,7 +1240,7 @@ def _c2_setup(args, local_rank, torch):
     from ba_b200 import lmp
     from ba_b200 import problems as P
     plat = lmp.Platform(local_rank)
-    stream = torch.cuda.current_stream()
+    stream = work_stream(torch)
     plat.set_stream(stream.cuda_stream)
     s = P.poisson_3d(args.cells)
     A = lmp.B200_CSR_lMatrix(s.rowptr, s.col, s.val, platform=plat)
@@ -1520,7 +1531,7 @@ def run_reference_coo(args, rank):
 def run_coo(args, rank, local_rank, world, torch, dist, barrier):
     from ba_b200 import lmp
     plat = lmp.Platform(local_rank)
-    stream = torch.cuda.current_stream()
+    stream = work_stream(torch)
     plat.set_stream(stream.cuda_stream)
     s, r, c, v = _coo_triplets(args.cells)
     dev = [torch.from_numpy(a).cuda() for a in (r, c, v)]
