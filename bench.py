@@ -81,7 +81,8 @@ def parse():
                     help="batch: partition ONE 1,024-system batch over the ranks by nnz (greedy, largest first; "
                          "strong scaling) instead of one seeded batch per rank (weak scaling)")
     ap.add_argument("--full-stream", action="store_true",
-                    help="serve: time the whole seeded 20,000-request stream once (tens of GPU-minutes)")
+                    help="serve: also serve the whole seeded request stream at the latency stream's arrival rate")
+    ap.add_argument("--stream-count", type=int, default=20000, help="serve --full-stream: requests of the stream")
     return ap.parse_args()
 
 
@@ -694,21 +695,33 @@ def run_serve(args, rank, local_rank, world, torch, dist, barrier):
     if args.full_stream:
         # the whole seeded stream, Poisson arrivals at the same fraction of the
         # measured throughput; only the result records are kept
-        full_reqs = serve_requests(SERVE_STREAM, rate, args.hi_dofs, rank)
+        full_reqs = serve_requests(args.stream_count, rate, args.hi_dofs, rank)
         S.reset_stats()
         f0 = time.monotonic()
-        ids = []
-        for rq in full_reqs:
+        pending, full_rs = [], []
+
+        def harvest():
+            # finished requests give up their stored solutions at once, so the
+            # host holds only what is in flight
+            keep = []
+            for rid in pending:
+                got = S.poll(rid, with_x=False)
+                if got is None:
+                    keep.append(rid)
+                else:
+                    full_rs.append(got[0])
+                    S.release(rid)
+            pending[:] = keep
+
+        for k, rq in enumerate(full_reqs):
             d = f0 + rq["t"] - time.monotonic()
             if d > 0:
                 time.sleep(d)
-            ids.append(S.submit_q1(rq["dim"], rq["cells"], rq["seed"], rq["sigma"]))
+            pending.append(S.submit_q1(rq["dim"], rq["cells"], rq["seed"], rq["sigma"]))
+            if k % 256 == 255:
+                harvest()
         S.drain(7200.0)
-        full_rs = []
-        for rid in ids:
-            r, _ = S.poll(rid, with_x=False)
-            full_rs.append(r)
-            S.release(rid)
+        harvest()
         st_full = S.stats()
         full = {"requests": len(full_reqs), "arrival_rate_per_s": rate, "wall_s": time.monotonic() - f0,
                 "solves_per_s": st_full["solves_per_s"], "p50_ms": st_full["p50_ms"], "p99_ms": st_full["p99_ms"],
