@@ -28,7 +28,13 @@
 // sliced ELL copy used by both SpMVs: slices of 32 rows, every row padded to
 // the system's longest row `ell`; entry k of row 32s+l sits at
 // (s*ell + k)*32 + l, so a warp reads 32 consecutive values per step and the
-// loads of one row do not depend on a row pointer.
+// loads of one row do not depend on a row pointer.  When every row's columns
+// are the row plus a subset of one ascending set of at most kMaxStencil
+// offsets (FE matrices on structured grids: the 9- and 27-point Q1
+// couplings), the copy holds values only: position k of a row is its entry
+// at column row + soff[k], 0 where the row has none, and no column is
+// stored (values-only "stencil" layout; the products a row adds are the same
+// in the same order, with exact zeros between them).
 //
 // Each system walks through phases; a phase changes only after every item of
 // the system has passed (last-arriver ticket), so all items of a system see
@@ -53,6 +59,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "internal.cuh"
@@ -62,6 +69,8 @@ namespace b200la {
 enum BatchPhase : int { PH_EMPTY = 0, PH_RESID = 1, PH_INNER = 2, PH_CORRECT = 3, PH_DONE = 4, PH_START = 5 };
 
 // Device descriptor of one system slot.
+constexpr int kMaxStencil = 27;
+
 template <typename T> struct SysDesc {
   int n;
   int nnz;
@@ -78,6 +87,8 @@ template <typename T> struct SysDesc {
   double *x;
   T *c, *r, *p, *Ap;
   const T *invd;
+  int stencil;        // 1: values-only layout, entry k of a row at column row + soff[k] (scol unused)
+  int soff[kMaxStencil];  // ascending column offsets of the stencil layout (ell of them)
 };
 
 // Per-system scalars and counters (device).
@@ -238,12 +249,35 @@ __device__ __forceinline__ V sell_row_t(const I *__restrict__ scol, const V *__r
   return sum;
 }
 
-template <typename V, typename X, int UNROLL = 9>
-__device__ __forceinline__ V sell_row(const void *scol, int col16, const V *__restrict__ sval, int ell,
-                                      const X *__restrict__ x, int slice, int lane) {
-  return col16 ? sell_row_t<V, X, short, UNROLL>((const short *)scol, sval, ell, x, slice, lane)
-               : sell_row_t<V, X, int, UNROLL>((const int *)scol, sval, ell, x, slice, lane);
+// The same from the values-only layout: column row + soff[k], clamped into
+// [0, n) where the row has no entry there (its value is 0).  soff points at
+// the system's offsets in global memory (the loop index is not a constant).
+template <typename V, typename X, int UNROLL>
+__device__ __forceinline__ V stencil_row(const int *__restrict__ soff, const V *__restrict__ sval, int ell, int n,
+                                         const X *__restrict__ x, int slice, int lane) {
+  const int64_t base = (int64_t)slice * ell * 32 + lane;
+  const V *vp = sval + base;
+  const int row = slice * 32 + lane;
+  V sum = V(0);
+#pragma unroll UNROLL
+  for (int k = 0; k < ell; ++k) {
+    const int c = min(max(row + __ldg(soff + k), 0), n - 1);
+    sum = fma(ld_stream(vp + k * 32), (V)ld_keep(x + c), sum);
+  }
+  return sum;
 }
+
+// A row from the system's sliced copy, whatever its column storage.
+template <typename V, typename X, int UNROLL = 9, typename T>
+__device__ __forceinline__ V sell_row(const SysDesc<T> &d, const SysDesc<T> *dg, const V *__restrict__ sval,
+                                      const X *__restrict__ x, int slice, int lane) {
+  if (d.stencil) return stencil_row<V, X, UNROLL>(dg->soff, sval, d.ell, d.n, x, slice, lane);
+  return d.col16 ? sell_row_t<V, X, short, UNROLL>((const short *)d.scol, sval, d.ell, x, slice, lane)
+                 : sell_row_t<V, X, int, UNROLL>((const int *)d.scol, sval, d.ell, x, slice, lane);
+}
+
+// Column type tag of the values-only layout (spmv_item's I).
+struct StencilCols {};
 
 // Warp-item loop shared by the pass kernels: warp w of the grid (W warps)
 // takes items w, w + W, w + 2W, ... and loads the next item's record while
@@ -374,9 +408,9 @@ namespace b200la {
 // or START.  It also seeds the next pass's slot of the double-buffered
 // scalars.
 template <typename T, bool PRE>
-__device__ __forceinline__ void resid_item(const Tile &tl, int t, const ItemGeo &ig, const SysDesc<T> &d, SysState &S,
-                                           double *part, int64_t part_stride, BatchGlobals *g,
-                                           const BatchParams &prm, int q) {
+__device__ __forceinline__ void resid_item(const Tile &tl, int t, const ItemGeo &ig, const SysDesc<T> &d,
+                                           const SysDesc<T> *dg, SysState &S, double *part, int64_t part_stride,
+                                           BatchGlobals *g, const BatchParams &prm, int q) {
   Acc<double> rr64;
   Acc<T> rrin, rzin;
   const int lane = threadIdx.x & 31;
@@ -384,7 +418,7 @@ __device__ __forceinline__ void resid_item(const Tile &tl, int t, const ItemGeo 
   const int end = tl.row0 + ig.rows;
   for (int sl = 0; sl < nsl; ++sl) {
     const int slice = (tl.row0 >> 5) + sl;
-    const double y = sell_row<double, double, 3>(d.scol, d.col16, d.sval64, d.ell, d.x, slice, lane);
+    const double y = sell_row<double, double, 3>(d, dg, d.sval64, d.x, slice, lane);
     const int row = slice * 32 + lane;
     if (row < end) {
       const double r64 = d.b[row] - y;
@@ -439,20 +473,23 @@ constexpr int kWin = 1280;  // values of p per warp window (FP32: 5 KB)
 
 template <typename T, typename I, int E, bool STAGE>
 __device__ __forceinline__ double spmv_item_fixed(int row0, int rows, const SysDesc<T> &d, int lane, T *win) {
+  // I = StencilCols: values-only layout, columns row + soff[k] (no column loads)
+  constexpr bool SC = std::is_same<I, StencilCols>::value;
+  using IC = typename std::conditional<SC, short, I>::type;
   Acc<T> acc;
   const int nsl = (rows + 31) >> 5;
   const int end = row0 + rows;
-  const I *__restrict__ scol = (const I *)d.scol;
+  const IC *__restrict__ scol = (const IC *)d.scol;
   const T *__restrict__ sval = d.sval;
   const T *__restrict__ p = d.p;
   int slice = row0 >> 5;
-  I cv[E];
+  IC cv[E];
   T vv[E];
   {
     const int64_t base = (int64_t)slice * E * 32 + lane;
 #pragma unroll
     for (int k = 0; k < E; ++k) {
-      cv[k] = ld_stream(scol + base + k * 32);
+      if (!SC) cv[k] = ld_stream(scol + base + k * 32);
       vv[k] = ld_stream(sval + base + k * 32);
     }
   }
@@ -468,7 +505,9 @@ __device__ __forceinline__ double spmv_item_fixed(int row0, int rows, const SysD
     T xs[E];
 #pragma unroll
     for (int k = 0; k < E; ++k) {
-      const int c = sizeof(I) == 2 ? row + (int)cv[k] : (int)cv[k];
+      // stencil: a column outside [0, n) belongs to an absent entry (value 0)
+      const int c = SC ? min(max(row + d.soff[k], 0), d.n - 1)
+                       : (sizeof(IC) == 2 ? row + (int)cv[k] : (int)cv[k]);
       xs[k] = STAGE ? win[c - lo] : ld_keep(p + c);
     }
     T vc[E];
@@ -478,7 +517,7 @@ __device__ __forceinline__ double spmv_item_fixed(int row0, int rows, const SysD
       const int64_t base = (int64_t)(slice + 1) * E * 32 + lane;
 #pragma unroll
       for (int k = 0; k < E; ++k) {
-        cv[k] = ld_stream(scol + base + k * 32);
+        if (!SC) cv[k] = ld_stream(scol + base + k * 32);
         vv[k] = ld_stream(sval + base + k * 32);
       }
     }
@@ -496,7 +535,9 @@ __device__ __forceinline__ double spmv_item_fixed(int row0, int rows, const SysD
 
 // Ap = A p over an item's rows and the item's share of p.Ap.
 template <typename T, typename I>
-__device__ __forceinline__ double spmv_item(int row0, int rows, const SysDesc<T> &d, int lane, T *win) {
+__device__ __forceinline__ double spmv_item(int row0, int rows, const SysDesc<T> &d, const SysDesc<T> *dg, int lane,
+                                            T *win) {
+  constexpr bool SC = std::is_same<I, StencilCols>::value;
   if (sizeof(T) == 4 && d.ell == 9) {
     if (win && rows + 2 * d.max_off <= kWin) return spmv_item_fixed<T, I, 9, true>(row0, rows, d, lane, win);
     return spmv_item_fixed<T, I, 9, false>(row0, rows, d, lane, nullptr);
@@ -504,10 +545,12 @@ __device__ __forceinline__ double spmv_item(int row0, int rows, const SysDesc<T>
   Acc<T> acc;
   const int nsl = (rows + 31) >> 5;
   const int end = row0 + rows;
-  const I *scol = (const I *)d.scol;
+  using IC = typename std::conditional<SC, short, I>::type;
+  const IC *scol = (const IC *)d.scol;
   for (int sl = 0; sl < nsl; ++sl) {
     const int slice = (row0 >> 5) + sl;
-    const T y = sell_row_t<T, T, I, 9>(scol, d.sval, d.ell, d.p, slice, lane);
+    const T y = SC ? stencil_row<T, T, 9>(dg->soff, d.sval, d.ell, d.n, d.p, slice, lane)
+                   : sell_row_t<T, T, IC, 9>(scol, d.sval, d.ell, d.p, slice, lane);
     const int row = slice * 32 + lane;
     if (row < end) {
       d.Ap[row] = y;
@@ -535,12 +578,13 @@ __global__ void __launch_bounds__(kBlock, 4) batch_spmv_kernel(PassLists L, cons
     const SysDesc<T> d = desc[tl.sys];
     const ItemGeo ig = item_geo(tl, t, d.n, tr);
     if (ph == PH_RESID) {
-      resid_item<T, PRE>(tl, t, ig, d, S, L.part[0], L.stride[0], g, prm, q);
+      resid_item<T, PRE>(tl, t, ig, d, desc + tl.sys, S, L.part[0], L.stride[0], g, prm, q);
       return;
     }
     // one column type per item, so each slice loop is a straight stream
-    double pap[1] = {d.col16 ? spmv_item<T, short>(tl.row0, ig.rows, d, lane, win)
-                             : spmv_item<T, int>(tl.row0, ig.rows, d, lane, win)};
+    double pap[1] = {d.stencil ? spmv_item<T, StencilCols>(tl.row0, ig.rows, d, desc + tl.sys, lane, win)
+                     : d.col16 ? spmv_item<T, short>(tl.row0, ig.rows, d, desc + tl.sys, lane, win)
+                               : spmv_item<T, int>(tl.row0, ig.rows, d, desc + tl.sys, lane, win)};
     put_partials<1>(L, st, 0, pap, t, tl.sys, d.n, tr);
   });
 }
@@ -777,6 +821,19 @@ __device__ void slot_setup_rows(const SysDesc<T> &d, unsigned *bad, int64_t firs
       pad = len > 0 ? d.col[start + len - 1] : (int)i;
     }
     const int64_t base = (i >> 5) * (int64_t)d.ell * 32 + (i & 31);
+    if (d.stencil) {
+      // values-only layout: position k holds the entry at column i + soff[k]
+      // (the device check made every row's offsets an ascending subset)
+      int j = start;
+      for (int k = 0; k < d.ell; ++k) {
+        const int64_t pos = base + (int64_t)k * 32;
+        double v = 0.0;
+        if (j < start + len && d.col[j] == (int)i + d.soff[k]) v = d.val64[j++];
+        const_cast<T *>(d.sval)[pos] = (T)v;
+        if ((const void *)d.sval64 != (const void *)d.sval) const_cast<double *>(d.sval64)[pos] = v;
+      }
+      continue;
+    }
     for (int k = 0; k < d.ell; ++k) {
       const bool real = k < len;
       const int64_t pos = base + (int64_t)k * 32;
@@ -857,7 +914,7 @@ __global__ void __launch_bounds__(kBlock, 6) batch_spmv_plain_kernel(const Tile 
     const int nsl = (rows + 31) >> 5;
     for (int sl = 0; sl < nsl; ++sl) {
       const int slice = (tl.row0 >> 5) + sl;
-      const T y = sell_row<T, T>(d.scol, d.col16, d.sval, d.ell, d.p, slice, lane);
+      const T y = sell_row<T, T>(d, desc + tl.sys, d.sval, d.p, slice, lane);
       const int row = slice * 32 + lane;
       if (row < tl.row0 + rows) d.Ap[row] = y;
     }
@@ -901,16 +958,40 @@ struct CsrCheck {
   unsigned long long err;  // ~0: valid
   int max_row;
   int max_off;
+  int stencil;             // 1 while every row checked fits the stencil below
+  int slen;                // offsets of the stencil (those of the middle row), 0: none
+  int soff[kMaxStencil];
 };
 
 __global__ void csr_check_init_kernel(int count, CsrCheck *c) {
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x)
-    c[k] = CsrCheck{~0ull, 0, 0};
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
+    CsrCheck z{};
+    z.err = ~0ull;
+    z.stencil = 1;
+    c[k] = z;
+  }
+}
+
+// The candidate stencil of a system: the column offsets of its middle row,
+// if that row's extent lies in [0, nnz], it has 1..kMaxStencil entries and
+// its columns ascend strictly; len 0 otherwise.  Every block derives the same
+// candidate (the row is checked before it is read).
+__device__ int stencil_candidate(int n, int nnz, const int *__restrict__ rowptr, const int *__restrict__ col,
+                                 int *off) {
+  const int m = n / 2;
+  const int a = rowptr[m], b = rowptr[m + 1];
+  if (a < 0 || b > nnz || b - a < 1 || b - a > kMaxStencil) return 0;
+  for (int j = a; j < b; ++j) {
+    off[j - a] = col[j] - m;
+    if (j > a && off[j - a] <= off[j - a - 1]) return 0;
+  }
+  return b - a;
 }
 
 __device__ void csr_check_rows(int n, int nnz, const int *__restrict__ rowptr, const int *__restrict__ col,
-                               CsrCheck *out, int first, int stride) {
+                               CsrCheck *out, int first, int stride, const int *soff, int slen) {
   int mr = 0, mo = 0;
+  bool fits = slen > 0;  // every row's offsets an ascending subset of soff
   unsigned long long err = ~0ull;
   for (int i = first; i < n; i += stride) {
     const int a = rowptr[i], b = rowptr[i + 1];
@@ -923,6 +1004,7 @@ __device__ void csr_check_rows(int n, int nnz, const int *__restrict__ rowptr, c
       continue;
     }
     mr = max(mr, b - a);
+    int k = 0;
     for (int j = a; j < b; ++j) {
       const int c = col[j];
       if (c < 0 || c >= n) {
@@ -930,11 +1012,17 @@ __device__ void csr_check_rows(int n, int nnz, const int *__restrict__ rowptr, c
         break;
       }
       mo = max(mo, abs(c - i));
+      if (fits) {
+        while (k < slen && soff[k] < c - i) ++k;
+        if (k < slen && soff[k] == c - i) ++k;
+        else fits = false;
+      }
     }
   }
   if (err != ~0ull) atomicMin(&out->err, err);
   if (mr) atomicMax(&out->max_row, mr);
   if (mo) atomicMax(&out->max_off, mo);
+  if (!fits) atomicMin(&out->stencil, 0);
 }
 
 // The uploaded CSR arrays of one add_many call, one job per system (n = 0:
@@ -947,11 +1035,22 @@ struct CheckJob {
 // csr_check for every job: blockIdx.y walks the jobs, blockIdx.x and the
 // threads the rows of one system; out[k] collects job k's verdict.
 __global__ void csr_check_many_kernel(const CheckJob *__restrict__ jobs, int count, CsrCheck *out) {
+  __shared__ int soff[kMaxStencil];
+  __shared__ int slen;
   for (int k = blockIdx.y; k < count; k += gridDim.y) {
     const CheckJob j = jobs[k];
+    __syncthreads();  // the previous job's stencil is no longer read
+    if (threadIdx.x == 0) {
+      slen = j.n > 0 ? stencil_candidate(j.n, j.nnz, j.rowptr, j.col, soff) : 0;
+      if (blockIdx.x == 0) {
+        out[k].slen = slen;
+        for (int q = 0; q < slen; ++q) out[k].soff[q] = soff[q];
+      }
+    }
+    __syncthreads();
     if (j.n > 0)
       csr_check_rows(j.n, j.nnz, j.rowptr, j.col, out + k, blockIdx.x * blockDim.x + threadIdx.x,
-                     gridDim.x * blockDim.x);
+                     gridDim.x * blockDim.x, soff, slen);
   }
 }
 
@@ -1067,10 +1166,10 @@ size_t csr_part_bytes(int64_t n, int64_t nnz, bool mixed) {
   b += 5 * align256(tb * n);  // c, r, p, Ap, invd
   return b;
 }
-size_t sell_part_bytes(int64_t n, int64_t ell, bool mixed, bool col16) {
+size_t sell_part_bytes(int64_t n, int64_t ell, bool mixed, bool col16, bool stencil = false) {
   const size_t tb = mixed ? 4 : 8;
   const size_t padded = (size_t)((n + 31) / 32) * 32 * (size_t)ell;
-  size_t b = align256((col16 ? 2 : 4) * padded) + align256(tb * padded);  // columns and values
+  size_t b = (stencil ? 0 : align256((col16 ? 2 : 4) * padded)) + align256(tb * padded);  // columns and values
   if (mixed) b += align256(8 * padded);                                     // FP64 values (residual)
   return b;
 }
@@ -1109,11 +1208,13 @@ int alloc_csr_part(BatchHandle B, int slot, int n, int64_t nnz, SysDesc<T> *out)
 
 // Allocates the sliced-ELL part (second chunk) once ell and the column type
 // are known.
+// stencil (soff of ell ascending offsets, or null): the values-only layout.
 template <typename T>
-int alloc_sell_part(BatchHandle B, int slot, int ell, bool col16, SysDesc<T> &d, cudaStream_t st) {
+int alloc_sell_part(BatchHandle B, int slot, int ell, bool col16, SysDesc<T> &d, cudaStream_t st,
+                    const int *stencil = nullptr) {
   HostSys &h = B->sys[slot];
   const bool mixed = B->kp.mixed != 0;
-  const size_t bytes = sell_part_bytes(d.n, ell, mixed, col16);
+  const size_t bytes = sell_part_bytes(d.n, ell, mixed, col16, stencil != nullptr);
   B_CUDA(cudaMallocAsync(&h.chunk2, bytes, st));
   h.bytes += bytes;
   char *p = (char *)h.chunk2;
@@ -1121,7 +1222,9 @@ int alloc_sell_part(BatchHandle B, int slot, int ell, bool col16, SysDesc<T> &d,
   const size_t padded = (size_t)((d.n + 31) / 32) * 32 * (size_t)ell;
   d.ell = ell;
   d.col16 = col16 ? 1 : 0;
-  d.scol = take((col16 ? 2 : 4) * padded);
+  d.stencil = stencil ? 1 : 0;
+  for (int k = 0; k < kMaxStencil; ++k) d.soff[k] = stencil && k < ell ? stencil[k] : 0;
+  d.scol = stencil ? nullptr : take((col16 ? 2 : 4) * padded);
   d.sval = (const T *)take(sizeof(T) * padded);
   d.sval64 = mixed ? (const double *)take(8 * padded) : (const double *)d.sval;
   return B200LA_OK;
@@ -1189,7 +1292,10 @@ int finish_stage(BatchHandle B, int slot, const CsrCheck &c, SysDesc<T> &d) {
     return fail(B200LA_ERR_MATRIX, "csr: a column of row %d is out of range [0,%d)", row, d.n);
   }
   const bool col16 = B->prm.index_bits != 32 && c.max_off <= 32767;
-  B_TRY(alloc_sell_part<T>(B, slot, std::max(c.max_row, 1), col16, d, B->xfer));
+  // values-only layout when every row fits the system's stencil (index_bits 0)
+  const bool stencil = B->prm.index_bits == 0 && c.stencil && c.slen >= c.max_row && c.slen > 0;
+  B_TRY(alloc_sell_part<T>(B, slot, stencil ? c.slen : std::max(c.max_row, 1), col16, d, B->xfer,
+                           stencil ? c.soff : nullptr));
   d.max_off = c.max_off;
   return B200LA_OK;
 }
@@ -1778,8 +1884,8 @@ int b200la_batch_create(b200la_ctx ctx, const b200la_batch_params *p, b200la_bat
   B_CHECK(p->inner_maxits >= 1 && p->inner_maxits <= 10000000, B200LA_ERR_INVALID, "batch_create: inner_maxits");
   B_CHECK(p->atol >= 0 && p->rtol >= 0 && p->dtol > 0, B200LA_ERR_INVALID, "batch_create: tolerances");
   B_CHECK(!p->mixed || (p->inner_rtol > 0 && p->inner_rtol < 1), B200LA_ERR_INVALID, "batch_create: inner_rtol");
-  B_CHECK(p->index_bits == 0 || p->index_bits == 32, B200LA_ERR_INVALID, "batch_create: index_bits %d (0 or 32)",
-          p->index_bits);
+  B_CHECK(p->index_bits == 0 || p->index_bits == 16 || p->index_bits == 32, B200LA_ERR_INVALID,
+          "batch_create: index_bits %d (0, 16 or 32)", p->index_bits);
   B_CHECK(p->tile_rows == 0 || (p->tile_rows >= 32 && p->tile_rows <= 65536 && p->tile_rows % 32 == 0),
           B200LA_ERR_INVALID, "batch_create: tile_rows %d (32..65536, multiple of 32)", p->tile_rows);
   b200la_batch B = new b200la_batch_s();
@@ -1860,7 +1966,20 @@ int b200la_batch_add_q1(b200la_batch B, int dim, int cells, uint64_t seed, doubl
     using T = decltype(tag);
     SysDesc<T> d{};
     B_TRY(alloc_csr_part<T>(B, slot, n, nnz, &d));
-    B_TRY(alloc_sell_part<T>(B, slot, ell, B->prm.index_bits != 32 && q1_col16(dim, cells), d, st));
+    // Q1 couplings: the node offsets dz*m^2 + dy*m + dx, ascending (m = cells + 1
+    // nodes per axis, m >= 3 so they are distinct); every row, Dirichlet rows
+    // included, stores an ascending subset of them
+    int stencil[kMaxStencil];
+    const bool use_stencil = B->prm.index_bits == 0 && cells >= 2;
+    if (use_stencil) {
+      const int64_t m = (int64_t)cells + 1;
+      int k = 0;
+      for (int dz = (dim == 3 ? -1 : 0); dz <= (dim == 3 ? 1 : 0); ++dz)
+        for (int dy = -1; dy <= 1; ++dy)
+          for (int dx = -1; dx <= 1; ++dx) stencil[k++] = (int)(dz * m * m + dy * m + dx);
+    }
+    B_TRY(alloc_sell_part<T>(B, slot, ell, B->prm.index_bits != 32 && q1_col16(dim, cells), d, st,
+                             use_stencil ? stencil : nullptr));
     d.max_off = (int)std::min<int64_t>(q1_max_off(dim, cells), INT32_MAX);
     B_TRY(q1_assemble(st, B->ctx->num_sms, dim, cells, seed, sigma, (int *)d.rowptr, (int *)d.col,
                       (double *)d.val64, (double *)d.b));

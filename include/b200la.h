@@ -418,8 +418,12 @@ typedef struct {
                          systems would give a kernel's warps fewer than one item each */
   int tile_rows;      /* rows per warp work item of every kernel, a multiple of 32
                          (0 = 256 SpMV, 1024 update, 512 direction; tunable) */
-  int index_bits;     /* sliced-ELL column storage: 0 = int16 offsets from the row when
-                         every column is within int16 of its row, else int32; 32 = int32 */
+  int index_bits;     /* sliced-ELL column storage: 0 = no columns at all when every row's columns
+                         are the row plus an ascending subset of one set of at most 27 offsets
+                         (structured-grid FE couplings: values only, the column of position k
+                         is row + offset k), else int16 offsets from the row when every column is
+                         within int16 of its row, else int32; 16 = int16 offsets when they fit,
+                         else int32; 32 = int32.  All three give the same results */
   double atol, rtol, dtol;  /* test on ||b - A x||_2 (FP64 mode: the CG recurrence residual) */
   double inner_rtol;        /* mixed: an inner pass ends at inner_rtol x its start residual */
   int restart_inner;        /* mixed: 0 = each pass continues the inner PCG from the replaced FP64

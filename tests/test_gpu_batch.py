@@ -439,3 +439,29 @@ def test_remove_and_reuse_slots_while_a_launch_is_in_flight(plat):
         np.testing.assert_array_equal(g.x, ref.x)
     assert B.info()[0] == 4
     B.close()
+
+
+@pytest.mark.parametrize("mixed", [True, False])
+def test_column_storages_give_the_same_bits(plat, mixed):
+    # the sliced copy stores no columns (values-only stencil layout, Q1
+    # systems), int16 offsets or int32 columns: each row adds the same
+    # products in the same order whatever the storage, so every system --
+    # uploaded CSR (stencil found by the device check), device-assembled Q1
+    # (stencil known), and a random matrix (no stencil) -- ends bit for bit
+    # the same in all three
+    systems = _mix(seed=9, count=9) + [P.random_spd(300, 4, density=0.02)]
+    q1 = [(2, 37, 5, 1.0), (3, 9, 6, 2.0), (2, 3, 7, 0.5)]
+    out = {}
+    for bits in (0, 16, 32):
+        B = Batch(16, mixed=mixed, precond=True, rtol=1e-9, index_bits=bits, platform=plat)
+        B.set_items(128, 512, 512, adaptive=False)
+        slots = B.add_many([(s.rowptr, s.col, s.val, s.b) for s in systems])
+        slots += [B.add_q1(*a) for a in q1]
+        B.solve(16)
+        out[bits] = B.results(slots)
+        B.close()
+    for k in range(len(out[0])):
+        for bits in (16, 32):
+            a, b = out[0][k], out[bits][k]
+            assert a.solver_state == lmp.kSolverSuccess and (a.iters, a.outer) == (b.iters, b.outer), (k, bits)
+            np.testing.assert_array_equal(a.x, b.x)
