@@ -743,24 +743,35 @@ __global__ void __launch_bounds__(kBlock, 4) batch_direction_kernel(PassLists L,
       using V = typename Vec16<T>::type;
       constexpr int W = Vec16<T>::n;
       const int nv = ig.rows / W;
-      for (int qv = lane; qv < nv; qv += 32) {
-        const int i = tl.row0 + qv * W;
-        V pv = *reinterpret_cast<const V *>(d.p + i);
-        V cv = *reinterpret_cast<const V *>(d.c + i);
-        const V rv = *reinterpret_cast<const V *>(d.r + i);
-        V dv;
-        if (PRE) dv = *reinterpret_cast<const V *>(d.invd + i);
-        T *ps = reinterpret_cast<T *>(&pv);
-        T *cs = reinterpret_cast<T *>(&cv);
-        const T *rs = reinterpret_cast<const T *>(&rv);
-        const T *ds = reinterpret_cast<const T *>(&dv);
+      // two vectors per lane per step: their eight loads are in flight together
+      for (int qv = lane; qv < nv; qv += 64) {
+        const bool two = qv + 32 < nv;
+        V pv[2], cv[2], rv[2], dv[2];
 #pragma unroll
-        for (int k = 0; k < W; ++k) {
-          cs[k] = fma(alpha, ps[k], cs[k]);
-          ps[k] = fma(beta, ps[k], PRE ? rs[k] * ds[k] : rs[k]);
+        for (int u = 0; u < 2; ++u) {
+          if (u == 1 && !two) break;
+          const int i = tl.row0 + (qv + 32 * u) * W;
+          pv[u] = *reinterpret_cast<const V *>(d.p + i);
+          cv[u] = *reinterpret_cast<const V *>(d.c + i);
+          rv[u] = *reinterpret_cast<const V *>(d.r + i);
+          if (PRE) dv[u] = *reinterpret_cast<const V *>(d.invd + i);
         }
-        *reinterpret_cast<V *>(d.c + i) = cv;
-        *reinterpret_cast<V *>(d.p + i) = pv;
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          if (u == 1 && !two) break;
+          T *ps = reinterpret_cast<T *>(&pv[u]);
+          T *cs = reinterpret_cast<T *>(&cv[u]);
+          const T *rs = reinterpret_cast<const T *>(&rv[u]);
+          const T *ds = reinterpret_cast<const T *>(&dv[u]);
+#pragma unroll
+          for (int k = 0; k < W; ++k) {
+            cs[k] = fma(alpha, ps[k], cs[k]);
+            ps[k] = fma(beta, ps[k], PRE ? rs[k] * ds[k] : rs[k]);
+          }
+          const int i = tl.row0 + (qv + 32 * u) * W;
+          *reinterpret_cast<V *>(d.c + i) = cv[u];
+          *reinterpret_cast<V *>(d.p + i) = pv[u];
+        }
       }
       for (int i = tl.row0 + nv * W + lane; i < end; i += 32) {
         const T pi = d.p[i];
