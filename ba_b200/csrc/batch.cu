@@ -495,9 +495,20 @@ __device__ __forceinline__ double spmv_item_fixed(int row0, int rows, const SysD
   }
   int lo = 0;
   if (STAGE) {
-    lo = max(row0 - d.max_off, 0);
-    const int hi = min(end + d.max_off, d.n);
-    for (int i = lo + lane; i < hi; i += 32) win[i - lo] = ld_keep(p + i);
+    // the window in 16-byte chunks by asynchronous copies (cp.async, L2 only):
+    // every lane issues all its chunks before waiting, so the window costs
+    // one round trip instead of one per load.  lo is rounded down to a chunk
+    // and the end up; a slot's vectors are 256-byte aligned allocations of
+    // whole 256-byte units, so the last chunk stays inside p's allocation
+    // (the values past n it reads are never gathered: columns are < n).
+    lo = max(row0 - d.max_off, 0) & ~3;
+    const int hi = (min(end + d.max_off, d.n) + 3) & ~3;
+    const unsigned wbase = (unsigned)__cvta_generic_to_shared(win);
+    for (int i = lo + 4 * lane; i < hi; i += 128)
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(wbase + 4u * (unsigned)(i - lo)),
+                   "l"(p + i)
+                   : "memory");
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
     __syncwarp();
   }
   for (int sl = 0; sl < nsl; ++sl, ++slice) {
@@ -539,7 +550,8 @@ __device__ __forceinline__ double spmv_item(int row0, int rows, const SysDesc<T>
                                             T *win) {
   constexpr bool SC = std::is_same<I, StencilCols>::value;
   if (sizeof(T) == 4 && d.ell == 9) {
-    if (win && rows + 2 * d.max_off <= kWin) return spmv_item_fixed<T, I, 9, true>(row0, rows, d, lane, win);
+    // (+6: the window's ends are rounded out to 16-byte chunks)
+    if (win && rows + 2 * d.max_off + 6 <= kWin) return spmv_item_fixed<T, I, 9, true>(row0, rows, d, lane, win);
     return spmv_item_fixed<T, I, 9, false>(row0, rows, d, lane, nullptr);
   }
   Acc<T> acc;
@@ -567,7 +579,7 @@ __global__ void __launch_bounds__(kBlock, 4) batch_spmv_kernel(PassLists L, cons
   const int lane = threadIdx.x & 31;
   // per-warp window of p for banded FP32 systems (see spmv_item_fixed)
   constexpr int kWinT = sizeof(T) == 4 ? kWin : 1;
-  __shared__ T win_all[kBlock / 32][kWinT];
+  __shared__ __align__(16) T win_all[kBlock / 32][kWinT];
   T *win = sizeof(T) == 4 ? win_all[threadIdx.x >> 5] : nullptr;
   const int tr = g->tile_rows[0];
   const int q = (int)(__ldg(&g->pass_total) & 1u);
