@@ -289,23 +289,29 @@ struct StencilCols {};
 // thousands of warps contend on one address; so was giving each warp a
 // contiguous run of items: 194 against 158 us for the 1,024-system K1, the
 // warps' concurrent reads then spread over the whole batch.)
+//
+// rev: walk the list from its end.  Consecutive pass kernels walk in
+// opposite directions (K1 forward on even passes, K2 the other way, K3 as
+// K1), so each kernel starts on the rows its predecessor touched last,
+// whose vectors are the likeliest to be still in L2.
 template <typename F>
-__device__ __forceinline__ void for_each_item(const Tile *__restrict__ tiles, int ntiles, const SysState *st,
+__device__ __forceinline__ void for_each_item(const Tile *__restrict__ tiles, int ntiles, const SysState *st, bool rev,
                                               F &&body) {
   const int nw = gridDim.x * (kBlock / 32);
-  int t = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
-  Tile tl = t < ntiles ? tiles[t] : Tile{};
-  Tile nx = t + nw < ntiles ? tiles[t + nw] : Tile{};
-  int ph = t < ntiles ? load_phase(st + tl.sys) : (int)PH_EMPTY;
-  while (t < ntiles) {
-    const int tn = t + nw;
-    const Tile nn = tn + nw < ntiles ? tiles[tn + nw] : Tile{};
-    const int nph = tn < ntiles ? load_phase(st + nx.sys) : (int)PH_EMPTY;
-    body(tl, t, ph);
+  int k = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);  // position in the walk
+  auto at = [&](int j) { return rev ? ntiles - 1 - j : j; };
+  Tile tl = k < ntiles ? tiles[at(k)] : Tile{};
+  Tile nx = k + nw < ntiles ? tiles[at(k + nw)] : Tile{};
+  int ph = k < ntiles ? load_phase(st + tl.sys) : (int)PH_EMPTY;
+  while (k < ntiles) {
+    const int kn = k + nw;
+    const Tile nn = kn + nw < ntiles ? tiles[at(kn + nw)] : Tile{};
+    const int nph = kn < ntiles ? load_phase(st + nx.sys) : (int)PH_EMPTY;
+    body(tl, at(k), ph);
     tl = nx;
     nx = nn;
     ph = nph;
-    t = tn;
+    k = kn;
   }
 }
 
@@ -595,7 +601,7 @@ __global__ void __launch_bounds__(kBlock, 4) batch_spmv_kernel(PassLists L, cons
   T *win = sizeof(T) == 4 ? win_all[threadIdx.x >> 5] : nullptr;
   const int tr = g->tile_rows[0];
   const int q = (int)(__ldg(&g->pass_total) & 1u);
-  for_each_item(L.tiles[0], g->ntiles[0], st, [&](const Tile &tl, int t, int ph) {
+  for_each_item(L.tiles[0], g->ntiles[0], st, q != 0, [&](const Tile &tl, int t, int ph) {
     if (ph != PH_INNER && ph != PH_RESID) return;
     SysState &S = st[tl.sys];
     const SysDesc<T> d = desc[tl.sys];
@@ -619,7 +625,7 @@ __global__ void __launch_bounds__(kBlock, 4) batch_update_kernel(PassLists L, co
   const int lane = threadIdx.x & 31;
   const int tr = g->tile_rows[1];
   const int q = (int)(__ldg(&g->pass_total) & 1u);
-  for_each_item(L.tiles[1], g->ntiles[1], st, [&](const Tile &tl, int t, int ph) {
+  for_each_item(L.tiles[1], g->ntiles[1], st, q == 0, [&](const Tile &tl, int t, int ph) {
     if (ph != PH_INNER) return;
     SysState &S = st[tl.sys];
     const SysDesc<T> d = desc[tl.sys];
@@ -686,7 +692,7 @@ __global__ void __launch_bounds__(kBlock, 4) batch_direction_kernel(PassLists L,
   const int lane = threadIdx.x & 31;
   const int tr = g->tile_rows[2];
   const int q = (int)(__ldg(&g->pass_total) & 1u);
-  for_each_item(L.tiles[2], g->ntiles[2], st, [&](const Tile &tl, int t, int ph) {
+  for_each_item(L.tiles[2], g->ntiles[2], st, q != 0, [&](const Tile &tl, int t, int ph) {
     if (ph != PH_INNER && ph != PH_START) return;
     SysState &S = st[tl.sys];
     const SysDesc<T> d = desc[tl.sys];
