@@ -51,8 +51,9 @@ def main():
                     help="instead: solve a batch of this many 2D systems (n~logU[16,256], sigma 1) twice")
     ap.add_argument("--chunk", type=int, default=64)
     ap.add_argument("--tile-rows", type=int, default=0)
-    ap.add_argument("--index-bits", type=int, default=0, choices=[0, 32],
-                    help="batch: sliced-ELL columns (0 = int16 offsets when they fit, 32 = int32)")
+    ap.add_argument("--index-bits", type=int, default=0, choices=[0, 16, 32],
+                    help="batch: sliced-ELL columns (0 = values only when every row fits the system's stencil, "
+                         "else int16 offsets when they fit; 16 = int16 offsets when they fit; 32 = int32)")
     ap.add_argument("--items", default="", help="batch: K1,K2,K3 item rows instead of tuning")
     ap.add_argument("--profile-only", action="store_true",
                     help="batch: skip the solves; time one inner pass kernel by kernel (b200la_batch_profile_pass)")
@@ -221,8 +222,9 @@ def batch_case(a):
     from .batch import Batch
     systems = P.batch_systems(a.batch, sigma=1.0, seed=P.SEED_BATCH)
     plat = lmp.init_platform(0)
-    B = Batch(len(systems), mixed=True, precond=True, rtol=1e-8, inner_rtol=1e-4, tile_rows=a.tile_rows,
-              index_bits=a.index_bits, platform=plat)
+    # the settings of bench.py's batch workload
+    B = Batch(len(systems), mixed=True, precond=True, rtol=1e-8, atol=0.0, dtol=1e8, inner_rtol=0.1, max_outer=60,
+              tile_rows=a.tile_rows, index_bits=a.index_bits, platform=plat)
     for s in systems:
         B.add_system(s)
     if a.items:
