@@ -498,7 +498,8 @@ def run_batch(args, rank, local_rank, world, torch, dist, barrier):
                 "precision": f"FP32 Jacobi-PCG inner solves (FP32 matrix values and vectors, compensated FP32 "
                              f"dots) inside FP64 refinement: the FP64 residual replaces the inner one every "
                              f"{inner_rtol:g}x reduction, the search direction is kept",
-                "spmv_schedule": "sliced ELL, 32 rows per slice, one row per lane",
+                "spmv_schedule": ("sliced ELL, 32 rows per slice, one row per lane; values only (columns = row + the "
+                                  "system's 9 stencil offsets), p window staged in shared memory"),
                 "p50_latency_ms": float(np.percentile(lat, 50)), "p99_latency_ms": float(np.percentile(lat, 99)),
                 "latency": "per-system device time from its first residual to its finish inside the step",
                 "converged": f"{ok}/{len(systems)}", "worst_true_rel_residual_sampled": worst,
