@@ -13,8 +13,8 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libb200la.so")
 
 F64, F32 = 0, 1
-FMT_CSR, FMT_SELL, FMT_SELL16 = 1, 4, 5
-FORMAT_NAMES = {FMT_CSR: "csr", FMT_SELL: "sell", FMT_SELL16: "sell16"}
+FMT_CSR, FMT_SELL, FMT_SELL16, FMT_STENCIL = 1, 4, 5, 6
+FORMAT_NAMES = {FMT_CSR: "csr", FMT_SELL: "sell", FMT_SELL16: "sell16", FMT_STENCIL: "stencil"}
 ITERATE, SUCCESS_ABS, SUCCESS_REL, FAIL_DIV, FAIL_MAXITS, FAIL_BREAKDOWN, DONE_FIXED = range(7)
 METHOD_JACOBI, METHOD_BICGSTAB, METHOD_GMRES = 1, 2, 3
 SOLVER_SUCCESS, SOLVER_EXCEEDED, SOLVER_ERROR = range(3)

@@ -686,7 +686,7 @@ int b200la_mat_cast(b200la_mat src, int dtype, b200la_mat *out) {
       cast_kernel<double, float><<<grid, kBlock, 0, s>>>(src->nnz, (double *)m->val, (const float *)src->val);
     B_CUDA(cudaGetLastError());
   }
-  if (is_sell(m->format)) B_TRY(sell_build(m, m->param, m->format == B200LA_FMT_SELL16));
+  if (is_sliced(m->format)) B_TRY(sliced_rebuild(m, m->format, m->param, src->sell.c, src->sell.sigma));
   B_CUDA(cudaStreamSynchronize(s));
   *out = m;
   return B200LA_OK;
@@ -708,12 +708,10 @@ int b200la_mat_zero_rows(b200la_mat m, const int *rows, int size, double alpha) 
     zero_rows_kernel<float><<<grid, kBlock, 0, s>>>(size, d_rows, m->rowptr, m->col, (float *)m->val, (float)alpha);
   B_CUDA(cudaGetLastError());
   B_CUDA(cudaFreeAsync(d_rows, s));
-  if (is_sell(m->format)) {
-    // the values changed: rebuild the sliced copy
-    const int w = m->param;
-    const bool c16 = m->format == B200LA_FMT_SELL16;
-    sell_free(m);
-    B_TRY(sell_build(m, w, c16));
+  if (is_sliced(m->format)) {
+    // the values changed: rebuild the sliced copy with the same geometry
+    const int C = m->sell.c, sigma = m->sell.sigma;
+    B_TRY(sliced_rebuild(m, m->format, m->param, C, sigma));
   }
   B_CUDA(cudaStreamSynchronize(s));
   return B200LA_OK;
@@ -784,6 +782,14 @@ int b200la_mat_set_format(b200la_mat m, int format, int param) {
     m->sched_gen += 1;
     return B200LA_OK;
   }
+  if (format == B200LA_FMT_STENCIL) {
+    B_CHECK(param == 1 || param == 2 || param == 4, B200LA_ERR_INVALID, "mat_set_format: STENCIL width %d", param);
+    B_TRY(stencil_build(m, param));
+    m->format = format;
+    m->param = param;
+    m->sched_gen += 1;
+    return B200LA_OK;
+  }
   return fail(B200LA_ERR_UNSUPPORTED, "mat_set_format: format %d", format);
 }
 
@@ -799,7 +805,7 @@ int b200la_mat_to_sell(b200la_mat m, int C, int sigma, int width, int col16) {
 
 int b200la_mat_get_sell(b200la_mat m, int *C, int *sigma, int64_t *padded) {
   B_CHECK(m && C && sigma, B200LA_ERR_INVALID, "mat_get_sell: null argument");
-  B_CHECK(is_sell(m->format), B200LA_ERR_INVALID, "mat_get_sell: the matrix's schedule is not sliced");
+  B_CHECK(is_sliced(m->format), B200LA_ERR_INVALID, "mat_get_sell: the matrix's schedule is not sliced");
   *C = m->sell.c;
   *sigma = m->sell.sigma;
   if (padded) *padded = m->sell.padded;

@@ -75,6 +75,8 @@ struct b200la_vec_s {
   bool owned;
 };
 
+constexpr int kStencilMax = 28;  // stored entries per row of the values-only copy (27 + padding)
+
 struct SellData {
   int nslices = 0;
   int width = 0;        // values per thread per step (1, 2 or 4)
@@ -89,6 +91,13 @@ struct SellData {
   int c = 32;                // rows per slice (SELL-C-sigma's C: 8, 16 or 32)
   int log2c = 5;
   int sigma = 1;             // rows per sorting window (1: no sorting)
+  // values-only copy (B200LA_FMT_STENCIL): every row stores `ell` entries,
+  // entry k at column row + soff[k] (clamped into [0, n); value 0 where the
+  // row has no entry there); no column storage
+  int stencil = 0;
+  int ell = 0;
+  int soff[kStencilMax] = {};
+  int off_lo = 0, off_hi = 0;  // smallest and largest offset
 };
 
 struct b200la_mat_s {

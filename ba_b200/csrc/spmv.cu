@@ -271,6 +271,144 @@ int sell_build(b200la_mat m, int width, bool col16, int C, int sigma) {
   return B200LA_OK;
 }
 
+// ---- values-only copy (B200LA_FMT_STENCIL) ---------------------------------
+struct StencilOffsets {
+  int v[kStencilMax];
+};
+
+// The first row of the longest length (the stencil's source).
+__global__ void longest_row_kernel(int n, const int *__restrict__ rowptr, int len, int *__restrict__ first) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+    if (rowptr[i + 1] - rowptr[i] == len) atomicMin(first, i);
+}
+
+// Every row's columns strictly ascending and each column - row one of the E
+// ascending offsets (a two-pointer walk); *bad = 1 otherwise.
+__global__ void stencil_check_kernel(int n, const int *__restrict__ rowptr, const int *__restrict__ col,
+                                     StencilOffsets off, int E, int *__restrict__ bad) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    int k = 0;
+    bool ok = true;
+    for (int j = rowptr[i]; j < rowptr[i + 1] && ok; ++j) {
+      const int d = col[j] - i;
+      while (k < E && off.v[k] < d) ++k;
+      ok = k < E && off.v[k] == d;
+      ++k;  // strictly ascending: the next column takes a later offset
+    }
+    if (!ok) *bad = 1;
+  }
+}
+
+// Thread t: position t % 32 of slice t / 32 (row 32s + r); entry k of the
+// row at s*EP*32 + ((k/W)*32 + r)*W + k%W, the row's value at column
+// row + off[k] or 0 (rows past n: all 0).
+template <typename T>
+__global__ void stencil_fill_kernel(int n, int nslices, int EP, int W, const int *__restrict__ rowptr,
+                                    const int *__restrict__ col, const T *__restrict__ val, StencilOffsets off,
+                                    T *__restrict__ sval) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int s = (int)(t >> 5), r = (int)(t & 31);
+  if (s >= nslices) return;
+  const int row = s * 32 + r;
+  int j = row < n ? rowptr[row] : 0;
+  const int end = row < n ? rowptr[row + 1] : 0;
+  T *base = sval + (int64_t)s * EP * 32;
+  for (int k = 0; k < EP; ++k) {
+    T v = T(0);
+    if (j < end && col[j] - row == off.v[k]) v = val[j++];
+    base[((k / W) * 32 + r) * W + k % W] = v;
+  }
+}
+
+int stencil_build(b200la_mat m, int width) {
+  B_CHECK(width == 1 || width == 2 || width == 4, B200LA_ERR_INVALID, "STENCIL: width %d (1, 2 or 4)", width);
+  SellData &cur = m->sell;
+  if (cur.stencil && cur.width == width && cur.val) return B200LA_OK;
+  B_CHECK(m->nrow == m->ncol && m->nrow > 0, B200LA_ERR_UNSUPPORTED, "STENCIL: square matrices only (%dx%d)",
+          m->nrow, m->ncol);
+  const int E = m->max_row;
+  B_CHECK(E == 9 || E == 27, B200LA_ERR_UNSUPPORTED, "STENCIL: longest row %d (9 or 27 entries)", E);
+  cudaStream_t s = m->ctx->stream;
+  const int n = m->nrow;
+  // the offsets of the first longest row
+  int *d_tmp = nullptr;
+  B_CUDA(cudaMallocAsync(&d_tmp, sizeof(int) * 2, s));
+  const int first_init = INT32_MAX;
+  B_CUDA(cudaMemcpyAsync(d_tmp, &first_init, sizeof(int), cudaMemcpyHostToDevice, s));
+  B_CUDA(cudaMemsetAsync(d_tmp + 1, 0, sizeof(int), s));
+  const int grid = std::min((n + kBlock - 1) / kBlock, m->ctx->num_sms * 8);
+  longest_row_kernel<<<grid, kBlock, 0, s>>>(n, m->rowptr, E, d_tmp);
+  B_CUDA(cudaGetLastError());
+  int first = 0, start = 0;
+  B_CUDA(cudaMemcpyAsync(&first, d_tmp, sizeof(int), cudaMemcpyDeviceToHost, s));
+  B_CUDA(cudaStreamSynchronize(s));
+  int rc = B200LA_OK;
+  StencilOffsets off{};
+  if (first == INT32_MAX) rc = fail(B200LA_ERR_UNSUPPORTED, "STENCIL: no row of the longest length");
+  if (rc == B200LA_OK) {
+    int cols[kStencilMax];
+    cudaError_t e = cudaMemcpyAsync(&start, m->rowptr + first, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(cols, m->col + start, sizeof(int) * E, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) rc = fail(B200LA_ERR_CUDA, "STENCIL: %s", cudaGetErrorString(e));
+    for (int k = 0; rc == B200LA_OK && k < E; ++k) {
+      off.v[k] = cols[k] - first;
+      if (k > 0 && off.v[k] <= off.v[k - 1])
+        rc = fail(B200LA_ERR_UNSUPPORTED, "STENCIL: the columns of row %d are not strictly ascending", first);
+    }
+  }
+  int bad = 0;
+  if (rc == B200LA_OK) {
+    stencil_check_kernel<<<grid, kBlock, 0, s>>>(n, m->rowptr, m->col, off, E, d_tmp + 1);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&bad, d_tmp + 1, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) rc = fail(B200LA_ERR_CUDA, "STENCIL: %s", cudaGetErrorString(e));
+    else if (bad) rc = fail(B200LA_ERR_UNSUPPORTED, "STENCIL: a row's columns are not in the stencil of row %d", first);
+  }
+  cudaFreeAsync(d_tmp, s);
+  B_TRY(rc);
+  sell_free(m);
+  m->sched_gen += 1;  // graphs holding the old copy's pointers re-capture
+  SellData &d = m->sell;
+  const int EP = (E + width - 1) / width * width;
+  for (int k = E; k < EP; ++k) off.v[k] = 0;  // padding: value 0 at the row's own column
+  d.stencil = 1;
+  d.width = width;
+  d.ell = EP;
+  d.c = 32;
+  d.log2c = 5;
+  d.sigma = 1;
+  d.nslices = (n + 31) / 32;
+  d.padded = (int64_t)d.nslices * 32 * EP;
+  d.off_lo = d.off_hi = 0;  // 0 included: the padding's column
+  for (int k = 0; k < EP; ++k) {
+    d.soff[k] = off.v[k];
+    d.off_lo = std::min(d.off_lo, off.v[k]);
+    d.off_hi = std::max(d.off_hi, off.v[k]);
+  }
+  B_CUDA(cudaMallocAsync(&d.val, dtype_size(m->dtype) * (size_t)d.padded, s));
+  const int fgrid = (int)(((int64_t)d.nslices * 32 + kBlock - 1) / kBlock);
+  if (m->dtype == B200LA_F64)
+    stencil_fill_kernel<double><<<fgrid, kBlock, 0, s>>>(n, d.nslices, EP, width, m->rowptr, m->col,
+                                                         (const double *)m->val, off, (double *)d.val);
+  else
+    stencil_fill_kernel<float><<<fgrid, kBlock, 0, s>>>(n, d.nslices, EP, width, m->rowptr, m->col,
+                                                        (const float *)m->val, off, (float *)d.val);
+  B_CUDA(cudaGetLastError());
+  B_CUDA(cudaStreamSynchronize(s));
+  return B200LA_OK;
+}
+
+int sliced_rebuild(b200la_mat m, int format, int param, int C, int sigma) {
+  sell_free(m);
+  if (format == B200LA_FMT_STENCIL) return stencil_build(m, param);
+  return sell_build(m, param, format == B200LA_FMT_SELL16, C, sigma);
+}
+
 }  // namespace b200la
 
 using namespace b200la;
@@ -281,7 +419,8 @@ extern "C" int b200la_mat_tune(b200la_mat m, int *format, int *param, double *us
   cudaStream_t s = c->stream;
   // candidates {format, param, C, sigma}: CSR lane groups; SELL and SELL16
   // with vector widths 1/2/4 and slice heights C = 32, 16, 8, rows in their
-  // order (sigma 1) or sorted by length within windows of 1,024 rows
+  // order (sigma 1) or sorted by length within windows of 1,024 rows; the
+  // values-only copy with widths 1/2/4 (matrices with a stencil)
   std::vector<std::array<int, 4>> fmts = {{B200LA_FMT_CSR, 2, 0, 0},  {B200LA_FMT_CSR, 4, 0, 0},
                                           {B200LA_FMT_CSR, 8, 0, 0},  {B200LA_FMT_CSR, 16, 0, 0},
                                           {B200LA_FMT_CSR, 32, 0, 0}};
@@ -289,6 +428,7 @@ extern "C" int b200la_mat_tune(b200la_mat m, int *format, int *param, double *us
     for (int sig : {1, 1024})
       for (int cc : {32, 16, 8})
         for (int w : {1, 2, 4}) fmts.push_back({f, w, cc, sig});
+  for (int w : {1, 2, 4}) fmts.push_back({B200LA_FMT_STENCIL, w, 32, 1});
   size_t es = dtype_size(m->dtype);
   void *x = nullptr, *y = nullptr;
   B_CUDA(cudaMallocAsync(&x, es * (m->ncol > 0 ? m->ncol : 1), s));
@@ -301,9 +441,14 @@ extern "C" int b200la_mat_tune(b200la_mat m, int *format, int *param, double *us
   float best = 1e30f;
   const int reps = 10;
   for (auto &fp : fmts) {
-    if (is_sell(fp[0])) {
-      // SELL copies cost extra HBM; skip them when they would pad badly.
-      if (b200la_mat_to_sell(m, fp[2], fp[3], fp[1], fp[0] == B200LA_FMT_SELL16) != B200LA_OK) continue;
+    if (is_sliced(fp[0])) {
+      // sliced copies cost extra HBM; skip them when they would pad badly
+      // (STENCIL: when the matrix has no stencil)
+      if (fp[0] == B200LA_FMT_STENCIL) {
+        if (b200la_mat_set_format(m, fp[0], fp[1]) != B200LA_OK) continue;
+      } else if (b200la_mat_to_sell(m, fp[2], fp[3], fp[1], fp[0] == B200LA_FMT_SELL16) != B200LA_OK) {
+        continue;
+      }
       if ((double)m->sell.padded > 1.25 * (double)m->nnz + 2.0 * fp[2] * m->sell.nslices) continue;
     } else if (b200la_mat_set_format(m, fp[0], fp[1]) != B200LA_OK) {
       continue;
@@ -317,7 +462,7 @@ extern "C" int b200la_mat_tune(b200la_mat m, int *format, int *param, double *us
     B_CUDA(cudaEventElapsedTime(&ms, e0, e1));
     // a sliced copy must beat the best so far by 1% to win, so C = 32
     // without sorting (listed first) is kept where the others only tie
-    if (ms < (is_sell(fp[0]) && is_sell(best_f) ? 0.99f : 1.0f) * best) {
+    if (ms < (is_sliced(fp[0]) && is_sliced(best_f) ? 0.99f : 1.0f) * best) {
       best = ms;
       best_f = fp[0];
       best_p = fp[1];
@@ -331,7 +476,7 @@ extern "C" int b200la_mat_tune(b200la_mat m, int *format, int *param, double *us
   cudaFreeAsync(y, s);
   if (is_sell(best_f)) B_TRY(b200la_mat_to_sell(m, best_c, best_sig, best_p, best_f == B200LA_FMT_SELL16));
   else B_TRY(b200la_mat_set_format(m, best_f, best_p));
-  if (!is_sell(best_f)) sell_free(m);
+  if (!is_sliced(best_f)) sell_free(m);
   if (format) *format = best_f;
   if (param) *param = best_p;
   if (usec) *usec = 1000.0 * best / reps;

@@ -171,6 +171,66 @@ template <typename T, int W, typename X = T> struct SellOp16 {
   }
 };
 
+// ---- values-only sliced ELL (a stencil of column offsets) -----------------
+// Square matrices whose every row's columns are a subset of one ascending
+// list of offsets (structured-grid FE matrices): 32-row slices, every row
+// EP entries (the stencil, padded to a multiple of W with offset 0), entry k
+// of the row at position r of slice s at s*EP*32 + ((k/W)*32 + r)*W + k%W,
+// value 0 where the row has no entry.  The column of entry k is
+// row + off[k] (a compile-time index into the operator's offsets, which sit
+// in the kernel's parameter space); slices whose columns all fall inside
+// [0, n) skip the clamp the border slices need.  No column bytes at all:
+// an FP64 3D Q1 row moves 8 bytes per entry instead of 10 (SELL16) or 12.
+// Products in ascending column order, the rows' stored order, so the bits
+// are SELL's (absent entries add 0 * x).
+template <typename T, int W, int EP, typename X = T> struct StencilOp {
+  using XT = X;
+  const T *__restrict__ val;
+  int n, nslices;
+  int lo, hi;  // smallest and largest offset
+  int off[EP];
+  static constexpr int kRowsPerBlock = kBlock;
+  __host__ __device__ int64_t work_items() const { return n; }
+  template <typename Emit> __device__ __forceinline__ void run(const X *__restrict__ x, Emit &emit) const {
+    using VV = typename VecW<T, W>::v;
+    const int lane = threadIdx.x & 31;
+    const int wpb = kBlock / 32;
+    for (int s = blockIdx.x * wpb + ((int)threadIdx.x >> 5); s < nslices; s += gridDim.x * wpb) {
+      const int row = s * 32 + lane;
+      const VV *vi = reinterpret_cast<const VV *>(val + (int64_t)s * EP * 32) + lane;
+      X sum = X(0);
+      if (s * 32 + lo >= 0 && s * 32 + 31 + hi < n) {
+#pragma unroll
+        for (int c = 0; c < EP / W; ++c) {
+          const VV vv = ld_vec_stream(vi + c * 32);
+#pragma unroll
+          for (int k = 0; k < W; ++k) sum = fma((X)lane_get<VV, T, W>(vv, k), ld_keep(x + row + off[c * W + k]), sum);
+        }
+      } else {
+#pragma unroll
+        for (int c = 0; c < EP / W; ++c) {
+          const VV vv = ld_vec_stream(vi + c * 32);
+#pragma unroll
+          for (int k = 0; k < W; ++k)
+            sum = fma((X)lane_get<VV, T, W>(vv, k), ld_keep(x + min(max(row + off[c * W + k], 0), n - 1)), sum);
+        }
+      }
+      if (row < n) emit(row, sum);
+    }
+  }
+};
+
+template <typename Op> Op stencil_op(const void *val, int n, const SellData &s) {
+  Op op;
+  op.val = (decltype(op.val))val;
+  op.n = n;
+  op.nslices = s.nslices;
+  op.lo = s.off_lo;
+  op.hi = s.off_hi;
+  for (int k = 0; k < (int)(sizeof(op.off) / sizeof(int)); ++k) op.off[k] = s.soff[k];
+  return op;
+}
+
 // ---- plain emitters --------------------------------------------------------
 template <typename T> struct StoreEmit {
   T *__restrict__ y;
@@ -219,6 +279,19 @@ template <typename T, typename X = T, typename F> int with_schedule(b200la_mat m
     }
     return fail(B200LA_ERR_INVALID, "SELL16 width %d", m->param);
   }
+  if (m->format == B200LA_FMT_STENCIL) {
+    const SellData &s = m->sell;
+    const int key = m->param * 100 + s.ell;
+    switch (key) {
+      case 109: return f(stencil_op<StencilOp<T, 1, 9, X>>(s.val, m->nrow, s));
+      case 210: return f(stencil_op<StencilOp<T, 2, 10, X>>(s.val, m->nrow, s));
+      case 412: return f(stencil_op<StencilOp<T, 4, 12, X>>(s.val, m->nrow, s));
+      case 127: return f(stencil_op<StencilOp<T, 1, 27, X>>(s.val, m->nrow, s));
+      case 228: return f(stencil_op<StencilOp<T, 2, 28, X>>(s.val, m->nrow, s));
+      case 428: return f(stencil_op<StencilOp<T, 4, 28, X>>(s.val, m->nrow, s));
+    }
+    return fail(B200LA_ERR_INVALID, "STENCIL width %d with %d entries per row", m->param, s.ell);
+  }
   switch (m->param) {
     case 1: return f(CsrOp<T, 1, X>{m->rowptr, m->col, val, m->nrow});
     case 2: return f(CsrOp<T, 2, X>{m->rowptr, m->col, val, m->nrow});
@@ -237,7 +310,15 @@ int spmv_nodiag_launch(b200la_mat m, const void *x, void *y, cudaStream_t s);
 // offsets (col16), C rows per slice, rows sorted by length within windows of
 // sigma rows (1 = no sorting; otherwise rounded up to a multiple of C).
 int sell_build(b200la_mat m, int width, bool col16 = false, int C = 32, int sigma = 1);
+// Builds the values-only copy (B200LA_FMT_STENCIL) with `width` entries per
+// vector load; B200LA_ERR_UNSUPPORTED when the matrix has no stencil.
+int stencil_build(b200la_mat m, int width);
 inline bool is_sell(int format) { return format == B200LA_FMT_SELL || format == B200LA_FMT_SELL16; }
+// any schedule with a sliced copy (rebuilt when the values change)
+inline bool is_sliced(int format) { return is_sell(format) || format == B200LA_FMT_STENCIL; }
+// frees the sliced copy and builds the one `format` / `param` name (C and
+// sigma for SELL-C-sigma) from the CSR: after the values changed
+int sliced_rebuild(b200la_mat m, int format, int param, int C, int sigma);
 void sell_free(b200la_mat m);
 
 }  // namespace b200la

@@ -33,7 +33,7 @@ import numpy as np
 
 from . import lmp
 from . import problems as P
-from ._lib import FMT_CSR, FMT_SELL, FMT_SELL16, FORMAT_NAMES, call, load
+from ._lib import FMT_CSR, FMT_SELL, FMT_SELL16, FMT_STENCIL, FORMAT_NAMES, call, load
 
 
 def main():
@@ -59,7 +59,8 @@ def main():
                     help="batch: skip the solves; time one inner pass kernel by kernel (b200la_batch_profile_pass)")
     ap.add_argument("--sell-table", action="store_true",
                     help="instead: time every SpMV schedule (CSR lane groups, SELL-C-sigma with C 8/16/32, sigma "
-                         "1/1024, widths 1/2/4, int32/int16 columns) on three matrices and print a table")
+                         "1/1024, widths 1/2/4, int32/int16 columns; the values-only stencil copy with widths 1/2/4) on "
+                         "three matrices and print a table")
     a = ap.parse_args()
     if a.sell_table:
         return sell_table(a)
@@ -73,7 +74,7 @@ def main():
         fmt, prm, us = A.tune()
     else:
         kind, prm = a.schedule.split("/")
-        fmt, prm = {"sell": FMT_SELL, "sell16": FMT_SELL16, "csr": FMT_CSR}[kind], int(prm)
+        fmt, prm = {"sell": FMT_SELL, "sell16": FMT_SELL16, "csr": FMT_CSR, "stencil": FMT_STENCIL}[kind], int(prm)
         A.set_format(fmt, prm)
         us = float("nan")
     x = lmp.B200_lVector.from_numpy(s.b.astype(dt), platform=plat, dtype=dt)
@@ -167,6 +168,12 @@ def sell_table(a):
                         padded = A.sell_padded()
                         rows.append((f"{'sell16' if col16 else 'sell'}/{w}", c, sigma, timed(),
                                      f"{padded / s.nnz - 1:.1%}"))
+        for w in (1, 2, 4):
+            try:
+                A.set_format(FMT_STENCIL, w)
+            except lmp.B200LAError:
+                continue
+            rows.append((f"stencil/{w}", 32, 1, timed(), f"{A.sell_padded() / s.nnz - 1:.1%}"))
         best = min(rows, key=lambda r: r[3])
         for r in rows:
             mark = " **" if r is best else ""

@@ -67,6 +67,9 @@ typedef struct b200la_batch_s *b200la_batch;
 #define B200LA_FMT_SELL 4 /* SELL-C-sigma (C = 32 and sigma = 1 unless b200la_mat_to_sell says otherwise) */
 #define B200LA_FMT_SELL16 5 /* SELL-32 with columns stored as int16 offsets from the row
                              (banded matrices: every |col - row| <= 32767) */
+#define B200LA_FMT_STENCIL 6 /* values-only sliced ELL: square matrices whose rows' columns all
+                              lie in one list of 9 or 27 offsets from the row (structured-grid
+                              Q1 matrices); no column storage */
 
 /* ---- library / context ---------------------------------------------------
  * replaces init_platform_gpu (lmp/cuda/platform_management_gpu.cu:78-143) */
@@ -185,8 +188,17 @@ int b200la_spmv_nodiag(b200la_mat m, b200la_vec x, b200la_vec y);
  * B200LA_ERR_MATRIX if a row has no stored nonzero diagonal. */
 int b200la_mat_inv_diag(b200la_mat m, b200la_vec out);
 /* Pick the SpMV schedule: format B200LA_FMT_CSR with `param` threads per row
- * (1..32, power of two), or B200LA_FMT_SELL with `param` rows per thread
- * chunk width (1, 2 or 4); builds the SELL copy on first use. */
+ * (1..32, power of two), or B200LA_FMT_SELL / SELL16 / STENCIL with `param`
+ * entries per vector load (1, 2 or 4); builds the sliced copy on first use.
+ * STENCIL (no reference counterpart): the stencil is the offsets of a
+ * longest row; every row's columns must be strictly ascending and a subset
+ * of it (checked on the device), and it must have 9 or 27 entries, else
+ * B200LA_ERR_UNSUPPORTED.  Each row stores one value per offset (0 where it
+ * has no entry; the list is padded with offset 0 to a multiple of `param`),
+ * so the copy holds values only; a row's products are added in ascending
+ * column order, its stored order, so the results are SELL's bits (the
+ * absent entries add 0 * x at a column the row does not read: a non-finite
+ * x there makes the row's sum NaN where CSR would not). */
 int b200la_mat_set_format(b200la_mat m, int format, int param);
 int b200la_mat_get_format(b200la_mat m, int *format, int *param);
 /* SELL-C-sigma (no reference counterpart: la_global.h:56 lists an ELL format
@@ -203,8 +215,9 @@ int b200la_mat_get_format(b200la_mat m, int *format, int *param);
 int b200la_mat_to_sell(b200la_mat m, int C, int sigma, int width, int col16);
 int b200la_mat_get_sell(b200la_mat m, int *C, int *sigma, int64_t *padded);
 /* Autotuner: times every schedule on this matrix (CSR lane groups 2..32;
- * SELL and SELL16 with width 1/2/4, C = 32/16/8 and sigma 1 or 1,024,
- * sliced copies padding more than 25% skipped) and keeps the fastest.
+ * SELL and SELL16 with width 1/2/4, C = 32/16/8 and sigma 1 or 1,024;
+ * STENCIL with width 1/2/4 where the matrix has a stencil; sliced copies
+ * padding more than 25% skipped) and keeps the fastest.
  * Writes the chosen format/param and its time per SpMV in microseconds;
  * b200la_mat_get_sell gives the chosen C and sigma. */
 int b200la_mat_tune(b200la_mat m, int *format, int *param, double *usec);

@@ -14,7 +14,7 @@ import pytest
 import oracle
 from ba_b200 import lmp
 from ba_b200 import problems as P
-from ba_b200._lib import FMT_CSR, FMT_SELL, FMT_SELL16, B200LAError
+from ba_b200._lib import FMT_CSR, FMT_SELL, FMT_SELL16, FMT_STENCIL, B200LAError
 
 pytestmark = pytest.mark.gpu
 
@@ -475,7 +475,107 @@ def test_sell_c_sigma_in_the_solver_and_the_tuner(plat):
     assert cg.Solve(b, x2) == lmp.kSolverSuccess
     assert np.linalg.norm(x2.numpy() - ref.x) <= 1e-10 * np.linalg.norm(ref.x)
     fmt, prm, us = A.tune()
-    assert us > 0 and fmt in (FMT_CSR, FMT_SELL, FMT_SELL16)
+    assert us > 0 and fmt in (FMT_CSR, FMT_SELL, FMT_SELL16)  # no stencil on the ragged matrix
     if fmt != FMT_CSR:
         C, sigma = A.get_sell()
         assert C in (8, 16, 32) and sigma in (1, 1024)
+
+
+def _off_stencil(s):
+    """The system with one extra entry in a short (border) row at an offset no
+    row of the matrix has: the longest rows keep the stencil, this row leaves
+    it."""
+    lens = np.diff(s.rowptr)
+    r = int(np.flatnonzero(lens < lens.max())[0])
+    lo, hi = int(s.rowptr[r]), int(s.rowptr[r + 1])
+    cols = s.col[lo:hi]
+    c = r + int(np.abs(s.col - np.repeat(np.arange(s.n), lens)).max()) + 1
+    c = c if c < s.n else r - (c - r)
+    pos = lo + int(np.searchsorted(cols, c))
+    col = np.insert(s.col, pos, c).astype(np.int32)
+    val = np.insert(s.val, pos, 0.25)
+    rowptr = s.rowptr.copy()
+    rowptr[r + 1:] += 1
+    return P.CSRSystem(s.dim, s.cells, rowptr, col, val, s.b, s.boundary, s.name + "_off")
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_stencil_copy_gives_the_sell_bits(plat, dtype):
+    """The values-only copy (B200LA_FMT_STENCIL: no column storage, entry k
+    of a row at column row + stencil[k]) adds each row's products in its
+    stored (ascending column) order, so y = A x and y += A x are SELL's bits
+    for every width, on 2D (9-entry) and 3D (27-entry) Q1 matrices with
+    Dirichlet rows and a ragged last slice; matrices without a 9/27-entry
+    stencil are refused with B200LA_ERR_UNSUPPORTED."""
+    cases = [P.poisson_2d(40), P.q1_system(2, 37, 5, 1.0), P.q1_system(3, 11, 3, 2.0), P.q1_system(3, 6, 4, 0.5)]
+    for s in cases:
+        xs = P.uniform01(8, s.n, stream=9) - 0.5
+        A = _mat(plat, s, dtype)
+        A.set_format(FMT_SELL, 1)
+        x = _vec(plat, xs, dtype)
+        y0 = x.CloneWithoutContent()
+        A.VectorMult(x, y0)
+        ref = y0.numpy()
+        E = int(np.diff(s.rowptr).max())
+        for w in (1, 2, 4):
+            A.set_format(FMT_STENCIL, w)
+            assert A.get_format() == (FMT_STENCIL, w)
+            assert A.sell_padded() == -(-s.n // 32) * 32 * (-(-E // w) * w)
+            y = x.CloneWithoutContent()
+            A.VectorMult(x, y)
+            np.testing.assert_array_equal(y.numpy(), ref, err_msg=f"{s.name} w{w}")
+            A.VectorMultAdd(x, y)
+            np.testing.assert_array_equal(y.numpy(), (ref + ref).astype(ref.dtype))
+    for bad in (P.random_spd(300, 3, density=0.02, empty_rows=5), _ragged(2000, 5), _off_stencil(P.poisson_2d(20)),
+                _off_stencil(P.q1_system(3, 5, 1, 1.0))):
+        A = _mat(plat, bad, dtype)
+        with pytest.raises(B200LAError) as e:
+            A.set_format(FMT_STENCIL, 1)
+        assert e.value.status == -7, bad.name
+        # the matrix still works on its previous schedule
+        x = _vec(plat, np.ones(bad.n), dtype)
+        y = x.CloneWithoutContent()
+        A.VectorMult(x, y)
+        np.testing.assert_allclose(y.numpy(), oracle.spmv(bad.rowptr, bad.col, bad.val, np.ones(bad.n)),
+                                   rtol=1e-5 if dtype == np.float32 else 1e-13, atol=1e-6)
+
+
+def test_stencil_copy_in_the_solvers(plat):
+    """CG on the values-only copy takes the SELL16 path's iterations and
+    solution bits (3D Q1, FP64, Jacobi); ZeroRows rebuilds the copy with the
+    new values; the tuner may pick it on a Q1 matrix and CG then matches the
+    oracle."""
+    s = P.q1_system(3, 14, 11, 1.0)
+    b = _vec(plat, s.b)
+    out = []
+    for fmt, w in ((FMT_SELL16, 1), (FMT_STENCIL, 1), (FMT_STENCIL, 4)):
+        A = _mat(plat, s)
+        A.set_format(fmt, w)
+        x = _vec(plat, np.zeros(s.n))
+        solver = lmp.setup_CG_solver(maxits=5000, atol=0.0, rtol=1e-10, dtol=1e8)
+        solver.SetupOperator(A)
+        assert solver.Solve(b, x) == lmp.kSolverSuccess
+        out.append((solver.iter(), x.numpy()))
+    for it, xs in out[1:]:
+        assert it == out[0][0]
+        np.testing.assert_array_equal(xs, out[0][1])
+    ref = oracle.cg(s.rowptr, s.col, s.val, s.b, maxits=5000, atol=0.0, rtol=1e-10, precond=True)
+    assert abs(out[0][0] - ref.iters) <= 1
+    # ZeroRows on the values-only schedule: the copy follows the new values
+    rows = np.arange(5, s.n, 97, dtype=np.int32)
+    A1, A2 = _mat(plat, s), _mat(plat, s)
+    A1.set_format(FMT_SELL, 1)
+    A2.set_format(FMT_STENCIL, 2)
+    for A in (A1, A2):
+        A.ZeroRows(rows, 3.0)
+    assert A2.get_format() == (FMT_STENCIL, 2)
+    xv = _vec(plat, P.uniform01(2, s.n, stream=3))
+    y1, y2 = xv.CloneWithoutContent(), xv.CloneWithoutContent()
+    A1.VectorMult(xv, y1)
+    A2.VectorMult(xv, y2)
+    np.testing.assert_array_equal(y1.numpy(), y2.numpy())
+    # the tuner on a Q1 matrix: whatever it picks, the solve matches
+    A = _mat(plat, P.q1_system(2, 120, 2, 1.0))
+    fmt, prm, us = A.tune()
+    assert fmt in (FMT_CSR, FMT_SELL, FMT_SELL16, FMT_STENCIL) and us > 0
+
