@@ -139,10 +139,16 @@ struct BatchGlobals {
 // One warp's work item: rows row0 .. row0 + tile_rows - 1 of one system (the
 // last item of a system is shorter).  Items of a system are consecutive in
 // the list, so its first item is t - row0 / tile_rows and it has
-// ceil(n / tile_rows) items; tile_rows is uniform over the list.
-struct __align__(8) Tile {
+// ceil(n / tile_rows) items; tile_rows is uniform over the list.  The record
+// also carries where the system's partial sums of the previous kernel's list
+// sit (K2 items: the system's K1 items; K3 items: its K2 items), so an item
+// can load them as soon as it has its record, without first looking the
+// system's descriptor or item table up.
+struct __align__(16) Tile {
   int sys;
-  int row0;  // a multiple of tile_rows (itself a multiple of 32)
+  int row0;    // a multiple of tile_rows (itself a multiple of 32)
+  int pfirst;  // the system's first item in the previous kernel's list
+  int pcount;  // and how many items it has there
 };
 
 // Geometry of item t: rows, first item of the system, items of the system.
@@ -354,13 +360,6 @@ struct PassLists {
 // own traffic.  Both paths add the partials in a fixed order.
 constexpr int kDirectItems = 1024;
 
-// Items of a system in list k: its first item and how many there are.
-__device__ __forceinline__ void sys_items(const PassLists &L, int k, int sys, int n, int tile_rows, int *first,
-                                          int *count) {
-  *first = __ldg(L.sysfirst + 3 * sys + k);
-  *count = (n + tile_rows - 1) / tile_rows;
-}
-
 // Sum of partial slot `slot` over a system's items in list k (all lanes).
 __device__ __forceinline__ double sum_partials(const PassLists &L, int k, int slot, int first, int count) {
   const int lane = threadIdx.x & 31;
@@ -404,12 +403,11 @@ __device__ __forceinline__ void put_partials(const PassLists &L, SysState *st, i
 }
 
 // The step size of the current inner iteration from K1's partials, as K2
-// computes it.  False on breakdown (p.Ap == 0 or alpha not finite).
-__device__ __forceinline__ bool step_alpha(const PassLists &L, const BatchGlobals *g, const SysState &S, int sys,
-                                           int n, double rz, double *alpha) {
-  int f, c;
-  sys_items(L, 0, sys, n, g->tile_rows[0], &f, &c);
-  const double pap = sys_total(L, S, 0, 0, f, c);
+// computes it (tl: a K2 item, whose record locates the system's K1 items).
+// False on breakdown (p.Ap == 0 or alpha not finite).
+__device__ __forceinline__ bool step_alpha(const PassLists &L, const Tile &tl, const SysState &S, double rz,
+                                           double *alpha) {
+  const double pap = sys_total(L, S, 0, 0, tl.pfirst, tl.pcount);
   const double a = rz / pap;
   *alpha = a;
   return pap != 0.0 && isfinite(a);
@@ -631,7 +629,7 @@ __global__ void __launch_bounds__(kBlock, 4) batch_update_kernel(PassLists L, co
     const SysDesc<T> d = desc[tl.sys];
     const ItemGeo ig = item_geo(tl, t, d.n, tr);
     double alpha_d;
-    const bool ok = step_alpha(L, g, S, tl.sys, d.n, __ldg(&S.rzb[q]), &alpha_d);
+    const bool ok = step_alpha(L, tl, S, __ldg(&S.rzb[q]), &alpha_d);
     if (t == ig.first && lane == 0) {  // the step, for K3
       S.alphab[q] = ok ? alpha_d : 0.0;
       S.okb[q] = ok ? 1 : 0;
@@ -725,10 +723,8 @@ __global__ void __launch_bounds__(kBlock, 4) batch_direction_kernel(PassLists L,
       alpha_d = 0.0;  // breakdown: no step; x takes the correction so far
       state = B200LA_FAIL_BREAKDOWN;
     } else {
-      int f2, c2;
-      sys_items(L, 1, tl.sys, d.n, g->tile_rows[1], &f2, &c2);
-      const double rr = sys_total(L, S, 1, 0, f2, c2);
-      const double rzs = sys_total(L, S, 1, 1, f2, c2);
+      const double rr = sys_total(L, S, 1, 0, tl.pfirst, tl.pcount);
+      const double rzs = sys_total(L, S, 1, 1, tl.pfirst, tl.pcount);
       res = sqrt(rr);
       rz_new = PRE ? rzs : rr;
       const int it1 = it + 1;
@@ -1542,8 +1538,15 @@ int upload_tiles(BatchHandle B, bool running_only, int *count, int64_t *alg_byte
       }
     L.used = rows;
     for (int s : run) {
-      B->sysfirst_host[3 * s + k] = (int)L.host.size();
-      for (int row0 = 0; row0 < B->sys[s].n; row0 += rows) L.host.push_back(Tile{s, row0});
+      const int n = B->sys[s].n;
+      const int first = (int)L.host.size();
+      B->sysfirst_host[3 * s + k] = first;
+      // the system's items in the previous kernel's list (K1: its own)
+      const int pk = k == 0 ? 0 : k - 1;
+      const int pfirst = k == 0 ? first : B->sysfirst_host[3 * s + pk];
+      const int prows = k == 0 ? rows : B->lst[pk].used;
+      const int pcount = (n + prows - 1) / prows;
+      for (int row0 = 0; row0 < n; row0 += rows) L.host.push_back(Tile{s, row0, pfirst, pcount});
     }
   }
   cudaStream_t st = B->ctx->stream;
