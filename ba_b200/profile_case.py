@@ -12,9 +12,10 @@ bicg_s, bicg_spmv_s, bicg_update, bicg_direction per pass, the first pass a
 restart; gm_update, gm_restart, gm_spmv, gm_arnoldi per pass, the first
 pass's gm_restart building V0) instead of the CG kernels.
 
-With --batch N: builds the standard batch of N 2D systems and solves it
-twice (the launches of interest are those of the second solve; set
-B200LA_GRAPHS=0 so the kernels launch one by one).  With --profile-only the
+With --batch N: builds the standard batch of N 2D systems (bench.py's batch
+settings) and solves it --solves times (default 2; the launches of interest
+are those of the last solve; set B200LA_GRAPHS=0 so the kernels launch one by
+one), compacting every --chunk passes, with --adaptive item shrinking.  With --profile-only the
 solves are skipped: one restart pass (K1 K2 K3) is followed by three timed
 inner passes (K1 K2 K3 each), the launches a profiler should capture.
 
@@ -49,7 +50,10 @@ def main():
     ap.add_argument("--basis", type=int, default=100, help="gmres: Krylov basis size")
     ap.add_argument("--batch", type=int, default=0,
                     help="instead: solve a batch of this many 2D systems (n~logU[16,256], sigma 1) twice")
-    ap.add_argument("--chunk", type=int, default=64)
+    ap.add_argument("--chunk", type=int, default=64, help="batch: passes per graph launch (compaction in between)")
+    ap.add_argument("--adaptive", action="store_true",
+                    help="batch: shrink items while the running systems give a kernel's warps fewer than one each")
+    ap.add_argument("--solves", type=int, default=2, help="batch: solves of the whole batch (timed one by one)")
     ap.add_argument("--tile-rows", type=int, default=0)
     ap.add_argument("--index-bits", type=int, default=0, choices=[0, 16, 32],
                     help="batch: sliced-ELL columns (0 = values only when every row fits the system's stencil, "
@@ -235,10 +239,12 @@ def batch_case(a):
     for s in systems:
         B.add_system(s)
     if a.items:
-        B.set_items(*[int(v) for v in a.items.split(",")], adaptive=False)
+        B.set_items(*[int(v) for v in a.items.split(",")], adaptive=a.adaptive)
         print(f"item rows (K1, K2, K3) {B.items()}")
     else:
         rows, us = B.tune()
+        if a.adaptive:
+            B.set_items(*rows, adaptive=True)
         print(f"tuned item rows (K1, K2, K3) {rows}: pass {us:.1f} us")
     if a.profile_only:
         # launch order: K1 K2 K3 of the restart pass, then K1 K2 K3 per timed pass
@@ -246,12 +252,13 @@ def batch_case(a):
         for name, t, b in zip(("K1 spmv+p.Ap", "K2 update", "K3 direction"), ms, nb):
             print(f"{name}: {t * 1e3:.1f} us, algorithmic {b} bytes -> {b / t / 1e6:.1f} GB/s")
         return
-    for _ in range(2):
+    for _ in range(a.solves):
         B.restart()
         t = time.perf_counter()
         passes = B.solve(a.chunk)
         dt = time.perf_counter() - t
-        print(f"batch {len(systems)} systems tile_rows {a.tile_rows or 'default'} chunk {a.chunk}: "
+        print(f"batch {len(systems)} systems tile_rows {a.tile_rows or 'default'} chunk {a.chunk} "
+              f"adaptive {int(a.adaptive)}: "
               f"{passes} passes, {dt * 1e3:.1f} ms wall")
 
 
