@@ -169,34 +169,75 @@ __device__ __forceinline__ unsigned long long globaltimer() {
   return t;
 }
 
-// Deterministic per-system reduction over warp items: the warp's sums go to
-// part[k][item]; the system's last item to finish (atomic ticket over
-// `count` items) adds the system's partials in a fixed order (lane-strided
-// sums, then a shuffle tree), whatever order the items finished in.
-// Returns true in every lane of that warp, with the totals in v[] of every
-// lane.  Must be called by all 32 lanes of the warp.
+// Sum of p[0..n) over the 32 lanes of a warp, in a fixed order: lane l adds
+// p[l + 128 j + 32 u] into chain u (u = 0..3), the four chains combine in a
+// fixed tree, then the lanes in the shuffle tree.  Every caller gets the same
+// bits for the same values, and each lane keeps four loads in flight (a
+// single chain waited for one L2 round trip per 32 values: the last item of
+// a system of 6,000 items spent ~100 us on it).  Read through L2 only: other
+// warps of the same kernel wrote the values.
+// The values sit at p[0], p[step], p[2 step], ...
+__device__ __forceinline__ double warp_sum_array(const double *p, int n, int step = 1) {
+  const int lane = threadIdx.x & 31;
+  double a[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int i = lane; i < n; i += 128) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int j = i + 32 * u;
+      if (j < n) a[u] += __ldcg(p + (int64_t)j * step);
+    }
+  }
+  return warp_sum((a[0] + a[1]) + (a[2] + a[3]));
+}
+
+// Deterministic per-system reduction over warp items, in two levels so that
+// no counter takes more than kGroup atomic increments per kernel: the warp's
+// sums go to part[k][item]; the last item to finish of each group of kGroup
+// consecutive items of the system (a ticket per group, gtick[leader], the
+// leader being the group's first item) adds the group's partials into
+// gpart[k][leader]; the last group to finish (the system's ticket over its
+// groups) adds the group sums.  Both levels add in a fixed order, so the
+// totals do not depend on the order in which items finished.  (One ticket
+// for all of a system's items queued thousands of returning atomics on one
+// address: 110 of 358 us of a K1 pass over 3D systems of 0.75 M rows.)
+// Returns true in every lane of the warp that completes the system, with
+// the totals in v[] of every lane.  Must be called by all 32 lanes.  The
+// tickets wrap back to 0 by themselves (atomicInc modulus).
+constexpr int kGroup = 64;
+
 template <int NV>
-__device__ __forceinline__ bool warp_sum_last(double (&v)[NV], double *part, int64_t stride, int item, int first,
-                                              int count, unsigned *ticket) {
+__device__ __forceinline__ bool warp_sum_last(double (&v)[NV], double *part, double *gpart, unsigned *gtick,
+                                              int64_t stride, int item, int first, int count, unsigned *ticket) {
   const int lane = threadIdx.x & 31;
 #pragma unroll
   for (int k = 0; k < NV; ++k) v[k] = warp_sum(v[k]);
+  const int gi = (item - first) / kGroup;
+  const int leader = first + gi * kGroup;
+  const int gsize = min(kGroup, count - gi * kGroup);
+  const int ngroups = (count + kGroup - 1) / kGroup;
   unsigned t = 0;
   if (lane == 0) {
 #pragma unroll
     for (int k = 0; k < NV; ++k) part[k * stride + item] = v[k];
     __threadfence();
-    t = atomicInc(ticket, (unsigned)count - 1);
+    t = atomicInc(gtick + leader, (unsigned)gsize - 1);
   }
   t = __shfl_sync(0xffffffffu, t, 0);
-  if (t != (unsigned)count - 1) return false;
+  if (t != (unsigned)gsize - 1) return false;
   __threadfence();
 #pragma unroll
-  for (int k = 0; k < NV; ++k) {
-    double a = 0.0;
-    for (int i = lane; i < count; i += 32) a += __ldcg(&part[k * stride + first + i]);
-    v[k] = warp_sum(a);
+  for (int k = 0; k < NV; ++k) v[k] = warp_sum_array(part + k * stride + leader, gsize);
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) gpart[k * stride + leader] = v[k];
+    __threadfence();
+    t = atomicInc(ticket, (unsigned)ngroups - 1);
   }
+  t = __shfl_sync(0xffffffffu, t, 0);
+  if (t != (unsigned)ngroups - 1) return false;
+  __threadfence();
+#pragma unroll
+  for (int k = 0; k < NV; ++k) v[k] = warp_sum_array(gpart + k * stride + first, ngroups, kGroup);
   return true;
 }
 
@@ -349,6 +390,8 @@ namespace b200la {
 struct PassLists {
   const Tile *tiles[3];
   double *part[3];           // [3][stride] partial sums per item
+  double *gpart[3];          // [3][stride] group sums of the two-level ticket path (at group leaders)
+  unsigned *gtick[3];        // [stride] group tickets of the two-level ticket path (at group leaders)
   int64_t stride[3];
   const int *sysfirst;       // [capacity][3]: each system's first item in each list
 };
@@ -360,7 +403,9 @@ struct PassLists {
 // own traffic.  Both paths add the partials in a fixed order.
 constexpr int kDirectItems = 1024;
 
-// Sum of partial slot `slot` over a system's items in list k (all lanes).
+// Sum of partial slot `slot` over a system's items in list k (all lanes; at
+// most kDirectItems values: one chain per lane measured faster here than
+// warp_sum_array's four).
 __device__ __forceinline__ double sum_partials(const PassLists &L, int k, int slot, int first, int count) {
   const int lane = threadIdx.x & 31;
   const double *p = L.part[k] + slot * L.stride[k] + first;
@@ -396,7 +441,8 @@ __device__ __forceinline__ void put_partials(const PassLists &L, SysState *st, i
   }
   const int first = __ldg(L.sysfirst + 3 * sys + k);
   SysState &S = st[sys];
-  if (warp_sum_last<NV>(v, L.part[k], L.stride[k], item, first, count, &S.ticket[k]) && lane == 0) {
+  if (warp_sum_last<NV>(v, L.part[k], L.gpart[k], L.gtick[k], L.stride[k], item, first, count, &S.ticket[k]) &&
+      lane == 0) {
 #pragma unroll
     for (int j = 0; j < NV; ++j) S.tot[k == 0 ? 0 : 1 + j] = v[j];
   }
@@ -425,8 +471,8 @@ namespace b200la {
 // scalars.
 template <typename T, bool PRE>
 __device__ __forceinline__ void resid_item(const Tile &tl, int t, const ItemGeo &ig, const SysDesc<T> &d,
-                                           const SysDesc<T> *dg, SysState &S, double *part, int64_t part_stride,
-                                           BatchGlobals *g, const BatchParams &prm, int q) {
+                                           const SysDesc<T> *dg, SysState &S, const PassLists &L, BatchGlobals *g,
+                                           const BatchParams &prm, int q) {
   Acc<double> rr64;
   Acc<T> rrin, rzin;
   const int lane = threadIdx.x & 31;
@@ -448,7 +494,8 @@ __device__ __forceinline__ void resid_item(const Tile &tl, int t, const ItemGeo 
     }
   }
   double v[3] = {rr64.value(), rrin.value(), rzin.value()};
-  if (warp_sum_last<3>(v, part, part_stride, t, ig.first, ig.count, &S.ticket[3]) && lane == 0) {
+  if (warp_sum_last<3>(v, L.part[0], L.gpart[0], L.gtick[0], L.stride[0], t, ig.first, ig.count, &S.ticket[3]) &&
+      lane == 0) {
     const double res = sqrt(v[0]);
     S.res = res;
     if (S.outer == 0) {
@@ -605,7 +652,7 @@ __global__ void __launch_bounds__(kBlock, 4) batch_spmv_kernel(PassLists L, cons
     const SysDesc<T> d = desc[tl.sys];
     const ItemGeo ig = item_geo(tl, t, d.n, tr);
     if (ph == PH_RESID) {
-      resid_item<T, PRE>(tl, t, ig, d, desc + tl.sys, S, L.part[0], L.stride[0], g, prm, q);
+      resid_item<T, PRE>(tl, t, ig, d, desc + tl.sys, S, L, g, prm, q);
       return;
     }
     // one column type per item, so each slice loop is a straight stream
@@ -1125,6 +1172,8 @@ struct ItemList {
   int64_t cap = 0;          // device capacity (items)
   Tile *dev = nullptr;      // [cap]
   double *part = nullptr;   // [3][cap]
+  double *gpart = nullptr;  // [3][cap] group sums (two-level ticket path)
+  unsigned *gtick = nullptr;  // [cap] group tickets, zero between kernels
   std::vector<Tile> host;
 };
 
@@ -1393,6 +1442,8 @@ PassLists pass_lists(BatchHandle B) {
   for (int k = 0; k < 3; ++k) {
     L.tiles[k] = B->lst[k].dev;
     L.part[k] = B->lst[k].part;
+    L.gpart[k] = B->lst[k].gpart;
+    L.gtick[k] = B->lst[k].gtick;
     L.stride[k] = B->lst[k].cap;
   }
   L.sysfirst = B->sysfirst;
@@ -1492,11 +1543,17 @@ int ensure_items(BatchHandle B, int k, int64_t nt) {
   const int64_t cap = std::max<int64_t>(nt, 2 * L.cap);
   if (L.dev) cudaFreeAsync(L.dev, st);
   if (L.part) cudaFreeAsync(L.part, st);
+  if (L.gpart) cudaFreeAsync(L.gpart, st);
+  if (L.gtick) cudaFreeAsync(L.gtick, st);
   L.dev = nullptr;
-  L.part = nullptr;
+  L.part = L.gpart = nullptr;
+  L.gtick = nullptr;
   L.cap = 0;
   B_CUDA(cudaMallocAsync(&L.dev, sizeof(Tile) * cap, st));
   B_CUDA(cudaMallocAsync(&L.part, sizeof(double) * 3 * cap, st));
+  B_CUDA(cudaMallocAsync(&L.gpart, sizeof(double) * 3 * cap, st));
+  B_CUDA(cudaMallocAsync(&L.gtick, sizeof(unsigned) * cap, st));
+  B_CUDA(cudaMemsetAsync(L.gtick, 0, sizeof(unsigned) * cap, st));
   L.cap = cap;
   if (B->exec) {
     cudaGraphExecDestroy(B->exec);
@@ -1888,6 +1945,8 @@ int b200la_batch_destroy(b200la_batch B) {
   for (ItemList &L : B->lst) {
     if (L.dev) cudaFreeAsync(L.dev, st);
     if (L.part) cudaFreeAsync(L.part, st);
+    if (L.gpart) cudaFreeAsync(L.gpart, st);
+    if (L.gtick) cudaFreeAsync(L.gtick, st);
   }
   if (B->jobs_dev) cudaFreeAsync(B->jobs_dev, st);
   if (B->st_host) cudaFreeHost(B->st_host);
