@@ -255,7 +255,9 @@ def test_add_many_matches_single_adds_and_reports_per_system_status(plat):
 def test_large_system_ticket_path_isolated_and_converged(plat):
     # 128-row items: the 3D system has 2,350 items in K1 and K2 (more than
     # kDirectItems = 1,024), so its p.Ap and r.r/r.z totals go through the
-    # last-arriver ticket, while the small systems re-add their partials.
+    # two-level last-arriver tickets (36 full groups of 64 items and one of
+    # 46, then the system's 37 group sums), while the small systems re-add
+    # their partials.
     big = P.q1_system(3, 66, 77, 1.0, "big3d_66")
     small = [P.q1_system(2, c, 500 + c, 1.0, f"s{c}") for c in (9, 30, 64)]
     kw = dict(mixed=True, precond=True, rtol=1e-8, platform=plat)
