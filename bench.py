@@ -952,14 +952,14 @@ def run_poisson3d(args, rank, local_rank, world, torch, dist, barrier):
             "cpu_baseline": cpu}))
 
 
-# ----------------------------------------------------------------- varcoef3d workload (C3)
+# ----------------------------------------------------------------- varcoef3d workload
 def varcoef3d_config(args, s):
     return {"workload": f"3d q1 lognormal sigma=2 diffusion {args.cells}^3 cells, rel 1e-10", "n": s.n,
             "nnz": s.nnz, "l2": "inputs larger than L2 (FP32 matrix 456 MB + FP64 matrix 685 MB)"}
 
 
 def varcoef3d_fp64_iters(cells):
-    """The reference's FP64 Jacobi-PCG iteration count on the C3 system (its
+    """The reference's FP64 Jacobi-PCG iteration count on the varcoef3d system (its
     recorded run), else None."""
     rec = fullsize_fixture().get(f"varcoef3d_{cells}/jacobi/rtol1e-10")
     return rec["iters"] if rec else None
@@ -1000,7 +1000,7 @@ def run_reference_varcoef3d(args, rank):
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
 
 
-# C3 mixed precision: the FP64 residual replaces the inner one every
+# varcoef3d mixed precision: the FP64 residual replaces the inner one every
 # VARCOEF_INNER reduction (direction kept)
 VARCOEF_INNER = 0.1
 
@@ -1182,7 +1182,7 @@ def run_varcoef3d(args, rank, local_rank, world, torch, dist, barrier):
             "cpu_baseline": cpu}))
 
 
-# ----------------------------------------------------------------- more solvers on the C2 matrix
+# ----------------------------------------------------------------- more solvers on the poisson3d matrix
 BICG_METRIC = "BiCGSTAB (right Jacobi) solves/s at 1e-10 rel. residual, FP64, 3D Q1 Poisson"
 JACOBI_METRIC = "Jacobi smoother sweeps/s (SmoothNormal), FP64, 3D Q1 Poisson"
 JACOBI_SWEEPS = 100

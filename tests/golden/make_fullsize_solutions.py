@@ -3,13 +3,13 @@ fingerprints (tests/golden/reference_fullsize_solutions.json): HiFlow3's own
 lmp CPU classes (oracle/_ref, NAIVE implementation, one thread -- the exact
 CG<LAD> iteration counts) solve
 
-* poisson3d_128 (3D Q1 Poisson, 128^3 cells) and
-  varcoef3d_128 (config 3: lognormal coefficient, sigma = 2) by FP64
+* poisson3d_128 (the 3D Q1 Poisson workload, 128^3 cells) and
+  varcoef3d_128 (the same grid with a lognormal coefficient, sigma = 2) by FP64
   Jacobi-PCG to rel. 1e-10 (the iteration count and solution the device's
   FP64 solve is held to) and to rel. 1e-13 (the FP64 CPU CG oracle that
   mixed-precision results state their error against);
 * a fixed stratified sample of 32 systems of the 1,024-system batch
-  (config 4, rank 0's seed) by FP64 Jacobi-PCG to rel. 1e-12 (the oracle of
+  workload (rank 0's seed) by FP64 Jacobi-PCG to rel. 1e-12 (the oracle of
   the batch's error statement).
 
 A solution is stored as problems.solution_probe(x): its norm, 64 Rademacher

@@ -83,7 +83,7 @@ def test_fp64_pcg_matches_reference_at_full_size(plat, c2, c3, name):
 
 @pytest.mark.parametrize("mode", ["kept", "kept_f64_vectors", "restart"])
 def test_mixed_precision_error_vs_cpu_oracle_c3(plat, c3, mode):
-    """C3: FP32 inner PCG inside FP64 refinement to 1e-10 on the sigma = 2
+    """FP32 inner PCG inside FP64 refinement to 1e-10 on the 128^3 sigma = 2
     lognormal matrix -- by default each pass replaces the inner residual by
     the FP64 one every 10x reduction and keeps the search direction; also
     with FP64 inner vectors, and restarted per pass (MPIR's form, inner
@@ -116,7 +116,7 @@ def test_mixed_precision_error_vs_cpu_oracle_c3(plat, c3, mode):
 
 
 def test_batch_sample_error_vs_cpu_oracle(plat):
-    """C4: the stratified sample of 32 systems of the 1,024-system batch,
+    """The stratified sample of 32 systems of the 1,024-system batch,
     solved in one mixed-precision batch to 1e-8; each system's error against
     the reference's FP64 CG to 1e-12 is bounded, and its true residual is at
     the tolerance."""
