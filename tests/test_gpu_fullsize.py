@@ -39,12 +39,12 @@ def plat():
 
 
 @pytest.fixture(scope="module")
-def c2():
+def poisson3d():
     return P.poisson_3d(128)
 
 
 @pytest.fixture(scope="module")
-def c3():
+def varcoef3d():
     return P.varcoef_3d(128, 2.0)
 
 
@@ -66,8 +66,8 @@ def _fp64_pcg(plat, s, rtol):
 
 
 @pytest.mark.parametrize("name", ["poisson3d_128", "varcoef3d_128"])
-def test_fp64_pcg_matches_reference_at_full_size(plat, c2, c3, name):
-    s = c2 if name == "poisson3d_128" else c3
+def test_fp64_pcg_matches_reference_at_full_size(plat, poisson3d, varcoef3d, name):
+    s = poisson3d if name == "poisson3d_128" else varcoef3d
     ref = FIX[f"{name}/jacobi/rtol1e-10"]
     assert (s.n, s.nnz) == (ref["n"], ref["nnz"])
     if name == "poisson3d_128":
@@ -82,7 +82,7 @@ def test_fp64_pcg_matches_reference_at_full_size(plat, c2, c3, name):
 
 
 @pytest.mark.parametrize("mode", ["kept", "kept_f64_vectors", "restart"])
-def test_mixed_precision_error_vs_cpu_oracle_c3(plat, c3, mode):
+def test_mixed_precision_error_vs_cpu_oracle_varcoef3d(plat, varcoef3d, mode):
     """FP32 inner PCG inside FP64 refinement to 1e-10 on the 128^3 sigma = 2
     lognormal matrix -- by default each pass replaces the inner residual by
     the FP64 one every 10x reduction and keeps the search direction; also
@@ -92,7 +92,7 @@ def test_mixed_precision_error_vs_cpu_oracle_c3(plat, c3, mode):
     1e-10, and the FP64 true residual to the tolerance.  Kept directions stay
     within 1.3x the reference's FP64 iteration count (685); restarts discard
     the Krylov space every pass and take ~1.5x."""
-    s = c3
+    s = varcoef3d
     oracle13 = FIX["varcoef3d_128/jacobi/rtol1e-13"]["probe"]
     ref_err = P.probe_error(FIX["varcoef3d_128/jacobi/rtol1e-10"]["probe"], oracle13)
     A = lmp.B200_CSR_lMatrix(s.rowptr, s.col, s.val, platform=plat)

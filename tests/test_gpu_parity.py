@@ -277,7 +277,7 @@ def test_cg_state_semantics(plat):
     np.testing.assert_array_equal(x1.numpy(), x2.numpy())
 
 
-def test_cg_c1_full_size(plat):
+def test_cg_poisson2d_256_full_size(plat):
     """Config-1 system (2D Q1 Poisson 256^2, 66,049 DOFs) at rel 1e-10."""
     s = P.poisson_2d(256)
     ref = oracle.cg(s.rowptr, s.col, s.val, s.b, maxits=5000, atol=0.0, rtol=1e-10)
@@ -306,7 +306,7 @@ def test_cg_3d_vs_oracle(plat):
     assert np.linalg.norm(x.numpy() - ref.x) <= 1e-10 * np.linalg.norm(ref.x) * 10
 
 
-def test_full_size_c2_properties(plat):
+def test_full_size_poisson3d_128_properties(plat):
     """128^3 Q1 Poisson (2,146,689 DOFs, 57,066,625 nnz): size-independent
     checks -- SpMV against scipy's CSR product, linearity, and a converged
     true residual."""

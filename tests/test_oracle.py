@@ -133,7 +133,7 @@ def test_mpir_reaches_fp64_solution():
 
 
 def test_generator_shapes():
-    # C1: 256^2 cells -> 66,049 DOFs, 591,361 nnz; Q1 counts (3n+1)^d nnz
+    # 2D Poisson, 256^2 cells -> 66,049 DOFs, 591,361 nnz; Q1 counts (3n+1)^d nnz
     c1 = P.poisson_2d(256)
     assert c1.n == 66049 and c1.nnz == 591361
     for n in (4, 9, 13):
