@@ -278,7 +278,7 @@ def test_cg_state_semantics(plat):
 
 
 def test_cg_poisson2d_256_full_size(plat):
-    """Config-1 system (2D Q1 Poisson 256^2, 66,049 DOFs) at rel 1e-10."""
+    """2D Q1 Poisson, 256^2 cells (66,049 DOFs), at rel 1e-10."""
     s = P.poisson_2d(256)
     ref = oracle.cg(s.rowptr, s.col, s.val, s.b, maxits=5000, atol=0.0, rtol=1e-10)
     A = _mat(plat, s)
