@@ -3,9 +3,10 @@ GPU (torch.distributed; NCCL on GPUs, gloo in the CPU tests).
 
 The batched and served workloads are sets of independent solves, so their
 ranks never exchange solver data: each rank owns its share of the systems (its
-own seeded batch or request stream, or a cost-balanced part of one batch from
-partition_by_cost) and only one scalar -- the step time -- is reduced, as the
-maximum over ranks.  The reference's multi-rank path, one system partitioned
+own seeded batch or request stream, a cost-balanced part of one batch from
+partition_by_cost, or its share of one request stream routed by route_jsq)
+and only one scalar -- the step time -- is reduced, as the maximum over
+ranks.  The reference's multi-rank path, one system partitioned
 by rows with a ghost halo (CoupledVector/CoupledMatrix,
 linear_algebra/coupled_vector.cc:890-973), lives in ba_b200/coupled.py.
 """
@@ -36,6 +37,39 @@ def partition_by_cost(costs, world: int) -> list[list[int]]:
         parts[r].append(i)
         heapq.heappush(heap, (load + float(costs[i]), r))
     return [sorted(p) for p in parts]
+
+
+def route_jsq(times, costs, world: int, drain_rate: float) -> list[int]:
+    """Route one request stream over `world` ranks, join the shortest queue
+    by outstanding work: request i arrives at times[i] (seconds, ascending)
+    with work costs[i] (e.g. its matrix nonzeros); every rank is a server
+    that works its backlog off at `drain_rate` cost units per second (0:
+    never, so the rule becomes least assigned work); the request goes to the
+    rank with the least backlog at its arrival; ties (idle ranks, at light
+    load) to the least work assigned so far, then to the lower rank.
+    Depends only on the stream, so every rank computes the same routing
+    without a message; a front end would run the same rule online with the
+    servers' reported backlogs.  Returns each request's rank."""
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    if len(times) != len(costs):
+        raise ValueError("times and costs differ in length")
+    backlog = [0.0] * world
+    assigned = [0.0] * world
+    last = None
+    out = []
+    for t, c in zip(times, costs):
+        if last is not None:
+            if t < last:
+                raise ValueError("arrival times must be ascending")
+            done = float(drain_rate) * (t - last)
+            backlog = [max(0.0, b - done) for b in backlog]
+        last = t
+        r = min(range(world), key=lambda k: (backlog[k], assigned[k], k))
+        backlog[r] += float(c)
+        assigned[r] += float(c)
+        out.append(r)
+    return out
 
 
 def _reduce(value: float, op: str, device: str) -> float:

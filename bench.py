@@ -79,7 +79,9 @@ def parse():
                          "(default: 0.1)")
     ap.add_argument("--split", action="store_true",
                     help="batch: partition ONE 1,024-system batch over the ranks by nnz (greedy, largest first; "
-                         "strong scaling) instead of one seeded batch per rank (weak scaling)")
+                         "strong scaling) instead of one seeded batch per rank (weak scaling); serve: route ONE "
+                         "request stream (N times the requests) over the ranks, join-shortest-queue by "
+                         "outstanding nonzeros")
     ap.add_argument("--full-stream", action="store_true",
                     help="serve: also serve the whole seeded request stream at the latency stream's arrival rate")
     ap.add_argument("--stream-count", type=int, default=20000, help="serve --full-stream: requests of the stream")
@@ -659,7 +661,21 @@ def run_serve(args, rank, local_rank, world, torch, dist, barrier):
     kw = dict(rtol=BATCH_RTOL, atol=0.0, dtol=1e8, inner_rtol=inner_rtol, max_outer=60, chunk_passes=CHUNK,
               platform=plat)
     R = args.requests
-    timed = serve_sample(args.steps * R, args.hi_dofs, rank, part=0)
+    split = args.split and world > 1
+
+    def req_cost(rq):  # a request's work: its matrix nonzeros (9 or 27 per row)
+        return rq["dofs"] * (9 if rq["dim"] == 2 else 27)
+
+    def my_share(reqs, drain_rate):
+        # every rank routes the same global stream the same way and keeps its part
+        route = D.route_jsq([rq.get("t", 0.0) for rq in reqs], [req_cost(rq) for rq in reqs], world, drain_rate)
+        return [rq for rq, r in zip(reqs, route) if r == rank]
+
+    if split:
+        all_timed = serve_sample(world * args.steps * R, args.hi_dofs, 0, part=0)
+        timed = my_share(all_timed, 0.0)
+    else:
+        timed = serve_sample(args.steps * R, args.hi_dofs, rank, part=0)
     warm = serve_requests(args.warmup * 4, 1.0, 2e4, rank, offset=50000)
     S = Server(SERVE_CAPACITY, mixed=True, precond=True, **kw)
     for w in range(args.warmup):
@@ -680,13 +696,19 @@ def run_serve(args, rank, local_rank, world, torch, dist, barrier):
     st_sat = S.stats()
     ms_max = D.max_over_ranks(e0.elapsed_time(e1))
     value = world * args.steps * R / (ms_max / 1e3)
+    # work a GPU drains per second at saturation (the split streams' routing)
+    drain = (sum(req_cost(rq) for rq in all_timed) / world if split else 0.0) / (ms_max / 1e3)
     ok = sum(1 for r, _ in results if r.solver_state == 0)
     d2h = int(sum(r.x.nbytes for r, _ in results)) // args.steps
     h2d = 4 * 8 * R  # request descriptors per step: dim, cells, seed, sigma
 
     # latency under a Poisson stream at a fraction of the measured throughput
     rate = max(args.load * value / world, 1e-3)
-    lat_reqs = serve_sample(args.latency_requests, args.hi_dofs, rank, part=1, rate=rate)
+    if split:
+        lat_reqs = my_share(serve_sample(world * args.latency_requests, args.hi_dofs, 0, part=1, rate=world * rate),
+                            drain)
+    else:
+        lat_reqs = serve_sample(args.latency_requests, args.hi_dofs, rank, part=1, rate=rate)
     S.reset_stats()
     lat_res = _serve_stream(S, lat_reqs, paced=True)
     st_lat = S.stats()
@@ -696,7 +718,10 @@ def run_serve(args, rank, local_rank, world, torch, dist, barrier):
     if args.full_stream:
         # the whole seeded stream, Poisson arrivals at the same fraction of the
         # measured throughput; only the result records are kept
-        full_reqs = serve_requests(args.stream_count, rate, args.hi_dofs, rank)
+        if split:
+            full_reqs = my_share(serve_requests(args.stream_count, world * rate, args.hi_dofs, 0), drain)
+        else:
+            full_reqs = serve_requests(args.stream_count, rate, args.hi_dofs, rank)
         S.reset_stats()
         f0 = time.monotonic()
         pending, full_rs = [], []
@@ -768,7 +793,9 @@ def run_serve(args, rank, local_rank, world, torch, dist, barrier):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
             "config": serve_config(args),
             "details": {
-                "parallelism": f"replicas x{world}",
+                "parallelism": (f"split x{world}: one request stream ({world}x the requests) routed over the "
+                                f"ranks, join-shortest-queue by outstanding nonzeros" if split
+                                else f"replicas x{world}"),
                 "server": f"FP32 Jacobi-PCG inner solves in FP64 refinement (residual replaced every "
                           f"{inner_rtol:g}x, direction kept), admitted by free HBM into {SERVE_CAPACITY} slots, "
                           f"continuous batching",

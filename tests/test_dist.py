@@ -76,3 +76,29 @@ def test_single_process_reductions_are_identity():
     assert D.max_over_ranks(3.5, device="cpu") == 3.5
     assert D.sum_over_ranks(2.0, device="cpu") == 2.0
     assert D.rank_seed(10, 0) == 10 and D.rank_seed(10, 3) == 10 + 3 * D.SEED_STRIDE
+
+
+def test_route_jsq_balances_outstanding_work():
+    # all at once: least assigned work, in arrival order, ties to the lower rank
+    assert D.route_jsq([0.0] * 5, [5, 3, 3, 1, 1], 2, 1.0) == [0, 1, 1, 0, 0]
+    # backlogs drain: at t = 5 rank 0 still holds 3 units, rank 1 none
+    assert D.route_jsq([0.0, 0.0, 5.0], [8, 2, 1], 2, 1.0) == [0, 1, 1]
+    # both idle again at t = 20: the one assigned less work so far
+    assert D.route_jsq([0.0, 0.0, 20.0], [2, 8, 1], 2, 1.0) == [0, 1, 0]
+    # a served stream: every request is routed, the split is deterministic,
+    # and the ranks' total work stays within one large request of each other
+    import numpy as np
+    rng = np.random.default_rng(5)
+    times = np.cumsum(rng.exponential(0.02, 400))
+    costs = np.exp(rng.uniform(np.log(1e3), np.log(2e6), 400))
+    for world in (1, 2, 4):
+        r = D.route_jsq(times, costs, world, 0.5 * world * costs.sum() / times[-1])
+        assert len(r) == 400 and set(r) <= set(range(world))
+        assert r == D.route_jsq(times, costs, world, 0.5 * world * costs.sum() / times[-1])
+        loads = [costs[np.array(r) == k].sum() for k in range(world)]
+        assert max(loads) - min(loads) <= 2 * costs.max()
+    with pytest.raises(ValueError):
+        D.route_jsq([1.0, 0.5], [1, 1], 2, 1.0)
+    with pytest.raises(ValueError):
+        D.route_jsq([0.0], [1], 0, 1.0)
+
