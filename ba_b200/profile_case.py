@@ -13,7 +13,7 @@ restart; gm_update, gm_restart, gm_spmv, gm_arnoldi per pass, the first
 pass's gm_restart building V0) instead of the CG kernels.
 
 With --batch N: builds the standard batch of N 2D systems (bench.py's batch
-settings) and solves it --solves times (default 2; the launches of interest
+settings; --batch-dim 3: N device-assembled 3D systems instead) and solves it --solves times (default 2; the launches of interest
 are those of the last solve; set B200LA_GRAPHS=0 so the kernels launch one by
 one), compacting every --chunk passes, with --adaptive item shrinking.  With --profile-only the
 solves are skipped: one restart pass (K1 K2 K3) is followed by three timed
@@ -51,6 +51,9 @@ def main():
     ap.add_argument("--batch", type=int, default=0,
                     help="instead: solve a batch of this many 2D systems (n~logU[16,256], sigma 1) twice")
     ap.add_argument("--chunk", type=int, default=64, help="batch: passes per graph launch (compaction in between)")
+    ap.add_argument("--batch-dim", type=int, default=2, choices=[2, 3],
+                    help="batch: 2 = bench.py's 2D batch; 3 = 3D Q1 systems of 40..90 cells per axis (cycled), "
+                         "assembled on the device")
     ap.add_argument("--adaptive", action="store_true",
                     help="batch: shrink items while the running systems give a kernel's warps fewer than one each")
     ap.add_argument("--solves", type=int, default=2, help="batch: solves of the whole batch (timed one by one)")
@@ -229,15 +232,26 @@ def solver_case(a, s, A, dt, fmt, prm, us, alg, sv):
         print(f"{a.solver} {name}: {ms[k]:.4f} ms, algorithmic {nbytes} bytes -> {nbytes / ms[k] / 1e6:.1f} GB/s")
 
 
+BATCH3D_CELLS = (40, 50, 60, 70, 80, 90)  # --batch-dim 3: cells per axis, cycled
+
+
 def batch_case(a):
     from .batch import Batch
-    systems = P.batch_systems(a.batch, sigma=1.0, seed=P.SEED_BATCH)
     plat = lmp.init_platform(0)
+    count = a.batch
     # the settings of bench.py's batch workload
-    B = Batch(len(systems), mixed=True, precond=True, rtol=1e-8, atol=0.0, dtol=1e8, inner_rtol=0.1, max_outer=60,
+    B = Batch(count, mixed=True, precond=True, rtol=1e-8, atol=0.0, dtol=1e8, inner_rtol=0.1, max_outer=60,
               tile_rows=a.tile_rows, index_bits=a.index_bits, platform=plat)
-    for s in systems:
-        B.add_system(s)
+    if a.batch_dim == 3:
+        # 3D Q1 systems (27 entries per row) of 41^3 .. 91^3 nodes, lognormal
+        # kappa sigma 1, assembled on the device (the served stream's 3D kind)
+        for i in range(count):
+            B.add_q1(3, BATCH3D_CELLS[i % len(BATCH3D_CELLS)], 100 + i, 1.0)
+        systems = list(range(count))
+    else:
+        systems = P.batch_systems(count, sigma=1.0, seed=P.SEED_BATCH)
+        for s in systems:
+            B.add_system(s)
     if a.items:
         B.set_items(*[int(v) for v in a.items.split(",")], adaptive=a.adaptive)
         print(f"item rows (K1, K2, K3) {B.items()}")
