@@ -574,7 +574,17 @@ def test_stencil_copy_in_the_solvers(plat):
     A1.VectorMult(xv, y1)
     A2.VectorMult(xv, y2)
     np.testing.assert_array_equal(y1.numpy(), y2.numpy())
-    # the tuner on a Q1 matrix: whatever it picks, the solve matches
+    # CastTo keeps the schedule: the FP32 copy is values-only too, with the
+    # FP32 SELL copy's bits
+    A3 = A2.CastTo(np.float32)
+    assert A3.get_format() == (FMT_STENCIL, 2) and A3.get_sell() == (32, 1)
+    x32 = _vec(plat, P.uniform01(4, s.n, stream=5), np.float32)
+    y3, y4 = x32.CloneWithoutContent(), x32.CloneWithoutContent()
+    A3.VectorMult(x32, y3)
+    A3.set_format(FMT_SELL, 1)
+    A3.VectorMult(x32, y4)
+    np.testing.assert_array_equal(y3.numpy(), y4.numpy())
+    # the tuner on a Q1 matrix keeps one of the schedules it timed
     A = _mat(plat, P.q1_system(2, 120, 2, 1.0))
     fmt, prm, us = A.tune()
     assert fmt in (FMT_CSR, FMT_SELL, FMT_SELL16, FMT_STENCIL) and us > 0
