@@ -72,6 +72,15 @@ def route_jsq(times, costs, world: int, drain_rate: float) -> list[int]:
     return out
 
 
+def stream_share(reqs, world: int, rank: int, drain_rate: float, cost) -> list:
+    """This rank's part of one request stream routed by route_jsq: reqs are
+    dicts with an arrival time "t" (0 when absent: all at once), cost(req)
+    their work.  Every rank gets a disjoint part; together they are the
+    stream, each part in arrival order."""
+    route = route_jsq([rq.get("t", 0.0) for rq in reqs], [cost(rq) for rq in reqs], world, drain_rate)
+    return [rq for rq, r in zip(reqs, route) if r == rank]
+
+
 def _reduce(value: float, op: str, device: str) -> float:
     import torch
     import torch.distributed as dist

@@ -668,8 +668,7 @@ def run_serve(args, rank, local_rank, world, torch, dist, barrier):
 
     def my_share(reqs, drain_rate):
         # every rank routes the same global stream the same way and keeps its part
-        route = D.route_jsq([rq.get("t", 0.0) for rq in reqs], [req_cost(rq) for rq in reqs], world, drain_rate)
-        return [rq for rq, r in zip(reqs, route) if r == rank]
+        return D.stream_share(reqs, world, rank, drain_rate, req_cost)
 
     if split:
         all_timed = serve_sample(world * args.steps * R, args.hi_dofs, 0, part=0)

@@ -38,10 +38,13 @@ def _rank_main(rank, world, port, out_dir):
         mx = D.max_over_ranks(my_ms, device="cpu")
         total = D.sum_over_ranks(len(sizes), device="cpu")
         rate = D.aggregate_rate(len(sizes), world, mx)
+        # one served stream, routed alike on every rank: this rank's share
+        stream = P.serve_stream(300, rate=40.0, hi_dofs=2e5, seed=P.SEED_SERVE)
+        share = D.stream_share(stream, world, rank, 5e6, lambda rq: rq["dofs"] * (9 if rq["dim"] == 2 else 27))
         dist.barrier()
         with open(os.path.join(out_dir, f"rank{rank}.json"), "w") as f:
             json.dump({"seed": seed, "sizes": [int(x) for x in sizes], "parts": parts, "max": mx,
-                       "total": total, "rate": rate}, f)
+                       "total": total, "rate": rate, "share": [rq["seed"] for rq in share]}, f)
     finally:
         dist.destroy_process_group()
 
@@ -57,6 +60,9 @@ def test_two_gloo_ranks(tmp_path):
     assert r[0]["max"] == r[1]["max"] == 125.0
     assert r[0]["total"] == r[1]["total"] == 128
     assert r[0]["rate"] == pytest.approx(2 * 64 / 0.125)
+    # the routed stream: disjoint shares that together are the whole stream
+    a, b = set(r[0]["share"]), set(r[1]["share"])
+    assert a and b and not (a & b) and len(a) + len(b) == 300
 
 
 def test_partition_by_cost_is_balanced_and_complete():
