@@ -245,7 +245,8 @@ def batch_config(args, systems):
     return {"workload": f"batched: {len(systems)} independent 2D Q1 systems, n~logU[16,256] cells, "
                         f"lognormal kappa sigma=1, rel. residual 1e-8",
             "systems": len(systems), "dofs_total": n_tot, "nnz_total": nnz_tot,
-            "l2": "inputs larger than L2 (1.3 GB FP64 CSR + 0.9 GB FP32 values per batch)"}
+            "l2": "inputs larger than L2 (per batch: 1.4 GB FP64 CSR as uploaded, 0.47 GB FP32 and 0.93 GB "
+                  "FP64 sliced values)"}
 
 
 def batch_cpu_sample_text(args, pick, nthreads):
